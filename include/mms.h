@@ -1,0 +1,238 @@
+/*
+ * mms.h — C ABI of mumatscale_b200, a B200-native implementation of the
+ * muMatScale cellular-automaton solidification step.
+ *
+ * The reference's hot path is a set of C functions over one subblock
+ * (SB_struct *lsp) and the global configuration (BB_struct *bp), called in a
+ * fixed order by doiteration() (calculate.c:193-352) from the time loop
+ * (loop.c:186-271).  This header replaces that boundary: a caller (the C
+ * host loop, a Python script, another language through its FFI) creates one
+ * context per GPU from the parsed input deck, advances it by whole
+ * timesteps, and reads fields, reductions and the grain table back.  All
+ * device memory belongs to the context; all host buffers belong to the
+ * caller.  Calls on one context are ordered on one internal CUDA stream and
+ * are not thread-safe for that context.  Every call returns an mms_status;
+ * nothing in the library exits the process (the reference aborts through
+ * error(), debug.h:54-58).
+ *
+ * The domain is the reference's global grid: NSubblocks x NCellsPerSB cells
+ * held as one device-resident array with a one-cell halo, indexed exactly
+ * like growth.c:70 on a single subblock:
+ *     idx = k*(gdimy+2)*(gdimx+2) + j*(gdimx+2) + i,  i,j,k in [0, gdim+1]
+ * with interior cells at 1..gdim.  When NSubblocks is not 1 1 1 the library
+ * still runs one domain, and reproduces the per-rank orderings of the
+ * reference's MPI run (grain ids, rand() streams, interface-list slots), so
+ * results match the reference run on that many ranks.
+ */
+#ifndef MMS_H
+#define MMS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MMS_ABI_VERSION 1
+
+typedef enum mms_status {
+    MMS_OK = 0,
+    MMS_ERR_ARG = 1,             /* invalid argument or unsupported option */
+    MMS_ERR_CUDA = 2,            /* a CUDA runtime call failed */
+    MMS_ERR_NO_DEVICE = 3,       /* no usable sm_100 device */
+    MMS_ERR_COURANT = 4,         /* Dsol/Dliq*dt/dx^2 > CourantLimit (growth.c:43-50) */
+    MMS_ERR_NEGATIVE_CE = 5,     /* ce < 0 after diffusion (growth.c:163-165) */
+    MMS_ERR_GRAIN_OVERFLOW = 6,  /* grain id beyond MaxTotGrains (grain.c:363-366) */
+    MMS_ERR_DECK = 7,            /* input deck could not be parsed (read_ctrl.c) */
+    MMS_ERR_IO = 8,              /* a file could not be written or read */
+    MMS_ERR_TIMEOUT = 9,         /* a bounded device-side wait expired */
+    MMS_ERR_STATE = 10,          /* call made in the wrong state */
+    MMS_ERR_NOMEM = 11           /* device or host allocation failed */
+} mms_status;
+
+typedef enum mms_precision {
+    MMS_PREC_F64 = 0,  /* plain form: all fields FP64, bit-exact to the reference */
+    MMS_PREC_F32 = 1   /* FP32 bulk ce/cl/fs; FP64 octahedra, thresholds, reductions */
+} mms_precision;
+
+/* FixedNuc x y z ax ay az threshold (read_ctrl.c:298-310); angles in degrees */
+typedef struct mms_fixed_nuc {
+    double x, y, z, ax, ay, az, threshold;
+} mms_fixed_nuc;
+
+/* NucVolume density[%] minx miny minz maxx maxy maxz threshold
+ * (read_ctrl.c:311-330); density is stored as a fraction (value/100) */
+typedef struct mms_nuc_volume {
+    double density, minx, miny, minz, maxx, maxy, maxz, threshold;
+} mms_nuc_volume;
+
+/* The subset of BB_struct (globals.h:273-403) that the hot path, its setup
+ * and the time loop read.  Names follow the reference. */
+typedef struct mms_params {
+    /* grid */
+    int gnsbx, gnsby, gnsbz;          /* NSubblocks */
+    int gsdimx, gsdimy, gsdimz;       /* NCellsPerSB */
+    int padBndyX, padBndyY, padBndyZ; /* FaceCtrl: 1 = pad (mold), 0 = wrap */
+    double origin_offset[3];
+    double cellSize;
+    double courant_limit;
+    unsigned int base_random_seed;    /* RandSeedVal */
+    /* time and termination */
+    double ts_delt;                   /* TimeStep */
+    double finish_time;               /* FinishTime (0 = off) */
+    double fs_finish;                 /* FsFinish */
+    /* growth */
+    double fsgrow, rev_fsgrow;        /* FSGrow, 1/FSGrow */
+    /* curvature */
+    int tip_curv;                     /* TipCurvature */
+    double gibbs_coef;                /* GibbsThomsonCoef */
+    /* alloy */
+    double liquidusTemp, solidusTemp, Cinit;
+    double m_solute0, m_solute0_a, m_solute0_b, m_solute0_c;
+    double part_coef, part_coef_a, part_coef_b, part_coef_c;
+    double Dsol, Dliq;
+    /* internal temperature (internal_temp_ctrl_t, globals.h:256-269) */
+    double initialTemperature, gradient, velocity, grad_coef, velo_coef, cool_rate;
+    /* laser analytical thermal model */
+    int thermal_ana, am, amlayer, amtracks;
+    double lpow, lv, lsd, lab, lhs, liniT, lthcon, lcp, rho, x0, y0, z0;
+    /* nucleation */
+    double maxGrainDensity, gnGaussCenter, gnGaussSigma;
+    double maxGrainDensitySurf, gnGaussCenterSurf, gnGaussSigmaSurf;
+    int doSurfaceNuc;                 /* MouldNuc */
+    int gnUseOrientation;             /* GNOriented */
+    uint64_t maxTotalGrains;          /* MaxTotGrains */
+    /* output and time loop */
+    int screenpfreq, data_write_freq, data_write_start, randomize_grains;
+    int vis_format;                   /* 0 none, 1 VTK, 2 XDMF */
+    char basefilename[256];
+    /* nucleation lists from the deck (owned by whoever filled them) */
+    const mms_fixed_nuc *fixed_nucs;
+    int n_fixed_nucs;
+    const mms_nuc_volume *nuc_volumes;
+    int n_nuc_volumes;
+    /* build options of this library */
+    int precision;                    /* mms_precision */
+    int device;                       /* CUDA device ordinal */
+} mms_params;
+
+typedef enum mms_field {
+    MMS_FIELD_CE = 0,            /* f64 [N]   equivalent concentration */
+    MMS_FIELD_CL = 1,            /* f64 [N]   liquid concentration */
+    MMS_FIELD_FS = 2,            /* f64 [N]   fraction solid */
+    MMS_FIELD_GR = 3,            /* i32 [N]   grain id, 0 = liquid */
+    MMS_FIELD_DC = 4,            /* f64 [3N]  octahedron centre offset, x,y,z per cell */
+    MMS_FIELD_D = 5,             /* f64 [N]   half diagonal (download only; grain cells) */
+    MMS_FIELD_NUC_THRESHOLD = 6, /* f32 [N]   nucleation undercooling, +inf = no site */
+    MMS_FIELD_TEMPERATURE = 7,   /* f64 [N]   temperature at the current timestep (download only) */
+    MMS_FIELD_MOLD = 8           /* i8  [N]   mold flag (download only) */
+} mms_field;
+
+typedef enum mms_reduction {
+    MMS_REDUCE_FS_FRACTION = 0,  /* computeFS (loop.c:173-183): sum min(1,fs) dx^3 / total volume */
+    MMS_REDUCE_SOLID_VOLUME = 1, /* solid_volume (growth.c:971-978) */
+    MMS_REDUCE_CE_SUM = 2        /* sum of ce over interior cells, compensated in FP64 */
+} mms_reduction;
+
+/* grain_t (globals.h:244-254) */
+typedef struct mms_grain {
+    double nuc_x, nuc_y, nuc_z;
+    uint64_t nuc_timestep;
+    double nuc_threshold;
+    double rotmat[3][3];
+    double rotang[3];
+} mms_grain;
+
+typedef struct mms_grain_summary {
+    int num_grains;              /* bp->num_grains - 1 */
+    double min_mm3, max_mm3, avg_mm3;
+} mms_grain_summary;
+
+typedef struct mms_ctx mms_ctx;
+
+/* ---- configuration (read_ctrl.c) ------------------------------------------ */
+
+/* set_defaults (read_ctrl.c:29-108). */
+mms_status mms_params_default(mms_params *p);
+
+/* read_config (read_ctrl.c:234-812) on top of *p, including GeoFileName /
+ * MatFileName / AlloyPropsFile0 includes.  FixedNuc and NucVolume lines are
+ * appended to heap arrays released by mms_params_free_lists(). */
+mms_status mms_deck_read(const char *path, mms_params *p);
+void mms_params_free_lists(mms_params *p);
+
+/* ---- context lifetime ------------------------------------------------------ */
+
+/* Allocates the device-resident domain and applies the reference's initial
+ * state: allocateFields + SetupInitialConditions (setup.c:41-236), the
+ * nucleation sites of init_nucleation_sites (grain.c:602-713) and
+ * init_sb_nucleation (grain.c:930-1010), each emulated rank drawing from its
+ * own srand(rank+1+seed) stream (ca_main.c:215).  Checks the Courant limit
+ * (growth.c:43-50).  The step counter starts at 0 (findStartTime,
+ * functions.c:512-576, always yields 0). */
+mms_status mms_create(const mms_params *p, mms_ctx **out);
+mms_status mms_destroy(mms_ctx *ctx);
+
+/* ---- stepping (doiteration, calculate.c:193-352) --------------------------- */
+
+/* Advances nsteps timesteps.  Each step increments the step counter and then
+ * runs, in the reference's order: temperature, nucleation scan
+ * (grain.c:1043), grain activation (grain.c:841), diffusion (growth.c:30),
+ * Gibbs-Thomson curvature when TipCurvature is 1 (curvature.c:31),
+ * fraction-solid change (growth.c:177), octahedron growth (growth.c:339),
+ * interface list (growth.c:461) and capture (growth.c:574). */
+mms_status mms_step(mms_ctx *ctx, int nsteps);
+
+mms_status mms_get_timestep(mms_ctx *ctx, uint64_t *timestep);
+/* bp->num_grains: grains created so far plus the "zero" grain */
+mms_status mms_get_num_grains(mms_ctx *ctx, int *num_grains);
+
+/* ---- fields and reductions ------------------------------------------------- */
+
+/* Copies a whole halo'd field between the device and a caller buffer in the
+ * layout described above.  N = (gdimx+2)(gdimy+2)(gdimz+2). */
+size_t mms_num_cells(const mms_ctx *ctx);
+mms_status mms_download(mms_ctx *ctx, mms_field field, void *host);
+mms_status mms_upload(mms_ctx *ctx, mms_field field, const void *host);
+mms_status mms_reduce(mms_ctx *ctx, mms_reduction what, double *out);
+
+/* ---- sites and orientations ------------------------------------------------ */
+
+/* Replaces every nucleation threshold: cells listed get the given threshold
+ * (0-based global interior cell coordinates), every other cell +inf.  This is
+ * what a pre-drawn site list injects in place of init_sb_nucleation. */
+mms_status mms_set_sites(mms_ctx *ctx, int64_t n, const int32_t *gxyz,
+                         const float *thresholds);
+/* Orientation override for grains that nucleate at the listed cells: their
+ * rotation matrix (row-major 3x3) replaces the one createGrains would build
+ * (grain.c:348-425); rand() is still consumed as in the reference. */
+mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxyz,
+                                     const double *rotmat9);
+
+/* ---- grain table and results ----------------------------------------------- */
+
+mms_status mms_get_grains(mms_ctx *ctx, int first, int count, mms_grain *out);
+/* output_grains (grain.c:751-833): writes <basefilename>_grains.csv when path
+ * is non-NULL and returns the summary line's numbers. */
+mms_status mms_output_grains(mms_ctx *ctx, const char *path, mms_grain_summary *out);
+
+/* ---- the time loop (loop.c:186-271) ----------------------------------------- */
+
+/* Runs the reference time loop to its termination (FinishTime / FsFinish,
+ * checked with the fraction solid refreshed every ScreenPFreq steps),
+ * printing the reference's screen lines and grain summary to stdout when
+ * verbose is non-zero. */
+mms_status mms_run(mms_ctx *ctx, int verbose);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+const char *mms_status_string(mms_status s);
+/* The most recent error message on this context (empty when none). */
+const char *mms_last_error(const mms_ctx *ctx);
+/* Number of device kernels this context has launched since creation. */
+uint64_t mms_kernel_launches(const mms_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MMS_H */

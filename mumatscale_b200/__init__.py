@@ -1,0 +1,312 @@
+"""mumatscale_b200 — B200-native muMatScale CA solidification step.
+
+The compute lives in the in-tree C-ABI library ``libmms_b200.so``
+(include/mms.h): hand-written sm_100a kernels plus their host side.  This
+module only binds that library with ctypes and mirrors the reference's
+interfaces: an input deck (read_ctrl.c) becomes :class:`Params`, a
+:class:`Domain` owns the device-resident fields of one GPU and advances
+them by whole timesteps (doiteration, calculate.c:193-352), and
+:meth:`Domain.run` is the reference time loop (loop.c:186-271).
+
+There is no CPU fallback: if the library or a CUDA device is missing, the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = [
+    "Params", "FixedNuc", "NucVolume", "Grain", "GrainSummary", "Domain", "MmsError",
+    "load_library", "library_path", "FIELD", "PREC_F64", "PREC_F32",
+]
+
+_PKG = Path(__file__).resolve().parent
+PREC_F64 = 0
+PREC_F32 = 1
+
+FIELD = {
+    "ce": 0, "cl": 1, "fs": 2, "gr": 3, "dc": 4, "d": 5,
+    "nuc_threshold": 6, "temperature": 7, "mold": 8,
+}
+_FIELD_DTYPE = {
+    0: (np.float64, 1), 1: (np.float64, 1), 2: (np.float64, 1), 3: (np.int32, 1),
+    4: (np.float64, 3), 5: (np.float64, 1), 6: (np.float32, 1), 7: (np.float64, 1),
+    8: (np.int8, 1),
+}
+REDUCE = {"fs_fraction": 0, "solid_volume": 1, "ce_sum": 2}
+
+
+class FixedNuc(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("x", "y", "z", "ax", "ay", "az", "threshold")]
+
+
+class NucVolume(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("density", "minx", "miny", "minz", "maxx", "maxy", "maxz", "threshold")]
+
+
+class Params(C.Structure):
+    """mms_params: the BB_struct subset (globals.h:273-403) the hot path reads."""
+    _fields_ = [
+        ("gnsbx", C.c_int), ("gnsby", C.c_int), ("gnsbz", C.c_int),
+        ("gsdimx", C.c_int), ("gsdimy", C.c_int), ("gsdimz", C.c_int),
+        ("padBndyX", C.c_int), ("padBndyY", C.c_int), ("padBndyZ", C.c_int),
+        ("origin_offset", C.c_double * 3),
+        ("cellSize", C.c_double), ("courant_limit", C.c_double),
+        ("base_random_seed", C.c_uint),
+        ("ts_delt", C.c_double), ("finish_time", C.c_double), ("fs_finish", C.c_double),
+        ("fsgrow", C.c_double), ("rev_fsgrow", C.c_double),
+        ("tip_curv", C.c_int), ("gibbs_coef", C.c_double),
+        ("liquidusTemp", C.c_double), ("solidusTemp", C.c_double), ("Cinit", C.c_double),
+        ("m_solute0", C.c_double), ("m_solute0_a", C.c_double), ("m_solute0_b", C.c_double),
+        ("m_solute0_c", C.c_double),
+        ("part_coef", C.c_double), ("part_coef_a", C.c_double), ("part_coef_b", C.c_double),
+        ("part_coef_c", C.c_double),
+        ("Dsol", C.c_double), ("Dliq", C.c_double),
+        ("initialTemperature", C.c_double), ("gradient", C.c_double), ("velocity", C.c_double),
+        ("grad_coef", C.c_double), ("velo_coef", C.c_double), ("cool_rate", C.c_double),
+        ("thermal_ana", C.c_int), ("am", C.c_int), ("amlayer", C.c_int), ("amtracks", C.c_int),
+        ("lpow", C.c_double), ("lv", C.c_double), ("lsd", C.c_double), ("lab", C.c_double),
+        ("lhs", C.c_double), ("liniT", C.c_double), ("lthcon", C.c_double), ("lcp", C.c_double),
+        ("rho", C.c_double), ("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double),
+        ("maxGrainDensity", C.c_double), ("gnGaussCenter", C.c_double),
+        ("gnGaussSigma", C.c_double),
+        ("maxGrainDensitySurf", C.c_double), ("gnGaussCenterSurf", C.c_double),
+        ("gnGaussSigmaSurf", C.c_double),
+        ("doSurfaceNuc", C.c_int), ("gnUseOrientation", C.c_int),
+        ("maxTotalGrains", C.c_uint64),
+        ("screenpfreq", C.c_int), ("data_write_freq", C.c_int), ("data_write_start", C.c_int),
+        ("randomize_grains", C.c_int), ("vis_format", C.c_int),
+        ("basefilename", C.c_char * 256),
+        ("fixed_nucs", C.POINTER(FixedNuc)), ("n_fixed_nucs", C.c_int),
+        ("nuc_volumes", C.POINTER(NucVolume)), ("n_nuc_volumes", C.c_int),
+        ("precision", C.c_int), ("device", C.c_int),
+    ]
+
+    @property
+    def grid(self) -> tuple[int, int, int]:
+        return (self.gnsbx * self.gsdimx, self.gnsby * self.gsdimy, self.gnsbz * self.gsdimz)
+
+    @property
+    def nranks(self) -> int:
+        return self.gnsbx * self.gnsby * self.gnsbz
+
+
+class Grain(C.Structure):
+    """grain_t (globals.h:244-254)."""
+    _fields_ = [("nuc_x", C.c_double), ("nuc_y", C.c_double), ("nuc_z", C.c_double),
+                ("nuc_timestep", C.c_uint64), ("nuc_threshold", C.c_double),
+                ("rotmat", (C.c_double * 3) * 3), ("rotang", C.c_double * 3)]
+
+
+class GrainSummary(C.Structure):
+    _fields_ = [("num_grains", C.c_int), ("min_mm3", C.c_double), ("max_mm3", C.c_double),
+                ("avg_mm3", C.c_double)]
+
+
+class MmsError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        msg = f"{where}: {_lib().mms_status_string(status).decode()} (status {status})"
+        if detail:
+            msg += f": {detail}"
+        super().__init__(msg)
+
+
+_LIB = None
+
+
+def library_path() -> Path:
+    return _PKG / "libmms_b200.so"
+
+
+def load_library(build_if_missing: bool = True) -> C.CDLL:
+    """Loads libmms_b200.so from the package directory (building it first
+    when it is missing and nvcc is available)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not path.exists() and build_if_missing:
+        from . import build as _build
+        _build.build()
+    if not path.exists():
+        raise OSError(f"{path} is missing; run `python -m mumatscale_b200.build`")
+    lib = C.CDLL(str(path))
+    P, I, D = C.c_void_p, C.c_int, C.c_double
+    sigs = {
+        "mms_params_default": (I, [C.POINTER(Params)]),
+        "mms_deck_read": (I, [C.c_char_p, C.POINTER(Params)]),
+        "mms_params_free_lists": (None, [C.POINTER(Params)]),
+        "mms_params_size": (C.c_size_t, []),
+        "mms_create": (I, [C.POINTER(Params), C.POINTER(P)]),
+        "mms_destroy": (I, [P]),
+        "mms_step": (I, [P, I]),
+        "mms_get_timestep": (I, [P, C.POINTER(C.c_uint64)]),
+        "mms_get_num_grains": (I, [P, C.POINTER(I)]),
+        "mms_num_cells": (C.c_size_t, [P]),
+        "mms_download": (I, [P, I, P]),
+        "mms_upload": (I, [P, I, P]),
+        "mms_reduce": (I, [P, I, C.POINTER(D)]),
+        "mms_set_sites": (I, [P, C.c_int64, P, P]),
+        "mms_set_site_orientations": (I, [P, C.c_int64, P, P]),
+        "mms_get_grains": (I, [P, I, I, C.POINTER(Grain)]),
+        "mms_output_grains": (I, [P, C.c_char_p, C.POINTER(GrainSummary)]),
+        "mms_run": (I, [P, I]),
+        "mms_status_string": (C.c_char_p, [I]),
+        "mms_last_error": (C.c_char_p, [P]),
+        "mms_kernel_launches": (C.c_uint64, [P]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.mms_params_size() != C.sizeof(Params):
+        raise OSError(f"mms_params layout mismatch: C {lib.mms_params_size()} vs "
+                      f"ctypes {C.sizeof(Params)}")
+    _LIB = lib
+    return lib
+
+
+def _lib() -> C.CDLL:
+    return load_library()
+
+
+def _check(status: int, where: str, ctx=None) -> None:
+    if status != 0:
+        detail = ""
+        if ctx:
+            detail = (_lib().mms_last_error(ctx) or b"").decode()
+        raise MmsError(status, where, detail)
+
+
+def default_params() -> Params:
+    """set_defaults (read_ctrl.c:29-108)."""
+    p = Params()
+    _check(_lib().mms_params_default(C.byref(p)), "mms_params_default")
+    return p
+
+
+def read_deck(path: str | os.PathLike, params: Params | None = None) -> Params:
+    """read_config (read_ctrl.c:234-812) on top of defaults (or ``params``)."""
+    p = params if params is not None else default_params()
+    _check(_lib().mms_deck_read(str(path).encode(), C.byref(p)), f"mms_deck_read({path})")
+    return p
+
+
+Params.default = staticmethod(default_params)
+Params.from_deck = staticmethod(read_deck)
+
+
+class Domain:
+    """One GPU's device-resident domain (one mms_ctx)."""
+
+    def __init__(self, params: Params, precision: int | None = None, device: int | None = None):
+        lib = _lib()
+        p = Params()
+        C.pointer(p)[0] = params
+        if precision is not None:
+            p.precision = precision
+        if device is not None:
+            p.device = device
+        ctx = C.c_void_p()
+        _check(lib.mms_create(C.byref(p), C.byref(ctx)), "mms_create")
+        self._ctx = ctx
+        self.params = p
+        self.shape = tuple(x + 2 for x in p.grid)  # halo'd (x, y, z)
+
+    # -- lifetime
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            _lib().mms_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- stepping
+    def step(self, nsteps: int = 1) -> None:
+        _check(_lib().mms_step(self._ctx, int(nsteps)), "mms_step", self._ctx)
+
+    def run(self, verbose: int = 0) -> None:
+        _check(_lib().mms_run(self._ctx, int(verbose)), "mms_run", self._ctx)
+
+    @property
+    def timestep(self) -> int:
+        v = C.c_uint64()
+        _check(_lib().mms_get_timestep(self._ctx, C.byref(v)), "mms_get_timestep", self._ctx)
+        return int(v.value)
+
+    @property
+    def num_grains(self) -> int:
+        v = C.c_int()
+        _check(_lib().mms_get_num_grains(self._ctx, C.byref(v)), "mms_get_num_grains", self._ctx)
+        return int(v.value)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(_lib().mms_kernel_launches(self._ctx))
+
+    # -- fields (halo'd, indexed [z, y, x] like growth.c:70)
+    def num_cells(self) -> int:
+        return int(_lib().mms_num_cells(self._ctx))
+
+    def download(self, name: str) -> np.ndarray:
+        f = FIELD[name]
+        dt, comp = _FIELD_DTYPE[f]
+        n = self.num_cells()
+        out = np.empty(n * comp, dtype=dt)
+        _check(_lib().mms_download(self._ctx, f, out.ctypes.data), f"mms_download({name})", self._ctx)
+        nx, ny, nz = self.shape
+        return out.reshape((nz, ny, nx, comp) if comp > 1 else (nz, ny, nx))
+
+    def upload(self, name: str, arr: np.ndarray) -> None:
+        f = FIELD[name]
+        dt, comp = _FIELD_DTYPE[f]
+        a = np.ascontiguousarray(arr, dtype=dt).reshape(-1)
+        if a.size != self.num_cells() * comp:
+            raise ValueError("field size mismatch")
+        _check(_lib().mms_upload(self._ctx, f, a.ctypes.data), f"mms_upload({name})", self._ctx)
+
+    def reduce(self, what: str = "fs_fraction") -> float:
+        v = C.c_double()
+        _check(_lib().mms_reduce(self._ctx, REDUCE[what], C.byref(v)), "mms_reduce", self._ctx)
+        return float(v.value)
+
+    # -- sites, orientations, grains
+    def set_sites(self, gxyz: np.ndarray, thresholds: np.ndarray) -> None:
+        g = np.ascontiguousarray(gxyz, dtype=np.int32).reshape(-1, 3)
+        t = np.ascontiguousarray(thresholds, dtype=np.float32).reshape(-1)
+        _check(_lib().mms_set_sites(self._ctx, len(t), g.ctypes.data, t.ctypes.data),
+               "mms_set_sites", self._ctx)
+
+    def set_site_orientations(self, gxyz: np.ndarray, rotmats: np.ndarray) -> None:
+        g = np.ascontiguousarray(gxyz, dtype=np.int32).reshape(-1, 3)
+        r = np.ascontiguousarray(rotmats, dtype=np.float64).reshape(-1, 9)
+        _check(_lib().mms_set_site_orientations(self._ctx, len(r), g.ctypes.data, r.ctypes.data),
+               "mms_set_site_orientations", self._ctx)
+
+    def grains(self) -> list[Grain]:
+        n = self.num_grains
+        arr = (Grain * n)()
+        _check(_lib().mms_get_grains(self._ctx, 0, n, arr), "mms_get_grains", self._ctx)
+        return list(arr)
+
+    def grain_summary(self, csv_path: str | None = None) -> GrainSummary:
+        s = GrainSummary()
+        path = csv_path.encode() if csv_path else None
+        _check(_lib().mms_output_grains(self._ctx, path, C.byref(s)), "mms_output_grains", self._ctx)
+        return s

@@ -1,0 +1,89 @@
+"""Builds the in-tree native artifacts of mumatscale_b200.
+
+    libmms_b200.so   the C-ABI library (include/mms.h): sm_100a kernels and
+                     the host side, CUDA runtime linked statically
+    mmsb200          the command-line driver (ca_main.c interface)
+
+Everything is compiled for sm_100a only.  Device code is compiled with
+-fmad=false so FP64 results match the reference's x86-64 build bit for bit.
+Usage:  python -m mumatscale_b200.build  [--force]
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "libmms_b200.so"
+EXE = PKG / "mmsb200"
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CXX = "/usr/bin/g++"
+CC = "/usr/bin/gcc"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CU_SOURCES = ["kernels.cu", "mms_api.cu"]
+CXX_SOURCES = ["deck.cpp"]
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {cmd[0]} ({r.returncode})")
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    headers = list(CSRC.glob("*.h")) + [ROOT / "include" / "mms.h"]
+    objs = []
+    for src in CU_SOURCES:
+        obj = BUILD / (src + ".o")
+        if force or _stale(obj, [CSRC / src] + headers):
+            cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-fmad=false", "-std=c++17",
+                   "-Xcompiler", "-fPIC", "-Xptxas", "-v" if verbose else "-O3",
+                   "-c", str(CSRC / src), "-o", str(obj)]
+            _run(cmd)
+        objs.append(obj)
+    for src in CXX_SOURCES:
+        obj = BUILD / (src + ".o")
+        if force or _stale(obj, [CSRC / src] + headers):
+            _run([CXX, "-O2", "-fPIC", "-std=c++17", "-Wall", "-c", str(CSRC / src), "-o", str(obj)])
+        objs.append(obj)
+    if force or _stale(LIB, objs):
+        _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), *map(str, objs),
+              "-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"])
+    main_src = CSRC / "mms_main.c"
+    if force or _stale(EXE, [main_src, LIB, ROOT / "include" / "mms.h"]):
+        _run([CC, "-O2", "-std=gnu11", "-o", str(EXE), str(main_src), str(LIB),
+              "-Wl,-rpath,$ORIGIN"])
+    return LIB
+
+
+def build_oracle(reference_present: bool | None = None) -> None:
+    """Builds the CPU checkers under oracle/_ref (test infrastructure)."""
+    oracle = ROOT / "oracle"
+    _run(["make", "-C", str(oracle), "oracle"])
+    if reference_present is None:
+        reference_present = Path("/root/reference/src").is_dir()
+    if reference_present:
+        _run(["make", "-C", str(oracle), "ref"])
+
+
+if __name__ == "__main__":
+    force = "--force" in sys.argv
+    if force and BUILD.exists():
+        shutil.rmtree(BUILD)
+    print(build(force=force, verbose="-v" in sys.argv))

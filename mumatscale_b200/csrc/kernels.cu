@@ -1,0 +1,1010 @@
+// kernels.cu — sm_100a kernels for one muMatScale CA timestep.
+//
+// Compiled with -fmad=false: every FP64 expression is evaluated with the
+// same rounding, in the same order, as the reference's gcc x86-64 build
+// (which contracts nothing), so the FP64 plain form is bit-identical to it.
+//
+// One step (doiteration, calculate.c:193-352) is this launch sequence on one
+// stream; every kernel reads the step number from the device control block,
+// so the sequence can be replayed (or graph-captured) without the host:
+//
+//   k_temp_am     AM quadrature temperature (temperature.c:62-123), AM only
+//   k_nuc         nucleation test over the pre-drawn sites (grain.c:1222-1285)
+//   k_act         ordered grain activation (grain.c:840-916, 347-425)
+//   k_curv        Gibbs-Thomson curvature (curvature.c:31-405), TipCurvature only
+//   k_diffuse_fs  diffusion + fs change fused (growth.c:30-170, 177-276)
+//   k_list_count  interface-list flags per block (growth.c:461-538)
+//   k_list_scan   ordered block offsets, per-rank dc_tmp bookkeeping (growth.c:642-660)
+//   k_list_zero   clears dc_tmp regions that the reference re-allocates zeroed
+//   k_capture     list write + octahedron capture (growth.c:339-407, 664-794)
+//   k_apply       dc copy-back and captured grain ids (growth.c:789, 797-807)
+//
+// Fields: ce in place; cl and fs ping-pong between two buffers, the state
+// after step t living in buffer (t & 1).  gr, dc in place.  d is never
+// stored: capture recomputes it from the solid neighbour's dc, fs and
+// grain rotation, which is exactly what grow_octahedra stored for it.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+
+#include "mms_internal.h"
+
+namespace mms {
+
+#define FULL_MASK 0xffffffffu
+
+__device__ __forceinline__ bool stalled(const Ctl *c)
+{
+    return *((volatile const int *)&c->stall) != 0;
+}
+
+__device__ __forceinline__ void raise_error(Ctl *c, int status)
+{
+    atomicCAS(&c->status, 0, status);
+    atomicExch(&c->stall, (int)STALL_ERROR);
+}
+
+// direct_temp_calc (temperature.c:24-61) for the analytic models; the AM
+// quadrature is precomputed into an array by k_temp_am.
+__device__ __forceinline__ double temp_cell(const Phys &p, const double *Tarr, long long cell,
+                                            long long J, long long K, unsigned long long ts)
+{
+    if (p.temp_mode == 2) return Tarr[cell];
+    double sim_time = (double)ts * p.ts_delt;
+    if (p.temp_mode == 0) return p.T0 - sim_time * p.cool_rate;
+    double ry = p.origin[1] + ((double)(int)J + 0.5) * p.cellSize;
+    double rz = p.origin[2] + ((double)(int)K + 0.5) * p.cellSize;
+    double axis = (p.gz_is_one ? ry : rz) - p.cellSize * 0.5;
+    double tgrad = p.gradient + p.grad_coef * sim_time;
+    double v = p.velocity + p.velo_coef * sim_time;
+    double vt = 0.5 * (v + p.velocity) * sim_time;
+    return p.T0 + tgrad * (axis - vt);
+}
+
+template <int NT>
+__device__ __forceinline__ int block_exclusive_scan(int v, int &total, int *sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(FULL_MASK, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = (lane < NT / 32) ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(FULL_MASK, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < NT / 32) sh[lane] = w;
+    }
+    __syncthreads();
+    int prefix = warp ? sh[warp - 1] : 0;
+    total = sh[NT / 32 - 1];
+    __syncthreads();
+    return prefix + x - v;
+}
+
+template <int NT>
+__device__ __forceinline__ int block_sum(int v, int *sh)
+{
+    int t;
+    block_exclusive_scan<NT>(v, t, sh);
+    return t;
+}
+
+// ------------------------------------------------------------ temperature
+// AM moving-source quadrature, direct_temp_calc thermal_ana == 1
+// (temperature.c:62-123), over every halo'd cell, for step ctl->timestep+1.
+__global__ void k_temp_am(KernelArgs a, double lsd, double lv, double lhs, double lab,
+                          double lpow, double liniT, double lthcon, double rho_cp, double x0,
+                          double y0, double z0, int amtracks, int nsbx_times_sbx)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const Geo &g = a.g;
+    const Phys &p = a.p;
+    long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (cell >= g.N) return;
+    unsigned long long ts = ctl->timestep + 1;
+    long long K = cell / g.sz, J = (cell % g.sz) / g.sy, I = cell % g.sy;
+    double sim_time = (double)ts * p.ts_delt;
+    double rx = p.origin[0] + ((double)(int)I + 0.5) * p.cellSize;
+    double ry = p.origin[1] + ((double)(int)J + 0.5) * p.cellSize;
+    double rz = p.origin[2] + ((double)(int)K + 0.5) * p.cellSize;
+    double invlv = 1. / lv;
+    double ls = lsd / (2. * 1.414);
+    double xlen = nsbx_times_sbx * p.cellSize;
+    xlen = xlen + lsd;
+    double tline = xlen * invlv;
+    double tpause = 1.5e-4 * invlv;
+    tline = tline + tpause;
+    double trackno = 0;
+    if (amtracks > 1) trackno = floor(sim_time / tline);
+    double xnow = x0 + (sim_time - trackno * tline) * lv;
+    double ynow = y0 + trackno * lhs;
+    double znow = z0;
+    double lx = rx - xnow, ly = ry - ynow, lz = rz - znow;
+    double T;
+    if (rz <= znow + p.cellSize) {
+        const int nt = 400;
+        double Tinteg = 0.0;
+        double pi15 = 5.568328;
+        double lalpha = lthcon / rho_cp;
+        double tsteady = 20 * lalpha * invlv * invlv;
+        double ldt = tsteady / nt;
+        double pw = (sim_time < 1e-4) ? 0.0 : lpow;
+        for (int i = 0; i < nt; i++) {
+            double lt = (0.5 + i) * ldt;
+            double Tlocal = sqrt(lalpha * lt) * (ls * ls + 4. * lalpha * lt);
+            Tinteg += ldt *
+                      exp(-((lx + lv * lt) * (lx + lv * lt) + ly * ly) / (ls * ls + 4. * lalpha * lt) -
+                          (lz * lz / (4. * lalpha * lt))) /
+                      Tlocal;
+        }
+        double Tfront = lab * pw * lalpha / (pi15 * lthcon);
+        T = liniT + Tfront * Tinteg;
+    } else {
+        T = 0.0;
+    }
+    a.d.T[cell] = T;
+    if (a.d.lsindex && T > p.Tliq) a.d.lsindex[cell] = 1;
+}
+
+// --------------------------------------------------------------- nucleation
+// cell_nucleation (grain.c:1222-1285) over the sparse site list: a cell with
+// an infinite threshold can never pass the test, so only sites are tested.
+template <typename Real>
+__global__ void k_nuc(KernelArgs a)
+{
+    Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const Geo &g = a.g;
+    const Phys &p = a.p;
+    long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    bool hit = false;
+    if (s < a.d.nsites) {
+        unsigned long long ts = ctl->timestep + 1;
+        long long c = a.d.site_cell[s];
+        if (a.d.gr[c] <= 0) {
+            const Real *cl = (const Real *)a.d.cl[(int)(ctl->timestep & 1ULL)];
+            long long K = c / g.sz, J = (c % g.sz) / g.sy;
+            double Ttemp = temp_cell(p, a.d.T, c, J, K, ts);
+            int layerno = 1, initnuc = 1;
+            if (p.am) {
+                double sim_time = (double)ts * p.ts_delt;
+                if (p.amlayer == 1) layerno = 1;
+                else if (p.amlayer > 1 && a.d.lsindex[c] == 1) layerno = 1;
+                else layerno = 0;
+                if (sim_time <= 1e-4) initnuc = 1;
+                else if (Ttemp >= p.Tsol) initnuc = 1;
+                else initnuc = 0;
+            }
+            if (layerno && initnuc) {
+                double Tunder = p.Tliq - Ttemp;
+                double m = p.ma * Ttemp * Ttemp + p.mb * Ttemp + p.mc;
+                Tunder += m * ((double)cl[c] - p.cinit);
+                if (Tunder > (double)a.d.site_thr[s]) hit = true;
+            }
+        }
+    }
+    if (hit) a.d.site_flag[s] = 1;
+    unsigned mask = __ballot_sync(FULL_MASK, hit);
+    if ((threadIdx.x & 31) == 0 && mask) atomicAdd(&ctl->ncand, __popc(mask));
+}
+
+__device__ long long find_key(const long long *keys, long long n, long long key)
+{
+    long long lo = 0, hi = n - 1;
+    while (lo <= hi) {
+        long long mid = (lo + hi) >> 1;
+        long long k = keys[mid];
+        if (k == key) {
+            while (mid > 0 && keys[mid - 1] == key) mid--;
+            return mid;
+        }
+        if (k < key) lo = mid + 1;
+        else hi = mid - 1;
+    }
+    return -1;
+}
+
+// activateNewGrains + createGrains (grain.c:840-916, 347-425) with
+// addNewGrain's per-rank cap (grain.c:88-109).  Candidates are gathered in
+// site order, which is (emulated rank, local raster) order, so grain ids
+// match the rank-ordered Allgatherv displacements (grain.c:892-904).
+constexpr int ACT_NT = 256;
+__global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
+{
+    Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    __shared__ int sh[ACT_NT / 32];
+    __shared__ int s_abort;
+    const int C = ctl->ncand;
+    const unsigned long long ts = ctl->timestep + 1;
+    if (C == 0) {
+        if (threadIdx.x == 0) {
+            ctl->timestep = ts;
+            ctl->new_grains = 0;
+        }
+        return;
+    }
+    // ordered gather of flagged sites
+    int off = 0;
+    for (long long base = 0; base < a.d.nsites; base += ACT_NT) {
+        long long s = base + threadIdx.x;
+        int f = (s < a.d.nsites) ? (int)a.d.site_flag[s] : 0;
+        int tot;
+        int pos = block_exclusive_scan<ACT_NT>(f, tot, sh);
+        if (f) a.d.cand[off + pos] = (int)s;
+        off += tot;
+    }
+    if (threadIdx.x == 0) s_abort = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const Phys &p = a.p;
+        const int nr = a.g.nranks;
+        int *cnt = rank_scratch;           // candidates per rank
+        int *acc = rank_scratch + nr;      // accepted per rank (after caps)
+        int *need = rank_scratch + 2 * nr; // random draws needed per rank
+        int *start = rank_scratch + 3 * nr;
+        for (int r = 0; r < nr; r++) cnt[r] = 0, need[r] = 0, start[r] = -1;
+        for (int i = 0; i < C; i++) {
+            int r = a.d.site_rank[a.d.cand[i]];
+            if (start[r] < 0) start[r] = i;
+            cnt[r]++;
+        }
+        const long long num_grains = ctl->num_grains;
+        const unsigned long long maxg = p.max_grains;
+        for (int r = 0; r < nr; r++) acc[r] = cnt[r];
+        long long new_act = C;
+        if ((unsigned long long)(num_grains + new_act) > maxg + 1) {
+            // the reference's createGrains stops at the first id above
+            // MaxTotGrains (grain.c:363-366, reached because nindex2 replaces
+            // the capped count, grain.c:1318)
+            ctl->status = MMS_ERR_GRAIN_OVERFLOW;
+            atomicExch(&ctl->stall, (int)STALL_ERROR);
+            s_abort = 1;
+        }
+        // dry run: orientation draws needed per rank
+        bool short_rng = false;
+        for (int r = 0; r < nr && p.use_orientation && !s_abort; r++) {
+            for (int i = 0; i < acc[r]; i++) {
+                long long cell = a.d.site_cell[a.d.cand[start[r] + i]];
+                if (find_key(a.d.nucpt_key, a.d.n_nucpt, cell) < 0) need[r]++;
+            }
+            if (a.d.rng_used[r] + need[r] > a.d.rng_cap) short_rng = true;
+        }
+        if (s_abort) {
+            // error raised above
+        } else if (short_rng) {
+            ctl->stall_step = ts;
+            atomicExch(&ctl->stall, (int)STALL_RNG);
+            s_abort = 1;
+        } else {
+            long long id = num_grains;
+            for (int r = 0; r < nr && !s_abort; r++) {
+                for (int i = 0; i < acc[r]; i++, id++) {
+                    if ((unsigned long long)id > maxg) {
+                        ctl->status = MMS_ERR_GRAIN_OVERFLOW;
+                        ctl->stall = STALL_ERROR;
+                        s_abort = 1;
+                        break;
+                    }
+                    int s = a.d.cand[start[r] + i];
+                    long long cell = a.d.site_cell[s];
+                    a.d.gr[cell] = (int)id;
+                    GrainLog lg;
+                    lg.cell = cell;
+                    lg.timestep = ts;
+                    lg.rank = r;
+                    const double *rot;
+                    long long j = find_key(a.d.nucpt_key, a.d.n_nucpt, cell);
+                    if (j >= 0) {
+                        rot = a.d.nucpt_rot + 9 * j;
+                        lg.kind = 0;
+                        lg.aux = a.d.nucpt_entry[j];
+                    } else if (p.use_orientation) {
+                        int k = a.d.rng_used[r]++;
+                        rot = a.d.rng_rot + ((long long)r * a.d.rng_cap + k) * 9;
+                        lg.kind = 1;
+                        lg.aux = a.d.rng_base[r] + k;
+                    } else {
+                        rot = a.d.zero_rot;
+                        lg.kind = 2;
+                        lg.aux = 0;
+                    }
+                    if (a.d.n_inj > 0) {
+                        long long q = find_key(a.d.inj_key, a.d.n_inj, cell);
+                        if (q >= 0) rot = a.d.inj_rot + 9 * q;
+                    }
+                    double *dst = a.d.grain_rot + 9 * id;
+                    for (int e = 0; e < 9; e++) dst[e] = rot[e];
+                    a.d.grain_log[id] = lg;
+                }
+            }
+            if (!s_abort) {
+                ctl->num_grains = (int)(num_grains + new_act);
+                ctl->new_grains = (int)new_act;
+                ctl->ncand = 0;
+                ctl->timestep = ts;
+            }
+        }
+    }
+    __syncthreads();
+    if (s_abort) return;
+    for (int i = threadIdx.x; i < C; i += ACT_NT) a.d.site_flag[a.d.cand[i]] = 0;
+}
+
+// ---------------------------------------------------------------- curvature
+// sb_curvature (curvature.c:31-405) on each emulated rank's local range
+// k,j,i in [2, dim-1], reading fs as it stands before fs_change.
+template <typename Real>
+__global__ void k_curv(KernelArgs a)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const Geo &g = a.g;
+    long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long total = (long long)g.nranks * g.sbcells;
+    if (v >= total) return;
+    int r = (int)(v / g.sbcells);
+    long long l = v % g.sbcells;
+    int i = (int)(l % g.sbx) + 1, j = (int)((l / g.sbx) % g.sby) + 1, k = (int)(l / ((long long)g.sbx * g.sby)) + 1;
+    int rx = r % g.nsbx, ry = (r / g.nsbx) % g.nsby, rz = r / (g.nsbx * g.nsby);
+    long long idx = (long long)(rz * g.sbz + k) * g.sz + (long long)(ry * g.sby + j) * g.sy + (rx * g.sbx + i);
+    const int dimx = g.sbx, dimy = g.sby, dimz = g.sbz;
+    if (i < 2 || i > dimx - 1 || j < 2 || j > dimy - 1 || k < 2 || k > dimz - 1) return;
+    const Real *fsr = (const Real *)a.d.fs[(int)((ctl->timestep - 1) & 1ULL)];
+    const int *gr = a.d.gr;
+    double *curv = a.d.curv;
+    auto fs = [&](long long q) { return (double)fsr[q]; };
+    curv[idx] = 0.0;
+    if (gr[idx] <= 0 || fs(idx) == 0) return;
+    const long long jgap = g.sy, kgap = g.sz;
+    int nbindex = gr[idx + 1] + gr[idx + jgap] + gr[idx - 1] + gr[idx - jgap] + gr[idx + kgap] + gr[idx - kgap];
+    if (!nbindex) return;
+    const int alpha = 2, beta = 4;
+    long long idl = idx + 1, idr = idx - 1, idf = idx + jgap, idb = idx - jgap;
+    long long idu = idx + kgap, idd = idx - kgap;
+    long long idur = idr + kgap, idul = idl + kgap, iddr = idr - kgap, iddl = idl - kgap;
+    long long idfr = idf - 1, idfl = idf + 1, idbr = idb - 1, idbl = idb + 1;
+    long long idub = idb + kgap, iduf = idf + kgap, iddf = idf - kgap, iddb = idb - kgap;
+    long long idufr = iduf - 1, idufl = iduf + 1, idubr = idub - 1, idubl = idub + 1;
+    long long iddbr = iddb - 1, iddbl = iddb + 1, iddfr = iddf - 1, iddfl = iddf + 1;
+    double fsl = (fs(idufl) + fs(idubl) + fs(iddbl) + fs(iddfl) +
+                  alpha * (fs(idul) + fs(iddl) + fs(idfl) + fs(idbl)) + beta * fs(idl)) / (1 + 4 * alpha + beta);
+    double fsr_ = (fs(idufr) + fs(idubr) + fs(iddbr) + fs(iddfr) +
+                   alpha * (fs(idur) + fs(iddr) + fs(idfr) + fs(idbr)) + beta * fs(idr)) / (1 + 4 * alpha + beta);
+    double fsf = (fs(idufl) + fs(idufr) + fs(iddfr) + fs(iddfl) +
+                  alpha * (fs(idfl) + fs(idfr) + fs(iduf) + fs(iddf)) + beta * fs(idf)) / (1 + 4 * alpha + beta);
+    double fsb = (fs(idubr) + fs(idubl) + fs(iddbl) + fs(iddbr) +
+                  alpha * (fs(idbl) + fs(idbr) + fs(idub) + fs(iddb)) + beta * fs(idb)) / (1 + 4 * alpha + beta);
+    double fsu = (fs(idufl) + fs(idufr) + fs(idubr) + fs(idubl) +
+                  alpha * (fs(idul) + fs(idur) + fs(idub) + fs(iduf)) + beta * fs(idl)) / (1 + 4 * alpha + beta);
+    double fsd = (fs(iddbr) + fs(iddbl) + fs(iddfl) + fs(iddfr) +
+                  alpha * (fs(iddr) + fs(iddl) + fs(iddf) + fs(iddb)) + beta * fs(idd)) / (1 + 4 * alpha + beta);
+    double nx = (fsl - fsr_) / 2.0, ny = (fsf - fsb) / 2.0, nz = (fsu - fsd) / 2.0;
+    double nall = sqrt(nx * nx + ny * ny + nz * nz);
+    if (!(nall)) {
+        nx = nx / nall;
+        ny = ny / nall;
+        nz = nz / nall;
+    }
+    int nor_dir = 0;
+    if (!(nx) || !(ny) || !(nz)) {
+        if ((fabs(nx) >= fabs(ny)) && (fabs(nx) >= fabs(nz))) nor_dir = 1;
+        else if ((fabs(ny) >= fabs(nz)) && (fabs(ny) >= fabs(nx))) nor_dir = 2;
+        else if ((fabs(nz) >= fabs(ny)) && (fabs(nz) >= fabs(nx))) nor_dir = 3;
+    }
+    long long st, a1, a2, b1, b2, c11, c12, c21, c22;
+    double ncomp;
+    int pos, dim;
+    if (nor_dir == 3) {
+        ncomp = nz; pos = k; dim = dimz; st = kgap;
+        a1 = idf; a2 = idb; b1 = idl; b2 = idr; c11 = idfl; c12 = idfr; c21 = idbl; c22 = idbr;
+    } else if (nor_dir == 2) {
+        ncomp = ny; pos = j; dim = dimy; st = jgap;
+        a1 = idu; a2 = idd; b1 = idl; b2 = idr; c11 = idul; c12 = idur; c21 = iddl; c22 = iddr;
+    } else if (nor_dir == 1) {
+        ncomp = nx; pos = i; dim = dimx; st = 1;
+        a1 = idu; a2 = idd; b1 = idf; b2 = idb; c11 = iduf; c12 = idub; c21 = iddf; c22 = iddb;
+    } else {
+        return;
+    }
+    double gamma = (acos(fabs(ncomp)) < 0.8) ? 0.0 : 0.2;
+    int t = (((pos + 2) <= dim) && (pos - 2) >= 1) ? 3 : 1;
+    double h = 0, hA1 = 0, hA2 = 0, hB1 = 0, hB2 = 0, hC11 = 0, hC12 = 0, hC22 = 0, hC21 = 0;
+    for (int n = -t; n <= t; n++) {
+        h += fs(idx + st * n);
+        hA1 += fs(a1 + st * n);
+        hA2 += fs(a2 + st * n);
+        hB1 += fs(b1 + st * n);
+        hB2 += fs(b2 + st * n);
+        hC11 += fs(c11 + st * n);
+        hC12 += fs(c12 + st * n);
+        hC22 += fs(c22 + st * n);
+        hC21 += fs(c21 + st * n);
+    }
+    double cs = a.p.cellSize;
+    double hx = (gamma * (hC11 - hC12) + hB1 - hB2 + gamma * (hC21 - hC22)) / (1 + 2 * gamma) / 2.0;
+    double hy = (gamma * (hC11 - hC21) + hA1 - hA2 + gamma * (hC12 - hC22)) / (1 + 2 * gamma) / 2.0;
+    double hxx = (gamma * (hC11 - 2 * hA1 + hC12) + hB1 - 2 * h + hB2 + gamma * (hC21 - 2 * hA2 + hC22)) / (cs) / (1 + 2 * gamma);
+    double hyy = (gamma * (hC11 - 2 * hB1 + hC21) + hA1 - 2 * h + hA2 + gamma * (hC12 - 2 * hB2 + hC22)) / (cs) / (1 + 2 * gamma);
+    double hxy = (hC11 - hC21 - hC12 + hC22) / cs / 4.0;
+    curv[idx] = (hxx + hyy + hxx * hy * hy + hyy * hx * hx - 2 * hxy * hx * hy) / pow((1 + hx * hx + hy * hy), 1.5);
+}
+
+// ------------------------------------------------ diffusion + fs change
+// One thread per (i,j) column of a TX x TY tile marching over ZC planes;
+// three halo'd planes of cl and fs live in a shared-memory ring.  Per cell
+// the arithmetic is sb_diffuse_alloy_decentered (growth.c:69-162) followed
+// by fs_change_diffuse (growth.c:220-273) on the same cell, with oce = the
+// ce value before diffusion, held in a register (calculate.c:269-280).
+constexpr int DTX = 32, DTY = 8;
+
+template <typename Real>
+struct PhysR {
+    Real rs, rl, liq_slope, k_inv, km, km_inv, m_inv, D_xt, cinit, Tliq, gibbs;
+};
+
+template <typename Real>
+__device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
+{
+    PhysR<Real> q;
+    q.rs = (Real)p.rs;
+    q.rl = (Real)p.rl;
+    q.liq_slope = (Real)p.liq_slope;
+    q.k_inv = (Real)p.k_inv;
+    q.km = (Real)p.km;
+    q.km_inv = (Real)p.km_inv;
+    q.m_inv = (Real)p.m_inv;
+    q.D_xt = (Real)p.D_xt;
+    q.cinit = (Real)p.cinit;
+    q.Tliq = (Real)p.Tliq;
+    q.gibbs = (Real)p.gibbs;
+    return q;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchunk)
+{
+    Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const Geo &g = a.g;
+    const Phys &p = a.p;
+    const unsigned long long ts = ctl->timestep;
+    const int pin = (int)((ts - 1) & 1ULL), pout = (int)(ts & 1ULL);
+    const Real *__restrict__ clI = (const Real *)a.d.cl[pin];
+    const Real *__restrict__ fsI = (const Real *)a.d.fs[pin];
+    Real *__restrict__ clO = (Real *)a.d.cl[pout];
+    Real *__restrict__ fsO = (Real *)a.d.fs[pout];
+    Real *__restrict__ ce = (Real *)a.d.ce;
+    int *__restrict__ gr = a.d.gr;
+    const PhysR<Real> q = phys_r<Real>(p);
+
+    __shared__ Real s_cl[3][DTY + 2][DTX + 2];
+    __shared__ Real s_fs[3][DTY + 2][DTX + 2];
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DTX + tx;
+    const int i0 = blockIdx.x * DTX + 1, j0 = blockIdx.y * DTY + 1;
+    const int i = i0 + tx, j = j0 + ty;
+    const int k0 = blockIdx.z * zchunk + 1;
+    const int k1 = min(k0 + zchunk - 1, g.gz);
+    const bool active = (i <= g.gx) && (j <= g.gy);
+    constexpr int PW = DTX + 2, PH = DTY + 2, PN = PW * PH;
+
+    auto load_plane = [&](int slot, int k) {
+        for (int e = tid; e < PN; e += DTX * DTY) {
+            int ey = e / PW, ex = e - ey * PW;
+            int ii = i0 - 1 + ex, jj = j0 - 1 + ey;
+            if (ii <= g.gx + 1 && jj <= g.gy + 1) {
+                long long c = (long long)k * g.sz + (long long)jj * g.sy + ii;
+                s_cl[slot][ey][ex] = clI[c];
+                s_fs[slot][ey][ex] = fsI[c];
+            }
+        }
+    };
+
+    load_plane(0, k0 - 1);
+    load_plane(1, k0);
+    int sm = 0, sc = 1, sp = 2;
+    const double one_x = (double)(1 - g.padx), one_y = (double)(1 - g.pady), one_z = (double)(1 - g.padz);
+    for (int k = k0; k <= k1; k++) {
+        load_plane(sp, k + 1);
+        __syncthreads();
+        if (active) {
+            const long long c = (long long)k * g.sz + (long long)j * g.sy + i;
+            const int ly = ty + 1, lx = tx + 1;
+            const Real conc = s_cl[sc][ly][lx];
+            const Real lspfs = s_fs[sc][ly][lx];
+            // neighbour order +x, -x, +y, -y, +z, -z (growth.c:85-113)
+            const Real nb_cl[6] = {s_cl[sc][ly][lx + 1], s_cl[sc][ly][lx - 1], s_cl[sc][ly + 1][lx],
+                                   s_cl[sc][ly - 1][lx], s_cl[sp][ly][lx], s_cl[sm][ly][lx]};
+            const Real nb_fs[6] = {s_fs[sc][ly][lx + 1], s_fs[sc][ly][lx - 1], s_fs[sc][ly + 1][lx],
+                                   s_fs[sc][ly - 1][lx], s_fs[sp][ly][lx], s_fs[sm][ly][lx]};
+            const Real one_m[6] = {(Real)(i == g.gx ? one_x : 1.0), (Real)(i == 1 ? one_x : 1.0),
+                                   (Real)(j == g.gy ? one_y : 1.0), (Real)(j == 1 ? one_y : 1.0),
+                                   (Real)(k == g.gz ? one_z : 1.0), (Real)(k == 1 ? one_z : 1.0)};
+            Real nbsum = 0;
+#pragma unroll
+            for (int n = 0; n < 6; n++) {
+                Real fs_av = (Real)0.5 * (lspfs + nb_fs[n]);
+                Real r = (q.rs * fs_av + q.rl * (1 - fs_av)) * one_m[n];
+                nbsum += r * (nb_cl[n] - conc);
+            }
+            const Real oce = ce[c];
+            const Real cen = oce + nbsum;
+            ce[c] = cen;
+            if (cen < 0) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
+
+            // fs_change_diffuse
+            const double Td = temp_cell(p, a.d.T, c, j, k, ts);
+            const Real Tcell = (Real)Td;
+            Real c_int = q.cinit + q.m_inv * (Tcell - q.Tliq);
+            Real Tunder = q.Tliq - Tcell;
+            Tunder += q.liq_slope * (conc - q.cinit);
+            const int grc = gr[c];
+            Real cl_new, fs_new;
+            if (grc <= 0 || Td < 1.0 || Td > p.Tliq) {
+                cl_new = cen;
+                fs_new = 0;
+                if (grc != 0) gr[c] = 0;
+            } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
+                cl_new = cen * q.k_inv;
+                fs_new = lspfs;
+            } else {
+                if (p.tip_curv) {
+                    const Real cv = (Real)a.d.curv[c];
+                    c_int = q.cinit + q.m_inv * (Tcell - q.Tliq + q.gibbs * cv);
+                }
+                Real dce = cen - oce;
+                Real dcl = (c_int - conc) * q.D_xt * 2 + dce / (1 - q.km * lspfs);
+                Real dfs = (dcl * ((Real)1. - q.km * lspfs) - dce) * q.km_inv / conc;
+                cl_new = conc + dcl;
+                fs_new = lspfs + dfs;
+                fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
+                if (fs_new < (Real)0.) {
+                    fs_new = 0.;
+                    gr[c] = 0;
+                    cl_new = cen;
+                }
+            }
+            clO[c] = cl_new;
+            fsO[c] = fs_new;
+        }
+        __syncthreads();
+        int t = sm;
+        sm = sc;
+        sc = sp;
+        sp = t;
+    }
+}
+
+// ------------------------------------------------------- interface list
+// grow_cell_reduction (growth.c:461-538): a non-mold liquid cell whose six
+// neighbours' grain ids sum above zero.  Blocks cover VB consecutive cells
+// of one emulated rank in local raster order, so block order = list order.
+constexpr int LIST_NT = 256;
+
+__device__ __forceinline__ long long list_cell_of(const Geo &g, int r, long long l)
+{
+    int i = (int)(l % g.sbx) + 1, j = (int)((l / g.sbx) % g.sby) + 1, k = (int)(l / ((long long)g.sbx * g.sby)) + 1;
+    int rx = r % g.nsbx, ry = (r / g.nsbx) % g.nsby, rz = r / (g.nsbx * g.nsby);
+    return (long long)(rz * g.sbz + k) * g.sz + (long long)(ry * g.sby + j) * g.sy + (rx * g.sbx + i);
+}
+
+__device__ __forceinline__ bool is_list_cell(const int *gr, const Geo &g, long long c)
+{
+    if (gr[c] > 0) return false;
+    int nb = gr[c + 1] + gr[c - 1] + gr[c + g.sy] + gr[c - g.sy] + gr[c + g.sz] + gr[c - g.sz];
+    return nb > 0;
+}
+
+__global__ void __launch_bounds__(LIST_NT) k_list_count(KernelArgs a)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    __shared__ int sh[LIST_NT / 32];
+    const Geo &g = a.g;
+    int r = (int)(blockIdx.x / g.blocks_per_rank);
+    long long chunk = blockIdx.x % g.blocks_per_rank;
+    long long l0 = chunk * g.vb, l1 = min(l0 + g.vb, g.sbcells);
+    int n = 0;
+    for (long long l = l0 + threadIdx.x; l < l1; l += LIST_NT) n += is_list_cell(a.d.gr, g, list_cell_of(g, r, l));
+    int tot = block_sum<LIST_NT>(n, sh);
+    if (threadIdx.x == 0) a.d.blk_cnt[blockIdx.x] = tot;
+}
+
+// Exclusive scan of block counts; per-rank list lengths and the dc_tmp
+// re-allocation rule of capture_octahedra_diffuse (growth.c:642-660): when
+// a rank's list outgrows its dc_tmp, the array is replaced by a zeroed one of
+// gindex + 100 entries.
+constexpr int SCAN_NT = 1024;
+__global__ void __launch_bounds__(SCAN_NT) k_list_scan(KernelArgs a, int nblocks)
+{
+    Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    __shared__ int sh[SCAN_NT / 32];
+    int run = 0;
+    for (int base = 0; base < nblocks; base += SCAN_NT) {
+        int b = base + threadIdx.x;
+        int v = (b < nblocks) ? a.d.blk_cnt[b] : 0;
+        int tot;
+        int ex = block_exclusive_scan<SCAN_NT>(v, tot, sh);
+        if (b < nblocks) a.d.blk_off[b] = run + ex;
+        run += tot;
+    }
+    __syncthreads();
+    const Geo &g = a.g;
+    int any_zero = 0;
+    for (int r = threadIdx.x; r < g.nranks; r += SCAN_NT) {
+        long long b0 = (long long)r * g.blocks_per_rank, b1 = b0 + g.blocks_per_rank;
+        int start = a.d.blk_off[b0];
+        int end = (b1 < nblocks) ? a.d.blk_off[b1] : run;
+        int gindex = end - start;
+        a.d.rank_gindex[r] = gindex;
+        int size = a.d.rank_dcsize[r];
+        if (gindex > size) {
+            a.d.rank_zero_upto[r] = size;
+            a.d.rank_dcsize[r] = gindex + 100;
+            if (size > 0) any_zero = 1;
+        } else {
+            a.d.rank_zero_upto[r] = 0;
+        }
+    }
+    any_zero = __syncthreads_or(any_zero);
+    if (threadIdx.x == 0) {
+        ctl->list_total = run;
+        ctl->zero_needed = any_zero;
+    }
+}
+
+__global__ void k_list_zero(KernelArgs a)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl) || !ctl->zero_needed) return;
+    int r = blockIdx.y;
+    int upto = a.d.rank_zero_upto[r];
+    Dc3 *base = a.d.dc_tmp + a.d.rank_dcbase[r];
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < upto; s += (long long)gridDim.x * blockDim.x)
+        base[s] = Dc3{0.0, 0.0, 0.0};
+}
+
+// capture_octahedra_diffuse, INDEX_SEP branch (growth.c:664-794), with
+// grow_octahedra's half diagonal (growth.c:372-403) evaluated for the solid
+// neighbour on demand.  Results go to per-slot buffers; k_apply commits them
+// after every capture has read the pre-capture grain ids (the reference's
+// ogr copy, growth.c:635-638).
+template <typename Real>
+__global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    __shared__ int sh[LIST_NT / 32];
+    const Geo &g = a.g;
+    const Phys &p = a.p;
+    const int r = (int)(blockIdx.x / g.blocks_per_rank);
+    const long long chunk = blockIdx.x % g.blocks_per_rank;
+    const long long l0 = chunk * g.vb, l1 = min(l0 + g.vb, g.sbcells);
+    const int pout = (int)(ctl->timestep & 1ULL);
+    const Real *fs = (const Real *)a.d.fs[pout];
+    const int *gr = a.d.gr;
+    const Dc3 *dc = a.d.dc;
+    const int rank_start = a.d.blk_off[(long long)r * g.blocks_per_rank];
+    int pos_base = a.d.blk_off[blockIdx.x];
+    const long long dcbase = a.d.rank_dcbase[r];
+    for (long long lb = l0; lb < l1; lb += LIST_NT) {
+        long long l = lb + threadIdx.x;
+        long long c = 0;
+        int f = 0;
+        if (l < l1) {
+            c = list_cell_of(g, r, l);
+            f = is_list_cell(gr, g, c);
+        }
+        int tot;
+        int pos = pos_base + block_exclusive_scan<LIST_NT>(f, tot, sh);
+        pos_base += tot;
+        if (!f) continue;
+        const int slot = pos - rank_start + 1;
+        a.d.list_cell[pos] = c;
+        // neighbour order +x, +y, -x, -y, +z, -z (growth.c:604-610, 674-677)
+        const long long ndxs[6] = {c + 1, c + g.sy, c - 1, c - g.sy, c + g.sz, c - g.sz};
+        const int nnx[6] = {1, 0, -1, 0, 0, 0}, nny[6] = {0, 1, 0, -1, 0, 0}, nnz[6] = {0, 0, 0, 0, 1, -1};
+        int found = -1, gid = 0;
+        double g00 = 0, g10 = 0, g20 = 0, g01 = 0, g11 = 0, g21 = 0, g02 = 0, g12 = 0, g22 = 0;
+        double dx = 0, dy = 0, dz = 0, dn = 0;
+        Dc3 dcn{0, 0, 0};
+        for (int n = 0; n < 6; n++) {
+            long long ndx = ndxs[n];
+            int id = gr[ndx];
+            if (id > 0 && (unsigned long long)id < p.max_grains) {
+                const double *R = a.d.grain_rot + 9 * (long long)id;
+                g00 = R[0]; g01 = R[1]; g02 = R[2];
+                g10 = R[3]; g11 = R[4]; g12 = R[5];
+                g20 = R[6]; g21 = R[7]; g22 = R[8];
+                dcn = dc[ndx];
+                // grow_octahedra for the neighbour
+                double rx0 = 0.0 - dcn.x, ry0 = 0.0 - dcn.y, rz0 = 0.0 - dcn.z;
+                double gx0 = g00 * rx0 + g10 * ry0 + g20 * rz0;
+                double gy0 = g01 * rx0 + g11 * ry0 + g21 * rz0;
+                double gz0 = g02 * rx0 + g12 * ry0 + g22 * rz0;
+                double ds1 = fabs(gx0) + fabs(gy0) + fabs(gz0);
+                ds1 = (ds1 < 1.5) ? ds1 : 1.5;
+                dn = ds1 + (double)fs[ndx] * p.fsgrow;
+                // capture test
+                double rx1 = -1.0 * nnx[n] - dcn.x;
+                double ry1 = -1.0 * nny[n] - dcn.y;
+                double rz1 = -1.0 * nnz[n] - dcn.z;
+                dx = g00 * rx1 + g10 * ry1 + g20 * rz1;
+                dy = g01 * rx1 + g11 * ry1 + g21 * rz1;
+                dz = g02 * rx1 + g12 * ry1 + g22 * rz1;
+                double dfs = dn - (fabs(dx) + fabs(dy) + fabs(dz));
+                if (dfs > 0) {
+                    found = n;
+                    gid = id;
+                    break;
+                }
+            }
+        }
+        if (found > -1) {
+            double ncx = 0., ncz = 0., ncy = 0.;
+            double ncd = (dn < 1.0) ? dn : 1.0;
+            double dd = dn - ncd;
+            if (dx + dy >= 0 && dx - dy > 0 && dx + dz > 0 && dx - dz >= 0) ncx = dd;
+            else if (dx + dy <= 0 && dx - dy < 0 && dx + dz < 0 && dx - dz <= 0) ncx = -1. * dd;
+            else if (dy + dx > 0 && dy - dx >= 0 && dy + dz >= 0 && dy - dz > 0) ncy = dd;
+            else if (dy + dx < 0 && dy - dx <= 0 && dy + dz <= 0 && dy - dz < 0) ncy = -1. * dd;
+            else if (dz + dx >= 0 && dz - dx > 0 && dz + dy > 0 && dz - dy >= 0) ncz = dd;
+            else ncz = -1. * dd;
+            Dc3 out;
+            out.x = dcn.x + (double)nnx[found] + g00 * ncx + g01 * ncy + g02 * ncz;
+            out.y = dcn.y + (double)nny[found] + g10 * ncx + g11 * ncy + g12 * ncz;
+            out.z = dcn.z + (double)nnz[found] + g20 * ncx + g21 * ncy + g22 * ncz;
+            a.d.dc_tmp[dcbase + slot] = out;
+        }
+        a.d.list_gid[pos] = gid;
+        // slot is recovered in k_apply from the position and the rank start
+    }
+}
+
+__global__ void k_apply(KernelArgs a)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const Geo &g = a.g;
+    const int total = ctl->list_total;
+    for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < total;
+         pos += (long long)gridDim.x * blockDim.x) {
+        long long c = a.d.list_cell[pos];
+        // emulated rank of the cell
+        long long K = c / g.sz, J = (c % g.sz) / g.sy, I = c % g.sy;
+        int rx = (int)((I - 1) / g.sbx), ry = (int)((J - 1) / g.sby), rz = (int)((K - 1) / g.sbz);
+        int r = rx + ry * g.nsbx + rz * g.nsbx * g.nsby;
+        int start = a.d.blk_off[(long long)r * g.blocks_per_rank];
+        int slot = (int)pos - start + 1;
+        a.d.dc[c] = a.d.dc_tmp[a.d.rank_dcbase[r] + slot];
+        int gid = a.d.list_gid[pos];
+        if (gid) a.d.gr[c] = gid;
+    }
+}
+
+// ------------------------------------------------------------ reductions
+constexpr int RED_NT = 256;
+// Per-block partial sums over interior cells of min(1, fs) (reduce_fs,
+// growth.c:541-566) or of ce (TwoSum-compensated).
+template <typename Real>
+__global__ void __launch_bounds__(RED_NT) k_reduce(KernelArgs a, int what, double *partial)
+{
+    const Ctl *ctl = a.d.ctl;
+    const Geo &g = a.g;
+    const int cur = (int)(ctl->timestep & 1ULL);
+    const Real *f = (what == MMS_REDUCE_CE_SUM) ? (const Real *)a.d.ce : (const Real *)a.d.fs[cur];
+    long long n = (long long)g.gx * g.gy * g.gz;
+    double s = 0.0, comp = 0.0;
+    for (long long v = blockIdx.x * (long long)RED_NT + threadIdx.x; v < n; v += (long long)gridDim.x * RED_NT) {
+        long long i = v % g.gx, j = (v / g.gx) % g.gy, k = v / ((long long)g.gx * g.gy);
+        long long c = (k + 1) * g.sz + (j + 1) * g.sy + (i + 1);
+        double x = (double)f[c];
+        if (what != MMS_REDUCE_CE_SUM) x = (1.0 < x) ? 1.0 : x;
+        double t = s + x;                      // TwoSum
+        double bp = t - s;
+        comp += (s - (t - bp)) + (x - bp);
+        s = t;
+    }
+    __shared__ double ss[RED_NT], sc[RED_NT];
+    ss[threadIdx.x] = s;
+    sc[threadIdx.x] = comp;
+    __syncthreads();
+    for (int w = RED_NT / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            double x = ss[threadIdx.x + w];
+            double t = ss[threadIdx.x] + x;
+            double bp = t - ss[threadIdx.x];
+            sc[threadIdx.x] += sc[threadIdx.x + w] + ((ss[threadIdx.x] - (t - bp)) + (x - bp));
+            ss[threadIdx.x] = t;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = ss[0];
+        partial[2 * blockIdx.x + 1] = sc[0];
+    }
+}
+
+// d for every cell (grow_octahedra semantics; 0 where no grain grows)
+template <typename Real>
+__global__ void k_compute_d(KernelArgs a, double *out)
+{
+    const Ctl *ctl = a.d.ctl;
+    const Geo &g = a.g;
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= g.N) return;
+    const Real *fs = (const Real *)a.d.fs[(int)(ctl->timestep & 1ULL)];
+    int id = a.d.gr[c];
+    double d = 0.0;
+    long long K = c / g.sz, J = (c % g.sz) / g.sy, I = c % g.sy;
+    bool interior = I >= 1 && I <= g.gx && J >= 1 && J <= g.gy && K >= 1 && K <= g.gz;
+    if (interior && id > 0 && (unsigned long long)id < a.p.max_grains) {
+        const double *R = a.d.grain_rot + 9 * (long long)id;
+        Dc3 v = a.d.dc[c];
+        double rx0 = 0.0 - v.x, ry0 = 0.0 - v.y, rz0 = 0.0 - v.z;
+        double gx0 = R[0] * rx0 + R[3] * ry0 + R[6] * rz0;
+        double gy0 = R[1] * rx0 + R[4] * ry0 + R[7] * rz0;
+        double gz0 = R[2] * rx0 + R[5] * ry0 + R[8] * rz0;
+        double ds1 = fabs(gx0) + fabs(gy0) + fabs(gz0);
+        ds1 = (ds1 < 1.5) ? ds1 : 1.5;
+        d = ds1 + (double)fs[c] * a.p.fsgrow;
+    }
+    out[c] = d;
+}
+
+__global__ void k_fill_temperature(KernelArgs a, double *out)
+{
+    const Ctl *ctl = a.d.ctl;
+    const Geo &g = a.g;
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= g.N) return;
+    long long K = c / g.sz, J = (c % g.sz) / g.sy;
+    out[c] = temp_cell(a.p, a.d.T, c, J, K, ctl->timestep);
+}
+
+// Conversion between the stored precision and FP64 host buffers.
+template <typename Real>
+__global__ void k_convert(KernelArgs a, int field, int to_device, double *buf)
+{
+    const Ctl *ctl = a.d.ctl;
+    const Geo &g = a.g;
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= g.N) return;
+    const int cur = (int)(ctl->timestep & 1ULL);
+    Real *f = nullptr, *f2 = nullptr;
+    if (field == MMS_FIELD_CE) f = (Real *)a.d.ce;
+    else if (field == MMS_FIELD_CL) f = (Real *)a.d.cl[cur], f2 = (Real *)a.d.cl[cur ^ 1];
+    else f = (Real *)a.d.fs[cur], f2 = (Real *)a.d.fs[cur ^ 1];
+    if (to_device) {
+        f[c] = (Real)buf[c];
+        if (f2) f2[c] = (Real)buf[c];
+    } else {
+        buf[c] = (double)f[c];
+    }
+}
+
+// ---------------------------------------------------------------- launch
+static int pick_zchunk(const Geo &g)
+{
+    long long tiles = (long long)((g.gx + DTX - 1) / DTX) * ((g.gy + DTY - 1) / DTY);
+    // aim for >= 8 blocks per SM on 148 SMs
+    long long want = 148LL * 8;
+    int zc = (int)((tiles * g.gz + want - 1) / want);
+    if (zc < 4) zc = 4;
+    if (zc > 64) zc = 64;
+    if (zc > g.gz) zc = g.gz;
+    return zc;
+}
+
+template <typename Real>
+static int launch_step_t(const KernelArgs &a, cudaStream_t st, int start_stage)
+{
+    int n = 0;
+    const Geo &g = a.g;
+    if (start_stage == 0 && a.d.nsites > 0) {
+        int nb = (int)((a.d.nsites + 255) / 256);
+        k_nuc<Real><<<nb, 256, 0, st>>>(a);
+        n++;
+    }
+    k_act<<<1, ACT_NT, 0, st>>>(a, a.d.act_scratch);
+    n++;
+    if (a.p.tip_curv) {
+        long long tot = (long long)g.nranks * g.sbcells;
+        k_curv<Real><<<(int)((tot + 255) / 256), 256, 0, st>>>(a);
+        n++;
+    }
+    {
+        int zc = pick_zchunk(g);
+        dim3 grid((g.gx + DTX - 1) / DTX, (g.gy + DTY - 1) / DTY, (g.gz + zc - 1) / zc);
+        k_diffuse_fs<Real><<<grid, dim3(DTX, DTY), 0, st>>>(a, zc);
+        n++;
+    }
+    int nblocks = (int)(g.blocks_per_rank * g.nranks);
+    k_list_count<<<nblocks, LIST_NT, 0, st>>>(a);
+    k_list_scan<<<1, SCAN_NT, 0, st>>>(a, nblocks);
+    k_list_zero<<<dim3(64, g.nranks), 256, 0, st>>>(a);
+    k_capture<Real><<<nblocks, LIST_NT, 0, st>>>(a);
+    k_apply<<<148 * 4, 256, 0, st>>>(a);
+    n += 5;
+    return n;
+}
+
+int launch_step(const KernelArgs &a, int precision, void *stream, int start_stage)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == MMS_PREC_F32) return launch_step_t<float>(a, st, start_stage);
+    return launch_step_t<double>(a, st, start_stage);
+}
+
+int launch_temp_am(const KernelArgs &a, void *stream, double lsd, double lv, double lhs, double lab,
+                   double lpow, double liniT, double lthcon, double rho_cp, double x0, double y0,
+                   double z0, int amtracks, int nsbx_times_sbx)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    int nb = (int)((a.g.N + 255) / 256);
+    k_temp_am<<<nb, 256, 0, st>>>(a, lsd, lv, lhs, lab, lpow, liniT, lthcon, rho_cp, x0, y0, z0,
+                                  amtracks, nsbx_times_sbx);
+    return 1;
+}
+
+int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nb = 148 * 4;
+    double *partial = a.d.red;
+    if (precision == MMS_PREC_F32) k_reduce<float><<<nb, RED_NT, 0, st>>>(a, what, partial);
+    else k_reduce<double><<<nb, RED_NT, 0, st>>>(a, what, partial);
+    static thread_local double h[2 * 148 * 4];
+    cudaMemcpyAsync(h, partial, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    double s = 0, c = 0;
+    for (int b = 0; b < nb; b++) {
+        double x = h[2 * b];
+        double t = s + x, bp = t - s;
+        c += (s - (t - bp)) + (x - bp) + h[2 * b + 1];
+        s = t;
+    }
+    *host_out = s + c;
+    return 1;
+}
+
+int launch_compute_d(const KernelArgs &a, int precision, double *dev_out, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    int nb = (int)((a.g.N + 255) / 256);
+    if (precision == MMS_PREC_F32) k_compute_d<float><<<nb, 256, 0, st>>>(a, dev_out);
+    else k_compute_d<double><<<nb, 256, 0, st>>>(a, dev_out);
+    return 1;
+}
+
+int launch_fill_temperature(const KernelArgs &a, double *dev_out, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    int nb = (int)((a.g.N + 255) / 256);
+    k_fill_temperature<<<nb, 256, 0, st>>>(a, dev_out);
+    return 1;
+}
+
+int launch_convert(const KernelArgs &a, int precision, int field, int to_device, double *dev_f64,
+                   void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    int nb = (int)((a.g.N + 255) / 256);
+    if (precision == MMS_PREC_F32) k_convert<float><<<nb, 256, 0, st>>>(a, field, to_device, dev_f64);
+    else k_convert<double><<<nb, 256, 0, st>>>(a, field, to_device, dev_f64);
+    return 1;
+}
+
+}  // namespace mms

@@ -1,0 +1,1196 @@
+// mms_api.cu — host side of the C ABI declared in include/mms.h.
+//
+// Owns one device-resident domain per context, applies the reference's
+// initial state and nucleation-site draws on the host (they are defined by
+// glibc rand() streams and must be replayed exactly), and drives the
+// per-step kernel sequence of kernels.cu on one CUDA stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cerrno>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <sys/time.h>
+#include <unordered_map>
+#include <vector>
+
+#include "mms_internal.h"
+
+using namespace mms;
+
+namespace {
+
+// One emulated MPI rank: its rand() stream (srand(rank+1+seed),
+// ca_main.c:215) and its list of deck-defined nucleation points (nuc_pt).
+struct NucPt {  // nucleation_t, globals.h:147-160
+    double x, y, z;
+    size_t cx, cy, cz;
+    double gx, gy, gz;
+    double threshold;
+};
+
+struct Rank {
+    struct random_data rd;
+    char state[128];
+    unsigned seed = 0;
+    long ncalls = 0;
+    long ncalls_presb = 0;  // calls made before init_sb_nucleation
+    int have_gauss = 0;
+    float gauss_next = 0.f;
+    int sbx = 0, sby = 0, sbz = 0;
+    std::vector<NucPt> nuc;
+    std::vector<std::array<double, 3>> angles;  // orientation draws after setup
+    long long rng_base = 0;                     // draw number of device table entry 0
+
+    void seed_with(unsigned s)
+    {
+        std::memset(&rd, 0, sizeof rd);
+        std::memset(state, 0, sizeof state);
+        initstate_r(s, state, sizeof state, &rd);
+        seed = s;
+        ncalls = 0;
+        have_gauss = 0;
+        gauss_next = 0.f;
+    }
+    int32_t rand_()
+    {
+        int32_t v;
+        random_r(&rd, &v);
+        ncalls++;
+        return v;
+    }
+    // getRandScale, functions.c:440-445
+    float scale() { return (float)rand_() / (float)RAND_MAX; }
+    // getRandomGaussian, functions.c:376-406
+    float gauss()
+    {
+        if (have_gauss) {
+            have_gauss = 0;
+            return gauss_next;
+        }
+        float n0, n1, s;
+        do {
+            n0 = ((float)rand_() / (float)(RAND_MAX / 2.0)) - 1.0;
+            n1 = ((float)rand_() / (float)(RAND_MAX / 2.0)) - 1.0;
+            s = n0 * n0 + n1 * n1;
+        } while (s >= 1.0 || s == 0);
+        float multiplier = sqrtf(-2.0 * log(s) / s);
+        float val = n0 * multiplier;
+        gauss_next = n1 * multiplier;
+        have_gauss = 1;
+        return val;
+    }
+};
+
+// nucleate_grain's rotation matrix (grain.c:314-336), row-major
+void rotmat_from_angles(double a0, double a1, double a2, double *R)
+{
+    double c0 = cos(a0), s0 = sin(a0), c1 = cos(a1), s1 = sin(a1), c2 = cos(a2), s2 = sin(a2);
+    R[0] = c2 * c0 - s2 * s1 * s0;          // [0][0]
+    R[3] = c2 * s0 + s2 * c1 * c0;          // [1][0]
+    R[6] = s2 * s1;                         // [2][0]
+    R[1] = -1. * s2 * c0 - c2 * c1 * s0;    // [0][1]
+    R[4] = -1. * s2 * s0 + c2 * c1 * c0;    // [1][1]
+    R[7] = c2 * s1;                         // [2][1]
+    R[2] = s1 * s0;                         // [0][2]
+    R[5] = -1. * s1 * c0;                   // [1][2]
+    R[8] = c1;                              // [2][2]
+}
+
+}  // namespace
+
+struct mms_ctx {
+    mms_params p{};
+    std::vector<mms_fixed_nuc> fixed;
+    std::vector<mms_nuc_volume> vols;
+    int prec = MMS_PREC_F64;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    KernelArgs ka{};
+    std::vector<Rank> ranks;
+    // host copy of the site list (sorted by emulated rank, local raster)
+    std::vector<long long> site_cell;
+    std::vector<float> site_thr;
+    std::vector<int> site_rank;
+    std::unordered_map<long long, size_t> site_index;  // cell -> site, built on demand
+    // deck nucleation points: key -> (rank, entry)
+    std::vector<std::pair<long long, std::pair<int, int>>> nucpt;
+    // orientation injection (host copy): key -> rotmat
+    std::vector<long long> inj_key;
+    std::vector<double> inj_rot;
+    // grain records rebuilt from the device log
+    std::vector<mms_grain> grains;
+    int grains_synced = 1;
+    Ctl *h_ctl = nullptr;  // pinned
+    uint64_t launches = 0;
+    bool stepped = false;
+    std::string err;
+    size_t bytes = 0;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+#define CU(call)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);              \
+            return MMS_ERR_CUDA;                                                        \
+        }                                                                               \
+    } while (0)
+
+template <typename T>
+mms_status dalloc(mms_ctx *ctx, T **ptr, size_t count)
+{
+    void *p = nullptr;
+    size_t bytes = sizeof(T) * (count ? count : 1);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return MMS_ERR_NOMEM;
+    }
+    cudaMemsetAsync(p, 0, bytes, ctx->stream);
+    ctx->allocs.push_back(p);
+    ctx->bytes += bytes;
+    *ptr = (T *)p;
+    return MMS_OK;
+}
+
+void dfree(mms_ctx *ctx, void *p)
+{
+    if (!p) return;
+    cudaFree(p);
+    ctx->allocs.erase(std::remove(ctx->allocs.begin(), ctx->allocs.end(), p), ctx->allocs.end());
+}
+
+long long cidx(const Geo &g, long long i, long long j, long long k) { return k * g.sz + j * g.sy + i; }
+
+// realcoord2scoord, functions.c:91-107
+void real2cell(const mms_params &p, double x, double y, double z, size_t *i, size_t *j, size_t *k)
+{
+    x = x - p.origin_offset[0] + p.cellSize * 0.1;
+    y = y - p.origin_offset[1] + p.cellSize * 0.1;
+    z = z - p.origin_offset[2] + p.cellSize * 0.1;
+    *i = (size_t)(x / p.cellSize);
+    *j = (size_t)(y / p.cellSize);
+    *k = (size_t)(z / p.cellSize);
+}
+
+// CELLCOORD2REALCOORDn, functions.h:284-286
+double cell2real(const mms_params &p, int axis, double i) { return p.origin_offset[axis] + (i + 0.5) * p.cellSize; }
+
+int rank_of_cell(const mms_params &p, size_t cx, size_t cy, size_t cz)
+{
+    long x = (long)(cx / (size_t)p.gsdimx), y = (long)(cy / (size_t)p.gsdimy), z = (long)(cz / (size_t)p.gsdimz);
+    if (!p.padBndyX) x = (x + p.gnsbx) % p.gnsbx;
+    if (!p.padBndyY) y = (y + p.gnsby) % p.gnsby;
+    if (!p.padBndyZ) z = (z + p.gnsbz) % p.gnsbz;
+    if (x < 0 || y < 0 || z < 0 || x >= p.gnsbx || y >= p.gnsby || z >= p.gnsbz) return -1;
+    return (int)(x + y * p.gnsbx + z * p.gnsbx * p.gnsby);
+}
+
+// setNucOrientation, grain.c:117-130
+void draw_orientation(const mms_params &p, Rank &r, NucPt &n)
+{
+    n.gx = n.gy = n.gz = 0.0;
+    if (p.gnUseOrientation) {
+        float acon = 4.0;
+        n.gx = M_PI / acon - 2 * (M_PI / acon * r.scale());
+        n.gy = M_PI / acon - 2 * (M_PI / acon * r.scale());
+        n.gz = M_PI / acon - 2 * (M_PI / acon * r.scale());
+    }
+}
+
+// distribute_nucleations (Knuth Algorithm S), grain.c:250-296
+template <typename F>
+void algorithm_s(Rank &r, size_t nc, size_t num, F select)
+{
+    size_t n = std::min(num, nc);
+    size_t N = nc, t = 0, m = 0, idx = 0;
+    if (n == 0) return;
+    do {
+        double U = r.scale();
+        if ((N - t) * U >= (n - m)) {
+            t++;
+        } else {
+            select(idx);
+            t++;
+            m++;
+        }
+        idx++;
+    } while (m < n);
+}
+
+// genRandomThreshold, grain.c:140-154
+float random_threshold(Rank &r, double center, double sigma)
+{
+    float t = 0.0;
+    do {
+        t = (float)(sigma * r.gauss() + center);
+    } while ((t < 1.0e-5) || (fabs(t - center) > (6.0 * sigma)));
+    return t;
+}
+
+// Host-side initial state: SetupInitialConditions (setup.c:41-94),
+// init_nucleation_sites (grain.c:602-713, rank 0) and init_sb_nucleation
+// (grain.c:930-1010, every rank).  Produces the dense threshold array.
+void setup_sites(mms_ctx *ctx, std::vector<float> &thr, const std::vector<signed char> &mold)
+{
+    const mms_params &p = ctx->p;
+    const Geo &g = ctx->ka.g;
+    Rank &r0 = ctx->ranks[0];
+    std::vector<NucPt> all;
+    for (const mms_fixed_nuc &f : ctx->fixed) {
+        NucPt n{};
+        n.x = f.x;
+        n.y = f.y;
+        n.z = f.z;
+        n.gx = (M_PI / 180.0) * f.ax;
+        n.gy = (M_PI / 180.0) * f.ay;
+        n.gz = (M_PI / 180.0) * f.az;
+        n.threshold = f.threshold;
+        real2cell(p, n.x, n.y, n.z, &n.cx, &n.cy, &n.cz);
+        all.push_back(n);
+    }
+    for (mms_nuc_volume v : ctx->vols) {
+        v.minx = std::max(v.minx, p.origin_offset[0]);
+        v.maxx = std::min(v.maxx, p.origin_offset[0] + (g.gx * p.cellSize));
+        v.miny = std::max(v.miny, p.origin_offset[1]);
+        v.maxy = std::min(v.maxy, p.origin_offset[1] + (g.gy * p.cellSize));
+        v.minz = std::max(v.minz, p.origin_offset[2]);
+        v.maxz = std::min(v.maxz, p.origin_offset[2] + (g.gz * p.cellSize));
+        size_t mn[3], mx[3];
+        real2cell(p, v.minx, v.miny, v.minz, &mn[0], &mn[1], &mn[2]);
+        real2cell(p, v.maxx, v.maxy, v.maxz, &mx[0], &mx[1], &mx[2]);
+        size_t count = (mx[0] - mn[0]) * (mx[1] - mn[1]) * (mx[2] - mn[2]);
+        size_t max_nucs = count * v.density;
+        size_t nx = mx[0] - mn[0], ny = mx[1] - mn[1];
+        algorithm_s(r0, count, max_nucs, [&](size_t index) {  // select_nuc_volume, grain.c:173-210
+            NucPt n{};
+            n.cx = mn[0] + index % nx;
+            n.cy = mn[1] + (index % (nx * ny)) / nx;
+            n.cz = mn[2] + index / (nx * ny);
+            n.threshold = v.threshold;
+            draw_orientation(p, r0, n);
+            n.x = cell2real(p, 0, (double)n.cx);
+            n.y = cell2real(p, 1, (double)n.cy);
+            n.z = cell2real(p, 2, (double)n.cz);
+            all.push_back(n);
+        });
+    }
+    for (const NucPt &n : all) {
+        size_t cx, cy, cz;
+        real2cell(p, n.x, n.y, n.z, &cx, &cy, &cz);
+        int sb = rank_of_cell(p, cx, cy, cz);
+        if (sb >= 0) ctx->ranks[sb].nuc.push_back(n);
+    }
+    // init_sb_nucleation per rank
+    const long long sbcells = g.sbcells;
+    std::vector<long long> vol, suf;
+    vol.reserve(sbcells);
+    suf.reserve(sbcells);
+    for (int ri = 0; ri < g.nranks; ri++) {
+        Rank &r = ctx->ranks[ri];
+        r.ncalls_presb = r.ncalls;
+        auto rcell = [&](long long i, long long j, long long k) {
+            return cidx(g, (long long)r.sbx * p.gsdimx + i, (long long)r.sby * p.gsdimy + j,
+                        (long long)r.sbz * p.gsdimz + k);
+        };
+        for (const NucPt &n : r.nuc) {
+            long long c = rcell(1 + (long long)(n.cx % (size_t)p.gsdimx), 1 + (long long)(n.cy % (size_t)p.gsdimy),
+                                1 + (long long)(n.cz % (size_t)p.gsdimz));
+            if (!mold[c]) thr[c] = (float)n.threshold;
+        }
+        vol.clear();
+        suf.clear();
+        for (long long z = 1; z <= p.gsdimz; z++)
+            for (long long y = 1; y <= p.gsdimy; y++)
+                for (long long x = 1; x <= p.gsdimx; x++) {
+                    long long c = rcell(x, y, z);
+                    if (!mold[c]) {
+                        vol.push_back(c);
+                        int surf = mold[c - 1] + mold[c + 1] + mold[c - g.sy] + mold[c + g.sy] + mold[c - g.sz] +
+                                   mold[c + g.sz];
+                        if (surf) suf.push_back(c);
+                    }
+                }
+        size_t v = vol.size(), s = suf.size();
+        double center = p.gnGaussCenter, sigma = p.gnGaussSigma;
+        auto sel = [&](const std::vector<long long> &cells) {
+            return [&, cells_ptr = &cells](size_t index) {  // select_if_not_fixed, grain.c:225-237
+                long long c = (*cells_ptr)[index];
+                if (thr[c] == INFINITY) thr[c] = random_threshold(r, center, sigma);
+            };
+        };
+        size_t count = p.maxGrainDensity * (v * pow(p.cellSize, 3.0));
+        algorithm_s(r, v, count, sel(vol));
+        if (p.doSurfaceNuc && (p.maxGrainDensitySurf > 0.0)) {
+            center = p.gnGaussCenterSurf;
+            sigma = p.gnGaussSigmaSurf;
+            count = p.maxGrainDensitySurf * (s * pow(p.cellSize, 2.0));
+            algorithm_s(r, s, count, sel(suf));
+        }
+    }
+}
+
+// Extract the sparse site list in (rank, local raster) order.
+void extract_sites(mms_ctx *ctx, const std::vector<float> &thr)
+{
+    const mms_params &p = ctx->p;
+    const Geo &g = ctx->ka.g;
+    ctx->site_cell.clear();
+    ctx->site_thr.clear();
+    ctx->site_rank.clear();
+    ctx->site_index.clear();
+    for (int ri = 0; ri < g.nranks; ri++) {
+        const Rank &r = ctx->ranks[ri];
+        for (long long z = 1; z <= p.gsdimz; z++)
+            for (long long y = 1; y <= p.gsdimy; y++)
+                for (long long x = 1; x <= p.gsdimx; x++) {
+                    long long c = cidx(g, (long long)r.sbx * p.gsdimx + x, (long long)r.sby * p.gsdimy + y,
+                                       (long long)r.sbz * p.gsdimz + z);
+                    if (thr[c] != INFINITY) {
+                        ctx->site_cell.push_back(c);
+                        ctx->site_thr.push_back(thr[c]);
+                        ctx->site_rank.push_back(ri);
+                    }
+                }
+    }
+}
+
+mms_status upload_sites(mms_ctx *ctx)
+{
+    DevPtrs &d = ctx->ka.d;
+    dfree(ctx, d.site_cell);
+    dfree(ctx, d.site_thr);
+    dfree(ctx, d.site_rank);
+    dfree(ctx, d.site_flag);
+    dfree(ctx, d.cand);
+    d.site_cell = nullptr;
+    d.site_thr = nullptr;
+    d.site_rank = nullptr;
+    d.site_flag = nullptr;
+    d.cand = nullptr;
+    size_t n = ctx->site_cell.size();
+    d.nsites = (long long)n;
+    mms_status st;
+    if ((st = dalloc(ctx, &d.site_cell, n)) || (st = dalloc(ctx, &d.site_thr, n)) ||
+        (st = dalloc(ctx, &d.site_rank, n)) || (st = dalloc(ctx, &d.site_flag, n)) || (st = dalloc(ctx, &d.cand, n)))
+        return st;
+    if (n) {
+        CU(cudaMemcpyAsync(d.site_cell, ctx->site_cell.data(), n * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(d.site_thr, ctx->site_thr.data(), n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(d.site_rank, ctx->site_rank.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+    return MMS_OK;
+}
+
+// nuc_pt lookup table: key = global halo'd cell, first entry of the rank's
+// list wins (createGrains' linear search, grain.c:392-401).
+mms_status upload_nucpt(mms_ctx *ctx)
+{
+    const Geo &g = ctx->ka.g;
+    DevPtrs &d = ctx->ka.d;
+    ctx->nucpt.clear();
+    for (int ri = 0; ri < g.nranks; ri++) {
+        const Rank &r = ctx->ranks[ri];
+        for (int j = 0; j < (int)r.nuc.size(); j++) {
+            const NucPt &n = r.nuc[j];
+            if (n.cx >= (size_t)g.gx || n.cy >= (size_t)g.gy || n.cz >= (size_t)g.gz) continue;
+            long long key = cidx(g, (long long)n.cx + 1, (long long)n.cy + 1, (long long)n.cz + 1);
+            ctx->nucpt.push_back({key, {ri, j}});
+        }
+    }
+    std::stable_sort(ctx->nucpt.begin(), ctx->nucpt.end(),
+                     [](const auto &a, const auto &b) { return a.first < b.first; });
+    size_t n = ctx->nucpt.size();
+    std::vector<long long> keys(n), entry(n);
+    std::vector<double> rot(9 * (n ? n : 1));
+    for (size_t i = 0; i < n; i++) {
+        keys[i] = ctx->nucpt[i].first;
+        entry[i] = ((long long)ctx->nucpt[i].second.first << 32) | (unsigned)ctx->nucpt[i].second.second;
+        const NucPt &np = ctx->ranks[ctx->nucpt[i].second.first].nuc[ctx->nucpt[i].second.second];
+        rotmat_from_angles(np.gx, np.gy, np.gz, &rot[9 * i]);
+    }
+    mms_status st;
+    dfree(ctx, d.nucpt_key);
+    dfree(ctx, d.nucpt_entry);
+    dfree(ctx, d.nucpt_rot);
+    if ((st = dalloc(ctx, &d.nucpt_key, n)) || (st = dalloc(ctx, &d.nucpt_entry, n)) || (st = dalloc(ctx, &d.nucpt_rot, 9 * n)))
+        return st;
+    d.n_nucpt = (long long)n;
+    if (n) {
+        CU(cudaMemcpyAsync(d.nucpt_key, keys.data(), n * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(d.nucpt_entry, entry.data(), n * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+        CU(cudaMemcpyAsync(d.nucpt_rot, rot.data(), 9 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+    return MMS_OK;
+}
+
+// Refill every rank's device table of orientation draws so that it starts
+// at the first unconsumed draw.  Called only with the stream idle.
+mms_status refill_rng(mms_ctx *ctx, bool force)
+{
+    const Geo &g = ctx->ka.g;
+    DevPtrs &d = ctx->ka.d;
+    if (!ctx->p.gnUseOrientation) return MMS_OK;
+    std::vector<int> used(g.nranks);
+    CU(cudaMemcpy(used.data(), d.rng_used, sizeof(int) * g.nranks, cudaMemcpyDeviceToHost));
+    bool any = force;
+    for (int r = 0; r < g.nranks; r++)
+        if (used[r] * 2 > d.rng_cap) any = true;
+    if (!any) return MMS_OK;
+    std::vector<double> tab((size_t)g.nranks * d.rng_cap * 9);
+    std::vector<long long> base(g.nranks);
+    for (int ri = 0; ri < g.nranks; ri++) {
+        Rank &r = ctx->ranks[ri];
+        r.rng_base += used[ri];
+        while ((long long)r.angles.size() < r.rng_base + d.rng_cap) {
+            NucPt n{};
+            draw_orientation(ctx->p, r, n);
+            r.angles.push_back({n.gx, n.gy, n.gz});
+        }
+        for (int k = 0; k < d.rng_cap; k++) {
+            const auto &a = r.angles[r.rng_base + k];
+            rotmat_from_angles(a[0], a[1], a[2], &tab[((size_t)ri * d.rng_cap + k) * 9]);
+        }
+        base[ri] = r.rng_base;
+    }
+    CU(cudaMemcpy(d.rng_rot, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(d.rng_base, base.data(), sizeof(long long) * g.nranks, cudaMemcpyHostToDevice));
+    CU(cudaMemset(d.rng_used, 0, sizeof(int) * g.nranks));
+    return MMS_OK;
+}
+
+void set_status(mms_ctx *ctx, mms_status s, const char *msg)
+{
+    if (msg) ctx->err = msg;
+    (void)s;
+}
+
+mms_status read_ctl(mms_ctx *ctx)
+{
+    CU(cudaMemcpyAsync(ctx->h_ctl, ctx->ka.d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return MMS_OK;
+}
+
+int launch_one_step(mms_ctx *ctx, int start_stage)
+{
+    int n = 0;
+    const mms_params &p = ctx->p;
+    if (start_stage == 0 && p.am) {
+        n += launch_temp_am(ctx->ka, ctx->stream, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
+                            p.rho * p.lcp, p.x0, p.y0, p.z0, p.amtracks, p.gnsbx * p.gsdimx);
+    }
+    n += launch_step(ctx->ka, ctx->prec, ctx->stream, start_stage);
+    return n;
+}
+
+// Pull grain records created since the last sync and rebuild grain_t.
+mms_status sync_grains(mms_ctx *ctx)
+{
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    int ng = ctx->h_ctl->num_grains;
+    if (ng <= ctx->grains_synced) return MMS_OK;
+    int first = ctx->grains_synced, cnt = ng - first;
+    std::vector<GrainLog> log(cnt);
+    CU(cudaMemcpy(log.data(), ctx->ka.d.grain_log + first, sizeof(GrainLog) * cnt, cudaMemcpyDeviceToHost));
+    if ((int)ctx->grains.size() < ng) ctx->grains.resize(ng);
+    const mms_params &p = ctx->p;
+    const Geo &g = ctx->ka.g;
+    for (int i = 0; i < cnt; i++) {
+        const GrainLog &lg = log[i];
+        mms_grain &gr = ctx->grains[first + i];
+        std::memset(&gr, 0, sizeof gr);
+        long long c = lg.cell;
+        long long K = c / g.sz, J = (c % g.sz) / g.sy, I = c % g.sy;
+        NucPt nuc{};
+        if (lg.kind == 0) {
+            int rr = (int)(lg.aux >> 32), jj = (int)(lg.aux & 0xffffffff);
+            nuc = ctx->ranks[rr].nuc[jj];
+        } else {
+            nuc.x = cell2real(p, 0, (double)(I - 1));
+            nuc.y = cell2real(p, 1, (double)(J - 1));
+            nuc.z = cell2real(p, 2, (double)(K - 1));
+            if (ctx->site_index.empty())
+                for (size_t s = 0; s < ctx->site_cell.size(); s++) ctx->site_index.emplace(ctx->site_cell[s], s);
+            auto it = ctx->site_index.find(c);
+            double thr = (it == ctx->site_index.end()) ? (double)INFINITY : (double)ctx->site_thr[it->second];
+            nuc.threshold = thr;
+            if (lg.kind == 1) {
+                const auto &a = ctx->ranks[lg.rank].angles[lg.aux];
+                nuc.gx = a[0];
+                nuc.gy = a[1];
+                nuc.gz = a[2];
+            }
+        }
+        double R[9];
+        rotmat_from_angles(nuc.gx, nuc.gy, nuc.gz, R);
+        auto ik = std::lower_bound(ctx->inj_key.begin(), ctx->inj_key.end(), c);
+        if (ik != ctx->inj_key.end() && *ik == c) std::memcpy(R, &ctx->inj_rot[9 * (ik - ctx->inj_key.begin())], sizeof R);
+        gr.nuc_x = nuc.x;
+        gr.nuc_y = nuc.y;
+        gr.nuc_z = nuc.z;
+        gr.nuc_timestep = lg.timestep;
+        gr.nuc_threshold = nuc.threshold;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) gr.rotmat[a][b] = R[3 * a + b];
+        gr.rotang[0] = nuc.gx;
+        gr.rotang[1] = nuc.gy;
+        gr.rotang[2] = nuc.gz;
+    }
+    ctx->grains_synced = ng;
+    return MMS_OK;
+}
+
+}  // namespace
+
+// ============================================================= public ABI
+extern "C" {
+
+const char *mms_status_string(mms_status s)
+{
+    switch (s) {
+    case MMS_OK: return "ok";
+    case MMS_ERR_ARG: return "invalid argument";
+    case MMS_ERR_CUDA: return "CUDA error";
+    case MMS_ERR_NO_DEVICE: return "no usable CUDA device";
+    case MMS_ERR_COURANT: return "Instability by Courant criterion, lower calculation time step";
+    case MMS_ERR_NEGATIVE_CE: return "negative ce: instability by Courant criterion";
+    case MMS_ERR_GRAIN_OVERFLOW: return "grain id beyond MaxTotGrains";
+    case MMS_ERR_DECK: return "input deck error";
+    case MMS_ERR_IO: return "file I/O error";
+    case MMS_ERR_TIMEOUT: return "device wait timed out";
+    case MMS_ERR_STATE: return "call made in the wrong state";
+    case MMS_ERR_NOMEM: return "out of memory";
+    }
+    return "unknown status";
+}
+
+const char *mms_last_error(const mms_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+uint64_t mms_kernel_launches(const mms_ctx *ctx) { return ctx ? ctx->launches : 0; }
+size_t mms_num_cells(const mms_ctx *ctx) { return ctx ? (size_t)ctx->ka.g.N : 0; }
+
+mms_status mms_create(const mms_params *pin, mms_ctx **out)
+{
+    if (!pin || !out) return MMS_ERR_ARG;
+    *out = nullptr;
+    const mms_params &p0 = *pin;
+    if (p0.gnsbx < 1 || p0.gnsby < 1 || p0.gnsbz < 1 || p0.gsdimx < 1 || p0.gsdimy < 1 || p0.gsdimz < 1 ||
+        p0.cellSize <= 0 || p0.ts_delt <= 0 || p0.maxTotalGrains < 1 || p0.maxTotalGrains > 0x7ffffffeULL)
+        return MMS_ERR_ARG;
+    if ((!p0.padBndyX && p0.gnsbx > 1) || (!p0.padBndyY && p0.gnsby > 1) || (!p0.padBndyZ && p0.gnsbz > 1))
+        return MMS_ERR_ARG;  // periodic exchange between subblocks is not supported
+    if (p0.am && p0.thermal_ana != 1) return MMS_ERR_ARG;
+    if (p0.precision != MMS_PREC_F64 && p0.precision != MMS_PREC_F32) return MMS_ERR_ARG;
+    // Courant check, growth.c:38-50
+    double dtx = p0.ts_delt / (p0.cellSize * p0.cellSize);
+    if (p0.Dsol * dtx > p0.courant_limit || p0.Dliq * dtx > p0.courant_limit) return MMS_ERR_COURANT;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p0.device) return MMS_ERR_NO_DEVICE;
+
+    mms_ctx *ctx = new mms_ctx();
+    ctx->p = p0;
+    for (int i = 0; i < p0.n_fixed_nucs; i++) ctx->fixed.push_back(p0.fixed_nucs[i]);
+    for (int i = 0; i < p0.n_nuc_volumes; i++) ctx->vols.push_back(p0.nuc_volumes[i]);
+    ctx->p.fixed_nucs = nullptr;
+    ctx->p.nuc_volumes = nullptr;
+    ctx->prec = p0.precision;
+    ctx->device = p0.device;
+    const mms_params &p = ctx->p;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) {
+        delete ctx;
+        return MMS_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, ctx->device);
+    if (prop.major < 10) {
+        delete ctx;
+        return MMS_ERR_NO_DEVICE;
+    }
+    cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    cudaMallocHost((void **)&ctx->h_ctl, sizeof(Ctl));
+
+    Geo &g = ctx->ka.g;
+    g.gx = p.gnsbx * p.gsdimx;
+    g.gy = p.gnsby * p.gsdimy;
+    g.gz = p.gnsbz * p.gsdimz;
+    g.sy = g.gx + 2;
+    g.sz = (long long)(g.gx + 2) * (g.gy + 2);
+    g.N = g.sz * (g.gz + 2);
+    g.sbx = p.gsdimx;
+    g.sby = p.gsdimy;
+    g.sbz = p.gsdimz;
+    g.nsbx = p.gnsbx;
+    g.nsby = p.gnsby;
+    g.nsbz = p.gnsbz;
+    g.nranks = p.gnsbx * p.gnsby * p.gnsbz;
+    g.sbcells = (long long)p.gsdimx * p.gsdimy * p.gsdimz;
+    g.padx = p.padBndyX;
+    g.pady = p.padBndyY;
+    g.padz = p.padBndyZ;
+    g.vb = 2048;
+    g.blocks_per_rank = (g.sbcells + g.vb - 1) / g.vb;
+
+    Phys &ph = ctx->ka.p;
+    ph.rs = p.Dsol * dtx;
+    ph.rl = p.Dliq * dtx;
+    ph.liq_slope = p.m_solute0;
+    ph.k_inv = 1.0 / p.part_coef;
+    ph.km = 1.0 - p.part_coef;
+    ph.km_inv = 1.0 / ph.km;
+    ph.m_inv = 1.0 / ph.liq_slope;
+    ph.D_xt = (p.Dliq / p.cellSize / p.cellSize) * p.ts_delt;
+    ph.cinit = p.Cinit;
+    ph.Tliq = p.liquidusTemp;
+    ph.Tsol = p.solidusTemp;
+    ph.tip_curv = p.tip_curv;
+    ph.gibbs = p.gibbs_coef;
+    ph.fsgrow = p.rev_fsgrow;
+    ph.max_grains = p.maxTotalGrains;
+    ph.ma = p.m_solute0_a;
+    ph.mb = p.m_solute0_b;
+    ph.mc = p.m_solute0_c;
+    ph.temp_mode = (p.thermal_ana == 0 && p.gradient == 0) ? 0 : (!p.am ? 1 : 2);
+    ph.T0 = p.initialTemperature;
+    ph.cool_rate = p.cool_rate;
+    ph.gradient = p.gradient;
+    ph.grad_coef = p.grad_coef;
+    ph.velocity = p.velocity;
+    ph.velo_coef = p.velo_coef;
+    ph.ts_delt = p.ts_delt;
+    ph.cellSize = p.cellSize;
+    for (int a = 0; a < 3; a++) ph.origin[a] = p.origin_offset[a];
+    ph.gz_is_one = (g.gz == 1);
+    ph.am = p.am;
+    ph.amlayer = p.amlayer;
+    ph.use_orientation = p.gnUseOrientation;
+    ph.cellSize3 = pow(p.cellSize, 3.0);
+
+    mms_status st = MMS_OK;
+    DevPtrs &d = ctx->ka.d;
+    const size_t N = (size_t)g.N;
+    const size_t rs = ctx->prec == MMS_PREC_F32 ? sizeof(float) : sizeof(double);
+    auto fail = [&](mms_status s) {
+        mms_destroy(ctx);
+        return s;
+    };
+    char *tmp;
+    if ((st = dalloc(ctx, &tmp, N * rs))) return fail(st);
+    d.ce = tmp;
+    for (int b = 0; b < 2; b++) {
+        if ((st = dalloc(ctx, &tmp, N * rs))) return fail(st);
+        d.cl[b] = tmp;
+        if ((st = dalloc(ctx, &tmp, N * rs))) return fail(st);
+        d.fs[b] = tmp;
+    }
+    if ((st = dalloc(ctx, &d.gr, N)) || (st = dalloc(ctx, &d.dc, N)) || (st = dalloc(ctx, &d.ctl, 1)))
+        return fail(st);
+    if (p.am) {
+        if ((st = dalloc(ctx, &d.T, N))) return fail(st);
+        if (p.amlayer > 1 && (st = dalloc(ctx, &d.lsindex, N))) return fail(st);
+    }
+    if (p.tip_curv && (st = dalloc(ctx, &d.curv, N))) return fail(st);
+    const size_t nb = (size_t)(g.blocks_per_rank * g.nranks);
+    if ((st = dalloc(ctx, &d.blk_cnt, nb)) || (st = dalloc(ctx, &d.blk_off, nb)) ||
+        (st = dalloc(ctx, &d.rank_gindex, g.nranks)) || (st = dalloc(ctx, &d.rank_dcsize, g.nranks)) ||
+        (st = dalloc(ctx, &d.rank_zero_upto, g.nranks)) || (st = dalloc(ctx, &d.rank_dcbase, g.nranks)) ||
+        (st = dalloc(ctx, &d.list_cell, (size_t)g.nranks * g.sbcells)) ||
+        (st = dalloc(ctx, &d.list_gid, (size_t)g.nranks * g.sbcells)) ||
+        (st = dalloc(ctx, &d.dc_tmp, (size_t)g.nranks * (g.sbcells + 101))) ||
+        (st = dalloc(ctx, &d.red, 2 * 148 * 4)) || (st = dalloc(ctx, &d.act_scratch, 4 * g.nranks)) ||
+        (st = dalloc(ctx, &d.rng_used, g.nranks)) || (st = dalloc(ctx, &d.rng_base, g.nranks)) ||
+        (st = dalloc(ctx, &d.grain_rot, 9 * (p.maxTotalGrains + 1))) ||
+        (st = dalloc(ctx, &d.grain_log, p.maxTotalGrains + 2)))
+        return fail(st);
+    {
+        std::vector<long long> base(g.nranks);
+        for (int r = 0; r < g.nranks; r++) base[r] = (long long)r * (g.sbcells + 101);
+        if (cudaMemcpy(d.rank_dcbase, base.data(), sizeof(long long) * g.nranks, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(MMS_ERR_CUDA);
+    }
+    {
+        double zr[9];
+        rotmat_from_angles(0.0, 0.0, 0.0, zr);
+        std::memcpy(d.zero_rot, zr, sizeof zr);
+    }
+
+    // ranks and their streams
+    ctx->ranks.resize(g.nranks);
+    for (int r = 0; r < g.nranks; r++) {
+        Rank &rk = ctx->ranks[r];
+        rk.sbx = r % p.gnsbx;
+        rk.sby = (r / p.gnsbx) % p.gnsby;
+        rk.sbz = r / (p.gnsbx * p.gnsby);
+        rk.seed_with((unsigned)r + 1 + p.base_random_seed);
+    }
+    // initial fields: ce = cl = Cinit everywhere, fs = gr = dc = 0 (setup.c:59-79)
+    std::vector<signed char> mold(N, 0);
+    for (long long K = 0; K < g.gz + 2; K++)
+        for (long long J = 0; J < g.gy + 2; J++)
+            for (long long I = 0; I < g.gx + 2; I++) {
+                int m = 0;
+                if (p.padBndyX && (I == 0 || I == g.gx + 1)) m = 1;
+                if (p.padBndyY && (J == 0 || J == g.gy + 1)) m = 1;
+                if (p.padBndyZ && (K == 0 || K == g.gz + 1)) m = 1;
+                mold[cidx(g, I, J, K)] = (signed char)m;
+            }
+    {
+        std::vector<double> init(N, p.Cinit);
+        double *dtmp;
+        if ((st = dalloc(ctx, &dtmp, N))) return fail(st);
+        if (cudaMemcpy(dtmp, init.data(), N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(MMS_ERR_CUDA);
+        ctx->launches += launch_convert(ctx->ka, ctx->prec, MMS_FIELD_CE, 1, dtmp, ctx->stream);
+        ctx->launches += launch_convert(ctx->ka, ctx->prec, MMS_FIELD_CL, 1, dtmp, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+        dfree(ctx, dtmp);
+    }
+    if (p.am && p.amlayer > 1) {
+        // tempPrepareSB_int lsindex (temperature.c:183-189) at timestep 0
+        ctx->launches += launch_temp_am(ctx->ka, ctx->stream, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
+                                        p.rho * p.lcp, p.x0, p.y0, p.z0, p.amtracks, p.gnsbx * p.gsdimx);
+    }
+    std::vector<float> thr(N, INFINITY);
+    setup_sites(ctx, thr, mold);
+    extract_sites(ctx, thr);
+    if ((st = upload_sites(ctx)) || (st = upload_nucpt(ctx))) return fail(st);
+    // orientation tables
+    if (p.gnUseOrientation) {
+        long long maxsites = 0;
+        std::vector<long long> per(g.nranks, 0);
+        for (int r : ctx->site_rank) per[r]++;
+        for (long long v : per) maxsites = std::max(maxsites, v);
+        d.rng_cap = (int)std::min<long long>(std::max<long long>(256, 2 * maxsites + 256), 1 << 22);
+        if ((st = dalloc(ctx, &d.rng_rot, (size_t)g.nranks * d.rng_cap * 9))) return fail(st);
+        if ((st = refill_rng(ctx, true))) return fail(st);
+    }
+    {
+        Ctl c{};
+        c.timestep = 0;
+        c.num_grains = 1;  // the "zero" grain (read_ctrl.c:51)
+        if (cudaMemcpy(d.ctl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess) return fail(MMS_ERR_CUDA);
+    }
+    ctx->grains.resize(1);
+    std::memset(&ctx->grains[0], 0, sizeof(mms_grain));
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(MMS_ERR_CUDA);
+    if (cudaGetLastError() != cudaSuccess) return fail(MMS_ERR_CUDA);
+    *out = ctx;
+    return MMS_OK;
+}
+
+mms_status mms_destroy(mms_ctx *ctx)
+{
+    if (!ctx) return MMS_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (void *p : ctx->allocs) cudaFree(p);
+    ctx->allocs.clear();
+    if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return MMS_OK;
+}
+
+mms_status mms_set_sites(mms_ctx *ctx, int64_t n, const int32_t *gxyz, const float *thresholds)
+{
+    if (!ctx || (n && (!gxyz || !thresholds))) return MMS_ERR_ARG;
+    if (ctx->stepped) return MMS_ERR_STATE;
+    cudaSetDevice(ctx->device);
+    const Geo &g = ctx->ka.g;
+    std::vector<float> thr((size_t)g.N, INFINITY);
+    for (int64_t s = 0; s < n; s++) {
+        long long x = gxyz[3 * s], y = gxyz[3 * s + 1], z = gxyz[3 * s + 2];
+        if (x < 0 || y < 0 || z < 0 || x >= g.gx || y >= g.gy || z >= g.gz) return MMS_ERR_ARG;
+        thr[cidx(g, x + 1, y + 1, z + 1)] = thresholds[s];
+    }
+    // rewind every stream to where init_sb_nucleation would start drawing
+    for (Rank &r : ctx->ranks) {
+        long keep = r.ncalls_presb;
+        r.seed_with(r.seed);
+        while (r.ncalls < keep) r.rand_();
+        r.angles.clear();
+        r.rng_base = 0;
+    }
+    extract_sites(ctx, thr);
+    mms_status st = upload_sites(ctx);
+    if (st) return st;
+    if (ctx->p.gnUseOrientation) {
+        CU(cudaMemset(ctx->ka.d.rng_used, 0, sizeof(int) * g.nranks));
+        st = refill_rng(ctx, true);
+    }
+    return st;
+}
+
+mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxyz, const double *rotmat9)
+{
+    if (!ctx || (n && (!gxyz || !rotmat9))) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    const Geo &g = ctx->ka.g;
+    std::vector<std::pair<long long, int64_t>> kv;
+    for (int64_t s = 0; s < n; s++) {
+        long long x = gxyz[3 * s], y = gxyz[3 * s + 1], z = gxyz[3 * s + 2];
+        if (x < 0 || y < 0 || z < 0 || x >= g.gx || y >= g.gy || z >= g.gz) return MMS_ERR_ARG;
+        kv.push_back({cidx(g, x + 1, y + 1, z + 1), s});
+    }
+    std::stable_sort(kv.begin(), kv.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+    ctx->inj_key.clear();
+    ctx->inj_rot.clear();
+    for (size_t i = 0; i < kv.size(); i++) {
+        if (i > 0 && kv[i].first == kv[i - 1].first) continue;  // first listed wins
+        ctx->inj_key.push_back(kv[i].first);
+        for (int e = 0; e < 9; e++) ctx->inj_rot.push_back(rotmat9[9 * kv[i].second + e]);
+    }
+    DevPtrs &d = ctx->ka.d;
+    dfree(ctx, d.inj_key);
+    dfree(ctx, d.inj_rot);
+    d.inj_key = nullptr;
+    d.inj_rot = nullptr;
+    size_t m = ctx->inj_key.size();
+    mms_status st;
+    if ((st = dalloc(ctx, &d.inj_key, m)) || (st = dalloc(ctx, &d.inj_rot, 9 * m))) return st;
+    d.n_inj = (long long)m;
+    if (m) {
+        CU(cudaMemcpy(d.inj_key, ctx->inj_key.data(), m * sizeof(long long), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(d.inj_rot, ctx->inj_rot.data(), 9 * m * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    return MMS_OK;
+}
+
+mms_status mms_step(mms_ctx *ctx, int nsteps)
+{
+    if (!ctx || nsteps < 0) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    ctx->stepped = true;
+    const int chunk = 256;
+    int done = 0;
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    if (ctx->h_ctl->status) return (mms_status)ctx->h_ctl->status;
+    unsigned long long ts0 = ctx->h_ctl->timestep;
+    while (done < nsteps) {
+        int n = std::min(chunk, nsteps - done);
+        for (int s = 0; s < n; s++) ctx->launches += launch_one_step(ctx, 0);
+        CU(cudaGetLastError());
+        if ((st = read_ctl(ctx))) return st;
+        Ctl &c = *ctx->h_ctl;
+        if (c.stall == STALL_ERROR) {
+            ctx->err = mms_status_string((mms_status)c.status);
+            return (mms_status)(c.status ? c.status : MMS_ERR_STATE);
+        }
+        while (c.stall == STALL_RNG) {
+            // a rank ran out of pre-drawn orientations at step stall_step:
+            // refill, then resume that step at the activation stage
+            if ((st = refill_rng(ctx, true))) return st;
+            int zero = 0;
+            CU(cudaMemcpy(&ctx->ka.d.ctl->stall, &zero, sizeof(int), cudaMemcpyHostToDevice));
+            ctx->launches += launch_one_step(ctx, 1);
+            unsigned long long target = ts0 + done + n;
+            if ((st = read_ctl(ctx))) return st;
+            while (c.stall == 0 && c.timestep < target) {
+                ctx->launches += launch_one_step(ctx, 0);
+                if ((st = read_ctl(ctx))) return st;
+            }
+            if (c.stall == STALL_ERROR) return (mms_status)(c.status ? c.status : MMS_ERR_STATE);
+        }
+        done += n;
+        if ((st = refill_rng(ctx, false))) return st;
+    }
+    return MMS_OK;
+}
+
+mms_status mms_get_timestep(mms_ctx *ctx, uint64_t *timestep)
+{
+    if (!ctx || !timestep) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    *timestep = ctx->h_ctl->timestep;
+    return MMS_OK;
+}
+
+mms_status mms_get_num_grains(mms_ctx *ctx, int *num_grains)
+{
+    if (!ctx || !num_grains) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    *num_grains = ctx->h_ctl->num_grains;
+    return MMS_OK;
+}
+
+mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
+{
+    if (!ctx || !host) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    const Geo &g = ctx->ka.g;
+    const size_t N = (size_t)g.N;
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    const int cur = (int)(ctx->h_ctl->timestep & 1ULL);
+    DevPtrs &d = ctx->ka.d;
+    switch (field) {
+    case MMS_FIELD_CE:
+    case MMS_FIELD_CL:
+    case MMS_FIELD_FS: {
+        if (ctx->prec == MMS_PREC_F64) {
+            const void *src = field == MMS_FIELD_CE ? d.ce : (field == MMS_FIELD_CL ? d.cl[cur] : d.fs[cur]);
+            CU(cudaMemcpy(host, src, N * sizeof(double), cudaMemcpyDeviceToHost));
+        } else {
+            double *tmp;
+            if ((st = dalloc(ctx, &tmp, N))) return st;
+            ctx->launches += launch_convert(ctx->ka, ctx->prec, field, 0, tmp, ctx->stream);
+            CU(cudaMemcpyAsync(host, tmp, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
+            dfree(ctx, tmp);
+        }
+        return MMS_OK;
+    }
+    case MMS_FIELD_GR:
+        CU(cudaMemcpy(host, d.gr, N * sizeof(int), cudaMemcpyDeviceToHost));
+        return MMS_OK;
+    case MMS_FIELD_DC:
+        CU(cudaMemcpy(host, d.dc, N * sizeof(Dc3), cudaMemcpyDeviceToHost));
+        return MMS_OK;
+    case MMS_FIELD_D:
+    case MMS_FIELD_TEMPERATURE: {
+        double *tmp;
+        if ((st = dalloc(ctx, &tmp, N))) return st;
+        if (field == MMS_FIELD_D) ctx->launches += launch_compute_d(ctx->ka, ctx->prec, tmp, ctx->stream);
+        else ctx->launches += launch_fill_temperature(ctx->ka, tmp, ctx->stream);
+        CU(cudaMemcpyAsync(host, tmp, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, tmp);
+        return MMS_OK;
+    }
+    case MMS_FIELD_NUC_THRESHOLD: {
+        float *t = (float *)host;
+        for (size_t c = 0; c < N; c++) t[c] = INFINITY;
+        for (size_t s = 0; s < ctx->site_cell.size(); s++) t[ctx->site_cell[s]] = ctx->site_thr[s];
+        return MMS_OK;
+    }
+    case MMS_FIELD_MOLD: {
+        signed char *m = (signed char *)host;
+        for (long long K = 0; K < g.gz + 2; K++)
+            for (long long J = 0; J < g.gy + 2; J++)
+                for (long long I = 0; I < g.gx + 2; I++) {
+                    int v = 0;
+                    if (g.padx && (I == 0 || I == g.gx + 1)) v = 1;
+                    if (g.pady && (J == 0 || J == g.gy + 1)) v = 1;
+                    if (g.padz && (K == 0 || K == g.gz + 1)) v = 1;
+                    m[cidx(g, I, J, K)] = (signed char)v;
+                }
+        return MMS_OK;
+    }
+    }
+    return MMS_ERR_ARG;
+}
+
+mms_status mms_upload(mms_ctx *ctx, mms_field field, const void *host)
+{
+    if (!ctx || !host) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    const Geo &g = ctx->ka.g;
+    const size_t N = (size_t)g.N;
+    mms_status st;
+    DevPtrs &d = ctx->ka.d;
+    switch (field) {
+    case MMS_FIELD_CE:
+    case MMS_FIELD_CL:
+    case MMS_FIELD_FS: {
+        double *tmp;
+        if ((st = dalloc(ctx, &tmp, N))) return st;
+        CU(cudaMemcpyAsync(tmp, host, N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        ctx->launches += launch_convert(ctx->ka, ctx->prec, field, 1, tmp, ctx->stream);
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, tmp);
+        return MMS_OK;
+    }
+    case MMS_FIELD_GR:
+        CU(cudaMemcpy(d.gr, host, N * sizeof(int), cudaMemcpyHostToDevice));
+        return MMS_OK;
+    case MMS_FIELD_DC:
+        CU(cudaMemcpy(d.dc, host, N * sizeof(Dc3), cudaMemcpyHostToDevice));
+        return MMS_OK;
+    case MMS_FIELD_NUC_THRESHOLD: {
+        std::vector<float> thr((const float *)host, (const float *)host + N);
+        extract_sites(ctx, thr);
+        return upload_sites(ctx);
+    }
+    default:
+        return MMS_ERR_ARG;
+    }
+}
+
+mms_status mms_reduce(mms_ctx *ctx, mms_reduction what, double *out)
+{
+    if (!ctx || !out) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    double s = 0;
+    ctx->launches += launch_reduce(ctx->ka, ctx->prec, what == MMS_REDUCE_CE_SUM ? MMS_REDUCE_CE_SUM : 0, &s, ctx->stream);
+    CU(cudaGetLastError());
+    const mms_params &p = ctx->p;
+    const Geo &g = ctx->ka.g;
+    if (what == MMS_REDUCE_CE_SUM) *out = s;
+    else if (what == MMS_REDUCE_SOLID_VOLUME) *out = s * pow(p.cellSize, 3.0);
+    else *out = (s * pow(p.cellSize, 3.0)) / ((g.gx * g.gy * g.gz) * pow(p.cellSize, 3));
+    return MMS_OK;
+}
+
+mms_status mms_get_grains(mms_ctx *ctx, int first, int count, mms_grain *out)
+{
+    if (!ctx || !out || first < 0 || count < 0) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status st = sync_grains(ctx);
+    if (st) return st;
+    for (int i = 0; i < count; i++) {
+        int gi = first + i;
+        if (gi < (int)ctx->grains.size()) out[i] = ctx->grains[gi];
+        else std::memset(&out[i], 0, sizeof(mms_grain));
+    }
+    return MMS_OK;
+}
+
+// output_grains (grain.c:751-833)
+mms_status mms_output_grains(mms_ctx *ctx, const char *path, mms_grain_summary *out)
+{
+    if (!ctx) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status st = sync_grains(ctx);
+    if (st) return st;
+    const Geo &g = ctx->ka.g;
+    const mms_params &p = ctx->p;
+    int ng = ctx->h_ctl->num_grains;
+    std::vector<int> gr((size_t)g.N);
+    CU(cudaMemcpy(gr.data(), ctx->ka.d.gr, sizeof(int) * g.N, cudaMemcpyDeviceToHost));
+    std::vector<size_t> sizes((size_t)ng + 1, 0);
+    for (long long k = 1; k <= g.gz; k++)
+        for (long long j = 1; j <= g.gy; j++)
+            for (long long i = 1; i <= g.gx; i++) {
+                int v = gr[cidx(g, i, j, k)];
+                if (v > 0 && v <= ng) sizes[v]++;
+            }
+    size_t minSize = sizes[1], maxSize = sizes[1], avgSize = 0, zeroCount = 0;
+    double cellVolume = pow(p.cellSize * 1000, 3.0);
+    FILE *fp = nullptr;
+    if (path) {
+        fp = std::fopen(path, "w");
+        if (!fp) {
+            ctx->err = std::string("Unable to open grain file ") + path;
+            return MMS_ERR_IO;
+        }
+        std::fprintf(fp, "Number,Nuc Timestep,Nuc Time,Nuc Threshold,X,Y,Z,CellX,CellY,CellZ,Rot1,Rot2,Rot3,"
+                         "Rotation Matrix,Size mm^3\n");
+    }
+    for (int i = 1; i < ng; i++) {
+        const mms_grain &gg = ctx->grains[i];
+        if (fp) {
+            size_t cx, cy, cz;
+            real2cell(p, gg.nuc_x, gg.nuc_y, gg.nuc_z, &cx, &cy, &cz);
+            std::fprintf(fp,
+                         "%d,%lu,%lg,%lg,%lg,%lg,%lg,%lu,%lu,%lu,%lg,%lg,%lg,[[%lg %lg %lg][%lg %lg %lg][%lg %lg %lg]],%lg\n",
+                         i, (unsigned long)gg.nuc_timestep, gg.nuc_timestep * p.ts_delt, gg.nuc_threshold, gg.nuc_x,
+                         gg.nuc_y, gg.nuc_z, cx, cy, cz, gg.rotang[0], gg.rotang[1], gg.rotang[2], gg.rotmat[0][0],
+                         gg.rotmat[0][1], gg.rotmat[0][2], gg.rotmat[1][0], gg.rotmat[1][1], gg.rotmat[1][2],
+                         gg.rotmat[2][0], gg.rotmat[2][1], gg.rotmat[2][2], sizes[i] * cellVolume);
+        }
+        if (sizes[i] < minSize) minSize = sizes[i];
+        if (sizes[i] > maxSize) maxSize = sizes[i];
+        avgSize += sizes[i];
+        if (sizes[i] == 0) zeroCount++;
+    }
+    if (fp) std::fclose(fp);
+    if (out) {
+        out->num_grains = ng - 1;
+        out->min_mm3 = minSize * cellVolume;
+        out->max_mm3 = maxSize * cellVolume;
+        out->avg_mm3 = ((double)avgSize / ((double)((ng - 1) - zeroCount)) * cellVolume);
+    }
+    return MMS_OK;
+}
+
+// loop (loop.c:185-271): screen lines every ScreenPFreq, termination by
+// FinishTime or FsFinish, grain summary at the end.  verbose: 0 quiet,
+// 1 screen output, 2 screen output in interactive mode (-i).
+mms_status mms_run(mms_ctx *ctx, int verbose)
+{
+    if (!ctx) return MMS_ERR_ARG;
+    const mms_params &p = ctx->p;
+    const char *leader = (verbose == 2) ? "        \r" : "";
+    const char *tailer = (verbose == 2) ? "" : "\n";
+    struct timeval tv;
+    gettimeofday(&tv, nullptr);
+    double t0 = tv.tv_sec + ((double)tv.tv_usec * 1.0e-6);
+    auto screen = [&](double fs) {
+        gettimeofday(&tv, nullptr);
+        double t = tv.tv_sec + ((double)tv.tv_usec * 1.0e-6);
+        int ng = 0;
+        mms_get_num_grains(ctx, &ng);
+        uint64_t ts = 0;
+        mms_get_timestep(ctx, &ts);
+        std::printf("%s%10g  %10g  %8.4lf%% %8d  %s \n", leader, t - t0, ts * p.ts_delt, 100.0 * fs, ng - 1, tailer);
+        std::fflush(stdout);
+    };
+    if (verbose && p.screenpfreq > 0) {
+        std::printf("\n%10s  %10s   %8s  %8s\n", "Wall Time", "Sim Time", "Fraction", "Grain NO");
+        std::printf("%10s  %10s   %8s\n", "(sec)  ", "(sec)  ", "Solid");
+        screen(0.0);
+    }
+    double fs = 0.0;
+    mms_status st;
+    uint64_t ts = 0;
+    if ((st = mms_get_timestep(ctx, &ts))) return st;
+    for (;;) {
+        // run to the next screen step, or to FinishTime if that comes first
+        uint64_t n = (p.screenpfreq > 0) ? (uint64_t)p.screenpfreq - (ts % (uint64_t)p.screenpfreq) : (1ULL << 30);
+        if (p.finish_time) {
+            // first t with t*ts_delt >= finish_time (checkDone, loop.c:155-156)
+            uint64_t t = (uint64_t)std::floor(p.finish_time / p.ts_delt);
+            while (t > 0 && ((t - 1) * p.ts_delt) >= p.finish_time) t--;
+            while ((t * p.ts_delt) < p.finish_time) t++;
+            if (t <= ts) t = ts + 1;
+            n = std::min<uint64_t>(n, t - ts);
+        }
+        if (n > (1ULL << 30)) n = 1ULL << 30;
+        if ((st = mms_step(ctx, (int)n))) return st;
+        ts += n;
+        if (p.screenpfreq > 0 && ts % (uint64_t)p.screenpfreq == 0) {
+            if ((st = mms_reduce(ctx, MMS_REDUCE_FS_FRACTION, &fs))) return st;
+            if (verbose) screen(fs);
+        }
+        bool done = false;
+        if (p.finish_time && ((ts * p.ts_delt) >= p.finish_time)) {
+            done = true;
+            if (verbose) std::printf("\nAuto-Finish time met.\n");
+        }
+        if (fs >= p.fs_finish) {
+            if (verbose) std::printf("\nSolid Fraction termination condition met.\n");
+            done = true;
+        }
+        if (done) break;
+    }
+    mms_grain_summary s;
+    char path[512];
+    std::snprintf(path, sizeof path, "%s_grains.csv", p.basefilename);
+    if ((st = mms_output_grains(ctx, verbose ? path : nullptr, &s))) return st;
+    if (verbose) {
+        std::printf("%d grains.  Min: %lg mm^3   Max: %lg mm^3   Average:  %lg mm^3\n", s.num_grains, s.min_mm3,
+                    s.max_mm3, s.avg_mm3);
+        std::printf("\nSimulation complete.  Shutting down.\n");
+        std::fflush(stdout);
+    }
+    return MMS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+// mms_internal.h — device-state layout shared by the host side (mms_api.cu)
+// and the sm_100a kernels (kernels.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mms.h"
+
+extern "C" size_t mms_params_size(void);
+
+namespace mms {
+
+// Octahedron centre offset (decentered_t, globals.h:141-144).
+struct Dc3 {
+    double x, y, z;
+};
+
+// Device control block: everything a step needs that changes between steps
+// lives here, so that a whole step (or a CUDA graph of many steps) runs with
+// no host involvement.
+struct Ctl {
+    unsigned long long timestep;  // bp->timestep after the last committed step
+    int num_grains;               // bp->num_grains (includes grain 0)
+    int ncand;                    // nucleation candidates found this step
+    int status;                   // first error (mms_status), 0 = ok
+    int stall;                    // non-zero: later kernels of the step do nothing
+    unsigned long long stall_step;
+    int list_total;               // interface-list length over all ranks this step
+    int zero_needed;              // dc_tmp regions to clear this step (bit per rank < 32, else flag)
+    int new_grains;               // grains created by the last activation
+    int pad0;
+};
+
+enum StallReason : int {
+    STALL_NONE = 0,
+    STALL_ERROR = 1,      // ctl->status holds the error
+    STALL_RNG = 2         // a rank ran out of pre-drawn orientations
+};
+
+// One record per created grain (index = grain id), enough for the host to
+// rebuild grain_t (globals.h:244-254) for output_grains and mms_get_grains.
+struct GrainLog {
+    long long cell;       // global halo'd linear index of the nucleus cell
+    unsigned long long timestep;
+    int kind;             // 0 = deck site (nuc_pt entry), 1 = random draw, 2 = zero angles
+    int rank;             // emulated rank that created it
+    long long aux;        // nuc_pt entry index, or per-rank draw number
+};
+
+// Geometry and physics constants passed to every kernel by value.
+struct Geo {
+    int gx, gy, gz;            // interior cells
+    long long sy, sz, N;       // halo'd strides and size
+    int sbx, sby, sbz;         // NCellsPerSB
+    int nsbx, nsby, nsbz;      // NSubblocks
+    int nranks;
+    long long sbcells;         // cells per subblock
+    int padx, pady, padz;      // pad (mold) faces
+    int vb;                    // cells per list block (scan granularity)
+    long long blocks_per_rank; // ceil(sbcells / vb)
+};
+
+struct Phys {
+    // diffusion (growth.c:38-40)
+    double rs, rl;
+    // fs change (growth.c:181-197)
+    double liq_slope, k_inv, km, km_inv, m_inv, D_xt, cinit, Tliq, Tsol;
+    int tip_curv;
+    double gibbs;
+    // growth (growth.c:348)
+    double fsgrow;
+    unsigned long long max_grains;
+    // nucleation (grain.c:1054-1059)
+    double ma, mb, mc;
+    // temperature (temperature.c:24-126)
+    int temp_mode;   // 0 isothermal, 1 linear, 2 AM quadrature (array)
+    double T0, cool_rate, gradient, grad_coef, velocity, velo_coef, ts_delt, cellSize;
+    double origin[3];
+    int gz_is_one;
+    int am, amlayer;
+    int use_orientation;
+    double cellSize3;
+};
+
+// Everything device-resident for one context.
+template <typename Real>
+struct Fields {
+    Real *ce;
+    Real *cl[2];
+    Real *fs[2];
+};
+
+struct DevPtrs {
+    void *ce;
+    void *cl[2];
+    void *fs[2];
+    int *gr;
+    Dc3 *dc;
+    double *T;            // AM temperature at the current step (N) or null
+    int *lsindex;         // AM layer flag or null
+    double *curv;         // curvature (N) when TipCurvature
+    // nucleation sites, sorted by (emulated rank, local raster)
+    long long nsites;
+    long long *site_cell;
+    float *site_thr;
+    int *site_rank;
+    unsigned char *site_flag;
+    int *cand;            // ordered candidate sites of the current step
+    // orientation sources
+    long long n_nucpt;
+    long long *nucpt_key;   // sorted global cell keys (first entry wins)
+    long long *nucpt_entry; // index into the rank's nuc_pt list (host side)
+    double *nucpt_rot;      // 9 per entry
+    long long n_inj;
+    long long *inj_key;
+    double *inj_rot;
+    double *rng_rot;        // nranks x rng_cap x 9
+    int rng_cap;
+    int *rng_used;          // per rank, draws consumed since rng_base
+    long long *rng_base;    // per rank, absolute draw number of table entry 0
+    int *act_scratch;       // 4 x nranks ints for k_act
+    double zero_rot[9];     // rotation for zero angles (GNOriented 0)
+    // grain table
+    double *grain_rot;      // (max_grains + 1) x 9
+    GrainLog *grain_log;    // (max_grains + 2)
+    // interface list and capture
+    int *blk_cnt;           // per list block
+    int *blk_off;
+    int *rank_gindex;       // per rank, list length
+    int *rank_dcsize;       // per rank, dc_tmp logical size
+    int *rank_zero_upto;    // per rank, slots to clear this step (0 = none)
+    long long *rank_dcbase; // per rank, offset of its dc_tmp region
+    long long *list_cell;   // list position -> cell
+    int *list_gid;          // list position -> captured grain id (0 = not captured)
+    Dc3 *dc_tmp;            // per-rank regions, 1-based slots
+    // reductions
+    double *red;            // scratch for partial sums
+    Ctl *ctl;
+};
+
+struct KernelArgs {
+    Geo g;
+    Phys p;
+    DevPtrs d;
+};
+
+// Launchers implemented in kernels.cu.  Each returns the number of kernels
+// it launched.
+// start_stage 0: whole step; 1: resume at grain activation (after a stall).
+int launch_step(const KernelArgs &a, int precision, void *stream, int start_stage);
+int launch_temp_am(const KernelArgs &a, void *stream, double lsd, double lv, double lhs, double lab,
+                   double lpow, double liniT, double lthcon, double rho_cp, double x0, double y0,
+                   double z0, int amtracks, int nsbx_times_sbx);
+int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream);
+int launch_fill_temperature(const KernelArgs &a, double *dev_out, void *stream);
+int launch_compute_d(const KernelArgs &a, int precision, double *dev_out, void *stream);
+int launch_convert(const KernelArgs &a, int precision, int field, int to_device, double *dev_f64,
+                   void *stream);
+
+}  // namespace mms
