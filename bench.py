@@ -1,0 +1,421 @@
+#!/usr/bin/env python3
+"""Throughput of the muMatScale CA step on B200: cell-updates/s.
+
+Workload: the multi-grain directional-solidification deck (256^3 cells,
+dx = 2 um, Al-Cu C0 = 4.5 wt%, m = -2.6 K/wt%, k = 0.14, D_l = 3e-9,
+D_s = 3e-13 m^2/s, G = 1e4 K/m along z, V = 1e-3 m/s, dt with
+D_l dt/dx^2 = 0.15, surface sites 1e10 m^-2 and bulk sites 1e13 m^-3 with
+undercooling N(2 K, 0.5 K), random orientations), restated as a
+reference-format deck so that the reference runs the same physics.  A
+"step" is one timestep (doiteration) of the whole domain; the metric counts
+interior cells x steps / second.
+
+GPU arm (default): the FP64 plain form is ``value`` (bit-identical to the
+reference); the FP32 form is reported beside it.  Timing: W untimed steps,
+then K steps bracketed by CUDA events on the stream the library launches
+on, synchronised on both sides; under torchrun every rank runs its own
+replica (the z-slab sharded version is not built: replicas only) and the
+maximum over ranks is taken.  Inputs (about 1.1 GB of fields) are larger
+than the 126 MB L2, so no flush is needed.
+
+Reference arm (--impl reference): the unmodified reference compiled from
+its sources (oracle/_ref/mmsref), run as MPI ranks over the host cores
+through the project's shared-memory MPI shim on the same deck decomposed
+into NSubblocks, timing K steps after W steps from per-step timestamps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s, FP32 form vs FP64 plain (1 B200); stencil HBM GB/s vs peak"
+UNIT = "cell-updates/s"
+N_CELL = 256
+# Al-Cu alloy: liquidus = 933.47 - 2.6*4.5 (pure-Al melting point assumed);
+# solidus = 933.47 - 2.6*4.5/0.14
+T_LIQ = 933.47 - 2.6 * 4.5
+T_SOL = 933.47 - 2.6 * 4.5 / 0.14
+DX = 2e-6
+DT = 0.15 * DX * DX / 3e-9
+# algorithmic bytes per cell of the dominant kernel k_diffuse_fs:
+# read ce, cl, fs + write ce, cl, fs + read gr
+BYTES_DIFFUSE = {"f64": 3 * 8 * 2 + 4, "f32": 3 * 4 * 2 + 4}
+# full-step dense bytes per cell-update (ce, cl, fs read+write, gr, threshold)
+BYTES_STEP = {"f64": 56, "f32": 32}
+
+
+def deck_text(nsb=(1, 1, 1), n=N_CELL, seed=20261203) -> str:
+    sb = [n // nsb[0], n // nsb[1], n // nsb[2]]
+    return f"""BaseFileName bench256
+NSubblocks {nsb[0]} {nsb[1]} {nsb[2]}
+NCellsPerSB {sb[0]} {sb[1]} {sb[2]}
+FaceCtrl 1 1 1 1 1 1
+CellSize {DX!r}
+FSGrow 0.66
+TimeStep {DT!r}
+RandSeedVal {seed}
+TipCurvature 0
+GibbsThomsonCoef 2.4e-7
+FinishTime 0
+FsFinish 1.1
+LiquidusTemp {T_LIQ!r}
+SolidusTemp {T_SOL!r}
+Cinit 4.5
+m_solute0 0 0 -2.6
+part_coef0 0 0 0.14
+Dsol 3e-13
+Dliq 3e-9
+InitialTemperature {T_LIQ - 2.5!r}
+Gradient 1e4
+Velocity 1e-3
+CoolingRate 0
+ScreenPFreq 0
+MaxGrainDensity 1e13
+GNGaussCentre 2.0
+GNGaussSigma 0.5
+MaxGrainDensitySurf 1e10
+GNGaussCentreSurf 2.0
+GNGaussSigmaSurf 0.5
+MaxTotGrains 1000000
+GNOriented 1
+"""
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- helpers
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peak_gbs() -> tuple[float, str]:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_cell(dtype: str):
+    f = ROOT / "profiles" / "k_diffuse_fs_traffic.json"
+    if f.exists():
+        try:
+            d = json.loads(f.read_text())
+            return d[dtype]["dram_bytes_per_cell"]
+        except Exception:
+            return None
+    return None
+
+
+def ref_procs(cores: int) -> tuple[int, tuple[int, int, int]]:
+    """Largest power of two <= min(cores, 64), split over z, y, x."""
+    n = 1
+    while n * 2 <= min(cores, 64):
+        n *= 2
+    nsb = [1, 1, 1]
+    k, ax = n, 2
+    while k > 1:
+        nsb[ax] *= 2
+        k //= 2
+        ax = (ax - 1) % 3
+    return n, (nsb[0], nsb[1], nsb[2])
+
+
+def run_reference(nsteps_w: int, nsteps_k: int, cores: int | None = None, timeout: float = 1800):
+    """Times the unmodified reference (oracle/_ref/mmsref) on the bench deck."""
+    ref = ROOT / "oracle" / "_ref" / "mmsref"
+    if not ref.exists():
+        return None, "oracle/_ref/mmsref not built"
+    cores = cores or (os.cpu_count() or 1)
+    nproc, nsb = ref_procs(cores)
+    with tempfile.TemporaryDirectory() as td:
+        deck = Path(td) / "bench.in"
+        text = deck_text(nsb).replace("FinishTime 0", f"FinishTime {(nsteps_w + nsteps_k - 0.5) * DT!r}")
+        deck.write_text(text)
+        times = Path(td) / "times.txt"
+        env = dict(os.environ, MMSREF_NP=str(nproc), MMSREF_STEP_TIMES=str(times), OMP_NUM_THREADS="1")
+        t0 = time.time()
+        r = subprocess.run([str(ref), "-c", str(deck)], cwd=td, env=env, capture_output=True, text=True,
+                           timeout=timeout)
+        wall = time.time() - t0
+        if r.returncode != 0:
+            return None, f"reference exited {r.returncode}: {r.stderr[-300:]}"
+        ts = {}
+        for line in times.read_text().split("\n"):
+            if line.strip():
+                a, b = line.split()
+                ts[int(a)] = float(b)
+        t_start = ts.get(nsteps_w)
+        t_end = ts.get(nsteps_w + nsteps_k)
+        if t_start is None or t_end is None:
+            return None, "reference step timestamps missing"
+        cells = N_CELL ** 3
+        sec = t_end - t_start
+        return {"value": cells * nsteps_k / sec, "sec": sec, "procs": nproc, "nsubblocks": nsb,
+                "wall": wall, "steps": nsteps_k}, None
+
+
+# ---------------------------------------------------------------- GPU arm
+def gpu_arm(args) -> None:
+    import numpy as np
+    import torch
+    import mumatscale_b200 as M
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    K, W = args.steps, args.warmup
+    cells = N_CELL ** 3
+    td = tempfile.mkdtemp()
+    deck = Path(td) / "bench.in"
+    deck.write_text(deck_text())
+    params = M.read_deck(deck)
+    out: dict = {}
+    launches_total = 0
+    for form, prec in (("f64", M.PREC_F64), ("f32", M.PREC_F32)):
+        dom = M.Domain(params, precision=prec, device=dev)
+        dom.set_stream(stream.cuda_stream)
+        dom.step(W)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = dom.kernel_launches
+        with ClockSampler(dev) as clk:
+            e0.record(stream)
+            dom.step(K)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        launches = dom.kernel_launches - l0
+        launches_total += launches
+        # per-kernel device time over a second timed pass of K steps
+        dom.set_profiling(True)
+        dom.step(K)
+        torch.cuda.synchronize()
+        ks = dom.kernel_stats()
+        dom.set_profiling(False)
+        out[form] = {"ms_total": ms, "launches": launches, "kernels": ks, "clocks": clk.summary(),
+                     "grains": dom.num_grains, "timestep": dom.timestep}
+        if form == "f64":
+            # end to end through the public API with host buffers: upload the
+            # whole state from pinned host memory, K steps each followed by a
+            # device->host read of the fraction solid (loop.c's screen value),
+            # and a final download of grain ids and ce
+            n = dom.num_cells()
+            host = {f: torch.empty(n * (3 if f == "dc" else 1),
+                                   dtype=torch.int32 if f == "gr" else torch.float64).pin_memory()
+                    for f in ("ce", "cl", "fs", "gr", "dc")}
+            for f, t in host.items():
+                arr = dom.download(f).reshape(-1)
+                t.numpy()[:] = arr
+            torch.cuda.synchronize()
+            barrier()
+            t0 = time.perf_counter()
+            h2d = 0
+            for f, t in host.items():
+                dom.upload(f, t.numpy())
+                h2d += t.numel() * t.element_size()
+            d2h = 0
+            for _ in range(K):
+                dom.step(1)
+                dom.reduce("fs_fraction")
+                d2h += 8
+            gr = dom.download("gr")
+            ce = dom.download("ce")
+            d2h += gr.nbytes + ce.nbytes
+            torch.cuda.synchronize()
+            e2e_s = max_over_ranks(time.perf_counter() - t0)
+            out["e2e"] = {"value": ws * cells * K / e2e_s, "unit": UNIT,
+                          "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K}
+        dom.close()
+        del dom
+
+    if rank != 0:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    f64, f32 = out["f64"], out["f32"]
+    value = ws * cells * K / (f64["ms_total"] / 1e3)
+    value32 = ws * cells * K / (f32["ms_total"] / 1e3)
+    peak, peak_kind = measured_peak_gbs()
+    kms, kn = f64["kernels"]["k_diffuse_fs"]
+    per_launch_s = kms / 1e3 / max(kn, 1)
+    achieved = BYTES_DIFFUSE["f64"] * cells / per_launch_s / 1e9
+    kms32, kn32 = f32["kernels"]["k_diffuse_fs"]
+    achieved32 = BYTES_DIFFUSE["f32"] * cells / (kms32 / 1e3 / max(kn32, 1)) / 1e9
+    tr = ncu_traffic_per_cell("f64")
+    step_ms = f64["ms_total"] / K
+    share = {k: round(v[0] / max(1e-9, sum(x[0] for x in f64["kernels"].values())), 4)
+             for k, v in f64["kernels"].items() if v[1]}
+    cpu = None
+    if not args.no_cpu_baseline:
+        res, why = run_reference(2, args.cpu_steps)
+        if res:
+            cpu = {"value": res["value"], "unit": UNIT, "cores": res["procs"], "kind": "reference",
+                   "sample": f"{res['steps']} timesteps of the same 256^3 deck after 2 warm-up steps, "
+                             f"{res['procs']} MPI ranks (NSubblocks {res['nsubblocks']}) of the reference "
+                             f"through the shared-memory MPI shim, {res['sec']:.2f} s"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "multi-grain directional solidification, 256^3 cells, FP64 plain form",
+                   "cells": cells, "dx_m": DX, "dt_s": DT, "G_K_per_m": 1e4, "V_m_per_s": 1e-3,
+                   "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (about 1.1 GB of fields)",
+                   "grains_after_run": f64["grains"]},
+        "fp32_form": {"value": value32, "ms_per_step": f32["ms_total"] / K, "ratio_vs_fp64": value32 / value,
+                      "k_diffuse_fs_gbs": achieved32},
+        "roofline": {"bound": "hbm", "kernel": "k_diffuse_fs", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_cell": BYTES_DIFFUSE["f64"],
+                     "traffic": (tr * cells) if tr else None,
+                     "kernel_ms_per_launch": per_launch_s * 1e3},
+        "kernel_share": share,
+        "e2e": out["e2e"],
+        "gpu_launches": f64["launches"],
+        "clocks": f64["clocks"],
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def reference_arm(args) -> None:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    res, why = run_reference(args.warmup, args.steps)
+    if not res:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    line = {
+        "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["sec"] * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "multi-grain directional solidification, 256^3 cells, FP64 plain form",
+                   "cells": N_CELL ** 3, "parallelism": f"{res['procs']} MPI ranks on host cores"},
+        "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": res["procs"], "kind": "reference",
+                         "sample": f"{args.steps} timesteps after {args.warmup}, NSubblocks {res['nsubblocks']}"},
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -161,6 +161,8 @@ mms_status mms_params_default(mms_params *p);
  * appended to heap arrays released by mms_params_free_lists(). */
 mms_status mms_deck_read(const char *path, mms_params *p);
 void mms_params_free_lists(mms_params *p);
+/* sizeof(mms_params), for FFI bindings to check their layout */
+size_t mms_params_size(void);
 
 /* ---- context lifetime ------------------------------------------------------ */
 
@@ -224,6 +226,20 @@ mms_status mms_output_grains(mms_ctx *ctx, const char *path, mms_grain_summary *
  * printing the reference's screen lines and grain summary to stdout when
  * verbose is non-zero. */
 mms_status mms_run(mms_ctx *ctx, int verbose);
+
+/* ---- streams and timing ----------------------------------------------------- */
+
+/* Runs all of this context's work on the caller's CUDA stream (a
+ * cudaStream_t passed as a plain pointer; NULL restores the context's own
+ * stream).  The stream must outlive its use by the context. */
+mms_status mms_set_stream(mms_ctx *ctx, void *cuda_stream);
+/* When on, every kernel launch is bracketed by CUDA events on the launching
+ * stream, and per-kernel device time accumulates for mms_kernel_stats. */
+mms_status mms_set_profiling(mms_ctx *ctx, int on);
+/* Kernel ids 0..mms_kernel_count()-1; name and accumulated statistics. */
+int mms_kernel_count(void);
+const char *mms_kernel_name(int id);
+mms_status mms_kernel_stats(mms_ctx *ctx, int id, double *total_ms, uint64_t *launches);
 
 /* ---- diagnostics ----------------------------------------------------------- */
 const char *mms_status_string(mms_status s);

@@ -160,6 +160,11 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_status_string": (C.c_char_p, [I]),
         "mms_last_error": (C.c_char_p, [P]),
         "mms_kernel_launches": (C.c_uint64, [P]),
+        "mms_set_stream": (I, [P, P]),
+        "mms_set_profiling": (I, [P, I]),
+        "mms_kernel_count": (I, []),
+        "mms_kernel_name": (C.c_char_p, [I]),
+        "mms_kernel_stats": (I, [P, I, C.POINTER(D), C.POINTER(C.c_uint64)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -259,6 +264,22 @@ class Domain:
     @property
     def kernel_launches(self) -> int:
         return int(_lib().mms_kernel_launches(self._ctx))
+
+    # -- streams and timing
+    def set_stream(self, cuda_stream: int | None) -> None:
+        _check(_lib().mms_set_stream(self._ctx, C.c_void_p(cuda_stream or 0)), "mms_set_stream", self._ctx)
+
+    def set_profiling(self, on: bool) -> None:
+        _check(_lib().mms_set_profiling(self._ctx, int(on)), "mms_set_profiling", self._ctx)
+
+    def kernel_stats(self) -> dict[str, tuple[float, int]]:
+        lib = _lib()
+        out = {}
+        for k in range(lib.mms_kernel_count()):
+            ms, n = C.c_double(), C.c_uint64()
+            _check(lib.mms_kernel_stats(self._ctx, k, C.byref(ms), C.byref(n)), "mms_kernel_stats", self._ctx)
+            out[lib.mms_kernel_name(k).decode()] = (ms.value, int(n.value))
+        return out
 
     # -- fields (halo'd, indexed [z, y, x] like growth.c:70)
     def num_cells(self) -> int:

@@ -908,54 +908,79 @@ static int pick_zchunk(const Geo &g)
     return zc;
 }
 
+#define PROF_BEGIN(id) \
+    if (prof) prof->begin(id, st)
+#define PROF_END(id) \
+    if (prof) prof->end(id, st)
+
 template <typename Real>
-static int launch_step_t(const KernelArgs &a, cudaStream_t st, int start_stage)
+static int launch_step_t(const KernelArgs &a, cudaStream_t st, int start_stage, Profiler *prof)
 {
     int n = 0;
     const Geo &g = a.g;
     if (start_stage == 0 && a.d.nsites > 0) {
         int nb = (int)((a.d.nsites + 255) / 256);
+        PROF_BEGIN(KID_NUC);
         k_nuc<Real><<<nb, 256, 0, st>>>(a);
+        PROF_END(KID_NUC);
         n++;
     }
+    PROF_BEGIN(KID_ACT);
     k_act<<<1, ACT_NT, 0, st>>>(a, a.d.act_scratch);
+    PROF_END(KID_ACT);
     n++;
     if (a.p.tip_curv) {
         long long tot = (long long)g.nranks * g.sbcells;
+        PROF_BEGIN(KID_CURV);
         k_curv<Real><<<(int)((tot + 255) / 256), 256, 0, st>>>(a);
+        PROF_END(KID_CURV);
         n++;
     }
     {
         int zc = pick_zchunk(g);
         dim3 grid((g.gx + DTX - 1) / DTX, (g.gy + DTY - 1) / DTY, (g.gz + zc - 1) / zc);
+        PROF_BEGIN(KID_DIFFUSE_FS);
         k_diffuse_fs<Real><<<grid, dim3(DTX, DTY), 0, st>>>(a, zc);
+        PROF_END(KID_DIFFUSE_FS);
         n++;
     }
     int nblocks = (int)(g.blocks_per_rank * g.nranks);
+    PROF_BEGIN(KID_LIST_COUNT);
     k_list_count<<<nblocks, LIST_NT, 0, st>>>(a);
+    PROF_END(KID_LIST_COUNT);
+    PROF_BEGIN(KID_LIST_SCAN);
     k_list_scan<<<1, SCAN_NT, 0, st>>>(a, nblocks);
+    PROF_END(KID_LIST_SCAN);
+    PROF_BEGIN(KID_LIST_ZERO);
     k_list_zero<<<dim3(64, g.nranks), 256, 0, st>>>(a);
+    PROF_END(KID_LIST_ZERO);
+    PROF_BEGIN(KID_CAPTURE);
     k_capture<Real><<<nblocks, LIST_NT, 0, st>>>(a);
+    PROF_END(KID_CAPTURE);
+    PROF_BEGIN(KID_APPLY);
     k_apply<<<148 * 4, 256, 0, st>>>(a);
+    PROF_END(KID_APPLY);
     n += 5;
     return n;
 }
 
-int launch_step(const KernelArgs &a, int precision, void *stream, int start_stage)
+int launch_step(const KernelArgs &a, int precision, void *stream, int start_stage, Profiler *prof)
 {
     cudaStream_t st = (cudaStream_t)stream;
-    if (precision == MMS_PREC_F32) return launch_step_t<float>(a, st, start_stage);
-    return launch_step_t<double>(a, st, start_stage);
+    if (precision == MMS_PREC_F32) return launch_step_t<float>(a, st, start_stage, prof);
+    return launch_step_t<double>(a, st, start_stage, prof);
 }
 
-int launch_temp_am(const KernelArgs &a, void *stream, double lsd, double lv, double lhs, double lab,
-                   double lpow, double liniT, double lthcon, double rho_cp, double x0, double y0,
+int launch_temp_am(const KernelArgs &a, void *stream, Profiler *prof, double lsd, double lv, double lhs,
+                   double lab, double lpow, double liniT, double lthcon, double rho_cp, double x0, double y0,
                    double z0, int amtracks, int nsbx_times_sbx)
 {
     cudaStream_t st = (cudaStream_t)stream;
     int nb = (int)((a.g.N + 255) / 256);
+    PROF_BEGIN(KID_TEMP_AM);
     k_temp_am<<<nb, 256, 0, st>>>(a, lsd, lv, lhs, lab, lpow, liniT, lthcon, rho_cp, x0, y0, z0,
                                   amtracks, nsbx_times_sbx);
+    PROF_END(KID_TEMP_AM);
     return 1;
 }
 

@@ -105,8 +105,67 @@ void rotmat_from_angles(double a0, double a1, double a2, double *R)
 
 }  // namespace
 
+// Event bracketing of kernel launches for mms_kernel_stats.
+struct EventProfiler : mms::Profiler {
+    struct Rec {
+        int kid;
+        cudaEvent_t a, b;
+    };
+    std::vector<cudaEvent_t> pool;
+    std::vector<Rec> pending;
+    double total_ms[mms::KID_COUNT] = {};
+    uint64_t count[mms::KID_COUNT] = {};
+    cudaEvent_t cur = nullptr;
+    cudaEvent_t get()
+    {
+        if (pool.empty()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            return e;
+        }
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    void begin(int kid, void *stream) override
+    {
+        (void)kid;
+        cur = get();
+        cudaEventRecord(cur, (cudaStream_t)stream);
+    }
+    void end(int kid, void *stream) override
+    {
+        cudaEvent_t e = get();
+        cudaEventRecord(e, (cudaStream_t)stream);
+        pending.push_back({kid, cur, e});
+    }
+    // stream must be idle
+    void collect()
+    {
+        for (const Rec &r : pending) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            total_ms[r.kid] += ms;
+            count[r.kid]++;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        pending.clear();
+    }
+    ~EventProfiler()
+    {
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+        for (const Rec &r : pending) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+    }
+};
+
 struct mms_ctx {
     mms_params p{};
+    cudaStream_t own_stream = nullptr;
+    EventProfiler *prof = nullptr;
     std::vector<mms_fixed_nuc> fixed;
     std::vector<mms_nuc_volume> vols;
     int prec = MMS_PREC_F64;
@@ -481,6 +540,7 @@ mms_status read_ctl(mms_ctx *ctx)
 {
     CU(cudaMemcpyAsync(ctx->h_ctl, ctx->ka.d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
+    if (ctx->prof) ctx->prof->collect();
     return MMS_OK;
 }
 
@@ -489,10 +549,10 @@ int launch_one_step(mms_ctx *ctx, int start_stage)
     int n = 0;
     const mms_params &p = ctx->p;
     if (start_stage == 0 && p.am) {
-        n += launch_temp_am(ctx->ka, ctx->stream, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
+        n += launch_temp_am(ctx->ka, ctx->stream, ctx->prof, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
                             p.rho * p.lcp, p.x0, p.y0, p.z0, p.amtracks, p.gnsbx * p.gsdimx);
     }
-    n += launch_step(ctx->ka, ctx->prec, ctx->stream, start_stage);
+    n += launch_step(ctx->ka, ctx->prec, ctx->stream, start_stage, ctx->prof);
     return n;
 }
 
@@ -579,6 +639,55 @@ const char *mms_status_string(mms_status s)
 }
 
 const char *mms_last_error(const mms_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+mms_status mms_set_stream(mms_ctx *ctx, void *cuda_stream)
+{
+    if (!ctx) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->stream = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own_stream;
+    return MMS_OK;
+}
+
+mms_status mms_set_profiling(mms_ctx *ctx, int on)
+{
+    if (!ctx) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (on && !ctx->prof) ctx->prof = new EventProfiler();
+    if (!on && ctx->prof) {
+        ctx->prof->collect();
+        delete ctx->prof;
+        ctx->prof = nullptr;
+    }
+    return MMS_OK;
+}
+
+int mms_kernel_count(void) { return mms::KID_COUNT; }
+
+const char *mms_kernel_name(int id)
+{
+    static const char *names[mms::KID_COUNT] = {"k_temp_am", "k_nuc", "k_act", "k_curv", "k_diffuse_fs",
+                                                "k_list_count", "k_list_scan", "k_list_zero", "k_capture",
+                                                "k_apply"};
+    return (id >= 0 && id < mms::KID_COUNT) ? names[id] : "";
+}
+
+mms_status mms_kernel_stats(mms_ctx *ctx, int id, double *total_ms, uint64_t *launches)
+{
+    if (!ctx || id < 0 || id >= mms::KID_COUNT || !total_ms || !launches) return MMS_ERR_ARG;
+    if (!ctx->prof) {
+        *total_ms = 0;
+        *launches = 0;
+        return MMS_OK;
+    }
+    cudaSetDevice(ctx->device);
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->prof->collect();
+    *total_ms = ctx->prof->total_ms[id];
+    *launches = ctx->prof->count[id];
+    return MMS_OK;
+}
 uint64_t mms_kernel_launches(const mms_ctx *ctx) { return ctx ? ctx->launches : 0; }
 size_t mms_num_cells(const mms_ctx *ctx) { return ctx ? (size_t)ctx->ka.g.N : 0; }
 
@@ -619,7 +728,8 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         delete ctx;
         return MMS_ERR_NO_DEVICE;
     }
-    cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+    ctx->stream = ctx->own_stream;
     cudaMallocHost((void **)&ctx->h_ctl, sizeof(Ctl));
 
     Geo &g = ctx->ka.g;
@@ -759,7 +869,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
     }
     if (p.am && p.amlayer > 1) {
         // tempPrepareSB_int lsindex (temperature.c:183-189) at timestep 0
-        ctx->launches += launch_temp_am(ctx->ka, ctx->stream, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
+        ctx->launches += launch_temp_am(ctx->ka, ctx->stream, nullptr, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
                                         p.rho * p.lcp, p.x0, p.y0, p.z0, p.amtracks, p.gnsbx * p.gsdimx);
     }
     std::vector<float> thr(N, INFINITY);
@@ -798,7 +908,8 @@ mms_status mms_destroy(mms_ctx *ctx)
     for (void *p : ctx->allocs) cudaFree(p);
     ctx->allocs.clear();
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx->prof;
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return MMS_OK;
 }

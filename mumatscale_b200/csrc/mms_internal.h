@@ -147,11 +147,24 @@ struct KernelArgs {
     DevPtrs d;
 };
 
+// Kernel ids for per-kernel timing.
+enum KernelId : int {
+    KID_TEMP_AM = 0, KID_NUC, KID_ACT, KID_CURV, KID_DIFFUSE_FS, KID_LIST_COUNT, KID_LIST_SCAN,
+    KID_LIST_ZERO, KID_CAPTURE, KID_APPLY, KID_COUNT
+};
+
+// Optional event bracketing of each launch (mms_set_profiling).
+struct Profiler {
+    virtual void begin(int kid, void *stream) = 0;
+    virtual void end(int kid, void *stream) = 0;
+    virtual ~Profiler() {}
+};
+
 // Launchers implemented in kernels.cu.  Each returns the number of kernels
 // it launched.
 // start_stage 0: whole step; 1: resume at grain activation (after a stall).
-int launch_step(const KernelArgs &a, int precision, void *stream, int start_stage);
-int launch_temp_am(const KernelArgs &a, void *stream, double lsd, double lv, double lhs, double lab,
+int launch_step(const KernelArgs &a, int precision, void *stream, int start_stage, Profiler *prof);
+int launch_temp_am(const KernelArgs &a, void *stream, Profiler *prof, double lsd, double lv, double lhs, double lab,
                    double lpow, double liniT, double lthcon, double rho_cp, double x0, double y0,
                    double z0, int amtracks, int nsbx_times_sbx);
 int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream);

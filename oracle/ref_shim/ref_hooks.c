@@ -5,7 +5,10 @@
  *
  *  --wrap=doiteration          (calculate.c:193)  dump the subblock's fields
  *                               after chosen steps (MMSREF_DUMP_DIR,
- *                               MMSREF_DUMP_STEPS="a,b,c" or MMSREF_DUMP_EVERY=k)
+ *                               MMSREF_DUMP_STEPS="a,b,c" or MMSREF_DUMP_EVERY=k);
+ *                               with MMSREF_STEP_TIMES=<file>, rank 0 appends
+ *                               "<timestep> <seconds>" after every step (the
+ *                               halo exchanges keep the ranks in lockstep)
  *  --wrap=init_sb_nucleation   (grain.c:931)      optionally replace the
  *                               pre-drawn nucleation thresholds by a site file
  *                               (MMSREF_INJECT_SITES); dump the thresholds
@@ -96,9 +99,22 @@ static void write_dump(const char *tag)
     fclose(f);
 }
 
+double MPI_Wtime(void);
+
 void __wrap_doiteration(void)
 {
     __real_doiteration();
+    static FILE *tf = NULL;
+    static int tf_checked = 0;
+    if (!tf_checked) {
+        tf_checked = 1;
+        const char *path = getenv("MMSREF_STEP_TIMES");
+        if (path && iproc == 0) tf = fopen(path, "w");
+    }
+    if (tf) {
+        fprintf(tf, "%llu %.9f\n", (unsigned long long)bp->timestep, MPI_Wtime());
+        fflush(tf);
+    }
     if (step_wanted(bp->timestep)) {
         char tag[64];
         snprintf(tag, sizeof tag, "s%llu", (unsigned long long)bp->timestep);

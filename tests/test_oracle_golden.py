@@ -1,0 +1,42 @@
+"""Pins the CPU oracle to the reference: every field of the oracle's state must
+hash identically to the reference's own dumps (tests/golden/*.json, made by
+tests/golden/make_golden.py from the unmodified reference sources).  CPU only."""
+from __future__ import annotations
+
+import pytest
+
+import mumatscale_b200 as M
+from conftest import GOLDEN_DECKS, golden, golden_deck
+from digests import digest, mismatches, state_digests
+
+
+@pytest.mark.parametrize("name", GOLDEN_DECKS)
+def test_oracle_matches_reference_dumps(built, name):
+    from _oracle import Oracle
+    rec = golden(name)
+    p = M.read_deck(golden_deck(name))
+    o = Oracle(p, curvature=bool(rec["env"].get("MMSREF_CURV")))
+    assert digest(o.download("nuc_threshold")) == rec["setup"]["nuc_threshold"]
+    last = 0
+    for s, want in rec["steps"].items():
+        s = int(s)
+        o.step(s - last)
+        last = s
+        assert o.timestep == s
+        assert o.num_grains == want["num_grains"]
+        bad = mismatches(state_digests(o), want["digest"])
+        assert not bad, f"{name} step {s}: fields differ from the reference: {bad}"
+    if "error_at_step" in rec:
+        with pytest.raises(RuntimeError, match="status 6"):
+            o.step(rec["error_at_step"] - last)
+
+
+def test_oracle_rand_matches_libc(built):
+    """The per-rank streams replay glibc rand() (ca_main.c:215 srand)."""
+    import ctypes
+    from _oracle import rand_sequence
+    libc = ctypes.CDLL("libc.so.6")
+    for seed in (1, 7, 3823798713):
+        libc.srand(ctypes.c_uint(seed))
+        want = [libc.rand() for _ in range(500)]
+        assert rand_sequence(seed, 500).tolist() == want
