@@ -164,6 +164,12 @@ void mms_params_free_lists(mms_params *p);
 /* sizeof(mms_params), for FFI bindings to check their layout */
 size_t mms_params_size(void);
 
+/* The reference's nucleation thresholds after setup (init_nucleation_sites,
+ * grain.c:602-713, and init_sb_nucleation, grain.c:930-1010, every emulated
+ * rank on its own rand() stream), written to thr_out[N] in the halo'd layout
+ * (+inf where there is no site).  Host only: needs no CUDA device. */
+mms_status mms_predraw_sites(const mms_params *p, float *thr_out);
+
 /* ---- context lifetime ------------------------------------------------------ */
 
 /* Allocates the device-resident domain and applies the reference's initial

@@ -160,6 +160,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_status_string": (C.c_char_p, [I]),
         "mms_last_error": (C.c_char_p, [P]),
         "mms_kernel_launches": (C.c_uint64, [P]),
+        "mms_predraw_sites": (I, [C.POINTER(Params), P]),
         "mms_set_stream": (I, [P, P]),
         "mms_set_profiling": (I, [P, I]),
         "mms_kernel_count": (I, []),
@@ -201,6 +202,15 @@ def read_deck(path: str | os.PathLike, params: Params | None = None) -> Params:
     p = params if params is not None else default_params()
     _check(_lib().mms_deck_read(str(path).encode(), C.byref(p)), f"mms_deck_read({path})")
     return p
+
+
+def predraw_sites(params: Params) -> np.ndarray:
+    """The reference's threshold field after setup, computed on the host
+    (no device needed); shape (z, y, x) of the halo'd grid."""
+    nx, ny, nz = (x + 2 for x in params.grid)
+    out = np.empty(nx * ny * nz, dtype=np.float32)
+    _check(_lib().mms_predraw_sites(C.byref(params), out.ctypes.data), "mms_predraw_sites")
+    return out.reshape(nz, ny, nx)
 
 
 Params.default = staticmethod(default_params)

@@ -118,3 +118,14 @@ def test_courant_check(built):
     with pytest.raises(M.MmsError) as e:
         M.Domain(p)
     assert e.value.status in (3, 4)  # no device here, or MMS_ERR_COURANT
+
+
+@pytest.mark.parametrize("name", ["small1", "small4", "nucvol1", "grad1", "am1", "cap1"])
+def test_predraw_sites_matches_reference(built, name):
+    """The product's host-side replay of the reference's site draws
+    (mms_predraw_sites) reproduces the reference's threshold field."""
+    from conftest import golden
+    from digests import digest
+    rec = golden(name)
+    p = M.read_deck(golden_deck(name))
+    assert digest(M.predraw_sites(p)) == rec["setup"]["nuc_threshold"]
