@@ -123,10 +123,14 @@ typedef enum mms_field {
     MMS_FIELD_FS = 2,            /* f64 [N]   fraction solid */
     MMS_FIELD_GR = 3,            /* i32 [N]   grain id, 0 = liquid */
     MMS_FIELD_DC = 4,            /* f64 [3N]  octahedron centre offset, x,y,z per cell */
-    MMS_FIELD_D = 5,             /* f64 [N]   half diagonal (download only; grain cells) */
+    MMS_FIELD_D = 5,             /* f64 [N]   half diagonal grow_octahedra gave cells that were
+                                                solid at the last growth step, 0 elsewhere
+                                                (download only) */
     MMS_FIELD_NUC_THRESHOLD = 6, /* f32 [N]   nucleation undercooling, +inf = no site */
     MMS_FIELD_TEMPERATURE = 7,   /* f64 [N]   temperature at the current timestep (download only) */
-    MMS_FIELD_MOLD = 8           /* i8  [N]   mold flag (download only) */
+    MMS_FIELD_MOLD = 8,          /* i8  [N]   mold flag (download only) */
+    MMS_FIELD_OGR = 9            /* i32 [N]   grain ids before the last capture, the
+                                                reference's ogr (growth.c:635-638; download only) */
 } mms_field;
 
 typedef enum mms_reduction {

@@ -874,6 +874,27 @@ __global__ void k_fill_temperature(KernelArgs a, double *out)
     out[c] = temp_cell(a.p, a.d.T, c, J, K, ctl->timestep);
 }
 
+// Zero the entries of cells captured by the last step (list cells whose
+// capture produced a grain id): turns gr into the reference's ogr, and
+// limits d to cells that were solid at the growth step.
+template <typename T>
+__global__ void k_mask_captured(KernelArgs a, T *out)
+{
+    const Ctl *ctl = a.d.ctl;
+    const int total = ctl->list_total;
+    for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < total;
+         pos += (long long)gridDim.x * blockDim.x)
+        if (a.d.list_gid[pos]) out[a.d.list_cell[pos]] = (T)0;
+}
+
+int launch_mask_captured(const KernelArgs &a, void *dev, int is_double, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (is_double) k_mask_captured<double><<<148 * 4, 256, 0, st>>>(a, (double *)dev);
+    else k_mask_captured<int><<<148 * 4, 256, 0, st>>>(a, (int *)dev);
+    return 1;
+}
+
 // Conversion between the stored precision and FP64 host buffers.
 template <typename Real>
 __global__ void k_convert(KernelArgs a, int field, int to_device, double *buf)

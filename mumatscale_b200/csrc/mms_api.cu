@@ -824,6 +824,16 @@ mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
     case MMS_FIELD_GR:
         CU(cudaMemcpy(host, d.gr, N * sizeof(int), cudaMemcpyDeviceToHost));
         return MMS_OK;
+    case MMS_FIELD_OGR: {
+        int *tmp;
+        if ((st = dalloc(ctx, &tmp, N))) return st;
+        CU(cudaMemcpyAsync(tmp, d.gr, N * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+        ctx->launches += launch_mask_captured(ctx->ka, tmp, 0, ctx->stream);
+        CU(cudaMemcpyAsync(host, tmp, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, tmp);
+        return MMS_OK;
+    }
     case MMS_FIELD_DC:
         CU(cudaMemcpy(host, d.dc, N * sizeof(Dc3), cudaMemcpyDeviceToHost));
         return MMS_OK;
@@ -831,8 +841,12 @@ mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
     case MMS_FIELD_TEMPERATURE: {
         double *tmp;
         if ((st = dalloc(ctx, &tmp, N))) return st;
-        if (field == MMS_FIELD_D) ctx->launches += launch_compute_d(ctx->ka, ctx->prec, tmp, ctx->stream);
-        else ctx->launches += launch_fill_temperature(ctx->ka, tmp, ctx->stream);
+        if (field == MMS_FIELD_D) {
+            ctx->launches += launch_compute_d(ctx->ka, ctx->prec, tmp, ctx->stream);
+            ctx->launches += launch_mask_captured(ctx->ka, tmp, 1, ctx->stream);
+        } else {
+            ctx->launches += launch_fill_temperature(ctx->ka, tmp, ctx->stream);
+        }
         CU(cudaMemcpyAsync(host, tmp, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaStreamSynchronize(ctx->stream));
         dfree(ctx, tmp);

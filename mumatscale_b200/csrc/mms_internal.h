@@ -170,6 +170,7 @@ int launch_temp_am(const KernelArgs &a, void *stream, Profiler *prof, double lsd
 int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream);
 int launch_fill_temperature(const KernelArgs &a, double *dev_out, void *stream);
 int launch_compute_d(const KernelArgs &a, int precision, double *dev_out, void *stream);
+int launch_mask_captured(const KernelArgs &a, void *dev, int is_double, void *stream);
 int launch_convert(const KernelArgs &a, int precision, int field, int to_device, double *dev_f64,
                    void *stream);
 

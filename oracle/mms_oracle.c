@@ -1153,7 +1153,13 @@ int mmso_get_field(mmso *o, int field, void *out)
     case MMS_FIELD_FS: memcpy(out, o->fs, N * sizeof(double)); break;
     case MMS_FIELD_GR: memcpy(out, o->gr, N * sizeof(int)); break;
     case MMS_FIELD_DC: memcpy(out, o->dc, N * sizeof(dc3)); break;
-    case MMS_FIELD_D: memcpy(out, o->d, N * sizeof(double)); break;
+    case MMS_FIELD_D: {
+        /* grow_octahedra's value where the cell was solid at the growth step */
+        double *dd = (double *)out;
+        for (size_t c = 0; c < N; c++) dd[c] = o->ogr[c] > 0 ? o->d[c] : 0.0;
+        break;
+    }
+    case MMS_FIELD_OGR: memcpy(out, o->ogr, N * sizeof(int)); break;
     case MMS_FIELD_NUC_THRESHOLD: memcpy(out, o->thr, N * sizeof(float)); break;
     case MMS_FIELD_TEMPERATURE: memcpy(out, o->T, N * sizeof(double)); break;
     case MMS_FIELD_MOLD: memcpy(out, o->mold, N); break;

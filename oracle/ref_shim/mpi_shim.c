@@ -45,7 +45,8 @@ typedef struct {
 typedef struct {
     pthread_mutex_t mu;
     pthread_cond_t cv;
-    pthread_barrier_t bar;
+    long bar_count;
+    long bar_gen;
     int np;
     int abort_flag;
     long seq;
@@ -150,6 +151,22 @@ static void arena_free(size_t payload_off)
 
 static void lock(void) { pthread_mutex_lock(&g_shm->mu); }
 static void unlock(void) { pthread_mutex_unlock(&g_shm->mu); }
+static pid_t g_parent = 0;
+
+/* Waits on the shared condition variable for at most one second, then
+ * returns; a rank that sees the abort flag, or (as a child) finds rank 0
+ * gone, exits instead of waiting forever.  Caller holds the mutex. */
+static void wait_or_die(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_REALTIME, &ts);
+    ts.tv_sec += 1;
+    pthread_cond_timedwait(&g_shm->cv, &g_shm->mu, &ts);
+    if (g_shm->abort_flag || (g_rank != 0 && getppid() != g_parent)) {
+        pthread_mutex_unlock(&g_shm->mu);
+        _exit(1);
+    }
+}
 
 /* ---- init / finalize ---------------------------------------------------- */
 static void shm_setup(int np)
@@ -181,10 +198,6 @@ static void shm_setup(int np)
     pthread_condattr_init(&ca);
     pthread_condattr_setpshared(&ca, PTHREAD_PROCESS_SHARED);
     pthread_cond_init(&g_shm->cv, &ca);
-    pthread_barrierattr_t ba;
-    pthread_barrierattr_init(&ba);
-    pthread_barrierattr_setpshared(&ba, PTHREAD_PROCESS_SHARED);
-    pthread_barrier_init(&g_shm->bar, &ba, (unsigned)np);
 }
 
 int MPI_Init_thread(int *argc, char ***argv, int required, int *provided)
@@ -198,6 +211,7 @@ int MPI_Init_thread(int *argc, char ***argv, int required, int *provided)
     shm_setup(np);
     fflush(stdout);
     fflush(stderr);
+    g_parent = getpid();
     for (int r = 1; r < np; r++) {
         pid_t pid = fork();
         if (pid < 0) {
@@ -225,6 +239,7 @@ int MPI_Finalize(void)
     fflush(stdout);
     fflush(stderr);
     MPI_Barrier(MPI_COMM_WORLD);
+    if (g_shm && g_shm->abort_flag) _exit(1);
     if (g_rank == 0) {
         int bad = 0;
         for (int r = 1; r < g_np; r++) {
@@ -242,10 +257,16 @@ int MPI_Abort(MPI_Comm comm, int code)
     (void)comm;
     fflush(stdout);
     fflush(stderr);
+    if (g_shm) {
+        /* every rank polls this flag in its waits and exits */
+        g_shm->abort_flag = 1;
+        pthread_cond_broadcast(&g_shm->cv);
+    }
     if (g_rank == 0) {
-        for (int r = 1; r < g_np; r++) kill(g_children[r], SIGKILL);
-    } else {
-        kill(getppid(), SIGTERM);
+        for (int r = 1; r < g_np; r++) {
+            int st;
+            waitpid(g_children[r], &st, 0);
+        }
     }
     _exit(code ? code : 1);
 }
@@ -256,7 +277,17 @@ int MPI_Comm_rank(MPI_Comm comm, int *rank) { (void)comm; *rank = g_rank; return
 int MPI_Barrier(MPI_Comm comm)
 {
     (void)comm;
-    if (g_np > 1) pthread_barrier_wait(&g_shm->bar);
+    if (g_np == 1) return MPI_SUCCESS;
+    lock();
+    long gen = g_shm->bar_gen;
+    if (++g_shm->bar_count == g_np) {
+        g_shm->bar_count = 0;
+        g_shm->bar_gen++;
+        pthread_cond_broadcast(&g_shm->cv);
+    } else {
+        while (g_shm->bar_gen == gen) wait_or_die();
+    }
+    unlock();
     return MPI_SUCCESS;
 }
 
@@ -377,7 +408,7 @@ static void complete_recv(struct mmsref_req *r, MPI_Status *st)
             m->used = 0;
             break;
         }
-        pthread_cond_wait(&g_shm->cv, &g_shm->mu);
+        wait_or_die();
     }
     unlock();
 }

@@ -26,7 +26,7 @@
  *   char[8] "MMSDUMP1"; int64 rank, nproc, sbx, sby, sbz, gsdimx, gsdimy,
  *   gsdimz, timestep, num_grains, maxTotalGrains, gindex;
  *   f64 ce[N], cl[N], fs[N], d[N]; f64 dc[3N] (x,y,z packed per cell);
- *   i32 gr[N]; f32 nuc_threshold[N]; f64 temperature[N];
+ *   i32 gr[N]; f32 nuc_threshold[N]; f64 temperature[N]; i32 ogr[N];
  *   grain_t grain_cache[num_grains] (136-byte records, globals.h:244)
  * with N = (gsdimx+2)(gsdimy+2)(gsdimz+2) in the reference's halo'd order.
  */
@@ -95,6 +95,7 @@ static void write_dump(const char *tag)
     fwrite(lsp->gr, sizeof(int), N, f);
     fwrite(lsp->nuc_threshold, sizeof(float), N, f);
     fwrite(lsp->temperature, sizeof(double), N, f);
+    fwrite(lsp->ogr, sizeof(int), N, f);
     fwrite(grain_cache, sizeof(grain_t), bp->num_grains, f);
     fclose(f);
 }

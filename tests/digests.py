@@ -12,9 +12,7 @@ def digest(a: np.ndarray) -> str:
 
 def state_digests(dom) -> dict:
     """dom: a mumatscale_b200.Domain or a tests._oracle.Oracle."""
-    gr = dom.download("gr")
-    out = {f: digest(dom.download(f)) for f in ("ce", "cl", "fs", "gr", "dc", "nuc_threshold")}
-    out["d"] = digest(np.where(gr > 0, dom.download("d"), 0.0))
+    out = {f: digest(dom.download(f)) for f in ("ce", "cl", "fs", "gr", "dc", "nuc_threshold", "d")}
     grains = dom.grains()
     rot = np.array([np.array(g.rotmat).reshape(9) for g in grains[1:]], dtype="<f8").reshape(-1, 9)
     out["grain_rotmat"] = digest(rot)

@@ -54,11 +54,12 @@ def digest(arr: np.ndarray) -> str:
 
 def field_digests(st: dict) -> dict:
     out = {}
-    gr = st["gr"]
     for f in FIELDS:
         a = st[f]
         if f == "d":
-            a = np.where(gr > 0, a, 0.0)
+            # d is defined where grow_octahedra computed it this step: cells
+            # solid before capture (ogr > 0); elsewhere it holds stale values
+            a = np.where(st["ogr"] > 0, a, 0.0)
         out[f] = digest(a)
     rot = np.array([g["rotmat"] for g in st["grains"]], dtype="<f8").reshape(-1, 9)
     out["grain_rotmat"] = digest(rot[1:])

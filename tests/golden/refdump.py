@@ -37,6 +37,7 @@ def read_dump(path: str | Path) -> dict:
     out["gr"] = take("<i4", n, shape)
     out["nuc_threshold"] = take("<f4", n, shape)
     out["temperature"] = take("<f8", n, shape)
+    out["ogr"] = take("<i4", n, shape)
     out["grains"] = np.frombuffer(raw, dtype=GRAIN_DTYPE, count=ngr, offset=off)
     return out
 
@@ -50,7 +51,7 @@ def assemble(dumps: list[dict], nsb: tuple[int, int, int]) -> dict:
     sx, sy, sz = d0["dims"]
     gx, gy, gz = sx * nsb[0], sy * nsb[1], sz * nsb[2]
     out = {k: d0[k] for k in ("timestep", "num_grains", "grains")}
-    for name in ("ce", "cl", "fs", "d", "dc", "gr", "nuc_threshold", "temperature"):
+    for name in ("ce", "cl", "fs", "d", "dc", "gr", "nuc_threshold", "temperature", "ogr"):
         a0 = d0[name]
         shape = (gz + 2, gy + 2, gx + 2) + a0.shape[3:]
         g = np.zeros(shape, dtype=a0.dtype)
