@@ -15,17 +15,24 @@ from digests import digest, mismatches, state_digests
 pytestmark = pytest.mark.gpu
 
 
+# The AM quadrature sums 400 exp() terms per cell (temperature.c:105-114);
+# CUDA's exp is not glibc's, so once the laser is on (t >= 1e-4 s, step 100
+# of am1) temperatures differ in the last bits and the AM deck is compared
+# with tolerances (test_am_tolerance) instead of bit for bit.
+EXACT_UNTIL = {"am1": 100}
+
+
 @pytest.mark.parametrize("name", GOLDEN_DECKS)
 def test_fp64_bit_exact_vs_reference(built, cuda_device, name):
     rec = golden(name)
-    if rec["env"].get("MMSREF_CURV") is None and name == "curv1":
-        pytest.skip("curvature deck needs the hook")
     p = M.read_deck(golden_deck(name))
     with M.Domain(p, precision=M.PREC_F64) as dom:
         assert digest(dom.download("nuc_threshold")) == rec["setup"]["nuc_threshold"]
         last = 0
         for s, want in rec["steps"].items():
             s = int(s)
+            if s > EXACT_UNTIL.get(name, 1 << 30):
+                break
             dom.step(s - last)
             last = s
             assert dom.timestep == s
@@ -37,6 +44,26 @@ def test_fp64_bit_exact_vs_reference(built, cuda_device, name):
                 dom.step(rec["error_at_step"] - last)
             assert e.value.status == 6  # MMS_ERR_GRAIN_OVERFLOW
         assert dom.kernel_launches > 0
+
+
+def test_am_tolerance(built, cuda_device):
+    """AM deck after the laser turns on: temperature differs from glibc's
+    exp in the last bits.  Bounds: identical grain count, grain-id mismatch
+    < 1 % of cells, solute (ce) relative L2 error < 1e-6."""
+    from _oracle import Oracle
+    p = M.read_deck(golden_deck("am1"))
+    o = Oracle(p)
+    with M.Domain(p) as dom:
+        for s in (100, 110, 120, 130):
+            o.step(s - o.timestep)
+            dom.step(s - dom.timestep)
+            T, T0 = dom.download("temperature"), o.download("temperature")
+            assert np.allclose(T, T0, rtol=1e-12, atol=1e-9)
+            assert dom.num_grains == o.num_grains
+            gr, gr0 = dom.download("gr"), o.download("gr")
+            assert (gr != gr0).mean() < 1e-2
+            ce, ce0 = dom.download("ce"), o.download("ce")
+            assert np.linalg.norm(ce - ce0) / np.linalg.norm(ce0) < 1e-6
 
 
 @pytest.mark.parametrize("name", ["small1", "small4", "grad1"])
