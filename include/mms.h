@@ -257,6 +257,9 @@ const char *mms_status_string(mms_status s);
 const char *mms_last_error(const mms_ctx *ctx);
 /* Number of device kernels this context has launched since creation. */
 uint64_t mms_kernel_launches(const mms_ctx *ctx);
+/* 1 when the stencil runs its TMA-fed variant (descriptors encoded), 0 when
+ * it uses its plain-load variant. */
+int mms_uses_tma(const mms_ctx *ctx);
 
 #ifdef __cplusplus
 }

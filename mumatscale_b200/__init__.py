@@ -160,6 +160,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_status_string": (C.c_char_p, [I]),
         "mms_last_error": (C.c_char_p, [P]),
         "mms_kernel_launches": (C.c_uint64, [P]),
+        "mms_uses_tma": (I, [P]),
         "mms_predraw_sites": (I, [C.POINTER(Params), P]),
         "mms_set_stream": (I, [P, P]),
         "mms_set_profiling": (I, [P, I]),
@@ -270,6 +271,10 @@ class Domain:
         v = C.c_int()
         _check(_lib().mms_get_num_grains(self._ctx, C.byref(v)), "mms_get_num_grains", self._ctx)
         return int(v.value)
+
+    @property
+    def uses_tma(self) -> bool:
+        return bool(_lib().mms_uses_tma(self._ctx))
 
     @property
     def kernel_launches(self) -> int:

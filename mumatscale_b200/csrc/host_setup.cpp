@@ -65,7 +65,8 @@ void rotmat_from_angles(double a0, double a1, double a2, double *R)
 
 
 namespace {
-long long cidx(const Geo &g, long long i, long long j, long long k) { return k * g.sz + j * g.sy + i; }
+// host arrays of the setup use the reference layout
+long long cidx(const Geo &g, long long i, long long j, long long k) { return ref_index(g, i, j, k); }
 }  // namespace
 
 // realcoord2scoord, functions.c:91-107
@@ -212,8 +213,8 @@ void setup_sites(const mms_params &p, const Geo &g, const std::vector<mms_fixed_
                     long long c = rcell(x, y, z);
                     if (!mold[c]) {
                         vol.push_back(c);
-                        int surf = mold[c - 1] + mold[c + 1] + mold[c - g.sy] + mold[c + g.sy] + mold[c - g.sz] +
-                                   mold[c + g.sz];
+                        int surf = mold[c - 1] + mold[c + 1] + mold[c - g.rsy] + mold[c + g.rsy] +
+                                   mold[c - g.rsz] + mold[c + g.rsz];
                         if (surf) suf.push_back(c);
                     }
                 }
@@ -243,9 +244,15 @@ Geo make_geo(const mms_params &p)
     g.gx = p.gnsbx * p.gsdimx;
     g.gy = p.gnsby * p.gsdimy;
     g.gz = p.gnsbz * p.gsdimz;
-    g.sy = g.gx + 2;
-    g.sz = (long long)(g.gx + 2) * (g.gy + 2);
+    g.rsy = g.gx + 2;
+    g.rsz = (long long)(g.gx + 2) * (g.gy + 2);
+    g.rN = g.rsz * (g.gz + 2);
+    g.P = (g.gx + 2 + 7) / 8 * 8;
+    g.sy = g.P;
+    g.sz = g.P * (g.gy + 2);
     g.N = g.sz * (g.gz + 2);
+    g.wpr = (g.gx + 31) / 32;
+    g.nwords = (long long)g.wpr * (g.gy + 2) * (g.gz + 2);
     g.sbx = p.gsdimx;
     g.sby = p.gsdimy;
     g.sbz = p.gsdimz;
@@ -257,14 +264,15 @@ Geo make_geo(const mms_params &p)
     g.padx = p.padBndyX;
     g.pady = p.padBndyY;
     g.padz = p.padBndyZ;
-    g.vb = 2048;
-    g.blocks_per_rank = (g.sbcells + g.vb - 1) / g.vb;
+    g.ppr = (p.gsdimx + 31) / 32;
+    g.pieces_per_rank = (long long)p.gsdimy * p.gsdimz * g.ppr;
+    g.blocks_per_rank = (g.pieces_per_rank + LIST_PIECES - 1) / LIST_PIECES;
     return g;
 }
 
 std::vector<signed char> make_mold(const Geo &g)
 {
-    std::vector<signed char> mold((size_t)g.N, 0);
+    std::vector<signed char> mold((size_t)g.rN, 0);
     for (long long K = 0; K < g.gz + 2; K++)
         for (long long J = 0; J < g.gy + 2; J++)
             for (long long I = 0; I < g.gx + 2; I++) {
@@ -304,7 +312,7 @@ extern "C" mms_status mms_predraw_sites(const mms_params *p, float *thr_out)
     std::vector<Rank> ranks;
     init_ranks(*p, g, ranks);
     std::vector<signed char> mold = make_mold(g);
-    std::vector<float> thr((size_t)g.N, INFINITY);
+    std::vector<float> thr((size_t)g.rN, INFINITY);
     std::vector<mms_fixed_nuc> fixed(p->fixed_nucs, p->fixed_nucs + p->n_fixed_nucs);
     std::vector<mms_nuc_volume> vols(p->nuc_volumes, p->nuc_volumes + p->n_nuc_volumes);
     setup_sites(*p, g, fixed, vols, ranks, thr, mold);

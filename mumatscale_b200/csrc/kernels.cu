@@ -12,21 +12,26 @@
 //   k_nuc         nucleation test over the pre-drawn sites (grain.c:1222-1285)
 //   k_act         ordered grain activation (grain.c:840-916, 347-425)
 //   k_curv        Gibbs-Thomson curvature (curvature.c:31-405), TipCurvature only
-//   k_diffuse_fs  diffusion + fs change fused (growth.c:30-170, 177-276)
-//   k_list_count  interface-list flags per block (growth.c:461-538)
+//   k_diffuse_fs  diffusion + fs change fused (growth.c:30-170, 177-276); also
+//                 writes the solid-cell bitmask (gr > 0 after fs change)
+//   k_list_flags  interface-list membership from the bitmask (growth.c:461-538)
+//   k_list_count  list length per block of rank-local raster pieces
 //   k_list_scan   ordered block offsets, per-rank dc_tmp bookkeeping (growth.c:642-660)
 //   k_list_zero   clears dc_tmp regions that the reference re-allocates zeroed
-//   k_capture     list write + octahedron capture (growth.c:339-407, 664-794)
+//   k_capture     ordered list write + octahedron capture (growth.c:339-407, 664-794)
 //   k_apply       dc copy-back and captured grain ids (growth.c:789, 797-807)
 //
 // Fields: ce in place; cl and fs ping-pong between two buffers, the state
 // after step t living in buffer (t & 1).  gr, dc in place.  d is never
 // stored: capture recomputes it from the solid neighbour's dc, fs and
 // grain rotation, which is exactly what grow_octahedra stored for it.
+// Arrays use the device layout of Geo (row pitch P).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 
 #include "mms_internal.h"
 
@@ -98,6 +103,60 @@ __device__ __forceinline__ int block_sum(int v, int *sh)
     return t;
 }
 
+// ------------------------------------------------------- mbarrier + TMA
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: gives up after about a second of polling.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity)
+{
+    for (unsigned it = 0; it < (1u << 22); it++) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (it > 32) __nanosleep(256);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                            unsigned long long *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_u32(dst)), "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
 // ------------------------------------------------------------ temperature
 // AM moving-source quadrature, direct_temp_calc thermal_ana == 1
 // (temperature.c:62-123), over every halo'd cell, for step ctl->timestep+1.
@@ -159,15 +218,19 @@ __global__ void k_temp_am(KernelArgs a, double lsd, double lv, double lhs, doubl
 // --------------------------------------------------------------- nucleation
 // cell_nucleation (grain.c:1222-1285) over the sparse site list: a cell with
 // an infinite threshold can never pass the test, so only sites are tested.
+// Each block keeps its candidates in site order (cand_stage) with a count,
+// so that k_act can gather them in (emulated rank, local raster) order.
+constexpr int NUC_NT = 256;
 template <typename Real>
-__global__ void k_nuc(KernelArgs a)
+__global__ void __launch_bounds__(NUC_NT) k_nuc(KernelArgs a)
 {
     Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
+    __shared__ int sh[NUC_NT / 32];
     const Geo &g = a.g;
     const Phys &p = a.p;
-    long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    bool hit = false;
+    long long s = blockIdx.x * (long long)NUC_NT + threadIdx.x;
+    int hit = 0;
     if (s < a.d.nsites) {
         unsigned long long ts = ctl->timestep + 1;
         long long c = a.d.site_cell[s];
@@ -189,13 +252,17 @@ __global__ void k_nuc(KernelArgs a)
                 double Tunder = p.Tliq - Ttemp;
                 double m = p.ma * Ttemp * Ttemp + p.mb * Ttemp + p.mc;
                 Tunder += m * ((double)cl[c] - p.cinit);
-                if (Tunder > (double)a.d.site_thr[s]) hit = true;
+                if (Tunder > (double)a.d.site_thr[s]) hit = 1;
             }
         }
     }
-    if (hit) a.d.site_flag[s] = 1;
-    unsigned mask = __ballot_sync(FULL_MASK, hit);
-    if ((threadIdx.x & 31) == 0 && mask) atomicAdd(&ctl->ncand, __popc(mask));
+    int tot;
+    int pos = block_exclusive_scan<NUC_NT>(hit, tot, sh);
+    if (hit) a.d.cand_stage[blockIdx.x * (long long)NUC_NT + pos] = (int)s;
+    if (threadIdx.x == 0) {
+        a.d.nuc_blk_cnt[blockIdx.x] = tot;
+        if (tot) atomicAdd(&ctl->ncand, tot);
+    }
 }
 
 __device__ long long find_key(const long long *keys, long long n, long long key)
@@ -214,10 +281,12 @@ __device__ long long find_key(const long long *keys, long long n, long long key)
     return -1;
 }
 
-// activateNewGrains + createGrains (grain.c:840-916, 347-425) with
-// addNewGrain's per-rank cap (grain.c:88-109).  Candidates are gathered in
-// site order, which is (emulated rank, local raster) order, so grain ids
-// match the rank-ordered Allgatherv displacements (grain.c:892-904).
+// activateNewGrains + createGrains (grain.c:840-916, 347-425).  Candidates
+// are gathered in site order, which is (emulated rank, local raster) order,
+// so grain ids match the rank-ordered Allgatherv displacements
+// (grain.c:892-904).  More candidates than MaxTotGrains leaves room for is
+// the reference's createGrains error (grain.c:363-366): nindex2 replaces the
+// capped count (grain.c:1318), so the cap never holds.
 constexpr int ACT_NT = 256;
 __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
 {
@@ -234,14 +303,14 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
         }
         return;
     }
-    // ordered gather of flagged sites
+    // ordered gather of the per-block candidate lists
     int off = 0;
-    for (long long base = 0; base < a.d.nsites; base += ACT_NT) {
-        long long s = base + threadIdx.x;
-        int f = (s < a.d.nsites) ? (int)a.d.site_flag[s] : 0;
+    for (int base = 0; base < a.d.nuc_blocks; base += ACT_NT) {
+        int b = base + threadIdx.x;
+        int n = (b < a.d.nuc_blocks) ? a.d.nuc_blk_cnt[b] : 0;
         int tot;
-        int pos = block_exclusive_scan<ACT_NT>(f, tot, sh);
-        if (f) a.d.cand[off + pos] = (int)s;
+        int pos = off + block_exclusive_scan<ACT_NT>(n, tot, sh);
+        for (int i = 0; i < n; i++) a.d.cand[pos + i] = a.d.cand_stage[(long long)b * NUC_NT + i];
         off += tot;
     }
     if (threadIdx.x == 0) s_abort = 0;
@@ -250,7 +319,6 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
         const Phys &p = a.p;
         const int nr = a.g.nranks;
         int *cnt = rank_scratch;           // candidates per rank
-        int *acc = rank_scratch + nr;      // accepted per rank (after caps)
         int *need = rank_scratch + 2 * nr; // random draws needed per rank
         int *start = rank_scratch + 3 * nr;
         for (int r = 0; r < nr; r++) cnt[r] = 0, need[r] = 0, start[r] = -1;
@@ -261,12 +329,7 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
         }
         const long long num_grains = ctl->num_grains;
         const unsigned long long maxg = p.max_grains;
-        for (int r = 0; r < nr; r++) acc[r] = cnt[r];
-        long long new_act = C;
-        if ((unsigned long long)(num_grains + new_act) > maxg + 1) {
-            // the reference's createGrains stops at the first id above
-            // MaxTotGrains (grain.c:363-366, reached because nindex2 replaces
-            // the capped count, grain.c:1318)
+        if ((unsigned long long)(num_grains + C) > maxg + 1) {
             ctl->status = MMS_ERR_GRAIN_OVERFLOW;
             atomicExch(&ctl->stall, (int)STALL_ERROR);
             s_abort = 1;
@@ -274,7 +337,7 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
         // dry run: orientation draws needed per rank
         bool short_rng = false;
         for (int r = 0; r < nr && p.use_orientation && !s_abort; r++) {
-            for (int i = 0; i < acc[r]; i++) {
+            for (int i = 0; i < cnt[r]; i++) {
                 long long cell = a.d.site_cell[a.d.cand[start[r] + i]];
                 if (find_key(a.d.nucpt_key, a.d.n_nucpt, cell) < 0) need[r]++;
             }
@@ -288,14 +351,8 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
             s_abort = 1;
         } else {
             long long id = num_grains;
-            for (int r = 0; r < nr && !s_abort; r++) {
-                for (int i = 0; i < acc[r]; i++, id++) {
-                    if ((unsigned long long)id > maxg) {
-                        ctl->status = MMS_ERR_GRAIN_OVERFLOW;
-                        ctl->stall = STALL_ERROR;
-                        s_abort = 1;
-                        break;
-                    }
+            for (int r = 0; r < nr; r++) {
+                for (int i = 0; i < cnt[r]; i++, id++) {
                     int s = a.d.cand[start[r] + i];
                     long long cell = a.d.site_cell[s];
                     a.d.gr[cell] = (int)id;
@@ -328,17 +385,12 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
                     a.d.grain_log[id] = lg;
                 }
             }
-            if (!s_abort) {
-                ctl->num_grains = (int)(num_grains + new_act);
-                ctl->new_grains = (int)new_act;
-                ctl->ncand = 0;
-                ctl->timestep = ts;
-            }
+            ctl->num_grains = (int)(num_grains + C);
+            ctl->new_grains = C;
+            ctl->ncand = 0;
+            ctl->timestep = ts;
         }
     }
-    __syncthreads();
-    if (s_abort) return;
-    for (int i = threadIdx.x; i < C; i += ACT_NT) a.d.site_flag[a.d.cand[i]] = 0;
 }
 
 // ---------------------------------------------------------------- curvature
@@ -441,13 +493,11 @@ __global__ void k_curv(KernelArgs a)
 }
 
 // ------------------------------------------------ diffusion + fs change
-// One thread per (i,j) column of a TX x TY tile marching over ZC planes;
-// three halo'd planes of cl and fs live in a shared-memory ring.  Per cell
-// the arithmetic is sb_diffuse_alloy_decentered (growth.c:69-162) followed
-// by fs_change_diffuse (growth.c:220-273) on the same cell, with oce = the
-// ce value before diffusion, held in a register (calculate.c:269-280).
-constexpr int DTX = 32, DTY = 8;
-
+// Per cell: sb_diffuse_alloy_decentered (growth.c:69-162) followed by
+// fs_change_diffuse (growth.c:220-273) on the same cell, with oce = the ce
+// value before diffusion, held in a register (calculate.c:269-280).  The
+// neighbour values are read before any cell of this step writes them: cl
+// and fs come from the previous step's buffer.
 template <typename Real>
 struct PhysR {
     Real rs, rl, liq_slope, k_inv, km, km_inv, m_inv, D_xt, cinit, Tliq, gibbs;
@@ -471,6 +521,189 @@ __device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
     return q;
 }
 
+// nb_* in the order +x, -x, +y, -y, +z, -z (growth.c:85-113); one_m[n] is
+// (1 - mold) of that neighbour.
+template <typename Real>
+__device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p, Real conc, Real lspfs,
+                                            const Real (&nb_cl)[6], const Real (&nb_fs)[6],
+                                            const Real (&one_m)[6], Real oce, int grc, double Td,
+                                            const double *curv, long long c, Real &cen, Real &cl_new,
+                                            Real &fs_new, int &gr_new)
+{
+    Real nbsum = 0;
+#pragma unroll
+    for (int n = 0; n < 6; n++) {
+        Real fs_av = (Real)0.5 * (lspfs + nb_fs[n]);
+        Real r = (q.rs * fs_av + q.rl * (1 - fs_av)) * one_m[n];
+        nbsum += r * (nb_cl[n] - conc);
+    }
+    cen = oce + nbsum;
+    const Real Tcell = (Real)Td;
+    Real c_int = q.cinit + q.m_inv * (Tcell - q.Tliq);
+    Real Tunder = q.Tliq - Tcell;
+    Tunder += q.liq_slope * (conc - q.cinit);
+    gr_new = grc;
+    if (grc <= 0 || Td < 1.0 || Td > p.Tliq) {
+        cl_new = cen;
+        fs_new = 0;
+        gr_new = 0;
+    } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
+        cl_new = cen * q.k_inv;
+        fs_new = lspfs;
+    } else {
+        if (p.tip_curv) {
+            const Real cv = (Real)curv[c];
+            c_int = q.cinit + q.m_inv * (Tcell - q.Tliq + q.gibbs * cv);
+        }
+        Real dce = cen - oce;
+        Real dcl = (c_int - conc) * q.D_xt * 2 + dce / (1 - q.km * lspfs);
+        Real dfs = (dcl * ((Real)1. - q.km * lspfs) - dce) * q.km_inv / conc;
+        cl_new = conc + dcl;
+        fs_new = lspfs + dfs;
+        fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
+        if (fs_new < (Real)0.) {
+            fs_new = 0.;
+            gr_new = 0;
+            cl_new = cen;
+        }
+    }
+}
+
+constexpr int DTX = 32, DTY = 8;
+
+// TMA-fed variant.  A CTA owns a 32 x 8 column of cells and marches up a
+// z-chunk; planes of cl and fs with their x/y halo (and ce, gr without) are
+// brought into a TS-deep shared-memory ring by cp.async.bulk.tensor, one
+// mbarrier per slot, issued TS-1 planes ahead of the plane being updated.
+constexpr int TS = 5;
+constexpr int round128(int b) { return (b + 127) / 128 * 128; }
+
+template <typename Real>
+struct Stage {
+    // box widths: a multiple of 16 bytes, starting at the aligned column i0-1
+    static constexpr int BXH = sizeof(Real) == 8 ? 34 : 36;  // cl, fs: DTY+2 rows
+    static constexpr int BXC = sizeof(Real) == 8 ? 34 : 36;  // ce: DTY rows
+    static constexpr int BXG = 36;                           // gr (int): DTY rows
+    static constexpr int CL = round128(BXH * (DTY + 2) * (int)sizeof(Real));
+    static constexpr int CE = round128(BXC * DTY * (int)sizeof(Real));
+    static constexpr int GR = round128(BXG * DTY * 4);
+    static constexpr int BYTES = 2 * CL + CE + GR;
+    static constexpr unsigned TX_HALO = 2u * BXH * (DTY + 2) * sizeof(Real);
+    static constexpr unsigned TX_CENTER = BXC * DTY * sizeof(Real) + BXG * DTY * 4u;
+};
+
+struct TmaMaps {
+    CUtensorMap cl[2], fs[2], ce, gr;
+};
+
+template <typename Real>
+__global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs_tma(const __grid_constant__ KernelArgs a,
+                                                             const __grid_constant__ TmaMaps maps, int zchunk)
+{
+    using L = Stage<Real>;
+    Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long bars[TS];
+    const Geo &g = a.g;
+    const Phys &p = a.p;
+    const unsigned long long ts = ctl->timestep;
+    const int pin = (int)((ts - 1) & 1ULL), pout = (int)(ts & 1ULL);
+    Real *__restrict__ clO = (Real *)a.d.cl[pout];
+    Real *__restrict__ fsO = (Real *)a.d.fs[pout];
+    Real *__restrict__ ce = (Real *)a.d.ce;
+    int *__restrict__ gr = a.d.gr;
+    const PhysR<Real> q = phys_r<Real>(p);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DTX + tx;
+    const int i0 = blockIdx.x * DTX + 1, j0 = blockIdx.y * DTY + 1;
+    const int i = i0 + tx, j = j0 + ty;
+    const int k0 = blockIdx.z * zchunk + 1;
+    const int k1 = min(k0 + zchunk - 1, g.gz);
+    const int nplanes = k1 - k0 + 3;  // k0-1 .. k1+1
+    const bool active = (i <= g.gx) && (j <= g.gy);
+    const CUtensorMap *mcl = &maps.cl[pin];
+    const CUtensorMap *mfs = &maps.fs[pin];
+
+    auto stage = [&](int s) { return smem + s * L::BYTES; };
+    auto issue = [&](int pl) {
+        const int s = pl % TS, k = k0 - 1 + pl;
+        const bool center = (k >= k0 && k <= k1);
+        mbar_expect_tx(&bars[s], L::TX_HALO + (center ? L::TX_CENTER : 0u));
+        tma_load_3d(stage(s), mcl, i0 - 1, j0 - 1, k, &bars[s]);
+        tma_load_3d(stage(s) + L::CL, mfs, i0 - 1, j0 - 1, k, &bars[s]);
+        if (center) {
+            tma_load_3d(stage(s) + 2 * L::CL, &maps.ce, i0 - 1, j0, k, &bars[s]);
+            tma_load_3d(stage(s) + 2 * L::CL + L::CE, &maps.gr, i0 - 1, j0, k, &bars[s]);
+        }
+    };
+    if (tid == 0) {
+        for (int s = 0; s < TS; s++) mbar_init(&bars[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int pl = 0; pl < TS && pl < nplanes; pl++) issue(pl);
+    int issued = min(TS, nplanes);  // same value in every thread
+
+    const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_z = (Real)(1 - g.padz);
+    const long long wrow = (long long)g.wpr;
+    for (int t = 0; t <= k1 - k0; t++) {
+        const int k = k0 + t;
+        bool ok = true;
+        for (int pl = t; pl <= t + 2; pl++) ok &= mbar_wait(&bars[pl % TS], (unsigned)((pl / TS) & 1));
+        if (__syncthreads_or(!ok)) {
+            // a copy did not land within the bound: report, then wait (again
+            // bounded) for every copy still in flight before leaving
+            if (tid == 0) {
+                raise_error(ctl, MMS_ERR_TIMEOUT);
+                for (int pl = t; pl < issued; pl++) mbar_wait(&bars[pl % TS], (unsigned)((pl / TS) & 1));
+            }
+            __syncthreads();
+            break;
+        }
+        int solid = 0;
+        if (active) {
+            const Real *cm = (const Real *)stage(t % TS);
+            const Real *cc = (const Real *)stage((t + 1) % TS);
+            const Real *cp = (const Real *)stage((t + 2) % TS);
+            const Real *fm = (const Real *)(stage(t % TS) + L::CL);
+            const Real *fc = (const Real *)(stage((t + 1) % TS) + L::CL);
+            const Real *fp = (const Real *)(stage((t + 2) % TS) + L::CL);
+            const Real *sce = (const Real *)(stage((t + 1) % TS) + 2 * L::CL);
+            const int *sgr = (const int *)(stage((t + 1) % TS) + 2 * L::CL + L::CE);
+            const int h = (ty + 1) * L::BXH + tx + 1;
+            const Real nb_cl[6] = {cc[h + 1], cc[h - 1], cc[h + L::BXH], cc[h - L::BXH], cp[h], cm[h]};
+            const Real nb_fs[6] = {fc[h + 1], fc[h - 1], fc[h + L::BXH], fc[h - L::BXH], fp[h], fm[h]};
+            const Real one_m[6] = {i == g.gx ? one_x : (Real)1, i == 1 ? one_x : (Real)1,
+                                   j == g.gy ? one_y : (Real)1, j == 1 ? one_y : (Real)1,
+                                   k == g.gz ? one_z : (Real)1, k == 1 ? one_z : (Real)1};
+            const long long c = (long long)k * g.sz + (long long)j * g.sy + i;
+            const Real oce = sce[ty * L::BXC + tx + 1];
+            const int grc = sgr[ty * L::BXG + tx + 1];
+            const double Td = temp_cell(p, a.d.T, c, j, k, ts);
+            Real cen, cl_new, fs_new;
+            int gr_new;
+            cell_update<Real>(q, p, cc[h], fc[h], nb_cl, nb_fs, one_m, oce, grc, Td, a.d.curv, c, cen, cl_new,
+                              fs_new, gr_new);
+            ce[c] = cen;
+            clO[c] = cl_new;
+            fsO[c] = fs_new;
+            if (gr_new != grc) gr[c] = gr_new;
+            if (cen < 0) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
+            solid = gr_new > 0;
+        }
+        const unsigned word = __ballot_sync(FULL_MASK, solid);
+        if (tx == 0 && j <= g.gy) a.d.solid_bits[((long long)k * (g.gy + 2) + j) * wrow + blockIdx.x] = word;
+        __syncthreads();
+        if (t + TS < nplanes) {
+            if (tid == 0) issue(t + TS);
+            issued = t + TS + 1;
+        }
+    }
+}
+
+// Plain-load variant (used when the driver cannot encode the TMA
+// descriptors): three halo'd planes in a shared ring filled by the threads.
 template <typename Real>
 __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchunk)
 {
@@ -514,70 +747,37 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchun
     load_plane(0, k0 - 1);
     load_plane(1, k0);
     int sm = 0, sc = 1, sp = 2;
-    const double one_x = (double)(1 - g.padx), one_y = (double)(1 - g.pady), one_z = (double)(1 - g.padz);
+    const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_z = (Real)(1 - g.padz);
     for (int k = k0; k <= k1; k++) {
         load_plane(sp, k + 1);
         __syncthreads();
+        int solid = 0;
         if (active) {
             const long long c = (long long)k * g.sz + (long long)j * g.sy + i;
             const int ly = ty + 1, lx = tx + 1;
-            const Real conc = s_cl[sc][ly][lx];
-            const Real lspfs = s_fs[sc][ly][lx];
-            // neighbour order +x, -x, +y, -y, +z, -z (growth.c:85-113)
             const Real nb_cl[6] = {s_cl[sc][ly][lx + 1], s_cl[sc][ly][lx - 1], s_cl[sc][ly + 1][lx],
                                    s_cl[sc][ly - 1][lx], s_cl[sp][ly][lx], s_cl[sm][ly][lx]};
             const Real nb_fs[6] = {s_fs[sc][ly][lx + 1], s_fs[sc][ly][lx - 1], s_fs[sc][ly + 1][lx],
                                    s_fs[sc][ly - 1][lx], s_fs[sp][ly][lx], s_fs[sm][ly][lx]};
-            const Real one_m[6] = {(Real)(i == g.gx ? one_x : 1.0), (Real)(i == 1 ? one_x : 1.0),
-                                   (Real)(j == g.gy ? one_y : 1.0), (Real)(j == 1 ? one_y : 1.0),
-                                   (Real)(k == g.gz ? one_z : 1.0), (Real)(k == 1 ? one_z : 1.0)};
-            Real nbsum = 0;
-#pragma unroll
-            for (int n = 0; n < 6; n++) {
-                Real fs_av = (Real)0.5 * (lspfs + nb_fs[n]);
-                Real r = (q.rs * fs_av + q.rl * (1 - fs_av)) * one_m[n];
-                nbsum += r * (nb_cl[n] - conc);
-            }
-            const Real oce = ce[c];
-            const Real cen = oce + nbsum;
-            ce[c] = cen;
-            if (cen < 0) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
-
-            // fs_change_diffuse
-            const double Td = temp_cell(p, a.d.T, c, j, k, ts);
-            const Real Tcell = (Real)Td;
-            Real c_int = q.cinit + q.m_inv * (Tcell - q.Tliq);
-            Real Tunder = q.Tliq - Tcell;
-            Tunder += q.liq_slope * (conc - q.cinit);
+            const Real one_m[6] = {i == g.gx ? one_x : (Real)1, i == 1 ? one_x : (Real)1,
+                                   j == g.gy ? one_y : (Real)1, j == 1 ? one_y : (Real)1,
+                                   k == g.gz ? one_z : (Real)1, k == 1 ? one_z : (Real)1};
             const int grc = gr[c];
-            Real cl_new, fs_new;
-            if (grc <= 0 || Td < 1.0 || Td > p.Tliq) {
-                cl_new = cen;
-                fs_new = 0;
-                if (grc != 0) gr[c] = 0;
-            } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
-                cl_new = cen * q.k_inv;
-                fs_new = lspfs;
-            } else {
-                if (p.tip_curv) {
-                    const Real cv = (Real)a.d.curv[c];
-                    c_int = q.cinit + q.m_inv * (Tcell - q.Tliq + q.gibbs * cv);
-                }
-                Real dce = cen - oce;
-                Real dcl = (c_int - conc) * q.D_xt * 2 + dce / (1 - q.km * lspfs);
-                Real dfs = (dcl * ((Real)1. - q.km * lspfs) - dce) * q.km_inv / conc;
-                cl_new = conc + dcl;
-                fs_new = lspfs + dfs;
-                fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
-                if (fs_new < (Real)0.) {
-                    fs_new = 0.;
-                    gr[c] = 0;
-                    cl_new = cen;
-                }
-            }
+            const double Td = temp_cell(p, a.d.T, c, j, k, ts);
+            Real cen, cl_new, fs_new;
+            int gr_new;
+            cell_update<Real>(q, p, s_cl[sc][ly][lx], s_fs[sc][ly][lx], nb_cl, nb_fs, one_m, ce[c], grc, Td,
+                              a.d.curv, c, cen, cl_new, fs_new, gr_new);
+            ce[c] = cen;
             clO[c] = cl_new;
             fsO[c] = fs_new;
+            if (gr_new != grc) gr[c] = gr_new;
+            if (cen < 0) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
+            solid = gr_new > 0;
         }
+        const unsigned word = __ballot_sync(FULL_MASK, solid);
+        if (tx == 0 && j <= g.gy)
+            a.d.solid_bits[((long long)k * (g.gy + 2) + j) * (long long)g.wpr + blockIdx.x] = word;
         __syncthreads();
         int t = sm;
         sm = sc;
@@ -587,23 +787,65 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchun
 }
 
 // ------------------------------------------------------- interface list
-// grow_cell_reduction (growth.c:461-538): a non-mold liquid cell whose six
-// neighbours' grain ids sum above zero.  Blocks cover VB consecutive cells
-// of one emulated rank in local raster order, so block order = list order.
+// grow_cell_reduction (growth.c:461-538): a non-mold liquid cell with a
+// solid face neighbour (all grain ids are >= 0, so "sum of the six
+// neighbours' ids > 0" is "some neighbour solid").  Interior cells are
+// never mold in one domain.
 constexpr int LIST_NT = 256;
 
-__device__ __forceinline__ long long list_cell_of(const Geo &g, int r, long long l)
+__global__ void __launch_bounds__(LIST_NT) k_list_flags(KernelArgs a)
 {
-    int i = (int)(l % g.sbx) + 1, j = (int)((l / g.sbx) % g.sby) + 1, k = (int)(l / ((long long)g.sbx * g.sby)) + 1;
-    int rx = r % g.nsbx, ry = (r / g.nsbx) % g.nsby, rz = r / (g.nsbx * g.nsby);
-    return (long long)(rz * g.sbz + k) * g.sz + (long long)(ry * g.sby + j) * g.sy + (rx * g.sbx + i);
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const Geo &g = a.g;
+    long long wi = blockIdx.x * (long long)LIST_NT + threadIdx.x;
+    if (wi >= g.nwords) return;
+    const unsigned *sb = a.d.solid_bits;
+    const long long wpr = g.wpr, plane = wpr * (g.gy + 2);
+    long long w = wi % wpr, row = wi / wpr;
+    long long J = row % (g.gy + 2), K = row / (g.gy + 2);
+    unsigned F = 0;
+    if (J >= 1 && J <= g.gy && K >= 1 && K <= g.gz) {
+        unsigned S = sb[wi];
+        unsigned Sl = w > 0 ? sb[wi - 1] : 0u, Sr = (w + 1 < wpr) ? sb[wi + 1] : 0u;
+        unsigned nb = (S << 1) | (Sl >> 31);
+        nb |= (S >> 1) | (Sr << 31);
+        nb |= sb[wi + wpr] | sb[wi - wpr] | sb[wi + plane] | sb[wi - plane];
+        long long nbits = g.gx - 32 * w;
+        unsigned valid = nbits >= 32 ? FULL_MASK : ((1u << nbits) - 1u);
+        F = ~S & nb & valid;
+    }
+    a.d.flag_bits[wi] = F;
 }
 
-__device__ __forceinline__ bool is_list_cell(const int *gr, const Geo &g, long long c)
+// A piece is 32 consecutive cells of one emulated rank's local row; pieces
+// are numbered in rank-local raster order, so list order = piece order.
+struct Piece {
+    unsigned bits;
+    long long base;  // device index of the piece's first cell
+};
+
+__device__ __forceinline__ Piece piece_of(const KernelArgs &a, int r, long long q)
 {
-    if (gr[c] > 0) return false;
-    int nb = gr[c + 1] + gr[c - 1] + gr[c + g.sy] + gr[c - g.sy] + gr[c + g.sz] + gr[c - g.sz];
-    return nb > 0;
+    const Geo &g = a.g;
+    Piece pc{0u, 0};
+    if (q >= g.pieces_per_rank) return pc;
+    long long lr = q / g.ppr;
+    int part = (int)(q % g.ppr);
+    int ly = (int)(lr % g.sby), lz = (int)(lr / g.sby);
+    int rx = r % g.nsbx, ry = (r / g.nsbx) % g.nsby, rz = r / (g.nsbx * g.nsby);
+    long long J = (long long)ry * g.sby + ly + 1, K = (long long)rz * g.sbz + lz + 1;
+    long long X0 = (long long)rx * g.sbx + 32LL * part;  // 0-based interior x
+    int len = min(32, g.sbx - 32 * part);
+    const unsigned *fb = a.d.flag_bits + (K * (g.gy + 2) + J) * (long long)g.wpr;
+    long long w = X0 >> 5;
+    int sh = (int)(X0 & 31);
+    unsigned bits = fb[w] >> sh;
+    if (sh && w + 1 < g.wpr) bits |= fb[w + 1] << (32 - sh);
+    if (len < 32) bits &= (1u << len) - 1u;
+    pc.bits = bits;
+    pc.base = K * g.sz + J * g.sy + X0 + 1;
+    return pc;
 }
 
 __global__ void __launch_bounds__(LIST_NT) k_list_count(KernelArgs a)
@@ -613,10 +855,9 @@ __global__ void __launch_bounds__(LIST_NT) k_list_count(KernelArgs a)
     __shared__ int sh[LIST_NT / 32];
     const Geo &g = a.g;
     int r = (int)(blockIdx.x / g.blocks_per_rank);
-    long long chunk = blockIdx.x % g.blocks_per_rank;
-    long long l0 = chunk * g.vb, l1 = min(l0 + g.vb, g.sbcells);
+    long long q0 = (blockIdx.x % g.blocks_per_rank) * (long long)LIST_PIECES;
     int n = 0;
-    for (long long l = l0 + threadIdx.x; l < l1; l += LIST_NT) n += is_list_cell(a.d.gr, g, list_cell_of(g, r, l));
+    for (int it = 0; it < LIST_PIECES / LIST_NT; it++) n += __popc(piece_of(a, r, q0 + it * LIST_NT + threadIdx.x).bits);
     int tot = block_sum<LIST_NT>(n, sh);
     if (threadIdx.x == 0) a.d.blk_cnt[blockIdx.x] = tot;
 }
@@ -676,11 +917,75 @@ __global__ void k_list_zero(KernelArgs a)
         base[s] = Dc3{0.0, 0.0, 0.0};
 }
 
-// capture_octahedra_diffuse, INDEX_SEP branch (growth.c:664-794), with
-// grow_octahedra's half diagonal (growth.c:372-403) evaluated for the solid
-// neighbour on demand.  Results go to per-slot buffers; k_apply commits them
-// after every capture has read the pre-capture grain ids (the reference's
-// ogr copy, growth.c:635-638).
+// capture_octahedra_diffuse, INDEX_SEP branch (growth.c:664-794), for the
+// list cell c, with grow_octahedra's half diagonal (growth.c:372-403)
+// evaluated for the solid neighbour on demand.  Returns the capturing
+// grain id (0 = not captured) and the new octahedron centre.
+template <typename Real>
+__device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs, long long c, Dc3 &out)
+{
+    const Geo &g = a.g;
+    const Phys &p = a.p;
+    const int *gr = a.d.gr;
+    const Dc3 *dc = a.d.dc;
+    // neighbour order +x, +y, -x, -y, +z, -z (growth.c:604-610, 674-677)
+    const long long ndxs[6] = {c + 1, c + g.sy, c - 1, c - g.sy, c + g.sz, c - g.sz};
+    const int nnx[6] = {1, 0, -1, 0, 0, 0}, nny[6] = {0, 1, 0, -1, 0, 0}, nnz[6] = {0, 0, 0, 0, 1, -1};
+    int found = -1, gid = 0;
+    double g00 = 0, g10 = 0, g20 = 0, g01 = 0, g11 = 0, g21 = 0, g02 = 0, g12 = 0, g22 = 0;
+    double dx = 0, dy = 0, dz = 0, dn = 0;
+    Dc3 dcn{0, 0, 0};
+#pragma unroll 1
+    for (int n = 0; n < 6; n++) {
+        long long ndx = ndxs[n];
+        int id = gr[ndx];
+        if (id > 0 && (unsigned long long)id < p.max_grains) {
+            const double *R = a.d.grain_rot + 9 * (long long)id;
+            g00 = R[0]; g01 = R[1]; g02 = R[2];
+            g10 = R[3]; g11 = R[4]; g12 = R[5];
+            g20 = R[6]; g21 = R[7]; g22 = R[8];
+            dcn = dc[ndx];
+            double rx0 = 0.0 - dcn.x, ry0 = 0.0 - dcn.y, rz0 = 0.0 - dcn.z;
+            double gx0 = g00 * rx0 + g10 * ry0 + g20 * rz0;
+            double gy0 = g01 * rx0 + g11 * ry0 + g21 * rz0;
+            double gz0 = g02 * rx0 + g12 * ry0 + g22 * rz0;
+            double ds1 = fabs(gx0) + fabs(gy0) + fabs(gz0);
+            ds1 = (ds1 < 1.5) ? ds1 : 1.5;
+            dn = ds1 + (double)fs[ndx] * p.fsgrow;
+            double rx1 = -1.0 * nnx[n] - dcn.x;
+            double ry1 = -1.0 * nny[n] - dcn.y;
+            double rz1 = -1.0 * nnz[n] - dcn.z;
+            dx = g00 * rx1 + g10 * ry1 + g20 * rz1;
+            dy = g01 * rx1 + g11 * ry1 + g21 * rz1;
+            dz = g02 * rx1 + g12 * ry1 + g22 * rz1;
+            double dfs = dn - (fabs(dx) + fabs(dy) + fabs(dz));
+            if (dfs > 0) {
+                found = n;
+                gid = id;
+                break;
+            }
+        }
+    }
+    if (found < 0) return 0;
+    double ncx = 0., ncz = 0., ncy = 0.;
+    double ncd = (dn < 1.0) ? dn : 1.0;
+    double dd = dn - ncd;
+    if (dx + dy >= 0 && dx - dy > 0 && dx + dz > 0 && dx - dz >= 0) ncx = dd;
+    else if (dx + dy <= 0 && dx - dy < 0 && dx + dz < 0 && dx - dz <= 0) ncx = -1. * dd;
+    else if (dy + dx > 0 && dy - dx >= 0 && dy + dz >= 0 && dy - dz > 0) ncy = dd;
+    else if (dy + dx < 0 && dy - dx <= 0 && dy + dz <= 0 && dy - dz < 0) ncy = -1. * dd;
+    else if (dz + dx >= 0 && dz - dx > 0 && dz + dy > 0 && dz - dy >= 0) ncz = dd;
+    else ncz = -1. * dd;
+    out.x = dcn.x + (double)nnx[found] + g00 * ncx + g01 * ncy + g02 * ncz;
+    out.y = dcn.y + (double)nny[found] + g10 * ncx + g11 * ncy + g12 * ncz;
+    out.z = dcn.z + (double)nnz[found] + g20 * ncx + g21 * ncy + g22 * ncz;
+    return gid;
+}
+
+// Writes this block's part of the ordered list, then captures its entries.
+// Results go to per-slot buffers; k_apply commits them after every capture
+// has read the pre-capture grain ids (the reference's ogr copy,
+// growth.c:635-638).
 template <typename Real>
 __global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
 {
@@ -688,88 +993,35 @@ __global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
     if (stalled(ctl)) return;
     __shared__ int sh[LIST_NT / 32];
     const Geo &g = a.g;
-    const Phys &p = a.p;
     const int r = (int)(blockIdx.x / g.blocks_per_rank);
-    const long long chunk = blockIdx.x % g.blocks_per_rank;
-    const long long l0 = chunk * g.vb, l1 = min(l0 + g.vb, g.sbcells);
+    const long long q0 = (blockIdx.x % g.blocks_per_rank) * (long long)LIST_PIECES;
+    const int first = a.d.blk_off[blockIdx.x];
+    const int count = a.d.blk_cnt[blockIdx.x];
+    if (count == 0) return;
+    int pos = first;
+    for (int it = 0; it < LIST_PIECES / LIST_NT; it++) {
+        Piece pc = piece_of(a, r, q0 + it * LIST_NT + threadIdx.x);
+        int tot;
+        int p0 = pos + block_exclusive_scan<LIST_NT>(__popc(pc.bits), tot, sh);
+        pos += tot;
+        unsigned b = pc.bits;
+        while (b) {
+            int bit = __ffs(b) - 1;
+            b &= b - 1;
+            a.d.list_cell[p0++] = pc.base + bit;
+        }
+    }
+    __syncthreads();
     const int pout = (int)(ctl->timestep & 1ULL);
     const Real *fs = (const Real *)a.d.fs[pout];
-    const int *gr = a.d.gr;
-    const Dc3 *dc = a.d.dc;
     const int rank_start = a.d.blk_off[(long long)r * g.blocks_per_rank];
-    int pos_base = a.d.blk_off[blockIdx.x];
     const long long dcbase = a.d.rank_dcbase[r];
-    for (long long lb = l0; lb < l1; lb += LIST_NT) {
-        long long l = lb + threadIdx.x;
-        long long c = 0;
-        int f = 0;
-        if (l < l1) {
-            c = list_cell_of(g, r, l);
-            f = is_list_cell(gr, g, c);
-        }
-        int tot;
-        int pos = pos_base + block_exclusive_scan<LIST_NT>(f, tot, sh);
-        pos_base += tot;
-        if (!f) continue;
-        const int slot = pos - rank_start + 1;
-        a.d.list_cell[pos] = c;
-        // neighbour order +x, +y, -x, -y, +z, -z (growth.c:604-610, 674-677)
-        const long long ndxs[6] = {c + 1, c + g.sy, c - 1, c - g.sy, c + g.sz, c - g.sz};
-        const int nnx[6] = {1, 0, -1, 0, 0, 0}, nny[6] = {0, 1, 0, -1, 0, 0}, nnz[6] = {0, 0, 0, 0, 1, -1};
-        int found = -1, gid = 0;
-        double g00 = 0, g10 = 0, g20 = 0, g01 = 0, g11 = 0, g21 = 0, g02 = 0, g12 = 0, g22 = 0;
-        double dx = 0, dy = 0, dz = 0, dn = 0;
-        Dc3 dcn{0, 0, 0};
-        for (int n = 0; n < 6; n++) {
-            long long ndx = ndxs[n];
-            int id = gr[ndx];
-            if (id > 0 && (unsigned long long)id < p.max_grains) {
-                const double *R = a.d.grain_rot + 9 * (long long)id;
-                g00 = R[0]; g01 = R[1]; g02 = R[2];
-                g10 = R[3]; g11 = R[4]; g12 = R[5];
-                g20 = R[6]; g21 = R[7]; g22 = R[8];
-                dcn = dc[ndx];
-                // grow_octahedra for the neighbour
-                double rx0 = 0.0 - dcn.x, ry0 = 0.0 - dcn.y, rz0 = 0.0 - dcn.z;
-                double gx0 = g00 * rx0 + g10 * ry0 + g20 * rz0;
-                double gy0 = g01 * rx0 + g11 * ry0 + g21 * rz0;
-                double gz0 = g02 * rx0 + g12 * ry0 + g22 * rz0;
-                double ds1 = fabs(gx0) + fabs(gy0) + fabs(gz0);
-                ds1 = (ds1 < 1.5) ? ds1 : 1.5;
-                dn = ds1 + (double)fs[ndx] * p.fsgrow;
-                // capture test
-                double rx1 = -1.0 * nnx[n] - dcn.x;
-                double ry1 = -1.0 * nny[n] - dcn.y;
-                double rz1 = -1.0 * nnz[n] - dcn.z;
-                dx = g00 * rx1 + g10 * ry1 + g20 * rz1;
-                dy = g01 * rx1 + g11 * ry1 + g21 * rz1;
-                dz = g02 * rx1 + g12 * ry1 + g22 * rz1;
-                double dfs = dn - (fabs(dx) + fabs(dy) + fabs(dz));
-                if (dfs > 0) {
-                    found = n;
-                    gid = id;
-                    break;
-                }
-            }
-        }
-        if (found > -1) {
-            double ncx = 0., ncz = 0., ncy = 0.;
-            double ncd = (dn < 1.0) ? dn : 1.0;
-            double dd = dn - ncd;
-            if (dx + dy >= 0 && dx - dy > 0 && dx + dz > 0 && dx - dz >= 0) ncx = dd;
-            else if (dx + dy <= 0 && dx - dy < 0 && dx + dz < 0 && dx - dz <= 0) ncx = -1. * dd;
-            else if (dy + dx > 0 && dy - dx >= 0 && dy + dz >= 0 && dy - dz > 0) ncy = dd;
-            else if (dy + dx < 0 && dy - dx <= 0 && dy + dz <= 0 && dy - dz < 0) ncy = -1. * dd;
-            else if (dz + dx >= 0 && dz - dx > 0 && dz + dy > 0 && dz - dy >= 0) ncz = dd;
-            else ncz = -1. * dd;
-            Dc3 out;
-            out.x = dcn.x + (double)nnx[found] + g00 * ncx + g01 * ncy + g02 * ncz;
-            out.y = dcn.y + (double)nny[found] + g10 * ncx + g11 * ncy + g12 * ncz;
-            out.z = dcn.z + (double)nnz[found] + g20 * ncx + g21 * ncy + g22 * ncz;
-            a.d.dc_tmp[dcbase + slot] = out;
-        }
-        a.d.list_gid[pos] = gid;
-        // slot is recovered in k_apply from the position and the rank start
+    for (int e = first + threadIdx.x; e < first + count; e += LIST_NT) {
+        const long long c = a.d.list_cell[e];
+        Dc3 out;
+        const int gid = capture_cell<Real>(a, fs, c, out);
+        if (gid) a.d.dc_tmp[dcbase + (e - rank_start + 1)] = out;
+        a.d.list_gid[e] = gid;
     }
 }
 
@@ -873,7 +1125,6 @@ __global__ void k_fill_temperature(KernelArgs a, double *out)
     long long K = c / g.sz, J = (c % g.sz) / g.sy;
     out[c] = temp_cell(a.p, a.d.T, c, J, K, ctl->timestep);
 }
-
 // Zero the entries of cells captured by the last step (list cells whose
 // capture produced a grain id): turns gr into the reference's ogr, and
 // limits d to cells that were solid at the growth step.
@@ -920,13 +1171,74 @@ __global__ void k_convert(KernelArgs a, int field, int to_device, double *buf)
 static int pick_zchunk(const Geo &g)
 {
     long long tiles = (long long)((g.gx + DTX - 1) / DTX) * ((g.gy + DTY - 1) / DTY);
-    // aim for >= 8 blocks per SM on 148 SMs
-    long long want = 148LL * 8;
-    int zc = (int)((tiles * g.gz + want - 1) / want);
+    // aim for >= 4 CTAs per SM on 148 SMs, chunks of at most 32 planes
+    long long want = 148LL * 4;
+    int zc = (int)((tiles * g.gz) / want);
     if (zc < 4) zc = 4;
-    if (zc > 64) zc = 64;
+    if (zc > 32) zc = 32;
     if (zc > g.gz) zc = g.gz;
     return zc;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+static bool encode3d(CUtensorMap *m, CUtensorMapDataType dt, int es, void *base, const Geo &g, int bx, int by)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)(g.gx + 2), (cuuint64_t)(g.gy + 2), (cuuint64_t)(g.gz + 2)};
+    cuuint64_t strides[2] = {(cuuint64_t)(g.P * es), (cuuint64_t)(g.P * (g.gy + 2) * es)};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    return fn(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename Real>
+static int make_tma_t(const KernelArgs &a, TmaHolder &out)
+{
+    static_assert(sizeof(TmaMaps) <= sizeof(out.bytes), "TMA holder too small");
+    using L = Stage<Real>;
+    TmaMaps m;
+    std::memset(&m, 0, sizeof m);
+    const CUtensorMapDataType dt = sizeof(Real) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const int es = (int)sizeof(Real);
+    bool ok = true;
+    for (int b = 0; b < 2; b++) {
+        ok &= encode3d(&m.cl[b], dt, es, a.d.cl[b], a.g, L::BXH, DTY + 2);
+        ok &= encode3d(&m.fs[b], dt, es, a.d.fs[b], a.g, L::BXH, DTY + 2);
+    }
+    ok &= encode3d(&m.ce, dt, es, a.d.ce, a.g, L::BXC, DTY);
+    ok &= encode3d(&m.gr, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, a.d.gr, a.g, L::BXG, DTY);
+    std::memcpy(out.bytes, &m, sizeof m);
+    out.ok = ok ? 1 : 0;
+    if (ok) {
+        cudaFuncSetAttribute(k_diffuse_fs_tma<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS * L::BYTES);
+    }
+    return out.ok;
+}
+
+int make_tma(const KernelArgs &a, int precision, TmaHolder &out)
+{
+    if (precision == MMS_PREC_F32) return make_tma_t<float>(a, out);
+    return make_tma_t<double>(a, out);
 }
 
 #define PROF_BEGIN(id) \
@@ -935,14 +1247,13 @@ static int pick_zchunk(const Geo &g)
     if (prof) prof->end(id, st)
 
 template <typename Real>
-static int launch_step_t(const KernelArgs &a, cudaStream_t st, int start_stage, Profiler *prof)
+static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st, int start_stage, Profiler *prof)
 {
     int n = 0;
     const Geo &g = a.g;
     if (start_stage == 0 && a.d.nsites > 0) {
-        int nb = (int)((a.d.nsites + 255) / 256);
         PROF_BEGIN(KID_NUC);
-        k_nuc<Real><<<nb, 256, 0, st>>>(a);
+        k_nuc<Real><<<a.d.nuc_blocks, NUC_NT, 0, st>>>(a);
         PROF_END(KID_NUC);
         n++;
     }
@@ -959,13 +1270,22 @@ static int launch_step_t(const KernelArgs &a, cudaStream_t st, int start_stage, 
     }
     {
         int zc = pick_zchunk(g);
-        dim3 grid((g.gx + DTX - 1) / DTX, (g.gy + DTY - 1) / DTY, (g.gz + zc - 1) / zc);
+        dim3 grid(g.wpr, (g.gy + DTY - 1) / DTY, (g.gz + zc - 1) / zc);
         PROF_BEGIN(KID_DIFFUSE_FS);
-        k_diffuse_fs<Real><<<grid, dim3(DTX, DTY), 0, st>>>(a, zc);
+        if (tma.ok) {
+            TmaMaps maps;
+            std::memcpy(&maps, tma.bytes, sizeof maps);
+            k_diffuse_fs_tma<Real><<<grid, dim3(DTX, DTY), TS * Stage<Real>::BYTES, st>>>(a, maps, zc);
+        } else {
+            k_diffuse_fs<Real><<<grid, dim3(DTX, DTY), 0, st>>>(a, zc);
+        }
         PROF_END(KID_DIFFUSE_FS);
         n++;
     }
     int nblocks = (int)(g.blocks_per_rank * g.nranks);
+    PROF_BEGIN(KID_LIST_FLAGS);
+    k_list_flags<<<(int)((g.nwords + LIST_NT - 1) / LIST_NT), LIST_NT, 0, st>>>(a);
+    PROF_END(KID_LIST_FLAGS);
     PROF_BEGIN(KID_LIST_COUNT);
     k_list_count<<<nblocks, LIST_NT, 0, st>>>(a);
     PROF_END(KID_LIST_COUNT);
@@ -981,15 +1301,15 @@ static int launch_step_t(const KernelArgs &a, cudaStream_t st, int start_stage, 
     PROF_BEGIN(KID_APPLY);
     k_apply<<<148 * 4, 256, 0, st>>>(a);
     PROF_END(KID_APPLY);
-    n += 5;
+    n += 6;
     return n;
 }
 
-int launch_step(const KernelArgs &a, int precision, void *stream, int start_stage, Profiler *prof)
+int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream, int start_stage, Profiler *prof)
 {
     cudaStream_t st = (cudaStream_t)stream;
-    if (precision == MMS_PREC_F32) return launch_step_t<float>(a, st, start_stage, prof);
-    return launch_step_t<double>(a, st, start_stage, prof);
+    if (precision == MMS_PREC_F32) return launch_step_t<float>(a, tma, st, start_stage, prof);
+    return launch_step_t<double>(a, tma, st, start_stage, prof);
 }
 
 int launch_temp_am(const KernelArgs &a, void *stream, Profiler *prof, double lsd, double lv, double lhs,

@@ -85,6 +85,7 @@ struct EventProfiler : mms::Profiler {
 
 struct mms_ctx {
     mms_params p{};
+    TmaHolder tma{};
     cudaStream_t own_stream = nullptr;
     EventProfiler *prof = nullptr;
     std::vector<mms_fixed_nuc> fixed;
@@ -150,7 +151,14 @@ void dfree(mms_ctx *ctx, void *p)
     ctx->allocs.erase(std::remove(ctx->allocs.begin(), ctx->allocs.end(), p), ctx->allocs.end());
 }
 
-long long cidx(const Geo &g, long long i, long long j, long long k) { return k * g.sz + j * g.sy + i; }
+// device-layout and reference-layout linear indices (see Geo)
+long long cidx(const Geo &g, long long i, long long j, long long k) { return dev_index(g, i, j, k); }
+long long rcidx(const Geo &g, long long i, long long j, long long k) { return ref_index(g, i, j, k); }
+
+// Pitched copies between the device layout and a caller's buffer in the
+// reference layout (rows of gx+2 elements of es bytes).
+cudaError_t copy_out(mms_ctx *ctx, void *host, const void *dev, size_t es);
+cudaError_t copy_in(mms_ctx *ctx, void *dev, const void *host, size_t es);
 
 // Extract the sparse site list in (rank, local raster) order.
 void extract_sites(mms_ctx *ctx, const std::vector<float> &thr)
@@ -166,10 +174,11 @@ void extract_sites(mms_ctx *ctx, const std::vector<float> &thr)
         for (long long z = 1; z <= p.gsdimz; z++)
             for (long long y = 1; y <= p.gsdimy; y++)
                 for (long long x = 1; x <= p.gsdimx; x++) {
-                    long long c = cidx(g, (long long)r.sbx * p.gsdimx + x, (long long)r.sby * p.gsdimy + y,
-                                       (long long)r.sbz * p.gsdimz + z);
+                    long long I = (long long)r.sbx * p.gsdimx + x, J = (long long)r.sby * p.gsdimy + y,
+                              K = (long long)r.sbz * p.gsdimz + z;
+                    long long c = rcidx(g, I, J, K);
                     if (thr[c] != INFINITY) {
-                        ctx->site_cell.push_back(c);
+                        ctx->site_cell.push_back(cidx(g, I, J, K));
                         ctx->site_thr.push_back(thr[c]);
                         ctx->site_rank.push_back(ri);
                     }
@@ -185,16 +194,22 @@ mms_status upload_sites(mms_ctx *ctx)
     dfree(ctx, d.site_rank);
     dfree(ctx, d.site_flag);
     dfree(ctx, d.cand);
+    dfree(ctx, d.cand_stage);
+    dfree(ctx, d.nuc_blk_cnt);
     d.site_cell = nullptr;
     d.site_thr = nullptr;
     d.site_rank = nullptr;
     d.site_flag = nullptr;
     d.cand = nullptr;
+    d.cand_stage = nullptr;
+    d.nuc_blk_cnt = nullptr;
     size_t n = ctx->site_cell.size();
     d.nsites = (long long)n;
+    d.nuc_blocks = (int)std::max<size_t>(1, (n + 255) / 256);
     mms_status st;
     if ((st = dalloc(ctx, &d.site_cell, n)) || (st = dalloc(ctx, &d.site_thr, n)) ||
-        (st = dalloc(ctx, &d.site_rank, n)) || (st = dalloc(ctx, &d.site_flag, n)) || (st = dalloc(ctx, &d.cand, n)))
+        (st = dalloc(ctx, &d.site_rank, n)) || (st = dalloc(ctx, &d.site_flag, n)) || (st = dalloc(ctx, &d.cand, n)) ||
+        (st = dalloc(ctx, &d.cand_stage, (size_t)d.nuc_blocks * 256)) || (st = dalloc(ctx, &d.nuc_blk_cnt, d.nuc_blocks)))
         return st;
     if (n) {
         CU(cudaMemcpyAsync(d.site_cell, ctx->site_cell.data(), n * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
@@ -305,7 +320,7 @@ int launch_one_step(mms_ctx *ctx, int start_stage)
         n += launch_temp_am(ctx->ka, ctx->stream, ctx->prof, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
                             p.rho * p.lcp, p.x0, p.y0, p.z0, p.amtracks, p.gnsbx * p.gsdimx);
     }
-    n += launch_step(ctx->ka, ctx->prec, ctx->stream, start_stage, ctx->prof);
+    n += launch_step(ctx->ka, ctx->tma, ctx->prec, ctx->stream, start_stage, ctx->prof);
     return n;
 }
 
@@ -365,6 +380,24 @@ mms_status sync_grains(mms_ctx *ctx)
     }
     ctx->grains_synced = ng;
     return MMS_OK;
+}
+
+cudaError_t copy_out(mms_ctx *ctx, void *host, const void *dev, size_t es)
+{
+    const Geo &g = ctx->ka.g;
+    cudaError_t e = cudaMemcpy2DAsync(host, (size_t)g.rsy * es, dev, (size_t)g.P * es, (size_t)g.rsy * es,
+                                      (size_t)(g.gy + 2) * (g.gz + 2), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(ctx->stream);
+}
+
+cudaError_t copy_in(mms_ctx *ctx, void *dev, const void *host, size_t es)
+{
+    const Geo &g = ctx->ka.g;
+    cudaError_t e = cudaMemcpy2DAsync(dev, (size_t)g.P * es, host, (size_t)g.rsy * es, (size_t)g.rsy * es,
+                                      (size_t)(g.gy + 2) * (g.gz + 2), cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(ctx->stream);
 }
 
 }  // namespace
@@ -442,7 +475,8 @@ mms_status mms_kernel_stats(mms_ctx *ctx, int id, double *total_ms, uint64_t *la
     return MMS_OK;
 }
 uint64_t mms_kernel_launches(const mms_ctx *ctx) { return ctx ? ctx->launches : 0; }
-size_t mms_num_cells(const mms_ctx *ctx) { return ctx ? (size_t)ctx->ka.g.N : 0; }
+size_t mms_num_cells(const mms_ctx *ctx) { return ctx ? (size_t)ctx->ka.g.rN : 0; }
+int mms_uses_tma(const mms_ctx *ctx) { return ctx ? ctx->tma.ok : 0; }
 
 mms_status mms_create(const mms_params *pin, mms_ctx **out)
 {
@@ -485,26 +519,8 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
     ctx->stream = ctx->own_stream;
     cudaMallocHost((void **)&ctx->h_ctl, sizeof(Ctl));
 
+    ctx->ka.g = make_geo(p);
     Geo &g = ctx->ka.g;
-    g.gx = p.gnsbx * p.gsdimx;
-    g.gy = p.gnsby * p.gsdimy;
-    g.gz = p.gnsbz * p.gsdimz;
-    g.sy = g.gx + 2;
-    g.sz = (long long)(g.gx + 2) * (g.gy + 2);
-    g.N = g.sz * (g.gz + 2);
-    g.sbx = p.gsdimx;
-    g.sby = p.gsdimy;
-    g.sbz = p.gsdimz;
-    g.nsbx = p.gnsbx;
-    g.nsby = p.gnsby;
-    g.nsbz = p.gnsbz;
-    g.nranks = p.gnsbx * p.gnsby * p.gnsbz;
-    g.sbcells = (long long)p.gsdimx * p.gsdimy * p.gsdimz;
-    g.padx = p.padBndyX;
-    g.pady = p.padBndyY;
-    g.padz = p.padBndyZ;
-    g.vb = 2048;
-    g.blocks_per_rank = (g.sbcells + g.vb - 1) / g.vb;
 
     Phys &ph = ctx->ka.p;
     ph.rs = p.Dsol * dtx;
@@ -558,7 +574,8 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         if ((st = dalloc(ctx, &tmp, N * rs))) return fail(st);
         d.fs[b] = tmp;
     }
-    if ((st = dalloc(ctx, &d.gr, N)) || (st = dalloc(ctx, &d.dc, N)) || (st = dalloc(ctx, &d.ctl, 1)))
+    if ((st = dalloc(ctx, &d.gr, N)) || (st = dalloc(ctx, &d.dc, N)) || (st = dalloc(ctx, &d.ctl, 1)) ||
+        (st = dalloc(ctx, &d.solid_bits, (size_t)g.nwords)) || (st = dalloc(ctx, &d.flag_bits, (size_t)g.nwords)))
         return fail(st);
     if (p.am) {
         if ((st = dalloc(ctx, &d.T, N))) return fail(st);
@@ -599,16 +616,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         rk.seed_with((unsigned)r + 1 + p.base_random_seed);
     }
     // initial fields: ce = cl = Cinit everywhere, fs = gr = dc = 0 (setup.c:59-79)
-    std::vector<signed char> mold(N, 0);
-    for (long long K = 0; K < g.gz + 2; K++)
-        for (long long J = 0; J < g.gy + 2; J++)
-            for (long long I = 0; I < g.gx + 2; I++) {
-                int m = 0;
-                if (p.padBndyX && (I == 0 || I == g.gx + 1)) m = 1;
-                if (p.padBndyY && (J == 0 || J == g.gy + 1)) m = 1;
-                if (p.padBndyZ && (K == 0 || K == g.gz + 1)) m = 1;
-                mold[cidx(g, I, J, K)] = (signed char)m;
-            }
+    std::vector<signed char> mold = make_mold(g);  // reference layout
     {
         std::vector<double> init(N, p.Cinit);
         double *dtmp;
@@ -625,10 +633,11 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         ctx->launches += launch_temp_am(ctx->ka, ctx->stream, nullptr, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
                                         p.rho * p.lcp, p.x0, p.y0, p.z0, p.amtracks, p.gnsbx * p.gsdimx);
     }
-    std::vector<float> thr(N, INFINITY);
+    std::vector<float> thr((size_t)g.rN, INFINITY);  // reference layout
     setup_sites(ctx->p, ctx->ka.g, ctx->fixed, ctx->vols, ctx->ranks, thr, mold);
     extract_sites(ctx, thr);
     if ((st = upload_sites(ctx)) || (st = upload_nucpt(ctx))) return fail(st);
+    make_tma(ctx->ka, ctx->prec, ctx->tma);
     // orientation tables
     if (p.gnUseOrientation) {
         long long maxsites = 0;
@@ -673,11 +682,11 @@ mms_status mms_set_sites(mms_ctx *ctx, int64_t n, const int32_t *gxyz, const flo
     if (ctx->stepped) return MMS_ERR_STATE;
     cudaSetDevice(ctx->device);
     const Geo &g = ctx->ka.g;
-    std::vector<float> thr((size_t)g.N, INFINITY);
+    std::vector<float> thr((size_t)g.rN, INFINITY);
     for (int64_t s = 0; s < n; s++) {
         long long x = gxyz[3 * s], y = gxyz[3 * s + 1], z = gxyz[3 * s + 2];
         if (x < 0 || y < 0 || z < 0 || x >= g.gx || y >= g.gy || z >= g.gz) return MMS_ERR_ARG;
-        thr[cidx(g, x + 1, y + 1, z + 1)] = thresholds[s];
+        thr[rcidx(g, x + 1, y + 1, z + 1)] = thresholds[s];
     }
     // rewind every stream to where init_sb_nucleation would start drawing
     for (Rank &r : ctx->ranks) {
@@ -799,7 +808,7 @@ mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
     if (!ctx || !host) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     const Geo &g = ctx->ka.g;
-    const size_t N = (size_t)g.N;
+    const size_t N = (size_t)g.N;  // device layout
     mms_status st = read_ctl(ctx);
     if (st) return st;
     const int cur = (int)(ctx->h_ctl->timestep & 1ULL);
@@ -810,32 +819,30 @@ mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
     case MMS_FIELD_FS: {
         if (ctx->prec == MMS_PREC_F64) {
             const void *src = field == MMS_FIELD_CE ? d.ce : (field == MMS_FIELD_CL ? d.cl[cur] : d.fs[cur]);
-            CU(cudaMemcpy(host, src, N * sizeof(double), cudaMemcpyDeviceToHost));
+            CU(copy_out(ctx, host, src, sizeof(double)));
         } else {
             double *tmp;
             if ((st = dalloc(ctx, &tmp, N))) return st;
             ctx->launches += launch_convert(ctx->ka, ctx->prec, field, 0, tmp, ctx->stream);
-            CU(cudaMemcpyAsync(host, tmp, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-            CU(cudaStreamSynchronize(ctx->stream));
+            CU(copy_out(ctx, host, tmp, sizeof(double)));
             dfree(ctx, tmp);
         }
         return MMS_OK;
     }
     case MMS_FIELD_GR:
-        CU(cudaMemcpy(host, d.gr, N * sizeof(int), cudaMemcpyDeviceToHost));
+        CU(copy_out(ctx, host, d.gr, sizeof(int)));
         return MMS_OK;
     case MMS_FIELD_OGR: {
         int *tmp;
         if ((st = dalloc(ctx, &tmp, N))) return st;
         CU(cudaMemcpyAsync(tmp, d.gr, N * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
         ctx->launches += launch_mask_captured(ctx->ka, tmp, 0, ctx->stream);
-        CU(cudaMemcpyAsync(host, tmp, N * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaStreamSynchronize(ctx->stream));
+        CU(copy_out(ctx, host, tmp, sizeof(int)));
         dfree(ctx, tmp);
         return MMS_OK;
     }
     case MMS_FIELD_DC:
-        CU(cudaMemcpy(host, d.dc, N * sizeof(Dc3), cudaMemcpyDeviceToHost));
+        CU(copy_out(ctx, host, d.dc, sizeof(Dc3)));
         return MMS_OK;
     case MMS_FIELD_D:
     case MMS_FIELD_TEMPERATURE: {
@@ -847,28 +854,19 @@ mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
         } else {
             ctx->launches += launch_fill_temperature(ctx->ka, tmp, ctx->stream);
         }
-        CU(cudaMemcpyAsync(host, tmp, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaStreamSynchronize(ctx->stream));
+        CU(copy_out(ctx, host, tmp, sizeof(double)));
         dfree(ctx, tmp);
         return MMS_OK;
     }
     case MMS_FIELD_NUC_THRESHOLD: {
         float *t = (float *)host;
-        for (size_t c = 0; c < N; c++) t[c] = INFINITY;
-        for (size_t s = 0; s < ctx->site_cell.size(); s++) t[ctx->site_cell[s]] = ctx->site_thr[s];
+        for (long long c = 0; c < g.rN; c++) t[c] = INFINITY;
+        for (size_t s = 0; s < ctx->site_cell.size(); s++) t[dev_to_ref(g, ctx->site_cell[s])] = ctx->site_thr[s];
         return MMS_OK;
     }
     case MMS_FIELD_MOLD: {
-        signed char *m = (signed char *)host;
-        for (long long K = 0; K < g.gz + 2; K++)
-            for (long long J = 0; J < g.gy + 2; J++)
-                for (long long I = 0; I < g.gx + 2; I++) {
-                    int v = 0;
-                    if (g.padx && (I == 0 || I == g.gx + 1)) v = 1;
-                    if (g.pady && (J == 0 || J == g.gy + 1)) v = 1;
-                    if (g.padz && (K == 0 || K == g.gz + 1)) v = 1;
-                    m[cidx(g, I, J, K)] = (signed char)v;
-                }
+        std::vector<signed char> m = make_mold(g);
+        std::memcpy(host, m.data(), m.size());
         return MMS_OK;
     }
     }
@@ -889,20 +887,20 @@ mms_status mms_upload(mms_ctx *ctx, mms_field field, const void *host)
     case MMS_FIELD_FS: {
         double *tmp;
         if ((st = dalloc(ctx, &tmp, N))) return st;
-        CU(cudaMemcpyAsync(tmp, host, N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CU(copy_in(ctx, tmp, host, sizeof(double)));
         ctx->launches += launch_convert(ctx->ka, ctx->prec, field, 1, tmp, ctx->stream);
         CU(cudaStreamSynchronize(ctx->stream));
         dfree(ctx, tmp);
         return MMS_OK;
     }
     case MMS_FIELD_GR:
-        CU(cudaMemcpy(d.gr, host, N * sizeof(int), cudaMemcpyHostToDevice));
+        CU(copy_in(ctx, d.gr, host, sizeof(int)));
         return MMS_OK;
     case MMS_FIELD_DC:
-        CU(cudaMemcpy(d.dc, host, N * sizeof(Dc3), cudaMemcpyHostToDevice));
+        CU(copy_in(ctx, d.dc, host, sizeof(Dc3)));
         return MMS_OK;
     case MMS_FIELD_NUC_THRESHOLD: {
-        std::vector<float> thr((const float *)host, (const float *)host + N);
+        std::vector<float> thr((const float *)host, (const float *)host + g.rN);
         extract_sites(ctx, thr);
         return upload_sites(ctx);
     }
@@ -950,13 +948,13 @@ mms_status mms_output_grains(mms_ctx *ctx, const char *path, mms_grain_summary *
     const Geo &g = ctx->ka.g;
     const mms_params &p = ctx->p;
     int ng = ctx->h_ctl->num_grains;
-    std::vector<int> gr((size_t)g.N);
-    CU(cudaMemcpy(gr.data(), ctx->ka.d.gr, sizeof(int) * g.N, cudaMemcpyDeviceToHost));
+    std::vector<int> gr((size_t)g.rN);
+    CU(copy_out(ctx, gr.data(), ctx->ka.d.gr, sizeof(int)));
     std::vector<size_t> sizes((size_t)ng + 1, 0);
     for (long long k = 1; k <= g.gz; k++)
         for (long long j = 1; j <= g.gy; j++)
             for (long long i = 1; i <= g.gx; i++) {
-                int v = gr[cidx(g, i, j, k)];
+                int v = gr[rcidx(g, i, j, k)];
                 if (v > 0 && v <= ng) sizes[v]++;
             }
     size_t minSize = sizes[1], maxSize = sizes[1], avgSize = 0, zeroCount = 0;

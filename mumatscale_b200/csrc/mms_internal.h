@@ -51,17 +51,45 @@ struct GrainLog {
 };
 
 // Geometry and physics constants passed to every kernel by value.
+// Two layouts of the same halo'd grid: the reference's (row length gx+2,
+// used by every host buffer crossing the ABI) and the device's, whose rows
+// are padded to a multiple of 8 elements so that every row starts 64-byte
+// aligned (TMA needs 16-byte strides).  Padding columns are never read.
 struct Geo {
     int gx, gy, gz;            // interior cells
-    long long sy, sz, N;       // halo'd strides and size
+    long long P;               // device row pitch in elements (>= gx+2)
+    long long sy, sz, N;       // device strides and size (sy = P)
+    long long rsy, rsz, rN;    // reference layout strides and size (rsy = gx+2)
     int sbx, sby, sbz;         // NCellsPerSB
     int nsbx, nsby, nsbz;      // NSubblocks
     int nranks;
     long long sbcells;         // cells per subblock
     int padx, pady, padz;      // pad (mold) faces
-    int vb;                    // cells per list block (scan granularity)
-    long long blocks_per_rank; // ceil(sbcells / vb)
+    // bitmasks: one bit per interior cell, rows of wpr 32-bit words,
+    // bit b of word w in row (j,k) = cell i = 1 + 32 w + b
+    int wpr;
+    long long nwords;          // wpr * (gy+2) * (gz+2)
+    // interface-list pieces: 32 consecutive cells of one emulated rank's
+    // local row; blocks of LIST_PIECES pieces in rank-local raster order
+    int ppr;                   // pieces per local row = ceil(sbx / 32)
+    long long pieces_per_rank; // sby * sbz * ppr
+    long long blocks_per_rank; // ceil(pieces_per_rank / LIST_PIECES)
 };
+
+constexpr int LIST_PIECES = 1024;
+
+inline long long dev_index(const Geo &g, long long i, long long j, long long k) { return k * g.sz + j * g.sy + i; }
+inline long long ref_index(const Geo &g, long long i, long long j, long long k) { return k * g.rsz + j * g.rsy + i; }
+inline long long ref_to_dev(const Geo &g, long long c)
+{
+    long long k = c / g.rsz, j = (c % g.rsz) / g.rsy, i = c % g.rsy;
+    return dev_index(g, i, j, k);
+}
+inline long long dev_to_ref(const Geo &g, long long c)
+{
+    long long k = c / g.sz, j = (c % g.sz) / g.sy, i = c % g.sy;
+    return ref_index(g, i, j, k);
+}
 
 struct Phys {
     // diffusion (growth.c:38-40)
@@ -99,6 +127,8 @@ struct DevPtrs {
     void *fs[2];
     int *gr;
     Dc3 *dc;
+    unsigned *solid_bits;  // gr > 0 after fs_change (written by the stencil)
+    unsigned *flag_bits;   // interface-list membership (grow_cell_reduction)
     double *T;            // AM temperature at the current step (N) or null
     int *lsindex;         // AM layer flag or null
     double *curv;         // curvature (N) when TipCurvature
@@ -109,6 +139,9 @@ struct DevPtrs {
     int *site_rank;
     unsigned char *site_flag;
     int *cand;            // ordered candidate sites of the current step
+    int *cand_stage;      // per nucleation block, its candidates in site order
+    int *nuc_blk_cnt;     // candidates per nucleation block
+    int nuc_blocks;
     // orientation sources
     long long n_nucpt;
     long long *nucpt_key;   // sorted global cell keys (first entry wins)
@@ -149,8 +182,14 @@ struct KernelArgs {
 
 // Kernel ids for per-kernel timing.
 enum KernelId : int {
-    KID_TEMP_AM = 0, KID_NUC, KID_ACT, KID_CURV, KID_DIFFUSE_FS, KID_LIST_COUNT, KID_LIST_SCAN,
-    KID_LIST_ZERO, KID_CAPTURE, KID_APPLY, KID_COUNT
+    KID_TEMP_AM = 0, KID_NUC, KID_ACT, KID_CURV, KID_DIFFUSE_FS, KID_LIST_FLAGS, KID_LIST_COUNT,
+    KID_LIST_SCAN, KID_LIST_ZERO, KID_CAPTURE, KID_APPLY, KID_COUNT
+};
+
+// Opaque storage for the stencil's TMA descriptors (built in kernels.cu).
+struct TmaHolder {
+    alignas(128) unsigned char bytes[6 * 128];
+    int ok;
 };
 
 // Optional event bracketing of each launch (mms_set_profiling).
@@ -163,7 +202,12 @@ struct Profiler {
 // Launchers implemented in kernels.cu.  Each returns the number of kernels
 // it launched.
 // start_stage 0: whole step; 1: resume at grain activation (after a stall).
-int launch_step(const KernelArgs &a, int precision, void *stream, int start_stage, Profiler *prof);
+int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream, int start_stage,
+                Profiler *prof);
+// Builds the TMA descriptors of the stencil for the current buffers;
+// returns 0 when the driver cannot encode them (the stencil then uses its
+// plain-load variant).
+int make_tma(const KernelArgs &a, int precision, TmaHolder &out);
 int launch_temp_am(const KernelArgs &a, void *stream, Profiler *prof, double lsd, double lv, double lhs, double lab,
                    double lpow, double liniT, double lthcon, double rho_cp, double x0, double y0,
                    double z0, int amtracks, int nsbx_times_sbx);

@@ -44,6 +44,7 @@ def test_fp64_bit_exact_vs_reference(built, cuda_device, name):
                 dom.step(rec["error_at_step"] - last)
             assert e.value.status == 6  # MMS_ERR_GRAIN_OVERFLOW
         assert dom.kernel_launches > 0
+        assert dom.uses_tma, "the stencil fell back to its plain-load variant"
 
 
 def test_am_tolerance(built, cuda_device):
