@@ -539,8 +539,17 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
     }
     cen = oce + nbsum;
     const Real Tcell = (Real)Td;
-    Real c_int = q.cinit + q.m_inv * (Tcell - q.Tliq);
-    Real Tunder = q.Tliq - Tcell;
+    Real c_int, Tunder;
+    if (sizeof(Real) == 8) {
+        c_int = q.cinit + q.m_inv * (Tcell - q.Tliq);
+        Tunder = q.Tliq - Tcell;
+    } else {
+        // FP32 form: the undercooling is taken in FP64 before rounding (T is
+        // ~1e3 K, the undercooling ~1 K)
+        const Real dT = (Real)(Td - p.Tliq);
+        c_int = q.cinit + q.m_inv * dT;
+        Tunder = -dT;
+    }
     Tunder += q.liq_slope * (conc - q.cinit);
     gr_new = grc;
     if (grc <= 0 || Td < 1.0 || Td > p.Tliq) {
@@ -553,9 +562,13 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
     } else {
         if (p.tip_curv) {
             const Real cv = (Real)curv[c];
-            c_int = q.cinit + q.m_inv * (Tcell - q.Tliq + q.gibbs * cv);
+            if (sizeof(Real) == 8) c_int = q.cinit + q.m_inv * (Tcell - q.Tliq + q.gibbs * cv);
+            else c_int = q.cinit + q.m_inv * ((Real)(Td - p.Tliq) + q.gibbs * cv);
         }
-        Real dce = cen - oce;
+        // FP64: dce = ce_new - oce exactly as the reference (growth.c:254);
+        // FP32 form: the diffusion increment itself, which the difference of
+        // two rounded ~5 wt% values would lose to cancellation
+        Real dce = (sizeof(Real) == 8) ? cen - oce : nbsum;
         Real dcl = (c_int - conc) * q.D_xt * 2 + dce / (1 - q.km * lspfs);
         Real dfs = (dcl * ((Real)1. - q.km * lspfs) - dce) * q.km_inv / conc;
         cl_new = conc + dcl;

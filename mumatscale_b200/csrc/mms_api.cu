@@ -453,9 +453,9 @@ int mms_kernel_count(void) { return mms::KID_COUNT; }
 
 const char *mms_kernel_name(int id)
 {
-    static const char *names[mms::KID_COUNT] = {"k_temp_am", "k_nuc", "k_act", "k_curv", "k_diffuse_fs",
-                                                "k_list_count", "k_list_scan", "k_list_zero", "k_capture",
-                                                "k_apply"};
+    static const char *names[mms::KID_COUNT] = {"k_temp_am",    "k_nuc",        "k_act",       "k_curv",
+                                                "k_diffuse_fs", "k_list_flags", "k_list_count", "k_list_scan",
+                                                "k_list_zero",  "k_capture",    "k_apply"};
     return (id >= 0 && id < mms::KID_COUNT) ? names[id] : "";
 }
 
