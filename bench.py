@@ -383,6 +383,22 @@ def gpu_arm(args) -> None:
         dist.destroy_process_group()
 
 
+def profile_arm(args) -> None:
+    """Workload for ncu captures: the same deck, one form, W + K steps, no
+    timing, no CPU baseline.  Usage:
+        ncu ... python bench.py --profile f64 --warmup 3 --steps 2"""
+    import mumatscale_b200 as M
+    td = tempfile.mkdtemp()
+    deck = Path(td) / "bench.in"
+    deck.write_text(deck_text(n=args.cells))
+    params = M.read_deck(deck)
+    dom = M.Domain(params, precision=M.PREC_F32 if args.profile == "f32" else M.PREC_F64)
+    dom.step(args.warmup + args.steps)
+    print(json.dumps({"profile": args.profile, "cells": args.cells ** 3, "steps": args.warmup + args.steps,
+                      "grains": dom.num_grains, "tma": dom.uses_tma}))
+    dom.close()
+
+
 def reference_arm(args) -> None:
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -412,10 +428,15 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", choices=["f64", "f32"], default=None,
+                    help="run the workload for an ncu capture only")
+    ap.add_argument("--cells", type=int, default=N_CELL, help="edge of the cubic domain (profile mode)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile:
+        profile_arm(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         gpu_arm(args)

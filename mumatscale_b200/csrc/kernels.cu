@@ -251,7 +251,8 @@ __global__ void __launch_bounds__(NUC_NT) k_nuc(KernelArgs a)
             if (layerno && initnuc) {
                 double Tunder = p.Tliq - Ttemp;
                 double m = p.ma * Ttemp * Ttemp + p.mb * Ttemp + p.mc;
-                Tunder += m * ((double)cl[c] - p.cinit);
+                // the FP32 form stores cl - Cinit
+                Tunder += m * ((sizeof(Real) == 8) ? ((double)cl[c] - p.cinit) : (double)cl[c]);
                 if (Tunder > (double)a.d.site_thr[s]) hit = 1;
             }
         }
@@ -500,7 +501,7 @@ __global__ void k_curv(KernelArgs a)
 // and fs come from the previous step's buffer.
 template <typename Real>
 struct PhysR {
-    Real rs, rl, liq_slope, k_inv, km, km_inv, m_inv, D_xt, cinit, Tliq, gibbs;
+    Real rs, rl, liq_slope, k_inv, km, km_inv, m_inv, D_xt, cinit, Tliq, gibbs, c0k;
 };
 
 template <typename Real>
@@ -518,11 +519,19 @@ __device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
     q.cinit = (Real)p.cinit;
     q.Tliq = (Real)p.Tliq;
     q.gibbs = (Real)p.gibbs;
+    q.c0k = (Real)(p.cinit * (p.k_inv - 1.0));
     return q;
 }
 
 // nb_* in the order +x, -x, +y, -y, +z, -z (growth.c:85-113); one_m[n] is
 // (1 - mold) of that neighbour.
+//
+// FP32 form: ce and cl are stored as deviations from Cinit (conc, nb_cl,
+// oce, and the results likewise), so that the liquid, where they stay close
+// to Cinit, keeps ~1e-10 wt% absolute resolution instead of float's 5e-7;
+// the undercooling T - Tliq is formed in FP64 before rounding, and the
+// solute increment dce is the diffusion sum itself rather than the
+// difference of two rounded ce values.
 template <typename Real>
 __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p, Real conc, Real lspfs,
                                             const Real (&nb_cl)[6], const Real (&nb_fs)[6],
@@ -538,46 +547,58 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
         nbsum += r * (nb_cl[n] - conc);
     }
     cen = oce + nbsum;
-    const Real Tcell = (Real)Td;
-    Real c_int, Tunder;
-    if (sizeof(Real) == 8) {
-        c_int = q.cinit + q.m_inv * (Tcell - q.Tliq);
-        Tunder = q.Tliq - Tcell;
-    } else {
-        // FP32 form: the undercooling is taken in FP64 before rounding (T is
-        // ~1e3 K, the undercooling ~1 K)
-        const Real dT = (Real)(Td - p.Tliq);
-        c_int = q.cinit + q.m_inv * dT;
-        Tunder = -dT;
-    }
-    Tunder += q.liq_slope * (conc - q.cinit);
     gr_new = grc;
-    if (grc <= 0 || Td < 1.0 || Td > p.Tliq) {
-        cl_new = cen;
-        fs_new = 0;
-        gr_new = 0;
-    } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
-        cl_new = cen * q.k_inv;
-        fs_new = lspfs;
-    } else {
-        if (p.tip_curv) {
-            const Real cv = (Real)curv[c];
-            if (sizeof(Real) == 8) c_int = q.cinit + q.m_inv * (Tcell - q.Tliq + q.gibbs * cv);
-            else c_int = q.cinit + q.m_inv * ((Real)(Td - p.Tliq) + q.gibbs * cv);
-        }
-        // FP64: dce = ce_new - oce exactly as the reference (growth.c:254);
-        // FP32 form: the diffusion increment itself, which the difference of
-        // two rounded ~5 wt% values would lose to cancellation
-        Real dce = (sizeof(Real) == 8) ? cen - oce : nbsum;
-        Real dcl = (c_int - conc) * q.D_xt * 2 + dce / (1 - q.km * lspfs);
-        Real dfs = (dcl * ((Real)1. - q.km * lspfs) - dce) * q.km_inv / conc;
-        cl_new = conc + dcl;
-        fs_new = lspfs + dfs;
-        fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
-        if (fs_new < (Real)0.) {
-            fs_new = 0.;
-            gr_new = 0;
+    if (sizeof(Real) == 8) {
+        // fs_change_diffuse, growth.c:220-272, operation for operation
+        const Real Tcell = (Real)Td;
+        Real c_int = q.cinit + q.m_inv * (Tcell - q.Tliq);
+        Real Tunder = q.Tliq - Tcell;
+        Tunder += q.liq_slope * (conc - q.cinit);
+        if (grc <= 0 || Td < 1.0 || Td > p.Tliq) {
             cl_new = cen;
+            fs_new = 0;
+            gr_new = 0;
+        } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
+            cl_new = cen * q.k_inv;
+            fs_new = lspfs;
+        } else {
+            if (p.tip_curv) c_int = q.cinit + q.m_inv * (Tcell - q.Tliq + q.gibbs * (Real)curv[c]);
+            Real dce = cen - oce;
+            Real dcl = (c_int - conc) * q.D_xt * 2 + dce / (1 - q.km * lspfs);
+            Real dfs = (dcl * ((Real)1. - q.km * lspfs) - dce) * q.km_inv / conc;
+            cl_new = conc + dcl;
+            fs_new = lspfs + dfs;
+            fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
+            if (fs_new < (Real)0.) {
+                fs_new = 0.;
+                gr_new = 0;
+                cl_new = cen;
+            }
+        }
+    } else {
+        const Real dT = (Real)(Td - p.Tliq);
+        Real c_int = q.m_inv * dT;               // c_int - Cinit
+        Real Tunder = -dT + q.liq_slope * conc;  // conc = cl - Cinit
+        if (grc <= 0 || Td < 1.0 || Td > p.Tliq) {
+            cl_new = cen;
+            fs_new = 0;
+            gr_new = 0;
+        } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
+            cl_new = cen * q.k_inv + q.c0k;      // ce / k - Cinit
+            fs_new = lspfs;
+        } else {
+            if (p.tip_curv) c_int = q.m_inv * (dT + q.gibbs * (Real)curv[c]);
+            const Real dce = nbsum;
+            Real dcl = (c_int - conc) * q.D_xt * 2 + dce / (1 - q.km * lspfs);
+            Real dfs = (dcl * ((Real)1. - q.km * lspfs) - dce) * q.km_inv / (conc + q.cinit);
+            cl_new = conc + dcl;
+            fs_new = lspfs + dfs;
+            fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
+            if (fs_new < (Real)0.) {
+                fs_new = 0.;
+                gr_new = 0;
+                cl_new = cen;
+            }
         }
     }
 }
@@ -588,7 +609,11 @@ constexpr int DTX = 32, DTY = 8;
 // z-chunk; planes of cl and fs with their x/y halo (and ce, gr without) are
 // brought into a TS-deep shared-memory ring by cp.async.bulk.tensor, one
 // mbarrier per slot, issued TS-1 planes ahead of the plane being updated.
-constexpr int TS = 5;
+// pipeline depth (planes in the ring): deeper for FP32, whose planes are smaller
+template <typename Real>
+struct Depth {
+    static constexpr int TS = sizeof(Real) == 8 ? 6 : 8;
+};
 constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 
 template <typename Real>
@@ -614,6 +639,7 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs_tma(const __grid_consta
                                                              const __grid_constant__ TmaMaps maps, int zchunk)
 {
     using L = Stage<Real>;
+    constexpr int TS = Depth<Real>::TS;
     Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -995,12 +1021,9 @@ __device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs,
     return gid;
 }
 
-// Writes this block's part of the ordered list, then captures its entries.
-// Results go to per-slot buffers; k_apply commits them after every capture
-// has read the pre-capture grain ids (the reference's ogr copy,
-// growth.c:635-638).
-template <typename Real>
-__global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
+// Writes this block's part of the ordered list (pieces in rank-local raster
+// order, positions from k_list_scan).
+__global__ void __launch_bounds__(LIST_NT) k_list_write(KernelArgs a)
 {
     const Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
@@ -1008,10 +1031,8 @@ __global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
     const Geo &g = a.g;
     const int r = (int)(blockIdx.x / g.blocks_per_rank);
     const long long q0 = (blockIdx.x % g.blocks_per_rank) * (long long)LIST_PIECES;
-    const int first = a.d.blk_off[blockIdx.x];
-    const int count = a.d.blk_cnt[blockIdx.x];
-    if (count == 0) return;
-    int pos = first;
+    if (a.d.blk_cnt[blockIdx.x] == 0) return;
+    int pos = a.d.blk_off[blockIdx.x];
     for (int it = 0; it < LIST_PIECES / LIST_NT; it++) {
         Piece pc = piece_of(a, r, q0 + it * LIST_NT + threadIdx.x);
         int tot;
@@ -1024,16 +1045,34 @@ __global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
             a.d.list_cell[p0++] = pc.base + bit;
         }
     }
-    __syncthreads();
-    const int pout = (int)(ctl->timestep & 1ULL);
-    const Real *fs = (const Real *)a.d.fs[pout];
-    const int rank_start = a.d.blk_off[(long long)r * g.blocks_per_rank];
-    const long long dcbase = a.d.rank_dcbase[r];
-    for (int e = first + threadIdx.x; e < first + count; e += LIST_NT) {
+}
+
+__device__ __forceinline__ int rank_of_dev_cell(const Geo &g, long long c)
+{
+    long long K = c / g.sz, J = (c % g.sz) / g.sy, I = c % g.sy;
+    int rx = (int)((I - 1) / g.sbx), ry = (int)((J - 1) / g.sby), rz = (int)((K - 1) / g.sbz);
+    return rx + ry * g.nsbx + rz * g.nsbx * g.nsby;
+}
+
+// Captures every list entry (grid-stride over the whole list, so the work
+// is balanced however the interface is distributed).  Results go to
+// per-slot buffers; k_apply commits them after every capture has read the
+// pre-capture grain ids (the reference's ogr copy, growth.c:635-638).
+template <typename Real>
+__global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const Geo &g = a.g;
+    const int total = ctl->list_total;
+    const Real *fs = (const Real *)a.d.fs[(int)(ctl->timestep & 1ULL)];
+    for (long long e = blockIdx.x * (long long)LIST_NT + threadIdx.x; e < total; e += (long long)gridDim.x * LIST_NT) {
         const long long c = a.d.list_cell[e];
+        const int r = (g.nranks == 1) ? 0 : rank_of_dev_cell(g, c);
+        const int rank_start = a.d.blk_off[(long long)r * g.blocks_per_rank];
         Dc3 out;
         const int gid = capture_cell<Real>(a, fs, c, out);
-        if (gid) a.d.dc_tmp[dcbase + (e - rank_start + 1)] = out;
+        if (gid) a.d.dc_tmp[a.d.rank_dcbase[r] + (e - rank_start + 1)] = out;
         a.d.list_gid[e] = gid;
     }
 }
@@ -1047,10 +1086,7 @@ __global__ void k_apply(KernelArgs a)
     for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < total;
          pos += (long long)gridDim.x * blockDim.x) {
         long long c = a.d.list_cell[pos];
-        // emulated rank of the cell
-        long long K = c / g.sz, J = (c % g.sz) / g.sy, I = c % g.sy;
-        int rx = (int)((I - 1) / g.sbx), ry = (int)((J - 1) / g.sby), rz = (int)((K - 1) / g.sbz);
-        int r = rx + ry * g.nsbx + rz * g.nsbx * g.nsby;
+        const int r = (g.nranks == 1) ? 0 : rank_of_dev_cell(g, c);
         int start = a.d.blk_off[(long long)r * g.blocks_per_rank];
         int slot = (int)pos - start + 1;
         a.d.dc[c] = a.d.dc_tmp[a.d.rank_dcbase[r] + slot];
@@ -1172,11 +1208,13 @@ __global__ void k_convert(KernelArgs a, int field, int to_device, double *buf)
     if (field == MMS_FIELD_CE) f = (Real *)a.d.ce;
     else if (field == MMS_FIELD_CL) f = (Real *)a.d.cl[cur], f2 = (Real *)a.d.cl[cur ^ 1];
     else f = (Real *)a.d.fs[cur], f2 = (Real *)a.d.fs[cur ^ 1];
+    // the FP32 form stores ce and cl as deviations from Cinit
+    const double off = (sizeof(Real) == 4 && field != MMS_FIELD_FS) ? a.p.cinit : 0.0;
     if (to_device) {
-        f[c] = (Real)buf[c];
-        if (f2) f2[c] = (Real)buf[c];
+        f[c] = (Real)(buf[c] - off);
+        if (f2) f2[c] = (Real)(buf[c] - off);
     } else {
-        buf[c] = (double)f[c];
+        buf[c] = (double)f[c] + off;
     }
 }
 
@@ -1243,7 +1281,8 @@ static int make_tma_t(const KernelArgs &a, TmaHolder &out)
     std::memcpy(out.bytes, &m, sizeof m);
     out.ok = ok ? 1 : 0;
     if (ok) {
-        cudaFuncSetAttribute(k_diffuse_fs_tma<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, TS * L::BYTES);
+        cudaFuncSetAttribute(k_diffuse_fs_tma<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             Depth<Real>::TS * L::BYTES);
     }
     return out.ok;
 }
@@ -1288,7 +1327,7 @@ static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t
         if (tma.ok) {
             TmaMaps maps;
             std::memcpy(&maps, tma.bytes, sizeof maps);
-            k_diffuse_fs_tma<Real><<<grid, dim3(DTX, DTY), TS * Stage<Real>::BYTES, st>>>(a, maps, zc);
+            k_diffuse_fs_tma<Real><<<grid, dim3(DTX, DTY), Depth<Real>::TS * Stage<Real>::BYTES, st>>>(a, maps, zc);
         } else {
             k_diffuse_fs<Real><<<grid, dim3(DTX, DTY), 0, st>>>(a, zc);
         }
@@ -1308,13 +1347,16 @@ static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t
     PROF_BEGIN(KID_LIST_ZERO);
     k_list_zero<<<dim3(64, g.nranks), 256, 0, st>>>(a);
     PROF_END(KID_LIST_ZERO);
+    PROF_BEGIN(KID_LIST_WRITE);
+    k_list_write<<<nblocks, LIST_NT, 0, st>>>(a);
+    PROF_END(KID_LIST_WRITE);
     PROF_BEGIN(KID_CAPTURE);
-    k_capture<Real><<<nblocks, LIST_NT, 0, st>>>(a);
+    k_capture<Real><<<148 * 8, LIST_NT, 0, st>>>(a);
     PROF_END(KID_CAPTURE);
     PROF_BEGIN(KID_APPLY);
     k_apply<<<148 * 4, 256, 0, st>>>(a);
     PROF_END(KID_APPLY);
-    n += 6;
+    n += 7;
     return n;
 }
 
@@ -1356,6 +1398,8 @@ int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out
         s = t;
     }
     *host_out = s + c;
+    if (precision == MMS_PREC_F32 && what == MMS_REDUCE_CE_SUM)  // deviations from Cinit were summed
+        *host_out += a.p.cinit * (double)((long long)a.g.gx * a.g.gy * a.g.gz);
     return 1;
 }
 

@@ -455,7 +455,7 @@ const char *mms_kernel_name(int id)
 {
     static const char *names[mms::KID_COUNT] = {"k_temp_am",    "k_nuc",        "k_act",       "k_curv",
                                                 "k_diffuse_fs", "k_list_flags", "k_list_count", "k_list_scan",
-                                                "k_list_zero",  "k_capture",    "k_apply"};
+                                                "k_list_zero",  "k_list_write", "k_capture",   "k_apply"};
     return (id >= 0 && id < mms::KID_COUNT) ? names[id] : "";
 }
 

@@ -183,7 +183,7 @@ struct KernelArgs {
 // Kernel ids for per-kernel timing.
 enum KernelId : int {
     KID_TEMP_AM = 0, KID_NUC, KID_ACT, KID_CURV, KID_DIFFUSE_FS, KID_LIST_FLAGS, KID_LIST_COUNT,
-    KID_LIST_SCAN, KID_LIST_ZERO, KID_CAPTURE, KID_APPLY, KID_COUNT
+    KID_LIST_SCAN, KID_LIST_ZERO, KID_LIST_WRITE, KID_CAPTURE, KID_APPLY, KID_COUNT
 };
 
 // Opaque storage for the stencil's TMA descriptors (built in kernels.cu).
