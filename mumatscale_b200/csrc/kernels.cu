@@ -14,11 +14,12 @@
 //   k_curv        Gibbs-Thomson curvature (curvature.c:31-405), TipCurvature only
 //   k_diffuse_fs  diffusion + fs change fused (growth.c:30-170, 177-276); also
 //                 writes the solid-cell bitmask (gr > 0 after fs change)
-//   k_list_flags  interface-list membership from the bitmask (growth.c:461-538)
-//   k_list_count  list length per block of rank-local raster pieces
+//   k_list_count  interface-list length per block of rank-local raster pieces,
+//                 membership from the bitmask (growth.c:461-538)
 //   k_list_scan   ordered block offsets, per-rank dc_tmp bookkeeping (growth.c:642-660)
-//   k_list_zero   clears dc_tmp regions that the reference re-allocates zeroed
-//   k_capture     ordered list write + octahedron capture (growth.c:339-407, 664-794)
+//   k_list_write  ordered list write; clears dc_tmp regions that the
+//                 reference re-allocates zeroed
+//   k_capture     octahedron capture over the list (growth.c:339-407, 664-794)
 //   k_apply       dc copy-back and captured grain ids (growth.c:789, 797-807)
 //
 // Fields: ce in place; cl and fs ping-pong between two buffers, the state
@@ -284,11 +285,14 @@ __device__ long long find_key(const long long *keys, long long n, long long key)
 
 // activateNewGrains + createGrains (grain.c:840-916, 347-425).  Candidates
 // are gathered in site order, which is (emulated rank, local raster) order,
-// so grain ids match the rank-ordered Allgatherv displacements
-// (grain.c:892-904).  More candidates than MaxTotGrains leaves room for is
-// the reference's createGrains error (grain.c:363-366): nindex2 replaces the
-// capped count (grain.c:1318), so the cap never holds.
-constexpr int ACT_NT = 256;
+// so candidate i gets grain id num_grains + i, as the rank-ordered
+// Allgatherv displacements give (grain.c:892-904); the k-th candidate of
+// rank r without a deck-defined orientation takes that rank's k-th
+// pre-drawn orientation.  More candidates than MaxTotGrains leaves room
+// for is the reference's createGrains error (grain.c:363-366): nindex2
+// replaces the capped count (grain.c:1318), so the cap never holds.
+// One CTA; every phase is parallel over candidates or ranks.
+constexpr int ACT_NT = 1024;
 __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
 {
     Ctl *ctl = a.d.ctl;
@@ -304,6 +308,13 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
         }
         return;
     }
+    const Phys &p = a.p;
+    const int nr = a.g.nranks;
+    int *need = rank_scratch;        // random draws per rank
+    int *first = rank_scratch + nr;  // first candidate of each rank
+    int *ex = a.d.cand_ex;           // per candidate: random draws before it
+    for (int r = threadIdx.x; r < nr; r += ACT_NT) need[r] = 0, first[r] = -1;
+    if (threadIdx.x == 0) s_abort = 0;
     // ordered gather of the per-block candidate lists
     int off = 0;
     for (int base = 0; base < a.d.nuc_blocks; base += ACT_NT) {
@@ -314,83 +325,91 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
         for (int i = 0; i < n; i++) a.d.cand[pos + i] = a.d.cand_stage[(long long)b * NUC_NT + i];
         off += tot;
     }
-    if (threadIdx.x == 0) s_abort = 0;
+    __syncthreads();
+    // orientation source per candidate, prefix count of random draws,
+    // per-rank first candidate and draw count
+    int run = 0;
+    for (int base = 0; base < C; base += ACT_NT) {
+        int i = base + threadIdx.x;
+        int rnd = 0, r = 0;
+        if (i < C) {
+            long long cell = a.d.site_cell[a.d.cand[i]];
+            r = a.d.site_rank[a.d.cand[i]];
+            rnd = (p.use_orientation && find_key(a.d.nucpt_key, a.d.n_nucpt, cell) < 0) ? 1 : 0;
+            if (i == 0 || a.d.site_rank[a.d.cand[i - 1]] != r) first[r] = i;
+            if (rnd) atomicAdd(&need[r], 1);
+        }
+        int tot;
+        int e = run + block_exclusive_scan<ACT_NT>(rnd, tot, sh);
+        if (i < C) ex[i] = e;
+        run += tot;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        const Phys &p = a.p;
-        const int nr = a.g.nranks;
-        int *cnt = rank_scratch;           // candidates per rank
-        int *need = rank_scratch + 2 * nr; // random draws needed per rank
-        int *start = rank_scratch + 3 * nr;
-        for (int r = 0; r < nr; r++) cnt[r] = 0, need[r] = 0, start[r] = -1;
-        for (int i = 0; i < C; i++) {
-            int r = a.d.site_rank[a.d.cand[i]];
-            if (start[r] < 0) start[r] = i;
-            cnt[r]++;
-        }
-        const long long num_grains = ctl->num_grains;
-        const unsigned long long maxg = p.max_grains;
-        if ((unsigned long long)(num_grains + C) > maxg + 1) {
+        if ((unsigned long long)(ctl->num_grains + (long long)C) > p.max_grains + 1) {
             ctl->status = MMS_ERR_GRAIN_OVERFLOW;
             atomicExch(&ctl->stall, (int)STALL_ERROR);
             s_abort = 1;
         }
-        // dry run: orientation draws needed per rank
-        bool short_rng = false;
-        for (int r = 0; r < nr && p.use_orientation && !s_abort; r++) {
-            for (int i = 0; i < cnt[r]; i++) {
-                long long cell = a.d.site_cell[a.d.cand[start[r] + i]];
-                if (find_key(a.d.nucpt_key, a.d.n_nucpt, cell) < 0) need[r]++;
-            }
-            if (a.d.rng_used[r] + need[r] > a.d.rng_cap) short_rng = true;
-        }
-        if (s_abort) {
-            // error raised above
-        } else if (short_rng) {
+    }
+    __syncthreads();
+    int short_rng = 0;
+    for (int r = threadIdx.x; r < nr && !s_abort; r += ACT_NT)
+        if (a.d.rng_used[r] + need[r] > a.d.rng_cap) short_rng = 1;
+    short_rng = __syncthreads_or(short_rng);
+    if (s_abort) return;
+    if (short_rng) {
+        // refill on the host, then this kernel runs again with the same
+        // candidates (nothing has been written yet)
+        if (threadIdx.x == 0) {
             ctl->stall_step = ts;
             atomicExch(&ctl->stall, (int)STALL_RNG);
-            s_abort = 1;
-        } else {
-            long long id = num_grains;
-            for (int r = 0; r < nr; r++) {
-                for (int i = 0; i < cnt[r]; i++, id++) {
-                    int s = a.d.cand[start[r] + i];
-                    long long cell = a.d.site_cell[s];
-                    a.d.gr[cell] = (int)id;
-                    GrainLog lg;
-                    lg.cell = cell;
-                    lg.timestep = ts;
-                    lg.rank = r;
-                    const double *rot;
-                    long long j = find_key(a.d.nucpt_key, a.d.n_nucpt, cell);
-                    if (j >= 0) {
-                        rot = a.d.nucpt_rot + 9 * j;
-                        lg.kind = 0;
-                        lg.aux = a.d.nucpt_entry[j];
-                    } else if (p.use_orientation) {
-                        int k = a.d.rng_used[r]++;
-                        rot = a.d.rng_rot + ((long long)r * a.d.rng_cap + k) * 9;
-                        lg.kind = 1;
-                        lg.aux = a.d.rng_base[r] + k;
-                    } else {
-                        rot = a.d.zero_rot;
-                        lg.kind = 2;
-                        lg.aux = 0;
-                    }
-                    if (a.d.n_inj > 0) {
-                        long long q = find_key(a.d.inj_key, a.d.n_inj, cell);
-                        if (q >= 0) rot = a.d.inj_rot + 9 * q;
-                    }
-                    double *dst = a.d.grain_rot + 9 * id;
-                    for (int e = 0; e < 9; e++) dst[e] = rot[e];
-                    a.d.grain_log[id] = lg;
-                }
-            }
-            ctl->num_grains = (int)(num_grains + C);
-            ctl->new_grains = C;
-            ctl->ncand = 0;
-            ctl->timestep = ts;
         }
+        return;
+    }
+    const long long num_grains = ctl->num_grains;
+    for (int i = threadIdx.x; i < C; i += ACT_NT) {
+        const int s = a.d.cand[i];
+        const long long cell = a.d.site_cell[s];
+        const int r = a.d.site_rank[s];
+        const long long id = num_grains + i;
+        a.d.gr[cell] = (int)id;
+        GrainLog lg;
+        lg.cell = cell;
+        lg.timestep = ts;
+        lg.rank = r;
+        const double *rot;
+        long long j = find_key(a.d.nucpt_key, a.d.n_nucpt, cell);
+        if (j >= 0) {
+            rot = a.d.nucpt_rot + 9 * j;
+            lg.kind = 0;
+            lg.aux = a.d.nucpt_entry[j];
+        } else if (p.use_orientation) {
+            // this rank's draws before candidate i
+            const int k = a.d.rng_used[r] + (ex[i] - ex[first[r]]);
+            rot = a.d.rng_rot + ((long long)r * a.d.rng_cap + k) * 9;
+            lg.kind = 1;
+            lg.aux = a.d.rng_base[r] + k;
+        } else {
+            rot = a.d.zero_rot;
+            lg.kind = 2;
+            lg.aux = 0;
+        }
+        if (a.d.n_inj > 0) {
+            long long q = find_key(a.d.inj_key, a.d.n_inj, cell);
+            if (q >= 0) rot = a.d.inj_rot + 9 * q;
+        }
+        double *dst = a.d.grain_rot + 9 * id;
+        for (int e = 0; e < 9; e++) dst[e] = rot[e];
+        a.d.grain_log[id] = lg;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nr; r += ACT_NT) a.d.rng_used[r] += need[r];
+    if (threadIdx.x == 0) {
+        ctl->num_grains = (int)(num_grains + C);
+        ctl->new_grains = C;
+        ctl->ncand = 0;
+        ctl->timestep = ts;
     }
 }
 
@@ -532,19 +551,30 @@ __device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
 // the undercooling T - Tliq is formed in FP64 before rounding, and the
 // solute increment dce is the diffusion sum itself rather than the
 // difference of two rounded ce values.
+// interior: no face of this cell touches the domain halo, so every (1 -
+// mold) factor is 1.0 and the multiplication by it (exact) is skipped.
 template <typename Real>
 __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p, Real conc, Real lspfs,
                                             const Real (&nb_cl)[6], const Real (&nb_fs)[6],
-                                            const Real (&one_m)[6], Real oce, int grc, double Td,
-                                            const double *curv, long long c, Real &cen, Real &cl_new,
-                                            Real &fs_new, int &gr_new)
+                                            const Real (&one_m)[6], bool interior, Real oce, int grc,
+                                            double Td, const double *curv, long long c, Real &cen,
+                                            Real &cl_new, Real &fs_new, int &gr_new)
 {
     Real nbsum = 0;
+    if (interior) {
 #pragma unroll
-    for (int n = 0; n < 6; n++) {
-        Real fs_av = (Real)0.5 * (lspfs + nb_fs[n]);
-        Real r = (q.rs * fs_av + q.rl * (1 - fs_av)) * one_m[n];
-        nbsum += r * (nb_cl[n] - conc);
+        for (int n = 0; n < 6; n++) {
+            Real fs_av = (Real)0.5 * (lspfs + nb_fs[n]);
+            Real r = (q.rs * fs_av + q.rl * (1 - fs_av));
+            nbsum += r * (nb_cl[n] - conc);
+        }
+    } else {
+#pragma unroll
+        for (int n = 0; n < 6; n++) {
+            Real fs_av = (Real)0.5 * (lspfs + nb_fs[n]);
+            Real r = (q.rs * fs_av + q.rl * (1 - fs_av)) * one_m[n];
+            nbsum += r * (nb_cl[n] - conc);
+        }
     }
     cen = oce + nbsum;
     gr_new = grc;
@@ -635,7 +665,7 @@ struct TmaMaps {
 };
 
 template <typename Real>
-__global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs_tma(const __grid_constant__ KernelArgs a,
+__global__ void __launch_bounds__(DTX *DTY, 4) k_diffuse_fs_tma(const __grid_constant__ KernelArgs a,
                                                              const __grid_constant__ TmaMaps maps, int zchunk)
 {
     using L = Stage<Real>;
@@ -675,10 +705,17 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs_tma(const __grid_consta
             tma_load_3d(stage(s) + 2 * L::CL + L::CE, &maps.gr, i0 - 1, j0, k, &bars[s]);
         }
     };
+    // temperature of each plane of the chunk when it depends on z only
+    // (direct_temp_calc's isothermal and gradient models in 3D)
+    __shared__ double sT[64];
+    __shared__ int s_abort;
+    const bool t_per_plane = (p.temp_mode == 0) || (p.temp_mode == 1 && !p.gz_is_one);
     if (tid == 0) {
         for (int s = 0; s < TS; s++) mbar_init(&bars[s], 1);
         fence_barrier_init();
+        s_abort = 0;
     }
+    if (t_per_plane && tid <= k1 - k0) sT[tid] = temp_cell(p, a.d.T, 0, 1, k0 + tid, ts);
     __syncthreads();
     if (tid == 0)
         for (int pl = 0; pl < TS && pl < nplanes; pl++) issue(pl);
@@ -688,20 +725,12 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs_tma(const __grid_consta
     const long long wrow = (long long)g.wpr;
     for (int t = 0; t <= k1 - k0; t++) {
         const int k = k0 + t;
-        bool ok = true;
-        for (int pl = t; pl <= t + 2; pl++) ok &= mbar_wait(&bars[pl % TS], (unsigned)((pl / TS) & 1));
-        if (__syncthreads_or(!ok)) {
-            // a copy did not land within the bound: report, then wait (again
-            // bounded) for every copy still in flight before leaving
-            if (tid == 0) {
-                raise_error(ctl, MMS_ERR_TIMEOUT);
-                for (int pl = t; pl < issued; pl++) mbar_wait(&bars[pl % TS], (unsigned)((pl / TS) & 1));
-            }
-            __syncthreads();
-            break;
-        }
+        // planes t and t+1 completed in earlier iterations
+        bool ok = mbar_wait(&bars[(t + 2) % TS], (unsigned)(((t + 2) / TS) & 1));
+        if (t == 0) ok &= mbar_wait(&bars[0], 0u) && mbar_wait(&bars[1 % TS], (unsigned)((1 / TS) & 1));
+        if (!ok) s_abort = 1;
         int solid = 0;
-        if (active) {
+        if (active && ok) {
             const Real *cm = (const Real *)stage(t % TS);
             const Real *cc = (const Real *)stage((t + 1) % TS);
             const Real *cp = (const Real *)stage((t + 2) % TS);
@@ -719,21 +748,32 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs_tma(const __grid_consta
             const long long c = (long long)k * g.sz + (long long)j * g.sy + i;
             const Real oce = sce[ty * L::BXC + tx + 1];
             const int grc = sgr[ty * L::BXG + tx + 1];
-            const double Td = temp_cell(p, a.d.T, c, j, k, ts);
+            const double Td = t_per_plane ? sT[t] : temp_cell(p, a.d.T, c, j, k, ts);
+            const bool interior = i > 1 && i < g.gx && j > 1 && j < g.gy && k > 1 && k < g.gz;
             Real cen, cl_new, fs_new;
             int gr_new;
-            cell_update<Real>(q, p, cc[h], fc[h], nb_cl, nb_fs, one_m, oce, grc, Td, a.d.curv, c, cen, cl_new,
-                              fs_new, gr_new);
+            cell_update<Real>(q, p, cc[h], fc[h], nb_cl, nb_fs, one_m, interior, oce, grc, Td, a.d.curv, c, cen,
+                              cl_new, fs_new, gr_new);
             ce[c] = cen;
             clO[c] = cl_new;
             fsO[c] = fs_new;
             if (gr_new != grc) gr[c] = gr_new;
-            if (cen < 0) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
+            // growth.c:163-165 (the FP32 form stores ce - Cinit)
+            if (sizeof(Real) == 8 ? cen < 0 : cen < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
             solid = gr_new > 0;
         }
         const unsigned word = __ballot_sync(FULL_MASK, solid);
         if (tx == 0 && j <= g.gy) a.d.solid_bits[((long long)k * (g.gy + 2) + j) * wrow + blockIdx.x] = word;
         __syncthreads();
+        if (s_abort) {
+            // a copy did not land within the bound: report, then wait (again
+            // bounded) for every copy still in flight before leaving
+            if (tid == 0) {
+                raise_error(ctl, MMS_ERR_TIMEOUT);
+                for (int pl = t; pl < issued; pl++) mbar_wait(&bars[pl % TS], (unsigned)((pl / TS) & 1));
+            }
+            break;
+        }
         if (t + TS < nplanes) {
             if (tid == 0) issue(t + TS);
             issued = t + TS + 1;
@@ -805,13 +845,15 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchun
             const double Td = temp_cell(p, a.d.T, c, j, k, ts);
             Real cen, cl_new, fs_new;
             int gr_new;
-            cell_update<Real>(q, p, s_cl[sc][ly][lx], s_fs[sc][ly][lx], nb_cl, nb_fs, one_m, ce[c], grc, Td,
-                              a.d.curv, c, cen, cl_new, fs_new, gr_new);
+            const bool interior = i > 1 && i < g.gx && j > 1 && j < g.gy && k > 1 && k < g.gz;
+            cell_update<Real>(q, p, s_cl[sc][ly][lx], s_fs[sc][ly][lx], nb_cl, nb_fs, one_m, interior, ce[c], grc,
+                              Td, a.d.curv, c, cen, cl_new, fs_new, gr_new);
             ce[c] = cen;
             clO[c] = cl_new;
             fsO[c] = fs_new;
             if (gr_new != grc) gr[c] = gr_new;
-            if (cen < 0) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
+            // growth.c:163-165 (the FP32 form stores ce - Cinit)
+            if (sizeof(Real) == 8 ? cen < 0 : cen < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
             solid = gr_new > 0;
         }
         const unsigned word = __ballot_sync(FULL_MASK, solid);
@@ -832,33 +874,21 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchun
 // never mold in one domain.
 constexpr int LIST_NT = 256;
 
-__global__ void __launch_bounds__(LIST_NT) k_list_flags(KernelArgs a)
+// 32 bits of a bitmask row starting at interior cell x (0-based, x >= -1);
+// bits outside the row read as 0 (halo cells are never solid).
+__device__ __forceinline__ unsigned row_bits(const unsigned *row, int wpr, long long x)
 {
-    const Ctl *ctl = a.d.ctl;
-    if (stalled(ctl)) return;
-    const Geo &g = a.g;
-    long long wi = blockIdx.x * (long long)LIST_NT + threadIdx.x;
-    if (wi >= g.nwords) return;
-    const unsigned *sb = a.d.solid_bits;
-    const long long wpr = g.wpr, plane = wpr * (g.gy + 2);
-    long long w = wi % wpr, row = wi / wpr;
-    long long J = row % (g.gy + 2), K = row / (g.gy + 2);
-    unsigned F = 0;
-    if (J >= 1 && J <= g.gy && K >= 1 && K <= g.gz) {
-        unsigned S = sb[wi];
-        unsigned Sl = w > 0 ? sb[wi - 1] : 0u, Sr = (w + 1 < wpr) ? sb[wi + 1] : 0u;
-        unsigned nb = (S << 1) | (Sl >> 31);
-        nb |= (S >> 1) | (Sr << 31);
-        nb |= sb[wi + wpr] | sb[wi - wpr] | sb[wi + plane] | sb[wi - plane];
-        long long nbits = g.gx - 32 * w;
-        unsigned valid = nbits >= 32 ? FULL_MASK : ((1u << nbits) - 1u);
-        F = ~S & nb & valid;
-    }
-    a.d.flag_bits[wi] = F;
+    long long w = (x >= 0) ? (x >> 5) : -1;
+    int sh = (int)(x - 32 * w);
+    unsigned lo = (w >= 0) ? row[w] : 0u;
+    unsigned hi = (w + 1 < wpr) ? row[w + 1] : 0u;
+    return sh ? (lo >> sh) | (hi << (32 - sh)) : lo;
 }
 
 // A piece is 32 consecutive cells of one emulated rank's local row; pieces
 // are numbered in rank-local raster order, so list order = piece order.
+// Its list membership bits come straight from the solid bitmask: liquid
+// and some face neighbour solid.
 struct Piece {
     unsigned bits;
     long long base;  // device index of the piece's first cell
@@ -876,11 +906,13 @@ __device__ __forceinline__ Piece piece_of(const KernelArgs &a, int r, long long 
     long long J = (long long)ry * g.sby + ly + 1, K = (long long)rz * g.sbz + lz + 1;
     long long X0 = (long long)rx * g.sbx + 32LL * part;  // 0-based interior x
     int len = min(32, g.sbx - 32 * part);
-    const unsigned *fb = a.d.flag_bits + (K * (g.gy + 2) + J) * (long long)g.wpr;
-    long long w = X0 >> 5;
-    int sh = (int)(X0 & 31);
-    unsigned bits = fb[w] >> sh;
-    if (sh && w + 1 < g.wpr) bits |= fb[w + 1] << (32 - sh);
+    const long long wpr = g.wpr, plane = wpr * (g.gy + 2);
+    const unsigned *row = a.d.solid_bits + (K * (g.gy + 2) + J) * wpr;
+    unsigned S = row_bits(row, g.wpr, X0);
+    unsigned nb = row_bits(row, g.wpr, X0 - 1) | row_bits(row, g.wpr, X0 + 1) |
+                  row_bits(row + wpr, g.wpr, X0) | row_bits(row - wpr, g.wpr, X0) |
+                  row_bits(row + plane, g.wpr, X0) | row_bits(row - plane, g.wpr, X0);
+    unsigned bits = ~S & nb;
     if (len < 32) bits &= (1u << len) - 1u;
     pc.bits = bits;
     pc.base = K * g.sz + J * g.sy + X0 + 1;
@@ -943,17 +975,6 @@ __global__ void __launch_bounds__(SCAN_NT) k_list_scan(KernelArgs a, int nblocks
         ctl->list_total = run;
         ctl->zero_needed = any_zero;
     }
-}
-
-__global__ void k_list_zero(KernelArgs a)
-{
-    const Ctl *ctl = a.d.ctl;
-    if (stalled(ctl) || !ctl->zero_needed) return;
-    int r = blockIdx.y;
-    int upto = a.d.rank_zero_upto[r];
-    Dc3 *base = a.d.dc_tmp + a.d.rank_dcbase[r];
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < upto; s += (long long)gridDim.x * blockDim.x)
-        base[s] = Dc3{0.0, 0.0, 0.0};
 }
 
 // capture_octahedra_diffuse, INDEX_SEP branch (growth.c:664-794), for the
@@ -1030,7 +1051,16 @@ __global__ void __launch_bounds__(LIST_NT) k_list_write(KernelArgs a)
     __shared__ int sh[LIST_NT / 32];
     const Geo &g = a.g;
     const int r = (int)(blockIdx.x / g.blocks_per_rank);
-    const long long q0 = (blockIdx.x % g.blocks_per_rank) * (long long)LIST_PIECES;
+    const long long chunk = blockIdx.x % g.blocks_per_rank;
+    const long long q0 = chunk * (long long)LIST_PIECES;
+    if (ctl->zero_needed) {
+        // this block's share of the rank's dc_tmp slots to clear
+        const long long upto = a.d.rank_zero_upto[r];
+        const long long span = (upto + g.blocks_per_rank - 1) / g.blocks_per_rank;
+        Dc3 *base = a.d.dc_tmp + a.d.rank_dcbase[r];
+        for (long long s = chunk * span + threadIdx.x; s < min(upto, (chunk + 1) * span); s += LIST_NT)
+            base[s] = Dc3{0.0, 0.0, 0.0};
+    }
     if (a.d.blk_cnt[blockIdx.x] == 0) return;
     int pos = a.d.blk_off[blockIdx.x];
     for (int it = 0; it < LIST_PIECES / LIST_NT; it++) {
@@ -1335,18 +1365,12 @@ static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t
         n++;
     }
     int nblocks = (int)(g.blocks_per_rank * g.nranks);
-    PROF_BEGIN(KID_LIST_FLAGS);
-    k_list_flags<<<(int)((g.nwords + LIST_NT - 1) / LIST_NT), LIST_NT, 0, st>>>(a);
-    PROF_END(KID_LIST_FLAGS);
     PROF_BEGIN(KID_LIST_COUNT);
     k_list_count<<<nblocks, LIST_NT, 0, st>>>(a);
     PROF_END(KID_LIST_COUNT);
     PROF_BEGIN(KID_LIST_SCAN);
     k_list_scan<<<1, SCAN_NT, 0, st>>>(a, nblocks);
     PROF_END(KID_LIST_SCAN);
-    PROF_BEGIN(KID_LIST_ZERO);
-    k_list_zero<<<dim3(64, g.nranks), 256, 0, st>>>(a);
-    PROF_END(KID_LIST_ZERO);
     PROF_BEGIN(KID_LIST_WRITE);
     k_list_write<<<nblocks, LIST_NT, 0, st>>>(a);
     PROF_END(KID_LIST_WRITE);
@@ -1356,7 +1380,7 @@ static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t
     PROF_BEGIN(KID_APPLY);
     k_apply<<<148 * 4, 256, 0, st>>>(a);
     PROF_END(KID_APPLY);
-    n += 7;
+    n += 5;
     return n;
 }
 

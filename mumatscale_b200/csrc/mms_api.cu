@@ -86,6 +86,11 @@ struct EventProfiler : mms::Profiler {
 struct mms_ctx {
     mms_params p{};
     TmaHolder tma{};
+    // one timestep captured as a CUDA graph (kernel arguments only change
+    // when sites or orientation overrides are replaced)
+    cudaGraphExec_t step_graph = nullptr;
+    int step_graph_kernels = 0;
+    bool use_graphs = true;
     cudaStream_t own_stream = nullptr;
     EventProfiler *prof = nullptr;
     std::vector<mms_fixed_nuc> fixed;
@@ -144,6 +149,12 @@ mms_status dalloc(mms_ctx *ctx, T **ptr, size_t count)
     return MMS_OK;
 }
 
+void drop_graph(mms_ctx *ctx)
+{
+    if (ctx->step_graph) cudaGraphExecDestroy(ctx->step_graph);
+    ctx->step_graph = nullptr;
+}
+
 void dfree(mms_ctx *ctx, void *p)
 {
     if (!p) return;
@@ -196,6 +207,7 @@ mms_status upload_sites(mms_ctx *ctx)
     dfree(ctx, d.cand);
     dfree(ctx, d.cand_stage);
     dfree(ctx, d.nuc_blk_cnt);
+    dfree(ctx, d.cand_ex);
     d.site_cell = nullptr;
     d.site_thr = nullptr;
     d.site_rank = nullptr;
@@ -203,13 +215,16 @@ mms_status upload_sites(mms_ctx *ctx)
     d.cand = nullptr;
     d.cand_stage = nullptr;
     d.nuc_blk_cnt = nullptr;
+    d.cand_ex = nullptr;
+    drop_graph(ctx);
     size_t n = ctx->site_cell.size();
     d.nsites = (long long)n;
     d.nuc_blocks = (int)std::max<size_t>(1, (n + 255) / 256);
     mms_status st;
     if ((st = dalloc(ctx, &d.site_cell, n)) || (st = dalloc(ctx, &d.site_thr, n)) ||
         (st = dalloc(ctx, &d.site_rank, n)) || (st = dalloc(ctx, &d.site_flag, n)) || (st = dalloc(ctx, &d.cand, n)) ||
-        (st = dalloc(ctx, &d.cand_stage, (size_t)d.nuc_blocks * 256)) || (st = dalloc(ctx, &d.nuc_blk_cnt, d.nuc_blocks)))
+        (st = dalloc(ctx, &d.cand_stage, (size_t)d.nuc_blocks * 256)) || (st = dalloc(ctx, &d.nuc_blk_cnt, d.nuc_blocks)) ||
+        (st = dalloc(ctx, &d.cand_ex, n)))
         return st;
     if (n) {
         CU(cudaMemcpyAsync(d.site_cell, ctx->site_cell.data(), n * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
@@ -309,6 +324,30 @@ mms_status read_ctl(mms_ctx *ctx)
     CU(cudaMemcpyAsync(ctx->h_ctl, ctx->ka.d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
     if (ctx->prof) ctx->prof->collect();
+    return MMS_OK;
+}
+
+int launch_one_step(mms_ctx *ctx, int start_stage);
+
+// Captures one whole step into a graph (once per kernel-argument set).
+mms_status ensure_graph(mms_ctx *ctx)
+{
+    if (ctx->step_graph) return MMS_OK;
+    cudaGraph_t g = nullptr;
+    CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    EventProfiler *saved = ctx->prof;
+    ctx->prof = nullptr;
+    int n = launch_one_step(ctx, 0);
+    ctx->prof = saved;
+    CU(cudaStreamEndCapture(ctx->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&ctx->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        ctx->step_graph = nullptr;
+        ctx->err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+        return MMS_ERR_CUDA;
+    }
+    ctx->step_graph_kernels = n;
     return MMS_OK;
 }
 
@@ -453,9 +492,10 @@ int mms_kernel_count(void) { return mms::KID_COUNT; }
 
 const char *mms_kernel_name(int id)
 {
-    static const char *names[mms::KID_COUNT] = {"k_temp_am",    "k_nuc",        "k_act",       "k_curv",
-                                                "k_diffuse_fs", "k_list_flags", "k_list_count", "k_list_scan",
-                                                "k_list_zero",  "k_list_write", "k_capture",   "k_apply"};
+    static const char *names[mms::KID_COUNT] = {"k_temp_am",    "k_nuc",         "k_act",
+                                                "k_curv",       "k_diffuse_fs",  "k_list_count",
+                                                "k_list_scan",  "k_list_write",  "k_capture",
+                                                "k_apply"};
     return (id >= 0 && id < mms::KID_COUNT) ? names[id] : "";
 }
 
@@ -575,7 +615,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         d.fs[b] = tmp;
     }
     if ((st = dalloc(ctx, &d.gr, N)) || (st = dalloc(ctx, &d.dc, N)) || (st = dalloc(ctx, &d.ctl, 1)) ||
-        (st = dalloc(ctx, &d.solid_bits, (size_t)g.nwords)) || (st = dalloc(ctx, &d.flag_bits, (size_t)g.nwords)))
+        (st = dalloc(ctx, &d.solid_bits, (size_t)g.nwords)))
         return fail(st);
     if (p.am) {
         if ((st = dalloc(ctx, &d.T, N))) return fail(st);
@@ -670,6 +710,7 @@ mms_status mms_destroy(mms_ctx *ctx)
     for (void *p : ctx->allocs) cudaFree(p);
     ctx->allocs.clear();
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+    drop_graph(ctx);
     delete ctx->prof;
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -726,6 +767,7 @@ mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxy
         for (int e = 0; e < 9; e++) ctx->inj_rot.push_back(rotmat9[9 * kv[i].second + e]);
     }
     DevPtrs &d = ctx->ka.d;
+    drop_graph(ctx);
     dfree(ctx, d.inj_key);
     dfree(ctx, d.inj_rot);
     d.inj_key = nullptr;
@@ -754,7 +796,15 @@ mms_status mms_step(mms_ctx *ctx, int nsteps)
     unsigned long long ts0 = ctx->h_ctl->timestep;
     while (done < nsteps) {
         int n = std::min(chunk, nsteps - done);
-        for (int s = 0; s < n; s++) ctx->launches += launch_one_step(ctx, 0);
+        if (ctx->use_graphs && !ctx->prof) {
+            if ((st = ensure_graph(ctx))) return st;
+            for (int s = 0; s < n; s++) {
+                CU(cudaGraphLaunch(ctx->step_graph, ctx->stream));
+                ctx->launches += ctx->step_graph_kernels;
+            }
+        } else {
+            for (int s = 0; s < n; s++) ctx->launches += launch_one_step(ctx, 0);
+        }
         CU(cudaGetLastError());
         if ((st = read_ctl(ctx))) return st;
         Ctl &c = *ctx->h_ctl;

@@ -128,7 +128,6 @@ struct DevPtrs {
     int *gr;
     Dc3 *dc;
     unsigned *solid_bits;  // gr > 0 after fs_change (written by the stencil)
-    unsigned *flag_bits;   // interface-list membership (grow_cell_reduction)
     double *T;            // AM temperature at the current step (N) or null
     int *lsindex;         // AM layer flag or null
     double *curv;         // curvature (N) when TipCurvature
@@ -140,6 +139,7 @@ struct DevPtrs {
     unsigned char *site_flag;
     int *cand;            // ordered candidate sites of the current step
     int *cand_stage;      // per nucleation block, its candidates in site order
+    int *cand_ex;         // per candidate: random orientation draws before it (k_act)
     int *nuc_blk_cnt;     // candidates per nucleation block
     int nuc_blocks;
     // orientation sources
@@ -182,8 +182,8 @@ struct KernelArgs {
 
 // Kernel ids for per-kernel timing.
 enum KernelId : int {
-    KID_TEMP_AM = 0, KID_NUC, KID_ACT, KID_CURV, KID_DIFFUSE_FS, KID_LIST_FLAGS, KID_LIST_COUNT,
-    KID_LIST_SCAN, KID_LIST_ZERO, KID_LIST_WRITE, KID_CAPTURE, KID_APPLY, KID_COUNT
+    KID_TEMP_AM = 0, KID_NUC, KID_ACT, KID_CURV, KID_DIFFUSE_FS, KID_LIST_COUNT, KID_LIST_SCAN,
+    KID_LIST_WRITE, KID_CAPTURE, KID_APPLY, KID_COUNT
 };
 
 // Opaque storage for the stencil's TMA descriptors (built in kernels.cu).
