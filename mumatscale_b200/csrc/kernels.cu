@@ -561,7 +561,20 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
                                             Real &cl_new, Real &fs_new, int &gr_new)
 {
     Real nbsum = 0;
-    if (interior) {
+    if (sizeof(Real) == 4) {
+        // FP32 form: the face coefficient rs fs_av + rl (1 - fs_av) written
+        // as A + B fs_n with fused multiply-adds
+        const float B = 0.5f * ((float)q.rs - (float)q.rl);
+        const float A = fmaf(B, (float)lspfs, (float)q.rl);
+        float acc = 0.f;
+#pragma unroll
+        for (int n = 0; n < 6; n++) {
+            float r = fmaf(B, (float)nb_fs[n], A);
+            if (!interior) r *= (float)one_m[n];
+            acc = fmaf(r, (float)nb_cl[n] - (float)conc, acc);
+        }
+        nbsum = (Real)acc;
+    } else if (interior) {
 #pragma unroll
         for (int n = 0; n < 6; n++) {
             Real fs_av = (Real)0.5 * (lspfs + nb_fs[n]);

@@ -87,7 +87,8 @@ def test_fp64_matches_oracle_every_step(built, cuda_device, name):
 def test_fp32_form_error(built, cuda_device):
     """FP32 bulk fields vs the FP64 oracle after 400 steps of small1.
     Tolerances: solute (ce) relative L2 error < 1e-5; grain-id mismatch
-    fraction < 1 %; fs max abs error < 5e-2."""
+    fraction < 0.1 %; fs max abs error < 1e-3; total solute relative
+    error < 1e-7."""
     from _oracle import Oracle
     p = M.read_deck(golden_deck("small1"))
     o = Oracle(p)
@@ -100,8 +101,9 @@ def test_fp32_form_error(built, cuda_device):
         mism = float((gr[1:-1, 1:-1, 1:-1] != gr0[1:-1, 1:-1, 1:-1]).mean())
         fs_err = float(np.abs(dom.download("fs") - o.download("fs")).max())
         assert rel_l2 < 1e-5, rel_l2
-        assert mism < 1e-2, mism
-        assert fs_err < 5e-2, fs_err
+        assert mism < 1e-3, mism
+        assert fs_err < 1e-3, fs_err
+        assert abs(dom.reduce("ce_sum") / o.reduce("ce_sum") - 1) < 1e-7
 
 
 def test_reductions(built, cuda_device):
