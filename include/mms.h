@@ -48,7 +48,9 @@ typedef enum mms_status {
     MMS_ERR_IO = 8,              /* a file could not be written or read */
     MMS_ERR_TIMEOUT = 9,         /* a bounded device-side wait expired */
     MMS_ERR_STATE = 10,          /* call made in the wrong state */
-    MMS_ERR_NOMEM = 11           /* device or host allocation failed */
+    MMS_ERR_NOMEM = 11,          /* device or host allocation failed */
+    MMS_ERR_SCRATCH_LIMIT = 12   /* grid larger than the fixed device scratch of
+                                    mms_reduce_field_noalloc (2^30 interior cells) */
 } mms_status;
 
 typedef enum mms_precision {
@@ -208,6 +210,28 @@ size_t mms_num_cells(const mms_ctx *ctx);
 mms_status mms_download(mms_ctx *ctx, mms_field field, void *host);
 mms_status mms_upload(mms_ctx *ctx, mms_field field, const void *host);
 mms_status mms_reduce(mms_ctx *ctx, mms_reduction what, double *out);
+
+/* Allocation-free form of mms_reduce over a caller-owned field.  It has no
+ * counterpart in the reference (whose reductions run on host arrays); it is
+ * for callers that may not allocate device memory where they reduce.
+ *   field       device pointer: ce or fs of a (gdimx, gdimy, gdimz) grid in
+ *               the halo'd layout above, FP64 (dtype MMS_PREC_F64) or FP32
+ *               (MMS_PREC_F32) elements, absolute values as mms_download
+ *               returns them
+ *   out         device pointer to one double, written asynchronously on
+ *               cuda_stream (a cudaStream_t; NULL = the legacy default stream)
+ * The result is the same sum as mms_reduce's, compensated in FP64, in a
+ * different summation order.  Intermediates live in a fixed 1 MiB device
+ * array of the library: grids above 2^30 interior cells return
+ * MMS_ERR_SCRATCH_LIMIT.  The array is shared by all calls on a device, so
+ * calls that may overlap on one device (unordered streams, several host
+ * threads) race.  The first call on a device looks up the array's address
+ * and should come before any stream capture on that device.  Nothing is
+ * allocated. */
+mms_status mms_reduce_field_noalloc(const void *field, mms_precision dtype,
+                                    int gdimx, int gdimy, int gdimz,
+                                    mms_reduction what, double cell_size,
+                                    double *out, void *cuda_stream);
 
 /* ---- sites and orientations ------------------------------------------------ */
 

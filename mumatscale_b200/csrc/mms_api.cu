@@ -459,6 +459,7 @@ const char *mms_status_string(mms_status s)
     case MMS_ERR_TIMEOUT: return "device wait timed out";
     case MMS_ERR_STATE: return "call made in the wrong state";
     case MMS_ERR_NOMEM: return "out of memory";
+    case MMS_ERR_SCRATCH_LIMIT: return "grid larger than the fixed device scratch (at most 2^30 interior cells)";
     }
     return "unknown status";
 }
