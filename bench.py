@@ -269,6 +269,7 @@ def gpu_arm(args) -> None:
     for form, prec in (("f64", M.PREC_F64), ("f32", M.PREC_F32)):
         dom = M.Domain(params, precision=prec, device=dev)
         dom.set_stream(stream.cuda_stream)
+        tile = dom.autotune(reps=5)  # stencil tile for this grid and form
         dom.step(W)
         torch.cuda.synchronize()
         barrier()
@@ -292,6 +293,7 @@ def gpu_arm(args) -> None:
         ks = dom.kernel_stats()
         dom.set_profiling(False)
         out[form] = {"ms_total": ms, "launches": launches, "kernels": ks, "clocks": clk.summary(),
+                     "tile": {"cells_per_thread": tile[0], "zchunk": tile[1], "cta_cells": [32 * tile[0], 8]},
                      "grains": dom.num_grains, "timestep": dom.timestep}
         if form == "f64":
             # end to end through the public API with host buffers: upload the
@@ -363,9 +365,10 @@ def gpu_arm(args) -> None:
         "config": {"workload": "multi-grain directional solidification, 256^3 cells, FP64 plain form",
                    "cells": cells, "dx_m": DX, "dt_s": DT, "G_K_per_m": 1e4, "V_m_per_s": 1e-3,
                    "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (about 1.1 GB of fields)",
-                   "grains_after_run": f64["grains"]},
+                   "grains_after_run": f64["grains"], "stencil_tile": f64["tile"]},
         "fp32_form": {"value": value32, "ms_per_step": f32["ms_total"] / K, "ratio_vs_fp64": value32 / value,
-                      "k_diffuse_fs_gbs": achieved32},
+                      "k_diffuse_fs_gbs": achieved32, "k_diffuse_fs_frac": achieved32 / peak,
+                      "stencil_tile": f32["tile"]},
         "roofline": {"bound": "hbm", "kernel": "k_diffuse_fs", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "algorithmic_bytes_per_cell": BYTES_DIFFUSE["f64"],
@@ -393,9 +396,12 @@ def profile_arm(args) -> None:
     deck.write_text(deck_text(n=args.cells))
     params = M.read_deck(deck)
     dom = M.Domain(params, precision=M.PREC_F32 if args.profile == "f32" else M.PREC_F64)
+    if args.tile != "auto":
+        cpt, zc = (int(v) for v in args.tile.split(","))
+        dom.set_stencil_tile(cpt, zc)
     dom.step(args.warmup + args.steps)
     print(json.dumps({"profile": args.profile, "cells": args.cells ** 3, "steps": args.warmup + args.steps,
-                      "grains": dom.num_grains, "tma": dom.uses_tma}))
+                      "grains": dom.num_grains, "tma": dom.uses_tma, "tile": dom.stencil_tile()}))
     dom.close()
 
 
@@ -431,6 +437,7 @@ def main() -> None:
     ap.add_argument("--profile", choices=["f64", "f32"], default=None,
                     help="run the workload for an ncu capture only")
     ap.add_argument("--cells", type=int, default=N_CELL, help="edge of the cubic domain (profile mode)")
+    ap.add_argument("--tile", default="auto", help="profile mode: stencil tile 'cells_per_thread,zchunk'")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -275,6 +275,50 @@ int mms_kernel_count(void);
 const char *mms_kernel_name(int id);
 mms_status mms_kernel_stats(mms_ctx *ctx, int id, double *total_ms, uint64_t *launches);
 
+/* Tile of the diffusion + fs-change stencil: cells per thread along x (1 or
+ * 2: CTA tiles of 32 x 8 or 64 x 8 cells) and planes per CTA along z (1-64;
+ * 0 = chosen from the grid size).  Results do not depend on the tile. */
+mms_status mms_set_stencil_tile(mms_ctx *ctx, int cells_per_thread, int zchunk);
+mms_status mms_get_stencil_tile(const mms_ctx *ctx, int *cells_per_thread, int *zchunk);
+/* Times every tile candidate on shadow copies of the fields the stencil
+ * writes (the domain's state is left as it was), keeps the fastest by median
+ * of `reps` launches and returns it (any output pointer may be NULL). */
+mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchunk, double *best_ms);
+
+/* ---- adjoint (frozen cellular automaton) -------------------------------------- */
+
+/* No counterpart in the reference.  Gradients of L = 1/2 sum over interior
+ * cells of (ce - target)^2 after a recorded run, with respect to D_l
+ * (Dliq), k (part_coef) and the Gibbs-Thomson coefficient, through the
+ * diffusion (growth.c:69-162) and fraction-solid change (growth.c:220-273)
+ * of every step, with the cellular automaton frozen: each cell's
+ * fs_change branch, nucleation, capture and the curvature are those of the
+ * recorded run.  Analytic temperature models only (not AnalyticalThermal 1). */
+typedef struct mms_adjoint_result {
+    double loss;
+    double dL_dDliq;
+    double dL_dpart_coef;
+    double dL_dgibbs;
+    int64_t steps;        /* recorded steps differentiated through */
+} mms_adjoint_result;
+
+/* Runs nsteps ordinary steps while recording, per step, the branch every
+ * cell took and (with TipCurvature) its curvature, and the state (ce, cl,
+ * fs) every checkpoint_every steps, starting with the current one.  Replaces
+ * an earlier record. */
+mms_status mms_adjoint_record(mms_ctx *ctx, int nsteps, int checkpoint_every);
+/* Loss and gradient for the recorded run; target_ce in the halo'd layout
+ * (FP64).  Each segment between checkpoints is recomputed from its
+ * checkpoint by frozen replay, then differentiated backwards. */
+mms_status mms_adjoint_gradient(mms_ctx *ctx, const double *target_ce, mms_adjoint_result *out);
+/* Loss of the frozen replay of the whole recorded run from its first
+ * checkpoint with Dliq, part_coef and GibbsThomsonCoef multiplied by
+ * scale[0..2] (scale 1,1,1 reproduces the recorded run): the function the
+ * gradient differentiates, for finite-difference checks. */
+mms_status mms_adjoint_replay_loss(mms_ctx *ctx, const double *target_ce, const double scale[3], double *loss);
+/* Frees the record. */
+mms_status mms_adjoint_release(mms_ctx *ctx);
+
 /* ---- diagnostics ----------------------------------------------------------- */
 const char *mms_status_string(mms_status s);
 /* The most recent error message on this context (empty when none). */

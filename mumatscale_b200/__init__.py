@@ -49,6 +49,11 @@ class NucVolume(C.Structure):
                 ("density", "minx", "miny", "minz", "maxx", "maxy", "maxz", "threshold")]
 
 
+class AdjointResult(C.Structure):
+    _fields_ = [("loss", C.c_double), ("dL_dDliq", C.c_double), ("dL_dpart_coef", C.c_double),
+                ("dL_dgibbs", C.c_double), ("steps", C.c_int64)]
+
+
 class Params(C.Structure):
     """mms_params: the BB_struct subset (globals.h:273-403) the hot path reads."""
     _fields_ = [
@@ -167,6 +172,13 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_kernel_count": (I, []),
         "mms_kernel_name": (C.c_char_p, [I]),
         "mms_kernel_stats": (I, [P, I, C.POINTER(D), C.POINTER(C.c_uint64)]),
+        "mms_set_stencil_tile": (I, [P, I, I]),
+        "mms_get_stencil_tile": (I, [P, C.POINTER(I), C.POINTER(I)]),
+        "mms_autotune": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(D)]),
+        "mms_adjoint_record": (I, [P, I, I]),
+        "mms_adjoint_gradient": (I, [P, P, C.POINTER(AdjointResult)]),
+        "mms_adjoint_replay_loss": (I, [P, P, C.POINTER(D), C.POINTER(D)]),
+        "mms_adjoint_release": (I, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -286,6 +298,53 @@ class Domain:
 
     def set_profiling(self, on: bool) -> None:
         _check(_lib().mms_set_profiling(self._ctx, int(on)), "mms_set_profiling", self._ctx)
+
+    def set_stencil_tile(self, cells_per_thread: int, zchunk: int = 0) -> None:
+        """Stencil CTA tile: (32 x cells_per_thread) x 8 cells, zchunk planes (0 = auto)."""
+        _check(_lib().mms_set_stencil_tile(self._ctx, cells_per_thread, zchunk), "mms_set_stencil_tile", self._ctx)
+
+    def stencil_tile(self) -> tuple[int, int]:
+        cpt, zc = C.c_int(), C.c_int()
+        _check(_lib().mms_get_stencil_tile(self._ctx, C.byref(cpt), C.byref(zc)), "mms_get_stencil_tile", self._ctx)
+        return cpt.value, zc.value
+
+    def autotune(self, reps: int = 5) -> tuple[int, int, float]:
+        """Picks the fastest stencil tile (state untouched); returns (cells_per_thread, zchunk, ms)."""
+        cpt, zc, ms = C.c_int(), C.c_int(), C.c_double()
+        _check(_lib().mms_autotune(self._ctx, reps, C.byref(cpt), C.byref(zc), C.byref(ms)), "mms_autotune",
+               self._ctx)
+        return cpt.value, zc.value, ms.value
+
+    # -- frozen-CA adjoint
+    def adjoint_record(self, nsteps: int, checkpoint_every: int = 100) -> None:
+        """Runs nsteps steps recording the CA decisions and checkpoints."""
+        _check(_lib().mms_adjoint_record(self._ctx, nsteps, checkpoint_every), "mms_adjoint_record", self._ctx)
+
+    def _target(self, target: np.ndarray) -> np.ndarray:
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        if t.size != self.num_cells():
+            raise ValueError("target must be a halo'd field of the domain")
+        return t
+
+    def adjoint_gradient(self, target_ce: np.ndarray) -> dict:
+        """Loss 1/2 sum (ce - target)^2 and its gradient w.r.t. Dliq, part_coef, GibbsThomsonCoef."""
+        t = self._target(target_ce)
+        r = AdjointResult()
+        _check(_lib().mms_adjoint_gradient(self._ctx, t.ctypes.data, C.byref(r)), "mms_adjoint_gradient",
+               self._ctx)
+        return {"loss": r.loss, "Dliq": r.dL_dDliq, "part_coef": r.dL_dpart_coef, "gibbs": r.dL_dgibbs,
+                "steps": int(r.steps)}
+
+    def adjoint_replay_loss(self, target_ce: np.ndarray, scale=(1.0, 1.0, 1.0)) -> float:
+        t = self._target(target_ce)
+        sc = (C.c_double * 3)(*scale)
+        out = C.c_double()
+        _check(_lib().mms_adjoint_replay_loss(self._ctx, t.ctypes.data, sc, C.byref(out)),
+               "mms_adjoint_replay_loss", self._ctx)
+        return out.value
+
+    def adjoint_release(self) -> None:
+        _check(_lib().mms_adjoint_release(self._ctx), "mms_adjoint_release", self._ctx)
 
     def kernel_stats(self) -> dict[str, tuple[float, int]]:
         lib = _lib()

@@ -27,7 +27,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = "/usr/bin/g++"
 CC = "/usr/bin/gcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels.cu", "mms_api.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels.cu", "mms_api.cu", "adjoint.cu", "noalloc.cu"]
 CXX_SOURCES = ["deck.cpp", "host_setup.cpp"]
 
 
@@ -47,7 +47,7 @@ def _stale(target: Path, deps: list[Path]) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
-    headers = list(CSRC.glob("*.h")) + [ROOT / "include" / "mms.h"]
+    headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "mms.h"]
     objs = []
     for src in CU_SOURCES:
         obj = BUILD / (src + ".o")

@@ -1,0 +1,52 @@
+// device_common.cuh — device helpers shared by the step kernels (kernels.cu)
+// and the adjoint (adjoint.cu).  Both are compiled with -fmad=false, so an
+// expression written here rounds the same way in either file.
+#pragma once
+
+#include "mms_internal.h"
+
+namespace mms {
+
+// direct_temp_calc (temperature.c:24-61) for the analytic models; the AM
+// quadrature is precomputed into an array by k_temp_am.
+__device__ __forceinline__ double temp_cell(const Phys &p, const double *Tarr, long long cell,
+                                            long long J, long long K, unsigned long long ts)
+{
+    if (p.temp_mode == 2) return Tarr[cell];
+    double sim_time = (double)ts * p.ts_delt;
+    if (p.temp_mode == 0) return p.T0 - sim_time * p.cool_rate;
+    double ry = p.origin[1] + ((double)(int)J + 0.5) * p.cellSize;
+    double rz = p.origin[2] + ((double)(int)K + 0.5) * p.cellSize;
+    double axis = (p.gz_is_one ? ry : rz) - p.cellSize * 0.5;
+    double tgrad = p.gradient + p.grad_coef * sim_time;
+    double v = p.velocity + p.velo_coef * sim_time;
+    double vt = 0.5 * (v + p.velocity) * sim_time;
+    return p.T0 + tgrad * (axis - vt);
+}
+
+// Physics constants in the stencil's arithmetic type.
+template <typename Real>
+struct PhysR {
+    Real rs, rl, liq_slope, k_inv, km, km_inv, m_inv, D_xt, cinit, Tliq, gibbs, c0k;
+};
+
+template <typename Real>
+__device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
+{
+    PhysR<Real> q;
+    q.rs = (Real)p.rs;
+    q.rl = (Real)p.rl;
+    q.liq_slope = (Real)p.liq_slope;
+    q.k_inv = (Real)p.k_inv;
+    q.km = (Real)p.km;
+    q.km_inv = (Real)p.km_inv;
+    q.m_inv = (Real)p.m_inv;
+    q.D_xt = (Real)p.D_xt;
+    q.cinit = (Real)p.cinit;
+    q.Tliq = (Real)p.Tliq;
+    q.gibbs = (Real)p.gibbs;
+    q.c0k = (Real)(p.cinit * (p.k_inv - 1.0));
+    return q;
+}
+
+}  // namespace mms

@@ -19,8 +19,8 @@
 //   k_list_scan   ordered block offsets, per-rank dc_tmp bookkeeping (growth.c:642-660)
 //   k_list_write  ordered list write; clears dc_tmp regions that the
 //                 reference re-allocates zeroed
-//   k_capture     octahedron capture over the list (growth.c:339-407, 664-794)
-//   k_apply       dc copy-back and captured grain ids (growth.c:789, 797-807)
+//   k_capture     octahedron capture over the list (growth.c:339-407, 664-794),
+//                 dc copy-back and captured grain ids (growth.c:789, 797-807)
 //
 // Fields: ce in place; cl and fs ping-pong between two buffers, the state
 // after step t living in buffer (t & 1).  gr, dc in place.  d is never
@@ -34,6 +34,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "device_common.cuh"
 #include "mms_internal.h"
 
 namespace mms {
@@ -51,22 +52,6 @@ __device__ __forceinline__ void raise_error(Ctl *c, int status)
     atomicExch(&c->stall, (int)STALL_ERROR);
 }
 
-// direct_temp_calc (temperature.c:24-61) for the analytic models; the AM
-// quadrature is precomputed into an array by k_temp_am.
-__device__ __forceinline__ double temp_cell(const Phys &p, const double *Tarr, long long cell,
-                                            long long J, long long K, unsigned long long ts)
-{
-    if (p.temp_mode == 2) return Tarr[cell];
-    double sim_time = (double)ts * p.ts_delt;
-    if (p.temp_mode == 0) return p.T0 - sim_time * p.cool_rate;
-    double ry = p.origin[1] + ((double)(int)J + 0.5) * p.cellSize;
-    double rz = p.origin[2] + ((double)(int)K + 0.5) * p.cellSize;
-    double axis = (p.gz_is_one ? ry : rz) - p.cellSize * 0.5;
-    double tgrad = p.gradient + p.grad_coef * sim_time;
-    double v = p.velocity + p.velo_coef * sim_time;
-    double vt = 0.5 * (v + p.velocity) * sim_time;
-    return p.T0 + tgrad * (axis - vt);
-}
 
 template <int NT>
 __device__ __forceinline__ int block_exclusive_scan(int v, int &total, int *sh)
@@ -518,29 +503,6 @@ __global__ void k_curv(KernelArgs a)
 // value before diffusion, held in a register (calculate.c:269-280).  The
 // neighbour values are read before any cell of this step writes them: cl
 // and fs come from the previous step's buffer.
-template <typename Real>
-struct PhysR {
-    Real rs, rl, liq_slope, k_inv, km, km_inv, m_inv, D_xt, cinit, Tliq, gibbs, c0k;
-};
-
-template <typename Real>
-__device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
-{
-    PhysR<Real> q;
-    q.rs = (Real)p.rs;
-    q.rl = (Real)p.rl;
-    q.liq_slope = (Real)p.liq_slope;
-    q.k_inv = (Real)p.k_inv;
-    q.km = (Real)p.km;
-    q.km_inv = (Real)p.km_inv;
-    q.m_inv = (Real)p.m_inv;
-    q.D_xt = (Real)p.D_xt;
-    q.cinit = (Real)p.cinit;
-    q.Tliq = (Real)p.Tliq;
-    q.gibbs = (Real)p.gibbs;
-    q.c0k = (Real)(p.cinit * (p.k_inv - 1.0));
-    return q;
-}
 
 // nb_* in the order +x, -x, +y, -y, +z, -z (growth.c:85-113); one_m[n] is
 // (1 - mold) of that neighbour.
@@ -558,7 +520,7 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
                                             const Real (&nb_cl)[6], const Real (&nb_fs)[6],
                                             const Real (&one_m)[6], bool interior, Real oce, int grc,
                                             double Td, const double *curv, long long c, Real &cen,
-                                            Real &cl_new, Real &fs_new, int &gr_new)
+                                            Real &cl_new, Real &fs_new, int &gr_new, int &br)
 {
     Real nbsum = 0;
     if (sizeof(Real) == 4) {
@@ -601,9 +563,11 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
             cl_new = cen;
             fs_new = 0;
             gr_new = 0;
+            br = BR_RESET;
         } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
             cl_new = cen * q.k_inv;
             fs_new = lspfs;
+            br = BR_KEEP;
         } else {
             if (p.tip_curv) c_int = q.cinit + q.m_inv * (Tcell - q.Tliq + q.gibbs * (Real)curv[c]);
             Real dce = cen - oce;
@@ -611,11 +575,13 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
             Real dfs = (dcl * ((Real)1. - q.km * lspfs) - dce) * q.km_inv / conc;
             cl_new = conc + dcl;
             fs_new = lspfs + dfs;
+            br = ((Real)1.0 < fs_new) ? BR_CLAMP : BR_GROW;
             fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
             if (fs_new < (Real)0.) {
                 fs_new = 0.;
                 gr_new = 0;
                 cl_new = cen;
+                br = BR_NEG;
             }
         }
     } else {
@@ -626,21 +592,30 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
             cl_new = cen;
             fs_new = 0;
             gr_new = 0;
+            br = BR_RESET;
         } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
             cl_new = cen * q.k_inv + q.c0k;      // ce / k - Cinit
             fs_new = lspfs;
+            br = BR_KEEP;
         } else {
             if (p.tip_curv) c_int = q.m_inv * (dT + q.gibbs * (Real)curv[c]);
-            const Real dce = nbsum;
-            Real dcl = (c_int - conc) * q.D_xt * 2 + dce / (1 - q.km * lspfs);
-            Real dfs = (dcl * ((Real)1. - q.km * lspfs) - dce) * q.km_inv / (conc + q.cinit);
+            // dce = the diffusion sum; dcl (u - 1/u terms) and dfs with the
+            // dce terms of growth.c:257-261 cancelled algebraically:
+            // dcl u - dce = (c_int - cl) 2 D_xt u
+            const float dce = (float)nbsum;
+            const float u = 1.f - (float)q.km * (float)lspfs;
+            const float t2 = ((float)c_int - (float)conc) * (2.f * (float)q.D_xt);
+            const float dcl = t2 + __fdividef(dce, u);
+            const float dfs = __fdividef(t2 * u * (float)q.km_inv, (float)conc + (float)q.cinit);
             cl_new = conc + dcl;
             fs_new = lspfs + dfs;
+            br = ((Real)1.0 < fs_new) ? BR_CLAMP : BR_GROW;
             fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
             if (fs_new < (Real)0.) {
                 fs_new = 0.;
                 gr_new = 0;
                 cl_new = cen;
+                br = BR_NEG;
             }
         }
     }
@@ -648,23 +623,28 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
 
 constexpr int DTX = 32, DTY = 8;
 
-// TMA-fed variant.  A CTA owns a 32 x 8 column of cells and marches up a
-// z-chunk; planes of cl and fs with their x/y halo (and ce, gr without) are
-// brought into a TS-deep shared-memory ring by cp.async.bulk.tensor, one
-// mbarrier per slot, issued TS-1 planes ahead of the plane being updated.
-// pipeline depth (planes in the ring): deeper for FP32, whose planes are smaller
-template <typename Real>
+// TMA-fed variant.  A CTA of 32 x 8 threads owns a (32 CPT) x 8 column of
+// cells (each thread CPT cells along x, 32 apart) and marches up a z-chunk;
+// planes of cl and fs with their x/y halo (and ce, gr without) are brought
+// into a TS-deep shared-memory ring by cp.async.bulk.tensor, one mbarrier
+// per slot, issued TS-1 planes ahead of the plane being updated.
+template <typename Real, int CPT>
 struct Depth {
-    static constexpr int TS = sizeof(Real) == 8 ? 6 : 8;
+    // planes in the ring: deeper for FP32, whose planes are smaller
+    static constexpr int TS = (sizeof(Real) == 4 && CPT == 1) ? 8 : 6;
+    // CTAs per SM the register budget is set for
+    static constexpr int MINB = CPT == 1 ? 4 : (sizeof(Real) == 4 ? 3 : 2);
 };
 constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 
-template <typename Real>
+template <typename Real, int CPT>
 struct Stage {
+    static constexpr int TX = DTX * CPT;
     // box widths: a multiple of 16 bytes, starting at the aligned column i0-1
-    static constexpr int BXH = sizeof(Real) == 8 ? 34 : 36;  // cl, fs: DTY+2 rows
-    static constexpr int BXC = sizeof(Real) == 8 ? 34 : 36;  // ce: DTY rows
-    static constexpr int BXG = 36;                           // gr (int): DTY rows
+    static constexpr int EPA = 16 / (int)sizeof(Real);
+    static constexpr int BXH = (TX + 2 + EPA - 1) / EPA * EPA;  // cl, fs: DTY+2 rows
+    static constexpr int BXC = BXH;                              // ce: DTY rows
+    static constexpr int BXG = (TX + 2 + 3) / 4 * 4;             // gr (int): DTY rows
     static constexpr int CL = round128(BXH * (DTY + 2) * (int)sizeof(Real));
     static constexpr int CE = round128(BXC * DTY * (int)sizeof(Real));
     static constexpr int GR = round128(BXG * DTY * 4);
@@ -677,12 +657,12 @@ struct TmaMaps {
     CUtensorMap cl[2], fs[2], ce, gr;
 };
 
-template <typename Real>
-__global__ void __launch_bounds__(DTX *DTY, 4) k_diffuse_fs_tma(const __grid_constant__ KernelArgs a,
-                                                             const __grid_constant__ TmaMaps maps, int zchunk)
+template <typename Real, int CPT>
+__global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
+    k_diffuse_fs_tma(const __grid_constant__ KernelArgs a, const __grid_constant__ TmaMaps maps, int zchunk)
 {
-    using L = Stage<Real>;
-    constexpr int TS = Depth<Real>::TS;
+    using L = Stage<Real, CPT>;
+    constexpr int TS = Depth<Real, CPT>::TS;
     Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -697,12 +677,11 @@ __global__ void __launch_bounds__(DTX *DTY, 4) k_diffuse_fs_tma(const __grid_con
     int *__restrict__ gr = a.d.gr;
     const PhysR<Real> q = phys_r<Real>(p);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DTX + tx;
-    const int i0 = blockIdx.x * DTX + 1, j0 = blockIdx.y * DTY + 1;
-    const int i = i0 + tx, j = j0 + ty;
+    const int i0 = blockIdx.x * L::TX + 1, j0 = blockIdx.y * DTY + 1;
+    const int j = j0 + ty;
     const int k0 = blockIdx.z * zchunk + 1;
     const int k1 = min(k0 + zchunk - 1, g.gz);
     const int nplanes = k1 - k0 + 3;  // k0-1 .. k1+1
-    const bool active = (i <= g.gx) && (j <= g.gy);
     const CUtensorMap *mcl = &maps.cl[pin];
     const CUtensorMap *mfs = &maps.fs[pin];
 
@@ -736,47 +715,78 @@ __global__ void __launch_bounds__(DTX *DTY, 4) k_diffuse_fs_tma(const __grid_con
 
     const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_z = (Real)(1 - g.padz);
     const long long wrow = (long long)g.wpr;
+    // plane-invariant per-cell values
+    int hh[CPT], hcc[CPT], hgg[CPT];
+    bool act[CPT], in_xy[CPT];
+    Real omx_p[CPT], omx_m[CPT];
+    const bool jrow = j <= g.gy;
+    const Real omy_p = j == g.gy ? one_y : (Real)1, omy_m = j == 1 ? one_y : (Real)1;
+#pragma unroll
+    for (int u = 0; u < CPT; u++) {
+        const int i = i0 + tx + DTX * u;
+        hh[u] = (ty + 1) * L::BXH + tx + DTX * u + 1;
+        hcc[u] = ty * L::BXC + tx + DTX * u + 1;
+        hgg[u] = ty * L::BXG + tx + DTX * u + 1;
+        act[u] = i <= g.gx && jrow;
+        in_xy[u] = i > 1 && i < g.gx && j > 1 && j < g.gy;
+        omx_p[u] = i == g.gx ? one_x : (Real)1;
+        omx_m[u] = i == 1 ? one_x : (Real)1;
+    }
+    // ring slots of planes t, t+1, t+2 and the phase of slot s2
+    int s0 = 0, s1 = 1 % TS, s2 = 2 % TS;
+    unsigned ph2 = (unsigned)((2 / TS) & 1);
+    long long crow = (long long)k0 * g.sz + (long long)j * g.sy;
     for (int t = 0; t <= k1 - k0; t++) {
         const int k = k0 + t;
         // planes t and t+1 completed in earlier iterations
-        bool ok = mbar_wait(&bars[(t + 2) % TS], (unsigned)(((t + 2) / TS) & 1));
+        bool ok = mbar_wait(&bars[s2], ph2);
         if (t == 0) ok &= mbar_wait(&bars[0], 0u) && mbar_wait(&bars[1 % TS], (unsigned)((1 / TS) & 1));
         if (!ok) s_abort = 1;
-        int solid = 0;
-        if (active && ok) {
-            const Real *cm = (const Real *)stage(t % TS);
-            const Real *cc = (const Real *)stage((t + 1) % TS);
-            const Real *cp = (const Real *)stage((t + 2) % TS);
-            const Real *fm = (const Real *)(stage(t % TS) + L::CL);
-            const Real *fc = (const Real *)(stage((t + 1) % TS) + L::CL);
-            const Real *fp = (const Real *)(stage((t + 2) % TS) + L::CL);
-            const Real *sce = (const Real *)(stage((t + 1) % TS) + 2 * L::CL);
-            const int *sgr = (const int *)(stage((t + 1) % TS) + 2 * L::CL + L::CE);
-            const int h = (ty + 1) * L::BXH + tx + 1;
-            const Real nb_cl[6] = {cc[h + 1], cc[h - 1], cc[h + L::BXH], cc[h - L::BXH], cp[h], cm[h]};
-            const Real nb_fs[6] = {fc[h + 1], fc[h - 1], fc[h + L::BXH], fc[h - L::BXH], fp[h], fm[h]};
-            const Real one_m[6] = {i == g.gx ? one_x : (Real)1, i == 1 ? one_x : (Real)1,
-                                   j == g.gy ? one_y : (Real)1, j == 1 ? one_y : (Real)1,
-                                   k == g.gz ? one_z : (Real)1, k == 1 ? one_z : (Real)1};
-            const long long c = (long long)k * g.sz + (long long)j * g.sy + i;
-            const Real oce = sce[ty * L::BXC + tx + 1];
-            const int grc = sgr[ty * L::BXG + tx + 1];
-            const double Td = t_per_plane ? sT[t] : temp_cell(p, a.d.T, c, j, k, ts);
-            const bool interior = i > 1 && i < g.gx && j > 1 && j < g.gy && k > 1 && k < g.gz;
-            Real cen, cl_new, fs_new;
-            int gr_new;
-            cell_update<Real>(q, p, cc[h], fc[h], nb_cl, nb_fs, one_m, interior, oce, grc, Td, a.d.curv, c, cen,
-                              cl_new, fs_new, gr_new);
-            ce[c] = cen;
-            clO[c] = cl_new;
-            fsO[c] = fs_new;
-            if (gr_new != grc) gr[c] = gr_new;
-            // growth.c:163-165 (the FP32 form stores ce - Cinit)
-            if (sizeof(Real) == 8 ? cen < 0 : cen < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
-            solid = gr_new > 0;
+        int solid[CPT];
+        const Real *cm = (const Real *)stage(s0);
+        const Real *cc = (const Real *)stage(s1);
+        const Real *cp = (const Real *)stage(s2);
+        const Real *fm = (const Real *)(stage(s0) + L::CL);
+        const Real *fc = (const Real *)(stage(s1) + L::CL);
+        const Real *fp = (const Real *)(stage(s2) + L::CL);
+        const Real *sce = (const Real *)(stage(s1) + 2 * L::CL);
+        const int *sgr = (const int *)(stage(s1) + 2 * L::CL + L::CE);
+        const Real omz_p = k == g.gz ? one_z : (Real)1, omz_m = k == 1 ? one_z : (Real)1;
+        const bool in_z = k > 1 && k < g.gz;
+        const double Tp = t_per_plane ? sT[t] : 0.0;
+#pragma unroll
+        for (int u = 0; u < CPT; u++) {
+            solid[u] = 0;
+            if (act[u] && ok) {
+                const int h = hh[u];
+                const int i = i0 + tx + DTX * u;
+                const Real nb_cl[6] = {cc[h + 1], cc[h - 1], cc[h + L::BXH], cc[h - L::BXH], cp[h], cm[h]};
+                const Real nb_fs[6] = {fc[h + 1], fc[h - 1], fc[h + L::BXH], fc[h - L::BXH], fp[h], fm[h]};
+                const Real one_m[6] = {omx_p[u], omx_m[u], omy_p, omy_m, omz_p, omz_m};
+                const long long c = crow + i;
+                const Real oce = sce[hcc[u]];
+                const int grc = sgr[hgg[u]];
+                const double Td = t_per_plane ? Tp : temp_cell(p, a.d.T, c, j, k, ts);
+                const bool interior = in_xy[u] && in_z;
+                Real cen, cl_new, fs_new;
+                int gr_new, br;
+                cell_update<Real>(q, p, cc[h], fc[h], nb_cl, nb_fs, one_m, interior, oce, grc, Td, a.d.curv, c,
+                                  cen, cl_new, fs_new, gr_new, br);
+                ce[c] = cen;
+                clO[c] = cl_new;
+                fsO[c] = fs_new;
+                if (gr_new != grc) gr[c] = gr_new;
+                // growth.c:163-165 (the FP32 form stores ce - Cinit)
+                if (sizeof(Real) == 8 ? cen < 0 : cen < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
+                solid[u] = gr_new > 0;
+            }
         }
-        const unsigned word = __ballot_sync(FULL_MASK, solid);
-        if (tx == 0 && j <= g.gy) a.d.solid_bits[((long long)k * (g.gy + 2) + j) * wrow + blockIdx.x] = word;
+#pragma unroll
+        for (int u = 0; u < CPT; u++) {
+            const unsigned word = __ballot_sync(FULL_MASK, solid[u]);
+            const int w = blockIdx.x * CPT + u;
+            if (tx == 0 && jrow && w < g.wpr) a.d.solid_bits[((long long)k * (g.gy + 2) + j) * wrow + w] = word;
+        }
         __syncthreads();
         if (s_abort) {
             // a copy did not land within the bound: report, then wait (again
@@ -791,12 +801,20 @@ __global__ void __launch_bounds__(DTX *DTY, 4) k_diffuse_fs_tma(const __grid_con
             if (tid == 0) issue(t + TS);
             issued = t + TS + 1;
         }
+        // advance the ring
+        s0 = s1;
+        s1 = s2;
+        s2 = (s2 + 1 == TS) ? 0 : s2 + 1;
+        if (s2 == 0) ph2 ^= 1u;
+        crow += g.sz;
     }
 }
 
 // Plain-load variant (used when the driver cannot encode the TMA
-// descriptors): three halo'd planes in a shared ring filled by the threads.
-template <typename Real>
+// descriptors, and for recording runs of the adjoint): three halo'd planes
+// in a shared ring filled by the threads.  REC: also stores, per cell, the
+// branch fs_change took and the curvature it used.
+template <typename Real, bool REC>
 __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchunk)
 {
     Ctl *ctl = a.d.ctl;
@@ -857,14 +875,22 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchun
             const int grc = gr[c];
             const double Td = temp_cell(p, a.d.T, c, j, k, ts);
             Real cen, cl_new, fs_new;
-            int gr_new;
+            int gr_new, br;
             const bool interior = i > 1 && i < g.gx && j > 1 && j < g.gy && k > 1 && k < g.gz;
             cell_update<Real>(q, p, s_cl[sc][ly][lx], s_fs[sc][ly][lx], nb_cl, nb_fs, one_m, interior, ce[c], grc,
-                              Td, a.d.curv, c, cen, cl_new, fs_new, gr_new);
+                              Td, a.d.curv, c, cen, cl_new, fs_new, gr_new, br);
             ce[c] = cen;
             clO[c] = cl_new;
             fsO[c] = fs_new;
             if (gr_new != grc) gr[c] = gr_new;
+            if (REC) {
+                // frozen-CA record of this step (adjoint replay)
+                const long long slot = (long long)(ts - a.d.rec_t0 - 1);
+                if (slot >= 0 && slot < a.d.rec_cap) {
+                    a.d.rec_flags[slot * g.N + c] = (unsigned char)br;
+                    if (p.tip_curv) a.d.rec_curv[slot * g.N + c] = a.d.curv[c];
+                }
+            }
             // growth.c:163-165 (the FP32 form stores ce - Cinit)
             if (sizeof(Real) == 8 ? cen < 0 : cen < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
             solid = gr_new > 0;
@@ -994,8 +1020,14 @@ __global__ void __launch_bounds__(SCAN_NT) k_list_scan(KernelArgs a, int nblocks
 // list cell c, with grow_octahedra's half diagonal (growth.c:372-403)
 // evaluated for the solid neighbour on demand.  Returns the capturing
 // grain id (0 = not captured) and the new octahedron centre.
+//
+// The pre-capture grain ids (ogr) of interior neighbours are read through
+// the solid bitmask (bit set <=> gr > 0 after fs_change), so that ids
+// written by captures of the same launch are never mistaken for them; the
+// gr of a solid cell, and of a halo cell, is not written during capture.
 template <typename Real>
-__device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs, long long c, Dc3 &out)
+__device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs, long long c, long long I,
+                                            long long J, long long K, Dc3 &out)
 {
     const Geo &g = a.g;
     const Phys &p = a.p;
@@ -1011,6 +1043,11 @@ __device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs,
 #pragma unroll 1
     for (int n = 0; n < 6; n++) {
         long long ndx = ndxs[n];
+        const long long In = I + nnx[n], Jn = J + nny[n], Kn = K + nnz[n];
+        if (In >= 1 && In <= g.gx && Jn >= 1 && Jn <= g.gy && Kn >= 1 && Kn <= g.gz) {
+            const unsigned w = a.d.solid_bits[(Kn * (g.gy + 2) + Jn) * (long long)g.wpr + ((In - 1) >> 5)];
+            if (!((w >> ((In - 1) & 31)) & 1u)) continue;
+        }
         int id = gr[ndx];
         if (id > 0 && (unsigned long long)id < p.max_grains) {
             const double *R = a.d.grain_rot + 9 * (long long)id;
@@ -1090,17 +1127,11 @@ __global__ void __launch_bounds__(LIST_NT) k_list_write(KernelArgs a)
     }
 }
 
-__device__ __forceinline__ int rank_of_dev_cell(const Geo &g, long long c)
-{
-    long long K = c / g.sz, J = (c % g.sz) / g.sy, I = c % g.sy;
-    int rx = (int)((I - 1) / g.sbx), ry = (int)((J - 1) / g.sby), rz = (int)((K - 1) / g.sbz);
-    return rx + ry * g.nsbx + rz * g.nsbx * g.nsby;
-}
-
-// Captures every list entry (grid-stride over the whole list, so the work
-// is balanced however the interface is distributed).  Results go to
-// per-slot buffers; k_apply commits them after every capture has read the
-// pre-capture grain ids (the reference's ogr copy, growth.c:635-638).
+// Captures every list entry and commits it at once (grid-stride over the
+// whole list, so the work is balanced however the interface is
+// distributed): dc_tmp slot of a captured entry, then the reference's
+// copy-back dc[cell] = dc_tmp[slot] for every entry, captured or not
+// (growth.c:789, 797-807), and the captured grain id.
 template <typename Real>
 __global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
 {
@@ -1111,30 +1142,24 @@ __global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
     const Real *fs = (const Real *)a.d.fs[(int)(ctl->timestep & 1ULL)];
     for (long long e = blockIdx.x * (long long)LIST_NT + threadIdx.x; e < total; e += (long long)gridDim.x * LIST_NT) {
         const long long c = a.d.list_cell[e];
-        const int r = (g.nranks == 1) ? 0 : rank_of_dev_cell(g, c);
+        const long long K = c / g.sz, J = (c - K * g.sz) / g.sy, I = c - K * g.sz - J * g.sy;
+        int r = 0;
+        if (g.nranks > 1) {
+            const int rx = (int)((I - 1) / g.sbx), ry = (int)((J - 1) / g.sby), rz = (int)((K - 1) / g.sbz);
+            r = rx + ry * g.nsbx + rz * g.nsbx * g.nsby;
+        }
         const int rank_start = a.d.blk_off[(long long)r * g.blocks_per_rank];
+        Dc3 *slot = a.d.dc_tmp + a.d.rank_dcbase[r] + (e - rank_start + 1);
         Dc3 out;
-        const int gid = capture_cell<Real>(a, fs, c, out);
-        if (gid) a.d.dc_tmp[a.d.rank_dcbase[r] + (e - rank_start + 1)] = out;
+        const int gid = capture_cell<Real>(a, fs, c, I, J, K, out);
+        if (gid) {
+            *slot = out;
+            a.d.dc[c] = out;
+            a.d.gr[c] = gid;
+        } else {
+            a.d.dc[c] = *slot;
+        }
         a.d.list_gid[e] = gid;
-    }
-}
-
-__global__ void k_apply(KernelArgs a)
-{
-    const Ctl *ctl = a.d.ctl;
-    if (stalled(ctl)) return;
-    const Geo &g = a.g;
-    const int total = ctl->list_total;
-    for (long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x; pos < total;
-         pos += (long long)gridDim.x * blockDim.x) {
-        long long c = a.d.list_cell[pos];
-        const int r = (g.nranks == 1) ? 0 : rank_of_dev_cell(g, c);
-        int start = a.d.blk_off[(long long)r * g.blocks_per_rank];
-        int slot = (int)pos - start + 1;
-        a.d.dc[c] = a.d.dc_tmp[a.d.rank_dcbase[r] + slot];
-        int gid = a.d.list_gid[pos];
-        if (gid) a.d.gr[c] = gid;
     }
 }
 
@@ -1262,9 +1287,9 @@ __global__ void k_convert(KernelArgs a, int field, int to_device, double *buf)
 }
 
 // ---------------------------------------------------------------- launch
-static int pick_zchunk(const Geo &g)
+static int pick_zchunk(const Geo &g, int tile_x)
 {
-    long long tiles = (long long)((g.gx + DTX - 1) / DTX) * ((g.gy + DTY - 1) / DTY);
+    long long tiles = (long long)((g.gx + tile_x - 1) / tile_x) * ((g.gy + DTY - 1) / DTY);
     // aim for >= 4 CTAs per SM on 148 SMs, chunks of at most 32 planes
     long long want = 148LL * 4;
     int zc = (int)((tiles * g.gz) / want);
@@ -1305,11 +1330,11 @@ static bool encode3d(CUtensorMap *m, CUtensorMapDataType dt, int es, void *base,
               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <typename Real>
+template <typename Real, int CPT>
 static int make_tma_t(const KernelArgs &a, TmaHolder &out)
 {
     static_assert(sizeof(TmaMaps) <= sizeof(out.bytes), "TMA holder too small");
-    using L = Stage<Real>;
+    using L = Stage<Real, CPT>;
     TmaMaps m;
     std::memset(&m, 0, sizeof m);
     const CUtensorMapDataType dt = sizeof(Real) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -1324,22 +1349,60 @@ static int make_tma_t(const KernelArgs &a, TmaHolder &out)
     std::memcpy(out.bytes, &m, sizeof m);
     out.ok = ok ? 1 : 0;
     if (ok) {
-        cudaFuncSetAttribute(k_diffuse_fs_tma<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             Depth<Real>::TS * L::BYTES);
+        cudaFuncSetAttribute(k_diffuse_fs_tma<Real, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             Depth<Real, CPT>::TS * L::BYTES);
     }
     return out.ok;
 }
 
 int make_tma(const KernelArgs &a, int precision, TmaHolder &out)
 {
-    if (precision == MMS_PREC_F32) return make_tma_t<float>(a, out);
-    return make_tma_t<double>(a, out);
+    if (out.cpt != 1 && out.cpt != 2) out.cpt = 1;
+    if (precision == MMS_PREC_F32)
+        return out.cpt == 2 ? make_tma_t<float, 2>(a, out) : make_tma_t<float, 1>(a, out);
+    return out.cpt == 2 ? make_tma_t<double, 2>(a, out) : make_tma_t<double, 1>(a, out);
 }
 
 #define PROF_BEGIN(id) \
     if (prof) prof->begin(id, st)
 #define PROF_END(id) \
     if (prof) prof->end(id, st)
+
+template <typename Real>
+static void launch_stencil_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st)
+{
+    const Geo &g = a.g;
+    const int cpt = (tma.ok && tma.cpt == 2) ? 2 : 1;
+    const int tile_x = DTX * cpt;
+    int zc = tma.zc > 0 ? (tma.zc < g.gz ? tma.zc : g.gz) : pick_zchunk(g, tile_x);
+    if (zc > 64) zc = 64;  // sT holds 64 planes
+    dim3 grid((g.gx + tile_x - 1) / tile_x, (g.gy + DTY - 1) / DTY, (g.gz + zc - 1) / zc);
+    if (a.d.rec_flags) {
+        // recording run: plain-load variant with 32-wide tiles
+        const int zr = pick_zchunk(g, DTX);
+        dim3 gr((g.gx + DTX - 1) / DTX, (g.gy + DTY - 1) / DTY, (g.gz + zr - 1) / zr);
+        k_diffuse_fs<Real, true><<<gr, dim3(DTX, DTY), 0, st>>>(a, zr);
+    } else if (tma.ok) {
+        TmaMaps maps;
+        std::memcpy(&maps, tma.bytes, sizeof maps);
+        if (cpt == 2)
+            k_diffuse_fs_tma<Real, 2><<<grid, dim3(DTX, DTY), Depth<Real, 2>::TS * Stage<Real, 2>::BYTES, st>>>(
+                a, maps, zc);
+        else
+            k_diffuse_fs_tma<Real, 1><<<grid, dim3(DTX, DTY), Depth<Real, 1>::TS * Stage<Real, 1>::BYTES, st>>>(
+                a, maps, zc);
+    } else {
+        k_diffuse_fs<Real, false><<<grid, dim3(DTX, DTY), 0, st>>>(a, zc);
+    }
+}
+
+int launch_stencil(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == MMS_PREC_F32) launch_stencil_t<float>(a, tma, st);
+    else launch_stencil_t<double>(a, tma, st);
+    return 1;
+}
 
 template <typename Real>
 static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st, int start_stage, Profiler *prof)
@@ -1363,20 +1426,10 @@ static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t
         PROF_END(KID_CURV);
         n++;
     }
-    {
-        int zc = pick_zchunk(g);
-        dim3 grid(g.wpr, (g.gy + DTY - 1) / DTY, (g.gz + zc - 1) / zc);
-        PROF_BEGIN(KID_DIFFUSE_FS);
-        if (tma.ok) {
-            TmaMaps maps;
-            std::memcpy(&maps, tma.bytes, sizeof maps);
-            k_diffuse_fs_tma<Real><<<grid, dim3(DTX, DTY), Depth<Real>::TS * Stage<Real>::BYTES, st>>>(a, maps, zc);
-        } else {
-            k_diffuse_fs<Real><<<grid, dim3(DTX, DTY), 0, st>>>(a, zc);
-        }
-        PROF_END(KID_DIFFUSE_FS);
-        n++;
-    }
+    PROF_BEGIN(KID_DIFFUSE_FS);
+    launch_stencil_t<Real>(a, tma, st);
+    PROF_END(KID_DIFFUSE_FS);
+    n++;
     int nblocks = (int)(g.blocks_per_rank * g.nranks);
     PROF_BEGIN(KID_LIST_COUNT);
     k_list_count<<<nblocks, LIST_NT, 0, st>>>(a);
@@ -1390,10 +1443,7 @@ static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t
     PROF_BEGIN(KID_CAPTURE);
     k_capture<Real><<<148 * 8, LIST_NT, 0, st>>>(a);
     PROF_END(KID_CAPTURE);
-    PROF_BEGIN(KID_APPLY);
-    k_apply<<<148 * 4, 256, 0, st>>>(a);
-    PROF_END(KID_APPLY);
-    n += 5;
+    n += 4;
     return n;
 }
 

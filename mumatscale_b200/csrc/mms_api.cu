@@ -119,6 +119,16 @@ struct mms_ctx {
     std::string err;
     size_t bytes = 0;
     std::vector<void *> allocs;
+    // frozen-CA record for the adjoint
+    struct AdjRec {
+        unsigned long long t0 = 0;
+        long long nrec = 0;
+        int every = 0;
+        long long nckpt = 0;
+        unsigned char *flags = nullptr;  // nrec x N
+        double *curv = nullptr;          // nrec x N (TipCurvature)
+        char *ckpt = nullptr;            // nckpt x 3 x N x element size
+    } adj;
 };
 
 namespace {
@@ -489,14 +499,136 @@ mms_status mms_set_profiling(mms_ctx *ctx, int on)
     return MMS_OK;
 }
 
+mms_status mms_set_stencil_tile(mms_ctx *ctx, int cells_per_thread, int zchunk)
+{
+    if (!ctx || (cells_per_thread != 1 && cells_per_thread != 2) || zchunk < 0 || zchunk > 64) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->tma.cpt = cells_per_thread;
+    ctx->tma.zc = zchunk;
+    make_tma(ctx->ka, ctx->prec, ctx->tma);
+    drop_graph(ctx);
+    return MMS_OK;
+}
+
+mms_status mms_get_stencil_tile(const mms_ctx *ctx, int *cells_per_thread, int *zchunk)
+{
+    if (!ctx || !cells_per_thread || !zchunk) return MMS_ERR_ARG;
+    *cells_per_thread = ctx->tma.ok ? ctx->tma.cpt : 1;
+    *zchunk = ctx->tma.zc;
+    return MMS_OK;
+}
+
+// Stencil tile autotuner.  Every candidate (cells per thread x z-chunk) runs
+// the diffusion + fs-change kernel on a shadow of the fields it writes (ce,
+// the next cl and fs, gr, the solid bitmask, the control block), so the
+// domain's state is untouched; the candidate with the lowest median time
+// over `reps` launches is kept.
+mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchunk, double *best_ms)
+{
+    if (!ctx || reps < 1) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status rs0 = read_ctl(ctx);
+    if (rs0) return rs0;
+    const Geo &g = ctx->ka.g;
+    const size_t N = (size_t)g.N;
+    const size_t rs = ctx->prec == MMS_PREC_F32 ? sizeof(float) : sizeof(double);
+    KernelArgs sa = ctx->ka;
+    const int pout = (int)((ctx->h_ctl->timestep + 1) & 1ULL);
+    std::vector<void *> shadow;
+    auto shadow_of = [&](const void *src, size_t bytes, void **dst) -> cudaError_t {
+        cudaError_t e = cudaMalloc(dst, bytes);
+        if (e != cudaSuccess) return e;
+        shadow.push_back(*dst);
+        return cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    };
+    auto release = [&]() {
+        cudaStreamSynchronize(ctx->stream);
+        for (void *q : shadow) cudaFree(q);
+    };
+    void *sce, *scl, *sfs, *sgr, *sbits, *sctl;
+    cudaError_t e;
+    if ((e = shadow_of(sa.d.ce, N * rs, &sce)) || (e = shadow_of(sa.d.cl[pout], N * rs, &scl)) ||
+        (e = shadow_of(sa.d.fs[pout], N * rs, &sfs)) || (e = shadow_of(sa.d.gr, N * sizeof(int), &sgr)) ||
+        (e = shadow_of(sa.d.solid_bits, (size_t)g.nwords * sizeof(unsigned), &sbits)) ||
+        (e = shadow_of(sa.d.ctl, sizeof(Ctl), &sctl))) {
+        release();
+        ctx->err = std::string("autotune shadow buffers: ") + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? MMS_ERR_NOMEM : MMS_ERR_CUDA;
+    }
+    sa.d.ce = sce;
+    sa.d.cl[pout] = scl;
+    sa.d.fs[pout] = sfs;
+    sa.d.gr = (int *)sgr;
+    sa.d.solid_bits = (unsigned *)sbits;
+    sa.d.ctl = (Ctl *)sctl;
+    Ctl c = *ctx->h_ctl;
+    c.timestep += 1;
+    c.status = 0;
+    c.stall = 0;
+    cudaMemcpyAsync(sctl, &c, sizeof c, cudaMemcpyHostToDevice, ctx->stream);
+
+    struct Cand {
+        int cpt, zc;
+    };
+    std::vector<Cand> cands;
+    for (int cpt = 1; cpt <= (ctx->tma.ok ? 2 : 1); cpt++)
+        for (int zc : {0, 8, 16, 32})
+            if (zc <= g.gz) cands.push_back({cpt, zc});
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e300;
+    Cand pick{ctx->tma.cpt, ctx->tma.zc};
+    for (const Cand &cd : cands) {
+        TmaHolder th{};
+        th.cpt = cd.cpt;
+        th.zc = cd.zc;
+        if (ctx->tma.ok && !make_tma(sa, ctx->prec, th)) continue;
+        std::vector<float> ms;
+        for (int r = 0; r < reps + 2; r++) {
+            cudaEventRecord(e0, ctx->stream);
+            launch_stencil(sa, th, ctx->prec, ctx->stream);
+            cudaEventRecord(e1, ctx->stream);
+            cudaEventSynchronize(e1);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (r >= 2) ms.push_back(t);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            release();
+            ctx->err = std::string("autotune launch: ") + cudaGetErrorString(e);
+            return MMS_ERR_CUDA;
+        }
+        std::sort(ms.begin(), ms.end());
+        double med = ms[ms.size() / 2];
+        if (med < best) {
+            best = med;
+            pick = cd;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    release();
+    ctx->tma.cpt = pick.cpt;
+    ctx->tma.zc = pick.zc;
+    make_tma(ctx->ka, ctx->prec, ctx->tma);
+    drop_graph(ctx);
+    if (cells_per_thread) *cells_per_thread = pick.cpt;
+    if (zchunk) *zchunk = pick.zc;
+    if (best_ms) *best_ms = best;
+    return MMS_OK;
+}
+
 int mms_kernel_count(void) { return mms::KID_COUNT; }
 
 const char *mms_kernel_name(int id)
 {
     static const char *names[mms::KID_COUNT] = {"k_temp_am",    "k_nuc",         "k_act",
                                                 "k_curv",       "k_diffuse_fs",  "k_list_count",
-                                                "k_list_scan",  "k_list_write",  "k_capture",
-                                                "k_apply"};
+                                                "k_list_scan",  "k_list_write",  "k_capture"};
     return (id >= 0 && id < mms::KID_COUNT) ? names[id] : "";
 }
 
@@ -1117,6 +1249,263 @@ mms_status mms_run(mms_ctx *ctx, int verbose)
         std::printf("\nSimulation complete.  Shutting down.\n");
         std::fflush(stdout);
     }
+    return MMS_OK;
+}
+
+}  // extern "C"
+
+// ============================================================ adjoint (host)
+namespace {
+
+size_t elem_size(const mms_ctx *ctx) { return ctx->prec == MMS_PREC_F32 ? sizeof(float) : sizeof(double); }
+
+void adj_stop_recording(mms_ctx *ctx)
+{
+    DevPtrs &d = ctx->ka.d;
+    if (d.rec_flags) {
+        d.rec_flags = nullptr;
+        d.rec_curv = nullptr;
+        d.rec_cap = 0;
+        drop_graph(ctx);
+    }
+}
+
+void adj_free(mms_ctx *ctx)
+{
+    adj_stop_recording(ctx);
+    dfree(ctx, ctx->adj.flags);
+    dfree(ctx, ctx->adj.curv);
+    dfree(ctx, ctx->adj.ckpt);
+    ctx->adj = mms_ctx::AdjRec{};
+}
+
+// state slot s of a buffer of 3 x N x es per slot
+char *state_slot(char *base, long long s, int f, size_t N, size_t es) { return base + ((size_t)s * 3 + f) * N * es; }
+
+mms_status adj_save_ckpt(mms_ctx *ctx, long long idx, unsigned long long ts)
+{
+    const size_t N = (size_t)ctx->ka.g.N, es = elem_size(ctx);
+    const int b = (int)(ts & 1ULL);
+    const void *src[3] = {ctx->ka.d.ce, ctx->ka.d.cl[b], ctx->ka.d.fs[b]};
+    for (int f = 0; f < 3; f++)
+        CU(cudaMemcpyAsync(state_slot(ctx->adj.ckpt, idx, f, N, es), src[f], N * es, cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+    return MMS_OK;
+}
+
+// Phys with Dliq, part_coef and the Gibbs-Thomson coefficient scaled, each
+// derived constant computed as mms_create computes it.
+Phys scaled_phys(const mms_ctx *ctx, const double scale[3])
+{
+    const mms_params &p = ctx->p;
+    Phys ph = ctx->ka.p;
+    const double dtx = p.ts_delt / (p.cellSize * p.cellSize);
+    const double Dliq = p.Dliq * scale[0], k = p.part_coef * scale[1];
+    ph.rl = Dliq * dtx;
+    ph.D_xt = (Dliq / p.cellSize / p.cellSize) * p.ts_delt;
+    ph.k_inv = 1.0 / k;
+    ph.km = 1.0 - k;
+    ph.km_inv = 1.0 / ph.km;
+    ph.gibbs = p.gibbs_coef * scale[2];
+    return ph;
+}
+
+}  // namespace
+
+extern "C" {
+
+mms_status mms_adjoint_release(mms_ctx *ctx)
+{
+    if (!ctx) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    adj_free(ctx);
+    return MMS_OK;
+}
+
+mms_status mms_adjoint_record(mms_ctx *ctx, int nsteps, int checkpoint_every)
+{
+    if (!ctx || nsteps < 1 || checkpoint_every < 1) return MMS_ERR_ARG;
+    if (ctx->ka.p.temp_mode == 2) {
+        ctx->err = "the adjoint supports the analytic temperature models only";
+        return MMS_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    if (ctx->h_ctl->status) return (mms_status)ctx->h_ctl->status;
+    adj_free(ctx);
+    const size_t N = (size_t)ctx->ka.g.N, es = elem_size(ctx);
+    mms_ctx::AdjRec &r = ctx->adj;
+    r.t0 = ctx->h_ctl->timestep;
+    r.nrec = nsteps;
+    r.every = checkpoint_every;
+    r.nckpt = (nsteps + checkpoint_every - 1) / checkpoint_every;
+    if ((st = dalloc(ctx, &r.flags, (size_t)nsteps * N)) ||
+        (ctx->p.tip_curv && (st = dalloc(ctx, &r.curv, (size_t)nsteps * N))) ||
+        (st = dalloc(ctx, &r.ckpt, (size_t)r.nckpt * 3 * N * es))) {
+        adj_free(ctx);
+        return st;
+    }
+    if ((st = adj_save_ckpt(ctx, 0, r.t0))) return st;
+    DevPtrs &d = ctx->ka.d;
+    d.rec_flags = r.flags;
+    d.rec_curv = r.curv;
+    d.rec_t0 = r.t0;
+    d.rec_cap = nsteps;
+    drop_graph(ctx);
+    long long done = 0;
+    while (done < nsteps) {
+        int n = (int)std::min<long long>(checkpoint_every, nsteps - done);
+        if ((st = mms_step(ctx, n))) {
+            adj_free(ctx);
+            return st;
+        }
+        done += n;
+        if (done < nsteps && (st = adj_save_ckpt(ctx, done / checkpoint_every, r.t0 + done))) return st;
+    }
+    adj_stop_recording(ctx);
+    CU(cudaStreamSynchronize(ctx->stream));
+    return MMS_OK;
+}
+
+mms_status mms_adjoint_replay_loss(mms_ctx *ctx, const double *target_ce, const double scale[3], double *loss)
+{
+    if (!ctx || !target_ce || !scale || !loss) return MMS_ERR_ARG;
+    if (!ctx->adj.nrec) return MMS_ERR_STATE;
+    cudaSetDevice(ctx->device);
+    const Geo &g = ctx->ka.g;
+    const size_t N = (size_t)g.N, es = elem_size(ctx);
+    const mms_ctx::AdjRec &r = ctx->adj;
+    const Phys ph = scaled_phys(ctx, scale);
+    char *buf = nullptr;
+    double *tgt = nullptr, *partial = nullptr, *dl = nullptr;
+    mms_status st;
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(ctx->stream);
+        dfree(ctx, buf);
+        dfree(ctx, tgt);
+        dfree(ctx, partial);
+        dfree(ctx, dl);
+    };
+    if ((st = dalloc(ctx, &buf, 2 * 3 * N * es)) || (st = dalloc(ctx, &tgt, N)) ||
+        (st = dalloc(ctx, &partial, (size_t)adj_nblocks(g))) || (st = dalloc(ctx, &dl, 1))) {
+        cleanup();
+        return st;
+    }
+    cudaError_t e = copy_in(ctx, tgt, target_ce, sizeof(double));
+    for (int b = 0; b < 2 && e == cudaSuccess; b++)
+        for (int f = 0; f < 3 && e == cudaSuccess; f++)
+            e = cudaMemcpyAsync(state_slot(buf, b, f, N, es), state_slot(r.ckpt, 0, f, N, es), N * es,
+                                cudaMemcpyDeviceToDevice, ctx->stream);
+    int cur = 0;
+    for (long long s = 0; s < r.nrec && e == cudaSuccess; s++) {
+        const void *x0[3] = {state_slot(buf, cur, 0, N, es), state_slot(buf, cur, 1, N, es),
+                             state_slot(buf, cur, 2, N, es)};
+        void *x1[3] = {state_slot(buf, 1 - cur, 0, N, es), state_slot(buf, 1 - cur, 1, N, es),
+                       state_slot(buf, 1 - cur, 2, N, es)};
+        launch_replay(g, ph, ctx->prec, x0, x1, r.flags + (size_t)s * N, r.curv ? r.curv + (size_t)s * N : nullptr,
+                      r.t0 + s + 1, ctx->stream);
+        cur = 1 - cur;
+    }
+    const double off = ctx->prec == MMS_PREC_F32 ? ctx->p.Cinit : 0.0;
+    if (e == cudaSuccess) {
+        launch_adj_terminal(g, ctx->prec, off, state_slot(buf, cur, 0, N, es), tgt, nullptr, nullptr, nullptr,
+                            partial, dl, ctx->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(loss, dl, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cleanup();
+    if (e != cudaSuccess) {
+        ctx->err = std::string("adjoint replay: ") + cudaGetErrorString(e);
+        return MMS_ERR_CUDA;
+    }
+    return MMS_OK;
+}
+
+mms_status mms_adjoint_gradient(mms_ctx *ctx, const double *target_ce, mms_adjoint_result *out)
+{
+    if (!ctx || !target_ce || !out) return MMS_ERR_ARG;
+    if (!ctx->adj.nrec) return MMS_ERR_STATE;
+    cudaSetDevice(ctx->device);
+    const Geo &g = ctx->ka.g;
+    const size_t N = (size_t)g.N, es = elem_size(ctx);
+    const mms_ctx::AdjRec &r = ctx->adj;
+    const Phys &ph = ctx->ka.p;
+    const int nb = adj_nblocks(g);
+    char *seg = nullptr, *lam = nullptr;
+    double *tgt = nullptr, *partial = nullptr, *acc = nullptr;
+    mms_status st;
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(ctx->stream);
+        dfree(ctx, seg);
+        dfree(ctx, lam);
+        dfree(ctx, tgt);
+        dfree(ctx, partial);
+        dfree(ctx, acc);
+    };
+    // acc: ADJ_SLOTS gradient sums, then the loss
+    if ((st = dalloc(ctx, &seg, (size_t)(r.every + 1) * 3 * N * es)) || (st = dalloc(ctx, &lam, 6 * N * es)) ||
+        (st = dalloc(ctx, &tgt, N)) || (st = dalloc(ctx, &partial, (size_t)nb * ADJ_SLOTS)) ||
+        (st = dalloc(ctx, &acc, ADJ_SLOTS + 1))) {
+        cleanup();
+        return st;
+    }
+    // adjoint buffers: lce, lcl[2], lfs[2], nu
+    char *lce = lam, *lcl[2] = {lam + N * es, lam + 2 * N * es}, *lfs[2] = {lam + 3 * N * es, lam + 4 * N * es},
+         *nu = lam + 5 * N * es;
+    cudaError_t e = copy_in(ctx, tgt, target_ce, sizeof(double));
+    const double off = ctx->prec == MMS_PREC_F32 ? ctx->p.Cinit : 0.0;
+    int lc = 0;
+    for (long long sg = r.nckpt - 1; sg >= 0 && e == cudaSuccess; sg--) {
+        const long long s0 = sg * r.every, s1 = std::min<long long>(s0 + r.every, r.nrec), L = s1 - s0;
+        // every slot starts as the checkpoint (halo cells never change)
+        for (long long l = 0; l <= L && e == cudaSuccess; l++)
+            for (int f = 0; f < 3 && e == cudaSuccess; f++)
+                e = cudaMemcpyAsync(state_slot(seg, l, f, N, es), state_slot(r.ckpt, sg, f, N, es), N * es,
+                                    cudaMemcpyDeviceToDevice, ctx->stream);
+        for (long long l = 0; l < L; l++) {
+            const void *x0[3] = {state_slot(seg, l, 0, N, es), state_slot(seg, l, 1, N, es),
+                                 state_slot(seg, l, 2, N, es)};
+            void *x1[3] = {state_slot(seg, l + 1, 0, N, es), state_slot(seg, l + 1, 1, N, es),
+                           state_slot(seg, l + 1, 2, N, es)};
+            const size_t s = (size_t)(s0 + l);
+            launch_replay(g, ph, ctx->prec, x0, x1, r.flags + s * N, r.curv ? r.curv + s * N : nullptr,
+                          r.t0 + s + 1, ctx->stream);
+        }
+        if (sg == r.nckpt - 1)
+            launch_adj_terminal(g, ctx->prec, off, state_slot(seg, L, 0, N, es), tgt, lce, lcl[lc], lfs[lc],
+                                partial, acc + ADJ_SLOTS, ctx->stream);
+        for (long long l = L - 1; l >= 0; l--) {
+            const void *x0[3] = {state_slot(seg, l, 0, N, es), state_slot(seg, l, 1, N, es),
+                                 state_slot(seg, l, 2, N, es)};
+            const size_t s = (size_t)(s0 + l);
+            launch_adj_step(g, ph, ctx->prec, x0, state_slot(seg, l + 1, 0, N, es), r.flags + s * N,
+                            r.curv ? r.curv + s * N : nullptr, lce, lcl[lc], lfs[lc], lcl[1 - lc], lfs[1 - lc], nu,
+                            partial, acc, r.t0 + s + 1, ctx->stream);
+            lc = 1 - lc;
+        }
+        if (e == cudaSuccess) e = cudaGetLastError();
+    }
+    double h[ADJ_SLOTS + 1] = {};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cleanup();
+    if (e != cudaSuccess) {
+        ctx->err = std::string("adjoint: ") + cudaGetErrorString(e);
+        return MMS_ERR_CUDA;
+    }
+    // chain rule to the deck parameters: rl = Dliq dt/dx^2, D_xt = Dliq/dx/dx dt,
+    // km = 1 - k, km_inv = 1/(1 - k), k_inv = 1/k
+    const mms_params &p = ctx->p;
+    const double dtx = p.ts_delt / (p.cellSize * p.cellSize);
+    const double k = p.part_coef, km = 1.0 - k;
+    out->loss = h[ADJ_SLOTS];
+    out->dL_dDliq = (h[0] + h[1]) * dtx;
+    out->dL_dpart_coef = -h[2] + h[3] / (km * km) - h[4] / (k * k);
+    out->dL_dgibbs = h[5];
+    out->steps = r.nrec;
     return MMS_OK;
 }
 

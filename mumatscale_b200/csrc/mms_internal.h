@@ -172,6 +172,22 @@ struct DevPtrs {
     // reductions
     double *red;            // scratch for partial sums
     Ctl *ctl;
+    // frozen-CA record for the adjoint (null when not recording): per step
+    // slot s (timestep rec_t0 + 1 + s), the fs_change branch of every cell
+    // and, with TipCurvature, the curvature it used
+    unsigned char *rec_flags;
+    double *rec_curv;
+    unsigned long long rec_t0;
+    long long rec_cap;
+};
+
+// fs_change_diffuse branches (growth.c:228-272), as recorded for the adjoint
+enum Branch : int {
+    BR_RESET = 0,  // liquid / out of range: cl = ce, fs = 0
+    BR_KEEP = 1,   // fully solid below liquidus: cl = ce / k
+    BR_GROW = 2,   // growth update
+    BR_CLAMP = 3,  // growth update with fs clamped to 1
+    BR_NEG = 4     // growth update gave fs < 0: cl = ce, fs = 0
 };
 
 struct KernelArgs {
@@ -183,13 +199,15 @@ struct KernelArgs {
 // Kernel ids for per-kernel timing.
 enum KernelId : int {
     KID_TEMP_AM = 0, KID_NUC, KID_ACT, KID_CURV, KID_DIFFUSE_FS, KID_LIST_COUNT, KID_LIST_SCAN,
-    KID_LIST_WRITE, KID_CAPTURE, KID_APPLY, KID_COUNT
+    KID_LIST_WRITE, KID_CAPTURE, KID_COUNT
 };
 
 // Opaque storage for the stencil's TMA descriptors (built in kernels.cu).
 struct TmaHolder {
     alignas(128) unsigned char bytes[6 * 128];
     int ok;
+    int cpt = 1;  // stencil tile: cells per thread along x (1 or 2)
+    int zc = 0;   // stencil z-chunk (0: chosen from the grid size)
 };
 
 // Optional event bracketing of each launch (mms_set_profiling).
@@ -208,6 +226,8 @@ int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *
 // returns 0 when the driver cannot encode them (the stencil then uses its
 // plain-load variant).
 int make_tma(const KernelArgs &a, int precision, TmaHolder &out);
+// the diffusion + fs-change stencil alone (tile autotuning)
+int launch_stencil(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream);
 int launch_temp_am(const KernelArgs &a, void *stream, Profiler *prof, double lsd, double lv, double lhs, double lab,
                    double lpow, double liniT, double lthcon, double rho_cp, double x0, double y0,
                    double z0, int amtracks, int nsbx_times_sbx);
@@ -217,5 +237,18 @@ int launch_compute_d(const KernelArgs &a, int precision, double *dev_out, void *
 int launch_mask_captured(const KernelArgs &a, void *dev, int is_double, void *stream);
 int launch_convert(const KernelArgs &a, int precision, int field, int to_device, double *dev_f64,
                    void *stream);
+
+// Frozen-CA replay and adjoint (adjoint.cu).  x0/x1: (ce, cl, fs) of one
+// state; ts: the timestep of the step being replayed or differentiated.
+constexpr int ADJ_SLOTS = 6;  // gradient slots: rl, D_xt, km, km_inv, k_inv, gibbs
+int adj_nblocks(const Geo &g);
+int launch_replay(const Geo &g, const Phys &p, int precision, const void *const x0[3], void *const x1[3],
+                  const unsigned char *flags, const double *curv, unsigned long long ts, void *stream);
+int launch_adj_step(const Geo &g, const Phys &p, int precision, const void *const x0[3], const void *ce1,
+                    const unsigned char *flags, const double *curv, void *lce, const void *lcl1, const void *lfs1,
+                    void *lcl0, void *lfs0, void *nu, double *partial, double *grad, unsigned long long ts,
+                    void *stream);
+int launch_adj_terminal(const Geo &g, int precision, double cinit_off, const void *ce, const double *target,
+                        void *lce, void *lcl, void *lfs, double *partial, double *loss_out, void *stream);
 
 }  // namespace mms

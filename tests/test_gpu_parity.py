@@ -163,3 +163,40 @@ def test_site_and_orientation_injection(built, cuda_device):
             dom.step(100)
             assert mismatches(state_digests(dom), state_digests(o)) == []
         assert dom.num_grains > 5
+
+
+@pytest.mark.parametrize("tile", [(2, 0), (1, 8), (2, 5), (1, 64)])
+@pytest.mark.parametrize("name", ["small4", "grad1", "curv1"])
+def test_stencil_tiles_bit_exact(built, cuda_device, name, tile):
+    """Every stencil tile (cells per thread, z-chunk) gives the reference's
+    state bit for bit."""
+    rec = golden(name)
+    p = M.read_deck(golden_deck(name))
+    with M.Domain(p, precision=M.PREC_F64) as dom:
+        dom.set_stencil_tile(*tile)
+        assert dom.stencil_tile() == tile
+        last = 0
+        for s, want in list(rec["steps"].items())[:4]:
+            s = int(s)
+            dom.step(s - last)
+            last = s
+            bad = mismatches(state_digests(dom), want["digest"])
+            assert not bad, f"{name} tile {tile} step {s}: {bad}"
+
+
+@pytest.mark.parametrize("prec", [M.PREC_F64, M.PREC_F32])
+def test_autotune_leaves_state(built, cuda_device, prec):
+    """The tuner times candidates on shadow buffers: the state, and every
+    later step, are what they would have been without it."""
+    p = M.read_deck(golden_deck("small4"))
+    with M.Domain(p, precision=prec) as a, M.Domain(p, precision=prec) as b:
+        a.step(60)
+        b.step(60)
+        before = state_digests(a)
+        cpt, zc, ms = a.autotune(reps=3)
+        assert cpt in (1, 2) and 0 <= zc <= 64 and ms > 0
+        assert a.stencil_tile() == (cpt, zc)
+        assert mismatches(state_digests(a), before) == []
+        a.step(60)
+        b.step(60)
+        assert mismatches(state_digests(a), state_digests(b)) == []
