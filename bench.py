@@ -387,22 +387,235 @@ def gpu_arm(args) -> None:
 
 
 def profile_arm(args) -> None:
-    """Workload for ncu captures: the same deck, one form, W + K steps, no
-    timing, no CPU baseline.  Usage:
+    """Workload for ncu captures: one form, W + K steps, no timing, no CPU
+    baseline.  --workload ds256 (default): the headline deck with --cells
+    per edge; --workload am: the AM melt-pool deck scaled by --cells/256
+    (x: 2 --cells, y: --cells, z: --cells/2) with its substrate.  Usage:
         ncu ... python bench.py --profile f64 --warmup 3 --steps 2"""
     import mumatscale_b200 as M
     td = tempfile.mkdtemp()
     deck = Path(td) / "bench.in"
-    deck.write_text(deck_text(n=args.cells))
-    params = M.read_deck(deck)
-    dom = M.Domain(params, precision=M.PREC_F32 if args.profile == "f32" else M.PREC_F64)
+    prec = M.PREC_F32 if args.profile == "f32" else M.PREC_F64
+    if args.workload == "am":
+        from mumatscale_b200 import workloads as W
+        dims = (2 * args.cells, args.cells, args.cells // 2)
+        deck.write_text(W.am_track(dims, 1e-6))
+        dom = M.Domain(M.read_deck(deck), precision=prec)
+        W.setup_substrate(dom, dims[2] - 8, 1e-6)
+        ncell = dims[0] * dims[1] * dims[2]
+    else:
+        deck.write_text(deck_text(n=args.cells))
+        dom = M.Domain(M.read_deck(deck), precision=prec)
+        ncell = args.cells ** 3
     if args.tile != "auto":
         cpt, zc = (int(v) for v in args.tile.split(","))
         dom.set_stencil_tile(cpt, zc)
     dom.step(args.warmup + args.steps)
-    print(json.dumps({"profile": args.profile, "cells": args.cells ** 3, "steps": args.warmup + args.steps,
-                      "grains": dom.num_grains, "tma": dom.uses_tma, "tile": dom.stencil_tile()}))
+    print(json.dumps({"profile": args.profile, "workload": args.workload, "cells": ncell,
+                      "steps": args.warmup + args.steps, "grains": dom.num_grains, "tma": dom.uses_tma,
+                      "tile": dom.stencil_tile()}))
     dom.close()
+
+
+def adjoint_workload(args) -> None:
+    """Adjoint calibration: the one-grain deck at 128^3, 2000 steps recorded
+    with checkpoints every 100; target ce from the same deck with D_l x 1.2
+    and k x 0.9; gradient of 1/2 |ce - target|^2 w.r.t. (D_l, k, Gibbs-
+    Thomson) by the FP64 and the FP32 adjoint, and central differences
+    (step 1e-4 relative) of the FP64 frozen replay.  Prints one JSON line."""
+    import torch
+    import mumatscale_b200 as M
+    from mumatscale_b200 import workloads as W
+    n, steps, every, h = args.cells if args.cells != N_CELL else 128, 2000, 100, 1e-4
+    deck, cells, thr, rot = W.one_grain(n)
+    td = tempfile.mkdtemp()
+    f = Path(td) / "adj.in"
+    f.write_text(deck)
+    p = M.read_deck(f)
+    pt = M.read_deck(f)
+    pt.Dliq *= 1.2
+    pt.part_coef *= 0.9
+    with M.Domain(pt) as d:
+        W.setup_one_grain(d, cells, thr, rot)
+        d.step(steps)
+        target = d.download("ce")
+    base = {"Dliq": p.Dliq, "part_coef": p.part_coef, "gibbs": p.gibbs_coef}
+    out = {}
+    for form, prec in (("f64", M.PREC_F64), ("f32", M.PREC_F32)):
+        with M.Domain(p, precision=prec) as dom:
+            W.setup_one_grain(dom, cells, thr, rot)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            dom.adjoint_record(steps, every)
+            t1 = time.perf_counter()
+            g = dom.adjoint_gradient(target)
+            t2 = time.perf_counter()
+            rec = {"loss": g["loss"], "dlogtheta": {k: g[k] * base[k] for k in base},
+                   "forward_record_s": t1 - t0, "gradient_s": t2 - t1,
+                   "grains": dom.num_grains, "fs_fraction": dom.reduce("fs_fraction")}
+            if form == "f64":
+                fd = {}
+                t3 = time.perf_counter()
+                for i, k in enumerate(base):
+                    up, dn = [1.0] * 3, [1.0] * 3
+                    up[i] += h
+                    dn[i] -= h
+                    fd[k] = (dom.adjoint_replay_loss(target, up) - dom.adjoint_replay_loss(target, dn)) / (2 * h)
+                rec["fd"] = fd
+                rec["fd_s"] = time.perf_counter() - t3
+            out[form] = rec
+    f64, f32 = out["f64"], out["f32"]
+    big = max(abs(v) for v in f64["dlogtheta"].values())
+    rel = {k: abs(f64["dlogtheta"][k] - f64["fd"][k]) / max(abs(f64["fd"][k]), 1e-6 * big) for k in base}
+    rel32 = {k: abs(f32["dlogtheta"][k] - f64["dlogtheta"][k]) / max(abs(f64["dlogtheta"][k]), 1e-6 * big)
+             for k in base}
+    cells_n = n ** 3
+    line = {"workload": f"adjoint calibration, one grain, {n}^3 cells, {steps} steps, checkpoints every {every}",
+            "metric": "dL/dlog(theta) agreement; adjoint cell-updates/s", "data": "synthetic",
+            "fp64": f64, "fp32": f32, "adjoint_vs_fd_rel": rel, "fp32_vs_fp64_rel": rel32,
+            "fd_step_rel": h,
+            "gradient_cell_updates_per_s": {"f64": cells_n * steps / f64["gradient_s"],
+                                            "f32": cells_n * steps / f32["gradient_s"]}}
+    print(json.dumps(line))
+
+
+def am_workload(args) -> None:
+    """AM single-track melt pool, 512 x 256 x 128 cells, dx = 1 um, substrate
+    of columnar grains (mean width 20 um): FP64 plain form and FP32 form
+    cell-updates/s, K timed steps after W, inputs resident in HBM.  The
+    reference's quadrature temperature is part of every step.  Prints one
+    JSON line."""
+    import torch
+    import mumatscale_b200 as M
+    from mumatscale_b200 import workloads as W
+    dims, dx = (512, 256, 128), 1e-6
+    td = tempfile.mkdtemp()
+    f = Path(td) / "am.in"
+    f.write_text(W.am_track(dims, dx))
+    p = M.read_deck(f)
+    cells = dims[0] * dims[1] * dims[2]
+    K, Wm = args.steps, args.warmup
+    stream = torch.cuda.current_stream()
+    out = {}
+    for form, prec in (("f64", M.PREC_F64), ("f32", M.PREC_F32)):
+        dom = M.Domain(p, precision=prec)
+        dom.set_stream(stream.cuda_stream)
+        ng = W.setup_substrate(dom, dims[2] - 8, dx)
+        tile = dom.autotune(reps=3)
+        dom.step(Wm)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            e0.record(stream)
+            dom.step(K)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        dom.set_profiling(True)
+        dom.step(K)
+        torch.cuda.synchronize()
+        ks = dom.kernel_stats()
+        dom.set_profiling(False)
+        tot = sum(v[0] for v in ks.values())
+        out[form] = {"value": cells * K / (ms / 1e3), "ms_per_step": ms / K,
+                     "temperature_share": ks["k_temp_am"][0] / tot if tot else None,
+                     "kernel_ms_per_step": {k: v[0] / K for k, v in ks.items() if v[1]},
+                     "substrate_grains": ng, "grains": dom.num_grains, "fs_fraction": dom.reduce("fs_fraction"),
+                     "tile": list(tile[:2]), "clocks": clk.summary()}
+        dom.close()
+    line = {"workload": "AM single-track melt pool, 512x256x128 cells, dx 1 um, columnar substrate",
+            "metric": UNIT, "unit": UNIT, "steps": K, "warmup": Wm, "data": "synthetic",
+            "f64": out["f64"], "f32": out["f32"], "ratio_f32_vs_f64": out["f32"]["value"] / out["f64"]["value"]}
+    print(json.dumps(line))
+
+
+def ensemble_workload(args) -> None:
+    """64 independent domains (edges from {32,48,64,96,128} per axis, cooling
+    10-1000 K/s, nucleation 1e11-1e14 m^-3, seeded) in the FP32 form, stepped
+    as one batch (one graph per step, one persistent stencil launch, tile
+    autotuned) for 3000 steps; beside it (N=1) the same domains stepped one
+    after another with mms_step.  Under torchrun the domains are dealt to
+    the ranks (domain i to rank i mod N): no collective on the data path,
+    timing is the max over ranks.  Rank 0 prints one JSON line."""
+    import torch
+    import mumatscale_b200 as M
+    from mumatscale_b200 import workloads as W
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    decks = W.ensemble(64)
+    td = Path(tempfile.mkdtemp())
+    ps_all = []
+    for i, d in enumerate(decks):
+        f = td / f"e{i}.in"
+        f.write_text(d)
+        ps_all.append(M.read_deck(f))
+    ps = ps_all[rank::ws]
+    cells_all = sum(p.gsdimx * p.gsdimy * p.gsdimz for p in ps_all)
+    steps = 3000 if args.steps == 200 else args.steps
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    with M.Batch(ps, precision=M.PREC_F32, device=dev) as b:
+        tune = b.autotune(reps=3)
+        b.step(args.warmup)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.step(steps)
+        torch.cuda.synchronize()
+        sec = max_over_ranks(time.perf_counter() - t0)
+        barrier()
+        grains = sum(d.num_grains - 1 for d in b.domains)
+        tile = b.stencil_tile()
+        launches = b.kernel_launches
+    seq = None
+    if ws == 1:
+        # the same domains one after another (each its own graph), fewer steps
+        seq_steps = min(steps, 300)
+        doms = [M.Domain(p, precision=M.PREC_F32) for p in ps]
+        for d in doms:
+            d.step(args.warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for d in doms:
+            d.step(seq_steps)
+        torch.cuda.synchronize()
+        seq = {"value": cells_all * seq_steps / (time.perf_counter() - t0), "steps": seq_steps}
+        for d in doms:
+            d.close()
+    if rank == 0:
+        line = {"workload": "ensemble of 64 independent domains, edges {32,48,64,96,128}, FP32 form",
+                "metric": UNIT, "unit": UNIT, "value": cells_all * steps / sec, "n_gpus": ws, "steps": steps,
+                "warmup": args.warmup, "cells_total": cells_all, "ms_per_step": sec * 1e3 / steps,
+                "scaling": "strong", "data": "synthetic",
+                "tile": {"cells_per_thread": tile[0], "zchunk": tile[1], "persistent_ctas": tile[2],
+                         "tuned_stencil_ms": tune[2]},
+                "grains_rank0": grains, "kernel_launches_per_step": launches / max(1, steps + args.warmup),
+                "sequential_domains": seq,
+                "timing": "host clock around synchronised runs of device-resident steps, max over ranks"}
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def reference_arm(args) -> None:
@@ -438,11 +651,21 @@ def main() -> None:
                     help="run the workload for an ncu capture only")
     ap.add_argument("--cells", type=int, default=N_CELL, help="edge of the cubic domain (profile mode)")
     ap.add_argument("--tile", default="auto", help="profile mode: stencil tile 'cells_per_thread,zchunk'")
+    ap.add_argument("--workload", default="ds256", choices=["ds256", "adjoint", "am", "ensemble"],
+                    help="ds256: the headline directional-solidification run (default); adjoint, am, "
+                         "ensemble: the adjoint calibration, AM melt-pool and batched-ensemble workloads "
+                         "(each its own JSON line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.profile:
         profile_arm(args)
+    elif args.workload == "adjoint" and args.impl != "reference":
+        adjoint_workload(args)
+    elif args.workload == "am" and args.impl != "reference":
+        am_workload(args)
+    elif args.workload == "ensemble" and args.impl != "reference":
+        ensemble_workload(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:

@@ -246,6 +246,13 @@ mms_status mms_set_sites(mms_ctx *ctx, int64_t n, const int32_t *gxyz,
 mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxyz,
                                      const double *rotmat9);
 
+/* A pre-filled microstructure (for example a substrate of columnar grains):
+ * defines grains 1..n with the given row-major rotation matrices, so that
+ * nucleated grains continue from id n+1.  Only before the first step; the
+ * caller then uploads gr (ids 1..n), fs and the concentrations of the
+ * cells those grains fill.  Their grain records carry no nucleus. */
+mms_status mms_set_grains(mms_ctx *ctx, int n, const double *rotmat9);
+
 /* ---- grain table and results ----------------------------------------------- */
 
 mms_status mms_get_grains(mms_ctx *ctx, int first, int count, mms_grain *out);
@@ -284,6 +291,31 @@ mms_status mms_get_stencil_tile(const mms_ctx *ctx, int *cells_per_thread, int *
  * writes (the domain's state is left as it was), keeps the fastest by median
  * of `reps` launches and returns it (any output pointer may be NULL). */
 mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchunk, double *best_ms);
+
+/* ---- batched independent domains --------------------------------------------- */
+
+/* No counterpart in the reference.  n independent domains (each its own
+ * deck: sizes, cooling, nucleation) stepped together on one device: per
+ * step one CUDA graph with every domain's nucleation, activation, list and
+ * capture as parallel branches and one persistent stencil launch over the
+ * tiles of all domains.  All params[i] must share precision and device.
+ * Each domain's state is exactly what mms_step would give it alone. */
+typedef struct mms_batch mms_batch;
+mms_status mms_batch_create(int n, const mms_params *params, mms_batch **out);
+mms_status mms_batch_destroy(mms_batch *b);
+int mms_batch_size(const mms_batch *b);
+/* The i-th domain's context, for uploads, downloads, reductions and grain
+ * records (not for mms_step while it belongs to the batch). */
+mms_ctx *mms_batch_domain(mms_batch *b, int i);
+mms_status mms_batch_step(mms_batch *b, int nsteps);
+/* Stencil tile of the persistent launch (as mms_set_stencil_tile). */
+mms_status mms_batch_set_stencil_tile(mms_batch *b, int cells_per_thread, int zchunk);
+mms_status mms_batch_get_stencil_tile(const mms_batch *b, int *cells_per_thread, int *zchunk, int *grid);
+/* Times the persistent stencil for every tile candidate on shadows of the
+ * fields it writes and keeps the fastest. */
+mms_status mms_batch_autotune(mms_batch *b, int reps, int *cells_per_thread, int *zchunk, double *best_ms);
+uint64_t mms_batch_kernel_launches(const mms_batch *b);
+const char *mms_batch_last_error(const mms_batch *b);
 
 /* ---- adjoint (frozen cellular automaton) -------------------------------------- */
 

@@ -179,6 +179,17 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_adjoint_gradient": (I, [P, P, C.POINTER(AdjointResult)]),
         "mms_adjoint_replay_loss": (I, [P, P, C.POINTER(D), C.POINTER(D)]),
         "mms_adjoint_release": (I, [P]),
+        "mms_set_grains": (I, [P, I, P]),
+        "mms_batch_create": (I, [I, C.POINTER(Params), C.POINTER(P)]),
+        "mms_batch_destroy": (I, [P]),
+        "mms_batch_size": (I, [P]),
+        "mms_batch_domain": (P, [P, I]),
+        "mms_batch_step": (I, [P, I]),
+        "mms_batch_set_stencil_tile": (I, [P, I, I]),
+        "mms_batch_get_stencil_tile": (I, [P, C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
+        "mms_batch_autotune": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(D)]),
+        "mms_batch_kernel_launches": (C.c_uint64, [P]),
+        "mms_batch_last_error": (C.c_char_p, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -388,6 +399,11 @@ class Domain:
         _check(_lib().mms_set_sites(self._ctx, len(t), g.ctypes.data, t.ctypes.data),
                "mms_set_sites", self._ctx)
 
+    def set_grains(self, rotmats: np.ndarray) -> None:
+        """Grains 1..n of a pre-filled microstructure (row-major 3x3 rotations)."""
+        r = np.ascontiguousarray(rotmats, dtype=np.float64).reshape(-1, 9)
+        _check(_lib().mms_set_grains(self._ctx, len(r), r.ctypes.data), "mms_set_grains", self._ctx)
+
     def set_site_orientations(self, gxyz: np.ndarray, rotmats: np.ndarray) -> None:
         g = np.ascontiguousarray(gxyz, dtype=np.int32).reshape(-1, 3)
         r = np.ascontiguousarray(rotmats, dtype=np.float64).reshape(-1, 9)
@@ -405,3 +421,83 @@ class Domain:
         path = csv_path.encode() if csv_path else None
         _check(_lib().mms_output_grains(self._ctx, path, C.byref(s)), "mms_output_grains", self._ctx)
         return s
+
+
+class _BatchDomain(Domain):
+    """A domain owned by a Batch: fields, reductions and grains, no stepping."""
+
+    def __init__(self, batch: "Batch", ctx, params: Params):
+        self._ctx = ctx
+        self._batch = batch
+        self.params = params
+        self.shape = tuple(x + 2 for x in params.grid)
+
+    def close(self) -> None:  # owned by the batch
+        self._ctx = None
+
+    def step(self, n: int = 1) -> None:
+        raise MmsError(10, "step", "a batched domain steps with its Batch")
+
+
+class Batch:
+    """Many independent domains stepped together (mms_batch_*): one CUDA graph
+    per step with a single persistent stencil launch over all domains."""
+
+    def __init__(self, params: list, precision: int = PREC_F64, device: int = 0):
+        arr = (Params * len(params))()
+        for i, p in enumerate(params):
+            C.memmove(C.byref(arr[i]), C.byref(p), C.sizeof(Params))
+            arr[i].precision = precision
+            arr[i].device = device
+        h = C.c_void_p()
+        _check(_lib().mms_batch_create(len(params), arr, C.byref(h)), "mms_batch_create")
+        self._b = h
+        self.domains = [_BatchDomain(self, C.c_void_p(_lib().mms_batch_domain(h, i)), arr[i])
+                        for i in range(len(params))]
+
+    def __len__(self) -> int:
+        return len(self.domains)
+
+    def _chk(self, st: int, where: str) -> None:
+        if st != 0:
+            raise MmsError(st, where, (_lib().mms_batch_last_error(self._b) or b"").decode())
+
+    def step(self, n: int = 1) -> None:
+        self._chk(_lib().mms_batch_step(self._b, n), "mms_batch_step")
+
+    def set_stencil_tile(self, cells_per_thread: int, zchunk: int = 0) -> None:
+        self._chk(_lib().mms_batch_set_stencil_tile(self._b, cells_per_thread, zchunk), "mms_batch_set_stencil_tile")
+
+    def stencil_tile(self) -> tuple[int, int, int]:
+        c, z, g = C.c_int(), C.c_int(), C.c_int()
+        self._chk(_lib().mms_batch_get_stencil_tile(self._b, C.byref(c), C.byref(z), C.byref(g)),
+                  "mms_batch_get_stencil_tile")
+        return c.value, z.value, g.value
+
+    def autotune(self, reps: int = 3) -> tuple[int, int, float]:
+        c, z, ms = C.c_int(), C.c_int(), C.c_double()
+        self._chk(_lib().mms_batch_autotune(self._b, reps, C.byref(c), C.byref(z), C.byref(ms)), "mms_batch_autotune")
+        return c.value, z.value, ms.value
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(_lib().mms_batch_kernel_launches(self._b))
+
+    def close(self) -> None:
+        if self._b:
+            for d in self.domains:
+                d.close()
+            _lib().mms_batch_destroy(self._b)
+            self._b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

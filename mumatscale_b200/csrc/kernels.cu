@@ -14,11 +14,9 @@
 //   k_curv        Gibbs-Thomson curvature (curvature.c:31-405), TipCurvature only
 //   k_diffuse_fs  diffusion + fs change fused (growth.c:30-170, 177-276); also
 //                 writes the solid-cell bitmask (gr > 0 after fs change)
-//   k_list_count  interface-list length per block of rank-local raster pieces,
-//                 membership from the bitmask (growth.c:461-538)
-//   k_list_scan   ordered block offsets, per-rank dc_tmp bookkeeping (growth.c:642-660)
-//   k_list_write  ordered list write; clears dc_tmp regions that the
-//                 reference re-allocates zeroed
+//   k_list        interface list in rank-local raster order, membership from
+//                 the bitmask (growth.c:461-538), in one pass (decoupled
+//                 look-back); per-rank dc_tmp bookkeeping (growth.c:642-660)
 //   k_capture     octahedron capture over the list (growth.c:339-407, 664-794),
 //                 dc copy-back and captured grain ids (growth.c:789, 797-807)
 //
@@ -145,60 +143,165 @@ __device__ __forceinline__ void fence_barrier_init()
 
 // ------------------------------------------------------------ temperature
 // AM moving-source quadrature, direct_temp_calc thermal_ana == 1
-// (temperature.c:62-123), over every halo'd cell, for step ctl->timestep+1.
-__global__ void k_temp_am(KernelArgs a, double lsd, double lv, double lhs, double lab,
-                          double lpow, double liniT, double lthcon, double rho_cp, double x0,
-                          double y0, double z0, int amtracks, int nsbx_times_sbx)
+// (temperature.c:62-123), for step ctl->timestep + 1 over every halo'd cell:
+//   T = liniT + Tfront sum_i ldt exp(-((lx + v t_i)^2 + ly^2)/a_i - lz^2/b_i) / Tl_i
+// with a_i = s^2 + 4 alpha t_i, b_i = 4 alpha t_i, 400 midpoint nodes t_i.
+// The exponential of the sum is the product of one factor per axis, so the
+// sum is a contraction over i of three tables, X_i(x), Y_i(y) and
+// Z_i(z) = ldt exp(-lz^2/b_i) / Tl_i, built once per step (k_am_tables),
+// instead of 400 exponentials per cell (k_am_contract).  Cells above the
+// substrate top (rz > znow + dx) get T = 0.
+constexpr int AM_NT = 400;
+
+struct AmStep {
+    double xnow, ynow, znow, lalpha, ls, ldt, Tfront, liniT;
+};
+
+__device__ __forceinline__ AmStep am_step(const Phys &p, const AmParams &m, unsigned long long ts)
+{
+    AmStep s;
+    const double sim_time = (double)ts * p.ts_delt;
+    const double invlv = 1. / m.lv;
+    s.ls = m.lsd / (2. * 1.414);
+    double xlen = m.nsbx_times_sbx * p.cellSize;
+    xlen = xlen + m.lsd;
+    double tline = xlen * invlv;
+    const double tpause = 1.5e-4 * invlv;
+    tline = tline + tpause;
+    double trackno = 0;
+    if (m.amtracks > 1) trackno = floor(sim_time / tline);
+    s.xnow = m.x0 + (sim_time - trackno * tline) * m.lv;
+    s.ynow = m.y0 + trackno * m.lhs;
+    s.znow = m.z0;
+    s.lalpha = m.lthcon / m.rho_cp;
+    const double tsteady = 20 * s.lalpha * invlv * invlv;
+    s.ldt = tsteady / AM_NT;
+    const double pw = (sim_time < 1e-4) ? 0.0 : m.lpow;
+    s.Tfront = m.lab * pw * s.lalpha / (5.568328 * m.lthcon);
+    s.liniT = m.liniT;
+    return s;
+}
+
+// tables: X [AM_NT][gx+2], Y [AM_NT][gy+2], Z [AM_NT][gz+2], then the
+// per-plane flag "below the substrate top" [gz+2]
+template <typename Real>
+__global__ void k_am_tables(KernelArgs a, AmParams m)
 {
     const Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
     const Geo &g = a.g;
     const Phys &p = a.p;
-    long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (cell >= g.N) return;
-    unsigned long long ts = ctl->timestep + 1;
-    long long K = cell / g.sz, J = (cell % g.sz) / g.sy, I = cell % g.sy;
-    double sim_time = (double)ts * p.ts_delt;
-    double rx = p.origin[0] + ((double)(int)I + 0.5) * p.cellSize;
-    double ry = p.origin[1] + ((double)(int)J + 0.5) * p.cellSize;
-    double rz = p.origin[2] + ((double)(int)K + 0.5) * p.cellSize;
-    double invlv = 1. / lv;
-    double ls = lsd / (2. * 1.414);
-    double xlen = nsbx_times_sbx * p.cellSize;
-    xlen = xlen + lsd;
-    double tline = xlen * invlv;
-    double tpause = 1.5e-4 * invlv;
-    tline = tline + tpause;
-    double trackno = 0;
-    if (amtracks > 1) trackno = floor(sim_time / tline);
-    double xnow = x0 + (sim_time - trackno * tline) * lv;
-    double ynow = y0 + trackno * lhs;
-    double znow = z0;
-    double lx = rx - xnow, ly = ry - ynow, lz = rz - znow;
-    double T;
-    if (rz <= znow + p.cellSize) {
-        const int nt = 400;
-        double Tinteg = 0.0;
-        double pi15 = 5.568328;
-        double lalpha = lthcon / rho_cp;
-        double tsteady = 20 * lalpha * invlv * invlv;
-        double ldt = tsteady / nt;
-        double pw = (sim_time < 1e-4) ? 0.0 : lpow;
-        for (int i = 0; i < nt; i++) {
-            double lt = (0.5 + i) * ldt;
-            double Tlocal = sqrt(lalpha * lt) * (ls * ls + 4. * lalpha * lt);
-            Tinteg += ldt *
-                      exp(-((lx + lv * lt) * (lx + lv * lt) + ly * ly) / (ls * ls + 4. * lalpha * lt) -
-                          (lz * lz / (4. * lalpha * lt))) /
-                      Tlocal;
+    const AmStep s = am_step(p, m, ctl->timestep + 1);
+    const int nx = g.gx + 2, ny = g.gy + 2, nz = g.gz + 2, nc = nx + ny + nz;
+    Real *X = (Real *)a.d.am_tab, *Y = X + (long long)AM_NT * nx, *Z = Y + (long long)AM_NT * ny;
+    int *zon = (int *)(Z + (long long)AM_NT * nz);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)AM_NT * nc;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e / nc), q = (int)(e % nc);
+        const double lt = (0.5 + i) * s.ldt;
+        const double ai = s.ls * s.ls + 4. * s.lalpha * lt;
+        if (q < nx) {
+            const double lx = (p.origin[0] + ((double)q + 0.5) * p.cellSize) - s.xnow;
+            const double u = lx + m.lv * lt;
+            X[(long long)i * nx + q] = (Real)exp(-(u * u) / ai);
+        } else if (q < nx + ny) {
+            const int J = q - nx;
+            const double ly = (p.origin[1] + ((double)J + 0.5) * p.cellSize) - s.ynow;
+            Y[(long long)i * ny + J] = (Real)exp(-(ly * ly) / ai);
+        } else {
+            const int K = q - nx - ny;
+            const double rz = p.origin[2] + ((double)K + 0.5) * p.cellSize;
+            const double lz = rz - s.znow;
+            const double Tlocal = sqrt(s.lalpha * lt) * ai;
+            Z[(long long)i * nz + K] = (Real)(s.ldt * exp(-(lz * lz / (4. * s.lalpha * lt))) / Tlocal);
+            if (i == 0) zon[K] = (rz <= s.znow + p.cellSize) ? 1 : 0;
         }
-        double Tfront = lab * pw * lalpha / (pi15 * lthcon);
-        T = liniT + Tfront * Tinteg;
-    } else {
-        T = 0.0;
     }
-    a.d.T[cell] = T;
-    if (a.d.lsindex && T > p.Tliq) a.d.lsindex[cell] = 1;
+}
+
+// T over tiles of 64 x-cells by 128 (y, z) rows: 16 x 16 threads, each
+// keeping 4 x 8 sums (x = lane + 16 m, rows = 8 consecutive), streaming the
+// node axis through shared memory 16 nodes at a time.  Per node a thread
+// loads 4 X values and 8 YZ products (two 16-byte loads shared by the half
+// warp) for 32 fused multiply-adds.
+constexpr int AMC_X = 64, AMC_YZ = 128, AMC_CH = 16, AMC_NT = 256, AMC_MX = 4, AMC_MY = 8;
+
+template <typename Real>
+__global__ void __launch_bounds__(AMC_NT) k_am_contract(KernelArgs a, AmParams m)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const Geo &g = a.g;
+    const Phys &p = a.p;
+    const int nx = g.gx + 2, ny = g.gy + 2, nz = g.gz + 2;
+    const Real *X = (const Real *)a.d.am_tab, *Y = X + (long long)AM_NT * nx, *Z = Y + (long long)AM_NT * ny;
+    const int *zon = (const int *)(Z + (long long)AM_NT * nz);
+    __shared__ __align__(16) Real sX[AMC_CH][AMC_X];
+    __shared__ __align__(16) Real sYZ[AMC_CH][AMC_YZ];
+    const int tid = threadIdx.x, xl = tid & 15, grp = tid >> 4;  // 16 x-lanes, 16 row groups
+    const int x0 = blockIdx.x * AMC_X;
+    const long long r0 = (long long)blockIdx.y * AMC_YZ;  // row = K * ny + J
+    const long long nrows = (long long)ny * nz;
+    __shared__ int s_any;
+    if (tid == 0) s_any = 0;
+    __syncthreads();
+    if (tid < AMC_YZ && r0 + tid < nrows && zon[(r0 + tid) / ny]) s_any = 1;
+    __syncthreads();
+    Real acc[AMC_MX][AMC_MY];
+#pragma unroll
+    for (int u = 0; u < AMC_MX; u++)
+#pragma unroll
+        for (int q = 0; q < AMC_MY; q++) acc[u][q] = 0;
+    if (s_any) {
+        // each thread stages the same x column and the same (y, z) row of
+        // every chunk: their table offsets are fixed for the whole sum
+        constexpr int XSTEP = AMC_NT / AMC_X, YSTEP = AMC_NT / AMC_YZ;  // nodes apart
+        const int xx = tid % AMC_X, xi0 = tid / AMC_X, rl = tid % AMC_YZ, yi0 = tid / AMC_YZ;
+        const bool xin = x0 + xx < nx;
+        const long long row = r0 + rl;
+        const bool rin = row < nrows;
+        const int Kr = rin ? (int)(row / ny) : 0, Jr = rin ? (int)(row - (long long)Kr * ny) : 0;
+        const Real *Xp = X + (x0 + xx), *Yp = Y + Jr, *Zp = Z + Kr;
+        for (int i0 = 0; i0 < AM_NT; i0 += AMC_CH) {
+#pragma unroll
+            for (int ii = xi0; ii < AMC_CH; ii += XSTEP)
+                sX[ii][xx] = xin ? Xp[(long long)(i0 + ii) * nx] : (Real)0;
+#pragma unroll
+            for (int ii = yi0; ii < AMC_CH; ii += YSTEP)
+                sYZ[ii][rl] = rin ? Yp[(long long)(i0 + ii) * ny] * Zp[(long long)(i0 + ii) * nz] : (Real)0;
+            __syncthreads();
+#pragma unroll 4
+            for (int ii = 0; ii < AMC_CH; ii++) {
+                Real xv[AMC_MX], yz[AMC_MY];
+#pragma unroll
+                for (int u = 0; u < AMC_MX; u++) xv[u] = sX[ii][xl + 16 * u];
+#pragma unroll
+                for (int q = 0; q < AMC_MY; q++) yz[q] = sYZ[ii][grp * AMC_MY + q];
+#pragma unroll
+                for (int u = 0; u < AMC_MX; u++)
+#pragma unroll
+                    for (int q = 0; q < AMC_MY; q++) acc[u][q] = fma(xv[u], yz[q], acc[u][q]);
+            }
+            __syncthreads();
+        }
+    }
+    const AmStep s = am_step(p, m, ctl->timestep + 1);
+#pragma unroll
+    for (int q = 0; q < AMC_MY; q++) {
+        const long long row = r0 + grp * AMC_MY + q;
+        if (row >= nrows) break;
+        const int K = (int)(row / ny), J = (int)(row - (long long)K * ny);
+        const bool on = zon[K] != 0;
+#pragma unroll
+        for (int u = 0; u < AMC_MX; u++) {
+            const int x = x0 + xl + 16 * u;
+            if (x >= nx) continue;
+            const long long c = (long long)K * g.sz + (long long)J * g.sy + x;
+            const double T = on ? s.liniT + s.Tfront * (double)acc[u][q] : 0.0;
+            a.d.T[c] = T;
+            if (a.d.lsindex && T > p.Tliq) a.d.lsindex[c] = 1;
+        }
+    }
 }
 
 // --------------------------------------------------------------- nucleation
@@ -286,6 +389,7 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
     __shared__ int s_abort;
     const int C = ctl->ncand;
     const unsigned long long ts = ctl->timestep + 1;
+    if (threadIdx.x == 0) ctl->list_ticket = 0;  // k_list block order of this step
     if (C == 0) {
         if (threadIdx.x == 0) {
             ctl->timestep = ts;
@@ -399,6 +503,21 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
 }
 
 // ---------------------------------------------------------------- curvature
+// x^1.5 for x >= 1, to the nearest double: the product x * sqrt(x) carried
+// exactly as a pair (fma gives the rounding error of the product and the
+// residual x - s^2 of the rounded square root s), so the one final rounding
+// matches a correctly rounded pow(x, 1.5) except when the exact value lies
+// within about 1e-16 ulp of a rounding boundary.
+__device__ __forceinline__ double pow_1_5(double x)
+{
+    const double s = sqrt(x);
+    const double res = fma(-s, s, x);     // x - s^2, exact
+    const double e = res / (2.0 * s);     // sqrt(x) - s to first order
+    const double ph = x * s;
+    const double pl = fma(x, s, -ph);     // x s - ph, exact
+    return ph + (pl + x * e);
+}
+
 // sb_curvature (curvature.c:31-405) on each emulated rank's local range
 // k,j,i in [2, dim-1], reading fs as it stands before fs_change.
 template <typename Real>
@@ -494,7 +613,7 @@ __global__ void k_curv(KernelArgs a)
     double hxx = (gamma * (hC11 - 2 * hA1 + hC12) + hB1 - 2 * h + hB2 + gamma * (hC21 - 2 * hA2 + hC22)) / (cs) / (1 + 2 * gamma);
     double hyy = (gamma * (hC11 - 2 * hB1 + hC21) + hA1 - 2 * h + hA2 + gamma * (hC12 - 2 * hB2 + hC22)) / (cs) / (1 + 2 * gamma);
     double hxy = (hC11 - hC21 - hC12 + hC22) / cs / 4.0;
-    curv[idx] = (hxx + hyy + hxx * hy * hy + hyy * hx * hx - 2 * hxy * hx * hy) / pow((1 + hx * hx + hy * hy), 1.5);
+    curv[idx] = (hxx + hyy + hxx * hy * hy + hyy * hx * hx - 2 * hxy * hx * hy) / pow_1_5((1 + hx * hx + hy * hy));
 }
 
 // ------------------------------------------------ diffusion + fs change
@@ -657,16 +776,30 @@ struct TmaMaps {
     CUtensorMap cl[2], fs[2], ce, gr;
 };
 
+// Shared-memory state of a stencil CTA, kept across the tiles a persistent
+// CTA processes: the ring, one mbarrier per slot (initialised once), the
+// per-plane temperatures and the abort flag.
+template <int TS>
+struct StencilShared {
+    unsigned long long bars[TS];
+    double sT[64];
+    int abort;
+};
+
+// One (32 CPT) x 8 x zchunk tile (bx, by, bz) of the diffusion + fs-change
+// update.  ring: planes this CTA has streamed through its ring before this
+// tile, so slot and phase continue across tiles.  Returns false when a copy
+// did not land within the bound (the error is raised, copies in flight are
+// drained).
 template <typename Real, int CPT>
-__global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
-    k_diffuse_fs_tma(const __grid_constant__ KernelArgs a, const __grid_constant__ TmaMaps maps, int zchunk)
+__device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps &maps, int zchunk, int bx, int by,
+                                             int bz, unsigned char *smem, StencilShared<Depth<Real, CPT>::TS> &sh,
+                                             unsigned &ring)
 {
     using L = Stage<Real, CPT>;
     constexpr int TS = Depth<Real, CPT>::TS;
     Ctl *ctl = a.d.ctl;
-    if (stalled(ctl)) return;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) unsigned long long bars[TS];
+    unsigned long long *bars = sh.bars;
     const Geo &g = a.g;
     const Phys &p = a.p;
     const unsigned long long ts = ctl->timestep;
@@ -677,17 +810,18 @@ __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
     int *__restrict__ gr = a.d.gr;
     const PhysR<Real> q = phys_r<Real>(p);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DTX + tx;
-    const int i0 = blockIdx.x * L::TX + 1, j0 = blockIdx.y * DTY + 1;
+    const int i0 = bx * L::TX + 1, j0 = by * DTY + 1;
     const int j = j0 + ty;
-    const int k0 = blockIdx.z * zchunk + 1;
+    const int k0 = bz * zchunk + 1;
     const int k1 = min(k0 + zchunk - 1, g.gz);
     const int nplanes = k1 - k0 + 3;  // k0-1 .. k1+1
     const CUtensorMap *mcl = &maps.cl[pin];
     const CUtensorMap *mfs = &maps.fs[pin];
+    const unsigned base = ring;
 
     auto stage = [&](int s) { return smem + s * L::BYTES; };
     auto issue = [&](int pl) {
-        const int s = pl % TS, k = k0 - 1 + pl;
+        const int s = (int)((base + pl) % TS), k = k0 - 1 + pl;
         const bool center = (k >= k0 && k <= k1);
         mbar_expect_tx(&bars[s], L::TX_HALO + (center ? L::TX_CENTER : 0u));
         tma_load_3d(stage(s), mcl, i0 - 1, j0 - 1, k, &bars[s]);
@@ -697,17 +831,12 @@ __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
             tma_load_3d(stage(s) + 2 * L::CL + L::CE, &maps.gr, i0 - 1, j0, k, &bars[s]);
         }
     };
+    auto phase = [&](int pl) { return (unsigned)(((base + pl) / TS) & 1u); };
     // temperature of each plane of the chunk when it depends on z only
     // (direct_temp_calc's isothermal and gradient models in 3D)
-    __shared__ double sT[64];
-    __shared__ int s_abort;
     const bool t_per_plane = (p.temp_mode == 0) || (p.temp_mode == 1 && !p.gz_is_one);
-    if (tid == 0) {
-        for (int s = 0; s < TS; s++) mbar_init(&bars[s], 1);
-        fence_barrier_init();
-        s_abort = 0;
-    }
-    if (t_per_plane && tid <= k1 - k0) sT[tid] = temp_cell(p, a.d.T, 0, 1, k0 + tid, ts);
+    if (tid == 0) sh.abort = 0;
+    if (t_per_plane && tid <= k1 - k0) sh.sT[tid] = temp_cell(p, a.d.T, 0, 1, k0 + tid, ts);
     __syncthreads();
     if (tid == 0)
         for (int pl = 0; pl < TS && pl < nplanes; pl++) issue(pl);
@@ -733,15 +862,16 @@ __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
         omx_m[u] = i == 1 ? one_x : (Real)1;
     }
     // ring slots of planes t, t+1, t+2 and the phase of slot s2
-    int s0 = 0, s1 = 1 % TS, s2 = 2 % TS;
-    unsigned ph2 = (unsigned)((2 / TS) & 1);
+    int s0 = (int)(base % TS), s1 = (int)((base + 1) % TS), s2 = (int)((base + 2) % TS);
+    unsigned ph2 = phase(2);
     long long crow = (long long)k0 * g.sz + (long long)j * g.sy;
+    bool alive = true;
     for (int t = 0; t <= k1 - k0; t++) {
         const int k = k0 + t;
         // planes t and t+1 completed in earlier iterations
         bool ok = mbar_wait(&bars[s2], ph2);
-        if (t == 0) ok &= mbar_wait(&bars[0], 0u) && mbar_wait(&bars[1 % TS], (unsigned)((1 / TS) & 1));
-        if (!ok) s_abort = 1;
+        if (t == 0) ok &= mbar_wait(&bars[s0], phase(0)) && mbar_wait(&bars[s1], phase(1));
+        if (!ok) sh.abort = 1;
         int solid[CPT];
         const Real *cm = (const Real *)stage(s0);
         const Real *cc = (const Real *)stage(s1);
@@ -753,7 +883,7 @@ __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
         const int *sgr = (const int *)(stage(s1) + 2 * L::CL + L::CE);
         const Real omz_p = k == g.gz ? one_z : (Real)1, omz_m = k == 1 ? one_z : (Real)1;
         const bool in_z = k > 1 && k < g.gz;
-        const double Tp = t_per_plane ? sT[t] : 0.0;
+        const double Tp = t_per_plane ? sh.sT[t] : 0.0;
 #pragma unroll
         for (int u = 0; u < CPT; u++) {
             solid[u] = 0;
@@ -784,17 +914,18 @@ __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
 #pragma unroll
         for (int u = 0; u < CPT; u++) {
             const unsigned word = __ballot_sync(FULL_MASK, solid[u]);
-            const int w = blockIdx.x * CPT + u;
+            const int w = bx * CPT + u;
             if (tx == 0 && jrow && w < g.wpr) a.d.solid_bits[((long long)k * (g.gy + 2) + j) * wrow + w] = word;
         }
         __syncthreads();
-        if (s_abort) {
+        if (sh.abort) {
             // a copy did not land within the bound: report, then wait (again
             // bounded) for every copy still in flight before leaving
             if (tid == 0) {
                 raise_error(ctl, MMS_ERR_TIMEOUT);
-                for (int pl = t; pl < issued; pl++) mbar_wait(&bars[pl % TS], (unsigned)((pl / TS) & 1));
+                for (int pl = t; pl < issued; pl++) mbar_wait(&bars[(base + pl) % TS], phase(pl));
             }
+            alive = false;
             break;
         }
         if (t + TS < nplanes) {
@@ -807,6 +938,81 @@ __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
         s2 = (s2 + 1 == TS) ? 0 : s2 + 1;
         if (s2 == 0) ph2 ^= 1u;
         crow += g.sz;
+    }
+    ring = base + (unsigned)nplanes;
+    return alive;
+}
+
+template <typename Real, int CPT>
+__global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
+    k_diffuse_fs_tma(const __grid_constant__ KernelArgs a, const __grid_constant__ TmaMaps maps, int zchunk)
+{
+    constexpr int TS = Depth<Real, CPT>::TS;
+    if (stalled(a.d.ctl)) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) StencilShared<TS> sh;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        for (int s = 0; s < TS; s++) mbar_init(&sh.bars[s], 1);
+        fence_barrier_init();
+    }
+    unsigned ring = 0;
+    stencil_tile<Real, CPT>(a, maps, zchunk, blockIdx.x, blockIdx.y, blockIdx.z, smem, sh, ring);
+}
+
+// Many independent domains in one persistent launch: every CTA walks the
+// concatenated tile space of all domains (tile_begin: the first tile of
+// each), copying the domain's kernel arguments to shared memory and
+// keeping its ring and barriers from tile to tile.  Domains whose step has
+// stalled are skipped.
+struct BatchItem {
+    TmaMaps maps;          // first: 128-byte aligned in the item array
+    KernelArgs a;
+    long long tile_begin;
+    int tiles_x, tiles_y, zchunk, pad;
+};
+
+template <typename Real, int CPT>
+__global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
+    k_diffuse_fs_batch(const BatchItem *__restrict__ items, int nitems, long long total_tiles)
+{
+    constexpr int TS = Depth<Real, CPT>::TS;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) StencilShared<TS> sh;
+    __shared__ __align__(16) KernelArgs sa;
+    __shared__ int s_item;
+    const int tid = threadIdx.y * DTX + threadIdx.x;
+    if (tid == 0) {
+        for (int s = 0; s < TS; s++) mbar_init(&sh.bars[s], 1);
+        fence_barrier_init();
+    }
+    unsigned ring = 0;
+    int cur = -1;
+    for (long long t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+        if (tid == 0) {
+            int lo = 0, hi = nitems - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) / 2;
+                if (items[mid].tile_begin <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            s_item = lo;
+        }
+        __syncthreads();
+        const int d = s_item;
+        if (d != cur) {
+            const int *src = (const int *)&items[d].a;
+            int *dst = (int *)&sa;
+            for (int e = tid; e < (int)(sizeof(KernelArgs) / sizeof(int)); e += DTX * DTY) dst[e] = src[e];
+            cur = d;
+        }
+        __syncthreads();
+        if (stalled(sa.d.ctl)) continue;
+        const BatchItem &it = items[d];
+        const long long local = t - it.tile_begin;
+        const int bx = (int)(local % it.tiles_x);
+        const int by = (int)((local / it.tiles_x) % it.tiles_y);
+        const int bz = (int)(local / ((long long)it.tiles_x * it.tiles_y));
+        if (!stencil_tile<Real, CPT>(sa, it.maps, it.zchunk, bx, by, bz, smem, sh, ring)) break;
     }
 }
 
@@ -938,9 +1144,12 @@ __device__ __forceinline__ Piece piece_of(const KernelArgs &a, int r, long long 
     const Geo &g = a.g;
     Piece pc{0u, 0};
     if (q >= g.pieces_per_rank) return pc;
-    long long lr = q / g.ppr;
-    int part = (int)(q % g.ppr);
-    int ly = (int)(lr % g.sby), lz = (int)(lr / g.sby);
+    // pieces of one rank number fewer than 2^31 (sby * sbz * ppr): 32-bit division
+    const unsigned qq = (unsigned)q, ppr = (unsigned)g.ppr, sby = (unsigned)g.sby;
+    const unsigned lr = qq / ppr;
+    const int part = (int)(qq - lr * ppr);
+    const unsigned lz = lr / sby;
+    const int ly = (int)(lr - lz * sby);
     int rx = r % g.nsbx, ry = (r / g.nsbx) % g.nsby, rz = r / (g.nsbx * g.nsby);
     long long J = (long long)ry * g.sby + ly + 1, K = (long long)rz * g.sbz + lz + 1;
     long long X0 = (long long)rx * g.sbx + 32LL * part;  // 0-based interior x
@@ -958,61 +1167,137 @@ __device__ __forceinline__ Piece piece_of(const KernelArgs &a, int r, long long 
     return pc;
 }
 
-__global__ void __launch_bounds__(LIST_NT) k_list_count(KernelArgs a)
+// Status word of a list block for the decoupled look-back: bits 34-63 the
+// step (low 30 bits of the timestep, so words of earlier steps never
+// match), bits 32-33 the state (1 = own count, 2 = inclusive prefix), bits
+// 0-31 the value.
+constexpr unsigned long long LS_AGG = 1ULL, LS_PRE = 2ULL;
+__device__ __forceinline__ unsigned long long ls_word(unsigned long long tag, unsigned long long state, int v)
 {
-    const Ctl *ctl = a.d.ctl;
-    if (stalled(ctl)) return;
-    __shared__ int sh[LIST_NT / 32];
-    const Geo &g = a.g;
-    int r = (int)(blockIdx.x / g.blocks_per_rank);
-    long long q0 = (blockIdx.x % g.blocks_per_rank) * (long long)LIST_PIECES;
-    int n = 0;
-    for (int it = 0; it < LIST_PIECES / LIST_NT; it++) n += __popc(piece_of(a, r, q0 + it * LIST_NT + threadIdx.x).bits);
-    int tot = block_sum<LIST_NT>(n, sh);
-    if (threadIdx.x == 0) a.d.blk_cnt[blockIdx.x] = tot;
+    return (tag << 34) | (state << 32) | (unsigned)v;
 }
 
-// Exclusive scan of block counts; per-rank list lengths and the dc_tmp
-// re-allocation rule of capture_octahedra_diffuse (growth.c:642-660): when
-// a rank's list outgrows its dc_tmp, the array is replaced by a zeroed one of
-// gindex + 100 entries.
-constexpr int SCAN_NT = 1024;
-__global__ void __launch_bounds__(SCAN_NT) k_list_scan(KernelArgs a, int nblocks)
+// Bounded wait for list block j's status word of this step; returns it,
+// or 0 after about a second.
+__device__ __forceinline__ unsigned long long ls_wait(const unsigned long long *st, long long j,
+                                                      unsigned long long tag, unsigned long long want_state)
+{
+    for (unsigned it = 0; it < (1u << 22); it++) {
+        unsigned long long w = *((volatile const unsigned long long *)&st[j]);
+        if ((w >> 34) == tag && ((w >> 32) & 3ULL) >= want_state) return w;
+        if (it > 32) __nanosleep(128);
+    }
+    return 0;
+}
+
+// grow_cell_reduction in one pass: every block counts its pieces, finds the
+// list position of its first entry by looking back over the status words
+// of the blocks before it, and writes its entries in piece order.  Blocks
+// take their list position from a ticket (reset by k_act each step), so a
+// block only ever waits on blocks that started before it.  The last block
+// of each emulated rank applies the dc_tmp re-allocation rule of
+// capture_octahedra_diffuse (growth.c:642-660): when the rank's list
+// outgrows its dc_tmp, the reference replaces it with a zeroed array of
+// gindex + 100 entries; here the slots that must read as zero this step are
+// recorded (rank_zero_upto) and k_capture clears them.
+__global__ void __launch_bounds__(LIST_NT) k_list(KernelArgs a, int nblocks)
 {
     Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
-    __shared__ int sh[SCAN_NT / 32];
-    int run = 0;
-    for (int base = 0; base < nblocks; base += SCAN_NT) {
-        int b = base + threadIdx.x;
-        int v = (b < nblocks) ? a.d.blk_cnt[b] : 0;
-        int tot;
-        int ex = block_exclusive_scan<SCAN_NT>(v, tot, sh);
-        if (b < nblocks) a.d.blk_off[b] = run + ex;
-        run += tot;
-    }
-    __syncthreads();
+    constexpr int NI = LIST_PIECES / LIST_NT;
+    __shared__ int sh[LIST_NT / 32];
+    __shared__ int s_b, s_excl, s_ok;
     const Geo &g = a.g;
-    int any_zero = 0;
-    for (int r = threadIdx.x; r < g.nranks; r += SCAN_NT) {
-        long long b0 = (long long)r * g.blocks_per_rank, b1 = b0 + g.blocks_per_rank;
-        int start = a.d.blk_off[b0];
-        int end = (b1 < nblocks) ? a.d.blk_off[b1] : run;
-        int gindex = end - start;
-        a.d.rank_gindex[r] = gindex;
-        int size = a.d.rank_dcsize[r];
-        if (gindex > size) {
-            a.d.rank_zero_upto[r] = size;
-            a.d.rank_dcsize[r] = gindex + 100;
-            if (size > 0) any_zero = 1;
-        } else {
-            a.d.rank_zero_upto[r] = 0;
+    unsigned long long *st = a.d.list_status;
+    const unsigned long long tag = ctl->timestep & 0x3fffffffULL;
+    if (threadIdx.x == 0) s_b = atomicAdd(&ctl->list_ticket, 1);
+    __syncthreads();
+    const int b = s_b;
+    if (b >= nblocks) {  // the ticket was not reset: never index past the block arrays
+        if (threadIdx.x == 0) raise_error(ctl, MMS_ERR_STATE);
+        return;
+    }
+    const int r = (int)(b / g.blocks_per_rank);
+    const long long q0 = (b % g.blocks_per_rank) * (long long)LIST_PIECES;
+    Piece pc[NI];
+    int ex[NI], tot[NI], agg = 0;
+#pragma unroll
+    for (int it = 0; it < NI; it++) {
+        pc[it] = piece_of(a, r, q0 + it * LIST_NT + threadIdx.x);
+        ex[it] = block_exclusive_scan<LIST_NT>(__popc(pc[it].bits), tot[it], sh);
+        agg += tot[it];
+    }
+    // warp 0: decoupled look-back, 32 predecessors per round
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int excl = 0, ok = 1;
+        if (b > 0) {
+            if (lane == 0) *((volatile unsigned long long *)&st[b]) = ls_word(tag, LS_AGG, agg);
+            long long j0 = b - 1;
+            while (true) {
+                const long long j = j0 - lane;
+                unsigned long long w = ls_word(tag, LS_PRE, 0);  // before block 0: prefix 0
+                if (j >= 0) w = ls_wait(st, j, tag, LS_AGG);
+                const int bad = __any_sync(FULL_MASK, w == 0);
+                if (bad) {
+                    ok = 0;
+                    break;
+                }
+                const unsigned pre = __ballot_sync(FULL_MASK, ((w >> 32) & 3ULL) == LS_PRE);
+                // nearest predecessor holding its inclusive prefix: the lowest lane
+                const int stop = pre ? __ffs(pre) - 1 : 31;
+                int v = (lane <= stop) ? (int)(w & 0xffffffffULL) : 0;
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL_MASK, v, o);
+                excl += v;
+                if (pre) break;
+                j0 -= 32;
+            }
+        }
+        if (lane == 0) {
+            a.d.blk_off[b] = excl;
+            __threadfence();
+            *((volatile unsigned long long *)&st[b]) = ls_word(tag, LS_PRE, excl + agg);
+            const long long first = (long long)r * g.blocks_per_rank;
+            if (ok && b == first + g.blocks_per_rank - 1) {
+                // last block of the rank: its list length and dc_tmp bookkeeping
+                int start = excl;
+                if (b != first) {
+                    if (ls_wait(st, first, tag, LS_PRE)) {
+                        __threadfence();
+                        start = *((volatile const int *)&a.d.blk_off[first]);
+                    } else {
+                        ok = 0;
+                    }
+                }
+                const int gindex = excl + agg - start;
+                a.d.rank_gindex[r] = gindex;
+                const int size = a.d.rank_dcsize[r];
+                if (gindex > size) {
+                    a.d.rank_zero_upto[r] = size;
+                    a.d.rank_dcsize[r] = gindex + 100;
+                } else {
+                    a.d.rank_zero_upto[r] = 0;
+                }
+            }
+            if (b == nblocks - 1) ctl->list_total = excl + agg;
+            if (!ok) raise_error(ctl, MMS_ERR_TIMEOUT);
+            s_excl = excl;
+            s_ok = ok;
         }
     }
-    any_zero = __syncthreads_or(any_zero);
-    if (threadIdx.x == 0) {
-        ctl->list_total = run;
-        ctl->zero_needed = any_zero;
+    __syncthreads();
+    if (!s_ok) return;
+    int pos = s_excl;
+#pragma unroll
+    for (int it = 0; it < NI; it++) {
+        int p0 = pos + ex[it];
+        pos += tot[it];
+        unsigned bits = pc[it].bits;
+        while (bits) {
+            const int bit = __ffs(bits) - 1;
+            bits &= bits - 1;
+            a.d.list_cell[p0++] = pc[it].base + bit;
+        }
     }
 }
 
@@ -1092,41 +1377,6 @@ __device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs,
     return gid;
 }
 
-// Writes this block's part of the ordered list (pieces in rank-local raster
-// order, positions from k_list_scan).
-__global__ void __launch_bounds__(LIST_NT) k_list_write(KernelArgs a)
-{
-    const Ctl *ctl = a.d.ctl;
-    if (stalled(ctl)) return;
-    __shared__ int sh[LIST_NT / 32];
-    const Geo &g = a.g;
-    const int r = (int)(blockIdx.x / g.blocks_per_rank);
-    const long long chunk = blockIdx.x % g.blocks_per_rank;
-    const long long q0 = chunk * (long long)LIST_PIECES;
-    if (ctl->zero_needed) {
-        // this block's share of the rank's dc_tmp slots to clear
-        const long long upto = a.d.rank_zero_upto[r];
-        const long long span = (upto + g.blocks_per_rank - 1) / g.blocks_per_rank;
-        Dc3 *base = a.d.dc_tmp + a.d.rank_dcbase[r];
-        for (long long s = chunk * span + threadIdx.x; s < min(upto, (chunk + 1) * span); s += LIST_NT)
-            base[s] = Dc3{0.0, 0.0, 0.0};
-    }
-    if (a.d.blk_cnt[blockIdx.x] == 0) return;
-    int pos = a.d.blk_off[blockIdx.x];
-    for (int it = 0; it < LIST_PIECES / LIST_NT; it++) {
-        Piece pc = piece_of(a, r, q0 + it * LIST_NT + threadIdx.x);
-        int tot;
-        int p0 = pos + block_exclusive_scan<LIST_NT>(__popc(pc.bits), tot, sh);
-        pos += tot;
-        unsigned b = pc.bits;
-        while (b) {
-            int bit = __ffs(b) - 1;
-            b &= b - 1;
-            a.d.list_cell[p0++] = pc.base + bit;
-        }
-    }
-}
-
 // Captures every list entry and commits it at once (grid-stride over the
 // whole list, so the work is balanced however the interface is
 // distributed): dc_tmp slot of a captured entry, then the reference's
@@ -1142,20 +1392,36 @@ __global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
     const Real *fs = (const Real *)a.d.fs[(int)(ctl->timestep & 1ULL)];
     for (long long e = blockIdx.x * (long long)LIST_NT + threadIdx.x; e < total; e += (long long)gridDim.x * LIST_NT) {
         const long long c = a.d.list_cell[e];
-        const long long K = c / g.sz, J = (c - K * g.sz) / g.sy, I = c - K * g.sz - J * g.sy;
+        long long K, J, I;
+        if (g.N < 0x7fffffffLL) {  // 32-bit division when every index fits
+            const unsigned cu = (unsigned)c, szu = (unsigned)g.sz, syu = (unsigned)g.sy;
+            const unsigned Ku = cu / szu, rem = cu - Ku * szu, Ju = rem / syu;
+            K = Ku;
+            J = Ju;
+            I = rem - Ju * syu;
+        } else {
+            K = c / g.sz;
+            J = (c - K * g.sz) / g.sy;
+            I = c - K * g.sz - J * g.sy;
+        }
         int r = 0;
         if (g.nranks > 1) {
             const int rx = (int)((I - 1) / g.sbx), ry = (int)((J - 1) / g.sby), rz = (int)((K - 1) / g.sbz);
             r = rx + ry * g.nsbx + rz * g.nsbx * g.nsby;
         }
         const int rank_start = a.d.blk_off[(long long)r * g.blocks_per_rank];
-        Dc3 *slot = a.d.dc_tmp + a.d.rank_dcbase[r] + (e - rank_start + 1);
+        const long long sl = e - rank_start + 1;
+        Dc3 *slot = a.d.dc_tmp + a.d.rank_dcbase[r] + sl;
         Dc3 out;
         const int gid = capture_cell<Real>(a, fs, c, I, J, K, out);
         if (gid) {
             *slot = out;
             a.d.dc[c] = out;
             a.d.gr[c] = gid;
+        } else if (sl <= a.d.rank_zero_upto[r]) {
+            // slot of a dc_tmp the reference re-allocated zeroed this step
+            *slot = Dc3{0.0, 0.0, 0.0};
+            a.d.dc[c] = Dc3{0.0, 0.0, 0.0};
         } else {
             a.d.dc[c] = *slot;
         }
@@ -1404,8 +1670,10 @@ int launch_stencil(const KernelArgs &a, const TmaHolder &tma, int precision, voi
     return 1;
 }
 
+// The kernels of a step before the stencil (nucleation, activation,
+// curvature) and after it (list, capture).
 template <typename Real>
-static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st, int start_stage, Profiler *prof)
+static int launch_pre_t(const KernelArgs &a, cudaStream_t st, int start_stage, Profiler *prof)
 {
     int n = 0;
     const Geo &g = a.g;
@@ -1426,25 +1694,110 @@ static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t
         PROF_END(KID_CURV);
         n++;
     }
+    return n;
+}
+
+template <typename Real>
+static int launch_post_t(const KernelArgs &a, cudaStream_t st, Profiler *prof)
+{
+    const Geo &g = a.g;
+    int nblocks = (int)(g.blocks_per_rank * g.nranks);
+    PROF_BEGIN(KID_LIST);
+    k_list<<<nblocks, LIST_NT, 0, st>>>(a, nblocks);
+    PROF_END(KID_LIST);
+    PROF_BEGIN(KID_CAPTURE);
+    k_capture<Real><<<148 * 8, LIST_NT, 0, st>>>(a);
+    PROF_END(KID_CAPTURE);
+    return 2;
+}
+
+template <typename Real>
+static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st, int start_stage, Profiler *prof)
+{
+    int n = launch_pre_t<Real>(a, st, start_stage, prof);
     PROF_BEGIN(KID_DIFFUSE_FS);
     launch_stencil_t<Real>(a, tma, st);
     PROF_END(KID_DIFFUSE_FS);
     n++;
-    int nblocks = (int)(g.blocks_per_rank * g.nranks);
-    PROF_BEGIN(KID_LIST_COUNT);
-    k_list_count<<<nblocks, LIST_NT, 0, st>>>(a);
-    PROF_END(KID_LIST_COUNT);
-    PROF_BEGIN(KID_LIST_SCAN);
-    k_list_scan<<<1, SCAN_NT, 0, st>>>(a, nblocks);
-    PROF_END(KID_LIST_SCAN);
-    PROF_BEGIN(KID_LIST_WRITE);
-    k_list_write<<<nblocks, LIST_NT, 0, st>>>(a);
-    PROF_END(KID_LIST_WRITE);
-    PROF_BEGIN(KID_CAPTURE);
-    k_capture<Real><<<148 * 8, LIST_NT, 0, st>>>(a);
-    PROF_END(KID_CAPTURE);
-    n += 4;
-    return n;
+    return n + launch_post_t<Real>(a, st, prof);
+}
+
+int launch_step_pre(const KernelArgs &a, int precision, void *stream, int start_stage)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    Profiler *prof = nullptr;
+    if (precision == MMS_PREC_F32) return launch_pre_t<float>(a, st, start_stage, prof);
+    return launch_pre_t<double>(a, st, start_stage, prof);
+}
+
+int launch_step_post(const KernelArgs &a, int precision, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    Profiler *prof = nullptr;
+    if (precision == MMS_PREC_F32) return launch_post_t<float>(a, st, prof);
+    return launch_post_t<double>(a, st, prof);
+}
+
+size_t batch_item_bytes() { return sizeof(BatchItem); }
+
+long long fill_batch_item(void *dst, const KernelArgs &a, const TmaHolder &tma, long long tile_begin)
+{
+    BatchItem it;
+    std::memset(&it, 0, sizeof it);
+    std::memcpy(&it.maps, tma.bytes, sizeof(TmaMaps));
+    it.a = a;
+    const Geo &g = a.g;
+    const int tile_x = DTX * (tma.cpt == 2 ? 2 : 1);
+    int zc = tma.zc > 0 ? (tma.zc < g.gz ? tma.zc : g.gz) : pick_zchunk(g, tile_x);
+    if (zc > 64) zc = 64;
+    it.tiles_x = (g.gx + tile_x - 1) / tile_x;
+    it.tiles_y = (g.gy + DTY - 1) / DTY;
+    it.zchunk = zc;
+    it.tile_begin = tile_begin;
+    std::memcpy(dst, &it, sizeof it);
+    return (long long)it.tiles_x * it.tiles_y * ((g.gz + zc - 1) / zc);
+}
+
+template <typename Real, int CPT>
+static int batch_grid_t()
+{
+    constexpr int bytes = Depth<Real, CPT>::TS * Stage<Real, CPT>::BYTES;
+    cudaFuncSetAttribute(k_diffuse_fs_batch<Real, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_diffuse_fs_batch<Real, CPT>, DTX * DTY, bytes);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (per_sm > 0 ? per_sm : 1) * sms;
+}
+
+int batch_grid(int precision, int cpt)
+{
+    if (precision == MMS_PREC_F32) return cpt == 2 ? batch_grid_t<float, 2>() : batch_grid_t<float, 1>();
+    return cpt == 2 ? batch_grid_t<double, 2>() : batch_grid_t<double, 1>();
+}
+
+int launch_stencil_batch(const void *items, int nitems, long long total_tiles, int precision, int cpt, int grid,
+                         void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const BatchItem *it = (const BatchItem *)items;
+    if (precision == MMS_PREC_F32) {
+        if (cpt == 2)
+            k_diffuse_fs_batch<float, 2><<<grid, dim3(DTX, DTY), Depth<float, 2>::TS * Stage<float, 2>::BYTES, st>>>(
+                it, nitems, total_tiles);
+        else
+            k_diffuse_fs_batch<float, 1><<<grid, dim3(DTX, DTY), Depth<float, 1>::TS * Stage<float, 1>::BYTES, st>>>(
+                it, nitems, total_tiles);
+    } else {
+        if (cpt == 2)
+            k_diffuse_fs_batch<double, 2><<<grid, dim3(DTX, DTY), Depth<double, 2>::TS * Stage<double, 2>::BYTES,
+                                            st>>>(it, nitems, total_tiles);
+        else
+            k_diffuse_fs_batch<double, 1><<<grid, dim3(DTX, DTY), Depth<double, 1>::TS * Stage<double, 1>::BYTES,
+                                            st>>>(it, nitems, total_tiles);
+    }
+    return 1;
 }
 
 int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream, int start_stage, Profiler *prof)
@@ -1454,17 +1807,23 @@ int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *
     return launch_step_t<double>(a, tma, st, start_stage, prof);
 }
 
-int launch_temp_am(const KernelArgs &a, void *stream, Profiler *prof, double lsd, double lv, double lhs,
-                   double lab, double lpow, double liniT, double lthcon, double rho_cp, double x0, double y0,
-                   double z0, int amtracks, int nsbx_times_sbx)
+int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof)
 {
     cudaStream_t st = (cudaStream_t)stream;
-    int nb = (int)((a.g.N + 255) / 256);
+    const Geo &g = a.g;
+    const long long tab = (long long)AM_NT * (g.gx + g.gy + g.gz + 6);
+    dim3 cg((unsigned)((g.gx + 2 + AMC_X - 1) / AMC_X),
+            (unsigned)(((long long)(g.gy + 2) * (g.gz + 2) + AMC_YZ - 1) / AMC_YZ));
     PROF_BEGIN(KID_TEMP_AM);
-    k_temp_am<<<nb, 256, 0, st>>>(a, lsd, lv, lhs, lab, lpow, liniT, lthcon, rho_cp, x0, y0, z0,
-                                  amtracks, nsbx_times_sbx);
+    if (precision == MMS_PREC_F32) {
+        k_am_tables<float><<<(unsigned)((tab + 255) / 256), 256, 0, st>>>(a, m);
+        k_am_contract<float><<<cg, AMC_NT, 0, st>>>(a, m);
+    } else {
+        k_am_tables<double><<<(unsigned)((tab + 255) / 256), 256, 0, st>>>(a, m);
+        k_am_contract<double><<<cg, AMC_NT, 0, st>>>(a, m);
+    }
     PROF_END(KID_TEMP_AM);
-    return 1;
+    return 2;
 }
 
 int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream)

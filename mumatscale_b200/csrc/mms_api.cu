@@ -152,7 +152,15 @@ mms_status dalloc(mms_ctx *ctx, T **ptr, size_t count)
         ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
         return MMS_ERR_NOMEM;
     }
-    cudaMemsetAsync(p, 0, bytes, ctx->stream);
+    // zeroed before returning: later host copies into this buffer go through
+    // the legacy default stream, which does not wait for ctx->stream
+    e = cudaMemsetAsync(p, 0, bytes, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(p);
+        ctx->err = std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
+        return MMS_ERR_CUDA;
+    }
     ctx->allocs.push_back(p);
     ctx->bytes += bytes;
     *ptr = (T *)p;
@@ -170,6 +178,28 @@ void dfree(mms_ctx *ctx, void *p)
     if (!p) return;
     cudaFree(p);
     ctx->allocs.erase(std::remove(ctx->allocs.begin(), ctx->allocs.end(), p), ctx->allocs.end());
+}
+
+// Host <-> device copies ordered on the context's stream and complete on
+// return.  (A plain cudaMemcpy from pageable memory may return before its
+// DMA has landed, and it is not ordered with the context's non-blocking
+// stream, whose kernels could then read a partly copied buffer.)
+cudaError_t h2d(mms_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(ctx->stream) : e;
+}
+
+cudaError_t d2h(mms_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(ctx->stream) : e;
+}
+
+cudaError_t dzero(mms_ctx *ctx, void *dst, size_t bytes)
+{
+    cudaError_t e = cudaMemsetAsync(dst, 0, bytes, ctx->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(ctx->stream) : e;
 }
 
 // device-layout and reference-layout linear indices (see Geo)
@@ -296,7 +326,7 @@ mms_status refill_rng(mms_ctx *ctx, bool force)
     DevPtrs &d = ctx->ka.d;
     if (!ctx->p.gnUseOrientation) return MMS_OK;
     std::vector<int> used(g.nranks);
-    CU(cudaMemcpy(used.data(), d.rng_used, sizeof(int) * g.nranks, cudaMemcpyDeviceToHost));
+    CU(d2h(ctx, used.data(), d.rng_used, sizeof(int) * g.nranks));
     bool any = force;
     for (int r = 0; r < g.nranks; r++)
         if (used[r] * 2 > d.rng_cap) any = true;
@@ -317,9 +347,9 @@ mms_status refill_rng(mms_ctx *ctx, bool force)
         }
         base[ri] = r.rng_base;
     }
-    CU(cudaMemcpy(d.rng_rot, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(d.rng_base, base.data(), sizeof(long long) * g.nranks, cudaMemcpyHostToDevice));
-    CU(cudaMemset(d.rng_used, 0, sizeof(int) * g.nranks));
+    CU(h2d(ctx, d.rng_rot, tab.data(), tab.size() * sizeof(double)));
+    CU(h2d(ctx, d.rng_base, base.data(), sizeof(long long) * g.nranks));
+    CU(dzero(ctx, d.rng_used, sizeof(int) * g.nranks));
     return MMS_OK;
 }
 
@@ -338,6 +368,25 @@ mms_status read_ctl(mms_ctx *ctx)
 }
 
 int launch_one_step(mms_ctx *ctx, int start_stage);
+
+AmParams am_params(const mms_params &p)
+{
+    AmParams m;
+    m.lsd = p.lsd;
+    m.lv = p.lv;
+    m.lhs = p.lhs;
+    m.lab = p.lab;
+    m.lpow = p.lpow;
+    m.liniT = p.liniT;
+    m.lthcon = p.lthcon;
+    m.rho_cp = p.rho * p.lcp;
+    m.x0 = p.x0;
+    m.y0 = p.y0;
+    m.z0 = p.z0;
+    m.amtracks = p.amtracks;
+    m.nsbx_times_sbx = p.gnsbx * p.gsdimx;
+    return m;
+}
 
 // Captures one whole step into a graph (once per kernel-argument set).
 mms_status ensure_graph(mms_ctx *ctx)
@@ -366,8 +415,7 @@ int launch_one_step(mms_ctx *ctx, int start_stage)
     int n = 0;
     const mms_params &p = ctx->p;
     if (start_stage == 0 && p.am) {
-        n += launch_temp_am(ctx->ka, ctx->stream, ctx->prof, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
-                            p.rho * p.lcp, p.x0, p.y0, p.z0, p.amtracks, p.gnsbx * p.gsdimx);
+        n += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, ctx->prof);
     }
     n += launch_step(ctx->ka, ctx->tma, ctx->prec, ctx->stream, start_stage, ctx->prof);
     return n;
@@ -382,7 +430,7 @@ mms_status sync_grains(mms_ctx *ctx)
     if (ng <= ctx->grains_synced) return MMS_OK;
     int first = ctx->grains_synced, cnt = ng - first;
     std::vector<GrainLog> log(cnt);
-    CU(cudaMemcpy(log.data(), ctx->ka.d.grain_log + first, sizeof(GrainLog) * cnt, cudaMemcpyDeviceToHost));
+    CU(d2h(ctx, log.data(), ctx->ka.d.grain_log + first, sizeof(GrainLog) * cnt));
     if ((int)ctx->grains.size() < ng) ctx->grains.resize(ng);
     const mms_params &p = ctx->p;
     const Geo &g = ctx->ka.g;
@@ -626,9 +674,7 @@ int mms_kernel_count(void) { return mms::KID_COUNT; }
 
 const char *mms_kernel_name(int id)
 {
-    static const char *names[mms::KID_COUNT] = {"k_temp_am",    "k_nuc",         "k_act",
-                                                "k_curv",       "k_diffuse_fs",  "k_list_count",
-                                                "k_list_scan",  "k_list_write",  "k_capture"};
+    static const char *names[mms::KID_COUNT] = {"k_temp_am", "k_nuc", "k_act", "k_curv", "k_diffuse_fs", "k_list", "k_capture"};
     return (id >= 0 && id < mms::KID_COUNT) ? names[id] : "";
 }
 
@@ -752,11 +798,12 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         return fail(st);
     if (p.am) {
         if ((st = dalloc(ctx, &d.T, N))) return fail(st);
+        if ((st = dalloc(ctx, &d.am_tab, (size_t)400 * (g.gx + g.gy + g.gz + 6) + (size_t)(g.gz + 2)))) return fail(st);
         if (p.amlayer > 1 && (st = dalloc(ctx, &d.lsindex, N))) return fail(st);
     }
     if (p.tip_curv && (st = dalloc(ctx, &d.curv, N))) return fail(st);
     const size_t nb = (size_t)(g.blocks_per_rank * g.nranks);
-    if ((st = dalloc(ctx, &d.blk_cnt, nb)) || (st = dalloc(ctx, &d.blk_off, nb)) ||
+    if ((st = dalloc(ctx, &d.list_status, nb)) || (st = dalloc(ctx, &d.blk_off, nb)) ||
         (st = dalloc(ctx, &d.rank_gindex, g.nranks)) || (st = dalloc(ctx, &d.rank_dcsize, g.nranks)) ||
         (st = dalloc(ctx, &d.rank_zero_upto, g.nranks)) || (st = dalloc(ctx, &d.rank_dcbase, g.nranks)) ||
         (st = dalloc(ctx, &d.list_cell, (size_t)g.nranks * g.sbcells)) ||
@@ -770,7 +817,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
     {
         std::vector<long long> base(g.nranks);
         for (int r = 0; r < g.nranks; r++) base[r] = (long long)r * (g.sbcells + 101);
-        if (cudaMemcpy(d.rank_dcbase, base.data(), sizeof(long long) * g.nranks, cudaMemcpyHostToDevice) != cudaSuccess)
+        if (h2d(ctx, d.rank_dcbase, base.data(), sizeof(long long) * g.nranks) != cudaSuccess)
             return fail(MMS_ERR_CUDA);
     }
     {
@@ -794,7 +841,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         std::vector<double> init(N, p.Cinit);
         double *dtmp;
         if ((st = dalloc(ctx, &dtmp, N))) return fail(st);
-        if (cudaMemcpy(dtmp, init.data(), N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        if (h2d(ctx, dtmp, init.data(), N * sizeof(double)) != cudaSuccess)
             return fail(MMS_ERR_CUDA);
         ctx->launches += launch_convert(ctx->ka, ctx->prec, MMS_FIELD_CE, 1, dtmp, ctx->stream);
         ctx->launches += launch_convert(ctx->ka, ctx->prec, MMS_FIELD_CL, 1, dtmp, ctx->stream);
@@ -803,8 +850,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
     }
     if (p.am && p.amlayer > 1) {
         // tempPrepareSB_int lsindex (temperature.c:183-189) at timestep 0
-        ctx->launches += launch_temp_am(ctx->ka, ctx->stream, nullptr, p.lsd, p.lv, p.lhs, p.lab, p.lpow, p.liniT, p.lthcon,
-                                        p.rho * p.lcp, p.x0, p.y0, p.z0, p.amtracks, p.gnsbx * p.gsdimx);
+        ctx->launches += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, nullptr);
     }
     std::vector<float> thr((size_t)g.rN, INFINITY);  // reference layout
     setup_sites(ctx->p, ctx->ka.g, ctx->fixed, ctx->vols, ctx->ranks, thr, mold);
@@ -825,7 +871,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         Ctl c{};
         c.timestep = 0;
         c.num_grains = 1;  // the "zero" grain (read_ctrl.c:51)
-        if (cudaMemcpy(d.ctl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess) return fail(MMS_ERR_CUDA);
+        if (h2d(ctx, d.ctl, &c, sizeof c) != cudaSuccess) return fail(MMS_ERR_CUDA);
     }
     ctx->grains.resize(1);
     std::memset(&ctx->grains[0], 0, sizeof(mms_grain));
@@ -847,6 +893,27 @@ mms_status mms_destroy(mms_ctx *ctx)
     delete ctx->prof;
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
+    return MMS_OK;
+}
+
+mms_status mms_set_grains(mms_ctx *ctx, int n, const double *rotmat9)
+{
+    if (!ctx || n < 0 || (n && !rotmat9)) return MMS_ERR_ARG;
+    if (ctx->stepped) return MMS_ERR_STATE;
+    if ((uint64_t)n + 1 > ctx->p.maxTotalGrains + 1) return MMS_ERR_GRAIN_OVERFLOW;
+    cudaSetDevice(ctx->device);
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    if (n) CU(h2d(ctx, ctx->ka.d.grain_rot + 9, rotmat9, sizeof(double) * 9 * (size_t)n));
+    Ctl c = *ctx->h_ctl;
+    c.num_grains = n + 1;
+    CU(h2d(ctx, ctx->ka.d.ctl, &c, sizeof c));
+    *ctx->h_ctl = c;
+    ctx->grains.assign((size_t)n + 1, mms_grain{});
+    for (int g = 0; g < n; g++)
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) ctx->grains[g + 1].rotmat[i][j] = rotmat9[9 * g + 3 * i + j];
+    ctx->grains_synced = n + 1;
     return MMS_OK;
 }
 
@@ -874,7 +941,7 @@ mms_status mms_set_sites(mms_ctx *ctx, int64_t n, const int32_t *gxyz, const flo
     mms_status st = upload_sites(ctx);
     if (st) return st;
     if (ctx->p.gnUseOrientation) {
-        CU(cudaMemset(ctx->ka.d.rng_used, 0, sizeof(int) * g.nranks));
+        CU(dzero(ctx, ctx->ka.d.rng_used, sizeof(int) * g.nranks));
         st = refill_rng(ctx, true);
     }
     return st;
@@ -910,8 +977,8 @@ mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxy
     if ((st = dalloc(ctx, &d.inj_key, m)) || (st = dalloc(ctx, &d.inj_rot, 9 * m))) return st;
     d.n_inj = (long long)m;
     if (m) {
-        CU(cudaMemcpy(d.inj_key, ctx->inj_key.data(), m * sizeof(long long), cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(d.inj_rot, ctx->inj_rot.data(), 9 * m * sizeof(double), cudaMemcpyHostToDevice));
+        CU(h2d(ctx, d.inj_key, ctx->inj_key.data(), m * sizeof(long long)));
+        CU(h2d(ctx, d.inj_rot, ctx->inj_rot.data(), 9 * m * sizeof(double)));
     }
     return MMS_OK;
 }
@@ -950,7 +1017,7 @@ mms_status mms_step(mms_ctx *ctx, int nsteps)
             // refill, then resume that step at the activation stage
             if ((st = refill_rng(ctx, true))) return st;
             int zero = 0;
-            CU(cudaMemcpy(&ctx->ka.d.ctl->stall, &zero, sizeof(int), cudaMemcpyHostToDevice));
+            CU(h2d(ctx, &ctx->ka.d.ctl->stall, &zero, sizeof(int)));
             ctx->launches += launch_one_step(ctx, 1);
             unsigned long long target = ts0 + done + n;
             if ((st = read_ctl(ctx))) return st;
@@ -1508,5 +1575,389 @@ mms_status mms_adjoint_gradient(mms_ctx *ctx, const double *target_ce, mms_adjoi
     out->steps = r.nrec;
     return MMS_OK;
 }
+
+}  // extern "C"
+
+// ============================================================ batched domains
+// Many independent domains stepped together: one CUDA graph per step holds
+// every domain's nucleation and activation (parallel branches), ONE
+// persistent stencil launch over the tiles of all domains, and every
+// domain's list and capture (parallel branches).
+struct mms_batch {
+    std::vector<mms_ctx *> doms;
+    int prec = MMS_PREC_F64;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> ev_fork, ev_join;
+    void *items = nullptr;  // device array of batch items
+    long long total_tiles = 0;
+    int cpt = 1, zc = 0, grid = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_kernels = 0;
+    uint64_t launches = 0;
+    std::string err;
+};
+
+namespace {
+
+void batch_drop_graph(mms_batch *b)
+{
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+}
+
+mms_status batch_build_items(mms_batch *b)
+{
+    const size_t ib = batch_item_bytes();
+    std::vector<unsigned char> host(ib * b->doms.size());
+    long long tiles = 0;
+    for (size_t i = 0; i < b->doms.size(); i++) {
+        mms_ctx *ctx = b->doms[i];
+        ctx->tma.cpt = b->cpt;
+        ctx->tma.zc = b->zc;
+        if (!make_tma(ctx->ka, ctx->prec, ctx->tma)) {
+            b->err = "TMA descriptors could not be encoded for a batched domain";
+            return MMS_ERR_CUDA;
+        }
+        drop_graph(ctx);
+        tiles += fill_batch_item(host.data() + ib * i, ctx->ka, ctx->tma, tiles);
+    }
+    if (b->items) cudaFree(b->items);
+    b->items = nullptr;
+    if (cudaMalloc(&b->items, host.size()) != cudaSuccess) {
+        b->err = "cudaMalloc of the batch items failed";
+        return MMS_ERR_NOMEM;
+    }
+    if (cudaMemcpyAsync(b->items, host.data(), host.size(), cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return MMS_ERR_CUDA;
+    b->total_tiles = tiles;
+    b->grid = batch_grid(b->prec, b->cpt);
+    batch_drop_graph(b);
+    return MMS_OK;
+}
+
+// One step of every domain, on b->stream (captured into the step graph).
+int batch_launch_step(mms_batch *b)
+{
+    int n = 0;
+    const size_t nd = b->doms.size();
+    cudaEventRecord(b->ev_fork[0], b->stream);
+    for (size_t i = 0; i < nd; i++) {
+        mms_ctx *ctx = b->doms[i];
+        cudaStream_t s = b->side[i];
+        cudaStreamWaitEvent(s, b->ev_fork[0], 0);
+        if (ctx->p.am) n += launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, s, nullptr);
+        n += launch_step_pre(ctx->ka, ctx->prec, s, 0);
+        cudaEventRecord(b->ev_join[i], s);
+        cudaStreamWaitEvent(b->stream, b->ev_join[i], 0);
+    }
+    n += launch_stencil_batch(b->items, (int)nd, b->total_tiles, b->prec, b->cpt, b->grid, b->stream);
+    cudaEventRecord(b->ev_fork[1], b->stream);
+    for (size_t i = 0; i < nd; i++) {
+        cudaStream_t s = b->side[i];
+        cudaStreamWaitEvent(s, b->ev_fork[1], 0);
+        n += launch_step_post(b->doms[i]->ka, b->prec, s);
+        cudaEventRecord(b->ev_join[i], s);
+        cudaStreamWaitEvent(b->stream, b->ev_join[i], 0);
+    }
+    return n;
+}
+
+mms_status batch_ensure_graph(mms_batch *b)
+{
+    if (b->graph) return MMS_OK;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return MMS_ERR_CUDA;
+    int n = batch_launch_step(b);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b->graph = nullptr;
+        b->err = std::string("batch graph: ") + cudaGetErrorString(e);
+        return MMS_ERR_CUDA;
+    }
+    b->graph_kernels = n;
+    return MMS_OK;
+}
+
+// Brings a domain whose step stalled on orientation draws up to `target`.
+mms_status batch_resume(mms_ctx *ctx, unsigned long long target)
+{
+    mms_status st;
+    Ctl &c = *ctx->h_ctl;
+    while (c.stall == STALL_RNG) {
+        if ((st = refill_rng(ctx, true))) return st;
+        int zero = 0;
+        CU(h2d(ctx, &ctx->ka.d.ctl->stall, &zero, sizeof(int)));
+        ctx->launches += launch_one_step(ctx, 1);
+        if ((st = read_ctl(ctx))) return st;
+        while (c.stall == 0 && c.timestep < target) {
+            ctx->launches += launch_one_step(ctx, 0);
+            if ((st = read_ctl(ctx))) return st;
+        }
+    }
+    if (c.stall == STALL_ERROR) {
+        ctx->err = mms_status_string((mms_status)c.status);
+        return (mms_status)(c.status ? c.status : MMS_ERR_STATE);
+    }
+    return MMS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mms_status mms_batch_destroy(mms_batch *b)
+{
+    if (!b) return MMS_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graph(b);
+    for (mms_ctx *ctx : b->doms) mms_destroy(ctx);
+    if (b->items) cudaFree(b->items);
+    for (cudaStream_t s : b->side) cudaStreamDestroy(s);
+    for (cudaEvent_t e : b->ev_fork) cudaEventDestroy(e);
+    for (cudaEvent_t e : b->ev_join) cudaEventDestroy(e);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return MMS_OK;
+}
+
+mms_status mms_batch_create(int n, const mms_params *params, mms_batch **out)
+{
+    if (!out || n < 1 || !params) return MMS_ERR_ARG;
+    *out = nullptr;
+    for (int i = 1; i < n; i++)
+        if (params[i].precision != params[0].precision || params[i].device != params[0].device) return MMS_ERR_ARG;
+    mms_batch *b = new mms_batch();
+    b->prec = params[0].precision == MMS_PREC_F32 ? MMS_PREC_F32 : MMS_PREC_F64;
+    b->device = params[0].device;
+    for (int i = 0; i < n; i++) {
+        mms_ctx *ctx = nullptr;
+        mms_status st = mms_create(&params[i], &ctx);
+        if (st) {
+            mms_batch_destroy(b);
+            return st;
+        }
+        b->doms.push_back(ctx);
+    }
+    cudaSetDevice(b->device);
+    cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    b->side.resize(n);
+    b->ev_join.resize(n);
+    b->ev_fork.resize(2);
+    for (int i = 0; i < n; i++) {
+        cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking);
+        cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming);
+    }
+    for (auto &e : b->ev_fork) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    for (mms_ctx *ctx : b->doms) mms_set_stream(ctx, b->stream);
+    mms_status st = batch_build_items(b);
+    if (st) {
+        mms_batch_destroy(b);
+        return st;
+    }
+    *out = b;
+    return MMS_OK;
+}
+
+int mms_batch_size(const mms_batch *b) { return b ? (int)b->doms.size() : 0; }
+
+mms_ctx *mms_batch_domain(mms_batch *b, int i)
+{
+    if (!b || i < 0 || i >= (int)b->doms.size()) return nullptr;
+    return b->doms[i];
+}
+
+mms_status mms_batch_step(mms_batch *b, int nsteps)
+{
+    if (!b || nsteps < 0) return MMS_ERR_ARG;
+    cudaSetDevice(b->device);
+    mms_status st;
+    const size_t nd = b->doms.size();
+    for (mms_ctx *ctx : b->doms) {
+        if ((st = read_ctl(ctx))) return st;
+        if (ctx->h_ctl->status) return (mms_status)ctx->h_ctl->status;
+        ctx->stepped = true;
+    }
+    std::vector<unsigned long long> ts0(nd);
+    for (size_t i = 0; i < nd; i++) ts0[i] = b->doms[i]->h_ctl->timestep;
+    const int chunk = 256;
+    int done = 0;
+    while (done < nsteps) {
+        const int n = std::min(chunk, nsteps - done);
+        if ((st = batch_ensure_graph(b))) return st;
+        for (int s = 0; s < n; s++) {
+            if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) {
+                b->err = "cudaGraphLaunch failed";
+                return MMS_ERR_CUDA;
+            }
+            b->launches += b->graph_kernels;
+        }
+        // every domain's control block, one synchronisation
+        for (mms_ctx *ctx : b->doms)
+            cudaMemcpyAsync(ctx->h_ctl, ctx->ka.d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, b->stream);
+        if (cudaStreamSynchronize(b->stream) != cudaSuccess) {
+            b->err = std::string("batch step: ") + cudaGetErrorString(cudaGetLastError());
+            return MMS_ERR_CUDA;
+        }
+        done += n;
+        for (size_t i = 0; i < nd; i++) {
+            mms_ctx *ctx = b->doms[i];
+            if (ctx->h_ctl->stall == STALL_ERROR) {
+                b->err = "domain " + std::to_string(i) + ": " + mms_status_string((mms_status)ctx->h_ctl->status);
+                return (mms_status)(ctx->h_ctl->status ? ctx->h_ctl->status : MMS_ERR_STATE);
+            }
+            if (ctx->h_ctl->stall == STALL_RNG && (st = batch_resume(ctx, ts0[i] + done))) {
+                b->err = "domain " + std::to_string(i) + ": " + ctx->err;
+                return st;
+            }
+            if ((st = refill_rng(ctx, false))) return st;
+        }
+    }
+    return MMS_OK;
+}
+
+mms_status mms_batch_set_stencil_tile(mms_batch *b, int cells_per_thread, int zchunk)
+{
+    if (!b || (cells_per_thread != 1 && cells_per_thread != 2) || zchunk < 0 || zchunk > 64) return MMS_ERR_ARG;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    b->cpt = cells_per_thread;
+    b->zc = zchunk;
+    return batch_build_items(b);
+}
+
+mms_status mms_batch_get_stencil_tile(const mms_batch *b, int *cells_per_thread, int *zchunk, int *grid)
+{
+    if (!b) return MMS_ERR_ARG;
+    if (cells_per_thread) *cells_per_thread = b->cpt;
+    if (zchunk) *zchunk = b->zc;
+    if (grid) *grid = b->grid;
+    return MMS_OK;
+}
+
+// Batch tile autotuner: the persistent stencil over all domains is timed for
+// every candidate tile on shadows of the fields it writes (as mms_autotune
+// does for one domain); the fastest by median of `reps` launches is kept.
+mms_status mms_batch_autotune(mms_batch *b, int reps, int *cells_per_thread, int *zchunk, double *best_ms)
+{
+    if (!b || reps < 1) return MMS_ERR_ARG;
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->stream);
+    const size_t nd = b->doms.size();
+    std::vector<void *> shadow;
+    auto release = [&]() {
+        cudaStreamSynchronize(b->stream);
+        for (void *q : shadow) cudaFree(q);
+    };
+    std::vector<KernelArgs> sargs(nd);
+    for (size_t i = 0; i < nd; i++) {
+        mms_ctx *ctx = b->doms[i];
+        mms_status st = read_ctl(ctx);
+        if (st) {
+            release();
+            return st;
+        }
+        const Geo &g = ctx->ka.g;
+        const size_t N = (size_t)g.N, rs = ctx->prec == MMS_PREC_F32 ? sizeof(float) : sizeof(double);
+        KernelArgs sa = ctx->ka;
+        const int pout = (int)((ctx->h_ctl->timestep + 1) & 1ULL);
+        auto sh = [&](const void *src, size_t bytes) -> void * {
+            void *d = nullptr;
+            if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
+            shadow.push_back(d);
+            cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, b->stream);
+            return d;
+        };
+        sa.d.ce = sh(sa.d.ce, N * rs);
+        sa.d.cl[pout] = sh(sa.d.cl[pout], N * rs);
+        sa.d.fs[pout] = sh(sa.d.fs[pout], N * rs);
+        sa.d.gr = (int *)sh(sa.d.gr, N * sizeof(int));
+        sa.d.solid_bits = (unsigned *)sh(sa.d.solid_bits, (size_t)g.nwords * sizeof(unsigned));
+        sa.d.ctl = (Ctl *)sh(sa.d.ctl, sizeof(Ctl));
+        if (!sa.d.ce || !sa.d.cl[pout] || !sa.d.fs[pout] || !sa.d.gr || !sa.d.solid_bits || !sa.d.ctl) {
+            release();
+            b->err = "autotune shadow buffers: out of memory";
+            return MMS_ERR_NOMEM;
+        }
+        Ctl c = *ctx->h_ctl;
+        c.timestep += 1;
+        c.status = 0;
+        c.stall = 0;
+        cudaMemcpyAsync(sa.d.ctl, &c, sizeof c, cudaMemcpyHostToDevice, b->stream);
+        cudaStreamSynchronize(b->stream);
+        sargs[i] = sa;
+    }
+    const size_t ib = batch_item_bytes();
+    std::vector<unsigned char> host(ib * nd);
+    void *ditems = nullptr;
+    if (cudaMalloc(&ditems, host.size()) != cudaSuccess) {
+        release();
+        return MMS_ERR_NOMEM;
+    }
+    shadow.push_back(ditems);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e300;
+    int bc = b->cpt, bz = b->zc;
+    for (int cpt = 1; cpt <= 2; cpt++)
+        for (int zc : {0, 8, 16, 32}) {
+            long long tiles = 0;
+            bool ok = true;
+            for (size_t i = 0; i < nd && ok; i++) {
+                TmaHolder th{};
+                th.cpt = cpt;
+                th.zc = zc;
+                ok = make_tma(sargs[i], b->prec, th) != 0;
+                tiles += fill_batch_item(host.data() + ib * i, sargs[i], th, tiles);
+            }
+            if (!ok) continue;
+            cudaMemcpyAsync(ditems, host.data(), host.size(), cudaMemcpyHostToDevice, b->stream);
+            cudaStreamSynchronize(b->stream);
+            const int grid = batch_grid(b->prec, cpt);
+            std::vector<float> ms;
+            for (int r = 0; r < reps + 2; r++) {
+                cudaEventRecord(e0, b->stream);
+                launch_stencil_batch(ditems, (int)nd, tiles, b->prec, cpt, grid, b->stream);
+                cudaEventRecord(e1, b->stream);
+                cudaEventSynchronize(e1);
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e0, e1);
+                if (r >= 2) ms.push_back(t);
+            }
+            if (cudaGetLastError() != cudaSuccess) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                release();
+                b->err = "batch autotune launch failed";
+                return MMS_ERR_CUDA;
+            }
+            std::sort(ms.begin(), ms.end());
+            if (ms[ms.size() / 2] < best) {
+                best = ms[ms.size() / 2];
+                bc = cpt;
+                bz = zc;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    release();
+    b->cpt = bc;
+    b->zc = bz;
+    mms_status st = batch_build_items(b);
+    if (cells_per_thread) *cells_per_thread = bc;
+    if (zchunk) *zchunk = bz;
+    if (best_ms) *best_ms = best;
+    return st;
+}
+
+uint64_t mms_batch_kernel_launches(const mms_batch *b) { return b ? b->launches : 0; }
+
+const char *mms_batch_last_error(const mms_batch *b) { return b ? b->err.c_str() : ""; }
 
 }  // extern "C"

@@ -29,7 +29,7 @@ struct Ctl {
     int stall;                    // non-zero: later kernels of the step do nothing
     unsigned long long stall_step;
     int list_total;               // interface-list length over all ranks this step
-    int zero_needed;              // dc_tmp regions to clear this step (bit per rank < 32, else flag)
+    int list_ticket;              // k_list blocks started this step
     int new_grains;               // grains created by the last activation
     int pad0;
 };
@@ -129,6 +129,7 @@ struct DevPtrs {
     Dc3 *dc;
     unsigned *solid_bits;  // gr > 0 after fs_change (written by the stencil)
     double *T;            // AM temperature at the current step (N) or null
+    double *am_tab;       // AM quadrature tables (400 x (gx+gy+gz+6)) and plane flags
     int *lsindex;         // AM layer flag or null
     double *curv;         // curvature (N) when TipCurvature
     // nucleation sites, sorted by (emulated rank, local raster)
@@ -160,11 +161,11 @@ struct DevPtrs {
     double *grain_rot;      // (max_grains + 1) x 9
     GrainLog *grain_log;    // (max_grains + 2)
     // interface list and capture
-    int *blk_cnt;           // per list block
-    int *blk_off;
+    unsigned long long *list_status;  // per list block: look-back status word
+    int *blk_off;           // per list block: list position of its first entry
     int *rank_gindex;       // per rank, list length
     int *rank_dcsize;       // per rank, dc_tmp logical size
-    int *rank_zero_upto;    // per rank, slots to clear this step (0 = none)
+    int *rank_zero_upto;    // per rank: slots 1..n read as zero this step (0 = none)
     long long *rank_dcbase; // per rank, offset of its dc_tmp region
     long long *list_cell;   // list position -> cell
     int *list_gid;          // list position -> captured grain id (0 = not captured)
@@ -198,8 +199,7 @@ struct KernelArgs {
 
 // Kernel ids for per-kernel timing.
 enum KernelId : int {
-    KID_TEMP_AM = 0, KID_NUC, KID_ACT, KID_CURV, KID_DIFFUSE_FS, KID_LIST_COUNT, KID_LIST_SCAN,
-    KID_LIST_WRITE, KID_CAPTURE, KID_COUNT
+    KID_TEMP_AM = 0, KID_NUC, KID_ACT, KID_CURV, KID_DIFFUSE_FS, KID_LIST, KID_CAPTURE, KID_COUNT
 };
 
 // Opaque storage for the stencil's TMA descriptors (built in kernels.cu).
@@ -228,9 +228,25 @@ int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *
 int make_tma(const KernelArgs &a, int precision, TmaHolder &out);
 // the diffusion + fs-change stencil alone (tile autotuning)
 int launch_stencil(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream);
-int launch_temp_am(const KernelArgs &a, void *stream, Profiler *prof, double lsd, double lv, double lhs, double lab,
-                   double lpow, double liniT, double lthcon, double rho_cp, double x0, double y0,
-                   double z0, int amtracks, int nsbx_times_sbx);
+// the kernels of a step before / after the stencil
+int launch_step_pre(const KernelArgs &a, int precision, void *stream, int start_stage);
+int launch_step_post(const KernelArgs &a, int precision, void *stream);
+// Batched stencil over many domains: one item per domain (opaque, built by
+// fill_batch_item, which returns the domain's tile count), one persistent
+// launch of batch_grid CTAs.
+size_t batch_item_bytes();
+long long fill_batch_item(void *dst, const KernelArgs &a, const TmaHolder &tma, long long tile_begin);
+int batch_grid(int precision, int cpt);
+int launch_stencil_batch(const void *items, int nitems, long long total_tiles, int precision, int cpt, int grid,
+                         void *stream);
+// AM laser parameters (BB_struct, read_ctrl.c) for the moving-source quadrature
+struct AmParams {
+    double lsd, lv, lhs, lab, lpow, liniT, lthcon, rho_cp, x0, y0, z0;
+    int amtracks, nsbx_times_sbx;
+};
+// Temperature of the next step for the AM model (tables + contraction);
+// FP32 tables and sums in the FP32 form.
+int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof);
 int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream);
 int launch_fill_temperature(const KernelArgs &a, double *dev_out, void *stream);
 int launch_compute_d(const KernelArgs &a, int precision, double *dev_out, void *stream);

@@ -606,6 +606,39 @@ static int cmp_long(const void *a, const void *b)
     return (x > y) - (x < y);
 }
 
+/* Pre-filled microstructure (the library's mms_set_grains): grains 1..n
+ * with the given rotation matrices; nucleated grains continue from n+1. */
+int mmso_set_grains(mmso *o, int n, const double *rot9)
+{
+    if (n < 0 || o->stepped || (uint64_t)n + 1 > o->p.maxTotalGrains + 1) return MMS_ERR_ARG;
+    if (n + 1 > o->grains_cap) {
+        long nc = n + 1024;
+        o->grains = (mms_grain *)realloc(o->grains, sizeof(mms_grain) * (size_t)nc);
+        o->grains_cap = nc;
+    }
+    memset(o->grains + 1, 0, sizeof(mms_grain) * (size_t)(o->grains_cap - 1));
+    for (int g = 0; g < n; g++)
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) o->grains[g + 1].rotmat[a][b] = rot9[9 * g + 3 * a + b];
+    o->num_grains = n + 1;
+    return MMS_OK;
+}
+
+/* Field upload in the halo'd layout (ce, cl, fs, gr, dc). */
+int mmso_set_field(mmso *o, int field, const void *in)
+{
+    size_t N = (size_t)o->N;
+    switch (field) {
+    case MMS_FIELD_CE: memcpy(o->ce, in, N * sizeof(double)); break;
+    case MMS_FIELD_CL: memcpy(o->cl, in, N * sizeof(double)); break;
+    case MMS_FIELD_FS: memcpy(o->fs, in, N * sizeof(double)); break;
+    case MMS_FIELD_GR: memcpy(o->gr, in, N * sizeof(int)); break;
+    case MMS_FIELD_DC: memcpy(o->dc, in, N * sizeof(dc3)); break;
+    default: return MMS_ERR_ARG;
+    }
+    return MMS_OK;
+}
+
 int mmso_set_site_orientations(mmso *o, int64_t n, const int32_t *gxyz, const double *rot9)
 {
     free(o->inj_idx);

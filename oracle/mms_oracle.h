@@ -24,6 +24,8 @@ mmso *mmso_create(const mms_params *p, int *status);
 void mmso_destroy(mmso *o);
 int mmso_set_sites(mmso *o, int64_t n, const int32_t *gxyz, const float *thr);
 int mmso_set_site_orientations(mmso *o, int64_t n, const int32_t *gxyz, const double *rot9);
+int mmso_set_grains(mmso *o, int n, const double *rot9);
+int mmso_set_field(mmso *o, int field, const void *in);
 /* enable the sb_curvature call before fs_change when TipCurvature is 1 */
 void mmso_enable_curvature(mmso *o, int on);
 int mmso_step(mmso *o, int nsteps);

@@ -33,6 +33,8 @@ def load():
     lib.mmso_destroy.argtypes = [P]
     lib.mmso_set_sites.argtypes = [P, C.c_int64, P, P]
     lib.mmso_set_site_orientations.argtypes = [P, C.c_int64, P, P]
+    lib.mmso_set_grains.argtypes = [P, C.c_int, P]
+    lib.mmso_set_field.argtypes = [P, C.c_int, P]
     lib.mmso_enable_curvature.argtypes = [P, C.c_int]
     lib.mmso_step.argtypes = [P, C.c_int]
     lib.mmso_timestep.restype = C.c_uint64
@@ -99,6 +101,20 @@ class Oracle:
         g = np.ascontiguousarray(gxyz, dtype=np.int32).reshape(-1, 3)
         r = np.ascontiguousarray(rot, dtype=np.float64).reshape(-1, 9)
         load().mmso_set_site_orientations(self._o, len(r), g.ctypes.data, r.ctypes.data)
+
+    def set_grains(self, rot):
+        r = np.ascontiguousarray(rot, dtype=np.float64).reshape(-1, 9)
+        st = load().mmso_set_grains(self._o, len(r), r.ctypes.data)
+        if st:
+            raise RuntimeError(f"mmso_set_grains failed with status {st}")
+
+    def upload(self, name, arr):
+        from mumatscale_b200 import FIELD
+        dt = np.int32 if name == "gr" else np.float64
+        a = np.ascontiguousarray(arr, dtype=dt)
+        st = load().mmso_set_field(self._o, FIELD[name], a.ctypes.data)
+        if st:
+            raise RuntimeError(f"mmso_set_field failed with status {st}")
 
     @property
     def timestep(self):

@@ -67,6 +67,29 @@ def test_am_tolerance(built, cuda_device):
             assert np.linalg.norm(ce - ce0) / np.linalg.norm(ce0) < 1e-6
 
 
+def test_am_fp32_form_error(built, cuda_device):
+    """AM deck in the FP32 form (FP32 quadrature tables and sums, FP32
+    stencil) against the FP64 oracle after the laser turns on.  Bounds:
+    temperature max error < 1e-5 of its maximum, grain-id mismatch < 1 % of
+    cells, ce relative L2 error < 1e-5."""
+    from _oracle import Oracle
+    p = M.read_deck(golden_deck("am1"))
+    o = Oracle(p)
+    with M.Domain(p, precision=M.PREC_F32) as dom:
+        for s in (110, 130):
+            o.step(s - o.timestep)
+            dom.step(s - dom.timestep)
+            T, T0 = dom.download("temperature"), o.download("temperature")
+            terr = float(np.abs(T - T0).max() / np.abs(T0).max())
+            assert terr < 1e-5, terr
+            gr, gr0 = dom.download("gr"), o.download("gr")
+            mism = float((gr != gr0).mean())
+            assert mism < 1e-2, mism
+            ce, ce0 = dom.download("ce"), o.download("ce")
+            rel = float(np.linalg.norm(ce - ce0) / np.linalg.norm(ce0))
+            assert rel < 1e-5, rel
+
+
 @pytest.mark.parametrize("name", ["small1", "small4", "grad1"])
 def test_fp64_matches_oracle_every_step(built, cuda_device, name):
     """Step-by-step equality for the first 150 steps (catches transient
