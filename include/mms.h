@@ -260,6 +260,25 @@ mms_status mms_get_grains(mms_ctx *ctx, int first, int count, mms_grain *out);
  * is non-NULL and returns the summary line's numbers. */
 mms_status mms_output_grains(mms_ctx *ctx, const char *path, mms_grain_summary *out);
 
+/* ParaView output in the layout of io_vtk.c: <base>_<ts>.pvtu naming one
+ * piece per subblock, <base>_<sbid>/<ts>.vtu with the cell arrays
+ * Temperature (Float64) and Grain (Int32) on hexahedral cells
+ * (writepvtu/writevtu, io_vtk.c:39-463), plain-text encoding.  base NULL =
+ * the deck's BaseFileName. */
+mms_status mms_write_vtk(mms_ctx *ctx, const char *base);
+/* The same files from caller arrays in the halo'd layout (host only). */
+mms_status mms_write_vtk_arrays(const mms_params *p, const char *base, int64_t timestep,
+                                const double *temperature, const int32_t *gr);
+
+/* Raw checkpoint of a context (device layout, this library's format): every
+ * array a later step reads, the grain table, the orientation tables and the
+ * state of the per-rank random streams, the sites and orientation
+ * overrides.  Loading into a context created from the same deck and form
+ * continues exactly as the saved context would have (the role of
+ * checkpoint.c's restart, checkpoint.c:955-1244, without HDF5). */
+mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path);
+mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path);
+
 /* ---- the time loop (loop.c:186-271) ----------------------------------------- */
 
 /* Runs the reference time loop to its termination (FinishTime / FsFinish,

@@ -180,6 +180,10 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_adjoint_replay_loss": (I, [P, P, C.POINTER(D), C.POINTER(D)]),
         "mms_adjoint_release": (I, [P]),
         "mms_set_grains": (I, [P, I, P]),
+        "mms_write_vtk": (I, [P, C.c_char_p]),
+        "mms_checkpoint_save": (I, [P, C.c_char_p]),
+        "mms_checkpoint_load": (I, [P, C.c_char_p]),
+        "mms_write_vtk_arrays": (I, [C.POINTER(Params), C.c_char_p, C.c_int64, P, P]),
         "mms_batch_create": (I, [I, C.POINTER(Params), C.POINTER(P)]),
         "mms_batch_destroy": (I, [P]),
         "mms_batch_size": (I, [P]),
@@ -212,6 +216,14 @@ def _check(status: int, where: str, ctx=None) -> None:
         if ctx:
             detail = (_lib().mms_last_error(ctx) or b"").decode()
         raise MmsError(status, where, detail)
+
+
+def write_vtk_arrays(params: Params, base: str, timestep: int, temperature: np.ndarray, gr: np.ndarray) -> None:
+    """ParaView files (io_vtk.c layout) from halo'd host arrays."""
+    t = np.ascontiguousarray(temperature, dtype=np.float64)
+    g = np.ascontiguousarray(gr, dtype=np.int32)
+    _check(_lib().mms_write_vtk_arrays(C.byref(params), base.encode(), timestep, t.ctypes.data, g.ctypes.data),
+           "mms_write_vtk_arrays")
 
 
 def default_params() -> Params:
@@ -398,6 +410,16 @@ class Domain:
         t = np.ascontiguousarray(thresholds, dtype=np.float32).reshape(-1)
         _check(_lib().mms_set_sites(self._ctx, len(t), g.ctypes.data, t.ctypes.data),
                "mms_set_sites", self._ctx)
+
+    def checkpoint_save(self, path: str) -> None:
+        _check(_lib().mms_checkpoint_save(self._ctx, str(path).encode()), "mms_checkpoint_save", self._ctx)
+
+    def checkpoint_load(self, path: str) -> None:
+        _check(_lib().mms_checkpoint_load(self._ctx, str(path).encode()), "mms_checkpoint_load", self._ctx)
+
+    def write_vtk(self, base: str | None = None) -> None:
+        """<base>_<ts>.pvtu + <base>_<sbid>/<ts>.vtu (io_vtk.c layout)."""
+        _check(_lib().mms_write_vtk(self._ctx, base.encode() if base else None), "mms_write_vtk", self._ctx)
 
     def set_grains(self, rotmats: np.ndarray) -> None:
         """Grains 1..n of a pre-filled microstructure (row-major 3x3 rotations)."""

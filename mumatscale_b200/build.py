@@ -28,7 +28,7 @@ CXX = "/usr/bin/g++"
 CC = "/usr/bin/gcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels.cu", "mms_api.cu", "adjoint.cu", "noalloc.cu"]
-CXX_SOURCES = ["deck.cpp", "host_setup.cpp"]
+CXX_SOURCES = ["deck.cpp", "host_setup.cpp", "output.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

@@ -219,16 +219,30 @@ __global__ void k_am_tables(KernelArgs a, AmParams m)
     }
 }
 
-// T over tiles of 64 x-cells by 128 (y, z) rows: 16 x 16 threads, each
-// keeping 4 x 8 sums (x = lane + 16 m, rows = 8 consecutive), streaming the
-// node axis through shared memory 16 nodes at a time.  Per node a thread
-// loads 4 X values and 8 YZ products (two 16-byte loads shared by the half
-// warp) for 32 fused multiply-adds.
-constexpr int AMC_X = 64, AMC_YZ = 128, AMC_CH = 16, AMC_NT = 256, AMC_MX = 4, AMC_MY = 8;
+// T over tiles of (XL MX) x-cells by (G MY) (y, z) rows, G = 256 / XL: each
+// thread keeps MX x MY sums (x cells XL apart, MY consecutive rows), streaming
+// the node axis through shared memory 16 nodes at a time; per node a thread
+// reads MX X values (consecutive across the x lanes, no bank conflicts) and
+// MY YZ products (the same for the lanes of one row group) for MX MY fused
+// multiply-adds.
+template <typename Real>
+struct AmTile;
+template <>
+struct AmTile<double> {
+    static constexpr int XL = 16, MX = 4, MY = 8, MINB = 2;
+};
+template <>
+struct AmTile<float> {
+    static constexpr int XL = 16, MX = 4, MY = 8, MINB = 2;
+};
+constexpr int AMC_CH = 16, AMC_NT = 256;
 
 template <typename Real>
-__global__ void __launch_bounds__(AMC_NT) k_am_contract(KernelArgs a, AmParams m)
+__global__ void __launch_bounds__(AMC_NT, AmTile<Real>::MINB) k_am_contract(KernelArgs a, AmParams m)
 {
+    using TL = AmTile<Real>;
+    constexpr int XL = TL::XL, MX = TL::MX, MY = TL::MY, G = AMC_NT / XL;
+    constexpr int TX = XL * MX, TR = G * MY;
     const Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
     const Geo &g = a.g;
@@ -236,65 +250,84 @@ __global__ void __launch_bounds__(AMC_NT) k_am_contract(KernelArgs a, AmParams m
     const int nx = g.gx + 2, ny = g.gy + 2, nz = g.gz + 2;
     const Real *X = (const Real *)a.d.am_tab, *Y = X + (long long)AM_NT * nx, *Z = Y + (long long)AM_NT * ny;
     const int *zon = (const int *)(Z + (long long)AM_NT * nz);
-    __shared__ __align__(16) Real sX[AMC_CH][AMC_X];
-    __shared__ __align__(16) Real sYZ[AMC_CH][AMC_YZ];
-    const int tid = threadIdx.x, xl = tid & 15, grp = tid >> 4;  // 16 x-lanes, 16 row groups
-    const int x0 = blockIdx.x * AMC_X;
-    const long long r0 = (long long)blockIdx.y * AMC_YZ;  // row = K * ny + J
+    __shared__ __align__(16) Real sX[AMC_CH][TX];
+    __shared__ __align__(16) Real sYZ[AMC_CH][TR];
+    const int tid = threadIdx.x, xl = tid % XL, grp = tid / XL;
+    const int x0 = blockIdx.x * TX;
+    const long long r0 = (long long)blockIdx.y * TR;  // row = K * ny + J
     const long long nrows = (long long)ny * nz;
     __shared__ int s_any;
     if (tid == 0) s_any = 0;
     __syncthreads();
-    if (tid < AMC_YZ && r0 + tid < nrows && zon[(r0 + tid) / ny]) s_any = 1;
+    for (int q = tid; q < TR; q += AMC_NT)
+        if (r0 + q < nrows && zon[(r0 + q) / ny]) s_any = 1;
     __syncthreads();
-    Real acc[AMC_MX][AMC_MY];
+    Real acc[MX][MY];
 #pragma unroll
-    for (int u = 0; u < AMC_MX; u++)
+    for (int u = 0; u < MX; u++)
 #pragma unroll
-        for (int q = 0; q < AMC_MY; q++) acc[u][q] = 0;
+        for (int q = 0; q < MY; q++) acc[u][q] = 0;
     if (s_any) {
-        // each thread stages the same x column and the same (y, z) row of
-        // every chunk: their table offsets are fixed for the whole sum
-        constexpr int XSTEP = AMC_NT / AMC_X, YSTEP = AMC_NT / AMC_YZ;  // nodes apart
-        const int xx = tid % AMC_X, xi0 = tid / AMC_X, rl = tid % AMC_YZ, yi0 = tid / AMC_YZ;
+        // each thread stages the same x columns and (y, z) rows of every
+        // chunk: their table offsets are fixed for the whole sum
+        constexpr int XSTEP = AMC_NT / TX;
+        const int xx = tid % TX, xi0 = tid / TX;
         const bool xin = x0 + xx < nx;
-        const long long row = r0 + rl;
-        const bool rin = row < nrows;
-        const int Kr = rin ? (int)(row / ny) : 0, Jr = rin ? (int)(row - (long long)Kr * ny) : 0;
-        const Real *Xp = X + (x0 + xx), *Yp = Y + Jr, *Zp = Z + Kr;
+        const Real *Xp = X + (x0 + xx);
+        static_assert(AMC_NT % TR == 0 || TR % AMC_NT == 0, "row staging");
+        constexpr int YSTEP = TR >= AMC_NT ? 1 : AMC_NT / TR;     // nodes apart
+        constexpr int RPT = TR >= AMC_NT ? TR / AMC_NT : 1;       // rows per thread
+        const int yi0 = TR >= AMC_NT ? 0 : tid / TR;
+        const Real *Yp[RPT];
+        const Real *Zp[RPT];
+        bool rin[RPT];
+#pragma unroll
+        for (int w = 0; w < RPT; w++) {
+            const int rl = (tid % (TR < AMC_NT ? TR : AMC_NT)) + w * AMC_NT;
+            const long long row = r0 + rl;
+            rin[w] = row < nrows;
+            const int Kr = rin[w] ? (int)(row / ny) : 0, Jr = rin[w] ? (int)(row - (long long)Kr * ny) : 0;
+            Yp[w] = Y + Jr;
+            Zp[w] = Z + Kr;
+        }
         for (int i0 = 0; i0 < AM_NT; i0 += AMC_CH) {
 #pragma unroll
             for (int ii = xi0; ii < AMC_CH; ii += XSTEP)
                 sX[ii][xx] = xin ? Xp[(long long)(i0 + ii) * nx] : (Real)0;
 #pragma unroll
             for (int ii = yi0; ii < AMC_CH; ii += YSTEP)
-                sYZ[ii][rl] = rin ? Yp[(long long)(i0 + ii) * ny] * Zp[(long long)(i0 + ii) * nz] : (Real)0;
+#pragma unroll
+                for (int w = 0; w < RPT; w++) {
+                    const int rl = (tid % (TR < AMC_NT ? TR : AMC_NT)) + w * AMC_NT;
+                    sYZ[ii][rl] = rin[w] ? Yp[w][(long long)(i0 + ii) * ny] * Zp[w][(long long)(i0 + ii) * nz]
+                                         : (Real)0;
+                }
             __syncthreads();
 #pragma unroll 4
             for (int ii = 0; ii < AMC_CH; ii++) {
-                Real xv[AMC_MX], yz[AMC_MY];
+                Real xv[MX], yz[MY];
 #pragma unroll
-                for (int u = 0; u < AMC_MX; u++) xv[u] = sX[ii][xl + 16 * u];
+                for (int u = 0; u < MX; u++) xv[u] = sX[ii][xl + XL * u];
 #pragma unroll
-                for (int q = 0; q < AMC_MY; q++) yz[q] = sYZ[ii][grp * AMC_MY + q];
+                for (int q = 0; q < MY; q++) yz[q] = sYZ[ii][grp * MY + q];
 #pragma unroll
-                for (int u = 0; u < AMC_MX; u++)
+                for (int u = 0; u < MX; u++)
 #pragma unroll
-                    for (int q = 0; q < AMC_MY; q++) acc[u][q] = fma(xv[u], yz[q], acc[u][q]);
+                    for (int q = 0; q < MY; q++) acc[u][q] = fma(xv[u], yz[q], acc[u][q]);
             }
             __syncthreads();
         }
     }
     const AmStep s = am_step(p, m, ctl->timestep + 1);
 #pragma unroll
-    for (int q = 0; q < AMC_MY; q++) {
-        const long long row = r0 + grp * AMC_MY + q;
+    for (int q = 0; q < MY; q++) {
+        const long long row = r0 + grp * MY + q;
         if (row >= nrows) break;
         const int K = (int)(row / ny), J = (int)(row - (long long)K * ny);
         const bool on = zon[K] != 0;
 #pragma unroll
-        for (int u = 0; u < AMC_MX; u++) {
-            const int x = x0 + xl + 16 * u;
+        for (int u = 0; u < MX; u++) {
+            const int x = x0 + xl + XL * u;
             if (x >= nx) continue;
             const long long c = (long long)K * g.sz + (long long)J * g.sy + x;
             const double T = on ? s.liniT + s.Tfront * (double)acc[u][q] : 0.0;
@@ -1219,12 +1252,14 @@ __global__ void __launch_bounds__(LIST_NT) k_list(KernelArgs a, int nblocks)
     }
     const int r = (int)(b / g.blocks_per_rank);
     const long long q0 = (b % g.blocks_per_rank) * (long long)LIST_PIECES;
-    Piece pc[NI];
+    // piece it of this thread: q0 + it * LIST_NT + thread (neighbouring
+    // threads read neighbouring bitmask words)
+    unsigned bits[NI];
     int ex[NI], tot[NI], agg = 0;
 #pragma unroll
     for (int it = 0; it < NI; it++) {
-        pc[it] = piece_of(a, r, q0 + it * LIST_NT + threadIdx.x);
-        ex[it] = block_exclusive_scan<LIST_NT>(__popc(pc[it].bits), tot[it], sh);
+        bits[it] = piece_of(a, r, q0 + it * LIST_NT + threadIdx.x).bits;
+        ex[it] = block_exclusive_scan<LIST_NT>(__popc(bits[it]), tot[it], sh);
         agg += tot[it];
     }
     // warp 0: decoupled look-back, 32 predecessors per round
@@ -1292,11 +1327,13 @@ __global__ void __launch_bounds__(LIST_NT) k_list(KernelArgs a, int nblocks)
     for (int it = 0; it < NI; it++) {
         int p0 = pos + ex[it];
         pos += tot[it];
-        unsigned bits = pc[it].bits;
-        while (bits) {
-            const int bit = __ffs(bits) - 1;
-            bits &= bits - 1;
-            a.d.list_cell[p0++] = pc[it].base + bit;
+        unsigned m = bits[it];
+        if (!m) continue;
+        const long long base = piece_of(a, r, q0 + it * LIST_NT + threadIdx.x).base;
+        while (m) {
+            const int bit = __ffs(m) - 1;
+            m &= m - 1;
+            a.d.list_cell[p0++] = base + bit;
         }
     }
 }
@@ -1812,15 +1849,18 @@ int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *
     cudaStream_t st = (cudaStream_t)stream;
     const Geo &g = a.g;
     const long long tab = (long long)AM_NT * (g.gx + g.gy + g.gz + 6);
-    dim3 cg((unsigned)((g.gx + 2 + AMC_X - 1) / AMC_X),
-            (unsigned)(((long long)(g.gy + 2) * (g.gz + 2) + AMC_YZ - 1) / AMC_YZ));
+    auto grid_of = [&](int tx, int tr) {
+        return dim3((unsigned)((g.gx + 2 + tx - 1) / tx), (unsigned)(((long long)(g.gy + 2) * (g.gz + 2) + tr - 1) / tr));
+    };
     PROF_BEGIN(KID_TEMP_AM);
     if (precision == MMS_PREC_F32) {
+        using T = AmTile<float>;
         k_am_tables<float><<<(unsigned)((tab + 255) / 256), 256, 0, st>>>(a, m);
-        k_am_contract<float><<<cg, AMC_NT, 0, st>>>(a, m);
+        k_am_contract<float><<<grid_of(T::XL * T::MX, AMC_NT / T::XL * T::MY), AMC_NT, 0, st>>>(a, m);
     } else {
+        using T = AmTile<double>;
         k_am_tables<double><<<(unsigned)((tab + 255) / 256), 256, 0, st>>>(a, m);
-        k_am_contract<double><<<cg, AMC_NT, 0, st>>>(a, m);
+        k_am_contract<double><<<grid_of(T::XL * T::MX, AMC_NT / T::XL * T::MY), AMC_NT, 0, st>>>(a, m);
     }
     PROF_END(KID_TEMP_AM);
     return 2;

@@ -438,6 +438,14 @@ mms_status sync_grains(mms_ctx *ctx)
         const GrainLog &lg = log[i];
         mms_grain &gr = ctx->grains[first + i];
         std::memset(&gr, 0, sizeof gr);
+        if (lg.kind == 3) {
+            // pre-filled grain (mms_set_grains): no nucleus, rotation from the table
+            double R[9];
+            CU(d2h(ctx, R, ctx->ka.d.grain_rot + 9 * (long long)(first + i), sizeof R));
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) gr.rotmat[a][b] = R[3 * a + b];
+            continue;
+        }
         long long c = lg.cell;
         long long K = c / g.sz, J = (c % g.sz) / g.sy, I = c % g.sy;
         NucPt nuc{};
@@ -498,6 +506,8 @@ cudaError_t copy_in(mms_ctx *ctx, void *dev, const void *host, size_t es)
 }
 
 }  // namespace
+
+const mms_params &ctx_params(const mms_ctx *ctx) { return ctx->p; }
 
 // ============================================================= public ABI
 extern "C" {
@@ -904,7 +914,12 @@ mms_status mms_set_grains(mms_ctx *ctx, int n, const double *rotmat9)
     cudaSetDevice(ctx->device);
     mms_status st = read_ctl(ctx);
     if (st) return st;
-    if (n) CU(h2d(ctx, ctx->ka.d.grain_rot + 9, rotmat9, sizeof(double) * 9 * (size_t)n));
+    if (n) {
+        CU(h2d(ctx, ctx->ka.d.grain_rot + 9, rotmat9, sizeof(double) * 9 * (size_t)n));
+        std::vector<GrainLog> log((size_t)n);
+        for (int g = 0; g < n; g++) log[g] = GrainLog{-1, 0ULL, 3, 0, (long long)(g + 1)};
+        CU(h2d(ctx, ctx->ka.d.grain_log + 1, log.data(), sizeof(GrainLog) * (size_t)n));
+    }
     Ctl c = *ctx->h_ctl;
     c.num_grains = n + 1;
     CU(h2d(ctx, ctx->ka.d.ctl, &c, sizeof c));
@@ -1959,5 +1974,203 @@ mms_status mms_batch_autotune(mms_batch *b, int reps, int *cells_per_thread, int
 uint64_t mms_batch_kernel_launches(const mms_batch *b) { return b ? b->launches : 0; }
 
 const char *mms_batch_last_error(const mms_batch *b) { return b ? b->err.c_str() : ""; }
+
+}  // extern "C"
+
+// ================================================================ checkpoint
+// Raw checkpoint of a context: every device array a later step reads (in
+// the device layout), the control block, the grain table and log, the
+// orientation tables, and the host side of the per-rank random streams
+// (call counts, cached Gaussian, drawn orientations), the site list and the
+// orientation overrides.  A context created from the same deck and loaded
+// from it continues exactly as the saved one would have.
+namespace {
+
+struct CkHeader {
+    char magic[8];
+    int32_t version, prec, gx, gy, gz, nranks, rng_cap, num_grains;
+    int64_t N, nsites, ninj, dctmp, P;
+    uint64_t timestep;
+};
+
+bool fwrite_all(FILE *fp, const void *p, size_t n) { return n == 0 || std::fwrite(p, 1, n, fp) == n; }
+bool fread_all(FILE *fp, void *p, size_t n) { return n == 0 || std::fread(p, 1, n, fp) == n; }
+
+}  // namespace
+
+extern "C" {
+
+mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path)
+{
+    if (!ctx || !path) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    const Geo &g = ctx->ka.g;
+    const DevPtrs &d = ctx->ka.d;
+    const size_t N = (size_t)g.N, es = ctx->prec == MMS_PREC_F32 ? sizeof(float) : sizeof(double);
+    const Ctl c = *ctx->h_ctl;
+    const int cur = (int)(c.timestep & 1ULL);
+    CkHeader h{};
+    std::memcpy(h.magic, "MMSCKPT", 8);
+    h.version = 1;
+    h.prec = ctx->prec;
+    h.gx = g.gx;
+    h.gy = g.gy;
+    h.gz = g.gz;
+    h.nranks = g.nranks;
+    h.rng_cap = d.rng_cap;
+    h.num_grains = c.num_grains;
+    h.N = (int64_t)N;
+    h.nsites = (int64_t)ctx->site_cell.size();
+    h.ninj = (int64_t)ctx->inj_key.size();
+    h.dctmp = (int64_t)g.nranks * (g.sbcells + 101);
+    h.P = g.P;
+    h.timestep = c.timestep;
+    FILE *fp = std::fopen(path, "wb");
+    if (!fp) return MMS_ERR_IO;
+    std::vector<unsigned char> buf;
+    bool ok = fwrite_all(fp, &h, sizeof h) && fwrite_all(fp, &c, sizeof c);
+    auto dev = [&](const void *src, size_t bytes) {
+        if (!ok) return;
+        buf.resize(bytes);
+        if (bytes && d2h(ctx, buf.data(), src, bytes) != cudaSuccess) ok = false;
+        ok = ok && fwrite_all(fp, buf.data(), bytes);
+    };
+    dev(d.ce, N * es);
+    dev(d.cl[cur], N * es);
+    dev(d.fs[cur], N * es);
+    dev(d.gr, N * sizeof(int));
+    dev(d.dc, N * sizeof(Dc3));
+    dev(d.dc_tmp, (size_t)h.dctmp * sizeof(Dc3));
+    dev(d.rank_dcsize, (size_t)g.nranks * sizeof(int));
+    dev(d.grain_rot, (size_t)c.num_grains * 9 * sizeof(double));
+    dev(d.grain_log, (size_t)c.num_grains * sizeof(GrainLog));
+    if (ctx->p.gnUseOrientation) {
+        dev(d.rng_rot, (size_t)g.nranks * d.rng_cap * 9 * sizeof(double));
+        dev(d.rng_used, (size_t)g.nranks * sizeof(int));
+        dev(d.rng_base, (size_t)g.nranks * sizeof(long long));
+    }
+    if (d.lsindex) dev(d.lsindex, N * sizeof(int));
+    for (const Rank &r : ctx->ranks) {
+        const int64_t na = (int64_t)r.angles.size();
+        ok = ok && fwrite_all(fp, &r.ncalls, sizeof r.ncalls) && fwrite_all(fp, &r.have_gauss, sizeof r.have_gauss) &&
+             fwrite_all(fp, &r.gauss_next, sizeof r.gauss_next) && fwrite_all(fp, &r.rng_base, sizeof r.rng_base) &&
+             fwrite_all(fp, &na, sizeof na) && fwrite_all(fp, r.angles.data(), (size_t)na * sizeof(r.angles[0]));
+    }
+    ok = ok && fwrite_all(fp, ctx->site_cell.data(), ctx->site_cell.size() * sizeof(long long)) &&
+         fwrite_all(fp, ctx->site_thr.data(), ctx->site_thr.size() * sizeof(float)) &&
+         fwrite_all(fp, ctx->site_rank.data(), ctx->site_rank.size() * sizeof(int)) &&
+         fwrite_all(fp, ctx->inj_key.data(), ctx->inj_key.size() * sizeof(long long)) &&
+         fwrite_all(fp, ctx->inj_rot.data(), ctx->inj_rot.size() * sizeof(double));
+    if (std::fclose(fp) != 0) ok = false;
+    return ok ? MMS_OK : MMS_ERR_IO;
+}
+
+mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path)
+{
+    if (!ctx || !path) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    const Geo &g = ctx->ka.g;
+    DevPtrs &d = ctx->ka.d;
+    const size_t N = (size_t)g.N, es = ctx->prec == MMS_PREC_F32 ? sizeof(float) : sizeof(double);
+    FILE *fp = std::fopen(path, "rb");
+    if (!fp) return MMS_ERR_IO;
+    CkHeader h{};
+    Ctl c{};
+    auto fail = [&](mms_status s, const char *why) {
+        std::fclose(fp);
+        ctx->err = why;
+        return s;
+    };
+    if (!fread_all(fp, &h, sizeof h) || std::memcmp(h.magic, "MMSCKPT", 8) != 0 || h.version != 1)
+        return fail(MMS_ERR_IO, "not a checkpoint of this library");
+    if (h.prec != ctx->prec || h.gx != g.gx || h.gy != g.gy || h.gz != g.gz || h.nranks != g.nranks ||
+        h.rng_cap != d.rng_cap || h.N != (int64_t)N || h.P != g.P ||
+        h.dctmp != (int64_t)g.nranks * (g.sbcells + 101) ||
+        (uint64_t)h.num_grains > ctx->p.maxTotalGrains + 1)
+        return fail(MMS_ERR_ARG, "checkpoint does not match this deck and form");
+    if (!fread_all(fp, &c, sizeof c)) return fail(MMS_ERR_IO, "truncated checkpoint");
+    const int cur = (int)(c.timestep & 1ULL);
+    std::vector<unsigned char> buf;
+    bool ok = true;
+    auto dev = [&](void *dst, size_t bytes) {
+        if (!ok) return;
+        buf.resize(bytes);
+        ok = fread_all(fp, buf.data(), bytes) && (bytes == 0 || h2d(ctx, dst, buf.data(), bytes) == cudaSuccess);
+    };
+    dev(d.ce, N * es);
+    dev(d.cl[cur], N * es);
+    dev(d.fs[cur], N * es);
+    dev(d.gr, N * sizeof(int));
+    dev(d.dc, N * sizeof(Dc3));
+    dev(d.dc_tmp, (size_t)h.dctmp * sizeof(Dc3));
+    dev(d.rank_dcsize, (size_t)g.nranks * sizeof(int));
+    dev(d.grain_rot, (size_t)h.num_grains * 9 * sizeof(double));
+    dev(d.grain_log, (size_t)h.num_grains * sizeof(GrainLog));
+    if (ctx->p.gnUseOrientation) {
+        dev(d.rng_rot, (size_t)g.nranks * d.rng_cap * 9 * sizeof(double));
+        dev(d.rng_used, (size_t)g.nranks * sizeof(int));
+        dev(d.rng_base, (size_t)g.nranks * sizeof(long long));
+    }
+    if (d.lsindex) dev(d.lsindex, N * sizeof(int));
+    if (!ok) return fail(MMS_ERR_IO, "truncated checkpoint");
+    for (Rank &r : ctx->ranks) {
+        long ncalls = 0;
+        int64_t na = 0;
+        ok = ok && fread_all(fp, &ncalls, sizeof ncalls) && fread_all(fp, &r.have_gauss, sizeof r.have_gauss) &&
+             fread_all(fp, &r.gauss_next, sizeof r.gauss_next) && fread_all(fp, &r.rng_base, sizeof r.rng_base) &&
+             fread_all(fp, &na, sizeof na);
+        if (!ok || na < 0) return fail(MMS_ERR_IO, "truncated checkpoint");
+        r.angles.resize((size_t)na);
+        ok = fread_all(fp, r.angles.data(), (size_t)na * sizeof(r.angles[0]));
+        // the random_r state: reseed and replay the same number of calls
+        const int hg = r.have_gauss;
+        const float gn = r.gauss_next;
+        r.seed_with(r.seed);
+        while (r.ncalls < ncalls) r.rand_();
+        r.have_gauss = hg;
+        r.gauss_next = gn;
+    }
+    ctx->site_cell.resize((size_t)h.nsites);
+    ctx->site_thr.resize((size_t)h.nsites);
+    ctx->site_rank.resize((size_t)h.nsites);
+    ctx->inj_key.resize((size_t)h.ninj);
+    ctx->inj_rot.resize((size_t)h.ninj * 9);
+    ok = ok && fread_all(fp, ctx->site_cell.data(), ctx->site_cell.size() * sizeof(long long)) &&
+         fread_all(fp, ctx->site_thr.data(), ctx->site_thr.size() * sizeof(float)) &&
+         fread_all(fp, ctx->site_rank.data(), ctx->site_rank.size() * sizeof(int)) &&
+         fread_all(fp, ctx->inj_key.data(), ctx->inj_key.size() * sizeof(long long)) &&
+         fread_all(fp, ctx->inj_rot.data(), ctx->inj_rot.size() * sizeof(double));
+    std::fclose(fp);
+    if (!ok) {
+        ctx->err = "truncated checkpoint";
+        return MMS_ERR_IO;
+    }
+    ctx->site_index.clear();
+    if ((st = upload_sites(ctx))) return st;
+    dfree(ctx, d.inj_key);
+    dfree(ctx, d.inj_rot);
+    d.inj_key = nullptr;
+    d.inj_rot = nullptr;
+    d.n_inj = (long long)ctx->inj_key.size();
+    if (d.n_inj) {
+        if ((st = dalloc(ctx, &d.inj_key, (size_t)d.n_inj)) || (st = dalloc(ctx, &d.inj_rot, 9 * (size_t)d.n_inj)))
+            return st;
+        CU(h2d(ctx, d.inj_key, ctx->inj_key.data(), (size_t)d.n_inj * sizeof(long long)));
+        CU(h2d(ctx, d.inj_rot, ctx->inj_rot.data(), 9 * (size_t)d.n_inj * sizeof(double)));
+    }
+    c.status = 0;
+    c.stall = 0;
+    CU(h2d(ctx, d.ctl, &c, sizeof c));
+    *ctx->h_ctl = c;
+    ctx->grains.assign(1, mms_grain{});
+    ctx->grains_synced = 1;
+    ctx->stepped = true;
+    drop_graph(ctx);
+    return MMS_OK;
+}
 
 }  // extern "C"

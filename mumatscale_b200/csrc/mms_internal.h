@@ -45,7 +45,8 @@ enum StallReason : int {
 struct GrainLog {
     long long cell;       // global halo'd linear index of the nucleus cell
     unsigned long long timestep;
-    int kind;             // 0 = deck site (nuc_pt entry), 1 = random draw, 2 = zero angles
+    int kind;             // 0 = deck site (nuc_pt entry), 1 = random draw, 2 = zero angles,
+                          // 3 = pre-filled grain (mms_set_grains)
     int rank;             // emulated rank that created it
     long long aux;        // nuc_pt entry index, or per-rank draw number
 };
@@ -268,3 +269,6 @@ int launch_adj_terminal(const Geo &g, int precision, double cinit_off, const voi
                         void *lce, void *lcl, void *lfs, double *partial, double *loss_out, void *stream);
 
 }  // namespace mms
+
+// the deck parameters a context was created with (mms_api.cu)
+const mms_params &ctx_params(const mms_ctx *ctx);
