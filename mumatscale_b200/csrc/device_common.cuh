@@ -7,6 +7,19 @@
 
 namespace mms {
 
+// A step stops at the first kernel that sees the stall flag.
+__device__ __forceinline__ bool stalled(const Ctl *c)
+{
+    return *((volatile const int *)&c->stall) != 0;
+}
+
+__device__ __forceinline__ void raise_error(Ctl *c, int status)
+{
+    atomicCAS(&c->status, 0, status);
+    atomicExch(&c->stall, (int)STALL_ERROR);
+}
+
+
 // direct_temp_calc (temperature.c:24-61) for the analytic models; the AM
 // quadrature is precomputed into an array by k_temp_am.
 __device__ __forceinline__ double temp_cell(const Phys &p, const double *Tarr, long long cell,
@@ -47,6 +60,39 @@ __device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
     q.gibbs = (Real)p.gibbs;
     q.c0k = (Real)(p.cinit * (p.k_inv - 1.0));
     return q;
+}
+
+// AM moving-source quadrature: nodes, and the source position and prefactor
+// of a step (direct_temp_calc thermal_ana == 1, temperature.c:62-123)
+constexpr int AM_NT = 400;
+
+struct AmStep {
+    double xnow, ynow, znow, lalpha, ls, ldt, Tfront, liniT;
+};
+
+__device__ __forceinline__ AmStep am_step(const Phys &p, const AmParams &m, unsigned long long ts)
+{
+    AmStep s;
+    const double sim_time = (double)ts * p.ts_delt;
+    const double invlv = 1. / m.lv;
+    s.ls = m.lsd / (2. * 1.414);
+    double xlen = m.nsbx_times_sbx * p.cellSize;
+    xlen = xlen + m.lsd;
+    double tline = xlen * invlv;
+    const double tpause = 1.5e-4 * invlv;
+    tline = tline + tpause;
+    double trackno = 0;
+    if (m.amtracks > 1) trackno = floor(sim_time / tline);
+    s.xnow = m.x0 + (sim_time - trackno * tline) * m.lv;
+    s.ynow = m.y0 + trackno * m.lhs;
+    s.znow = m.z0;
+    s.lalpha = m.lthcon / m.rho_cp;
+    const double tsteady = 20 * s.lalpha * invlv * invlv;
+    s.ldt = tsteady / AM_NT;
+    const double pw = (sim_time < 1e-4) ? 0.0 : m.lpow;
+    s.Tfront = m.lab * pw * s.lalpha / (5.568328 * m.lthcon);
+    s.liniT = m.liniT;
+    return s;
 }
 
 }  // namespace mms

@@ -39,16 +39,6 @@ namespace mms {
 
 #define FULL_MASK 0xffffffffu
 
-__device__ __forceinline__ bool stalled(const Ctl *c)
-{
-    return *((volatile const int *)&c->stall) != 0;
-}
-
-__device__ __forceinline__ void raise_error(Ctl *c, int status)
-{
-    atomicCAS(&c->status, 0, status);
-    atomicExch(&c->stall, (int)STALL_ERROR);
-}
 
 
 template <int NT>
@@ -151,37 +141,6 @@ __device__ __forceinline__ void fence_barrier_init()
 // Z_i(z) = ldt exp(-lz^2/b_i) / Tl_i, built once per step (k_am_tables),
 // instead of 400 exponentials per cell (k_am_contract).  Cells above the
 // substrate top (rz > znow + dx) get T = 0.
-constexpr int AM_NT = 400;
-
-struct AmStep {
-    double xnow, ynow, znow, lalpha, ls, ldt, Tfront, liniT;
-};
-
-__device__ __forceinline__ AmStep am_step(const Phys &p, const AmParams &m, unsigned long long ts)
-{
-    AmStep s;
-    const double sim_time = (double)ts * p.ts_delt;
-    const double invlv = 1. / m.lv;
-    s.ls = m.lsd / (2. * 1.414);
-    double xlen = m.nsbx_times_sbx * p.cellSize;
-    xlen = xlen + m.lsd;
-    double tline = xlen * invlv;
-    const double tpause = 1.5e-4 * invlv;
-    tline = tline + tpause;
-    double trackno = 0;
-    if (m.amtracks > 1) trackno = floor(sim_time / tline);
-    s.xnow = m.x0 + (sim_time - trackno * tline) * m.lv;
-    s.ynow = m.y0 + trackno * m.lhs;
-    s.znow = m.z0;
-    s.lalpha = m.lthcon / m.rho_cp;
-    const double tsteady = 20 * s.lalpha * invlv * invlv;
-    s.ldt = tsteady / AM_NT;
-    const double pw = (sim_time < 1e-4) ? 0.0 : m.lpow;
-    s.Tfront = m.lab * pw * s.lalpha / (5.568328 * m.lthcon);
-    s.liniT = m.liniT;
-    return s;
-}
-
 // tables: X [AM_NT][gx+2], Y [AM_NT][gy+2], Z [AM_NT][gz+2], then the
 // per-plane flag "below the substrate top" [gz+2]
 template <typename Real>
@@ -344,14 +303,14 @@ __global__ void __launch_bounds__(AMC_NT, AmTile<Real>::MINB) k_am_contract(Kern
 // so that k_act can gather them in (emulated rank, local raster) order.
 constexpr int NUC_NT = 256;
 template <typename Real>
-__global__ void __launch_bounds__(NUC_NT) k_nuc(KernelArgs a)
+__device__ __forceinline__ void nuc_body(const KernelArgs &a, int bid)
 {
     Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
     __shared__ int sh[NUC_NT / 32];
     const Geo &g = a.g;
     const Phys &p = a.p;
-    long long s = blockIdx.x * (long long)NUC_NT + threadIdx.x;
+    long long s = bid * (long long)NUC_NT + threadIdx.x;
     int hit = 0;
     if (s < a.d.nsites) {
         unsigned long long ts = ctl->timestep + 1;
@@ -381,11 +340,17 @@ __global__ void __launch_bounds__(NUC_NT) k_nuc(KernelArgs a)
     }
     int tot;
     int pos = block_exclusive_scan<NUC_NT>(hit, tot, sh);
-    if (hit) a.d.cand_stage[blockIdx.x * (long long)NUC_NT + pos] = (int)s;
+    if (hit) a.d.cand_stage[bid * (long long)NUC_NT + pos] = (int)s;
     if (threadIdx.x == 0) {
-        a.d.nuc_blk_cnt[blockIdx.x] = tot;
+        a.d.nuc_blk_cnt[bid] = tot;
         if (tot) atomicAdd(&ctl->ncand, tot);
     }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(NUC_NT) k_nuc(KernelArgs a)
+{
+    nuc_body<Real>(a, blockIdx.x);
 }
 
 __device__ long long find_key(const long long *keys, long long n, long long key)
@@ -414,7 +379,7 @@ __device__ long long find_key(const long long *keys, long long n, long long key)
 // replaces the capped count (grain.c:1318), so the cap never holds.
 // One CTA; every phase is parallel over candidates or ranks.
 constexpr int ACT_NT = 1024;
-__global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
+__device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
 {
     Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
@@ -533,6 +498,11 @@ __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
         ctl->ncand = 0;
         ctl->timestep = ts;
     }
+}
+
+__global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
+{
+    act_body(a, rank_scratch);
 }
 
 // ---------------------------------------------------------------- curvature
@@ -1233,7 +1203,7 @@ __device__ __forceinline__ unsigned long long ls_wait(const unsigned long long *
 // outgrows its dc_tmp, the reference replaces it with a zeroed array of
 // gindex + 100 entries; here the slots that must read as zero this step are
 // recorded (rank_zero_upto) and k_capture clears them.
-__global__ void __launch_bounds__(LIST_NT) k_list(KernelArgs a, int nblocks)
+__device__ __forceinline__ void list_body(const KernelArgs &a, int nblocks)
 {
     Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
@@ -1338,6 +1308,11 @@ __global__ void __launch_bounds__(LIST_NT) k_list(KernelArgs a, int nblocks)
     }
 }
 
+__global__ void __launch_bounds__(LIST_NT) k_list(KernelArgs a, int nblocks)
+{
+    list_body(a, nblocks);
+}
+
 // capture_octahedra_diffuse, INDEX_SEP branch (growth.c:664-794), for the
 // list cell c, with grow_octahedra's half diagonal (growth.c:372-403)
 // evaluated for the solid neighbour on demand.  Returns the capturing
@@ -1420,14 +1395,14 @@ __device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs,
 // copy-back dc[cell] = dc_tmp[slot] for every entry, captured or not
 // (growth.c:789, 797-807), and the captured grain id.
 template <typename Real>
-__global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
+__device__ __forceinline__ void capture_body(const KernelArgs &a, int bid, int nb)
 {
     const Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
     const Geo &g = a.g;
     const int total = ctl->list_total;
     const Real *fs = (const Real *)a.d.fs[(int)(ctl->timestep & 1ULL)];
-    for (long long e = blockIdx.x * (long long)LIST_NT + threadIdx.x; e < total; e += (long long)gridDim.x * LIST_NT) {
+    for (long long e = bid * (long long)LIST_NT + threadIdx.x; e < total; e += (long long)nb * LIST_NT) {
         const long long c = a.d.list_cell[e];
         long long K, J, I;
         if (g.N < 0x7fffffffLL) {  // 32-bit division when every index fits
@@ -1465,6 +1440,78 @@ __global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
         a.d.list_gid[e] = gid;
     }
 }
+
+template <typename Real>
+__global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
+{
+    capture_body<Real>(a, blockIdx.x, gridDim.x);
+}
+
+// The small kernels of a step over many domains, one launch each: block b
+// belongs to the domain d with begin[d] <= b < begin[d + 1] (begin: prefix
+// sums of the domains' block counts), copies that domain's kernel arguments
+// to shared memory and runs the single-domain body with its local block.
+__device__ __forceinline__ int batch_find(const int *__restrict__ begin, int n, int b)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (begin[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int NT>
+__device__ __forceinline__ int batch_enter(const void *items, size_t stride, const int *begin, int n,
+                                           KernelArgs &sa, int &local)
+{
+    __shared__ int s_d;
+    if (threadIdx.x == 0) s_d = batch_find(begin, n, (int)blockIdx.x);
+    __syncthreads();
+    const int d = s_d;
+    const int *src = (const int *)((const unsigned char *)items + stride * (size_t)d);
+    int *dst = (int *)&sa;
+    for (int e = threadIdx.x; e < (int)(sizeof(KernelArgs) / sizeof(int)); e += NT) dst[e] = src[e];
+    __syncthreads();
+    local = (int)blockIdx.x - begin[d];
+    return d;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(NUC_NT) k_nuc_batch(const void *items, size_t stride, const int *begin, int n)
+{
+    __shared__ __align__(16) KernelArgs sa;
+    int local;
+    batch_enter<NUC_NT>(items, stride, begin, n, sa, local);
+    nuc_body<Real>(sa, local);
+}
+
+__global__ void __launch_bounds__(ACT_NT) k_act_batch(const void *items, size_t stride, const int *begin, int n)
+{
+    __shared__ __align__(16) KernelArgs sa;
+    int local;
+    batch_enter<ACT_NT>(items, stride, begin, n, sa, local);
+    act_body(sa, sa.d.act_scratch);
+}
+
+__global__ void __launch_bounds__(LIST_NT) k_list_batch(const void *items, size_t stride, const int *begin, int n)
+{
+    __shared__ __align__(16) KernelArgs sa;
+    int local;
+    const int d = batch_enter<LIST_NT>(items, stride, begin, n, sa, local);
+    list_body(sa, begin[d + 1] - begin[d]);
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(LIST_NT) k_capture_batch(const void *items, size_t stride, const int *begin, int n)
+{
+    __shared__ __align__(16) KernelArgs sa;
+    int local;
+    const int d = batch_enter<LIST_NT>(items, stride, begin, n, sa, local);
+    capture_body<Real>(sa, local, begin[d + 1] - begin[d]);
+}
+
 
 // ------------------------------------------------------------ reductions
 constexpr int RED_NT = 256;
@@ -1759,6 +1806,15 @@ static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t
     return n + launch_post_t<Real>(a, st, prof);
 }
 
+int launch_curv(const KernelArgs &a, int precision, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long tot = (long long)a.g.nranks * a.g.sbcells;
+    if (precision == MMS_PREC_F32) k_curv<float><<<(int)((tot + 255) / 256), 256, 0, st>>>(a);
+    else k_curv<double><<<(int)((tot + 255) / 256), 256, 0, st>>>(a);
+    return 1;
+}
+
 int launch_step_pre(const KernelArgs &a, int precision, void *stream, int start_stage)
 {
     cudaStream_t st = (cudaStream_t)stream;
@@ -1814,6 +1870,45 @@ int batch_grid(int precision, int cpt)
     return cpt == 2 ? batch_grid_t<double, 2>() : batch_grid_t<double, 1>();
 }
 
+// Blocks per domain of the batched small kernels (0 for a domain that
+// launches no such kernel).
+int batch_blocks(const KernelArgs &a, int which)
+{
+    const Geo &g = a.g;
+    switch (which) {
+    case 0: return a.d.nsites > 0 ? a.d.nuc_blocks : 0;                       // k_nuc
+    case 1: return 1;                                                          // k_act
+    case 2: return (int)(g.blocks_per_rank * g.nranks);                       // k_list
+    default: {                                                                 // k_capture
+        long long nb = ((long long)g.gx * g.gy * g.gz) / (LIST_NT * 64);
+        return (int)(nb < 1 ? 1 : (nb > 148 * 8 ? 148 * 8 : nb));
+    }
+    }
+}
+
+size_t batch_item_args_offset() { return offsetof(BatchItem, a); }
+
+int launch_small_batch(int which, const void *items, const int *begin, int n, int total, int precision,
+                       void *stream)
+{
+    if (total <= 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    const void *args = (const unsigned char *)items + offsetof(BatchItem, a);
+    const size_t stride = sizeof(BatchItem);
+    switch (which) {
+    case 0:
+        if (precision == MMS_PREC_F32) k_nuc_batch<float><<<total, NUC_NT, 0, st>>>(args, stride, begin, n);
+        else k_nuc_batch<double><<<total, NUC_NT, 0, st>>>(args, stride, begin, n);
+        break;
+    case 1: k_act_batch<<<total, ACT_NT, 0, st>>>(args, stride, begin, n); break;
+    case 2: k_list_batch<<<total, LIST_NT, 0, st>>>(args, stride, begin, n); break;
+    default:
+        if (precision == MMS_PREC_F32) k_capture_batch<float><<<total, LIST_NT, 0, st>>>(args, stride, begin, n);
+        else k_capture_batch<double><<<total, LIST_NT, 0, st>>>(args, stride, begin, n);
+    }
+    return 1;
+}
+
 int launch_stencil_batch(const void *items, int nitems, long long total_tiles, int precision, int cpt, int grid,
                          void *stream)
 {
@@ -1854,9 +1949,9 @@ int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *
     };
     PROF_BEGIN(KID_TEMP_AM);
     if (precision == MMS_PREC_F32) {
-        using T = AmTile<float>;
+        // tables in FP32; the contraction on the tensor cores (am_tc.cu)
         k_am_tables<float><<<(unsigned)((tab + 255) / 256), 256, 0, st>>>(a, m);
-        k_am_contract<float><<<grid_of(T::XL * T::MX, AMC_NT / T::XL * T::MY), AMC_NT, 0, st>>>(a, m);
+        launch_am_contract_tc(a, m, st);
     } else {
         using T = AmTile<double>;
         k_am_tables<double><<<(unsigned)((tab + 255) / 256), 256, 0, st>>>(a, m);

@@ -858,6 +858,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         cudaStreamSynchronize(ctx->stream);
         dfree(ctx, dtmp);
     }
+    if (p.am && ctx->prec == MMS_PREC_F32) am_tc_prepare();
     if (p.am && p.amlayer > 1) {
         // tempPrepareSB_int lsindex (temperature.c:183-189) at timestep 0
         ctx->launches += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, nullptr);
@@ -1607,6 +1608,11 @@ struct mms_batch {
     std::vector<cudaEvent_t> ev_fork, ev_join;
     void *items = nullptr;  // device array of batch items
     long long total_tiles = 0;
+    // prefix sums of the small kernels' blocks per domain (nucleation,
+    // activation, list, capture), n + 1 each, on the device
+    int *begin = nullptr;
+    int totals[4] = {0, 0, 0, 0};
+    int graph_totals[4] = {-1, -1, -1, -1};
     int cpt = 1, zc = 0, grid = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
@@ -1620,6 +1626,37 @@ void batch_drop_graph(mms_batch *b)
 {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
+}
+
+// Kernel arguments of every domain (sites and tables can be replaced
+// between calls) and the small kernels' block prefixes; the step graph is
+// dropped when a launch's block total changed.
+mms_status batch_refresh(mms_batch *b)
+{
+    const size_t nd = b->doms.size(), ib = batch_item_bytes();
+    if (!b->items) return MMS_OK;
+    std::vector<unsigned char> host(ib * nd);
+    std::vector<int> begin(4 * (nd + 1), 0);
+    long long tiles = 0;
+    for (size_t i = 0; i < nd; i++) {
+        mms_ctx *ctx = b->doms[i];
+        tiles += fill_batch_item(host.data() + ib * i, ctx->ka, ctx->tma, tiles);
+        for (int w = 0; w < 4; w++) begin[w * (nd + 1) + i + 1] = begin[w * (nd + 1) + i] + batch_blocks(ctx->ka, w);
+    }
+    if (!b->begin && cudaMalloc(&b->begin, sizeof(int) * begin.size()) != cudaSuccess) {
+        b->err = "cudaMalloc of the batch prefixes failed";
+        return MMS_ERR_NOMEM;
+    }
+    if (cudaMemcpyAsync(b->items, host.data(), host.size(), cudaMemcpyHostToDevice, b->stream) != cudaSuccess ||
+        cudaMemcpyAsync(b->begin, begin.data(), sizeof(int) * begin.size(), cudaMemcpyHostToDevice, b->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return MMS_ERR_CUDA;
+    for (int w = 0; w < 4; w++) {
+        b->totals[w] = begin[w * (nd + 1) + nd];
+        if (b->totals[w] != b->graph_totals[w]) batch_drop_graph(b);
+    }
+    return MMS_OK;
 }
 
 mms_status batch_build_items(mms_batch *b)
@@ -1650,33 +1687,45 @@ mms_status batch_build_items(mms_batch *b)
     b->total_tiles = tiles;
     b->grid = batch_grid(b->prec, b->cpt);
     batch_drop_graph(b);
-    return MMS_OK;
+    return batch_refresh(b);
 }
 
-// One step of every domain, on b->stream (captured into the step graph).
+// One step of every domain, on b->stream (captured into the step graph):
+// AM temperatures as parallel branches, then one launch each of nucleation
+// and activation over all domains, curvature branches (TipCurvature decks),
+// the persistent stencil, and one launch each of list and capture.
 int batch_launch_step(mms_batch *b)
 {
     int n = 0;
-    const size_t nd = b->doms.size();
-    cudaEventRecord(b->ev_fork[0], b->stream);
-    for (size_t i = 0; i < nd; i++) {
-        mms_ctx *ctx = b->doms[i];
-        cudaStream_t s = b->side[i];
-        cudaStreamWaitEvent(s, b->ev_fork[0], 0);
-        if (ctx->p.am) n += launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, s, nullptr);
-        n += launch_step_pre(ctx->ka, ctx->prec, s, 0);
-        cudaEventRecord(b->ev_join[i], s);
-        cudaStreamWaitEvent(b->stream, b->ev_join[i], 0);
-    }
-    n += launch_stencil_batch(b->items, (int)nd, b->total_tiles, b->prec, b->cpt, b->grid, b->stream);
-    cudaEventRecord(b->ev_fork[1], b->stream);
-    for (size_t i = 0; i < nd; i++) {
-        cudaStream_t s = b->side[i];
-        cudaStreamWaitEvent(s, b->ev_fork[1], 0);
-        n += launch_step_post(b->doms[i]->ka, b->prec, s);
-        cudaEventRecord(b->ev_join[i], s);
-        cudaStreamWaitEvent(b->stream, b->ev_join[i], 0);
-    }
+    const int nd = (int)b->doms.size();
+    auto branches = [&](auto &&fn) {
+        bool any = false;
+        for (int i = 0; i < nd; i++) {
+            mms_ctx *ctx = b->doms[i];
+            if (!fn(ctx, nullptr)) continue;
+            if (!any) cudaEventRecord(b->ev_fork[0], b->stream);
+            any = true;
+            cudaStreamWaitEvent(b->side[i], b->ev_fork[0], 0);
+            n += fn(ctx, b->side[i]);
+            cudaEventRecord(b->ev_join[i], b->side[i]);
+            cudaStreamWaitEvent(b->stream, b->ev_join[i], 0);
+        }
+    };
+    // fn(ctx, nullptr) asks whether the domain has such work
+    branches([&](mms_ctx *ctx, cudaStream_t s) -> int {
+        if (!ctx->p.am) return 0;
+        return s ? launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, s, nullptr) : 1;
+    });
+    const int *bg = b->begin;
+    n += launch_small_batch(0, b->items, bg, nd, b->totals[0], b->prec, b->stream);
+    n += launch_small_batch(1, b->items, bg + (nd + 1), nd, b->totals[1], b->prec, b->stream);
+    branches([&](mms_ctx *ctx, cudaStream_t s) -> int {
+        if (!ctx->p.tip_curv) return 0;
+        return s ? launch_curv(ctx->ka, ctx->prec, s) : 1;
+    });
+    n += launch_stencil_batch(b->items, nd, b->total_tiles, b->prec, b->cpt, b->grid, b->stream);
+    n += launch_small_batch(2, b->items, bg + 2 * (nd + 1), nd, b->totals[2], b->prec, b->stream);
+    n += launch_small_batch(3, b->items, bg + 3 * (nd + 1), nd, b->totals[3], b->prec, b->stream);
     return n;
 }
 
@@ -1695,6 +1744,7 @@ mms_status batch_ensure_graph(mms_batch *b)
         return MMS_ERR_CUDA;
     }
     b->graph_kernels = n;
+    for (int w = 0; w < 4; w++) b->graph_totals[w] = b->totals[w];
     return MMS_OK;
 }
 
@@ -1733,6 +1783,7 @@ mms_status mms_batch_destroy(mms_batch *b)
     batch_drop_graph(b);
     for (mms_ctx *ctx : b->doms) mms_destroy(ctx);
     if (b->items) cudaFree(b->items);
+    if (b->begin) cudaFree(b->begin);
     for (cudaStream_t s : b->side) cudaStreamDestroy(s);
     for (cudaEvent_t e : b->ev_fork) cudaEventDestroy(e);
     for (cudaEvent_t e : b->ev_join) cudaEventDestroy(e);
@@ -1798,6 +1849,7 @@ mms_status mms_batch_step(mms_batch *b, int nsteps)
         if (ctx->h_ctl->status) return (mms_status)ctx->h_ctl->status;
         ctx->stepped = true;
     }
+    if ((st = batch_refresh(b))) return st;
     std::vector<unsigned long long> ts0(nd);
     for (size_t i = 0; i < nd; i++) ts0[i] = b->doms[i]->h_ctl->timestep;
     const int chunk = 256;

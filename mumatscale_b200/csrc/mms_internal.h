@@ -232,6 +232,7 @@ int launch_stencil(const KernelArgs &a, const TmaHolder &tma, int precision, voi
 // the kernels of a step before / after the stencil
 int launch_step_pre(const KernelArgs &a, int precision, void *stream, int start_stage);
 int launch_step_post(const KernelArgs &a, int precision, void *stream);
+int launch_curv(const KernelArgs &a, int precision, void *stream);
 // Batched stencil over many domains: one item per domain (opaque, built by
 // fill_batch_item, which returns the domain's tile count), one persistent
 // launch of batch_grid CTAs.
@@ -240,11 +241,20 @@ long long fill_batch_item(void *dst, const KernelArgs &a, const TmaHolder &tma, 
 int batch_grid(int precision, int cpt);
 int launch_stencil_batch(const void *items, int nitems, long long total_tiles, int precision, int cpt, int grid,
                          void *stream);
+// The other kernels of a step over all domains, one launch each: which = 0
+// nucleation, 1 activation, 2 interface list, 3 capture; begin: device
+// prefix sums (n + 1) of batch_blocks over the domains, total = begin[n].
+int batch_blocks(const KernelArgs &a, int which);
+int launch_small_batch(int which, const void *items, const int *begin, int n, int total, int precision,
+                       void *stream);
 // AM laser parameters (BB_struct, read_ctrl.c) for the moving-source quadrature
 struct AmParams {
     double lsd, lv, lhs, lab, lpow, liniT, lthcon, rho_cp, x0, y0, z0;
     int amtracks, nsbx_times_sbx;
 };
+// FP32 AM contraction on the tensor cores (am_tc.cu)
+int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream);
+int am_tc_prepare();
 // Temperature of the next step for the AM model (tables + contraction);
 // FP32 tables and sums in the FP32 form.
 int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof);
