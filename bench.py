@@ -153,10 +153,8 @@ class ClockSampler:
 
 # --------------------------------------------------------------- helpers
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from mumatscale_b200.distributed import dist_env as env
+    return env()
 
 
 def measured_peak_gbs() -> tuple[float, str]:
@@ -535,8 +533,9 @@ def ensemble_workload(args) -> None:
     as one batch (one graph per step, one persistent stencil launch, tile
     autotuned) for 3000 steps; beside it (N=1) the same domains stepped one
     after another with mms_step.  Under torchrun the domains are dealt to
-    the ranks (domain i to rank i mod N): no collective on the data path,
-    timing is the max over ranks.  Rank 0 prints one JSON line."""
+    the ranks by size (largest first to the least-loaded rank): no collective
+    on the data path, timing is the max over ranks.  Rank 0 prints one JSON
+    line."""
     import torch
     import mumatscale_b200 as M
     from mumatscale_b200 import workloads as W
@@ -556,8 +555,10 @@ def ensemble_workload(args) -> None:
         f = td / f"e{i}.in"
         f.write_text(d)
         ps_all.append(M.read_deck(f))
-    ps = ps_all[rank::ws]
-    cells_all = sum(p.gsdimx * p.gsdimy * p.gsdimz for p in ps_all)
+    from mumatscale_b200.distributed import shard_balanced
+    sizes = [p.gsdimx * p.gsdimy * p.gsdimz for p in ps_all]
+    ps = [ps_all[i] for i in shard_balanced(sizes, ws)[rank]]
+    cells_all = sum(sizes)
     steps = 3000 if args.steps == 200 else args.steps
 
     def barrier():
