@@ -382,11 +382,17 @@ class Domain:
     def num_cells(self) -> int:
         return int(_lib().mms_num_cells(self._ctx))
 
-    def download(self, name: str) -> np.ndarray:
+    def download(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """The halo'd field as [z, y, x(, component)]; `out` (contiguous, the
+        field's dtype and size, e.g. a view of pinned memory) is filled instead
+        of a new array."""
         f = FIELD[name]
         dt, comp = _FIELD_DTYPE[f]
         n = self.num_cells()
-        out = np.empty(n * comp, dtype=dt)
+        if out is None:
+            out = np.empty(n * comp, dtype=dt)
+        elif out.dtype != dt or out.size != n * comp or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous array of the field's dtype and size")
         _check(_lib().mms_download(self._ctx, f, out.ctypes.data), f"mms_download({name})", self._ctx)
         nx, ny, nz = self.shape
         return out.reshape((nz, ny, nx, comp) if comp > 1 else (nz, ny, nx))

@@ -155,13 +155,10 @@ __global__ void __launch_bounds__(TC_NT, 2) k_am_contract_tc(KernelArgs a, AmPar
 
     unsigned ph[2] = {0u, 0u};
     int step = 0, c = 0;
-    for (int i0 = 0; i0 < AM_NT; i0 += TC_KC, c++) {
-        const int b = c & 1;
-        unsigned char *set = tsm + b * TC_SET;
-        unsigned char *A_hi = set, *A_lo = set + TC_KS * TC_A_BYTES;
-        unsigned char *B_hi = set + 2 * TC_KS * TC_A_BYTES, *B_lo = B_hi + TC_KS * TC_B_BYTES;
-        // loads first (all in flight together), then the split stores
-        float av[TC_KC / 2], bv[TC_KC];
+    // operands of the next chunk, loaded one chunk ahead so that their
+    // latency overlaps the stores, fences and MMA issue of the current one
+    float av[TC_KC / 2], bv[TC_KC];
+    auto load_chunk = [&](int i0) {
 #pragma unroll
         for (int j = 0; j < TC_KC / 2; j++) {
             const int k = sk0 + 2 * j;
@@ -169,6 +166,13 @@ __global__ void __launch_bounds__(TC_NT, 2) k_am_contract_tc(KernelArgs a, AmPar
         }
 #pragma unroll
         for (int k = 0; k < TC_KC; k++) bv[k] = bcol ? __ldg(Xc + (long long)(i0 + k) * nx) : 0.f;
+    };
+    load_chunk(0);
+    for (int i0 = 0; i0 < AM_NT; i0 += TC_KC, c++) {
+        const int b = c & 1;
+        unsigned char *set = tsm + b * TC_SET;
+        unsigned char *A_hi = set, *A_lo = set + TC_KS * TC_A_BYTES;
+        unsigned char *B_hi = set + 2 * TC_KS * TC_A_BYTES, *B_lo = B_hi + TC_KS * TC_B_BYTES;
         // this buffer's previous MMAs (chunk c - 2) must be complete
         if (c >= 2) {
             if (!tc_bar_wait(&bar[b], ph[b])) s_abort = 1;
@@ -195,6 +199,7 @@ __global__ void __launch_bounds__(TC_NT, 2) k_am_contract_tc(KernelArgs a, AmPar
                 *(float *)(B_lo + off) = lo;
             }
         }
+        if (i0 + TC_KC < AM_NT) load_chunk(i0 + TC_KC);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {

@@ -1524,17 +1524,34 @@ __global__ void __launch_bounds__(RED_NT) k_reduce(KernelArgs a, int what, doubl
     const Geo &g = a.g;
     const int cur = (int)(ctl->timestep & 1ULL);
     const Real *f = (what == MMS_REDUCE_CE_SUM) ? (const Real *)a.d.ce : (const Real *)a.d.fs[cur];
-    long long n = (long long)g.gx * g.gy * g.gz;
+    const long long rows = (long long)g.gy * g.gz;
     double s = 0.0, comp = 0.0;
-    for (long long v = blockIdx.x * (long long)RED_NT + threadIdx.x; v < n; v += (long long)gridDim.x * RED_NT) {
-        long long i = v % g.gx, j = (v / g.gx) % g.gy, k = v / ((long long)g.gx * g.gy);
-        long long c = (k + 1) * g.sz + (j + 1) * g.sy + (i + 1);
-        double x = (double)f[c];
+    auto add = [&](double x) {
         if (what != MMS_REDUCE_CE_SUM) x = (1.0 < x) ? 1.0 : x;
-        double t = s + x;                      // TwoSum
+        double t = s + x;                          // TwoSum
         double bp = t - s;
         comp += (s - (t - bp)) + (x - bp);
         s = t;
+    };
+    // a block per interior row at a time (four rows' loads in flight), the
+    // threads along x
+    constexpr int U = 4;
+    for (long long r0 = (long long)blockIdx.x * U; r0 < rows; r0 += (long long)gridDim.x * U) {
+        const Real *row[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const long long r = r0 + u < rows ? r0 + u : r0;
+            const long long k = r / g.gy + 1, j = r - (k - 1) * g.gy + 1;
+            row[u] = f + k * g.sz + j * g.sy;
+        }
+        for (int i = 1 + (int)threadIdx.x; i <= g.gx; i += RED_NT) {
+            double x[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) x[u] = (double)row[u][i];
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (r0 + u < rows) add(x[u]);
+        }
     }
     __shared__ double ss[RED_NT], sc[RED_NT];
     ss[threadIdx.x] = s;
@@ -1961,26 +1978,70 @@ int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *
     return 2;
 }
 
-int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream)
+// Folds the per-block (sum, compensation) pairs in a fixed order.
+__global__ void __launch_bounds__(1024) k_reduce_fold(double *partial, int nb)
+{
+    __shared__ double ss[1024], sc[1024];
+    double s = 0, c = 0;
+    for (int b = threadIdx.x; b < nb; b += 1024) {
+        const double x = partial[2 * b];
+        const double t = s + x, bp = t - s;
+        c += (s - (t - bp)) + (x - bp) + partial[2 * b + 1];
+        s = t;
+    }
+    ss[threadIdx.x] = s;
+    sc[threadIdx.x] = c;
+    __syncthreads();
+    for (int w = 512; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            const double x = ss[threadIdx.x + w];
+            const double t = ss[threadIdx.x] + x, bp = t - ss[threadIdx.x];
+            sc[threadIdx.x] += sc[threadIdx.x + w] + ((ss[threadIdx.x] - (t - bp)) + (x - bp));
+            ss[threadIdx.x] = t;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[2 * nb] = ss[0] + sc[0];
+}
+
+int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream, double *pinned)
 {
     cudaStream_t st = (cudaStream_t)stream;
-    const int nb = 148 * 4;
+    const int nb = RED_BLOCKS;
     double *partial = a.d.red;
     if (precision == MMS_PREC_F32) k_reduce<float><<<nb, RED_NT, 0, st>>>(a, what, partial);
     else k_reduce<double><<<nb, RED_NT, 0, st>>>(a, what, partial);
-    static thread_local double h[2 * 148 * 4];
-    cudaMemcpyAsync(h, partial, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, st);
+    k_reduce_fold<<<1, 1024, 0, st>>>(partial, nb);
+    cudaMemcpyAsync(pinned, partial + 2 * nb, sizeof(double), cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);
-    double s = 0, c = 0;
-    for (int b = 0; b < nb; b++) {
-        double x = h[2 * b];
-        double t = s + x, bp = t - s;
-        c += (s - (t - bp)) + (x - bp) + h[2 * b + 1];
-        s = t;
-    }
-    *host_out = s + c;
+    *host_out = *pinned;
     if (precision == MMS_PREC_F32 && what == MMS_REDUCE_CE_SUM)  // deviations from Cinit were summed
         *host_out += a.p.cinit * (double)((long long)a.g.gx * a.g.gy * a.g.gz);
+    return 2;
+}
+
+// Rows of row_bytes bytes from one pitch to another (the reference's halo'd
+// layout to the padded device layout and back), 4-byte words when possible.
+__global__ void k_repack(unsigned char *__restrict__ dst, long long dst_pitch, const unsigned char *__restrict__ src,
+                         long long src_pitch, int row_bytes, long long rows)
+{
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        unsigned char *d = dst + r * dst_pitch;
+        const unsigned char *q = src + r * src_pitch;
+        if ((row_bytes & 3) == 0 && (dst_pitch & 3) == 0 && (src_pitch & 3) == 0) {
+            for (int w = threadIdx.x; w < row_bytes / 4; w += blockDim.x) ((unsigned *)d)[w] = ((const unsigned *)q)[w];
+        } else {
+            for (int b = threadIdx.x; b < row_bytes; b += blockDim.x) d[b] = q[b];
+        }
+    }
+}
+
+int launch_repack(void *dst, long long dst_pitch, const void *src, long long src_pitch, int row_bytes, long long rows,
+                  void *stream)
+{
+    const long long nb = rows < 148 * 64 ? rows : 148 * 64;
+    k_repack<<<(unsigned)(nb > 0 ? nb : 1), 256, 0, (cudaStream_t)stream>>>(
+        (unsigned char *)dst, dst_pitch, (const unsigned char *)src, src_pitch, row_bytes, rows);
     return 1;
 }
 

@@ -114,11 +114,15 @@ struct mms_ctx {
     std::vector<mms_grain> grains;
     int grains_synced = 1;
     Ctl *h_ctl = nullptr;  // pinned
+    double *h_red = nullptr;  // pinned reduction result
     uint64_t launches = 0;
     bool stepped = false;
     std::string err;
     size_t bytes = 0;
     std::vector<void *> allocs;
+    void *stage = nullptr;    // field staging buffer for host copies
+    size_t stage_bytes = 0;
+    int rng_checked_grains = -1;  // grain count at the last orientation-table check
     // frozen-CA record for the adjoint
     struct AdjRec {
         unsigned long long t0 = 0;
@@ -325,6 +329,9 @@ mms_status refill_rng(mms_ctx *ctx, bool force)
     const Geo &g = ctx->ka.g;
     DevPtrs &d = ctx->ka.d;
     if (!ctx->p.gnUseOrientation) return MMS_OK;
+    // draws are consumed only by new grains: nothing to check otherwise
+    if (!force && ctx->h_ctl->num_grains == ctx->rng_checked_grains) return MMS_OK;
+    ctx->rng_checked_grains = ctx->h_ctl->num_grains;
     std::vector<int> used(g.nranks);
     CU(d2h(ctx, used.data(), d.rng_used, sizeof(int) * g.nranks));
     bool any = force;
@@ -487,11 +494,39 @@ mms_status sync_grains(mms_ctx *ctx)
     return MMS_OK;
 }
 
+// staging buffer of one whole field in the reference layout (grown on demand)
+void *stage_buffer(mms_ctx *ctx, size_t bytes)
+{
+    if (ctx->stage_bytes < bytes) {
+        dfree(ctx, ctx->stage);
+        ctx->stage = nullptr;
+        ctx->stage_bytes = 0;
+        char *p = nullptr;
+        if (dalloc(ctx, &p, bytes) != MMS_OK) return nullptr;
+        ctx->stage = p;
+        ctx->stage_bytes = bytes;
+    }
+    return ctx->stage;
+}
+
+// Field copies between the device layout and a caller buffer in the
+// reference layout: one contiguous host<->device copy of the whole field
+// through a staging buffer, re-pitched on the device (row-by-row 2D copies
+// of ~2 KB rows run far below the link's bandwidth).
 cudaError_t copy_out(mms_ctx *ctx, void *host, const void *dev, size_t es)
 {
     const Geo &g = ctx->ka.g;
-    cudaError_t e = cudaMemcpy2DAsync(host, (size_t)g.rsy * es, dev, (size_t)g.P * es, (size_t)g.rsy * es,
-                                      (size_t)(g.gy + 2) * (g.gz + 2), cudaMemcpyDeviceToHost, ctx->stream);
+    const long long rows = (long long)(g.gy + 2) * (g.gz + 2);
+    void *st = stage_buffer(ctx, (size_t)g.rN * es);
+    cudaError_t e;
+    if (!st) {
+        e = cudaMemcpy2DAsync(host, (size_t)g.rsy * es, dev, (size_t)g.P * es, (size_t)g.rsy * es, (size_t)rows,
+                              cudaMemcpyDeviceToHost, ctx->stream);
+    } else {
+        launch_repack(st, g.rsy * (long long)es, dev, g.P * (long long)es, (int)(g.rsy * (long long)es), rows,
+                      ctx->stream);
+        e = cudaMemcpyAsync(host, st, (size_t)g.rN * es, cudaMemcpyDeviceToHost, ctx->stream);
+    }
     if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(ctx->stream);
 }
@@ -499,8 +534,18 @@ cudaError_t copy_out(mms_ctx *ctx, void *host, const void *dev, size_t es)
 cudaError_t copy_in(mms_ctx *ctx, void *dev, const void *host, size_t es)
 {
     const Geo &g = ctx->ka.g;
-    cudaError_t e = cudaMemcpy2DAsync(dev, (size_t)g.P * es, host, (size_t)g.rsy * es, (size_t)g.rsy * es,
-                                      (size_t)(g.gy + 2) * (g.gz + 2), cudaMemcpyHostToDevice, ctx->stream);
+    const long long rows = (long long)(g.gy + 2) * (g.gz + 2);
+    void *st = stage_buffer(ctx, (size_t)g.rN * es);
+    cudaError_t e;
+    if (!st) {
+        e = cudaMemcpy2DAsync(dev, (size_t)g.P * es, host, (size_t)g.rsy * es, (size_t)g.rsy * es, (size_t)rows,
+                              cudaMemcpyHostToDevice, ctx->stream);
+    } else {
+        e = cudaMemcpyAsync(st, host, (size_t)g.rN * es, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            launch_repack(dev, g.P * (long long)es, st, g.rsy * (long long)es, (int)(g.rsy * (long long)es), rows,
+                          ctx->stream);
+    }
     if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(ctx->stream);
 }
@@ -747,6 +792,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
     cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     ctx->stream = ctx->own_stream;
     cudaMallocHost((void **)&ctx->h_ctl, sizeof(Ctl));
+    cudaMallocHost((void **)&ctx->h_red, sizeof(double));
 
     ctx->ka.g = make_geo(p);
     Geo &g = ctx->ka.g;
@@ -819,7 +865,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         (st = dalloc(ctx, &d.list_cell, (size_t)g.nranks * g.sbcells)) ||
         (st = dalloc(ctx, &d.list_gid, (size_t)g.nranks * g.sbcells)) ||
         (st = dalloc(ctx, &d.dc_tmp, (size_t)g.nranks * (g.sbcells + 101))) ||
-        (st = dalloc(ctx, &d.red, 2 * 148 * 4)) || (st = dalloc(ctx, &d.act_scratch, 4 * g.nranks)) ||
+        (st = dalloc(ctx, &d.red, 2 * RED_BLOCKS + 1)) || (st = dalloc(ctx, &d.act_scratch, 4 * g.nranks)) ||
         (st = dalloc(ctx, &d.rng_used, g.nranks)) || (st = dalloc(ctx, &d.rng_base, g.nranks)) ||
         (st = dalloc(ctx, &d.grain_rot, 9 * (p.maxTotalGrains + 1))) ||
         (st = dalloc(ctx, &d.grain_log, p.maxTotalGrains + 2)))
@@ -900,6 +946,7 @@ mms_status mms_destroy(mms_ctx *ctx)
     for (void *p : ctx->allocs) cudaFree(p);
     ctx->allocs.clear();
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+    if (ctx->h_red) cudaFreeHost(ctx->h_red);
     drop_graph(ctx);
     delete ctx->prof;
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -1180,7 +1227,8 @@ mms_status mms_reduce(mms_ctx *ctx, mms_reduction what, double *out)
     if (!ctx || !out) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     double s = 0;
-    ctx->launches += launch_reduce(ctx->ka, ctx->prec, what == MMS_REDUCE_CE_SUM ? MMS_REDUCE_CE_SUM : 0, &s, ctx->stream);
+    ctx->launches += launch_reduce(ctx->ka, ctx->prec, what == MMS_REDUCE_CE_SUM ? MMS_REDUCE_CE_SUM : 0, &s, ctx->stream,
+                                   ctx->h_red);
     CU(cudaGetLastError());
     const mms_params &p = ctx->p;
     const Geo &g = ctx->ka.g;

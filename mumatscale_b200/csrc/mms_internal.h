@@ -258,9 +258,12 @@ int am_tc_prepare();
 // Temperature of the next step for the AM model (tables + contraction);
 // FP32 tables and sums in the FP32 form.
 int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof);
-int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream);
+constexpr int RED_BLOCKS = 148 * 8;  // partial sums of k_reduce (red holds 2 per block + 1)
+int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream, double *pinned);
 int launch_fill_temperature(const KernelArgs &a, double *dev_out, void *stream);
 int launch_compute_d(const KernelArgs &a, int precision, double *dev_out, void *stream);
+int launch_repack(void *dst, long long dst_pitch, const void *src, long long src_pitch, int row_bytes, long long rows,
+                  void *stream);
 int launch_mask_captured(const KernelArgs &a, void *dev, int is_double, void *stream);
 int launch_convert(const KernelArgs &a, int precision, int field, int to_device, double *dev_f64,
                    void *stream);
