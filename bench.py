@@ -621,6 +621,101 @@ def ensemble_workload(args) -> None:
         dist.destroy_process_group()
 
 
+def slabs_workload(args) -> None:
+    """One 256^3 domain (the headline deck with NSubblocks 1 x 1 x 8) split
+    into N z-slabs, one per rank (torchrun), exchanging boundary planes and
+    new-grain lists over NCCL twice per step (mumatscale_b200.slabs): strong
+    scaling of one domain.  FP64 plain form; device-timed with CUDA events on
+    the slab's stream, max over ranks.  With one process it also times the
+    same domain as 2 and 4 slabs on the one device (in-process group, device
+    copies for the exchanges) beside the unsplit domain: the cost of the
+    exchange points themselves.  Rank 0 prints one JSON line."""
+    import datetime
+    import torch
+    import mumatscale_b200 as M
+    from mumatscale_b200.slabs import DistributedSlab
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    td = tempfile.mkdtemp()
+    deck = Path(td) / "slabs.in"
+    deck.write_text(deck_text(nsb=(1, 1, 8)))
+    params = M.read_deck(deck)
+    cells = N_CELL ** 3
+    K, W = args.steps, args.warmup
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    if ws > 1:
+        s = DistributedSlab(params, precision=M.PREC_F64, device=dev)
+        s.step(W)
+        st = s.stream
+        run = s.step
+        launches0 = s.dom.kernel_launches
+    else:
+        s = M.Domain(params, precision=M.PREC_F64, device=dev)
+        st = torch.cuda.current_stream()
+        s.set_stream(st.cuda_stream)
+        s.step(W)
+        run = s.step
+        launches0 = s.kernel_launches
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        e0.record(st)
+        run(K)
+        e1.record(st)
+        torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    launches = (s.dom.kernel_launches if ws > 1 else s.kernel_launches) - launches0
+    grains = s.dom.num_grains if ws > 1 else s.num_grains
+    s.close()
+    group = None
+    if ws == 1:
+        group = {}
+        for n in (2, 4):
+            with M.SlabGroup(params, n, precision=M.PREC_F64, devices=(dev,)) as g:
+                g.step(W)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                g.step(min(K, 100))
+                torch.cuda.synchronize()
+                sec = time.perf_counter() - t0
+                group[f"{n}_slabs_one_device"] = {"value": cells * min(K, 100) / sec,
+                                                  "ms_per_step": sec * 1e3 / min(K, 100)}
+    if rank == 0:
+        line = {"workload": "one 256^3 domain (NSubblocks 1 x 1 x 8) split into z-slabs, one per GPU, FP64",
+                "metric": UNIT, "unit": UNIT, "value": cells * K / (ms / 1e3), "n_gpus": ws, "steps": K,
+                "warmup": W, "ms_per_step": ms / K, "scaling": "strong", "data": "synthetic", "dtype": "f64",
+                "parallelism": f"z-slabs x{ws}, NCCL send/recv of boundary planes + all-gathers per step",
+                "gpu_launches": launches, "grains": grains, "clocks": clk.summary(),
+                "one_device_groups": group,
+                "timing": "CUDA events on the slab's stream around K steps, max over ranks"}
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def reference_arm(args) -> None:
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -654,10 +749,10 @@ def main() -> None:
                     help="run the workload for an ncu capture only")
     ap.add_argument("--cells", type=int, default=N_CELL, help="edge of the cubic domain (profile mode)")
     ap.add_argument("--tile", default="auto", help="profile mode: stencil tile 'cells_per_thread,zchunk'")
-    ap.add_argument("--workload", default="ds256", choices=["ds256", "adjoint", "am", "ensemble"],
+    ap.add_argument("--workload", default="ds256", choices=["ds256", "adjoint", "am", "ensemble", "slabs"],
                     help="ds256: the headline directional-solidification run (default); adjoint, am, "
-                         "ensemble: the adjoint calibration, AM melt-pool and batched-ensemble workloads "
-                         "(each its own JSON line)")
+                         "ensemble, slabs: the adjoint calibration, AM melt-pool, batched-ensemble and "
+                         "one-domain-over-N-GPUs workloads (each its own JSON line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -669,6 +764,8 @@ def main() -> None:
         am_workload(args)
     elif args.workload == "ensemble" and args.impl != "reference":
         ensemble_workload(args)
+    elif args.workload == "slabs" and args.impl != "reference":
+        slabs_workload(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:

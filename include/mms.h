@@ -336,6 +336,69 @@ mms_status mms_batch_autotune(mms_batch *b, int reps, int *cells_per_thread, int
 uint64_t mms_batch_kernel_launches(const mms_batch *b);
 const char *mms_batch_last_error(const mms_batch *b);
 
+/* ---- one domain split into z-slabs over devices ------------------------------- */
+
+/* The reference runs one domain as NSubblocks MPI ranks that exchange halo
+ * planes and grain lists inside doiteration (calculate.c:193-352; ranks
+ * numbered x fastest, functions.c:310,327).  Here the domain is cut
+ * into nslabs z-slabs of whole subblock layers (nslabs <= NSubblocks z),
+ * one context per slab, each on its own device or all on one: slab s owns
+ * layers [s nz / nslabs, (s + 1) nz / nslabs) and their emulated ranks, so
+ * their random streams, interface lists and dc_tmp slots never cross a
+ * slab.  Stepped together, the slabs give the single context's fields,
+ * grain ids and grain records bit for bit.  Each slab's fields, downloads
+ * and reductions are its own (reference layout of the slab: nz = its
+ * layers); coordinates in mms_set_sites and mms_set_site_orientations are
+ * the whole domain's.  Not with TipCurvature (its stencil reaches three
+ * planes) nor with a periodic z axis; no adjoint on a slab. */
+typedef struct mms_slab_layout {
+    int nslabs, slab;
+    int z_begin;     /* first interior z cell of the slab in the whole domain (0-based) */
+    int z_cells;     /* interior z cells */
+    int rank_begin;  /* first emulated rank (x fastest, then y, then z) */
+    int rank_count;
+} mms_slab_layout;
+
+/* The layout alone, from the whole domain's parameters (no device). */
+mms_status mms_slab_layout_of(const mms_params *global, int nslabs, int slab, mms_slab_layout *out);
+/* Context of slab `slab` of the domain `global` describes (its device:
+ * global->device). */
+mms_status mms_slab_create(const mms_params *global, int nslabs, int slab, mms_ctx **out);
+mms_status mms_slab_get_layout(const mms_ctx *ctx, mms_slab_layout *out);
+/* Steps all slabs of a domain in this process: slabs[s] is slab s.  The
+ * exchanges are device copies (peer copies between devices) ordered by
+ * events on the slabs' streams. */
+mms_status mms_slab_group_step(mms_ctx *const *slabs, int nslabs, int nsteps);
+
+/* One process per device: the caller runs the exchanges (e.g. with NCCL).
+ * A step that starts at timestep t is
+ *   mms_slab_launch(ctx, 0, 0); exchange point 0;
+ *   mms_slab_launch(ctx, 1, 0); exchange point 1;
+ *   mms_slab_launch(ctx, 2, 0);
+ * with the transfers mms_slab_exchange_plan lists for (point, t), issued on
+ * the context's stream (mms_set_stream).  Halo entries: send `bytes` from
+ * `send` to slab `peer` and receive as many from it into `recv`; a slab's
+ * entries for peer q and q's entries for it pair up in list order.  Gather
+ * entry: every slab contributes `bytes` from `send`; `recv` receives the
+ * nslabs contributions in slab order.  After some steps, mms_slab_poll
+ * reports whether activation stalled for want of pre-drawn orientations;
+ * every slab then stalls at the same step, and the steps launched after it
+ * did nothing.  mms_slab_refill on every slab, then the stalled step again
+ * with mms_slab_launch(ctx, 0, 1) in place of phase 0, resumes. */
+typedef enum mms_xfer_kind { MMS_XFER_HALO = 0, MMS_XFER_GATHER = 1 } mms_xfer_kind;
+typedef struct mms_slab_xfer {
+    int kind;        /* mms_xfer_kind */
+    int peer;        /* halo: the neighbouring slab; gather: -1 */
+    void *send;      /* device memory of this context */
+    void *recv;
+    uint64_t bytes;
+} mms_slab_xfer;
+mms_status mms_slab_launch(mms_ctx *ctx, int phase, int resume);
+mms_status mms_slab_exchange_plan(mms_ctx *ctx, int point, uint64_t timestep, mms_slab_xfer *out, int max,
+                                  int *n);
+mms_status mms_slab_poll(mms_ctx *ctx, uint64_t *timestep, int *stalled);
+mms_status mms_slab_refill(mms_ctx *ctx);
+
 /* ---- adjoint (frozen cellular automaton) -------------------------------------- */
 
 /* No counterpart in the reference.  Gradients of L = 1/2 sum over interior

@@ -22,6 +22,7 @@ import numpy as np
 __all__ = [
     "Params", "FixedNuc", "NucVolume", "Grain", "GrainSummary", "Domain", "MmsError",
     "load_library", "library_path", "FIELD", "PREC_F64", "PREC_F32",
+    "Batch", "SlabLayout", "SlabDomain", "SlabGroup", "slab_layout",
 ]
 
 _PKG = Path(__file__).resolve().parent
@@ -106,6 +107,22 @@ class Grain(C.Structure):
     _fields_ = [("nuc_x", C.c_double), ("nuc_y", C.c_double), ("nuc_z", C.c_double),
                 ("nuc_timestep", C.c_uint64), ("nuc_threshold", C.c_double),
                 ("rotmat", (C.c_double * 3) * 3), ("rotang", C.c_double * 3)]
+
+
+class SlabLayout(C.Structure):
+    """mms_slab_layout: the z-range and emulated ranks one slab owns."""
+    _fields_ = [("nslabs", C.c_int), ("slab", C.c_int), ("z_begin", C.c_int), ("z_cells", C.c_int),
+                ("rank_begin", C.c_int), ("rank_count", C.c_int)]
+
+
+class SlabXfer(C.Structure):
+    """mms_slab_xfer: one transfer of a slab exchange point."""
+    _fields_ = [("kind", C.c_int), ("peer", C.c_int), ("send", C.c_void_p), ("recv", C.c_void_p),
+                ("bytes", C.c_uint64)]
+
+
+XFER_HALO = 0
+XFER_GATHER = 1
 
 
 class GrainSummary(C.Structure):
@@ -194,6 +211,14 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_batch_autotune": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(D)]),
         "mms_batch_kernel_launches": (C.c_uint64, [P]),
         "mms_batch_last_error": (C.c_char_p, [P]),
+        "mms_slab_layout_of": (I, [C.POINTER(Params), I, I, C.POINTER(SlabLayout)]),
+        "mms_slab_create": (I, [C.POINTER(Params), I, I, C.POINTER(P)]),
+        "mms_slab_get_layout": (I, [P, C.POINTER(SlabLayout)]),
+        "mms_slab_group_step": (I, [C.POINTER(P), I, I]),
+        "mms_slab_launch": (I, [P, I, I]),
+        "mms_slab_exchange_plan": (I, [P, I, C.c_uint64, C.POINTER(SlabXfer), I, C.POINTER(I)]),
+        "mms_slab_poll": (I, [P, C.POINTER(C.c_uint64), C.POINTER(I)]),
+        "mms_slab_refill": (I, [P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -529,3 +554,148 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------ one domain split into z-slabs
+def slab_layout(params: Params, nslabs: int, slab: int) -> SlabLayout:
+    """Which whole-domain z cells and emulated ranks slab `slab` of `nslabs`
+    owns (no device needed)."""
+    out = SlabLayout()
+    _check(_lib().mms_slab_layout_of(C.byref(params), nslabs, slab, C.byref(out)), "mms_slab_layout_of")
+    return out
+
+
+class SlabDomain(Domain):
+    """One z-slab of a domain split over devices (mms_slab_create): whole
+    layers of subblocks, with a one-plane halo that the step's two exchanges
+    fill from the neighbouring slabs.  Fields, downloads and reductions are
+    the slab's own; grain records cover the whole domain."""
+
+    def __init__(self, params: Params, nslabs: int, slab: int, precision: int | None = None,
+                 device: int | None = None):
+        lib = _lib()
+        p = Params()
+        C.pointer(p)[0] = params
+        if precision is not None:
+            p.precision = precision
+        if device is not None:
+            p.device = device
+        ctx = C.c_void_p()
+        _check(lib.mms_slab_create(C.byref(p), nslabs, slab, C.byref(ctx)), "mms_slab_create")
+        self._ctx = ctx
+        self.global_params = p
+        self.layout = SlabLayout()
+        _check(lib.mms_slab_get_layout(ctx, C.byref(self.layout)), "mms_slab_get_layout", ctx)
+        sp = Params()
+        C.pointer(sp)[0] = p
+        sp.gnsbz = self.layout.z_cells // p.gsdimz
+        self.params = sp
+        self.shape = tuple(x + 2 for x in sp.grid)
+
+    def step(self, nsteps: int = 1) -> None:
+        if self.layout.nslabs == 1:
+            super().step(nsteps)
+        else:
+            raise MmsError(1, "step", "a slab steps with its group (SlabGroup, or launch/exchange per phase)")
+
+    # -- caller-driven stepping (one process per device)
+    def launch(self, phase: int, resume: bool = False) -> None:
+        _check(_lib().mms_slab_launch(self._ctx, phase, int(resume)), "mms_slab_launch", self._ctx)
+
+    def exchange_plan(self, point: int, timestep: int) -> list[tuple[int, int, int, int, int]]:
+        """(kind, peer, send pointer, recv pointer, bytes) of exchange point
+        0 or 1 of the step that starts at `timestep`."""
+        n = C.c_int()
+        buf = (SlabXfer * 32)()
+        _check(_lib().mms_slab_exchange_plan(self._ctx, point, timestep, buf, 32, C.byref(n)),
+               "mms_slab_exchange_plan", self._ctx)
+        return [(x.kind, x.peer, int(x.send or 0), int(x.recv or 0), int(x.bytes)) for x in buf[:n.value]]
+
+    def poll(self) -> tuple[int, bool]:
+        """(timestep, stalled for want of pre-drawn orientations)."""
+        t, s = C.c_uint64(), C.c_int()
+        _check(_lib().mms_slab_poll(self._ctx, C.byref(t), C.byref(s)), "mms_slab_poll", self._ctx)
+        return int(t.value), bool(s.value)
+
+    def refill(self) -> None:
+        _check(_lib().mms_slab_refill(self._ctx), "mms_slab_refill", self._ctx)
+
+
+class SlabGroup:
+    """All slabs of one domain in this process (mms_slab_group_step): each on
+    devices[s % len(devices)], exchanges as device (peer) copies."""
+
+    def __init__(self, params: Params, nslabs: int, precision: int = PREC_F64, devices=(0,)):
+        self.slabs = [SlabDomain(params, nslabs, s, precision, devices[s % len(devices)])
+                      for s in range(nslabs)]
+        self.params = self.slabs[0].global_params
+        self._arr = (C.c_void_p * nslabs)(*[d._ctx.value for d in self.slabs])
+
+    def __len__(self) -> int:
+        return len(self.slabs)
+
+    def step(self, n: int = 1) -> None:
+        st = _lib().mms_slab_group_step(self._arr, len(self.slabs), int(n))
+        if st != 0:
+            detail = "; ".join(filter(None, ((_lib().mms_last_error(d._ctx) or b"").decode() for d in self.slabs)))
+            raise MmsError(st, "mms_slab_group_step", detail)
+
+    @property
+    def timestep(self) -> int:
+        return self.slabs[0].timestep
+
+    @property
+    def num_grains(self) -> int:
+        return self.slabs[0].num_grains
+
+    def download(self, name: str) -> np.ndarray:
+        """The whole domain's halo'd field [z, y, x(, c)], assembled from the
+        slabs' interior planes (the outer halo planes from the end slabs)."""
+        parts = [d.download(name) for d in self.slabs]
+        planes = [parts[0][:1]] + [q[1:-1] for q in parts] + [parts[-1][-1:]]
+        return np.concatenate(planes, axis=0)
+
+    def reduce(self, what: str = "fs_fraction") -> float:
+        """Sums over the slabs (the reference's MPI_Allreduce order differs
+        from one domain's, as here)."""
+        if what == "fs_fraction":
+            nx, ny, nz = self.params.grid
+            v = sum(d.reduce("solid_volume") for d in self.slabs)
+            return v / (nx * ny * nz * self.params.cellSize ** 3)
+        return sum(d.reduce(what) for d in self.slabs)
+
+    def grains(self) -> list[Grain]:
+        return self.slabs[0].grains()
+
+    def set_sites(self, gxyz: np.ndarray, thresholds: np.ndarray) -> None:
+        for d in self.slabs:
+            d.set_sites(gxyz, thresholds)
+
+    def set_site_orientations(self, gxyz: np.ndarray, rotmats: np.ndarray) -> None:
+        for d in self.slabs:
+            d.set_site_orientations(gxyz, rotmats)
+
+    def set_grains(self, rotmats: np.ndarray) -> None:
+        for d in self.slabs:
+            d.set_grains(rotmats)
+
+    def upload(self, name: str, arr: np.ndarray) -> None:
+        """Uploads the whole domain's halo'd field [z, y, x(, c)] slab by slab."""
+        a = np.asarray(arr)
+        for d in self.slabs:
+            z0 = d.layout.z_begin
+            d.upload(name, a[z0:z0 + d.layout.z_cells + 2])
+
+    @property
+    def kernel_launches(self) -> int:
+        return sum(d.kernel_launches for d in self.slabs)
+
+    def close(self) -> None:
+        for d in self.slabs:
+            d.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -84,10 +84,11 @@ __global__ void __launch_bounds__(ADJ_NT) k_replay(Geo g, Phys p, const Real *__
         nb_cl[n] = cl0[c + o[n]];
         nb_fs[n] = fs0[c + o[n]];
     }
-    const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_z = (Real)(1 - g.padz);
+    const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_zp = (Real)(1 - g.padz_hi),
+               one_zm = (Real)(1 - g.padz_lo);
     const Real one_m[6] = {i == g.gx ? one_x : (Real)1, i == 1 ? one_x : (Real)1,
                            j == g.gy ? one_y : (Real)1, j == 1 ? one_y : (Real)1,
-                           k == g.gz ? one_z : (Real)1, k == 1 ? one_z : (Real)1};
+                           k == g.gz ? one_zp : (Real)1, k == 1 ? one_zm : (Real)1};
     const bool interior = i > 1 && i < g.gx && j > 1 && j < g.gy && k > 1 && k < g.gz;
     // diffusion sum: cell_update's expressions
     Real nbsum = 0;
@@ -211,10 +212,11 @@ __global__ void __launch_bounds__(ADJ_NT) k_adj_b(Geo g, Phys p, const unsigned 
         nb_offsets(g, o);
         const Real conc = cl0[c] + off, lspfs = fs0[c];
         const Real nu_c = nu[c];
-        const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_z = (Real)(1 - g.padz);
+        const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_zp = (Real)(1 - g.padz_hi),
+               one_zm = (Real)(1 - g.padz_lo);
         const Real one_m[6] = {i == g.gx ? one_x : (Real)1, i == 1 ? one_x : (Real)1,
                                j == g.gy ? one_y : (Real)1, j == 1 ? one_y : (Real)1,
-                               k == g.gz ? one_z : (Real)1, k == 1 ? one_z : (Real)1};
+                               k == g.gz ? one_zp : (Real)1, k == 1 ? one_zm : (Real)1};
         Real gcl = 0, gfs = 0, grl = 0;
 #pragma unroll
         for (int n = 0; n < 6; n++) {

@@ -21,7 +21,8 @@ __device__ __forceinline__ void raise_error(Ctl *c, int status)
 
 
 // direct_temp_calc (temperature.c:24-61) for the analytic models; the AM
-// quadrature is precomputed into an array by k_temp_am.
+// quadrature is precomputed into an array by k_temp_am.  K is the local
+// plane; p.kz0 places a slab's planes in the whole domain.
 __device__ __forceinline__ double temp_cell(const Phys &p, const double *Tarr, long long cell,
                                             long long J, long long K, unsigned long long ts)
 {
@@ -29,7 +30,7 @@ __device__ __forceinline__ double temp_cell(const Phys &p, const double *Tarr, l
     double sim_time = (double)ts * p.ts_delt;
     if (p.temp_mode == 0) return p.T0 - sim_time * p.cool_rate;
     double ry = p.origin[1] + ((double)(int)J + 0.5) * p.cellSize;
-    double rz = p.origin[2] + ((double)(int)K + 0.5) * p.cellSize;
+    double rz = p.origin[2] + ((double)((int)K + p.kz0) + 0.5) * p.cellSize;
     double axis = (p.gz_is_one ? ry : rz) - p.cellSize * 0.5;
     double tgrad = p.gradient + p.grad_coef * sim_time;
     double v = p.velocity + p.velo_coef * sim_time;

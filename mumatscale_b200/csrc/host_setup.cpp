@@ -263,7 +263,7 @@ Geo make_geo(const mms_params &p)
     g.sbcells = (long long)p.gsdimx * p.gsdimy * p.gsdimz;
     g.padx = p.padBndyX;
     g.pady = p.padBndyY;
-    g.padz = p.padBndyZ;
+    g.padz_lo = g.padz_hi = p.padBndyZ;
     g.ppr = (p.gsdimx + 31) / 32;
     g.pieces_per_rank = (long long)p.gsdimy * p.gsdimz * g.ppr;
     g.blocks_per_rank = (g.pieces_per_rank + LIST_PIECES - 1) / LIST_PIECES;
@@ -279,7 +279,7 @@ std::vector<signed char> make_mold(const Geo &g)
                 int m = 0;
                 if (g.padx && (I == 0 || I == g.gx + 1)) m = 1;
                 if (g.pady && (J == 0 || J == g.gy + 1)) m = 1;
-                if (g.padz && (K == 0 || K == g.gz + 1)) m = 1;
+                if ((g.padz_lo && K == 0) || (g.padz_hi && K == g.gz + 1)) m = 1;
                 mold[(size_t)cidx(g, I, J, K)] = (signed char)m;
             }
     return mold;

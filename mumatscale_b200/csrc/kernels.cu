@@ -169,7 +169,7 @@ __global__ void k_am_tables(KernelArgs a, AmParams m)
             Y[(long long)i * ny + J] = (Real)exp(-(ly * ly) / ai);
         } else {
             const int K = q - nx - ny;
-            const double rz = p.origin[2] + ((double)K + 0.5) * p.cellSize;
+            const double rz = p.origin[2] + ((double)(K + p.kz0) + 0.5) * p.cellSize;
             const double lz = rz - s.znow;
             const double Tlocal = sqrt(s.lalpha * lt) * ai;
             Z[(long long)i * nz + K] = (Real)(s.ldt * exp(-(lz * lz / (4. * s.lalpha * lt))) / Tlocal);
@@ -379,30 +379,16 @@ __device__ long long find_key(const long long *keys, long long n, long long key)
 // replaces the capped count (grain.c:1318), so the cap never holds.
 // One CTA; every phase is parallel over candidates or ranks.
 constexpr int ACT_NT = 1024;
-__device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
+
+// Ordered gather of the per-block candidate lists into cand[0, C), then per
+// candidate its orientation source and the prefix count of random draws
+// (cand_ex), per rank its first candidate and its number of draws.
+__device__ __forceinline__ void act_gather(const KernelArgs &a, int C, int *need, int *first, int *sh)
 {
-    Ctl *ctl = a.d.ctl;
-    if (stalled(ctl)) return;
-    __shared__ int sh[ACT_NT / 32];
-    __shared__ int s_abort;
-    const int C = ctl->ncand;
-    const unsigned long long ts = ctl->timestep + 1;
-    if (threadIdx.x == 0) ctl->list_ticket = 0;  // k_list block order of this step
-    if (C == 0) {
-        if (threadIdx.x == 0) {
-            ctl->timestep = ts;
-            ctl->new_grains = 0;
-        }
-        return;
-    }
     const Phys &p = a.p;
     const int nr = a.g.nranks;
-    int *need = rank_scratch;        // random draws per rank
-    int *first = rank_scratch + nr;  // first candidate of each rank
-    int *ex = a.d.cand_ex;           // per candidate: random draws before it
+    int *ex = a.d.cand_ex;
     for (int r = threadIdx.x; r < nr; r += ACT_NT) need[r] = 0, first[r] = -1;
-    if (threadIdx.x == 0) s_abort = 0;
-    // ordered gather of the per-block candidate lists
     int off = 0;
     for (int base = 0; base < a.d.nuc_blocks; base += ACT_NT) {
         int b = base + threadIdx.x;
@@ -413,8 +399,6 @@ __device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
         off += tot;
     }
     __syncthreads();
-    // orientation source per candidate, prefix count of random draws,
-    // per-rank first candidate and draw count
     int run = 0;
     for (int base = 0; base < C; base += ACT_NT) {
         int i = base + threadIdx.x;
@@ -432,39 +416,37 @@ __device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
         run += tot;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        if ((unsigned long long)(ctl->num_grains + (long long)C) > p.max_grains + 1) {
-            ctl->status = MMS_ERR_GRAIN_OVERFLOW;
-            atomicExch(&ctl->stall, (int)STALL_ERROR);
-            s_abort = 1;
-        }
-    }
-    __syncthreads();
+}
+
+// Some rank lacks pre-drawn orientations for its draws of this step (block-wide).
+__device__ __forceinline__ bool act_short(const KernelArgs &a, const int *need)
+{
     int short_rng = 0;
-    for (int r = threadIdx.x; r < nr && !s_abort; r += ACT_NT)
+    for (int r = threadIdx.x; r < a.g.nranks; r += ACT_NT)
         if (a.d.rng_used[r] + need[r] > a.d.rng_cap) short_rng = 1;
-    short_rng = __syncthreads_or(short_rng);
-    if (s_abort) return;
-    if (short_rng) {
-        // refill on the host, then this kernel runs again with the same
-        // candidates (nothing has been written yet)
-        if (threadIdx.x == 0) {
-            ctl->stall_step = ts;
-            atomicExch(&ctl->stall, (int)STALL_RNG);
-        }
-        return;
-    }
-    const long long num_grains = ctl->num_grains;
+    return __syncthreads_or(short_rng) != 0;
+}
+
+// Grain id0 + i for candidate i: gr, rotation and record; with rows, the
+// record as the other slabs of a split domain receive it.
+__device__ __forceinline__ void act_assign(const KernelArgs &a, int C, long long id0, unsigned long long ts,
+                                           const int *first, SlabRow *rows)
+{
+    const Phys &p = a.p;
+    const Geo &g = a.g;
+    const int *ex = a.d.cand_ex;
     for (int i = threadIdx.x; i < C; i += ACT_NT) {
         const int s = a.d.cand[i];
         const long long cell = a.d.site_cell[s];
         const int r = a.d.site_rank[s];
-        const long long id = num_grains + i;
+        const long long id = id0 + i;
         a.d.gr[cell] = (int)id;
         GrainLog lg;
         lg.cell = cell;
         lg.timestep = ts;
-        lg.rank = r;
+        lg.rank = r + a.d.rank0;
+        lg.thr = a.d.site_thr[s];
+        lg.pad = 0;
         const double *rot;
         long long j = find_key(a.d.nucpt_key, a.d.n_nucpt, cell);
         if (j >= 0) {
@@ -489,7 +471,58 @@ __device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
         double *dst = a.d.grain_rot + 9 * id;
         for (int e = 0; e < 9; e++) dst[e] = rot[e];
         a.d.grain_log[id] = lg;
+        if (rows) {
+            SlabRow &row = rows[i];
+            for (int e = 0; e < 9; e++) row.rot[e] = rot[e];
+            const long long K = cell / g.sz, J = (cell % g.sz) / g.sy, I = cell % g.sy;
+            lg.cell = (K + p.kz0) * g.rsz + J * g.rsy + I;
+            row.lg = lg;
+        }
     }
+}
+
+__device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
+{
+    Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    __shared__ int sh[ACT_NT / 32];
+    __shared__ int s_abort;
+    const int C = ctl->ncand;
+    const unsigned long long ts = ctl->timestep + 1;
+    if (threadIdx.x == 0) ctl->list_ticket = 0;  // k_list block order of this step
+    if (C == 0) {
+        if (threadIdx.x == 0) {
+            ctl->timestep = ts;
+            ctl->new_grains = 0;
+        }
+        return;
+    }
+    const Phys &p = a.p;
+    const int nr = a.g.nranks;
+    int *need = rank_scratch;        // random draws per rank
+    int *first = rank_scratch + nr;  // first candidate of each rank
+    if (threadIdx.x == 0) s_abort = 0;
+    act_gather(a, C, need, first, sh);
+    if (threadIdx.x == 0) {
+        if ((unsigned long long)(ctl->num_grains + (long long)C) > p.max_grains + 1) {
+            ctl->status = MMS_ERR_GRAIN_OVERFLOW;
+            atomicExch(&ctl->stall, (int)STALL_ERROR);
+            s_abort = 1;
+        }
+    }
+    __syncthreads();
+    if (s_abort) return;
+    if (act_short(a, need)) {
+        // refill on the host, then this kernel runs again with the same
+        // candidates (nothing has been written yet)
+        if (threadIdx.x == 0) {
+            ctl->stall_step = ts;
+            atomicExch(&ctl->stall, (int)STALL_RNG);
+        }
+        return;
+    }
+    const long long num_grains = ctl->num_grains;
+    act_assign(a, C, num_grains, ts, first, nullptr);
     __syncthreads();
     for (int r = threadIdx.x; r < nr; r += ACT_NT) a.d.rng_used[r] += need[r];
     if (threadIdx.x == 0) {
@@ -497,6 +530,112 @@ __device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
         ctl->new_grains = C;
         ctl->ncand = 0;
         ctl->timestep = ts;
+    }
+}
+
+// Slab of a split domain, before the first exchange: this slab's half of
+// activation (gather, draws needed), published as {candidates, short of
+// draws} for every slab to see.
+__global__ void __launch_bounds__(ACT_NT) k_act_local(KernelArgs a)
+{
+    Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    __shared__ int sh[ACT_NT / 32];
+    const int C = ctl->ncand;
+    if (threadIdx.x == 0) ctl->list_ticket = 0;
+    if (C > a.d.slab_cap) {  // more candidates than the row buffer holds
+        if (threadIdx.x == 0) raise_error(ctl, MMS_ERR_SCRATCH_LIMIT);
+        return;
+    }
+    int short_rng = 0;
+    if (C > 0) {
+        int *need = a.d.act_scratch, *first = a.d.act_scratch + a.g.nranks;
+        act_gather(a, C, need, first, sh);
+        short_rng = act_short(a, need) ? 1 : 0;
+    }
+    if (threadIdx.x == 0) {
+        a.d.x1_send[0] = C;
+        a.d.x1_send[1] = short_rng;
+    }
+}
+
+// Slab of a split domain, after the first exchange: grain ids continue
+// over the slabs in slab order, which is emulated-rank order because every
+// slab holds whole layers of subblocks.  Every slab takes the same
+// decision on overflow and on a shortage of draws anywhere, so a stalled
+// step stalls every slab at the same kernel.
+__global__ void __launch_bounds__(ACT_NT) k_act_slab(KernelArgs a)
+{
+    Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    __shared__ int s_abort;
+    const unsigned long long ts = ctl->timestep + 1;
+    const int S = a.d.nslabs;
+    long long total = 0, off = 0;
+    int any_short = 0;
+    for (int s = 0; s < S; s++) {
+        const int c = a.d.x1_recv[2 * s];
+        if (s < a.d.slab) off += c;
+        total += c;
+        any_short |= a.d.x1_recv[2 * s + 1];
+    }
+    const int C = ctl->ncand;
+    if (threadIdx.x == 0) {
+        s_abort = 0;
+        if (total > 0 && (unsigned long long)(ctl->num_grains + total) > a.p.max_grains + 1) {
+            ctl->status = MMS_ERR_GRAIN_OVERFLOW;
+            atomicExch(&ctl->stall, (int)STALL_ERROR);
+            s_abort = 1;
+        } else if (any_short) {
+            ctl->stall_step = ts;
+            atomicExch(&ctl->stall, (int)STALL_RNG);
+            s_abort = 1;
+        }
+    }
+    __syncthreads();
+    if (s_abort) return;
+    const long long num_grains = ctl->num_grains;
+    if (C > 0) {
+        const int nr = a.g.nranks;
+        const int *need = a.d.act_scratch, *first = a.d.act_scratch + nr;
+        act_assign(a, C, num_grains + off, ts, first, a.d.x2_send);
+        __syncthreads();
+        for (int r = threadIdx.x; r < nr; r += ACT_NT) a.d.rng_used[r] += need[r];
+    }
+    if (threadIdx.x == 0) {
+        ctl->num_grains = (int)(num_grains + total);
+        ctl->new_grains = (int)total;
+        ctl->ncand = 0;
+        ctl->timestep = ts;
+    }
+}
+
+// Slab of a split domain, after the second exchange: rotations and records
+// of the grains the other slabs created this step.
+__global__ void __launch_bounds__(256) k_slab_merge(KernelArgs a)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const int S = a.d.nslabs;
+    long long total = 0;
+    for (int s = 0; s < S; s++) total += a.d.x1_recv[2 * s];
+    const long long base = ctl->num_grains - total;
+    long long off = 0;
+    for (int s = 0; s < S; s++) {
+        const int c = a.d.x1_recv[2 * s];
+        if (s != a.d.slab) {
+            const int n = c < a.d.slab_cap ? c : a.d.slab_cap;
+            const SlabRow *rows = a.d.x2_recv + (long long)s * a.d.slab_cap;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                const long long id = base + off + i;
+                double *dst = a.d.grain_rot + 9 * id;
+                for (int e = 0; e < 9; e++) dst[e] = rows[i].rot[e];
+                GrainLog lg = rows[i].lg;
+                lg.kind |= GL_REMOTE;
+                a.d.grain_log[id] = lg;
+            }
+        }
+        off += c;
     }
 }
 
@@ -845,7 +984,8 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
         for (int pl = 0; pl < TS && pl < nplanes; pl++) issue(pl);
     int issued = min(TS, nplanes);  // same value in every thread
 
-    const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_z = (Real)(1 - g.padz);
+    const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_zp = (Real)(1 - g.padz_hi),
+               one_zm = (Real)(1 - g.padz_lo);
     const long long wrow = (long long)g.wpr;
     // plane-invariant per-cell values
     int hh[CPT], hcc[CPT], hgg[CPT];
@@ -884,7 +1024,7 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
         const Real *fp = (const Real *)(stage(s2) + L::CL);
         const Real *sce = (const Real *)(stage(s1) + 2 * L::CL);
         const int *sgr = (const int *)(stage(s1) + 2 * L::CL + L::CE);
-        const Real omz_p = k == g.gz ? one_z : (Real)1, omz_m = k == 1 ? one_z : (Real)1;
+        const Real omz_p = k == g.gz ? one_zp : (Real)1, omz_m = k == 1 ? one_zm : (Real)1;
         const bool in_z = k > 1 && k < g.gz;
         const double Tp = t_per_plane ? sh.sT[t] : 0.0;
 #pragma unroll
@@ -1066,7 +1206,8 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchun
     load_plane(0, k0 - 1);
     load_plane(1, k0);
     int sm = 0, sc = 1, sp = 2;
-    const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_z = (Real)(1 - g.padz);
+    const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_zp = (Real)(1 - g.padz_hi),
+               one_zm = (Real)(1 - g.padz_lo);
     for (int k = k0; k <= k1; k++) {
         load_plane(sp, k + 1);
         __syncthreads();
@@ -1080,7 +1221,7 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchun
                                    s_fs[sc][ly - 1][lx], s_fs[sp][ly][lx], s_fs[sm][ly][lx]};
             const Real one_m[6] = {i == g.gx ? one_x : (Real)1, i == 1 ? one_x : (Real)1,
                                    j == g.gy ? one_y : (Real)1, j == 1 ? one_y : (Real)1,
-                                   k == g.gz ? one_z : (Real)1, k == 1 ? one_z : (Real)1};
+                                   k == g.gz ? one_zp : (Real)1, k == 1 ? one_zm : (Real)1};
             const int grc = gr[c];
             const double Td = temp_cell(p, a.d.T, c, j, k, ts);
             Real cen, cl_new, fs_new;
@@ -1821,6 +1962,34 @@ static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t
     PROF_END(KID_DIFFUSE_FS);
     n++;
     return n + launch_post_t<Real>(a, st, prof);
+}
+
+template <typename Real>
+static int launch_slab_phase_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st, int phase, int resume)
+{
+    int n = 0;
+    if (phase == 0) {
+        if (!resume && a.d.nsites > 0) {
+            k_nuc<Real><<<a.d.nuc_blocks, NUC_NT, 0, st>>>(a);
+            n++;
+        }
+        k_act_local<<<1, ACT_NT, 0, st>>>(a);
+        return n + 1;
+    }
+    if (phase == 1) {
+        k_act_slab<<<1, ACT_NT, 0, st>>>(a);
+        launch_stencil_t<Real>(a, tma, st);
+        return 2;
+    }
+    k_slab_merge<<<1, 256, 0, st>>>(a);
+    return 1 + launch_post_t<Real>(a, st, nullptr);
+}
+
+int launch_slab_phase(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream, int phase, int resume)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == MMS_PREC_F32) return launch_slab_phase_t<float>(a, tma, st, phase, resume);
+    return launch_slab_phase_t<double>(a, tma, st, phase, resume);
 }
 
 int launch_curv(const KernelArgs &a, int precision, void *stream)

@@ -123,6 +123,14 @@ struct mms_ctx {
     void *stage = nullptr;    // field staging buffer for host copies
     size_t stage_bytes = 0;
     int rng_checked_grains = -1;  // grain count at the last orientation-table check
+    // z-slab split of one domain: p holds this slab's parameters (its
+    // layers of subblocks), gp and gg the whole domain's; ranks holds every
+    // emulated rank of the whole domain, of which this slab owns
+    // [r0, r0 + ka.g.nranks)
+    int nslabs = 1, slab = 0, r0 = 0, kz0 = 0;
+    mms_params gp{};
+    Geo gg{};
+    std::vector<cudaEvent_t> slab_events;  // mms_slab_group_step's ordering events
     // frozen-CA record for the adjoint
     struct AdjRec {
         unsigned long long t0 = 0;
@@ -215,7 +223,8 @@ long long rcidx(const Geo &g, long long i, long long j, long long k) { return re
 cudaError_t copy_out(mms_ctx *ctx, void *host, const void *dev, size_t es);
 cudaError_t copy_in(mms_ctx *ctx, void *dev, const void *host, size_t es);
 
-// Extract the sparse site list in (rank, local raster) order.
+// Extract the sparse site list in (rank, local raster) order from the
+// whole domain's threshold array (reference layout), for this context's ranks.
 void extract_sites(mms_ctx *ctx, const std::vector<float> &thr)
 {
     const mms_params &p = ctx->p;
@@ -225,15 +234,15 @@ void extract_sites(mms_ctx *ctx, const std::vector<float> &thr)
     ctx->site_rank.clear();
     ctx->site_index.clear();
     for (int ri = 0; ri < g.nranks; ri++) {
-        const Rank &r = ctx->ranks[ri];
+        const Rank &r = ctx->ranks[ctx->r0 + ri];
         for (long long z = 1; z <= p.gsdimz; z++)
             for (long long y = 1; y <= p.gsdimy; y++)
                 for (long long x = 1; x <= p.gsdimx; x++) {
                     long long I = (long long)r.sbx * p.gsdimx + x, J = (long long)r.sby * p.gsdimy + y,
                               K = (long long)r.sbz * p.gsdimz + z;
-                    long long c = rcidx(g, I, J, K);
+                    long long c = rcidx(ctx->gg, I, J, K);
                     if (thr[c] != INFINITY) {
-                        ctx->site_cell.push_back(cidx(g, I, J, K));
+                        ctx->site_cell.push_back(cidx(g, I, J, K - ctx->kz0));
                         ctx->site_thr.push_back(thr[c]);
                         ctx->site_rank.push_back(ri);
                     }
@@ -287,12 +296,14 @@ mms_status upload_nucpt(mms_ctx *ctx)
     DevPtrs &d = ctx->ka.d;
     ctx->nucpt.clear();
     for (int ri = 0; ri < g.nranks; ri++) {
-        const Rank &r = ctx->ranks[ri];
+        const int R = ctx->r0 + ri;
+        const Rank &r = ctx->ranks[R];
         for (int j = 0; j < (int)r.nuc.size(); j++) {
             const NucPt &n = r.nuc[j];
-            if (n.cx >= (size_t)g.gx || n.cy >= (size_t)g.gy || n.cz >= (size_t)g.gz) continue;
-            long long key = cidx(g, (long long)n.cx + 1, (long long)n.cy + 1, (long long)n.cz + 1);
-            ctx->nucpt.push_back({key, {ri, j}});
+            const long long kz = (long long)n.cz - ctx->kz0;
+            if (n.cx >= (size_t)g.gx || n.cy >= (size_t)g.gy || kz < 0 || kz >= g.gz) continue;
+            long long key = cidx(g, (long long)n.cx + 1, (long long)n.cy + 1, kz + 1);
+            ctx->nucpt.push_back({key, {R, j}});
         }
     }
     std::stable_sort(ctx->nucpt.begin(), ctx->nucpt.end(),
@@ -341,7 +352,7 @@ mms_status refill_rng(mms_ctx *ctx, bool force)
     std::vector<double> tab((size_t)g.nranks * d.rng_cap * 9);
     std::vector<long long> base(g.nranks);
     for (int ri = 0; ri < g.nranks; ri++) {
-        Rank &r = ctx->ranks[ri];
+        Rank &r = ctx->ranks[ctx->r0 + ri];
         r.rng_base += used[ri];
         while ((long long)r.angles.size() < r.rng_base + d.rng_cap) {
             NucPt n{};
@@ -429,6 +440,9 @@ int launch_one_step(mms_ctx *ctx, int start_stage)
 }
 
 // Pull grain records created since the last sync and rebuild grain_t.
+// A grain made by another slab of a split domain carries its whole-domain
+// cell and emulated rank; every slab replays every rank's stream, so its
+// orientation draw is found here too.
 mms_status sync_grains(mms_ctx *ctx)
 {
     mms_status st = read_ctl(ctx);
@@ -438,6 +452,13 @@ mms_status sync_grains(mms_ctx *ctx)
     int first = ctx->grains_synced, cnt = ng - first;
     std::vector<GrainLog> log(cnt);
     CU(d2h(ctx, log.data(), ctx->ka.d.grain_log + first, sizeof(GrainLog) * cnt));
+    bool need_rot = false;
+    for (const GrainLog &lg : log) need_rot |= (lg.kind == 3) || (lg.kind & GL_REMOTE);
+    std::vector<double> rows;
+    if (need_rot) {
+        rows.resize((size_t)cnt * 9);
+        CU(d2h(ctx, rows.data(), ctx->ka.d.grain_rot + 9 * (long long)first, sizeof(double) * 9 * cnt));
+    }
     if ((int)ctx->grains.size() < ng) ctx->grains.resize(ng);
     const mms_params &p = ctx->p;
     const Geo &g = ctx->ka.g;
@@ -447,38 +468,53 @@ mms_status sync_grains(mms_ctx *ctx)
         std::memset(&gr, 0, sizeof gr);
         if (lg.kind == 3) {
             // pre-filled grain (mms_set_grains): no nucleus, rotation from the table
-            double R[9];
-            CU(d2h(ctx, R, ctx->ka.d.grain_rot + 9 * (long long)(first + i), sizeof R));
             for (int a = 0; a < 3; a++)
-                for (int b = 0; b < 3; b++) gr.rotmat[a][b] = R[3 * a + b];
+                for (int b = 0; b < 3; b++) gr.rotmat[a][b] = rows[9 * (size_t)i + 3 * a + b];
             continue;
         }
-        long long c = lg.cell;
-        long long K = c / g.sz, J = (c % g.sz) / g.sy, I = c % g.sy;
+        const bool remote = (lg.kind & GL_REMOTE) != 0;
+        const int kind = lg.kind & ~GL_REMOTE;
+        long long c = lg.cell, I, J, K;  // whole-domain interior-based cell coordinates
+        if (remote) {
+            K = c / ctx->gg.rsz;
+            J = (c % ctx->gg.rsz) / ctx->gg.rsy;
+            I = c % ctx->gg.rsy;
+        } else {
+            K = c / g.sz + ctx->kz0;
+            J = (c % g.sz) / g.sy;
+            I = c % g.sy;
+        }
         NucPt nuc{};
-        if (lg.kind == 0) {
+        if (kind == 0) {
             int rr = (int)(lg.aux >> 32), jj = (int)(lg.aux & 0xffffffff);
             nuc = ctx->ranks[rr].nuc[jj];
         } else {
             nuc.x = cell2real(p, 0, (double)(I - 1));
             nuc.y = cell2real(p, 1, (double)(J - 1));
             nuc.z = cell2real(p, 2, (double)(K - 1));
-            if (ctx->site_index.empty())
-                for (size_t s = 0; s < ctx->site_cell.size(); s++) ctx->site_index.emplace(ctx->site_cell[s], s);
-            auto it = ctx->site_index.find(c);
-            double thr = (it == ctx->site_index.end()) ? (double)INFINITY : (double)ctx->site_thr[it->second];
-            nuc.threshold = thr;
-            if (lg.kind == 1) {
-                const auto &a = ctx->ranks[lg.rank].angles[lg.aux];
+            nuc.threshold = (double)lg.thr;
+            if (kind == 1) {
+                Rank &rk = ctx->ranks[lg.rank];
+                while ((long long)rk.angles.size() <= lg.aux) {  // another slab's rank
+                    NucPt n{};
+                    draw_orientation(ctx->p, rk, n);
+                    rk.angles.push_back({n.gx, n.gy, n.gz});
+                }
+                const auto &a = rk.angles[lg.aux];
                 nuc.gx = a[0];
                 nuc.gy = a[1];
                 nuc.gz = a[2];
             }
         }
         double R[9];
-        rotmat_from_angles(nuc.gx, nuc.gy, nuc.gz, R);
-        auto ik = std::lower_bound(ctx->inj_key.begin(), ctx->inj_key.end(), c);
-        if (ik != ctx->inj_key.end() && *ik == c) std::memcpy(R, &ctx->inj_rot[9 * (ik - ctx->inj_key.begin())], sizeof R);
+        if (remote) {
+            std::memcpy(R, &rows[9 * (size_t)i], sizeof R);
+        } else {
+            rotmat_from_angles(nuc.gx, nuc.gy, nuc.gz, R);
+            auto ik = std::lower_bound(ctx->inj_key.begin(), ctx->inj_key.end(), c);
+            if (ik != ctx->inj_key.end() && *ik == c)
+                std::memcpy(R, &ctx->inj_rot[9 * (ik - ctx->inj_key.begin())], sizeof R);
+        }
         gr.nuc_x = nuc.x;
         gr.nuc_y = nuc.y;
         gr.nuc_z = nuc.z;
@@ -549,6 +585,8 @@ cudaError_t copy_in(mms_ctx *ctx, void *dev, const void *host, size_t es)
     if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(ctx->stream);
 }
+
+mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out);
 
 }  // namespace
 
@@ -752,11 +790,74 @@ uint64_t mms_kernel_launches(const mms_ctx *ctx) { return ctx ? ctx->launches : 
 size_t mms_num_cells(const mms_ctx *ctx) { return ctx ? (size_t)ctx->ka.g.rN : 0; }
 int mms_uses_tma(const mms_ctx *ctx) { return ctx ? ctx->tma.ok : 0; }
 
-mms_status mms_create(const mms_params *pin, mms_ctx **out)
+mms_status mms_create(const mms_params *pin, mms_ctx **out) { return create_ctx(pin, 1, 0, out); }
+
+mms_status mms_slab_create(const mms_params *global, int nslabs, int slab, mms_ctx **out)
+{
+    return create_ctx(global, nslabs, slab, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Layers of subblocks [L0, L1) of slab `slab` of nslabs (as even as integer
+// division makes them).
+bool slab_span(const mms_params &p, int nslabs, int slab, int &L0, int &L1)
+{
+    if (nslabs < 1 || slab < 0 || slab >= nslabs || nslabs > p.gnsbz) return false;
+    L0 = (int)((long long)slab * p.gnsbz / nslabs);
+    L1 = (int)((long long)(slab + 1) * p.gnsbz / nslabs);
+    return true;
+}
+
+// Largest number of nucleation sites any slab holds: the capacity of every
+// slab's row buffer of new grains (the same on every slab, computed from
+// the whole domain's thresholds).
+int slab_capacity(const mms_ctx *ctx, const std::vector<float> &thr)
+{
+    const Geo &G = ctx->gg;
+    std::vector<long long> per_plane((size_t)G.gz + 2, 0);
+    for (long long K = 1; K <= G.gz; K++)
+        for (long long J = 1; J <= G.gy; J++)
+            for (long long I = 1; I <= G.gx; I++)
+                if (thr[(size_t)rcidx(G, I, J, K)] != INFINITY) per_plane[K]++;
+    long long cap = 1;
+    for (int s = 0; s < ctx->nslabs; s++) {
+        int L0, L1;
+        slab_span(ctx->gp, ctx->nslabs, s, L0, L1);
+        long long n = 0;
+        for (long long K = (long long)L0 * G.sbz + 1; K <= (long long)L1 * G.sbz; K++) n += per_plane[K];
+        cap = std::max(cap, n);
+    }
+    return (int)std::min<long long>(cap, 1LL << 30);
+}
+
+mms_status alloc_slab_rows(mms_ctx *ctx, int cap)
+{
+    DevPtrs &d = ctx->ka.d;
+    if (ctx->nslabs < 2) return MMS_OK;
+    if (d.x2_send && d.slab_cap == cap) return MMS_OK;
+    dfree(ctx, d.x2_send);
+    dfree(ctx, d.x2_recv);
+    d.x2_send = d.x2_recv = nullptr;
+    d.slab_cap = cap;
+    drop_graph(ctx);
+    mms_status st;
+    if ((st = dalloc(ctx, &d.x2_send, (size_t)cap)) || (st = dalloc(ctx, &d.x2_recv, (size_t)cap * ctx->nslabs)))
+        return st;
+    return MMS_OK;
+}
+
+mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out)
 {
     if (!pin || !out) return MMS_ERR_ARG;
     *out = nullptr;
     const mms_params &p0 = *pin;
+    int L0 = 0, L1 = 0;
+    if (p0.gnsbz < 1 || !slab_span(p0, nslabs, slab, L0, L1)) return MMS_ERR_ARG;
+    // the curvature stencil reaches three planes, beyond a slab's one-plane halo
+    if (nslabs > 1 && p0.tip_curv) return MMS_ERR_ARG;
     if (p0.gnsbx < 1 || p0.gnsby < 1 || p0.gnsbz < 1 || p0.gsdimx < 1 || p0.gsdimy < 1 || p0.gsdimz < 1 ||
         p0.cellSize <= 0 || p0.ts_delt <= 0 || p0.maxTotalGrains < 1 || p0.maxTotalGrains > 0x7ffffffeULL)
         return MMS_ERR_ARG;
@@ -776,6 +877,12 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
     for (int i = 0; i < p0.n_nuc_volumes; i++) ctx->vols.push_back(p0.nuc_volumes[i]);
     ctx->p.fixed_nucs = nullptr;
     ctx->p.nuc_volumes = nullptr;
+    ctx->gp = ctx->p;
+    ctx->nslabs = nslabs;
+    ctx->slab = slab;
+    ctx->p.gnsbz = L1 - L0;
+    ctx->kz0 = L0 * p0.gsdimz;
+    ctx->r0 = L0 * p0.gnsbx * p0.gnsby;
     ctx->prec = p0.precision;
     ctx->device = p0.device;
     const mms_params &p = ctx->p;
@@ -794,8 +901,12 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
     cudaMallocHost((void **)&ctx->h_ctl, sizeof(Ctl));
     cudaMallocHost((void **)&ctx->h_red, sizeof(double));
 
+    ctx->gg = make_geo(ctx->gp);
     ctx->ka.g = make_geo(p);
     Geo &g = ctx->ka.g;
+    // a slab's inner z faces border the neighbouring slab, not the mold
+    g.padz_lo = (slab == 0) ? p0.padBndyZ : 0;
+    g.padz_hi = (slab == nslabs - 1) ? p0.padBndyZ : 0;
 
     Phys &ph = ctx->ka.p;
     ph.rs = p.Dsol * dtx;
@@ -826,7 +937,8 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
     ph.ts_delt = p.ts_delt;
     ph.cellSize = p.cellSize;
     for (int a = 0; a < 3; a++) ph.origin[a] = p.origin_offset[a];
-    ph.gz_is_one = (g.gz == 1);
+    ph.gz_is_one = (ctx->gg.gz == 1);
+    ph.kz0 = ctx->kz0;
     ph.am = p.am;
     ph.amlayer = p.amlayer;
     ph.use_orientation = p.gnUseOrientation;
@@ -882,9 +994,11 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         std::memcpy(d.zero_rot, zr, sizeof zr);
     }
 
-    // ranks and their streams
-    ctx->ranks.resize(g.nranks);
-    for (int r = 0; r < g.nranks; r++) {
+    // every rank of the whole domain and its stream (a slab replays all of
+    // them: rank 0 draws sites for every rank, and grain records of other
+    // slabs refer to their ranks' draws)
+    ctx->ranks.resize(ctx->gg.nranks);
+    for (int r = 0; r < ctx->gg.nranks; r++) {
         Rank &rk = ctx->ranks[r];
         rk.sbx = r % p.gnsbx;
         rk.sby = (r / p.gnsbx) % p.gnsby;
@@ -892,7 +1006,7 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         rk.seed_with((unsigned)r + 1 + p.base_random_seed);
     }
     // initial fields: ce = cl = Cinit everywhere, fs = gr = dc = 0 (setup.c:59-79)
-    std::vector<signed char> mold = make_mold(g);  // reference layout
+    std::vector<signed char> mold = make_mold(ctx->gg);  // whole domain, reference layout
     {
         std::vector<double> init(N, p.Cinit);
         double *dtmp;
@@ -909,10 +1023,18 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
         // tempPrepareSB_int lsindex (temperature.c:183-189) at timestep 0
         ctx->launches += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, nullptr);
     }
-    std::vector<float> thr((size_t)g.rN, INFINITY);  // reference layout
-    setup_sites(ctx->p, ctx->ka.g, ctx->fixed, ctx->vols, ctx->ranks, thr, mold);
+    std::vector<float> thr((size_t)ctx->gg.rN, INFINITY);  // whole domain, reference layout
+    setup_sites(ctx->gp, ctx->gg, ctx->fixed, ctx->vols, ctx->ranks, thr, mold);
     extract_sites(ctx, thr);
     if ((st = upload_sites(ctx)) || (st = upload_nucpt(ctx))) return fail(st);
+    d.nslabs = nslabs;
+    d.slab = slab;
+    d.rank0 = ctx->r0;
+    if (nslabs > 1) {
+        if ((st = dalloc(ctx, &d.x1_send, 2)) || (st = dalloc(ctx, &d.x1_recv, 2 * (size_t)nslabs)) ||
+            (st = alloc_slab_rows(ctx, slab_capacity(ctx, thr))))
+            return fail(st);
+    }
     make_tma(ctx->ka, ctx->prec, ctx->tma);
     // orientation tables
     if (p.gnUseOrientation) {
@@ -938,6 +1060,10 @@ mms_status mms_create(const mms_params *pin, mms_ctx **out)
     return MMS_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
 mms_status mms_destroy(mms_ctx *ctx)
 {
     if (!ctx) return MMS_OK;
@@ -945,6 +1071,8 @@ mms_status mms_destroy(mms_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (void *p : ctx->allocs) cudaFree(p);
     ctx->allocs.clear();
+    for (cudaEvent_t e : ctx->slab_events) cudaEventDestroy(e);
+    ctx->slab_events.clear();
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
     if (ctx->h_red) cudaFreeHost(ctx->h_red);
     drop_graph(ctx);
@@ -965,7 +1093,7 @@ mms_status mms_set_grains(mms_ctx *ctx, int n, const double *rotmat9)
     if (n) {
         CU(h2d(ctx, ctx->ka.d.grain_rot + 9, rotmat9, sizeof(double) * 9 * (size_t)n));
         std::vector<GrainLog> log((size_t)n);
-        for (int g = 0; g < n; g++) log[g] = GrainLog{-1, 0ULL, 3, 0, (long long)(g + 1)};
+        for (int g = 0; g < n; g++) log[g] = GrainLog{-1, 0ULL, 3, 0, (long long)(g + 1), 0.f, 0};
         CU(h2d(ctx, ctx->ka.d.grain_log + 1, log.data(), sizeof(GrainLog) * (size_t)n));
     }
     Ctl c = *ctx->h_ctl;
@@ -985,12 +1113,12 @@ mms_status mms_set_sites(mms_ctx *ctx, int64_t n, const int32_t *gxyz, const flo
     if (!ctx || (n && (!gxyz || !thresholds))) return MMS_ERR_ARG;
     if (ctx->stepped) return MMS_ERR_STATE;
     cudaSetDevice(ctx->device);
-    const Geo &g = ctx->ka.g;
-    std::vector<float> thr((size_t)g.rN, INFINITY);
+    const Geo &g = ctx->ka.g, &G = ctx->gg;
+    std::vector<float> thr((size_t)G.rN, INFINITY);  // whole domain
     for (int64_t s = 0; s < n; s++) {
         long long x = gxyz[3 * s], y = gxyz[3 * s + 1], z = gxyz[3 * s + 2];
-        if (x < 0 || y < 0 || z < 0 || x >= g.gx || y >= g.gy || z >= g.gz) return MMS_ERR_ARG;
-        thr[rcidx(g, x + 1, y + 1, z + 1)] = thresholds[s];
+        if (x < 0 || y < 0 || z < 0 || x >= G.gx || y >= G.gy || z >= G.gz) return MMS_ERR_ARG;
+        thr[rcidx(G, x + 1, y + 1, z + 1)] = thresholds[s];
     }
     // rewind every stream to where init_sb_nucleation would start drawing
     for (Rank &r : ctx->ranks) {
@@ -1003,6 +1131,7 @@ mms_status mms_set_sites(mms_ctx *ctx, int64_t n, const int32_t *gxyz, const flo
     extract_sites(ctx, thr);
     mms_status st = upload_sites(ctx);
     if (st) return st;
+    if (ctx->nslabs > 1 && (st = alloc_slab_rows(ctx, slab_capacity(ctx, thr)))) return st;
     if (ctx->p.gnUseOrientation) {
         CU(dzero(ctx, ctx->ka.d.rng_used, sizeof(int) * g.nranks));
         st = refill_rng(ctx, true);
@@ -1014,12 +1143,14 @@ mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxy
 {
     if (!ctx || (n && (!gxyz || !rotmat9))) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
-    const Geo &g = ctx->ka.g;
+    const Geo &g = ctx->ka.g, &G = ctx->gg;
     std::vector<std::pair<long long, int64_t>> kv;
     for (int64_t s = 0; s < n; s++) {
         long long x = gxyz[3 * s], y = gxyz[3 * s + 1], z = gxyz[3 * s + 2];
-        if (x < 0 || y < 0 || z < 0 || x >= g.gx || y >= g.gy || z >= g.gz) return MMS_ERR_ARG;
-        kv.push_back({cidx(g, x + 1, y + 1, z + 1), s});
+        if (x < 0 || y < 0 || z < 0 || x >= G.gx || y >= G.gy || z >= G.gz) return MMS_ERR_ARG;
+        const long long zl = z - ctx->kz0;  // whole-domain z; another slab's cells are skipped
+        if (zl < 0 || zl >= g.gz) continue;
+        kv.push_back({cidx(g, x + 1, y + 1, zl + 1), s});
     }
     std::stable_sort(kv.begin(), kv.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
     ctx->inj_key.clear();
@@ -1049,6 +1180,10 @@ mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxy
 mms_status mms_step(mms_ctx *ctx, int nsteps)
 {
     if (!ctx || nsteps < 0) return MMS_ERR_ARG;
+    if (ctx->nslabs > 1) {
+        ctx->err = "a slab of a split domain steps with its group (mms_slab_group_step, mms_slab_launch)";
+        return MMS_ERR_ARG;
+    }
     cudaSetDevice(ctx->device);
     ctx->stepped = true;
     const int chunk = 256;
@@ -1456,7 +1591,7 @@ mms_status mms_adjoint_release(mms_ctx *ctx)
 
 mms_status mms_adjoint_record(mms_ctx *ctx, int nsteps, int checkpoint_every)
 {
-    if (!ctx || nsteps < 1 || checkpoint_every < 1) return MMS_ERR_ARG;
+    if (!ctx || nsteps < 1 || checkpoint_every < 1 || ctx->nslabs > 1) return MMS_ERR_ARG;
     if (ctx->ka.p.temp_mode == 2) {
         ctx->err = "the adjoint supports the analytic temperature models only";
         return MMS_ERR_ARG;
@@ -2113,7 +2248,7 @@ mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path)
     const int cur = (int)(c.timestep & 1ULL);
     CkHeader h{};
     std::memcpy(h.magic, "MMSCKPT", 8);
-    h.version = 1;
+    h.version = 2;
     h.prec = ctx->prec;
     h.gx = g.gx;
     h.gy = g.gy;
@@ -2185,7 +2320,7 @@ mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path)
         ctx->err = why;
         return s;
     };
-    if (!fread_all(fp, &h, sizeof h) || std::memcmp(h.magic, "MMSCKPT", 8) != 0 || h.version != 1)
+    if (!fread_all(fp, &h, sizeof h) || std::memcmp(h.magic, "MMSCKPT", 8) != 0 || h.version != 2)
         return fail(MMS_ERR_IO, "not a checkpoint of this library");
     if (h.prec != ctx->prec || h.gx != g.gx || h.gy != g.gy || h.gz != g.gz || h.nranks != g.nranks ||
         h.rng_cap != d.rng_cap || h.N != (int64_t)N || h.P != g.P ||
@@ -2270,6 +2405,290 @@ mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path)
     ctx->grains_synced = 1;
     ctx->stepped = true;
     drop_graph(ctx);
+    return MMS_OK;
+}
+
+}  // extern "C"
+
+// ============================================== z-slab split of one domain
+// The reference splits its domain into NSubblocks MPI ranks that exchange
+// halo planes and grain lists inside doiteration (calculate.c:193-352).
+// Here the split is into z-slabs of whole subblock layers, one context per
+// slab: the emulated ranks, their streams, interface lists and dc_tmp
+// slots stay inside one slab, and a step needs two exchanges:
+//   point 0, after nucleation: the cl and fs boundary planes of the step's
+//     input buffers, and every slab's {candidates, short of draws};
+//   point 1, after the stencil: the fs (output buffer), gr, dc and solid
+//     bitmask boundary planes, and every slab's new grains.
+namespace {
+
+// Transfers of one exchange point for the step that starts at timestep ts
+// (its input buffers are ts & 1).  Halo entries come per neighbour in a
+// fixed field order, so a slab's entries for peer q and q's entries for
+// this slab pair up one to one.
+void slab_plan(mms_ctx *ctx, int point, unsigned long long ts, std::vector<mms_slab_xfer> &out)
+{
+    out.clear();
+    const Geo &g = ctx->ka.g;
+    const DevPtrs &d = ctx->ka.d;
+    const size_t es = elem_size(ctx);
+    const int bin = (int)(ts & 1ULL), bout = (int)((ts + 1) & 1ULL);
+    struct Field {
+        void *base;
+        size_t plane;  // bytes of one z-plane
+    };
+    std::vector<Field> f;
+    if (point == 0) {
+        f.push_back({d.cl[bin], (size_t)g.sz * es});
+        f.push_back({d.fs[bin], (size_t)g.sz * es});
+    } else {
+        f.push_back({d.fs[bout], (size_t)g.sz * es});
+        f.push_back({d.gr, (size_t)g.sz * sizeof(int)});
+        f.push_back({d.dc, (size_t)g.sz * sizeof(Dc3)});
+        f.push_back({d.solid_bits, (size_t)g.wpr * (g.gy + 2) * sizeof(unsigned)});
+    }
+    auto plane = [](const Field &x, long long k) { return (void *)((char *)x.base + (size_t)k * x.plane); };
+    if (ctx->slab > 0)
+        for (const Field &x : f) out.push_back({MMS_XFER_HALO, ctx->slab - 1, plane(x, 1), plane(x, 0), x.plane});
+    if (ctx->slab < ctx->nslabs - 1)
+        for (const Field &x : f)
+            out.push_back({MMS_XFER_HALO, ctx->slab + 1, plane(x, g.gz), plane(x, g.gz + 1), x.plane});
+    if (point == 0) out.push_back({MMS_XFER_GATHER, -1, d.x1_send, d.x1_recv, 2 * sizeof(int)});
+    else out.push_back({MMS_XFER_GATHER, -1, d.x2_send, d.x2_recv, (uint64_t)d.slab_cap * sizeof(SlabRow)});
+}
+
+mms_status slab_launch(mms_ctx *ctx, int phase, int resume)
+{
+    cudaSetDevice(ctx->device);
+    if (phase == 0 && !resume && ctx->p.am)
+        ctx->launches += launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, ctx->stream, nullptr);
+    ctx->launches += launch_slab_phase(ctx->ka, ctx->tma, ctx->prec, ctx->stream, phase, resume);
+    CU(cudaGetLastError());
+    return MMS_OK;
+}
+
+// Slab b pulls what point `point` brings it, on its own stream, after the
+// phase each source slab recorded in ev[source].
+mms_status slab_pull(mms_ctx *const *slabs, int S, int b, int point, unsigned long long ts, int ev)
+{
+    mms_ctx *ctx = slabs[b];
+    std::vector<mms_slab_xfer> mine, theirs;
+    slab_plan(ctx, point, ts, mine);
+    cudaSetDevice(ctx->device);
+    auto copy = [&](void *dst, const mms_ctx *src_ctx, const void *src, size_t bytes) -> cudaError_t {
+        cudaError_t e = cudaStreamWaitEvent(ctx->stream, src_ctx->slab_events[ev], 0);
+        if (e != cudaSuccess) return e;
+        if (src_ctx->device == ctx->device)
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+        return cudaMemcpyPeerAsync(dst, ctx->device, src, src_ctx->device, bytes, ctx->stream);
+    };
+    for (int peer : {b - 1, b + 1}) {
+        if (peer < 0 || peer >= S) continue;
+        slab_plan(slabs[peer], point, ts, theirs);
+        std::vector<const mms_slab_xfer *> a, q;
+        for (const mms_slab_xfer &x : mine)
+            if (x.kind == MMS_XFER_HALO && x.peer == peer) a.push_back(&x);
+        for (const mms_slab_xfer &x : theirs)
+            if (x.kind == MMS_XFER_HALO && x.peer == b) q.push_back(&x);
+        if (a.size() != q.size()) {
+            ctx->err = "slab exchange plans do not pair";
+            return MMS_ERR_STATE;
+        }
+        for (size_t i = 0; i < a.size(); i++) CU(copy(a[i]->recv, slabs[peer], q[i]->send, a[i]->bytes));
+    }
+    const mms_slab_xfer *gm = nullptr;
+    for (const mms_slab_xfer &x : mine)
+        if (x.kind == MMS_XFER_GATHER) gm = &x;
+    for (int a = 0; a < S; a++) {
+        slab_plan(slabs[a], point, ts, theirs);
+        for (const mms_slab_xfer &x : theirs)
+            if (x.kind == MMS_XFER_GATHER) {
+                if (x.bytes != gm->bytes) {
+                    ctx->err = "slab gather sizes differ";
+                    return MMS_ERR_STATE;
+                }
+                CU(copy((char *)gm->recv + (size_t)a * gm->bytes, slabs[a], x.send, x.bytes));
+            }
+    }
+    return MMS_OK;
+}
+
+// One step of every slab (resume: the step that stalled at activation).
+// Events per slab: 0 after phase 0, 1 after phase 1, 2 after its pulls of
+// point 1; phase 2 of every slab waits for every slab's pulls, since they
+// read its planes and rows.
+mms_status slab_group_one(mms_ctx *const *slabs, int S, unsigned long long ts, int resume)
+{
+    mms_status st;
+    auto record = [&](int s, int ev) -> mms_status {
+        mms_ctx *ctx = slabs[s];
+        cudaSetDevice(ctx->device);
+        CU(cudaEventRecord(ctx->slab_events[ev], ctx->stream));
+        return MMS_OK;
+    };
+    for (int s = 0; s < S; s++)
+        if ((st = slab_launch(slabs[s], 0, resume)) || (st = record(s, 0))) return st;
+    for (int s = 0; s < S; s++)
+        if ((st = slab_pull(slabs, S, s, 0, ts, 0))) return st;
+    for (int s = 0; s < S; s++)
+        if ((st = slab_launch(slabs[s], 1, 0)) || (st = record(s, 1))) return st;
+    for (int s = 0; s < S; s++)
+        if ((st = slab_pull(slabs, S, s, 1, ts, 1)) || (st = record(s, 2))) return st;
+    for (int s = 0; s < S; s++) {
+        mms_ctx *ctx = slabs[s];
+        cudaSetDevice(ctx->device);
+        for (int q = 0; q < S; q++)
+            if (q != s) CU(cudaStreamWaitEvent(ctx->stream, slabs[q]->slab_events[2], 0));
+        if ((st = slab_launch(ctx, 2, 0))) return st;
+    }
+    return MMS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mms_status mms_slab_layout_of(const mms_params *global, int nslabs, int slab, mms_slab_layout *out)
+{
+    if (!global || !out) return MMS_ERR_ARG;
+    int L0, L1;
+    if (global->gnsbz < 1 || !slab_span(*global, nslabs, slab, L0, L1)) return MMS_ERR_ARG;
+    out->nslabs = nslabs;
+    out->slab = slab;
+    out->z_begin = L0 * global->gsdimz;
+    out->z_cells = (L1 - L0) * global->gsdimz;
+    out->rank_begin = L0 * global->gnsbx * global->gnsby;
+    out->rank_count = (L1 - L0) * global->gnsbx * global->gnsby;
+    return MMS_OK;
+}
+
+mms_status mms_slab_get_layout(const mms_ctx *ctx, mms_slab_layout *out)
+{
+    if (!ctx) return MMS_ERR_ARG;
+    return mms_slab_layout_of(&ctx->gp, ctx->nslabs, ctx->slab, out);
+}
+
+mms_status mms_slab_launch(mms_ctx *ctx, int phase, int resume)
+{
+    if (!ctx || phase < 0 || phase > 2 || (resume && phase != 0)) return MMS_ERR_ARG;
+    ctx->stepped = true;
+    return slab_launch(ctx, phase, resume);
+}
+
+mms_status mms_slab_exchange_plan(mms_ctx *ctx, int point, uint64_t timestep, mms_slab_xfer *out, int max, int *n)
+{
+    if (!ctx || !n || point < 0 || point > 1 || max < 0 || (max && !out)) return MMS_ERR_ARG;
+    if (ctx->nslabs < 2) {
+        *n = 0;
+        return MMS_OK;
+    }
+    std::vector<mms_slab_xfer> v;
+    slab_plan(ctx, point, timestep, v);
+    *n = (int)v.size();
+    if ((int)v.size() > max) return MMS_ERR_ARG;
+    std::copy(v.begin(), v.end(), out);
+    return MMS_OK;
+}
+
+mms_status mms_slab_poll(mms_ctx *ctx, uint64_t *timestep, int *stalled)
+{
+    if (!ctx) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    const Ctl &c = *ctx->h_ctl;
+    if (c.stall == STALL_ERROR) return (mms_status)(c.status ? c.status : MMS_ERR_STATE);
+    if (timestep) *timestep = c.timestep;
+    if (stalled) *stalled = (c.stall == STALL_RNG) ? 1 : 0;
+    return MMS_OK;
+}
+
+mms_status mms_slab_refill(mms_ctx *ctx)
+{
+    if (!ctx) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    if ((st = refill_rng(ctx, ctx->h_ctl->stall == STALL_RNG))) return st;
+    if (ctx->h_ctl->stall == STALL_RNG) {
+        int zero = 0;
+        CU(h2d(ctx, &ctx->ka.d.ctl->stall, &zero, sizeof(int)));
+    }
+    return MMS_OK;
+}
+
+mms_status mms_slab_group_step(mms_ctx *const *slabs, int nslabs, int nsteps)
+{
+    if (!slabs || nslabs < 1 || nsteps < 0) return MMS_ERR_ARG;
+    for (int s = 0; s < nslabs; s++) {
+        mms_ctx *c = slabs[s];
+        if (!c || c->nslabs != nslabs || c->slab != s || c->prec != slabs[0]->prec ||
+            c->gg.N != slabs[0]->gg.N || c->ka.d.slab_cap != slabs[0]->ka.d.slab_cap)
+            return MMS_ERR_ARG;
+    }
+    if (nslabs == 1) return mms_step(slabs[0], nsteps);
+    mms_status st;
+    for (int s = 0; s < nslabs; s++) {
+        mms_ctx *c = slabs[s];
+        c->stepped = true;
+        cudaSetDevice(c->device);
+        while (c->slab_events.size() < 3) {
+            cudaEvent_t e;
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+                c->err = "cudaEventCreateWithFlags failed";
+                return MMS_ERR_CUDA;
+            }
+            c->slab_events.push_back(e);
+        }
+        for (int q = 0; q < nslabs; q++)
+            if (slabs[q]->device != c->device) {
+                cudaError_t e = cudaDeviceEnablePeerAccess(slabs[q]->device, 0);
+                if (e != cudaSuccess) cudaGetLastError();  // already enabled, or copies are staged
+            }
+    }
+    // every slab at the same step, none stalled
+    uint64_t ts = 0;
+    for (int s = 0; s < nslabs; s++) {
+        uint64_t t;
+        int stl;
+        if ((st = mms_slab_poll(slabs[s], &t, &stl))) return st;
+        if (s == 0) ts = t;
+        if (t != ts || stl) {
+            slabs[s]->err = "slabs are not at the same step";
+            return MMS_ERR_STATE;
+        }
+    }
+    const uint64_t target = ts + (uint64_t)nsteps;
+    const int chunk = 256;
+    while (ts < target) {
+        const int n = (int)std::min<uint64_t>(chunk, target - ts);
+        for (int k = 0; k < n; k++)
+            if ((st = slab_group_one(slabs, nslabs, ts + k, 0))) return st;
+        // a stall stops every slab at the same activation, and the steps
+        // launched after it do nothing (their exchanges copy unchanged data)
+        int stl = 0;
+        uint64_t t = 0;
+        for (int s = 0; s < nslabs; s++) {
+            int x;
+            uint64_t ts_s;
+            if ((st = mms_slab_poll(slabs[s], &ts_s, &x))) return st;
+            if (s == 0) t = ts_s, stl = x;
+            if (ts_s != t || x != stl) {
+                slabs[s]->err = "slabs diverged";
+                return MMS_ERR_STATE;
+            }
+        }
+        if (stl) {
+            for (int s = 0; s < nslabs; s++)
+                if ((st = mms_slab_refill(slabs[s]))) return st;
+            if ((st = slab_group_one(slabs, nslabs, t, 1))) return st;
+            ts = t + 1;
+            continue;  // poll again before going on
+        }
+        ts = t;
+        for (int s = 0; s < nslabs; s++)
+            if ((st = refill_rng(slabs[s], false))) return st;
+    }
     return MMS_OK;
 }
 

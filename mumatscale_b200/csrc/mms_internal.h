@@ -43,12 +43,24 @@ enum StallReason : int {
 // One record per created grain (index = grain id), enough for the host to
 // rebuild grain_t (globals.h:244-254) for output_grains and mms_get_grains.
 struct GrainLog {
-    long long cell;       // global halo'd linear index of the nucleus cell
+    long long cell;       // device index of the nucleus cell; for a grain made by
+                          // another slab (kind | GL_REMOTE), its reference-layout
+                          // index in the whole domain
     unsigned long long timestep;
     int kind;             // 0 = deck site (nuc_pt entry), 1 = random draw, 2 = zero angles,
                           // 3 = pre-filled grain (mms_set_grains)
-    int rank;             // emulated rank that created it
+    int rank;             // emulated rank that created it (numbered over the whole domain)
     long long aux;        // nuc_pt entry index, or per-rank draw number
+    float thr;            // nucleation threshold of the site
+    int pad;
+};
+constexpr int GL_REMOTE = 8;
+
+// A new grain as one slab publishes it to the others (z-slab split of one
+// domain over several devices): its rotation and its record.
+struct SlabRow {
+    double rot[9];
+    GrainLog lg;
 };
 
 // Geometry and physics constants passed to every kernel by value.
@@ -65,7 +77,8 @@ struct Geo {
     int nsbx, nsby, nsbz;      // NSubblocks
     int nranks;
     long long sbcells;         // cells per subblock
-    int padx, pady, padz;      // pad (mold) faces
+    int padx, pady;            // pad (mold) faces
+    int padz_lo, padz_hi;      // z faces: pad, or (0) a neighbouring slab's plane
     // bitmasks: one bit per interior cell, rows of wpr 32-bit words,
     // bit b of word w in row (j,k) = cell i = 1 + 32 w + b
     int wpr;
@@ -109,6 +122,7 @@ struct Phys {
     double T0, cool_rate, gradient, grad_coef, velocity, velo_coef, ts_delt, cellSize;
     double origin[3];
     int gz_is_one;
+    int kz0;         // global z of interior plane 1 minus 1 (a slab's offset; 0 for a whole domain)
     int am, amlayer;
     int use_orientation;
     double cellSize3;
@@ -174,6 +188,15 @@ struct DevPtrs {
     // reductions
     double *red;            // scratch for partial sums
     Ctl *ctl;
+    // z-slab split of one domain (nslabs > 1): this slab's index, the
+    // whole-domain number of its first emulated rank, the capacity of its
+    // grain-row buffer; x1: per slab {candidates, short of draws} gathered
+    // before activation; x2: per slab its new grains, gathered after it
+    int nslabs, slab, rank0, slab_cap;
+    int *x1_send;           // 2
+    int *x1_recv;           // 2 x nslabs
+    SlabRow *x2_send;       // slab_cap
+    SlabRow *x2_recv;       // nslabs x slab_cap
     // frozen-CA record for the adjoint (null when not recording): per step
     // slot s (timestep rec_t0 + 1 + s), the fs_change branch of every cell
     // and, with TipCurvature, the curvature it used
@@ -233,6 +256,12 @@ int launch_stencil(const KernelArgs &a, const TmaHolder &tma, int precision, voi
 int launch_step_pre(const KernelArgs &a, int precision, void *stream, int start_stage);
 int launch_step_post(const KernelArgs &a, int precision, void *stream);
 int launch_curv(const KernelArgs &a, int precision, void *stream);
+// One slab of a z-slab split, in three parts around the two exchanges of a
+// step: phase 0 nucleation and the local half of activation (resume: only
+// the latter), phase 1 grain ids and the stencil, phase 2 the other slabs'
+// new grains, interface list and capture.
+int launch_slab_phase(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream, int phase,
+                      int resume);
 // Batched stencil over many domains: one item per domain (opaque, built by
 // fill_batch_item, which returns the domain's tile count), one persistent
 // launch of batch_grid CTAs.
