@@ -267,6 +267,8 @@ Geo make_geo(const mms_params &p)
     g.ppr = (p.gsdimx + 31) / 32;
     g.pieces_per_rank = (long long)p.gsdimy * p.gsdimz * g.ppr;
     g.blocks_per_rank = (g.pieces_per_rank + LIST_PIECES - 1) / LIST_PIECES;
+    g.ppr_m = div_magic((unsigned)g.ppr);
+    g.sby_m = div_magic((unsigned)g.sby);
     return g;
 }
 

@@ -1311,6 +1311,45 @@ __device__ __forceinline__ Piece piece_of(const KernelArgs &a, int r, long long 
     return pc;
 }
 
+// q / d and q % d for 32-bit q with m = floor(2^32 / d): the estimate
+// __umulhi(q, m) is the quotient or one less.
+__device__ __forceinline__ unsigned fast_divmod(unsigned q, unsigned d, unsigned m, unsigned &rem)
+{
+    unsigned k = __umulhi(q, m);
+    unsigned r = q - k * d;
+    if (r >= d) {
+        k++;
+        r -= d;
+    }
+    rem = r;
+    return k;
+}
+
+// piece_of for subblock rows that start on a bitmask word (sbx a multiple
+// of 32): seven aligned words per piece; (rx, ry, rz) is rank r's subblock.
+__device__ __forceinline__ Piece piece_aligned(const KernelArgs &a, int rx, int ry, int rz, long long q)
+{
+    const Geo &g = a.g;
+    Piece pc{0u, 0};
+    if (q >= g.pieces_per_rank) return pc;
+    unsigned part, ly;
+    const unsigned lr = fast_divmod((unsigned)q, (unsigned)g.ppr, g.ppr_m, part);
+    const unsigned lz = fast_divmod(lr, (unsigned)g.sby, g.sby_m, ly);
+    const long long J = (long long)ry * g.sby + ly + 1, K = (long long)rz * g.sbz + lz + 1;
+    const long long X0 = (long long)rx * g.sbx + 32LL * part;  // 0-based interior x, a multiple of 32
+    const long long wpr = g.wpr, plane = wpr * (g.gy + 2);
+    const long long w = X0 >> 5;
+    const unsigned *row = a.d.solid_bits + (K * (g.gy + 2) + J) * wpr + w;
+    const unsigned C = row[0];
+    const unsigned L = (w > 0) ? row[-1] : 0u;
+    const unsigned R = (w + 1 < wpr) ? row[1] : 0u;
+    const unsigned nb = ((C << 1) | (L >> 31)) | ((C >> 1) | (R << 31)) | row[wpr] | row[-wpr] | row[plane] |
+                        row[-plane];
+    pc.bits = ~C & nb;  // sbx - 32 part >= 32: all 32 cells belong to the piece
+    pc.base = K * g.sz + J * g.sy + X0 + 1;
+    return pc;
+}
+
 // Status word of a list block for the decoupled look-back: bits 34-63 the
 // step (low 30 bits of the timestep, so words of earlier steps never
 // match), bits 32-33 the state (1 = own count, 2 = inclusive prefix), bits
@@ -1366,10 +1405,19 @@ __device__ __forceinline__ void list_body(const KernelArgs &a, int nblocks)
     // piece it of this thread: q0 + it * LIST_NT + thread (neighbouring
     // threads read neighbouring bitmask words)
     unsigned bits[NI];
+    long long base[NI];
     int ex[NI], tot[NI], agg = 0;
+    const bool aligned = (g.sbx & 31) == 0;
+    const int rx = r % g.nsbx, ry = (r / g.nsbx) % g.nsby, rz = r / (g.nsbx * g.nsby);
 #pragma unroll
     for (int it = 0; it < NI; it++) {
-        bits[it] = piece_of(a, r, q0 + it * LIST_NT + threadIdx.x).bits;
+        const long long q = q0 + it * LIST_NT + threadIdx.x;
+        const Piece pc = aligned ? piece_aligned(a, rx, ry, rz, q) : piece_of(a, r, q);
+        bits[it] = pc.bits;
+        base[it] = pc.base;
+    }
+#pragma unroll
+    for (int it = 0; it < NI; it++) {
         ex[it] = block_exclusive_scan<LIST_NT>(__popc(bits[it]), tot[it], sh);
         agg += tot[it];
     }
@@ -1439,12 +1487,10 @@ __device__ __forceinline__ void list_body(const KernelArgs &a, int nblocks)
         int p0 = pos + ex[it];
         pos += tot[it];
         unsigned m = bits[it];
-        if (!m) continue;
-        const long long base = piece_of(a, r, q0 + it * LIST_NT + threadIdx.x).base;
         while (m) {
             const int bit = __ffs(m) - 1;
             m &= m - 1;
-            a.d.list_cell[p0++] = base + bit;
+            a.d.list_cell[p0++] = base[it] + bit;
         }
     }
 }
@@ -1474,19 +1520,28 @@ __device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs,
     // neighbour order +x, +y, -x, -y, +z, -z (growth.c:604-610, 674-677)
     const long long ndxs[6] = {c + 1, c + g.sy, c - 1, c - g.sy, c + g.sz, c - g.sz};
     const int nnx[6] = {1, 0, -1, 0, 0, 0}, nny[6] = {0, 1, 0, -1, 0, 0}, nnz[6] = {0, 0, 0, 0, 1, -1};
-    int found = -1, gid = 0;
+    int found = -1, gid = 0, fx = 0, fy = 0, fz = 0;
     double g00 = 0, g10 = 0, g20 = 0, g01 = 0, g11 = 0, g21 = 0, g02 = 0, g12 = 0, g22 = 0;
     double dx = 0, dy = 0, dz = 0, dn = 0;
     Dc3 dcn{0, 0, 0};
-#pragma unroll 1
+    // the six neighbours' pre-capture grain ids, their loads issued
+    // together: an interior neighbour counts only if its solid bit is set
+    // (a liquid neighbour's gr may be changing under a concurrent capture
+    // and is then discarded); a halo neighbour's gr is never written here
+    int ids[6];
+#pragma unroll
+    for (int n = 0; n < 6; n++) {
+        const long long In = I + nnx[n], Jn = J + nny[n], Kn = K + nnz[n];
+        const bool inside = In >= 1 && In <= g.gx && Jn >= 1 && Jn <= g.gy && Kn >= 1 && Kn <= g.gz;
+        unsigned w = 1u;
+        if (inside) w = a.d.solid_bits[(Kn * (g.gy + 2) + Jn) * (long long)g.wpr + ((In - 1) >> 5)] >> ((In - 1) & 31);
+        const int gv = *((volatile const int *)&gr[ndxs[n]]);
+        ids[n] = (w & 1u) ? gv : 0;
+    }
+#pragma unroll
     for (int n = 0; n < 6; n++) {
         long long ndx = ndxs[n];
-        const long long In = I + nnx[n], Jn = J + nny[n], Kn = K + nnz[n];
-        if (In >= 1 && In <= g.gx && Jn >= 1 && Jn <= g.gy && Kn >= 1 && Kn <= g.gz) {
-            const unsigned w = a.d.solid_bits[(Kn * (g.gy + 2) + Jn) * (long long)g.wpr + ((In - 1) >> 5)];
-            if (!((w >> ((In - 1) & 31)) & 1u)) continue;
-        }
-        int id = gr[ndx];
+        int id = ids[n];
         if (id > 0 && (unsigned long long)id < p.max_grains) {
             const double *R = a.d.grain_rot + 9 * (long long)id;
             g00 = R[0]; g01 = R[1]; g02 = R[2];
@@ -1509,6 +1564,9 @@ __device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs,
             double dfs = dn - (fabs(dx) + fabs(dy) + fabs(dz));
             if (dfs > 0) {
                 found = n;
+                fx = nnx[n];
+                fy = nny[n];
+                fz = nnz[n];
                 gid = id;
                 break;
             }
@@ -1524,9 +1582,9 @@ __device__ __forceinline__ int capture_cell(const KernelArgs &a, const Real *fs,
     else if (dy + dx < 0 && dy - dx <= 0 && dy + dz <= 0 && dy - dz < 0) ncy = -1. * dd;
     else if (dz + dx >= 0 && dz - dx > 0 && dz + dy > 0 && dz - dy >= 0) ncz = dd;
     else ncz = -1. * dd;
-    out.x = dcn.x + (double)nnx[found] + g00 * ncx + g01 * ncy + g02 * ncz;
-    out.y = dcn.y + (double)nny[found] + g10 * ncx + g11 * ncy + g12 * ncz;
-    out.z = dcn.z + (double)nnz[found] + g20 * ncx + g21 * ncy + g22 * ncz;
+    out.x = dcn.x + (double)fx + g00 * ncx + g01 * ncy + g02 * ncz;
+    out.y = dcn.y + (double)fy + g10 * ncx + g11 * ncy + g12 * ncz;
+    out.z = dcn.z + (double)fz + g20 * ncx + g21 * ncy + g22 * ncz;
     return gid;
 }
 
@@ -1583,7 +1641,7 @@ __device__ __forceinline__ void capture_body(const KernelArgs &a, int bid, int n
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(LIST_NT) k_capture(KernelArgs a)
+__global__ void __launch_bounds__(LIST_NT, 3) k_capture(KernelArgs a)
 {
     capture_body<Real>(a, blockIdx.x, gridDim.x);
 }

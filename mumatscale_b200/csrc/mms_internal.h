@@ -88,7 +88,12 @@ struct Geo {
     int ppr;                   // pieces per local row = ceil(sbx / 32)
     long long pieces_per_rank; // sby * sbz * ppr
     long long blocks_per_rank; // ceil(pieces_per_rank / LIST_PIECES)
+    // floor(2^32 / d) for d = ppr and d = sby (0xffffffff for d = 1): the
+    // quotient of a 32-bit q by d is __umulhi(q, m) or one more
+    unsigned ppr_m, sby_m;
 };
+
+inline unsigned div_magic(unsigned d) { return d <= 1 ? 0xffffffffu : (unsigned)((1ULL << 32) / d); }
 
 constexpr int LIST_PIECES = 1024;
 
