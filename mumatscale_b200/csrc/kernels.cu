@@ -1726,14 +1726,15 @@ __global__ void __launch_bounds__(RED_NT) k_reduce(KernelArgs a, int what, doubl
     const long long rows = (long long)g.gy * g.gz;
     double s = 0.0, comp = 0.0;
     auto add = [&](double x) {
-        if (what != MMS_REDUCE_CE_SUM) x = (1.0 < x) ? 1.0 : x;
         double t = s + x;                          // TwoSum
         double bp = t - s;
         comp += (s - (t - bp)) + (x - bp);
         s = t;
     };
     // a block per interior row at a time (four rows' loads in flight), the
-    // threads along x
+    // threads along x.  The four values a thread loads together are summed
+    // pairwise and the group enters the running sum with compensation (the
+    // FP64 pipe, not memory, bounded the kernel with one TwoSum per value).
     constexpr int U = 4;
     for (long long r0 = (long long)blockIdx.x * U; r0 < rows; r0 += (long long)gridDim.x * U) {
         const Real *row[U];
@@ -1746,10 +1747,12 @@ __global__ void __launch_bounds__(RED_NT) k_reduce(KernelArgs a, int what, doubl
         for (int i = 1 + (int)threadIdx.x; i <= g.gx; i += RED_NT) {
             double x[U];
 #pragma unroll
-            for (int u = 0; u < U; u++) x[u] = (double)row[u][i];
-#pragma unroll
-            for (int u = 0; u < U; u++)
-                if (r0 + u < rows) add(x[u]);
+            for (int u = 0; u < U; u++) {
+                double v = (double)row[u][i];
+                if (what != MMS_REDUCE_CE_SUM) v = (1.0 < v) ? 1.0 : v;
+                x[u] = (r0 + u < rows) ? v : 0.0;
+            }
+            add((x[0] + x[1]) + (x[2] + x[3]));
         }
     }
     __shared__ double ss[RED_NT], sc[RED_NT];
@@ -1849,6 +1852,35 @@ __global__ void k_convert(KernelArgs a, int field, int to_device, double *buf)
         if (f2) f2[c] = (Real)(buf[c] - off);
     } else {
         buf[c] = (double)f[c] + off;
+    }
+}
+
+// k_convert between a field and FP64 values in the reference's halo'd
+// layout (ref, row length gx + 2), one block per row of cells at a time.
+template <typename Real>
+__global__ void k_convert_ref(KernelArgs a, int field, int to_device, double *ref)
+{
+    const Ctl *ctl = a.d.ctl;
+    const Geo &g = a.g;
+    const int cur = (int)(ctl->timestep & 1ULL);
+    Real *f = nullptr, *f2 = nullptr;
+    if (field == MMS_FIELD_CE) f = (Real *)a.d.ce;
+    else if (field == MMS_FIELD_CL) f = (Real *)a.d.cl[cur], f2 = (Real *)a.d.cl[cur ^ 1];
+    else f = (Real *)a.d.fs[cur], f2 = (Real *)a.d.fs[cur ^ 1];
+    const double off = (sizeof(Real) == 4 && field != MMS_FIELD_FS) ? a.p.cinit : 0.0;
+    const long long rows = (long long)(g.gy + 2) * (g.gz + 2);
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        Real *fr = f + r * g.P, *fr2 = f2 ? f2 + r * g.P : nullptr;
+        double *rr = ref + r * g.rsy;
+        for (int i = threadIdx.x; i < g.rsy; i += blockDim.x) {
+            if (to_device) {
+                const Real v = (Real)(rr[i] - off);
+                fr[i] = v;
+                if (fr2) fr2[i] = v;
+            } else {
+                rr[i] = (double)fr[i] + off;
+            }
+        }
     }
 }
 
@@ -2286,6 +2318,16 @@ int launch_fill_temperature(const KernelArgs &a, double *dev_out, void *stream)
     cudaStream_t st = (cudaStream_t)stream;
     int nb = (int)((a.g.N + 255) / 256);
     k_fill_temperature<<<nb, 256, 0, st>>>(a, dev_out);
+    return 1;
+}
+
+int launch_convert_ref(const KernelArgs &a, int precision, int field, int to_device, double *ref_f64, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long rows = (long long)(a.g.gy + 2) * (a.g.gz + 2);
+    const int nb = (int)(rows < 148LL * 16 ? rows : 148LL * 16);
+    if (precision == MMS_PREC_F32) k_convert_ref<float><<<nb, 256, 0, st>>>(a, field, to_device, ref_f64);
+    else k_convert_ref<double><<<nb, 256, 0, st>>>(a, field, to_device, ref_f64);
     return 1;
 }
 

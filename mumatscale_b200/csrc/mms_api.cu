@@ -1269,11 +1269,11 @@ mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
             const void *src = field == MMS_FIELD_CE ? d.ce : (field == MMS_FIELD_CL ? d.cl[cur] : d.fs[cur]);
             CU(copy_out(ctx, host, src, sizeof(double)));
         } else {
-            double *tmp;
-            if ((st = dalloc(ctx, &tmp, N))) return st;
-            ctx->launches += launch_convert(ctx->ka, ctx->prec, field, 0, tmp, ctx->stream);
-            CU(copy_out(ctx, host, tmp, sizeof(double)));
-            dfree(ctx, tmp);
+            double *stg = (double *)stage_buffer(ctx, (size_t)g.rN * sizeof(double));
+            if (!stg) return MMS_ERR_NOMEM;
+            ctx->launches += launch_convert_ref(ctx->ka, ctx->prec, field, 0, stg, ctx->stream);
+            CU(cudaMemcpyAsync(host, stg, (size_t)g.rN * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            CU(cudaStreamSynchronize(ctx->stream));
         }
         return MMS_OK;
     }
@@ -1333,12 +1333,27 @@ mms_status mms_upload(mms_ctx *ctx, mms_field field, const void *host)
     case MMS_FIELD_CE:
     case MMS_FIELD_CL:
     case MMS_FIELD_FS: {
-        double *tmp;
-        if ((st = dalloc(ctx, &tmp, N))) return st;
-        CU(copy_in(ctx, tmp, host, sizeof(double)));
-        ctx->launches += launch_convert(ctx->ka, ctx->prec, field, 1, tmp, ctx->stream);
+        // cl and fs are written to both step buffers (the stencil writes
+        // only interior cells of its output buffer)
+        if ((st = read_ctl(ctx))) return st;
+        const int cur = (int)(ctx->h_ctl->timestep & 1ULL);
+        if (ctx->prec == MMS_PREC_F64) {
+            void *dst = field == MMS_FIELD_CE ? d.ce : (field == MMS_FIELD_CL ? d.cl[cur] : d.fs[cur]);
+            CU(copy_in(ctx, dst, host, sizeof(double)));
+            if (field != MMS_FIELD_CE) {
+                void *other = field == MMS_FIELD_CL ? d.cl[cur ^ 1] : d.fs[cur ^ 1];
+                CU(cudaMemcpyAsync(other, dst, N * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+                CU(cudaStreamSynchronize(ctx->stream));
+            }
+            return MMS_OK;
+        }
+        // FP32 form: the doubles land in the staging buffer and are
+        // converted from the reference layout on the device
+        double *stg = (double *)stage_buffer(ctx, (size_t)g.rN * sizeof(double));
+        if (!stg) return MMS_ERR_NOMEM;
+        CU(cudaMemcpyAsync(stg, host, (size_t)g.rN * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        ctx->launches += launch_convert_ref(ctx->ka, ctx->prec, field, 1, stg, ctx->stream);
         CU(cudaStreamSynchronize(ctx->stream));
-        dfree(ctx, tmp);
         return MMS_OK;
     }
     case MMS_FIELD_GR:

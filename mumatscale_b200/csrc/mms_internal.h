@@ -301,6 +301,8 @@ int launch_repack(void *dst, long long dst_pitch, const void *src, long long src
 int launch_mask_captured(const KernelArgs &a, void *dev, int is_double, void *stream);
 int launch_convert(const KernelArgs &a, int precision, int field, int to_device, double *dev_f64,
                    void *stream);
+// the same between the field and FP64 values in the reference layout
+int launch_convert_ref(const KernelArgs &a, int precision, int field, int to_device, double *ref_f64, void *stream);
 
 // Frozen-CA replay and adjoint (adjoint.cu).  x0/x1: (ce, cl, fs) of one
 // state; ts: the timestep of the step being replayed or differentiated.
