@@ -269,6 +269,30 @@ mms_status mms_write_vtk(mms_ctx *ctx, const char *base);
 /* The same files from caller arrays in the halo'd layout (host only). */
 mms_status mms_write_vtk_arrays(const mms_params *p, const char *base, int64_t timestep,
                                 const double *temperature, const int32_t *gr);
+/* XDMF output as xdmf_writeMain + xdmf_writeSubblocks (io_xdmf.c:141-673):
+ * <base>_ts.xmf, the time series of every write since the first one to this
+ * base; <base>_r<rank>/<ts>.raw per emulated rank (Temperature, CE as
+ * float32, Grain as int32, FracSolid as float32, each the subblock's interior
+ * with z slowest, in that order); <base>_gbl.raw (with RandomizeGrains the
+ * grain renumbering as uint64, then the grain angles X, Y, Z as float32).
+ * The reference writes these datasets with HDF5, which is absent here: the
+ * index addresses the raw files with Format="Binary" and Seek offsets.
+ * With RandomizeGrains, a write after the grain count grew draws a new
+ * renumbering from rank 0's rand() stream (getRenumberArray,
+ * io_xdmf.c:344-375), which shifts rank 0's later orientation draws exactly
+ * as in the reference.  base NULL: the deck's BaseFileName.  mms_run writes
+ * these (or VTK) itself for DataFormat XDMF (VTK) with DataWriteFreq > 0.
+ * Not on a slab of a split domain. */
+mms_status mms_write_xdmf(mms_ctx *ctx, const char *base);
+/* The files of one write from halo'd host arrays (reference layout): series
+ * lists the timesteps of the time series, the last being this write's;
+ * rotang [num_grains][3]; renumber NULL unless RandomizeGrains. */
+mms_status mms_write_xdmf_arrays(const mms_params *p, const char *base, const int64_t *series, int nseries,
+                                 const double *temperature, const double *ce, const int32_t *gr, const double *fs,
+                                 int num_grains, const double *rotang, const uint64_t *renumber);
+/* The grain renumbering of the last XDMF write (count entries; up to
+ * capacity copied to out). */
+mms_status mms_xdmf_renumbering(mms_ctx *ctx, int capacity, uint64_t *out, int *count);
 
 /* Raw checkpoint of a context (device layout, this library's format): every
  * array a later step reads, the grain table, the orientation tables and the

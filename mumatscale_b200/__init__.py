@@ -211,6 +211,9 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_batch_autotune": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(D)]),
         "mms_batch_kernel_launches": (C.c_uint64, [P]),
         "mms_batch_last_error": (C.c_char_p, [P]),
+        "mms_write_xdmf": (I, [P, C.c_char_p]),
+        "mms_write_xdmf_arrays": (I, [C.POINTER(Params), C.c_char_p, P, I, P, P, P, P, I, P, P]),
+        "mms_xdmf_renumbering": (I, [P, I, P, C.POINTER(I)]),
         "mms_slab_layout_of": (I, [C.POINTER(Params), I, I, C.POINTER(SlabLayout)]),
         "mms_slab_create": (I, [C.POINTER(Params), I, I, C.POINTER(P)]),
         "mms_slab_get_layout": (I, [P, C.POINTER(SlabLayout)]),
@@ -249,6 +252,22 @@ def write_vtk_arrays(params: Params, base: str, timestep: int, temperature: np.n
     g = np.ascontiguousarray(gr, dtype=np.int32)
     _check(_lib().mms_write_vtk_arrays(C.byref(params), base.encode(), timestep, t.ctypes.data, g.ctypes.data),
            "mms_write_vtk_arrays")
+
+
+def write_xdmf_arrays(params: Params, base: str, series, temperature: np.ndarray, ce: np.ndarray,
+                      gr: np.ndarray, fs: np.ndarray, rotang: np.ndarray, renumber: np.ndarray | None = None) -> None:
+    """XDMF files (io_xdmf.c layout, raw binary datasets) from halo'd host
+    arrays; series: the time series' timesteps, the last being this write's."""
+    ser = np.ascontiguousarray(series, dtype=np.int64)
+    t = np.ascontiguousarray(temperature, dtype=np.float64)
+    c = np.ascontiguousarray(ce, dtype=np.float64)
+    g = np.ascontiguousarray(gr, dtype=np.int32)
+    f = np.ascontiguousarray(fs, dtype=np.float64)
+    a = np.ascontiguousarray(rotang, dtype=np.float64).reshape(-1, 3)
+    r = None if renumber is None else np.ascontiguousarray(renumber, dtype=np.uint64)
+    _check(_lib().mms_write_xdmf_arrays(C.byref(params), base.encode(), ser.ctypes.data, len(ser), t.ctypes.data,
+                                        c.ctypes.data, g.ctypes.data, f.ctypes.data, len(a), a.ctypes.data,
+                                        None if r is None else r.ctypes.data), "mms_write_xdmf_arrays")
 
 
 def default_params() -> Params:
@@ -451,6 +470,20 @@ class Domain:
     def write_vtk(self, base: str | None = None) -> None:
         """<base>_<ts>.pvtu + <base>_<sbid>/<ts>.vtu (io_vtk.c layout)."""
         _check(_lib().mms_write_vtk(self._ctx, base.encode() if base else None), "mms_write_vtk", self._ctx)
+
+    def write_xdmf(self, base: str | None = None) -> None:
+        """<base>_ts.xmf + <base>_r<rank>/<ts>.raw + <base>_gbl.raw (io_xdmf.c
+        layout with raw binary datasets); with RandomizeGrains this draws the
+        grain renumbering from rank 0's stream as the reference does."""
+        _check(_lib().mms_write_xdmf(self._ctx, base.encode() if base else None), "mms_write_xdmf", self._ctx)
+
+    def xdmf_renumbering(self) -> np.ndarray:
+        n = C.c_int()
+        _check(_lib().mms_xdmf_renumbering(self._ctx, 0, None, C.byref(n)), "mms_xdmf_renumbering", self._ctx)
+        out = np.empty(n.value, dtype=np.uint64)
+        _check(_lib().mms_xdmf_renumbering(self._ctx, n.value, out.ctypes.data, C.byref(n)), "mms_xdmf_renumbering",
+               self._ctx)
+        return out
 
     def set_grains(self, rotmats: np.ndarray) -> None:
         """Grains 1..n of a pre-filled microstructure (row-major 3x3 rotations)."""

@@ -18,6 +18,38 @@ void Rank::seed_with(unsigned s)
     have_gauss = 0;
     gauss_next = 0.f;
 }
+namespace {
+// rd's pointers re-expressed against another copy of the state buffer
+void rebase(struct random_data &rd, const char *from, char *to)
+{
+    auto mv = [&](int32_t *q) { return q ? (int32_t *)(to + ((const char *)q - from)) : nullptr; };
+    rd.fptr = mv(rd.fptr);
+    rd.rptr = mv(rd.rptr);
+    rd.state = mv(rd.state);
+    rd.end_ptr = mv(rd.end_ptr);
+}
+}  // namespace
+
+void Rank::save(RngState &out) const
+{
+    std::memcpy(out.state, state, sizeof state);
+    out.rd = rd;
+    rebase(out.rd, state, out.state);
+    out.ncalls = ncalls;
+    out.have_gauss = have_gauss;
+    out.gauss_next = gauss_next;
+}
+
+void Rank::restore(const RngState &in)
+{
+    std::memcpy(state, in.state, sizeof state);
+    rd = in.rd;
+    rebase(rd, in.state, state);
+    ncalls = in.ncalls;
+    have_gauss = in.have_gauss;
+    gauss_next = in.gauss_next;
+}
+
 int32_t Rank::rand_()
 {
     int32_t v;

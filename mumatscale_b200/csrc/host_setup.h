@@ -25,6 +25,16 @@ struct NucPt {  // nucleation_t, globals.h:147-160
     double threshold;
 };
 
+// A copy of one rand() stream's position (the random_r state holds pointers
+// into its own buffer, so copies rebase them).
+struct RngState {
+    struct random_data rd;
+    char state[128];
+    long ncalls = 0;
+    int have_gauss = 0;
+    float gauss_next = 0.f;
+};
+
 struct Rank {
     struct random_data rd;
     char state[128];
@@ -39,6 +49,8 @@ struct Rank {
     long long rng_base = 0;                     // draw number of device table entry 0
 
     void seed_with(unsigned s);
+    void save(RngState &out) const;
+    void restore(const RngState &in);
     int32_t rand_();
     // getRandScale, functions.c:440-445
     float scale();

@@ -131,6 +131,15 @@ struct mms_ctx {
     mms_params gp{};
     Geo gg{};
     std::vector<cudaEvent_t> slab_events;  // mms_slab_group_step's ordering events
+    // XDMF output: rank 0's rand() stream where its first still-undrawn
+    // orientation begins (r0_snap_k draws after setup and any renumbering),
+    // the grain renumbering of the last write, the time series written
+    RngState r0_snap;
+    long long r0_snap_k = 0;
+    bool r0_snap_valid = false;
+    std::vector<uint64_t> renumber;
+    std::vector<int64_t> xdmf_series;
+    std::string xdmf_base;
     // frozen-CA record for the adjoint
     struct AdjRec {
         unsigned long long t0 = 0;
@@ -353,6 +362,12 @@ mms_status refill_rng(mms_ctx *ctx, bool force)
     std::vector<long long> base(g.nranks);
     for (int ri = 0; ri < g.nranks; ri++) {
         Rank &r = ctx->ranks[ctx->r0 + ri];
+        if (ctx->r0 + ri == 0 && !ctx->r0_snap_valid) {
+            // rank 0's stream before its first orientation draw
+            r.save(ctx->r0_snap);
+            ctx->r0_snap_k = (long long)r.angles.size();
+            ctx->r0_snap_valid = true;
+        }
         r.rng_base += used[ri];
         while ((long long)r.angles.size() < r.rng_base + d.rng_cap) {
             NucPt n{};
@@ -1128,6 +1143,7 @@ mms_status mms_set_sites(mms_ctx *ctx, int64_t n, const int32_t *gxyz, const flo
         r.angles.clear();
         r.rng_base = 0;
     }
+    ctx->r0_snap_valid = false;
     extract_sites(ctx, thr);
     mms_status st = upload_sites(ctx);
     if (st) return st;
@@ -1491,9 +1507,17 @@ mms_status mms_run(mms_ctx *ctx, int verbose)
     mms_status st;
     uint64_t ts = 0;
     if ((st = mms_get_timestep(ctx, &ts))) return st;
+    // data files as writeData (loop.c:116-128): VTK or XDMF, at the start,
+    // every DataWriteFreq steps from DataWriteStart, and at the end
+    const bool data = p.data_write_freq > 0 && (p.vis_format == 1 || p.vis_format == 2);
+    auto write_data = [&]() -> mms_status {
+        return p.vis_format == 1 ? mms_write_vtk(ctx, nullptr) : mms_write_xdmf(ctx, nullptr);
+    };
+    if (data && ts == 0 && (st = write_data())) return st;
     for (;;) {
         // run to the next screen step, or to FinishTime if that comes first
         uint64_t n = (p.screenpfreq > 0) ? (uint64_t)p.screenpfreq - (ts % (uint64_t)p.screenpfreq) : (1ULL << 30);
+        if (data) n = std::min<uint64_t>(n, (uint64_t)p.data_write_freq - (ts % (uint64_t)p.data_write_freq));
         if (p.finish_time) {
             // first t with t*ts_delt >= finish_time (checkDone, loop.c:155-156)
             uint64_t t = (uint64_t)std::floor(p.finish_time / p.ts_delt);
@@ -1505,6 +1529,9 @@ mms_status mms_run(mms_ctx *ctx, int verbose)
         if (n > (1ULL << 30)) n = 1ULL << 30;
         if ((st = mms_step(ctx, (int)n))) return st;
         ts += n;
+        if (data && ts >= (uint64_t)p.data_write_start && ts % (uint64_t)p.data_write_freq == 0 &&
+            (st = write_data()))
+            return st;
         if (p.screenpfreq > 0 && ts % (uint64_t)p.screenpfreq == 0) {
             if ((st = mms_reduce(ctx, MMS_REDUCE_FS_FRACTION, &fs))) return st;
             if (verbose) screen(fs);
@@ -1520,6 +1547,7 @@ mms_status mms_run(mms_ctx *ctx, int verbose)
         }
         if (done) break;
     }
+    if (data && ts % (uint64_t)p.data_write_freq != 0 && (st = write_data())) return st;
     mms_grain_summary s;
     char path[512];
     std::snprintf(path, sizeof path, "%s_grains.csv", p.basefilename);
@@ -2263,7 +2291,7 @@ mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path)
     const int cur = (int)(c.timestep & 1ULL);
     CkHeader h{};
     std::memcpy(h.magic, "MMSCKPT", 8);
-    h.version = 2;
+    h.version = 3;
     h.prec = ctx->prec;
     h.gx = g.gx;
     h.gy = g.gy;
@@ -2313,6 +2341,17 @@ mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path)
          fwrite_all(fp, ctx->site_rank.data(), ctx->site_rank.size() * sizeof(int)) &&
          fwrite_all(fp, ctx->inj_key.data(), ctx->inj_key.size() * sizeof(long long)) &&
          fwrite_all(fp, ctx->inj_rot.data(), ctx->inj_rot.size() * sizeof(double));
+    {
+        // XDMF state: rank 0's stream position before its undrawn
+        // orientations (as a call count) and the last grain renumbering
+        const int32_t sv = ctx->r0_snap_valid ? 1 : 0;
+        const int64_t nr = (int64_t)ctx->renumber.size();
+        ok = ok && fwrite_all(fp, &sv, sizeof sv) && fwrite_all(fp, &ctx->r0_snap_k, sizeof ctx->r0_snap_k) &&
+             fwrite_all(fp, &ctx->r0_snap.ncalls, sizeof ctx->r0_snap.ncalls) &&
+             fwrite_all(fp, &ctx->r0_snap.have_gauss, sizeof ctx->r0_snap.have_gauss) &&
+             fwrite_all(fp, &ctx->r0_snap.gauss_next, sizeof ctx->r0_snap.gauss_next) && fwrite_all(fp, &nr, sizeof nr) &&
+             fwrite_all(fp, ctx->renumber.data(), (size_t)nr * sizeof(uint64_t));
+    }
     if (std::fclose(fp) != 0) ok = false;
     return ok ? MMS_OK : MMS_ERR_IO;
 }
@@ -2335,7 +2374,7 @@ mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path)
         ctx->err = why;
         return s;
     };
-    if (!fread_all(fp, &h, sizeof h) || std::memcmp(h.magic, "MMSCKPT", 8) != 0 || h.version != 2)
+    if (!fread_all(fp, &h, sizeof h) || std::memcmp(h.magic, "MMSCKPT", 8) != 0 || h.version != 3)
         return fail(MMS_ERR_IO, "not a checkpoint of this library");
     if (h.prec != ctx->prec || h.gx != g.gx || h.gy != g.gy || h.gz != g.gz || h.nranks != g.nranks ||
         h.rng_cap != d.rng_cap || h.N != (int64_t)N || h.P != g.P ||
@@ -2394,6 +2433,30 @@ mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path)
          fread_all(fp, ctx->site_rank.data(), ctx->site_rank.size() * sizeof(int)) &&
          fread_all(fp, ctx->inj_key.data(), ctx->inj_key.size() * sizeof(long long)) &&
          fread_all(fp, ctx->inj_rot.data(), ctx->inj_rot.size() * sizeof(double));
+    {
+        int32_t sv = 0;
+        int64_t nr = 0;
+        long snap_calls = 0;
+        int hg = 0;
+        float gn = 0.f;
+        ok = ok && fread_all(fp, &sv, sizeof sv) && fread_all(fp, &ctx->r0_snap_k, sizeof ctx->r0_snap_k) &&
+             fread_all(fp, &snap_calls, sizeof snap_calls) && fread_all(fp, &hg, sizeof hg) &&
+             fread_all(fp, &gn, sizeof gn) && fread_all(fp, &nr, sizeof nr) && nr >= 0;
+        if (ok) {
+            ctx->renumber.resize((size_t)nr);
+            ok = fread_all(fp, ctx->renumber.data(), (size_t)nr * sizeof(uint64_t));
+        }
+        ctx->r0_snap_valid = ok && sv && !ctx->ranks.empty();
+        if (ctx->r0_snap_valid) {
+            // the stream position by replay from the seed
+            Rank tmp;
+            tmp.seed_with(ctx->ranks[0].seed);
+            while (tmp.ncalls < snap_calls) tmp.rand_();
+            tmp.have_gauss = hg;
+            tmp.gauss_next = gn;
+            tmp.save(ctx->r0_snap);
+        }
+    }
     std::fclose(fp);
     if (!ok) {
         ctx->err = "truncated checkpoint";
@@ -2704,6 +2767,102 @@ mms_status mms_slab_group_step(mms_ctx *const *slabs, int nslabs, int nsteps)
         for (int s = 0; s < nslabs; s++)
             if ((st = refill_rng(slabs[s], false))) return st;
     }
+    return MMS_OK;
+}
+
+}  // extern "C"
+
+// ===================================================================== XDMF
+namespace {
+
+// getRenumberArray (io_xdmf.c:344-375): when the grain count has grown since
+// the last renumbering, a fresh shuffle of the ids 1..n-1 drawn from rank
+// 0's rand() stream.  Those draws come at the point the run has reached on
+// that stream: after its setup draws and the orientation draws consumed so
+// far.  Rank 0's later orientations therefore follow them, so its
+// pre-drawn orientation table is redrawn from there.
+mms_status xdmf_renumber(mms_ctx *ctx)
+{
+    const int ng = ctx->h_ctl->num_grains;
+    if (!ctx->renumber.empty() && (size_t)ng <= ctx->renumber.size()) return MMS_OK;
+    Rank &r = ctx->ranks[0];
+    const DevPtrs &d = ctx->ka.d;
+    long long k = 0;  // orientation draws rank 0 has consumed
+    if (ctx->p.gnUseOrientation && d.rng_used) {
+        int used0 = 0;
+        CU(d2h(ctx, &used0, d.rng_used, sizeof(int)));
+        k = r.rng_base + used0;
+    }
+    if (ctx->r0_snap_valid) {
+        r.restore(ctx->r0_snap);
+        for (long long i = ctx->r0_snap_k; i < k; i++) {
+            NucPt n{};
+            draw_orientation(ctx->p, r, n);
+        }
+    } else if (k != 0) {
+        ctx->err = "rank 0's stream position is unknown";
+        return MMS_ERR_STATE;
+    }
+    std::vector<uint64_t> a((size_t)ng);
+    for (int i = 0; i < ng; i++) a[i] = (uint64_t)i;
+    for (int i = 1; i < ng; i++) {
+        int pic;
+        do {
+            pic = r.rand_() % ng;
+        } while (pic == 0);
+        std::swap(a[pic], a[i]);
+    }
+    ctx->renumber.swap(a);
+    r.save(ctx->r0_snap);
+    ctx->r0_snap_k = k;
+    ctx->r0_snap_valid = true;
+    if (ctx->p.gnUseOrientation && d.rng_used) {
+        r.angles.resize((size_t)k);
+        return refill_rng(ctx, true);
+    }
+    return MMS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mms_status mms_write_xdmf(mms_ctx *ctx, const char *basename)
+{
+    if (!ctx || ctx->nslabs > 1) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    const mms_params &p = ctx->p;
+    const size_t n = (size_t)ctx->ka.g.rN;
+    std::vector<double> T(n), ce(n), fs(n);
+    std::vector<int32_t> gr(n);
+    mms_status st;
+    if ((st = mms_download(ctx, MMS_FIELD_TEMPERATURE, T.data())) || (st = mms_download(ctx, MMS_FIELD_CE, ce.data())) ||
+        (st = mms_download(ctx, MMS_FIELD_GR, gr.data())) || (st = mms_download(ctx, MMS_FIELD_FS, fs.data())) ||
+        (st = sync_grains(ctx)))
+        return st;
+    const int ng = ctx->h_ctl->num_grains;
+    std::vector<double> ang((size_t)ng * 3);
+    for (int i = 0; i < ng; i++)
+        for (int a = 0; a < 3; a++) ang[3 * (size_t)i + a] = ctx->grains[i].rotang[a];
+    if (p.randomize_grains && (st = xdmf_renumber(ctx))) return st;
+    const std::string base = basename ? basename : p.basefilename;
+    const int64_t ts = (int64_t)ctx->h_ctl->timestep;
+    if (base != ctx->xdmf_base) {
+        ctx->xdmf_base = base;
+        ctx->xdmf_series.clear();
+    }
+    if (ctx->xdmf_series.empty() || ctx->xdmf_series.back() != ts) ctx->xdmf_series.push_back(ts);
+    return mms_write_xdmf_arrays(&p, base.c_str(), ctx->xdmf_series.data(), (int)ctx->xdmf_series.size(), T.data(),
+                                 ce.data(), gr.data(), fs.data(), ng, ang.data(),
+                                 p.randomize_grains ? ctx->renumber.data() : nullptr);
+}
+
+mms_status mms_xdmf_renumbering(mms_ctx *ctx, int capacity, uint64_t *out, int *count)
+{
+    if (!ctx || !count || capacity < 0 || (capacity && !out)) return MMS_ERR_ARG;
+    *count = (int)ctx->renumber.size();
+    std::copy(ctx->renumber.begin(), ctx->renumber.begin() + std::min<size_t>(ctx->renumber.size(), (size_t)capacity),
+              out);
     return MMS_OK;
 }
 

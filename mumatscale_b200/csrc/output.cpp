@@ -146,3 +146,226 @@ extern "C" mms_status mms_write_vtk(mms_ctx *ctx, const char *basename)
     if ((st = mms_get_timestep(ctx, &ts))) return st;
     return mms_write_vtk_arrays(&p, basename ? basename : p.basefilename, (int64_t)ts, T.data(), gr.data());
 }
+
+// ------------------------------------------------------------------- XDMF
+// The reference's XDMF output (io_xdmf.c): a time-series index
+// <base>_ts.xmf (writeXDMFTimeSeries, io_xdmf.c:483-497, grids as
+// writeXDMFGrids, io_xdmf.c:141-305, global items as writeGlobalData,
+// io_xdmf.c:378-404), per-rank heavy data <base>_r<rank>/<ts>.raw
+// (xdmf_writeSubblocks, io_xdmf.c:561-673: Temperature, CE, Grain,
+// FracSolid of the subblock's interior, float32 / int32, z slowest) and the
+// global grain data <base>_gbl.raw (writeGlobalHeavyData, io_xdmf.c:408-468:
+// GrainRenumber as uint64 when RandomizeGrains, then GrainAngleX/Y/Z as
+// float32).  libhdf5 is absent, so each dataset is a little-endian block of
+// a raw file that the index addresses with Format="Binary" and a Seek
+// offset; the index states each block's true number type (the reference's
+// index says Precision 8 for datasets it writes as float32).
+namespace {
+
+std::string local_name(const std::string &base)
+{
+    const size_t k = base.rfind('/');
+    return k == std::string::npos ? base : base.substr(k + 1);
+}
+
+std::string rank_file(const std::string &base, int rank, long long ts)
+{
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "_r%d/%05lld.raw", rank, ts);
+    return base + buf;
+}
+
+bool write_all(FILE *fp, const void *p, size_t n) { return n == 0 || std::fwrite(p, 1, n, fp) == n; }
+
+// one subblock's interior of the global halo'd arrays, as the four blocks
+bool write_rank_raw(const mms_params &p, const std::string &base, long long ts, int s, const double *T,
+                    const double *ce, const int32_t *gr, const double *fs)
+{
+    const int dimx = p.gsdimx, dimy = p.gsdimy, dimz = p.gsdimz;
+    const int sx = s % p.gnsbx, sy = (s / p.gnsbx) % p.gnsby, sz = s / (p.gnsbx * p.gnsby);
+    const long long gx = (long long)p.gnsbx * dimx, gy = (long long)p.gnsby * dimy;
+    const long long rsy = gx + 2, rsz = rsy * (gy + 2);
+    char dir[600];
+    std::snprintf(dir, sizeof dir, "%s_r%d", base.c_str(), s);
+    if (mkdir(dir, 0755) != 0 && errno != EEXIST) return false;
+    FILE *fp = std::fopen(rank_file(base, s, ts).c_str(), "wb");
+    if (!fp) return false;
+    const size_t n = (size_t)dimx * dimy * dimz;
+    std::vector<float> f(n);
+    std::vector<int32_t> g(n);
+    auto each = [&](auto fn) {
+        size_t q = 0;
+        for (int k = 1; k <= dimz; k++)
+            for (int j = 1; j <= dimy; j++)
+                for (int i = 1; i <= dimx; i++, q++)
+                    fn(q, (long long)(sz * dimz + k) * rsz + (long long)(sy * dimy + j) * rsy + (sx * dimx + i));
+    };
+    bool ok = true;
+    each([&](size_t q, long long c) { f[q] = (float)T[c]; });
+    ok = ok && write_all(fp, f.data(), n * sizeof(float));
+    each([&](size_t q, long long c) { f[q] = (float)ce[c]; });
+    ok = ok && write_all(fp, f.data(), n * sizeof(float));
+    each([&](size_t q, long long c) { g[q] = gr[c]; });
+    ok = ok && write_all(fp, g.data(), n * sizeof(int32_t));
+    each([&](size_t q, long long c) { f[q] = (float)fs[c]; });
+    ok = ok && write_all(fp, f.data(), n * sizeof(float));
+    return (std::fclose(fp) == 0) && ok;
+}
+
+bool write_global_raw(const std::string &base, int ng, const double *rotang, const uint64_t *renumber)
+{
+    FILE *fp = std::fopen((base + "_gbl.raw").c_str(), "wb");
+    if (!fp) return false;
+    bool ok = true;
+    if (renumber) ok = write_all(fp, renumber, (size_t)ng * sizeof(uint64_t));
+    std::vector<float> a((size_t)ng);
+    for (int d = 0; d < 3 && ok; d++) {
+        for (int i = 0; i < ng; i++) a[i] = (float)rotang[3 * (size_t)i + d];
+        ok = write_all(fp, a.data(), a.size() * sizeof(float));
+    }
+    return (std::fclose(fp) == 0) && ok;
+}
+
+void xmf_block(FILE *fp, const char *ind, const char *type, int prec, long long seek, const mms_params &p,
+               const std::string &file)
+{
+    std::fprintf(fp,
+                 "%s<DataItem Format=\"Binary\" Endian=\"Little\" Seek=\"%lld\" NumberType=\"%s\" Precision=\"%d\" "
+                 "Dimensions=\"%d %d %d\">\n",
+                 ind, seek, type, prec, p.gsdimz, p.gsdimy, p.gsdimx);
+    std::fprintf(fp, "%s\t%s\n", ind, file.c_str());
+    std::fprintf(fp, "%s</DataItem>\n", ind);
+}
+
+void xmf_grids(FILE *fp, const mms_params &p, const std::string &lbase, long long ts, bool renumber)
+{
+    const char *ind = "\t\t\t";
+    const double t = (double)ts * p.ts_delt;
+    const long long n = (long long)p.gsdimx * p.gsdimy * p.gsdimz;
+    std::fprintf(fp, "%s<Grid Name=\"Full Volume at time %g\" GridType=\"Collection\" CollectionType=\"Spatial\">\n",
+                 ind, t);
+    std::fprintf(fp, "%s\t<Time Value=\"%g\" />\n", ind, t);
+    const int nsub = p.gnsbx * p.gnsby * p.gnsbz;
+    for (int s = 0; s < nsub; s++) {
+        const int cx = s % p.gnsbx, cy = (s / p.gnsbx) % p.gnsby, cz = s / (p.gnsbx * p.gnsby);
+        const std::string file = rank_file(lbase, s, ts);
+        std::fprintf(fp, "%s\t<Grid Name=\"SubBlock %dx%dx%d (%d)\" GridType=\"Uniform\">\n", ind, cx, cy, cz, s);
+        std::fprintf(fp, "%s\t\t<Topology TopologyType=\"3DCoRectMesh\" Dimensions=\"%u %u %u\" />\n", ind,
+                     p.gsdimz + 1, p.gsdimy + 1, p.gsdimx + 1);
+        std::fprintf(fp, "%s\t\t<Geometry GeometryType=\"ORIGIN_DXDYDZ\">\n", ind);
+        std::fprintf(fp, "%s\t\t\t<DataItem Format=\"XML\" Dimensions=\"3\">\n", ind);
+        // getSBRealBounds (functions.c:153-173): the subblock's first cell
+        // centre less half a cell, printed z y x
+        const double rx = real_coord(p, 0, (long long)cx * p.gsdimx) - p.cellSize / 2.0;
+        const double ry = real_coord(p, 1, (long long)cy * p.gsdimy) - p.cellSize / 2.0;
+        const double rz = real_coord(p, 2, (long long)cz * p.gsdimz) - p.cellSize / 2.0;
+        std::fprintf(fp, "%s\t\t\t\t%e %e %e\n", ind, rz, ry, rx);
+        std::fprintf(fp, "%s\t\t\t</DataItem>\n", ind);
+        std::fprintf(fp, "%s\t\t\t<DataItem Format=\"XML\" Dimensions=\"3\">\n", ind);
+        std::fprintf(fp, "%s\t\t\t\t%e %e %e\n", ind, p.cellSize, p.cellSize, p.cellSize);
+        std::fprintf(fp, "%s\t\t\t</DataItem>\n", ind);
+        std::fprintf(fp, "%s\t\t</Geometry>\n", ind);
+        const std::string a = std::string(ind) + "\t\t\t";
+        std::fprintf(fp, "%s\t\t<Attribute Name=\"Temperature\" Center=\"Cell\">\n", ind);
+        xmf_block(fp, a.c_str(), "Float", 4, 0, p, file);
+        std::fprintf(fp, "%s\t\t</Attribute>\n", ind);
+        std::fprintf(fp, "%s\t\t<Attribute Name=\"Solute Composition\" Center=\"Cell\">\n", ind);
+        xmf_block(fp, a.c_str(), "Float", 4, 4 * n, p, file);
+        std::fprintf(fp, "%s\t\t</Attribute>\n", ind);
+        std::fprintf(fp, "%s\t\t<Attribute Name=\"Grain\" Center=\"Cell\">\n", ind);
+        const std::string a2 = a + "\t";
+        if (renumber) {
+            std::fprintf(fp,
+                         "%s<DataItem ItemType=\"Function\" NumberType=\"UInt\" Dimensions=\"%u %u %u\" "
+                         "Function=\"$0[$1]\">\n",
+                         a.c_str(), p.gsdimz, p.gsdimy, p.gsdimx);
+            std::fprintf(fp, "%s<DataItem Reference=\"XML\" Dimensions=\"%u %u %u\">\n", a2.c_str(), p.gsdimz, p.gsdimy,
+                         p.gsdimx);
+            std::fprintf(fp, "%s\t/Xdmf/Domain/DataItem[@Name=\"Grain Renumber\"]\n", a2.c_str());
+            std::fprintf(fp, "%s</DataItem>\n", a2.c_str());
+            xmf_block(fp, a2.c_str(), "Int", 4, 8 * n, p, file);
+            std::fprintf(fp, "%s</DataItem>\n", a.c_str());
+        } else {
+            xmf_block(fp, a.c_str(), "Int", 4, 8 * n, p, file);
+        }
+        std::fprintf(fp, "%s\t\t</Attribute>\n", ind);
+        std::fprintf(fp, "%s\t\t<Attribute Name=\"Grain Angle\" Center=\"Cell\" AttributeType=\"Vector\">\n", ind);
+        std::fprintf(fp,
+                     "%s<DataItem ItemType=\"Function\" NumberType=\"Float\" Dimensions=\"%u %u %u 3\" "
+                     "Function=\"$1[$0], $2[$0], $3[$0]\">\n",
+                     a.c_str(), p.gsdimz, p.gsdimy, p.gsdimx);
+        xmf_block(fp, a2.c_str(), "Int", 4, 8 * n, p, file);
+        for (char d : {'X', 'Y', 'Z'}) {
+            std::fprintf(fp, "%s<DataItem Reference=\"XML\" Dimensions=\"%u %u %u\">\n", a2.c_str(), p.gsdimz, p.gsdimy,
+                         p.gsdimx);
+            std::fprintf(fp, "%s\t/Xdmf/Domain/DataItem[@Name=\"Grain Angle %c\"]\n", a2.c_str(), d);
+            std::fprintf(fp, "%s</DataItem>\n", a2.c_str());
+        }
+        std::fprintf(fp, "%s</DataItem>\n", a.c_str());
+        std::fprintf(fp, "%s\t\t</Attribute>\n", ind);
+        std::fprintf(fp, "%s\t\t<Attribute Name=\"Fraction Solid\" Center=\"Cell\">\n", ind);
+        xmf_block(fp, a.c_str(), "Float", 4, 12 * n, p, file);
+        std::fprintf(fp, "%s\t\t</Attribute>\n", ind);
+        std::fprintf(fp, "%s\t</Grid>\n", ind);
+    }
+    std::fprintf(fp, "%s</Grid>\n", ind);
+}
+
+bool write_xmf(const mms_params &p, const std::string &base, const int64_t *series, int nseries, int ng,
+               bool renumber)
+{
+    FILE *fp = std::fopen((base + "_ts.xmf").c_str(), "w");
+    if (!fp) return false;
+    const std::string lbase = local_name(base);
+    std::fprintf(fp, "<?xml version=\"1.0\" ?>\n");
+    std::fprintf(fp, "<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n");
+    std::fprintf(fp, "<Xdmf xmlns:xi=\"http://www.w3.org/2001/XInclude\" Version=\"2.0\">\n");
+    std::fprintf(fp, "\t<Domain>\n");
+    std::fprintf(fp, "\t\t<Information Name=\"Description\">\n");
+    std::fprintf(fp, "\t\t\tSimulation time series data\n");
+    std::fprintf(fp, "\t\t</Information>\n");
+    std::fprintf(fp, "\t\t<Grid Name=\"Time Series\" GridType=\"Collection\" CollectionType=\"Temporal\">\n");
+    for (int i = 0; i < nseries; i++) xmf_grids(fp, p, lbase, (long long)series[i], renumber);
+    std::fprintf(fp, "\t\t</Grid>\n");
+    const std::string gfile = lbase + "_gbl.raw";
+    long long off = 0;
+    if (renumber) {
+        std::fprintf(fp,
+                     "\t\t<DataItem Name=\"Grain Renumber\" Format=\"Binary\" Endian=\"Little\" Seek=\"0\" "
+                     "Dimensions=\"%d\" NumberType=\"UInt\" Precision=\"8\">\n",
+                     ng);
+        std::fprintf(fp, "\t\t\t%s\n\t\t</DataItem>\n", gfile.c_str());
+        off = 8LL * ng;
+    }
+    for (char d : {'X', 'Y', 'Z'}) {
+        std::fprintf(fp,
+                     "\t\t<DataItem Name=\"Grain Angle %c\" Format=\"Binary\" Endian=\"Little\" Seek=\"%lld\" "
+                     "Dimensions=\"%d\" NumberType=\"Float\" Precision=\"4\">\n",
+                     d, off, ng);
+        std::fprintf(fp, "\t\t\t%s\n\t\t</DataItem>\n", gfile.c_str());
+        off += 4LL * ng;
+    }
+    std::fprintf(fp, "\t</Domain>\n");
+    std::fprintf(fp, "</Xdmf>\n");
+    return std::fclose(fp) == 0;
+}
+
+}  // namespace
+
+extern "C" mms_status mms_write_xdmf_arrays(const mms_params *p, const char *basename, const int64_t *series,
+                                            int nseries, const double *temperature, const double *ce,
+                                            const int32_t *gr, const double *fs, int num_grains,
+                                            const double *rotang, const uint64_t *renumber)
+{
+    if (!p || !basename || !series || nseries < 1 || !temperature || !ce || !gr || !fs || num_grains < 1 ||
+        !rotang)
+        return MMS_ERR_ARG;
+    const std::string base(basename);
+    const long long ts = (long long)series[nseries - 1];
+    const int nsub = p->gnsbx * p->gnsby * p->gnsbz;
+    for (int s = 0; s < nsub; s++)
+        if (!write_rank_raw(*p, base, ts, s, temperature, ce, gr, fs)) return MMS_ERR_IO;
+    if (!write_global_raw(base, num_grains, rotang, renumber)) return MMS_ERR_IO;
+    if (!write_xmf(*p, base, series, nseries, num_grains, renumber != nullptr)) return MMS_ERR_IO;
+    return MMS_OK;
+}

@@ -90,6 +90,8 @@ struct mmso {
     long ninj;
     int warned;
     int stepped;
+    uint64_t *renum;    /* grain renumbering of the last XDMF write */
+    int renum_n;
 };
 
 /* ---------------------------------------------------------------- RNG ---- */
@@ -566,7 +568,7 @@ void mmso_destroy(mmso *o)
     if (!o) return;
     free(o->ce); free(o->oce); free(o->cl); free(o->fs); free(o->d); free(o->T);
     free(o->curv); free(o->dc); free(o->gr); free(o->ogr); free(o->lsindex);
-    free(o->thr); free(o->mold); free(o->grains); free(o->inj_idx); free(o->inj_rot);
+    free(o->thr); free(o->mold); free(o->grains); free(o->inj_idx); free(o->inj_rot); free(o->renum);
     for (int r = 0; r < o->nranks; r++) {
         free(o->ranks[r].nuc);
         free(o->ranks[r].list);
@@ -1295,4 +1297,31 @@ int mmso_run(mmso *o, int verbose)
                s.min_mm3, s.max_mm3, s.avg_mm3);
     }
     return MMS_OK;
+}
+
+/* getRenumberArray (io_xdmf.c:344-375), called by the reference's XDMF
+ * writer on rank 0 with RandomizeGrains: when the grain count has grown
+ * since the last call, a fresh shuffle of ids 1..n-1 drawn from rank 0's
+ * rand() stream, which its later orientation draws then follow.  Returns
+ * the renumbering's length; up to cap entries go to out. */
+int mmso_xdmf_renumber(mmso *o, uint64_t *out, int cap)
+{
+    const int ng = o->num_grains;
+    if (!o->renum || ng > o->renum_n) {
+        free(o->renum);
+        o->renum = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)ng);
+        for (int i = 0; i < ng; i++) o->renum[i] = (uint64_t)i;
+        for (int i = 1; i < ng; i++) {
+            int pic;
+            do {
+                pic = rng_rand(&o->ranks[0]) % ng;
+            } while (pic == 0);
+            uint64_t t = o->renum[pic];
+            o->renum[pic] = o->renum[i];
+            o->renum[i] = t;
+        }
+        o->renum_n = ng;
+    }
+    for (int i = 0; i < cap && i < o->renum_n; i++) out[i] = o->renum[i];
+    return o->renum_n;
 }

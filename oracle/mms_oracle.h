@@ -37,6 +37,8 @@ double mmso_reduce(mmso *o, int what);
 void mmso_get_grains(mmso *o, int first, int count, mms_grain *out);
 void mmso_grain_summary(mmso *o, mms_grain_summary *s);
 int mmso_run(mmso *o, int verbose);
+/* the reference XDMF writer's grain renumbering on rank 0's stream */
+int mmso_xdmf_renumber(mmso *o, uint64_t *out, int cap);
 /* glibc rand() replay check: n values of srand(seed) + rand() */
 void mmso_rand_sequence(unsigned seed, int n, int32_t *out);
 

@@ -49,6 +49,7 @@ def load():
     lib.mmso_grain_summary.argtypes = [P, C.POINTER(GrainSummary)]
     lib.mmso_run.argtypes = [P, C.c_int]
     lib.mmso_rand_sequence.argtypes = [C.c_uint, C.c_int, P]
+    lib.mmso_xdmf_renumber.argtypes = [P, P, C.c_int]
     _LIB = lib
     return lib
 
@@ -132,6 +133,13 @@ class Oracle:
         load().mmso_get_field(self._o, f, out.ctypes.data)
         nx, ny, nz = self.shape
         return out.reshape((nz, ny, nx, comp) if comp > 1 else (nz, ny, nx))
+
+    def xdmf_renumber(self) -> np.ndarray:
+        """The reference XDMF writer's grain renumbering (rank 0's stream)."""
+        n = load().mmso_xdmf_renumber(self._o, None, 0)
+        out = np.empty(n, dtype=np.uint64)
+        load().mmso_xdmf_renumber(self._o, out.ctypes.data, n)
+        return out
 
     def reduce(self, what="fs_fraction"):
         return float(load().mmso_reduce(self._o, {"fs_fraction": 0, "solid_volume": 1, "ce_sum": 2}[what]))

@@ -6,8 +6,11 @@ import xml.etree.ElementTree as ET
 import numpy as np
 import pytest
 
+from pathlib import Path
+
 import mumatscale_b200 as M
 from conftest import golden_deck
+from digests import mismatches, state_digests
 
 
 def _arr(piece, name):
@@ -67,3 +70,151 @@ def test_vtk_from_device(built, cuda_device, tmp_path):
         grain = np.array(_arr(piece, "Grain").text.split(), dtype=int)
         gr = dom.download("gr")[1:-1, 1:-1, 1:-1]
         assert np.array_equal(grain, np.transpose(gr, (2, 1, 0)).ravel())
+
+
+# ---------------------------------------------------------------- XDMF
+def _xdmf_item(d: Path, item) -> np.ndarray:
+    """A Format="Binary" DataItem of the index, read from its raw file."""
+    dt = {("Float", "4"): "<f4", ("Int", "4"): "<i4", ("UInt", "8"): "<u8"}[(item.get("NumberType"),
+                                                                          item.get("Precision"))]
+    dims = tuple(int(x) for x in item.get("Dimensions").split())
+    n = int(np.prod(dims))
+    return np.fromfile(d / item.text.strip(), dtype=dt, count=n, offset=int(item.get("Seek"))).reshape(dims)
+
+
+def _check_xdmf(tmp: Path, base: str, p, series, fields, rotang, renumber):
+    """Index structure (io_xdmf.c:141-305, 378-404) and every dataset against
+    the halo'd arrays it was written from (fields: name -> [z, y, x])."""
+    import xml.etree.ElementTree as ET
+    root = ET.parse(tmp / f"{base}_ts.xmf").getroot()
+    dom = root.find("Domain")
+    series_grid = dom.find("Grid")
+    assert series_grid.get("CollectionType") == "Temporal"
+    grids = series_grid.findall("Grid")
+    assert len(grids) == len(series)
+    nsub = p.gnsbx * p.gnsby * p.gnsbz
+    sd = (p.gsdimz, p.gsdimy, p.gsdimx)
+    glob = {it.get("Name"): it for it in dom.findall("DataItem")}
+    for d, ax in enumerate("XYZ"):
+        np.testing.assert_array_equal(_xdmf_item(tmp, glob[f"Grain Angle {ax}"]),
+                                      rotang[:, d].astype(np.float32))
+    if renumber is not None:
+        np.testing.assert_array_equal(_xdmf_item(tmp, glob["Grain Renumber"]), renumber)
+    else:
+        assert "Grain Renumber" not in glob
+    last = grids[-1]
+    assert float(last.find("Time").get("Value")) == pytest.approx(series[-1] * p.ts_delt)
+    blocks = last.findall("Grid")
+    assert len(blocks) == nsub
+    for s, g in enumerate(blocks):
+        cx, cy, cz = s % p.gnsbx, (s // p.gnsbx) % p.gnsby, s // (p.gnsbx * p.gnsby)
+        assert g.get("Name") == f"SubBlock {cx}x{cy}x{cz} ({s})"
+        assert g.find("Topology").get("Dimensions") == f"{sd[0] + 1} {sd[1] + 1} {sd[2] + 1}"
+        origin = [float(v) for v in g.find("Geometry").findall("DataItem")[0].text.split()]
+        want = [p.origin_offset[2] + cz * sd[0] * p.cellSize, p.origin_offset[1] + cy * sd[1] * p.cellSize,
+                p.origin_offset[0] + cx * sd[2] * p.cellSize]
+        assert origin == pytest.approx(want, rel=1e-5, abs=1e-12)
+        sl = (slice(cz * sd[0] + 1, (cz + 1) * sd[0] + 1), slice(cy * sd[1] + 1, (cy + 1) * sd[1] + 1),
+              slice(cx * sd[2] + 1, (cx + 1) * sd[2] + 1))
+        att = {a.get("Name"): a for a in g.findall("Attribute")}
+        for name, key, dt in (("Temperature", "temperature", np.float32), ("Solute Composition", "ce", np.float32),
+                              ("Fraction Solid", "fs", np.float32)):
+            np.testing.assert_array_equal(_xdmf_item(tmp, att[name].find("DataItem")), fields[key][sl].astype(dt))
+        grain_item = att["Grain"].find(".//DataItem[@Format='Binary']")
+        np.testing.assert_array_equal(_xdmf_item(tmp, grain_item), fields["gr"][sl])
+        fn = att["Grain"].find("DataItem")
+        assert (fn.get("ItemType") == "Function") == (renumber is not None)
+
+
+def test_xdmf_arrays_layout(built, tmp_path):
+    """Two writes of a 2 x 1 x 2 subblock deck from host arrays: the index
+    lists both timesteps; every dataset of the second one reads back."""
+    p = M.default_params()
+    p.gnsbx, p.gnsby, p.gnsbz = 2, 1, 2
+    p.gsdimx, p.gsdimy, p.gsdimz = 5, 4, 3
+    p.cellSize, p.ts_delt = 2e-6, 1e-4
+    nx, ny, nz = (v + 2 for v in p.grid)
+    rng = np.random.default_rng(3)
+    f = {"temperature": rng.normal(900, 5, (nz, ny, nx)), "ce": rng.random((nz, ny, nx)),
+         "fs": rng.random((nz, ny, nx)), "gr": rng.integers(0, 7, (nz, ny, nx)).astype(np.int32)}
+    rot = rng.normal(size=(7, 3))
+    ren = rng.permutation(7).astype(np.uint64)
+    base = str(tmp_path / "xd")
+    for series in ([0], [0, 10]):
+        M.write_xdmf_arrays(p, base, series, f["temperature"], f["ce"], f["gr"], f["fs"], rot, ren)
+    _check_xdmf(tmp_path, "xd", p, [0, 10], f, rot, ren)
+    M.write_xdmf_arrays(p, base, [0], f["temperature"], f["ce"], f["gr"], f["fs"], rot, None)
+    _check_xdmf(tmp_path, "xd", p, [0], f, rot, None)
+
+
+def test_oracle_xdmf_renumbering_shifts_rank0_draws(built):
+    """The reference's XDMF writer draws its grain renumbering from rank 0's
+    rand() stream (io_xdmf.c:344-375): a permutation fixing 0, redrawn only
+    when the grain count grew, and later orientation draws of rank 0 follow
+    it, so the same deck with XDMF writes evolves differently."""
+    from _oracle import Oracle
+    p = M.read_deck(golden_deck("small4"))
+    a, b = Oracle(p), Oracle(p)
+    for s in (60, 120, 180, 260):
+        a.step(s - a.timestep)
+        b.step(s - b.timestep)
+        if s < 260:
+            r = a.xdmf_renumber()
+            assert r[0] == 0 and sorted(r.tolist()) == list(range(a.num_grains))
+            assert np.array_equal(a.xdmf_renumber(), r)  # same grain count: no new draws
+    assert mismatches(state_digests(a), state_digests(b))
+
+
+@pytest.mark.gpu
+def test_xdmf_writes_bit_exact_vs_oracle(built, cuda_device, tmp_path):
+    """small4 with XDMF writes at steps 60, 120, 180 (RandomizeGrains 1):
+    the device run's renumberings equal the oracle's, its state stays
+    bit-identical to the oracle's through step 260, and the files of the last
+    write hold the device fields."""
+    from _oracle import Oracle
+    p = M.read_deck(golden_deck("small4"))
+    o = Oracle(p)
+    base = str(tmp_path / "s4")
+    with M.Domain(p, precision=M.PREC_F64) as dom:
+        for s in (60, 120, 180, 260):
+            o.step(s - o.timestep)
+            dom.step(s - dom.timestep)
+            assert mismatches(state_digests(dom), state_digests(o)) == [], s
+            if s < 260:
+                dom.write_xdmf(base)
+                np.testing.assert_array_equal(dom.xdmf_renumbering(), o.xdmf_renumber())
+                if s == 180:
+                    fields = {k: dom.download(k) for k in ("temperature", "ce", "fs", "gr")}
+                    rot = np.array([list(g.rotang) for g in dom.grains()])
+                    _check_xdmf(tmp_path, "s4", p, [60, 120, 180], fields, rot, dom.xdmf_renumbering())
+        assert dom.num_grains == o.num_grains
+
+
+@pytest.mark.gpu
+def test_run_loop_writes_xdmf_like_reference(built, cuda_device, tmp_path):
+    """mms_run on small4 with DataFormat XDMF and DataWriteFreq 100: writes
+    at steps 0, 100, ..., 400 and at the last step, 401 (FinishTime 0.4005;
+    writeData, loop.c:199-256), the index lists them all, and the end state
+    equals the oracle stepped with the same renumberings."""
+    from _oracle import Oracle
+    text = golden_deck("small4").read_text()
+    text = "\n".join(l for l in text.splitlines() if not l.startswith("BaseFileName"))
+    text += f"\nBaseFileName {tmp_path}/r4\nDataFormat XDMF\nDataWriteFreq 100\n"
+    deck = tmp_path / "r4.in"
+    deck.write_text(text)
+    p = M.read_deck(deck)
+    o = Oracle(p)
+    o.xdmf_renumber()
+    for s in (100, 200, 300, 400, 401):
+        o.step(s - o.timestep)
+        o.xdmf_renumber()
+    with M.Domain(p, precision=M.PREC_F64) as dom:
+        dom.run(verbose=0)
+        assert dom.timestep == 401
+        assert mismatches(state_digests(dom), state_digests(o)) == []
+        np.testing.assert_array_equal(dom.xdmf_renumbering(), o.xdmf_renumber())
+    import xml.etree.ElementTree as ET
+    grids = ET.parse(tmp_path / "r4_ts.xmf").getroot().find("Domain").find("Grid").findall("Grid")
+    times = [round(float(g.find("Time").get("Value")) / p.ts_delt) for g in grids]
+    assert times == [0, 100, 200, 300, 400, 401]
+    assert (tmp_path / "r4_r3" / "00401.raw").exists()
