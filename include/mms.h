@@ -117,6 +117,14 @@ typedef struct mms_params {
     /* build options of this library */
     int precision;                    /* mms_precision */
     int device;                       /* CUDA device ordinal */
+    /* No counterpart in the reference.  0: the volume and surface sites of
+     * init_sb_nucleation (grain.c:930-1010) drawn on the host from each
+     * rank's rand() stream, exactly as the reference draws them (O(cells)
+     * host work).  1: drawn on the device from a counter-based generator
+     * (Philox4x32-10) keyed by RandSeedVal: the same site densities
+     * and threshold distributions, not the reference's sequence.  FixedNuc
+     * and NucVolume sites are the reference's in both. */
+    int site_setup;
 } mms_params;
 
 typedef enum mms_field {

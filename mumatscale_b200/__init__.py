@@ -90,7 +90,7 @@ class Params(C.Structure):
         ("basefilename", C.c_char * 256),
         ("fixed_nucs", C.POINTER(FixedNuc)), ("n_fixed_nucs", C.c_int),
         ("nuc_volumes", C.POINTER(NucVolume)), ("n_nuc_volumes", C.c_int),
-        ("precision", C.c_int), ("device", C.c_int),
+        ("precision", C.c_int), ("device", C.c_int), ("site_setup", C.c_int),
     ]
 
     @property

@@ -27,7 +27,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = "/usr/bin/g++"
 CC = "/usr/bin/gcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels.cu", "mms_api.cu", "adjoint.cu", "am_tc.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels.cu", "mms_api.cu", "adjoint.cu", "am_tc.cu", "noalloc.cu", "sites.cu"]
 CXX_SOURCES = ["deck.cpp", "host_setup.cpp", "output.cpp"]
 
 

@@ -170,9 +170,8 @@ float random_threshold(Rank &r, double center, double sigma)
 // Host-side initial state: SetupInitialConditions (setup.c:41-94),
 // init_nucleation_sites (grain.c:602-713, rank 0) and init_sb_nucleation
 // (grain.c:930-1010, every rank).  Produces the dense threshold array.
-void setup_sites(const mms_params &p, const Geo &g, const std::vector<mms_fixed_nuc> &fixed,
-                 const std::vector<mms_nuc_volume> &vols, std::vector<Rank> &ranks, std::vector<float> &thr,
-                 const std::vector<signed char> &mold)
+void assign_deck_sites(const mms_params &p, const Geo &g, const std::vector<mms_fixed_nuc> &fixed,
+                       const std::vector<mms_nuc_volume> &vols, std::vector<Rank> &ranks)
 {
     Rank &r0 = ranks[0];
     std::vector<NucPt> all;
@@ -220,6 +219,13 @@ void setup_sites(const mms_params &p, const Geo &g, const std::vector<mms_fixed_
         int sb = rank_of_cell(p, cx, cy, cz);
         if (sb >= 0) ranks[sb].nuc.push_back(n);
     }
+}
+
+void setup_sites(const mms_params &p, const Geo &g, const std::vector<mms_fixed_nuc> &fixed,
+                 const std::vector<mms_nuc_volume> &vols, std::vector<Rank> &ranks, std::vector<float> &thr,
+                 const std::vector<signed char> &mold)
+{
+    assign_deck_sites(p, g, fixed, vols, ranks);
     // init_sb_nucleation per rank
     const long long sbcells = g.sbcells;
     std::vector<long long> vol, suf;

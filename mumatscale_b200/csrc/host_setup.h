@@ -74,6 +74,10 @@ Geo make_geo(const mms_params &p);
 std::vector<signed char> make_mold(const Geo &g);
 // Seeds every emulated rank (ca_main.c:215) and assigns its subblock.
 void init_ranks(const mms_params &p, const Geo &g, std::vector<Rank> &ranks);
+// init_nucleation_sites (grain.c:602-713, rank 0): the deck's FixedNuc and
+// NucVolume points (rank 0 draws the latter), distributed to their ranks.
+void assign_deck_sites(const mms_params &p, const Geo &g, const std::vector<mms_fixed_nuc> &fixed,
+                       const std::vector<mms_nuc_volume> &vols, std::vector<Rank> &ranks);
 // init_nucleation_sites (grain.c:602-713, rank 0) and init_sb_nucleation
 // (grain.c:930-1010, every rank): fills the dense threshold array (+inf where
 // no site) and each rank's deck-defined nucleation points.

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <ctime>
+#include <map>
 #include <string>
 #include <sys/time.h>
 #include <unordered_map>
@@ -22,6 +23,7 @@
 
 #include "host_setup.h"
 #include "mms_internal.h"
+#include "sites.h"
 
 using namespace mms;
 
@@ -848,6 +850,87 @@ int slab_capacity(const mms_ctx *ctx, const std::vector<float> &thr)
     return (int)std::min<long long>(cap, 1LL << 30);
 }
 
+// mms_params.site_setup 1: the volume and surface sites of
+// init_sb_nucleation (grain.c:930-1010) drawn on the device (sites.cu), with
+// each rank's selection probability the reference's site count over its
+// candidate cells: floor(rho_v V dx^3) / V and floor(rho_s S dx^2) / S, V
+// its non-mold cells (all interior cells) and S those next to a pad face;
+// the deck-defined sites of the ranks are presets, the last one at a cell
+// winning, as the dense writes of init_sb_nucleation leave them.
+mms_status device_sites(mms_ctx *ctx)
+{
+    const mms_params &P = ctx->gp;
+    const Geo &G = ctx->gg, &g = ctx->ka.g;
+    const int nr = G.nranks;
+    const long long sbc = G.sbcells;
+    std::vector<double> pv((size_t)nr), ps((size_t)nr);
+    // indices of [lo, hi] (1-based, whole domain of n) not on a pad face
+    auto inner = [](long long lo, long long hi, long long n, int pad) {
+        long long c = hi - lo + 1;
+        if (pad) {
+            if (lo <= 1 && 1 <= hi) c--;
+            if (n != 1 && lo <= n && n <= hi) c--;
+        }
+        return c;
+    };
+    std::map<long long, float> pre;
+    for (int r = 0; r < nr; r++) {
+        Rank &rk = ctx->ranks[r];
+        rk.ncalls_presb = rk.ncalls;
+        const long long v = sbc;
+        const long long nin = inner((long long)rk.sbx * P.gsdimx + 1, (long long)(rk.sbx + 1) * P.gsdimx, G.gx, P.padBndyX) *
+                              inner((long long)rk.sby * P.gsdimy + 1, (long long)(rk.sby + 1) * P.gsdimy, G.gy, P.padBndyY) *
+                              inner((long long)rk.sbz * P.gsdimz + 1, (long long)(rk.sbz + 1) * P.gsdimz, G.gz, P.padBndyZ);
+        const long long sn = v - nin;
+        size_t cv = (size_t)(P.maxGrainDensity * (v * pow(P.cellSize, 3.0)));
+        cv = std::min<size_t>(cv, (size_t)v);
+        pv[r] = v ? (double)cv / (double)v : 0.0;
+        size_t cs = 0;
+        if (P.doSurfaceNuc && (P.maxGrainDensitySurf > 0.0)) cs = (size_t)(P.maxGrainDensitySurf * (sn * pow(P.cellSize, 2.0)));
+        cs = std::min<size_t>(cs, (size_t)sn);
+        ps[r] = sn ? (double)cs / (double)sn : 0.0;
+        for (const NucPt &n : rk.nuc) {
+            const long long lx = (long long)(n.cx % (size_t)P.gsdimx), ly = (long long)(n.cy % (size_t)P.gsdimy),
+                            lz = (long long)(n.cz % (size_t)P.gsdimz);
+            pre[(long long)r * sbc + (lz * P.gsdimy + ly) * P.gsdimx + lx] = (float)n.threshold;
+        }
+    }
+    std::vector<long long> pq;
+    std::vector<float> pt;
+    for (const auto &kv : pre) {
+        pq.push_back(kv.first);
+        pt.push_back(kv.second);
+    }
+    SiteDrawArgs a{};
+    a.total = (long long)g.nranks * sbc;
+    a.qbase = (long long)ctx->r0 * sbc;
+    a.sbcells = sbc;
+    a.sbx = P.gsdimx;
+    a.sby = P.gsdimy;
+    a.sbz = P.gsdimz;
+    a.nsbx = P.gnsbx;
+    a.nsby = P.gnsby;
+    a.gx = G.gx;
+    a.gy = G.gy;
+    a.gz = G.gz;
+    a.padx = P.padBndyX;
+    a.pady = P.padBndyY;
+    a.padz = P.padBndyZ;
+    a.rank0 = ctx->r0;
+    a.kz0 = ctx->kz0;
+    a.dsy = g.sy;
+    a.dsz = g.sz;
+    a.seed = P.base_random_seed;
+    a.vol_centre = P.gnGaussCenter;
+    a.vol_sigma = P.gnGaussSigma;
+    a.surf_centre = P.gnGaussCenterSurf;
+    a.surf_sigma = P.gnGaussSigmaSurf;
+    ctx->site_index.clear();
+    if (site_draw_device(a, pv, ps, pq, pt, ctx->site_cell, ctx->site_thr, ctx->site_rank, ctx->err))
+        return MMS_ERR_CUDA;
+    return MMS_OK;
+}
+
 mms_status alloc_slab_rows(mms_ctx *ctx, int cap)
 {
     DevPtrs &d = ctx->ka.d;
@@ -873,6 +956,9 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
     if (p0.gnsbz < 1 || !slab_span(p0, nslabs, slab, L0, L1)) return MMS_ERR_ARG;
     // the curvature stencil reaches three planes, beyond a slab's one-plane halo
     if (nslabs > 1 && p0.tip_curv) return MMS_ERR_ARG;
+    if (p0.site_setup != 0 && p0.site_setup != 1) return MMS_ERR_ARG;
+    // device-drawn sites give no whole-domain site count for the slabs' row buffers
+    if (nslabs > 1 && p0.site_setup) return MMS_ERR_ARG;
     if (p0.gnsbx < 1 || p0.gnsby < 1 || p0.gnsbz < 1 || p0.gsdimx < 1 || p0.gsdimy < 1 || p0.gsdimz < 1 ||
         p0.cellSize <= 0 || p0.ts_delt <= 0 || p0.maxTotalGrains < 1 || p0.maxTotalGrains > 0x7ffffffeULL)
         return MMS_ERR_ARG;
@@ -1021,7 +1107,6 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
         rk.seed_with((unsigned)r + 1 + p.base_random_seed);
     }
     // initial fields: ce = cl = Cinit everywhere, fs = gr = dc = 0 (setup.c:59-79)
-    std::vector<signed char> mold = make_mold(ctx->gg);  // whole domain, reference layout
     {
         std::vector<double> init(N, p.Cinit);
         double *dtmp;
@@ -1038,9 +1123,16 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
         // tempPrepareSB_int lsindex (temperature.c:183-189) at timestep 0
         ctx->launches += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, nullptr);
     }
-    std::vector<float> thr((size_t)ctx->gg.rN, INFINITY);  // whole domain, reference layout
-    setup_sites(ctx->gp, ctx->gg, ctx->fixed, ctx->vols, ctx->ranks, thr, mold);
-    extract_sites(ctx, thr);
+    std::vector<float> thr;  // whole domain, reference layout (host site setup)
+    if (p.site_setup == 1) {
+        assign_deck_sites(ctx->gp, ctx->gg, ctx->fixed, ctx->vols, ctx->ranks);
+        if ((st = device_sites(ctx))) return fail(st);
+    } else {
+        const std::vector<signed char> mold = make_mold(ctx->gg);
+        thr.assign((size_t)ctx->gg.rN, INFINITY);
+        setup_sites(ctx->gp, ctx->gg, ctx->fixed, ctx->vols, ctx->ranks, thr, mold);
+        extract_sites(ctx, thr);
+    }
     if ((st = upload_sites(ctx)) || (st = upload_nucpt(ctx))) return fail(st);
     d.nslabs = nslabs;
     d.slab = slab;
