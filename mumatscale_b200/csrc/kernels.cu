@@ -891,10 +891,12 @@ constexpr int DTX = 32, DTY = 8;
 // per slot, issued TS-1 planes ahead of the plane being updated.
 template <typename Real, int CPT>
 struct Depth {
-    // planes in the ring: deeper for FP32, whose planes are smaller
-    static constexpr int TS = (sizeof(Real) == 4 && CPT == 1) ? 8 : 6;
+    // planes in the ring: deeper for FP32 with one cell per thread, whose
+    // planes are smaller; five for FP32 with two, so that four CTAs' rings
+    // fit in shared memory
+    static constexpr int TS = (sizeof(Real) == 4 && CPT == 1) ? 8 : (sizeof(Real) == 4 ? 5 : 6);
     // CTAs per SM the register budget is set for
-    static constexpr int MINB = CPT == 1 ? 4 : (sizeof(Real) == 4 ? 3 : 2);
+    static constexpr int MINB = CPT == 1 ? 4 : (sizeof(Real) == 4 ? 4 : 2);
 };
 constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 
