@@ -892,11 +892,11 @@ constexpr int DTX = 32, DTY = 8;
 template <typename Real, int CPT>
 struct Depth {
     // planes in the ring: deeper for FP32 with one cell per thread, whose
-    // planes are smaller; five for FP32 with two, so that four CTAs' rings
-    // fit in shared memory
-    static constexpr int TS = (sizeof(Real) == 4 && CPT == 1) ? 8 : (sizeof(Real) == 4 ? 5 : 6);
+    // planes are smaller; with two cells per thread, five (FP32) or four
+    // (FP64) planes, so that four (three) CTAs' rings fit in shared memory
+    static constexpr int TS = (sizeof(Real) == 4 && CPT == 1) ? 8 : (CPT == 1 ? 6 : (sizeof(Real) == 4 ? 5 : 4));
     // CTAs per SM the register budget is set for
-    static constexpr int MINB = CPT == 1 ? 4 : (sizeof(Real) == 4 ? 4 : 2);
+    static constexpr int MINB = CPT == 1 ? 4 : (sizeof(Real) == 4 ? 4 : 3);
 };
 constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 
