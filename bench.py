@@ -664,6 +664,7 @@ def slabs_workload(args) -> None:
 
     if ws > 1:
         s = DistributedSlab(params, precision=M.PREC_F64, device=dev)
+        s.dom.autotune(reps=5)  # stencil tile for this slab's grid
         s.step(W)
         st = s.stream
         run = s.step
@@ -672,6 +673,7 @@ def slabs_workload(args) -> None:
         s = M.Domain(params, precision=M.PREC_F64, device=dev)
         st = torch.cuda.current_stream()
         s.set_stream(st.cuda_stream)
+        s.autotune(reps=5)
         s.step(W)
         run = s.step
         launches0 = s.kernel_launches
@@ -694,6 +696,8 @@ def slabs_workload(args) -> None:
         group = {}
         for n in (2, 4):
             with M.SlabGroup(params, n, precision=M.PREC_F64, devices=(dev,)) as g:
+                for d in g.slabs:
+                    d.autotune(reps=3)
                 g.step(W)
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
