@@ -1738,13 +1738,18 @@ __global__ void __launch_bounds__(RED_NT) k_reduce(KernelArgs a, int what, doubl
     // pairwise and the group enters the running sum with compensation (the
     // FP64 pipe, not memory, bounded the kernel with one TwoSum per value).
     constexpr int U = 4;
+    // rows number fewer than 2^32: (k, j) of a row by a 32-bit
+    // multiply-high division (a 64-bit division per row cost more than the
+    // sums)
+    const unsigned gy = (unsigned)g.gy, gy_m = gy <= 1 ? 0xffffffffu : (unsigned)((1ULL << 32) / gy);
     for (long long r0 = (long long)blockIdx.x * U; r0 < rows; r0 += (long long)gridDim.x * U) {
         const Real *row[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const long long r = r0 + u < rows ? r0 + u : r0;
-            const long long k = r / g.gy + 1, j = r - (k - 1) * g.gy + 1;
-            row[u] = f + k * g.sz + j * g.sy;
+            const unsigned r = (unsigned)(r0 + u < rows ? r0 + u : r0);
+            unsigned jj;
+            const unsigned kk = fast_divmod(r, gy, gy_m, jj);
+            row[u] = f + (long long)(kk + 1) * g.sz + (long long)(jj + 1) * g.sy;
         }
         for (int i = 1 + (int)threadIdx.x; i <= g.gx; i += RED_NT) {
             double x[U];
