@@ -142,6 +142,11 @@ struct mms_ctx {
     std::vector<uint64_t> renumber;
     std::vector<int64_t> xdmf_series;
     std::string xdmf_base;
+    // h_ctl holds the device control block as it stands: set at the end of
+    // mms_step, cleared by every call that runs kernels writing the block
+    // (steps, the adjoint's record, slab and batch steps, tuning) or writes
+    // it from the host; reductions, copies and conversions never write it
+    bool ctl_known = false;
     // frozen-CA record for the adjoint
     struct AdjRec {
         unsigned long long t0 = 0;
@@ -684,6 +689,7 @@ mms_status mms_get_stencil_tile(const mms_ctx *ctx, int *cells_per_thread, int *
 // over `reps` launches is kept.
 mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchunk, double *best_ms)
 {
+    if (ctx) ctx->ctl_known = false;
     if (!ctx || reps < 1) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     mms_status rs0 = read_ctl(ctx);
@@ -1193,6 +1199,7 @@ mms_status mms_set_grains(mms_ctx *ctx, int n, const double *rotmat9)
 {
     if (!ctx || n < 0 || (n && !rotmat9)) return MMS_ERR_ARG;
     if (ctx->stepped) return MMS_ERR_STATE;
+    ctx->ctl_known = false;
     if ((uint64_t)n + 1 > ctx->p.maxTotalGrains + 1) return MMS_ERR_GRAIN_OVERFLOW;
     cudaSetDevice(ctx->device);
     mms_status st = read_ctl(ctx);
@@ -1296,8 +1303,10 @@ mms_status mms_step(mms_ctx *ctx, int nsteps)
     ctx->stepped = true;
     const int chunk = 256;
     int done = 0;
-    mms_status st = read_ctl(ctx);
-    if (st) return st;
+    mms_status st = MMS_OK;
+    // the previous step call ended by reading the control block
+    if (!ctx->ctl_known && (st = read_ctl(ctx))) return st;
+    ctx->ctl_known = false;
     if (ctx->h_ctl->status) return (mms_status)ctx->h_ctl->status;
     unsigned long long ts0 = ctx->h_ctl->timestep;
     while (done < nsteps) {
@@ -1336,6 +1345,7 @@ mms_status mms_step(mms_ctx *ctx, int nsteps)
         done += n;
         if ((st = refill_rng(ctx, false))) return st;
     }
+    ctx->ctl_known = true;
     return MMS_OK;
 }
 
@@ -1726,6 +1736,7 @@ mms_status mms_adjoint_release(mms_ctx *ctx)
 
 mms_status mms_adjoint_record(mms_ctx *ctx, int nsteps, int checkpoint_every)
 {
+    if (ctx) ctx->ctl_known = false;
     if (!ctx || nsteps < 1 || checkpoint_every < 1 || ctx->nslabs > 1) return MMS_ERR_ARG;
     if (ctx->ka.p.temp_mode == 2) {
         ctx->err = "the adjoint supports the analytic temperature models only";
@@ -2163,6 +2174,7 @@ mms_status mms_batch_step(mms_batch *b, int nsteps)
     mms_status st;
     const size_t nd = b->doms.size();
     for (mms_ctx *ctx : b->doms) {
+        ctx->ctl_known = false;
         if ((st = read_ctl(ctx))) return st;
         if (ctx->h_ctl->status) return (mms_status)ctx->h_ctl->status;
         ctx->stepped = true;
@@ -2450,6 +2462,7 @@ mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path)
 
 mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path)
 {
+    if (ctx) ctx->ctl_known = false;
     if (!ctx || !path) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     mms_status st = read_ctl(ctx);
@@ -2630,6 +2643,7 @@ void slab_plan(mms_ctx *ctx, int point, unsigned long long ts, std::vector<mms_s
 mms_status slab_launch(mms_ctx *ctx, int phase, int resume)
 {
     cudaSetDevice(ctx->device);
+    ctx->ctl_known = false;
     if (phase == 0 && !resume && ctx->p.am)
         ctx->launches += launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, ctx->stream, nullptr);
     ctx->launches += launch_slab_phase(ctx->ka, ctx->tma, ctx->prec, ctx->stream, phase, resume);
@@ -2776,6 +2790,7 @@ mms_status mms_slab_poll(mms_ctx *ctx, uint64_t *timestep, int *stalled)
 mms_status mms_slab_refill(mms_ctx *ctx)
 {
     if (!ctx) return MMS_ERR_ARG;
+    ctx->ctl_known = false;
     cudaSetDevice(ctx->device);
     mms_status st = read_ctl(ctx);
     if (st) return st;
