@@ -95,7 +95,7 @@ struct Geo {
 
 inline unsigned div_magic(unsigned d) { return d <= 1 ? 0xffffffffu : (unsigned)((1ULL << 32) / d); }
 
-constexpr int LIST_PIECES = 1024;
+constexpr int LIST_PIECES = 512;
 
 inline long long dev_index(const Geo &g, long long i, long long j, long long k) { return k * g.sz + j * g.sy + i; }
 inline long long ref_index(const Geo &g, long long i, long long j, long long k) { return k * g.rsz + j * g.rsy + i; }
