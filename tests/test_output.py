@@ -218,3 +218,28 @@ def test_run_loop_writes_xdmf_like_reference(built, cuda_device, tmp_path):
     times = [round(float(g.find("Time").get("Value")) / p.ts_delt) for g in grids]
     assert times == [0, 100, 200, 300, 400, 401]
     assert (tmp_path / "r4_r3" / "00401.raw").exists()
+
+
+@pytest.mark.gpu
+def test_run_loop_writes_vtk(built, cuda_device, tmp_path):
+    """mms_run with DataFormat VTK and DataWriteFreq 200 on small4 (to step
+    401): ParaView files at steps 0, 200, 400 and 401 (writeData,
+    loop.c:199-256), one piece per subblock, the last holding the end state."""
+    text = golden_deck("small4").read_text()
+    text = "\n".join(l for l in text.splitlines() if not l.startswith("BaseFileName"))
+    text += f"\nBaseFileName {tmp_path}/v4\nDataFormat VTK\nDataWriteFreq 200\n"
+    deck = tmp_path / "v4.in"
+    deck.write_text(text)
+    p = M.read_deck(deck)
+    with M.Domain(p, precision=M.PREC_F64) as dom:
+        dom.run(verbose=0)
+        gr = dom.download("gr")
+    for ts in (0, 200, 400, 401):
+        assert (tmp_path / f"v4_{ts}.pvtu").exists(), ts
+    nsub = p.gnsbx * p.gnsby * p.gnsbz
+    piece = ET.parse(tmp_path / "v4_0000" / "401.vtu").getroot()
+    got = np.array(_arr(piece, "Grain").text.split(), dtype=np.int32)
+    sd = (p.gsdimz, p.gsdimy, p.gsdimx)
+    # subblock 0, cells in the reference's x-major order (x outer, z inner)
+    want = gr[1:sd[0] + 1, 1:sd[1] + 1, 1:sd[2] + 1].transpose(2, 1, 0).reshape(-1)
+    assert nsub == 4 and np.array_equal(got, want)

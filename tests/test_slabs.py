@@ -154,11 +154,13 @@ def test_slabs_equal_single_domain(built, cuda_device, prec, nslabs):
 
 
 @pytest.mark.gpu
-def test_slabs_am_quadrature(built, cuda_device):
+@pytest.mark.parametrize("prec", [M.PREC_F64, M.PREC_F32])
+def test_slabs_am_quadrature(built, cuda_device, prec):
     """AM deck (moving-source quadrature, whole-domain z in the slab's
-    temperature) as two slabs: bit for bit the single domain's."""
+    temperature; the FP32 form's contraction on the tensor cores) as two
+    slabs: bit for bit the single domain's."""
     p = _deck("am1", nsbz=2, sdimz=6)
-    with M.Domain(p) as dom, M.SlabGroup(p, 2) as grp:
+    with M.Domain(p, precision=prec) as dom, M.SlabGroup(p, 2, precision=prec) as grp:
         for n in (50, 80):
             dom.step(n)
             grp.step(n)
