@@ -92,6 +92,8 @@ struct mms_ctx {
     // when sites or orientation overrides are replaced)
     cudaGraphExec_t step_graph = nullptr;
     int step_graph_kernels = 0;
+    // GRAPH_STEPS consecutive steps in one graph (fewer graph boundaries)
+    cudaGraphExec_t multi_graph = nullptr;
     bool use_graphs = true;
     cudaStream_t own_stream = nullptr;
     EventProfiler *prof = nullptr;
@@ -195,10 +197,14 @@ mms_status dalloc(mms_ctx *ctx, T **ptr, size_t count)
     return MMS_OK;
 }
 
+constexpr int GRAPH_STEPS = 8;
+
 void drop_graph(mms_ctx *ctx)
 {
     if (ctx->step_graph) cudaGraphExecDestroy(ctx->step_graph);
     ctx->step_graph = nullptr;
+    if (ctx->multi_graph) cudaGraphExecDestroy(ctx->multi_graph);
+    ctx->multi_graph = nullptr;
 }
 
 void dfree(mms_ctx *ctx, void *p)
@@ -428,25 +434,38 @@ AmParams am_params(const mms_params &p)
     return m;
 }
 
-// Captures one whole step into a graph (once per kernel-argument set).
+// Captures one whole step, and GRAPH_STEPS consecutive steps, into graphs
+// (once per kernel-argument set).  A step that stalls turns the kernels
+// after it into no-ops, so a multi-step graph stops where separate
+// launches would.
 mms_status ensure_graph(mms_ctx *ctx)
 {
-    if (ctx->step_graph) return MMS_OK;
-    cudaGraph_t g = nullptr;
-    CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    if (ctx->step_graph && ctx->multi_graph) return MMS_OK;
     EventProfiler *saved = ctx->prof;
     ctx->prof = nullptr;
-    int n = launch_one_step(ctx, 0);
+    auto capture = [&](int steps, cudaGraphExec_t *out) -> int {
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return -1;
+        int n = 0;
+        for (int k = 0; k < steps; k++) n += launch_one_step(ctx, 0);
+        if (cudaStreamEndCapture(ctx->stream, &g) != cudaSuccess) return -1;
+        const cudaError_t e = cudaGraphInstantiate(out, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            *out = nullptr;
+            return -1;
+        }
+        return n;
+    };
+    const int n1 = ctx->step_graph ? ctx->step_graph_kernels : capture(1, &ctx->step_graph);
+    const int nm = n1 >= 0 ? capture(GRAPH_STEPS, &ctx->multi_graph) : -1;
     ctx->prof = saved;
-    CU(cudaStreamEndCapture(ctx->stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&ctx->step_graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-        ctx->step_graph = nullptr;
-        ctx->err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+    if (n1 < 0 || nm < 0) {
+        drop_graph(ctx);
+        ctx->err = "capturing the step graphs failed";
         return MMS_ERR_CUDA;
     }
-    ctx->step_graph_kernels = n;
+    ctx->step_graph_kernels = n1;
     return MMS_OK;
 }
 
@@ -1313,7 +1332,12 @@ mms_status mms_step(mms_ctx *ctx, int nsteps)
         int n = std::min(chunk, nsteps - done);
         if (ctx->use_graphs && !ctx->prof) {
             if ((st = ensure_graph(ctx))) return st;
-            for (int s = 0; s < n; s++) {
+            int s = 0;
+            for (; s + GRAPH_STEPS <= n; s += GRAPH_STEPS) {
+                CU(cudaGraphLaunch(ctx->multi_graph, ctx->stream));
+                ctx->launches += (uint64_t)ctx->step_graph_kernels * GRAPH_STEPS;
+            }
+            for (; s < n; s++) {
                 CU(cudaGraphLaunch(ctx->step_graph, ctx->stream));
                 ctx->launches += ctx->step_graph_kernels;
             }
