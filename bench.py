@@ -296,8 +296,9 @@ def gpu_arm(args) -> None:
         if form == "f64":
             # end to end through the public API with host buffers: upload the
             # whole state from pinned host memory, K steps each followed by a
-            # device->host read of the fraction solid (loop.c's screen value),
-            # and a final download of grain ids and ce
+            # device->host read of the fraction solid (loop.c's screen value,
+            # one mms_step_reduce call per step), and a final download of
+            # grain ids and ce
             n = dom.num_cells()
             host = {f: torch.empty(n * (3 if f == "dc" else 1),
                                    dtype=torch.int32 if f == "gr" else torch.float64).pin_memory()
@@ -316,8 +317,7 @@ def gpu_arm(args) -> None:
                 h2d += t.numel() * t.element_size()
             d2h = 0
             for _ in range(K):
-                dom.step(1)
-                dom.reduce("fs_fraction")
+                dom.step_reduce(1, "fs_fraction")
                 d2h += 8
             gr = dom.download("gr", out=host_out["gr"].numpy())
             ce = dom.download("ce", out=host_out["ce"].numpy())

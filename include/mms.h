@@ -217,7 +217,18 @@ mms_status mms_get_num_grains(mms_ctx *ctx, int *num_grains);
 size_t mms_num_cells(const mms_ctx *ctx);
 mms_status mms_download(mms_ctx *ctx, mms_field field, void *host);
 mms_status mms_upload(mms_ctx *ctx, mms_field field, const void *host);
+/* computeFS / solid_volume (loop.c:173-183, growth.c:541-566) and the ce
+ * sum, by a pass over the field (FP64, compensated). */
 mms_status mms_reduce(mms_ctx *ctx, mms_reduction what, double *out);
+
+/* mms_step followed by mms_reduce, with one synchronisation: the reference
+ * loop's doiteration followed by computeFS at a screen-output step
+ * (loop.c:227-234).  For the fraction-solid reductions the last step's
+ * stencil also leaves one sum per tile, and those few thousand values are
+ * folded instead of reading the field again (mms_reduce does the same until
+ * the next call that steps or writes fields).  Both are FP64 sums within a
+ * few ulps of each other, in different orders. */
+mms_status mms_step_reduce(mms_ctx *ctx, int nsteps, mms_reduction what, double *out);
 
 /* Allocation-free form of mms_reduce over a caller-owned field.  It has no
  * counterpart in the reference (whose reductions run on host arrays); it is

@@ -174,6 +174,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_download": (I, [P, I, P]),
         "mms_upload": (I, [P, I, P]),
         "mms_reduce": (I, [P, I, C.POINTER(D)]),
+        "mms_step_reduce": (I, [P, I, I, C.POINTER(D)]),
         "mms_set_sites": (I, [P, C.c_int64, P, P]),
         "mms_set_site_orientations": (I, [P, C.c_int64, P, P]),
         "mms_get_grains": (I, [P, I, I, C.POINTER(Grain)]),
@@ -452,6 +453,14 @@ class Domain:
     def reduce(self, what: str = "fs_fraction") -> float:
         v = C.c_double()
         _check(_lib().mms_reduce(self._ctx, REDUCE[what], C.byref(v)), "mms_reduce", self._ctx)
+        return float(v.value)
+
+    def step_reduce(self, nsteps: int = 1, what: str = "fs_fraction") -> float:
+        """step(nsteps) then reduce(what) with one synchronisation (the
+        reference loop's doiteration + computeFS, loop.c:227-234)."""
+        v = C.c_double()
+        _check(_lib().mms_step_reduce(self._ctx, int(nsteps), REDUCE[what], C.byref(v)), "mms_step_reduce",
+               self._ctx)
         return float(v.value)
 
     # -- sites, orientations, grains

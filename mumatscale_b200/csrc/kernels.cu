@@ -927,18 +927,21 @@ template <int TS>
 struct StencilShared {
     unsigned long long bars[TS];
     double sT[64];
+    double fsum[DTY];
     int abort;
 };
 
 // One (32 CPT) x 8 x zchunk tile (bx, by, bz) of the diffusion + fs-change
 // update.  ring: planes this CTA has streamed through its ring before this
-// tile, so slot and phase continue across tiles.  Returns false when a copy
-// did not land within the bound (the error is raised, copies in flight are
-// drained).
+// tile, so slot and phase continue across tiles.  part (may be null): the
+// tile's sum of the new fraction solid goes to part[2 part_idx] (and 0 to
+// part[2 part_idx + 1], the compensation slot of k_reduce_fold).  Returns
+// false when a copy did not land within the bound (the error is raised,
+// copies in flight are drained).
 template <typename Real, int CPT>
 __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps &maps, int zchunk, int bx, int by,
                                              int bz, unsigned char *smem, StencilShared<Depth<Real, CPT>::TS> &sh,
-                                             unsigned &ring)
+                                             unsigned &ring, double *part = nullptr, long long part_idx = 0)
 {
     using L = Stage<Real, CPT>;
     constexpr int TS = Depth<Real, CPT>::TS;
@@ -1011,6 +1014,7 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
     unsigned ph2 = phase(2);
     long long crow = (long long)k0 * g.sz + (long long)j * g.sy;
     bool alive = true;
+    double fsum = 0.0;  // this thread's new fs values, in plane order
     for (int t = 0; t <= k1 - k0; t++) {
         const int k = k0 + t;
         // planes t and t+1 completed in earlier iterations
@@ -1054,6 +1058,7 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
                 // growth.c:163-165 (the FP32 form stores ce - Cinit)
                 if (sizeof(Real) == 8 ? cen < 0 : cen < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
                 solid[u] = gr_new > 0;
+                if (part) fsum += (double)fs_new;
             }
         }
 #pragma unroll
@@ -1085,10 +1090,26 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
         crow += g.sz;
     }
     ring = base + (unsigned)nplanes;
+    if (part && alive) {
+        // fixed-order tree: lanes, then the 8 warps
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) fsum += __shfl_down_sync(FULL_MASK, fsum, o);
+        if (tx == 0) sh.fsum[ty] = fsum;
+        __syncthreads();
+        if (tid == 0) {
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < DTY; w++) v += sh.fsum[w];
+            part[2 * part_idx] = v;
+            part[2 * part_idx + 1] = 0.0;
+        }
+    }
     return alive;
 }
 
-template <typename Real, int CPT>
+// SUMFS: each tile also leaves its sum of the new fraction solid in
+// a.d.fs_part (the step a reduction follows; ~3 % slower otherwise).
+template <typename Real, int CPT, bool SUMFS>
 __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
     k_diffuse_fs_tma(const __grid_constant__ KernelArgs a, const __grid_constant__ TmaMaps maps, int zchunk)
 {
@@ -1101,7 +1122,9 @@ __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
         fence_barrier_init();
     }
     unsigned ring = 0;
-    stencil_tile<Real, CPT>(a, maps, zchunk, blockIdx.x, blockIdx.y, blockIdx.z, smem, sh, ring);
+    stencil_tile<Real, CPT>(a, maps, zchunk, blockIdx.x, blockIdx.y, blockIdx.z, smem, sh, ring,
+                            SUMFS ? a.d.fs_part : nullptr,
+                            ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
 }
 
 // Many independent domains in one persistent launch: every CTA walks the
@@ -1954,7 +1977,9 @@ static int make_tma_t(const KernelArgs &a, TmaHolder &out)
     std::memcpy(out.bytes, &m, sizeof m);
     out.ok = ok ? 1 : 0;
     if (ok) {
-        cudaFuncSetAttribute(k_diffuse_fs_tma<Real, CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_diffuse_fs_tma<Real, CPT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             Depth<Real, CPT>::TS * L::BYTES);
+        cudaFuncSetAttribute(k_diffuse_fs_tma<Real, CPT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              Depth<Real, CPT>::TS * L::BYTES);
     }
     return out.ok;
@@ -1974,7 +1999,7 @@ int make_tma(const KernelArgs &a, int precision, TmaHolder &out)
     if (prof) prof->end(id, st)
 
 template <typename Real>
-static void launch_stencil_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st)
+static void launch_stencil_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st, bool sumfs = false)
 {
     const Geo &g = a.g;
     const int cpt = (tma.ok && tma.cpt == 2) ? 2 : 1;
@@ -1990,15 +2015,32 @@ static void launch_stencil_t(const KernelArgs &a, const TmaHolder &tma, cudaStre
     } else if (tma.ok) {
         TmaMaps maps;
         std::memcpy(&maps, tma.bytes, sizeof maps);
-        if (cpt == 2)
-            k_diffuse_fs_tma<Real, 2><<<grid, dim3(DTX, DTY), Depth<Real, 2>::TS * Stage<Real, 2>::BYTES, st>>>(
-                a, maps, zc);
-        else
-            k_diffuse_fs_tma<Real, 1><<<grid, dim3(DTX, DTY), Depth<Real, 1>::TS * Stage<Real, 1>::BYTES, st>>>(
-                a, maps, zc);
+        const dim3 blk(DTX, DTY);
+        const int b2 = Depth<Real, 2>::TS * Stage<Real, 2>::BYTES, b1 = Depth<Real, 1>::TS * Stage<Real, 1>::BYTES;
+        if (cpt == 2 && sumfs) k_diffuse_fs_tma<Real, 2, true><<<grid, blk, b2, st>>>(a, maps, zc);
+        else if (cpt == 2) k_diffuse_fs_tma<Real, 2, false><<<grid, blk, b2, st>>>(a, maps, zc);
+        else if (sumfs) k_diffuse_fs_tma<Real, 1, true><<<grid, blk, b1, st>>>(a, maps, zc);
+        else k_diffuse_fs_tma<Real, 1, false><<<grid, blk, b1, st>>>(a, maps, zc);
     } else {
         k_diffuse_fs<Real, false><<<grid, dim3(DTX, DTY), 0, st>>>(a, zc);
     }
+}
+
+// Tiles of the TMA stencil launch, each of which leaves its sum of the new
+// fraction solid in a.d.fs_part; 0 when the step runs another variant.
+long long stencil_parts(const KernelArgs &a, const TmaHolder &tma)
+{
+    if (!tma.ok || a.d.rec_flags || !a.d.fs_part) return 0;
+    const Geo &g = a.g;
+    const int tile_x = DTX * (tma.cpt == 2 ? 2 : 1);
+    int zc = tma.zc > 0 ? (tma.zc < g.gz ? tma.zc : g.gz) : pick_zchunk(g, tile_x);
+    if (zc > 64) zc = 64;
+    return (long long)((g.gx + tile_x - 1) / tile_x) * ((g.gy + DTY - 1) / DTY) * ((g.gz + zc - 1) / zc);
+}
+
+long long stencil_parts_max(const Geo &g)
+{
+    return (long long)((g.gx + DTX - 1) / DTX) * ((g.gy + DTY - 1) / DTY) * g.gz;
 }
 
 int launch_stencil(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream)
@@ -2051,11 +2093,12 @@ static int launch_post_t(const KernelArgs &a, cudaStream_t st, Profiler *prof)
 }
 
 template <typename Real>
-static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st, int start_stage, Profiler *prof)
+static int launch_step_t(const KernelArgs &a, const TmaHolder &tma, cudaStream_t st, int start_stage, Profiler *prof,
+                         bool sumfs)
 {
     int n = launch_pre_t<Real>(a, st, start_stage, prof);
     PROF_BEGIN(KID_DIFFUSE_FS);
-    launch_stencil_t<Real>(a, tma, st);
+    launch_stencil_t<Real>(a, tma, st, sumfs);
     PROF_END(KID_DIFFUSE_FS);
     n++;
     return n + launch_post_t<Real>(a, st, prof);
@@ -2215,11 +2258,12 @@ int launch_stencil_batch(const void *items, int nitems, long long total_tiles, i
     return 1;
 }
 
-int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream, int start_stage, Profiler *prof)
+int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream, int start_stage, Profiler *prof,
+                bool sumfs)
 {
     cudaStream_t st = (cudaStream_t)stream;
-    if (precision == MMS_PREC_F32) return launch_step_t<float>(a, tma, st, start_stage, prof);
-    return launch_step_t<double>(a, tma, st, start_stage, prof);
+    if (precision == MMS_PREC_F32) return launch_step_t<float>(a, tma, st, start_stage, prof, sumfs);
+    return launch_step_t<double>(a, tma, st, start_stage, prof, sumfs);
 }
 
 int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof)
@@ -2268,6 +2312,16 @@ __global__ void __launch_bounds__(1024) k_reduce_fold(double *partial, int nb)
         __syncthreads();
     }
     if (threadIdx.x == 0) partial[2 * nb] = ss[0] + sc[0];
+}
+
+// Folds the last step's per-tile fraction-solid sums (stencil_parts of
+// them) and copies the total to pinned memory; the caller synchronises.
+int launch_fold_fs(const KernelArgs &a, long long nparts, void *stream, double *pinned)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    k_reduce_fold<<<1, 1024, 0, st>>>(a.d.fs_part, (int)nparts);
+    cudaMemcpyAsync(pinned, a.d.fs_part + 2 * nparts, sizeof(double), cudaMemcpyDeviceToHost, st);
+    return 1;
 }
 
 int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream, double *pinned)

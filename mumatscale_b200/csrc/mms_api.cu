@@ -94,6 +94,9 @@ struct mms_ctx {
     int step_graph_kernels = 0;
     // GRAPH_STEPS consecutive steps in one graph (fewer graph boundaries)
     cudaGraphExec_t multi_graph = nullptr;
+    // one step whose stencil also leaves its per-tile fraction-solid sums
+    // (the last step of mms_step_reduce)
+    cudaGraphExec_t sum_graph = nullptr;
     bool use_graphs = true;
     cudaStream_t own_stream = nullptr;
     EventProfiler *prof = nullptr;
@@ -149,6 +152,11 @@ struct mms_ctx {
     // (steps, the adjoint's record, slab and batch steps, tuning) or writes
     // it from the host; reductions, copies and conversions never write it
     bool ctl_known = false;
+    // d.fs_part holds the per-tile fraction-solid sums of the current
+    // fields: set by a successful mms_step_reduce whose last stencil left
+    // them, cleared by every other step, wherever ctl_known is, and by
+    // every call that writes fields or changes the stencil tile
+    bool fs_part_valid = false;
     // frozen-CA record for the adjoint
     struct AdjRec {
         unsigned long long t0 = 0;
@@ -205,6 +213,8 @@ void drop_graph(mms_ctx *ctx)
     ctx->step_graph = nullptr;
     if (ctx->multi_graph) cudaGraphExecDestroy(ctx->multi_graph);
     ctx->multi_graph = nullptr;
+    if (ctx->sum_graph) cudaGraphExecDestroy(ctx->sum_graph);
+    ctx->sum_graph = nullptr;
 }
 
 void dfree(mms_ctx *ctx, void *p)
@@ -413,7 +423,7 @@ mms_status read_ctl(mms_ctx *ctx)
     return MMS_OK;
 }
 
-int launch_one_step(mms_ctx *ctx, int start_stage);
+int launch_one_step(mms_ctx *ctx, int start_stage, bool sumfs = false);
 
 AmParams am_params(const mms_params &p)
 {
@@ -440,14 +450,14 @@ AmParams am_params(const mms_params &p)
 // launches would.
 mms_status ensure_graph(mms_ctx *ctx)
 {
-    if (ctx->step_graph && ctx->multi_graph) return MMS_OK;
+    if (ctx->step_graph && ctx->multi_graph && ctx->sum_graph) return MMS_OK;
     EventProfiler *saved = ctx->prof;
     ctx->prof = nullptr;
-    auto capture = [&](int steps, cudaGraphExec_t *out) -> int {
+    auto capture = [&](int steps, cudaGraphExec_t *out, bool sumfs = false) -> int {
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return -1;
         int n = 0;
-        for (int k = 0; k < steps; k++) n += launch_one_step(ctx, 0);
+        for (int k = 0; k < steps; k++) n += launch_one_step(ctx, 0, sumfs);
         if (cudaStreamEndCapture(ctx->stream, &g) != cudaSuccess) return -1;
         const cudaError_t e = cudaGraphInstantiate(out, g, 0);
         cudaGraphDestroy(g);
@@ -458,9 +468,10 @@ mms_status ensure_graph(mms_ctx *ctx)
         return n;
     };
     const int n1 = ctx->step_graph ? ctx->step_graph_kernels : capture(1, &ctx->step_graph);
-    const int nm = n1 >= 0 ? capture(GRAPH_STEPS, &ctx->multi_graph) : -1;
+    const int nm = n1 >= 0 && !ctx->multi_graph ? capture(GRAPH_STEPS, &ctx->multi_graph) : 0;
+    const int ns = n1 >= 0 && nm >= 0 && !ctx->sum_graph ? capture(1, &ctx->sum_graph, true) : 0;
     ctx->prof = saved;
-    if (n1 < 0 || nm < 0) {
+    if (n1 < 0 || nm < 0 || ns < 0) {
         drop_graph(ctx);
         ctx->err = "capturing the step graphs failed";
         return MMS_ERR_CUDA;
@@ -469,14 +480,14 @@ mms_status ensure_graph(mms_ctx *ctx)
     return MMS_OK;
 }
 
-int launch_one_step(mms_ctx *ctx, int start_stage)
+int launch_one_step(mms_ctx *ctx, int start_stage, bool sumfs)
 {
     int n = 0;
     const mms_params &p = ctx->p;
     if (start_stage == 0 && p.am) {
         n += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, ctx->prof);
     }
-    n += launch_step(ctx->ka, ctx->tma, ctx->prec, ctx->stream, start_stage, ctx->prof);
+    n += launch_step(ctx->ka, ctx->tma, ctx->prec, ctx->stream, start_stage, ctx->prof, sumfs);
     return n;
 }
 
@@ -690,6 +701,7 @@ mms_status mms_set_stencil_tile(mms_ctx *ctx, int cells_per_thread, int zchunk)
     ctx->tma.zc = zchunk;
     make_tma(ctx->ka, ctx->prec, ctx->tma);
     drop_graph(ctx);
+    ctx->fs_part_valid = false;
     return MMS_OK;
 }
 
@@ -708,7 +720,7 @@ mms_status mms_get_stencil_tile(const mms_ctx *ctx, int *cells_per_thread, int *
 // over `reps` launches is kept.
 mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchunk, double *best_ms)
 {
-    if (ctx) ctx->ctl_known = false;
+    if (ctx) ctx->ctl_known = ctx->fs_part_valid = false;
     if (!ctx || reps < 1) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     mms_status rs0 = read_ctl(ctx);
@@ -1103,7 +1115,8 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
         (st = dalloc(ctx, &d.list_cell, (size_t)g.nranks * g.sbcells)) ||
         (st = dalloc(ctx, &d.list_gid, (size_t)g.nranks * g.sbcells)) ||
         (st = dalloc(ctx, &d.dc_tmp, (size_t)g.nranks * (g.sbcells + 101))) ||
-        (st = dalloc(ctx, &d.red, 2 * RED_BLOCKS + 1)) || (st = dalloc(ctx, &d.act_scratch, 4 * g.nranks)) ||
+        (st = dalloc(ctx, &d.red, 2 * RED_BLOCKS + 1)) || (st = dalloc(ctx, &d.fs_part, 2 * stencil_parts_max(g) + 1)) ||
+        (st = dalloc(ctx, &d.act_scratch, 4 * g.nranks)) ||
         (st = dalloc(ctx, &d.rng_used, g.nranks)) || (st = dalloc(ctx, &d.rng_base, g.nranks)) ||
         (st = dalloc(ctx, &d.grain_rot, 9 * (p.maxTotalGrains + 1))) ||
         (st = dalloc(ctx, &d.grain_log, p.maxTotalGrains + 2)))
@@ -1218,7 +1231,7 @@ mms_status mms_set_grains(mms_ctx *ctx, int n, const double *rotmat9)
 {
     if (!ctx || n < 0 || (n && !rotmat9)) return MMS_ERR_ARG;
     if (ctx->stepped) return MMS_ERR_STATE;
-    ctx->ctl_known = false;
+    ctx->ctl_known = ctx->fs_part_valid = false;
     if ((uint64_t)n + 1 > ctx->p.maxTotalGrains + 1) return MMS_ERR_GRAIN_OVERFLOW;
     cudaSetDevice(ctx->device);
     mms_status st = read_ctl(ctx);
@@ -1311,8 +1324,14 @@ mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxy
     return MMS_OK;
 }
 
-mms_status mms_step(mms_ctx *ctx, int nsteps)
+// nsteps steps.  fold_fs: the last step runs the stencil that leaves
+// per-tile fraction-solid sums, which are folded and copied to ctx->h_red
+// before the closing control-block read, so one synchronisation covers
+// both; *folded says whether that copy holds the fields as they stand (not
+// after a stall, whose resumed steps come later).
+static mms_status step_impl(mms_ctx *ctx, int nsteps, bool fold_fs, bool *folded)
 {
+    *folded = false;
     if (!ctx || nsteps < 0) return MMS_ERR_ARG;
     if (ctx->nslabs > 1) {
         ctx->err = "a slab of a split domain steps with its group (mms_slab_group_step, mms_slab_launch)";
@@ -1325,25 +1344,33 @@ mms_status mms_step(mms_ctx *ctx, int nsteps)
     mms_status st = MMS_OK;
     // the previous step call ended by reading the control block
     if (!ctx->ctl_known && (st = read_ctl(ctx))) return st;
-    ctx->ctl_known = false;
+    ctx->ctl_known = ctx->fs_part_valid = false;
     if (ctx->h_ctl->status) return (mms_status)ctx->h_ctl->status;
     unsigned long long ts0 = ctx->h_ctl->timestep;
     while (done < nsteps) {
         int n = std::min(chunk, nsteps - done);
+        const long long nparts = stencil_parts(ctx->ka, ctx->tma);
+        bool fold_now = fold_fs && done + n >= nsteps && nparts > 0;
+        const int plain = n - (fold_now ? 1 : 0);  // steps without the sums
         if (ctx->use_graphs && !ctx->prof) {
             if ((st = ensure_graph(ctx))) return st;
             int s = 0;
-            for (; s + GRAPH_STEPS <= n; s += GRAPH_STEPS) {
+            for (; s + GRAPH_STEPS <= plain; s += GRAPH_STEPS) {
                 CU(cudaGraphLaunch(ctx->multi_graph, ctx->stream));
                 ctx->launches += (uint64_t)ctx->step_graph_kernels * GRAPH_STEPS;
             }
-            for (; s < n; s++) {
+            for (; s < plain; s++) {
                 CU(cudaGraphLaunch(ctx->step_graph, ctx->stream));
                 ctx->launches += ctx->step_graph_kernels;
             }
+            if (fold_now) {
+                CU(cudaGraphLaunch(ctx->sum_graph, ctx->stream));
+                ctx->launches += ctx->step_graph_kernels;
+            }
         } else {
-            for (int s = 0; s < n; s++) ctx->launches += launch_one_step(ctx, 0);
+            for (int s = 0; s < n; s++) ctx->launches += launch_one_step(ctx, 0, s >= plain);
         }
+        if (fold_now) ctx->launches += launch_fold_fs(ctx->ka, nparts, ctx->stream, ctx->h_red);
         CU(cudaGetLastError());
         if ((st = read_ctl(ctx))) return st;
         Ctl &c = *ctx->h_ctl;
@@ -1351,6 +1378,8 @@ mms_status mms_step(mms_ctx *ctx, int nsteps)
             ctx->err = mms_status_string((mms_status)c.status);
             return (mms_status)(c.status ? c.status : MMS_ERR_STATE);
         }
+        if (c.stall == STALL_RNG) fold_now = false;
+        *folded = fold_now;
         while (c.stall == STALL_RNG) {
             // a rank ran out of pre-drawn orientations at step stall_step:
             // refill, then resume that step at the activation stage
@@ -1370,7 +1399,57 @@ mms_status mms_step(mms_ctx *ctx, int nsteps)
         if ((st = refill_rng(ctx, false))) return st;
     }
     ctx->ctl_known = true;
+    ctx->fs_part_valid = *folded;
     return MMS_OK;
+}
+
+mms_status mms_step(mms_ctx *ctx, int nsteps)
+{
+    bool folded;
+    return step_impl(ctx, nsteps, false, &folded);
+}
+
+// A sum of the fraction solid (each cell's fs capped at 1) or of ce over
+// the domain, in the unit of `what` (computeFS, solid_volume,
+// loop.c:173-183, growth.c:541-566).
+static double reduce_scaled(const mms_ctx *ctx, mms_reduction what, double s)
+{
+    const mms_params &p = ctx->p;
+    const Geo &g = ctx->ka.g;
+    if (what == MMS_REDUCE_CE_SUM) return s;
+    if (what == MMS_REDUCE_SOLID_VOLUME) return s * pow(p.cellSize, 3.0);
+    return (s * pow(p.cellSize, 3.0)) / ((g.gx * g.gy * g.gz) * pow(p.cellSize, 3));
+}
+
+// The fs sum of the current fields: from the last step's per-tile sums when
+// they are current, else a pass over the field.
+static mms_status fs_sum(mms_ctx *ctx, double *s)
+{
+    const long long nparts = ctx->fs_part_valid ? stencil_parts(ctx->ka, ctx->tma) : 0;
+    if (nparts > 0) {
+        ctx->launches += launch_fold_fs(ctx->ka, nparts, ctx->stream, ctx->h_red);
+        CU(cudaGetLastError());
+        CU(cudaStreamSynchronize(ctx->stream));
+        *s = *ctx->h_red;
+        return MMS_OK;
+    }
+    ctx->launches += launch_reduce(ctx->ka, ctx->prec, 0, s, ctx->stream, ctx->h_red);
+    CU(cudaGetLastError());
+    return MMS_OK;
+}
+
+mms_status mms_step_reduce(mms_ctx *ctx, int nsteps, mms_reduction what, double *out)
+{
+    if (!ctx || !out) return MMS_ERR_ARG;
+    const bool fs = what != MMS_REDUCE_CE_SUM;
+    bool folded = false;
+    mms_status st = step_impl(ctx, nsteps, fs, &folded);
+    if (st) return st;
+    if (folded) {
+        *out = reduce_scaled(ctx, what, *ctx->h_red);
+        return MMS_OK;
+    }
+    return mms_reduce(ctx, what, out);
 }
 
 mms_status mms_get_timestep(mms_ctx *ctx, uint64_t *timestep)
@@ -1467,6 +1546,7 @@ mms_status mms_upload(mms_ctx *ctx, mms_field field, const void *host)
 {
     if (!ctx || !host) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
+    ctx->fs_part_valid = false;
     const Geo &g = ctx->ka.g;
     const size_t N = (size_t)g.N;
     mms_status st;
@@ -1519,14 +1599,14 @@ mms_status mms_reduce(mms_ctx *ctx, mms_reduction what, double *out)
     if (!ctx || !out) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     double s = 0;
-    ctx->launches += launch_reduce(ctx->ka, ctx->prec, what == MMS_REDUCE_CE_SUM ? MMS_REDUCE_CE_SUM : 0, &s, ctx->stream,
-                                   ctx->h_red);
-    CU(cudaGetLastError());
-    const mms_params &p = ctx->p;
-    const Geo &g = ctx->ka.g;
-    if (what == MMS_REDUCE_CE_SUM) *out = s;
-    else if (what == MMS_REDUCE_SOLID_VOLUME) *out = s * pow(p.cellSize, 3.0);
-    else *out = (s * pow(p.cellSize, 3.0)) / ((g.gx * g.gy * g.gz) * pow(p.cellSize, 3));
+    if (what == MMS_REDUCE_CE_SUM) {
+        ctx->launches += launch_reduce(ctx->ka, ctx->prec, MMS_REDUCE_CE_SUM, &s, ctx->stream, ctx->h_red);
+        CU(cudaGetLastError());
+    } else {
+        mms_status st = fs_sum(ctx, &s);
+        if (st) return st;
+    }
+    *out = reduce_scaled(ctx, what, s);
     return MMS_OK;
 }
 
@@ -1760,7 +1840,7 @@ mms_status mms_adjoint_release(mms_ctx *ctx)
 
 mms_status mms_adjoint_record(mms_ctx *ctx, int nsteps, int checkpoint_every)
 {
-    if (ctx) ctx->ctl_known = false;
+    if (ctx) ctx->ctl_known = ctx->fs_part_valid = false;
     if (!ctx || nsteps < 1 || checkpoint_every < 1 || ctx->nslabs > 1) return MMS_ERR_ARG;
     if (ctx->ka.p.temp_mode == 2) {
         ctx->err = "the adjoint supports the analytic temperature models only";
@@ -1810,6 +1890,7 @@ mms_status mms_adjoint_replay_loss(mms_ctx *ctx, const double *target_ce, const 
     if (!ctx || !target_ce || !scale || !loss) return MMS_ERR_ARG;
     if (!ctx->adj.nrec) return MMS_ERR_STATE;
     cudaSetDevice(ctx->device);
+    ctx->fs_part_valid = false;
     const Geo &g = ctx->ka.g;
     const size_t N = (size_t)g.N, es = elem_size(ctx);
     const mms_ctx::AdjRec &r = ctx->adj;
@@ -1865,6 +1946,7 @@ mms_status mms_adjoint_gradient(mms_ctx *ctx, const double *target_ce, mms_adjoi
     if (!ctx || !target_ce || !out) return MMS_ERR_ARG;
     if (!ctx->adj.nrec) return MMS_ERR_STATE;
     cudaSetDevice(ctx->device);
+    ctx->fs_part_valid = false;
     const Geo &g = ctx->ka.g;
     const size_t N = (size_t)g.N, es = elem_size(ctx);
     const mms_ctx::AdjRec &r = ctx->adj;
@@ -2198,7 +2280,7 @@ mms_status mms_batch_step(mms_batch *b, int nsteps)
     mms_status st;
     const size_t nd = b->doms.size();
     for (mms_ctx *ctx : b->doms) {
-        ctx->ctl_known = false;
+        ctx->ctl_known = ctx->fs_part_valid = false;
         if ((st = read_ctl(ctx))) return st;
         if (ctx->h_ctl->status) return (mms_status)ctx->h_ctl->status;
         ctx->stepped = true;
@@ -2486,7 +2568,7 @@ mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path)
 
 mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path)
 {
-    if (ctx) ctx->ctl_known = false;
+    if (ctx) ctx->ctl_known = ctx->fs_part_valid = false;
     if (!ctx || !path) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     mms_status st = read_ctl(ctx);
@@ -2667,7 +2749,7 @@ void slab_plan(mms_ctx *ctx, int point, unsigned long long ts, std::vector<mms_s
 mms_status slab_launch(mms_ctx *ctx, int phase, int resume)
 {
     cudaSetDevice(ctx->device);
-    ctx->ctl_known = false;
+    ctx->ctl_known = ctx->fs_part_valid = false;
     if (phase == 0 && !resume && ctx->p.am)
         ctx->launches += launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, ctx->stream, nullptr);
     ctx->launches += launch_slab_phase(ctx->ka, ctx->tma, ctx->prec, ctx->stream, phase, resume);
@@ -2814,7 +2896,7 @@ mms_status mms_slab_poll(mms_ctx *ctx, uint64_t *timestep, int *stalled)
 mms_status mms_slab_refill(mms_ctx *ctx)
 {
     if (!ctx) return MMS_ERR_ARG;
-    ctx->ctl_known = false;
+    ctx->ctl_known = ctx->fs_part_valid = false;
     cudaSetDevice(ctx->device);
     mms_status st = read_ctl(ctx);
     if (st) return st;

@@ -192,6 +192,7 @@ struct DevPtrs {
     Dc3 *dc_tmp;            // per-rank regions, 1-based slots
     // reductions
     double *red;            // scratch for partial sums
+    double *fs_part;        // per stencil tile: (sum of the new fs, 0), then the folded total
     Ctl *ctl;
     // z-slab split of one domain (nslabs > 1): this slab's index, the
     // whole-domain number of its first emulated rank, the capacity of its
@@ -249,8 +250,10 @@ struct Profiler {
 // Launchers implemented in kernels.cu.  Each returns the number of kernels
 // it launched.
 // start_stage 0: whole step; 1: resume at grain activation (after a stall).
+// sumfs: the TMA stencil also leaves its per-tile fraction-solid sums in
+// a.d.fs_part (see stencil_parts).
 int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *stream, int start_stage,
-                Profiler *prof);
+                Profiler *prof, bool sumfs = false);
 // Builds the TMA descriptors of the stencil for the current buffers;
 // returns 0 when the driver cannot encode them (the stencil then uses its
 // plain-load variant).
@@ -294,6 +297,14 @@ int am_tc_prepare();
 int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof);
 constexpr int RED_BLOCKS = 148 * 8;  // partial sums of k_reduce (red holds 2 per block + 1)
 int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream, double *pinned);
+// The TMA stencil launched with sumfs leaves each tile's sum of the new
+// fraction solid in a.d.fs_part: stencil_parts is the tile count of the
+// current launch (0 when the step runs another variant), stencil_parts_max
+// the most any tile choice gives; launch_fold_fs folds them and copies the
+// total to pinned memory (the caller synchronises).
+long long stencil_parts(const KernelArgs &a, const TmaHolder &tma);
+long long stencil_parts_max(const Geo &g);
+int launch_fold_fs(const KernelArgs &a, long long nparts, void *stream, double *pinned);
 int launch_fill_temperature(const KernelArgs &a, double *dev_out, void *stream);
 int launch_compute_d(const KernelArgs &a, int precision, double *dev_out, void *stream);
 int launch_repack(void *dst, long long dst_pitch, const void *src, long long src_pitch, int row_bytes, long long rows,
