@@ -524,7 +524,8 @@ __device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
     const long long num_grains = ctl->num_grains;
     act_assign(a, C, num_grains, ts, first, nullptr);
     __syncthreads();
-    for (int r = threadIdx.x; r < nr; r += ACT_NT) a.d.rng_used[r] += need[r];
+    for (int r = threadIdx.x; r < nr; r += ACT_NT)
+        if (need[r]) atomicMax(&ctl->rng_used_max, a.d.rng_used[r] += need[r]);
     if (threadIdx.x == 0) {
         ctl->num_grains = (int)(num_grains + C);
         ctl->new_grains = C;
@@ -600,7 +601,8 @@ __global__ void __launch_bounds__(ACT_NT) k_act_slab(KernelArgs a)
         const int *need = a.d.act_scratch, *first = a.d.act_scratch + nr;
         act_assign(a, C, num_grains + off, ts, first, a.d.x2_send);
         __syncthreads();
-        for (int r = threadIdx.x; r < nr; r += ACT_NT) a.d.rng_used[r] += need[r];
+        for (int r = threadIdx.x; r < nr; r += ACT_NT)
+            if (need[r]) atomicMax(&ctl->rng_used_max, a.d.rng_used[r] += need[r]);
     }
     if (threadIdx.x == 0) {
         ctl->num_grains = (int)(num_grains + total);

@@ -372,9 +372,11 @@ mms_status refill_rng(mms_ctx *ctx, bool force)
     const Geo &g = ctx->ka.g;
     DevPtrs &d = ctx->ka.d;
     if (!ctx->p.gnUseOrientation) return MMS_OK;
-    // draws are consumed only by new grains: nothing to check otherwise
+    // draws are consumed only by new grains: nothing to check otherwise;
+    // no rank past half its table: no refill yet
     if (!force && ctx->h_ctl->num_grains == ctx->rng_checked_grains) return MMS_OK;
     ctx->rng_checked_grains = ctx->h_ctl->num_grains;
+    if (!force && (long long)ctx->h_ctl->rng_used_max * 2 <= d.rng_cap) return MMS_OK;
     std::vector<int> used(g.nranks);
     CU(d2h(ctx, used.data(), d.rng_used, sizeof(int) * g.nranks));
     bool any = force;
@@ -406,6 +408,8 @@ mms_status refill_rng(mms_ctx *ctx, bool force)
     CU(h2d(ctx, d.rng_rot, tab.data(), tab.size() * sizeof(double)));
     CU(h2d(ctx, d.rng_base, base.data(), sizeof(long long) * g.nranks));
     CU(dzero(ctx, d.rng_used, sizeof(int) * g.nranks));
+    CU(dzero(ctx, &d.ctl->rng_used_max, sizeof(int)));
+    ctx->h_ctl->rng_used_max = 0;
     return MMS_OK;
 }
 

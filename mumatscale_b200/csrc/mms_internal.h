@@ -31,7 +31,7 @@ struct Ctl {
     int list_total;               // interface-list length over all ranks this step
     int list_ticket;              // k_list blocks started this step
     int new_grains;               // grains created by the last activation
-    int pad0;
+    int rng_used_max;             // the most draws any rank consumed since the last refill
 };
 
 enum StallReason : int {
