@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 
 #include "device_common.cuh"
 #include "mms_internal.h"
@@ -1742,50 +1743,58 @@ __global__ void __launch_bounds__(LIST_NT) k_capture_batch(const void *items, si
 // ------------------------------------------------------------ reductions
 constexpr int RED_NT = 256;
 // Per-block partial sums over interior cells of min(1, fs) (reduce_fs,
-// growth.c:541-566) or of ce (TwoSum-compensated).
+// growth.c:541-566) or of ce.  A warp per interior row at a time: the lanes
+// load the row's 16-byte vectors from element VEC on (rows start on a
+// 64-byte boundary, so these are aligned), and the head (elements 1 ..
+// VEC-1) and tail (after the last whole vector) one element per lane.  Each
+// lane adds its values plainly and enters the row's total into its running
+// sum with compensation (TwoSum).  A warp issues every load of a row before
+// adding (four or more 16-byte loads per lane in flight).
 template <typename Real>
 __global__ void __launch_bounds__(RED_NT) k_reduce(KernelArgs a, int what, double *partial)
 {
+    typedef typename std::conditional<sizeof(Real) == 8, double2, float4>::type V;
+    constexpr int VEC = 16 / (int)sizeof(Real);
     const Ctl *ctl = a.d.ctl;
     const Geo &g = a.g;
     const int cur = (int)(ctl->timestep & 1ULL);
     const Real *f = (what == MMS_REDUCE_CE_SUM) ? (const Real *)a.d.ce : (const Real *)a.d.fs[cur];
-    const long long rows = (long long)g.gy * g.gz;
-    double s = 0.0, comp = 0.0;
-    auto add = [&](double x) {
-        double t = s + x;                          // TwoSum
-        double bp = t - s;
-        comp += (s - (t - bp)) + (x - bp);
-        s = t;
-    };
-    // a block per interior row at a time (four rows' loads in flight), the
-    // threads along x.  The four values a thread loads together are summed
-    // pairwise and the group enters the running sum with compensation (the
-    // FP64 pipe, not memory, bounded the kernel with one TwoSum per value).
-    constexpr int U = 4;
-    // rows number fewer than 2^32: (k, j) of a row by a 32-bit
-    // multiply-high division (a 64-bit division per row cost more than the
-    // sums)
+    const bool cap = what != MMS_REDUCE_CE_SUM;
+    const unsigned rows = (unsigned)((long long)g.gy * g.gz);  // fewer than 2^32
+    const int lane = threadIdx.x & 31;
+    const unsigned warp = (blockIdx.x * RED_NT + threadIdx.x) >> 5, nwarps = (gridDim.x * RED_NT) >> 5;
+    const int gx = g.gx;
+    const int nfull = max(0, (gx + 1) / VEC - 1);        // vectors covering [VEC, VEC (nfull + 1))
+    const int nhead = min(VEC - 1, gx), tail0 = VEC * (nfull + 1), ntail = max(0, gx - tail0 + 1);
+    // this lane's head or tail element (0: none)
+    const int lone = lane < nhead ? 1 + lane : (lane - nhead < ntail ? tail0 + lane - nhead : 0);
     const unsigned gy = (unsigned)g.gy, gy_m = gy <= 1 ? 0xffffffffu : (unsigned)((1ULL << 32) / gy);
-    for (long long r0 = (long long)blockIdx.x * U; r0 < rows; r0 += (long long)gridDim.x * U) {
-        const Real *row[U];
+    auto val = [&](Real v) -> double { return (double)((cap && (Real)1 < v) ? (Real)1 : v); };
+    double s = 0.0, comp = 0.0;
+    for (unsigned r = warp; r < rows; r += nwarps) {
+        unsigned jj;
+        const unsigned kk = fast_divmod(r, gy, gy_m, jj);
+        const Real *row = f + (long long)(kk + 1) * g.sz + (long long)(jj + 1) * g.sy;
+        const V *vrow = (const V *)(row + VEC);
+        double acc = lone ? val(__ldg(row + lone)) : 0.0;
+        // the same trip count in every lane: loads past the row's last
+        // vector are predicated off and read as zeros
+        for (int p0 = 0; p0 < nfull; p0 += 128) {
+            V x[4];
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-            const unsigned r = (unsigned)(r0 + u < rows ? r0 + u : r0);
-            unsigned jj;
-            const unsigned kk = fast_divmod(r, gy, gy_m, jj);
-            row[u] = f + (long long)(kk + 1) * g.sz + (long long)(jj + 1) * g.sy;
-        }
-        for (int i = 1 + (int)threadIdx.x; i <= g.gx; i += RED_NT) {
-            double x[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                double v = (double)row[u][i];
-                if (what != MMS_REDUCE_CE_SUM) v = (1.0 < v) ? 1.0 : v;
-                x[u] = (r0 + u < rows) ? v : 0.0;
+            for (int k = 0; k < 4; k++) {
+                const int p = p0 + lane + 32 * k;
+                if (p < nfull) x[k] = __ldg(vrow + p);
+                else std::memset(&x[k], 0, sizeof(V));
             }
-            add((x[0] + x[1]) + (x[2] + x[3]));
+            const Real *e0 = (const Real *)&x[0], *e1 = (const Real *)&x[1], *e2 = (const Real *)&x[2],
+                       *e3 = (const Real *)&x[3];
+#pragma unroll
+            for (int e = 0; e < VEC; e++) acc += (val(e0[e]) + val(e1[e])) + (val(e2[e]) + val(e3[e]));
         }
+        const double t = s + acc, bp = t - s;  // TwoSum
+        comp += (s - (t - bp)) + (acc - bp);
+        s = t;
     }
     __shared__ double ss[RED_NT], sc[RED_NT];
     ss[threadIdx.x] = s;
@@ -2326,10 +2335,27 @@ int launch_fold_fs(const KernelArgs &a, long long nparts, void *stream, double *
     return 1;
 }
 
+// Blocks of k_reduce that are resident at once (at most RED_BLOCKS): every
+// warp then takes the same number of rows, give or take one.
+template <typename Real>
+static int reduce_grid()
+{
+    static int nb = 0;
+    if (!nb) {
+        int per_sm = 0, dev = 0, sms = 148;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_reduce<Real>, RED_NT, 0);
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        nb = (per_sm > 0 ? per_sm : 1) * sms;
+        if (nb > RED_BLOCKS) nb = RED_BLOCKS;
+    }
+    return nb;
+}
+
 int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream, double *pinned)
 {
     cudaStream_t st = (cudaStream_t)stream;
-    const int nb = RED_BLOCKS;
+    const int nb = precision == MMS_PREC_F32 ? reduce_grid<float>() : reduce_grid<double>();
     double *partial = a.d.red;
     if (precision == MMS_PREC_F32) k_reduce<float><<<nb, RED_NT, 0, st>>>(a, what, partial);
     else k_reduce<double><<<nb, RED_NT, 0, st>>>(a, what, partial);

@@ -98,3 +98,17 @@ def test_fraction_with_per_kernel_timing(built, cuda_device):
         b.set_profiling(True)
         assert a.step_reduce(50, "fs_fraction") == b.step_reduce(50, "fs_fraction")
         assert _close(b.reduce("fs_fraction"), _field_fraction(b))
+
+
+@pytest.mark.parametrize("prec", [M.PREC_F64, M.PREC_F32])
+@pytest.mark.parametrize("sdimx", [5, 15, 33, 67])
+def test_field_pass_ragged_rows(built, cuda_device, prec, sdimx):
+    """The field pass over rows whose length is not a multiple of the
+    16-byte vector: head and tail elements are each counted once."""
+    p = M.read_deck(golden_deck("small4"))
+    p.gsdimx = sdimx
+    with M.Domain(p, precision=prec) as dom:
+        dom.step(40)
+        assert _close(dom.reduce("fs_fraction"), _field_fraction(dom))
+        ce = dom.download("ce")[1:-1, 1:-1, 1:-1]
+        assert abs(dom.reduce("ce_sum") / float(np.sum(ce)) - 1) < 1e-12
