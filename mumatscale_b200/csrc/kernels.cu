@@ -1771,31 +1771,59 @@ __global__ void __launch_bounds__(RED_NT) k_reduce(KernelArgs a, int what, doubl
     const unsigned gy = (unsigned)g.gy, gy_m = gy <= 1 ? 0xffffffffu : (unsigned)((1ULL << 32) / gy);
     auto val = [&](Real v) -> double { return (double)((cap && (Real)1 < v) ? (Real)1 : v); };
     double s = 0.0, comp = 0.0;
-    for (unsigned r = warp; r < rows; r += nwarps) {
+    // units of work: (row, chunk of up to 128 vectors); a warp walks its
+    // rows' units in order with the next unit's loads in flight while it
+    // adds the current one (two register buffers, used in turn)
+    const int nchunks = max(1, (nfull + 127) / 128);
+    struct Buf {
+        V x[4];
+        Real lone;
+    };
+    auto load = [&](unsigned r, int c, Buf &b) {
         unsigned jj;
         const unsigned kk = fast_divmod(r, gy, gy_m, jj);
         const Real *row = f + (long long)(kk + 1) * g.sz + (long long)(jj + 1) * g.sy;
         const V *vrow = (const V *)(row + VEC);
-        double acc = lone ? val(__ldg(row + lone)) : 0.0;
-        // the same trip count in every lane: loads past the row's last
-        // vector are predicated off and read as zeros
-        for (int p0 = 0; p0 < nfull; p0 += 128) {
-            V x[4];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int p = p0 + lane + 32 * k;
-                if (p < nfull) x[k] = __ldg(vrow + p);
-                else std::memset(&x[k], 0, sizeof(V));
-            }
-            const Real *e0 = (const Real *)&x[0], *e1 = (const Real *)&x[1], *e2 = (const Real *)&x[2],
-                       *e3 = (const Real *)&x[3];
-#pragma unroll
-            for (int e = 0; e < VEC; e++) acc += (val(e0[e]) + val(e1[e])) + (val(e2[e]) + val(e3[e]));
+        for (int k = 0; k < 4; k++) {
+            const int p = 128 * c + lane + 32 * k;
+            if (p < nfull) b.x[k] = __ldg(vrow + p);
+            else std::memset(&b.x[k], 0, sizeof(V));
         }
+        b.lone = (c == 0 && lone) ? __ldg(row + lone) : (Real)0;
+    };
+    auto add_unit = [&](const Buf &b) {
+        const Real *e0 = (const Real *)&b.x[0], *e1 = (const Real *)&b.x[1], *e2 = (const Real *)&b.x[2],
+                   *e3 = (const Real *)&b.x[3];
+        double acc = val(b.lone);
+#pragma unroll
+        for (int e = 0; e < VEC; e++) acc += (val(e0[e]) + val(e1[e])) + (val(e2[e]) + val(e3[e]));
         const double t = s + acc, bp = t - s;  // TwoSum
         comp += (s - (t - bp)) + (acc - bp);
         s = t;
-    }
+    };
+    unsigned r = warp;
+    int c = 0;
+    Buf A, B;
+    if (r < rows) load(r, c, A);
+    // one unit: start loading the next into nb, then add cb
+    auto unit = [&](Buf &cb, Buf &nb) -> bool {
+        int cn = c + 1;
+        unsigned rn = r;
+        if (cn == nchunks) {
+            cn = 0;
+            rn = r + nwarps;
+        }
+        const bool more = rn < rows;
+        if (more) load(rn, cn, nb);
+        add_unit(cb);
+        r = rn;
+        c = cn;
+        return more;
+    };
+    if (r < rows)
+        while (unit(A, B) && unit(B, A)) {
+        }
     __shared__ double ss[RED_NT], sc[RED_NT];
     ss[threadIdx.x] = s;
     sc[threadIdx.x] = comp;
