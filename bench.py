@@ -411,9 +411,16 @@ def profile_arm(args) -> None:
         cpt, zc = (int(v) for v in args.tile.split(","))
         dom.set_stencil_tile(cpt, zc)
     dom.step(args.warmup + args.steps)
+    # --reduce R: R rounds of a step with the fraction-solid tile sums
+    # (mms_step_reduce), a plain step and a field pass (mms_reduce)
+    fs = []
+    for _ in range(args.reduce):
+        summed = dom.step_reduce(1, "fs_fraction")
+        dom.step(1)
+        fs.append((summed, dom.reduce("fs_fraction")))
     print(json.dumps({"profile": args.profile, "workload": args.workload, "cells": ncell,
-                      "steps": args.warmup + args.steps, "grains": dom.num_grains, "tma": dom.uses_tma,
-                      "tile": dom.stencil_tile()}))
+                      "steps": args.warmup + args.steps + 2 * args.reduce, "grains": dom.num_grains,
+                      "tma": dom.uses_tma, "tile": dom.stencil_tile(), "fs_fraction": fs}))
     dom.close()
 
 
@@ -752,6 +759,8 @@ def main() -> None:
     ap.add_argument("--profile", choices=["f64", "f32"], default=None,
                     help="run the workload for an ncu capture only")
     ap.add_argument("--cells", type=int, default=N_CELL, help="edge of the cubic domain (profile mode)")
+    ap.add_argument("--reduce", type=int, default=0,
+                    help="profile mode: rounds of (step with tile sums, plain step, field reduction) after the steps")
     ap.add_argument("--tile", default="auto", help="profile mode: stencil tile 'cells_per_thread,zchunk'")
     ap.add_argument("--workload", default="ds256", choices=["ds256", "adjoint", "am", "ensemble", "slabs"],
                     help="ds256: the headline directional-solidification run (default); adjoint, am, "

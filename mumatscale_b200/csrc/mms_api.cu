@@ -1737,13 +1737,18 @@ mms_status mms_run(mms_ctx *ctx, int verbose)
             n = std::min<uint64_t>(n, t - ts);
         }
         if (n > (1ULL << 30)) n = 1ULL << 30;
-        if ((st = mms_step(ctx, (int)n))) return st;
+        // a chunk that ends on a screen step also sums the fraction solid
+        const bool screen_step = p.screenpfreq > 0 && (ts + n) % (uint64_t)p.screenpfreq == 0;
+        double fs_now = fs;
+        if (screen_step) st = mms_step_reduce(ctx, (int)n, MMS_REDUCE_FS_FRACTION, &fs_now);
+        else st = mms_step(ctx, (int)n);
+        if (st) return st;
         ts += n;
         if (data && ts >= (uint64_t)p.data_write_start && ts % (uint64_t)p.data_write_freq == 0 &&
             (st = write_data()))
             return st;
-        if (p.screenpfreq > 0 && ts % (uint64_t)p.screenpfreq == 0) {
-            if ((st = mms_reduce(ctx, MMS_REDUCE_FS_FRACTION, &fs))) return st;
+        if (screen_step) {
+            fs = fs_now;
             if (verbose) screen(fs);
         }
         bool done = false;
