@@ -99,17 +99,61 @@ GNOriented 1
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML read from a thread every 5 ms (the device found by its PCI
+    bus id), else nvidia-smi every 100 ms.  Reads only; changes nothing."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.proc = None
         self.lines: list[str] = []
+        self.nvml = None
+        self.samples: list[tuple[float, float, set]] = []  # (sm MHz, max MHz, reasons)
+        self._stop = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        import torch
+        pr = torch.cuda.get_device_properties(self.gpu)
+        try:
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            pass
+        try:
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(pr.uuid))
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def _poll(self):
+        nv, h = self.nvml
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self._stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((sm, mx, {k for k, b in bits.items() if r & b}))
+            except Exception:
+                pass
+            self._stop.wait(0.005)
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self._t = threading.Thread(target=self._poll, daemon=True)
+            self._t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
@@ -125,6 +169,9 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        self._stop.set()
+        if self.nvml:
+            self._t.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -134,7 +181,10 @@ class ClockSampler:
 
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s, m, r in self.samples:
+            sm.append(s)
+            mx = m
+            reasons |= r
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
@@ -144,11 +194,12 @@ class ClockSampler:
                 mx = float(parts[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+            for nm, v in zip(self.NAMES, parts[5:9]):
                 if v.lower() in ("active", "1"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 # --------------------------------------------------------------- helpers

@@ -49,8 +49,11 @@ typedef enum mms_status {
     MMS_ERR_TIMEOUT = 9,         /* a bounded device-side wait expired */
     MMS_ERR_STATE = 10,          /* call made in the wrong state */
     MMS_ERR_NOMEM = 11,          /* device or host allocation failed */
-    MMS_ERR_SCRATCH_LIMIT = 12   /* grid larger than the fixed device scratch of
+    MMS_ERR_SCRATCH_LIMIT = 12,  /* grid larger than the fixed device scratch of
                                     mms_reduce_field_noalloc (2^30 interior cells) */
+    MMS_ERR_BOUNDS = 13          /* a kernel index outside its buffer (only the
+                                    bounds-checked build, libmms_b200_bounds.so,
+                                    checks; the access is skipped) */
 } mms_status;
 
 typedef enum mms_precision {

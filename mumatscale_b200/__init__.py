@@ -143,7 +143,10 @@ _LIB = None
 
 
 def library_path() -> Path:
-    return _PKG / "libmms_b200.so"
+    """The in-tree libmms_b200.so, or the library MMS_LIBRARY names (for
+    instance the bounds-checked build, libmms_b200_bounds.so)."""
+    alt = os.environ.get("MMS_LIBRARY")
+    return Path(alt) if alt else _PKG / "libmms_b200.so"
 
 
 def load_library(build_if_missing: bool = True) -> C.CDLL:

@@ -1,12 +1,16 @@
 """Builds the in-tree native artifacts of mumatscale_b200.
 
-    libmms_b200.so   the C-ABI library (include/mms.h): sm_100a kernels and
-                     the host side, CUDA runtime linked statically
-    mmsb200          the command-line driver (ca_main.c interface)
+    libmms_b200.so         the C-ABI library (include/mms.h): sm_100a kernels
+                           and the host side, CUDA runtime linked statically
+    libmms_b200_bounds.so  the same with kernel index checks (-DMMS_BOUNDS):
+                           an index outside its buffer raises MMS_ERR_BOUNDS
+                           and the access is skipped; selected at run time by
+                           MMS_LIBRARY=<path> (tests/test_bounds.py)
+    mmsb200                the command-line driver (ca_main.c interface)
 
 Everything is compiled for sm_100a only.  Device code is compiled with
 -fmad=false so FP64 results match the reference's x86-64 build bit for bit.
-Usage:  python -m mumatscale_b200.build  [--force]
+Usage:  python -m mumatscale_b200.build  [--force] [--bounds]
 """
 from __future__ import annotations
 
@@ -21,6 +25,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libmms_b200.so"
+BUILD_BOUNDS = PKG / "_build_bounds"
+LIB_BOUNDS = PKG / "libmms_b200_bounds.so"
 EXE = PKG / "mmsb200"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -45,18 +51,28 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
+def build(force: bool = False, verbose: bool = False, bounds: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + [ROOT / "include" / "mms.h"]
+    if bounds:
+        build(force, verbose)  # the host objects are shared
+        BUILD_BOUNDS.mkdir(exist_ok=True)
     objs = []
     for src in CU_SOURCES:
-        obj = BUILD / (src + ".o")
+        obj = (BUILD_BOUNDS if bounds else BUILD) / (src + ".o")
         if force or _stale(obj, [CSRC / src] + headers):
             cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-fmad=false", "-std=c++17",
                    "-Xcompiler", "-fPIC", "-Xptxas", "-v" if verbose else "-O3",
+                   *(["-DMMS_BOUNDS"] if bounds else []),
                    "-c", str(CSRC / src), "-o", str(obj)]
             _run(cmd)
         objs.append(obj)
+    if bounds:
+        objs += [BUILD / (src + ".o") for src in CXX_SOURCES]
+        if force or _stale(LIB_BOUNDS, objs):
+            _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB_BOUNDS), *map(str, objs),
+                  "-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"])
+        return LIB_BOUNDS
     for src in CXX_SOURCES:
         obj = BUILD / (src + ".o")
         if force or _stale(obj, [CSRC / src] + headers):
@@ -86,4 +102,4 @@ if __name__ == "__main__":
     force = "--force" in sys.argv
     if force and BUILD.exists():
         shutil.rmtree(BUILD)
-    print(build(force=force, verbose="-v" in sys.argv))
+    print(build(force=force, verbose="-v" in sys.argv, bounds="--bounds" in sys.argv))

@@ -19,6 +19,24 @@ __device__ __forceinline__ void raise_error(Ctl *c, int status)
     atomicExch(&c->stall, (int)STALL_ERROR);
 }
 
+// Index check of the bounds-checked build (compiled with -DMMS_BOUNDS): an
+// index outside [0, n) raises MMS_ERR_BOUNDS (the step stops at its next
+// kernel) and the caller skips the access.  The ordinary build compiles the
+// check out.
+__device__ __forceinline__ bool in_bounds(Ctl *c, long long i, long long n)
+{
+#ifdef MMS_BOUNDS
+    if ((unsigned long long)i < (unsigned long long)n) return true;
+    raise_error(c, MMS_ERR_BOUNDS);
+    return false;
+#else
+    (void)c;
+    (void)i;
+    (void)n;
+    return true;
+#endif
+}
+
 
 // direct_temp_calc (temperature.c:24-61) for the analytic models; the AM
 // quadrature is precomputed into an array by k_temp_am.  K is the local

@@ -438,9 +438,13 @@ __device__ __forceinline__ void act_assign(const KernelArgs &a, int C, long long
     const int *ex = a.d.cand_ex;
     for (int i = threadIdx.x; i < C; i += ACT_NT) {
         const int s = a.d.cand[i];
+        if (!in_bounds(a.d.ctl, s, a.d.nsites)) continue;
         const long long cell = a.d.site_cell[s];
         const int r = a.d.site_rank[s];
         const long long id = id0 + i;
+        if (!in_bounds(a.d.ctl, cell, g.N) || !in_bounds(a.d.ctl, r, g.nranks) ||
+            !in_bounds(a.d.ctl, id, (long long)p.max_grains + 1))
+            continue;
         a.d.gr[cell] = (int)id;
         GrainLog lg;
         lg.cell = cell;
@@ -457,6 +461,7 @@ __device__ __forceinline__ void act_assign(const KernelArgs &a, int C, long long
         } else if (p.use_orientation) {
             // this rank's draws before candidate i
             const int k = a.d.rng_used[r] + (ex[i] - ex[first[r]]);
+            if (!in_bounds(a.d.ctl, k, a.d.rng_cap)) continue;
             rot = a.d.rng_rot + ((long long)r * a.d.rng_cap + k) * 9;
             lg.kind = 1;
             lg.aux = a.d.rng_base[r] + k;
@@ -1054,6 +1059,7 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
                 int gr_new, br;
                 cell_update<Real>(q, p, cc[h], fc[h], nb_cl, nb_fs, one_m, interior, oce, grc, Td, a.d.curv, c,
                                   cen, cl_new, fs_new, gr_new, br);
+                if (!in_bounds(ctl, c, g.N)) continue;
                 ce[c] = cen;
                 clO[c] = cl_new;
                 fsO[c] = fs_new;
@@ -1068,7 +1074,10 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
         for (int u = 0; u < CPT; u++) {
             const unsigned word = __ballot_sync(FULL_MASK, solid[u]);
             const int w = bx * CPT + u;
-            if (tx == 0 && jrow && w < g.wpr) a.d.solid_bits[((long long)k * (g.gy + 2) + j) * wrow + w] = word;
+            if (tx == 0 && jrow && w < g.wpr) {
+                const long long wi = ((long long)k * (g.gy + 2) + j) * wrow + w;
+                if (in_bounds(ctl, wi, g.nwords)) a.d.solid_bits[wi] = word;
+            }
         }
         __syncthreads();
         if (sh.abort) {
@@ -1518,7 +1527,9 @@ __device__ __forceinline__ void list_body(const KernelArgs &a, int nblocks)
         while (m) {
             const int bit = __ffs(m) - 1;
             m &= m - 1;
-            a.d.list_cell[p0++] = base[it] + bit;
+            if (in_bounds(ctl, p0, (long long)g.nranks * g.sbcells) && in_bounds(ctl, base[it] + bit, g.N))
+                a.d.list_cell[p0] = base[it] + bit;
+            p0++;
         }
     }
 }
@@ -1629,8 +1640,11 @@ __device__ __forceinline__ void capture_body(const KernelArgs &a, int bid, int n
     const Geo &g = a.g;
     const int total = ctl->list_total;
     const Real *fs = (const Real *)a.d.fs[(int)(ctl->timestep & 1ULL)];
+    Ctl *ctl_w = a.d.ctl;
     for (long long e = bid * (long long)LIST_NT + threadIdx.x; e < total; e += (long long)nb * LIST_NT) {
+        if (!in_bounds(ctl_w, e, (long long)g.nranks * g.sbcells)) break;
         const long long c = a.d.list_cell[e];
+        if (!in_bounds(ctl_w, c, g.N)) continue;
         long long K, J, I;
         if (g.N < 0x7fffffffLL) {  // 32-bit division when every index fits
             const unsigned cu = (unsigned)c, szu = (unsigned)g.sz, syu = (unsigned)g.sy;
@@ -1648,8 +1662,12 @@ __device__ __forceinline__ void capture_body(const KernelArgs &a, int bid, int n
             const int rx = (int)((I - 1) / g.sbx), ry = (int)((J - 1) / g.sby), rz = (int)((K - 1) / g.sbz);
             r = rx + ry * g.nsbx + rz * g.nsbx * g.nsby;
         }
+        if (!in_bounds(ctl_w, I - 1, g.gx) || !in_bounds(ctl_w, J - 1, g.gy) || !in_bounds(ctl_w, K - 1, g.gz) ||
+            !in_bounds(ctl_w, r, g.nranks))
+            continue;
         const int rank_start = a.d.blk_off[(long long)r * g.blocks_per_rank];
         const long long sl = e - rank_start + 1;
+        if (!in_bounds(ctl_w, a.d.rank_dcbase[r] + sl, (long long)g.nranks * (g.sbcells + 101))) continue;
         Dc3 *slot = a.d.dc_tmp + a.d.rank_dcbase[r] + sl;
         Dc3 out;
         const int gid = capture_cell<Real>(a, fs, c, I, J, K, out);

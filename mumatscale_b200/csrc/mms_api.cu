@@ -21,6 +21,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "host_setup.h"
 #include "mms_internal.h"
 #include "sites.h"
@@ -204,6 +206,15 @@ mms_status dalloc(mms_ctx *ctx, T **ptr, size_t count)
     *ptr = (T *)p;
     return MMS_OK;
 }
+
+// NVTX range over a library call or a phase of one (Nsight Systems and
+// other NVTX tools show them; without a tool attached the calls do nothing)
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
 
 constexpr int GRAPH_STEPS = 8;
 
@@ -667,6 +678,7 @@ const char *mms_status_string(mms_status s)
     case MMS_ERR_STATE: return "call made in the wrong state";
     case MMS_ERR_NOMEM: return "out of memory";
     case MMS_ERR_SCRATCH_LIMIT: return "grid larger than the fixed device scratch (at most 2^30 interior cells)";
+    case MMS_ERR_BOUNDS: return "a kernel index outside its buffer (bounds-checked build)";
     }
     return "unknown status";
 }
@@ -724,6 +736,7 @@ mms_status mms_get_stencil_tile(const mms_ctx *ctx, int *cells_per_thread, int *
 // over `reps` launches is kept.
 mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchunk, double *best_ms)
 {
+    Range range("mms_autotune");
     if (ctx) ctx->ctl_known = ctx->fs_part_valid = false;
     if (!ctx || reps < 1) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
@@ -1335,6 +1348,7 @@ mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxy
 // after a stall, whose resumed steps come later).
 static mms_status step_impl(mms_ctx *ctx, int nsteps, bool fold_fs, bool *folded)
 {
+    Range range("mms_step");
     *folded = false;
     if (!ctx || nsteps < 0) return MMS_ERR_ARG;
     if (ctx->nslabs > 1) {
@@ -1376,7 +1390,10 @@ static mms_status step_impl(mms_ctx *ctx, int nsteps, bool fold_fs, bool *folded
         }
         if (fold_now) ctx->launches += launch_fold_fs(ctx->ka, nparts, ctx->stream, ctx->h_red);
         CU(cudaGetLastError());
-        if ((st = read_ctl(ctx))) return st;
+        {
+            Range wait("steps on the device");
+            if ((st = read_ctl(ctx))) return st;
+        }
         Ctl &c = *ctx->h_ctl;
         if (c.stall == STALL_ERROR) {
             ctx->err = mms_status_string((mms_status)c.status);
@@ -1387,6 +1404,7 @@ static mms_status step_impl(mms_ctx *ctx, int nsteps, bool fold_fs, bool *folded
         while (c.stall == STALL_RNG) {
             // a rank ran out of pre-drawn orientations at step stall_step:
             // refill, then resume that step at the activation stage
+            Range stall("orientation refill and resume");
             if ((st = refill_rng(ctx, true))) return st;
             int zero = 0;
             CU(h2d(ctx, &ctx->ka.d.ctl->stall, &zero, sizeof(int)));
@@ -1478,6 +1496,7 @@ mms_status mms_get_num_grains(mms_ctx *ctx, int *num_grains)
 
 mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
 {
+    Range range("mms_download");
     if (!ctx || !host) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     const Geo &g = ctx->ka.g;
@@ -1548,6 +1567,7 @@ mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
 
 mms_status mms_upload(mms_ctx *ctx, mms_field field, const void *host)
 {
+    Range range("mms_upload");
     if (!ctx || !host) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     ctx->fs_part_valid = false;
@@ -1600,6 +1620,7 @@ mms_status mms_upload(mms_ctx *ctx, mms_field field, const void *host)
 
 mms_status mms_reduce(mms_ctx *ctx, mms_reduction what, double *out)
 {
+    Range range("mms_reduce");
     if (!ctx || !out) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     double s = 0;
@@ -1691,6 +1712,7 @@ mms_status mms_output_grains(mms_ctx *ctx, const char *path, mms_grain_summary *
 // 1 screen output, 2 screen output in interactive mode (-i).
 mms_status mms_run(mms_ctx *ctx, int verbose)
 {
+    Range range("mms_run");
     if (!ctx) return MMS_ERR_ARG;
     const mms_params &p = ctx->p;
     const char *leader = (verbose == 2) ? "        \r" : "";
@@ -1849,6 +1871,7 @@ mms_status mms_adjoint_release(mms_ctx *ctx)
 
 mms_status mms_adjoint_record(mms_ctx *ctx, int nsteps, int checkpoint_every)
 {
+    Range range("mms_adjoint_record");
     if (ctx) ctx->ctl_known = ctx->fs_part_valid = false;
     if (!ctx || nsteps < 1 || checkpoint_every < 1 || ctx->nslabs > 1) return MMS_ERR_ARG;
     if (ctx->ka.p.temp_mode == 2) {
@@ -1952,6 +1975,7 @@ mms_status mms_adjoint_replay_loss(mms_ctx *ctx, const double *target_ce, const 
 
 mms_status mms_adjoint_gradient(mms_ctx *ctx, const double *target_ce, mms_adjoint_result *out)
 {
+    Range range("mms_adjoint_gradient");
     if (!ctx || !target_ce || !out) return MMS_ERR_ARG;
     if (!ctx->adj.nrec) return MMS_ERR_STATE;
     cudaSetDevice(ctx->device);
@@ -2284,6 +2308,7 @@ mms_ctx *mms_batch_domain(mms_batch *b, int i)
 
 mms_status mms_batch_step(mms_batch *b, int nsteps)
 {
+    Range range("mms_batch_step");
     if (!b || nsteps < 0) return MMS_ERR_ARG;
     cudaSetDevice(b->device);
     mms_status st;
@@ -2499,6 +2524,7 @@ extern "C" {
 
 mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path)
 {
+    Range range("mms_checkpoint_save");
     if (!ctx || !path) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     mms_status st = read_ctl(ctx);
@@ -2577,6 +2603,7 @@ mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path)
 
 mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path)
 {
+    Range range("mms_checkpoint_load");
     if (ctx) ctx->ctl_known = ctx->fs_part_valid = false;
     if (!ctx || !path) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
@@ -2919,6 +2946,7 @@ mms_status mms_slab_refill(mms_ctx *ctx)
 
 mms_status mms_slab_group_step(mms_ctx *const *slabs, int nslabs, int nsteps)
 {
+    Range range("mms_slab_group_step");
     if (!slabs || nslabs < 1 || nsteps < 0) return MMS_ERR_ARG;
     for (int s = 0; s < nslabs; s++) {
         mms_ctx *c = slabs[s];
@@ -3051,6 +3079,7 @@ extern "C" {
 
 mms_status mms_write_xdmf(mms_ctx *ctx, const char *basename)
 {
+    Range range("mms_write_xdmf");
     if (!ctx || ctx->nslabs > 1) return MMS_ERR_ARG;
     cudaSetDevice(ctx->device);
     const mms_params &p = ctx->p;
