@@ -11,6 +11,9 @@ the library lists (``mms_slab_exchange_plan``):
 * point 1, after the stencil: the fs, gr, dc and solid-bitmask boundary
   planes, and an all-gather of every slab's new grains.
 
+Reductions (fraction solid, solid volume, ce sum) are each slab's own sum
+followed by an all-reduce over the group.
+
 Transports: ``"nccl"`` runs the plane swaps as batched NCCL send/recv and
 the gathers as NCCL all-gathers, straight from device memory on the
 slab's stream; ``"host"`` stages every transfer through host memory, for
@@ -68,6 +71,7 @@ class DistributedSlab:
         import torch
         import torch.distributed as dist
         self.group = group
+        self.params = params
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
         torch.cuda.set_device(device)
@@ -142,6 +146,22 @@ class DistributedSlab:
                 ts = t + 1
                 continue
             ts = t
+
+    def reduce(self, what: str = "fs_fraction") -> float:
+        """The whole domain's value: this slab's sum, then a sum over the
+        group's ranks (computeFS's MPI_Allreduce, loop.c:173-183; the
+        summation order differs from one domain's).  Every rank calls it."""
+        import torch
+        import torch.distributed as dist
+        local = self.dom.reduce("solid_volume" if what == "fs_fraction" else what)
+        dev = self.device if dist.get_backend(self.group) == "nccl" else "cpu"
+        t = torch.tensor([local], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+        v = float(t.item())
+        if what == "fs_fraction":
+            nx, ny, nz = self.params.grid
+            v /= nx * ny * nz * self.params.cellSize ** 3
+        return v
 
     @property
     def timestep(self) -> int:

@@ -41,6 +41,7 @@ def main() -> int:
     out["nuc"] = np.array([[x.nuc_x, x.nuc_y, x.nuc_z, x.nuc_threshold, float(x.nuc_timestep)] for x in g])
     out["z_begin"] = np.array(d.layout.z_begin)
     out["timestep"] = np.array(s.timestep)
+    out["red"] = np.array([s.reduce(w) for w in ("fs_fraction", "solid_volume", "ce_sum")])
     np.savez(os.path.join(a.out, f"slab{dist.get_rank()}.npz"), **out)
     s.close()
     dist.barrier()

@@ -106,6 +106,55 @@ def test_slab_exchange_two_gloo_ranks():
     assert res[0][1] == res[1][1] == [1] * 5 + [2] * 5
 
 
+class _StubSlab:
+    """A slab whose own sums are given: the group reduction alone."""
+
+    def __init__(self, sums: dict):
+        self.sums = sums
+
+    def reduce(self, what: str) -> float:
+        return self.sums[what]
+
+
+def _reduce_rank(rank: int, world: int, port: int, q) -> None:
+    import torch.distributed as dist
+    from mumatscale_b200.slabs import DistributedSlab
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        s = object.__new__(DistributedSlab)
+        p = M.default_params()
+        p.gnsbx, p.gnsby, p.gnsbz = 1, 1, 2
+        p.gsdimx, p.gsdimy, p.gsdimz = 4, 4, 4
+        p.cellSize = 2.0
+        s.group, s.params, s.device = None, p, "cpu"
+        s.dom = _StubSlab({"solid_volume": 8.0 * (rank + 1), "ce_sum": 10.0 + rank})
+        q.put((rank, s.reduce("fs_fraction"), s.reduce("solid_volume"), s.reduce("ce_sum")))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_slab_reductions_two_gloo_ranks():
+    """Each rank's sum all-reduced; the fraction solid from the total solid
+    volume over the whole domain's volume (4 x 4 x 8 cells of 2^3)."""
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_reduce_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = [q.get(timeout=120) for _ in ps]
+    for p in ps:
+        p.join(60)
+        assert p.exitcode == 0
+    for _, fs, vol, ce in res:
+        assert vol == 24.0 and ce == 21.0
+        assert fs == 24.0 / (4 * 4 * 8 * 8.0)
+
+
 # --------------------------------------------------------------------- GPU
 @pytest.mark.gpu
 def test_slabs_match_reference_dumps(built, cuda_device):
@@ -210,7 +259,12 @@ def test_distributed_slabs_host_transport(built, cuda_device, tmp_path):
                 loc = q[f]
                 assert np.array_equal(loc[1:-1], whole[z0 + 1:z0 + loc.shape[0] - 1]), f
         ga = _grain_table(dom.grains())
+        want = [dom.reduce(w) for w in ("fs_fraction", "solid_volume", "ce_sum")]
+        assert want[0] > 0
         for q in parts:
             assert int(q["timestep"]) == steps
             gb = np.concatenate([q["rot"], q["ang"], q["nuc"]], axis=1)
             assert np.array_equal(ga, gb)
+            # the group's all-reduced sums: every rank holds the domain's
+            for got, w in zip(q["red"], want):
+                assert abs(got - w) <= 1e-12 * abs(w), (got, w)
