@@ -1990,16 +1990,17 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
 
 static EncodeTiledFn encode_fn()
 {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    // looked up once, thread-safely (a static initialised by a call), so a
+    // context created on another thread meanwhile never sees a half-done
+    // lookup and falls back to the plain-load stencil
+    static const EncodeTiledFn fn = [] {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn)p;
-    }
+            return (EncodeTiledFn)p;
+        return (EncodeTiledFn) nullptr;
+    }();
     return fn;
 }
 
@@ -2386,15 +2387,15 @@ int launch_fold_fs(const KernelArgs &a, long long nparts, void *stream, double *
 template <typename Real>
 static int reduce_grid()
 {
-    static int nb = 0;
-    if (!nb) {
+    // computed once, thread-safely (a static initialised by a call)
+    static const int nb = [] {
         int per_sm = 0, dev = 0, sms = 148;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_reduce<Real>, RED_NT, 0);
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        nb = (per_sm > 0 ? per_sm : 1) * sms;
-        if (nb > RED_BLOCKS) nb = RED_BLOCKS;
-    }
+        const int v = (per_sm > 0 ? per_sm : 1) * sms;
+        return v < RED_BLOCKS ? v : RED_BLOCKS;
+    }();
     return nb;
 }
 
