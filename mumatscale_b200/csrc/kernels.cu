@@ -2347,7 +2347,9 @@ int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *
 }
 
 // Folds the per-block (sum, compensation) pairs in a fixed order.
-__global__ void __launch_bounds__(1024) k_reduce_fold(double *partial, int nb)
+// Thread 0 gets the total of nb (sum, compensation) pairs, folded in a
+// fixed order; every thread of the 1024 must call it.
+__device__ __forceinline__ double fold_pairs(const double *partial, int nb)
 {
     __shared__ double ss[1024], sc[1024];
     double s = 0, c = 0;
@@ -2369,7 +2371,26 @@ __global__ void __launch_bounds__(1024) k_reduce_fold(double *partial, int nb)
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) partial[2 * nb] = ss[0] + sc[0];
+    return ss[0] + sc[0];
+}
+
+__global__ void __launch_bounds__(1024) k_reduce_fold(double *partial, int nb)
+{
+    const double v = fold_pairs(partial, nb);
+    if (threadIdx.x == 0) partial[2 * nb] = v;
+}
+
+// The same fold, written with the step's control block straight into
+// host memory the device can address (no copies after the kernel).
+__global__ void __launch_bounds__(1024) k_fold_out(const double *partial, int nb, const Ctl *ctl, double *host_sum,
+                                                   Ctl *host_ctl)
+{
+    const double v = fold_pairs(partial, nb);
+    static_assert(sizeof(Ctl) % sizeof(unsigned long long) == 0, "Ctl is copied in 8-byte words");
+    constexpr int W = (int)(sizeof(Ctl) / sizeof(unsigned long long));
+    if (threadIdx.x < W)
+        ((unsigned long long *)host_ctl)[threadIdx.x] = ((const volatile unsigned long long *)ctl)[threadIdx.x];
+    if (threadIdx.x == 0) *host_sum = v;
 }
 
 // Folds the last step's per-tile fraction-solid sums (stencil_parts of
@@ -2379,6 +2400,12 @@ int launch_fold_fs(const KernelArgs &a, long long nparts, void *stream, double *
     cudaStream_t st = (cudaStream_t)stream;
     k_reduce_fold<<<1, 1024, 0, st>>>(a.d.fs_part, (int)nparts);
     cudaMemcpyAsync(pinned, a.d.fs_part + 2 * nparts, sizeof(double), cudaMemcpyDeviceToHost, st);
+    return 1;
+}
+
+int launch_fold_fs_out(const KernelArgs &a, long long nparts, void *stream, double *host_sum, void *host_ctl)
+{
+    k_fold_out<<<1, 1024, 0, (cudaStream_t)stream>>>(a.d.fs_part, (int)nparts, a.d.ctl, host_sum, (Ctl *)host_ctl);
     return 1;
 }
 

@@ -124,6 +124,9 @@ struct mms_ctx {
     int grains_synced = 1;
     Ctl *h_ctl = nullptr;  // pinned
     double *h_red = nullptr;  // pinned reduction result
+    // h_ctl and h_red as the device addresses them (null: copies instead)
+    Ctl *d_hctl = nullptr;
+    double *d_hred = nullptr;
     uint64_t launches = 0;
     bool stepped = false;
     std::string err;
@@ -1055,6 +1058,12 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
     ctx->stream = ctx->own_stream;
     cudaMallocHost((void **)&ctx->h_ctl, sizeof(Ctl));
     cudaMallocHost((void **)&ctx->h_red, sizeof(double));
+    if (!ctx->h_ctl || !ctx->h_red || cudaHostGetDevicePointer((void **)&ctx->d_hctl, ctx->h_ctl, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&ctx->d_hred, ctx->h_red, 0) != cudaSuccess) {
+        ctx->d_hctl = nullptr;
+        ctx->d_hred = nullptr;
+        cudaGetLastError();
+    }
 
     ctx->gg = make_geo(ctx->gp);
     ctx->ka.g = make_geo(p);
@@ -1388,9 +1397,17 @@ static mms_status step_impl(mms_ctx *ctx, int nsteps, bool fold_fs, bool *folded
         } else {
             for (int s = 0; s < n; s++) ctx->launches += launch_one_step(ctx, 0, s >= plain);
         }
-        if (fold_now) ctx->launches += launch_fold_fs(ctx->ka, nparts, ctx->stream, ctx->h_red);
-        CU(cudaGetLastError());
-        {
+        if (fold_now && ctx->d_hctl) {
+            // the fold kernel writes the sum and the control block to host
+            // memory itself: the wait is the only thing left
+            ctx->launches += launch_fold_fs_out(ctx->ka, nparts, ctx->stream, ctx->d_hred, ctx->d_hctl);
+            CU(cudaGetLastError());
+            Range wait("steps on the device");
+            CU(cudaStreamSynchronize(ctx->stream));
+            if (ctx->prof) ctx->prof->collect();
+        } else {
+            if (fold_now) ctx->launches += launch_fold_fs(ctx->ka, nparts, ctx->stream, ctx->h_red);
+            CU(cudaGetLastError());
             Range wait("steps on the device");
             if ((st = read_ctl(ctx))) return st;
         }

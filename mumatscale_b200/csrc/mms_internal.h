@@ -305,6 +305,10 @@ int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out
 long long stencil_parts(const KernelArgs &a, const TmaHolder &tma);
 long long stencil_parts_max(const Geo &g);
 int launch_fold_fs(const KernelArgs &a, long long nparts, void *stream, double *pinned);
+// The same fold, written together with the control block (ctl) straight to
+// pinned host memory through device-usable pointers; the caller
+// synchronises, after which both are current on the host.
+int launch_fold_fs_out(const KernelArgs &a, long long nparts, void *stream, double *host_sum, void *host_ctl);
 int launch_fill_temperature(const KernelArgs &a, double *dev_out, void *stream);
 int launch_compute_d(const KernelArgs &a, int precision, double *dev_out, void *stream);
 int launch_repack(void *dst, long long dst_pitch, const void *src, long long src_pitch, int row_bytes, long long rows,
