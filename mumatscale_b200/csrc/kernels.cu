@@ -2348,10 +2348,11 @@ int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *
 
 // Folds the per-block (sum, compensation) pairs in a fixed order.
 // Thread 0 gets the total of nb (sum, compensation) pairs, folded in a
-// fixed order; every thread of the 1024 must call it.
+// fixed order (strided per thread, then lanes, then the 32 warps, each
+// merge a TwoSum); every thread of the 1024 must call it.
 __device__ __forceinline__ double fold_pairs(const double *partial, int nb)
 {
-    __shared__ double ss[1024], sc[1024];
+    __shared__ double ws[32], wc[32];
     double s = 0, c = 0;
     for (int b = threadIdx.x; b < nb; b += 1024) {
         const double x = partial[2 * b];
@@ -2359,19 +2360,32 @@ __device__ __forceinline__ double fold_pairs(const double *partial, int nb)
         c += (s - (t - bp)) + (x - bp) + partial[2 * b + 1];
         s = t;
     }
-    ss[threadIdx.x] = s;
-    sc[threadIdx.x] = c;
-    __syncthreads();
-    for (int w = 512; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            const double x = ss[threadIdx.x + w];
-            const double t = ss[threadIdx.x] + x, bp = t - ss[threadIdx.x];
-            sc[threadIdx.x] += sc[threadIdx.x + w] + ((ss[threadIdx.x] - (t - bp)) + (x - bp));
-            ss[threadIdx.x] = t;
-        }
-        __syncthreads();
+    auto merge = [&](double x, double xc) {
+        const double t = s + x, bp = t - s;
+        c += xc + ((s - (t - bp)) + (x - bp));
+        s = t;
+    };
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double x = __shfl_down_sync(FULL_MASK, s, o), xc = __shfl_down_sync(FULL_MASK, c, o);
+        merge(x, xc);
     }
-    return ss[0] + sc[0];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        ws[w] = s;
+        wc[w] = c;
+    }
+    __syncthreads();
+    if (w == 0) {
+        s = ws[lane];
+        c = wc[lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double x = __shfl_down_sync(FULL_MASK, s, o), xc = __shfl_down_sync(FULL_MASK, c, o);
+            merge(x, xc);
+        }
+    }
+    return s + c;
 }
 
 __global__ void __launch_bounds__(1024) k_reduce_fold(double *partial, int nb)
