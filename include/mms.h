@@ -51,9 +51,12 @@ typedef enum mms_status {
     MMS_ERR_NOMEM = 11,          /* device or host allocation failed */
     MMS_ERR_SCRATCH_LIMIT = 12,  /* grid larger than the fixed device scratch of
                                     mms_reduce_field_noalloc (2^30 interior cells) */
-    MMS_ERR_BOUNDS = 13          /* a kernel index outside its buffer (only the
+    MMS_ERR_BOUNDS = 13,         /* a kernel index outside its buffer (only the
                                     bounds-checked build, libmms_b200_bounds.so,
                                     checks; the access is skipped) */
+    MMS_ERR_SLAB_CAPACITY = 14   /* a slab's fixed per-step candidate row buffer
+                                    (sized at creation from the sites it holds)
+                                    was too small */
 } mms_status;
 
 typedef enum mms_precision {
@@ -247,9 +250,12 @@ mms_status mms_step_reduce(mms_ctx *ctx, int nsteps, mms_reduction what, double 
  * array of the library: grids above 2^30 interior cells return
  * MMS_ERR_SCRATCH_LIMIT.  The array is shared by all calls on a device, so
  * calls that may overlap on one device (unordered streams, several host
- * threads) race.  The first call on a device looks up the array's address
- * and should come before any stream capture on that device.  Nothing is
- * allocated. */
+ * threads) race.  The array's address is looked up on the first call in
+ * each CUDA context (and again when a call finds another context current on
+ * that device, e.g. after a reset): that first call should come before any
+ * stream capture in the context.  Kernels are launched with
+ * cudaLaunchKernel and its return code checked, so a pending error of the
+ * caller's own CUDA work is not cleared.  Nothing is allocated. */
 mms_status mms_reduce_field_noalloc(const void *field, mms_precision dtype,
                                     int gdimx, int gdimy, int gdimz,
                                     mms_reduction what, double cell_size,

@@ -92,10 +92,12 @@ def build_oracle(reference_present: bool | None = None) -> None:
     """Builds the CPU checkers under oracle/_ref (test infrastructure)."""
     oracle = ROOT / "oracle"
     _run(["make", "-C", str(oracle), "oracle"])
+    # the reference's sources: REF_SRC, the same variable oracle/Makefile reads
+    ref_src = os.environ.get("REF_SRC", "/root/reference/src")
     if reference_present is None:
-        reference_present = Path("/root/reference/src").is_dir()
+        reference_present = Path(ref_src).is_dir()
     if reference_present:
-        _run(["make", "-C", str(oracle), "ref"])
+        _run(["make", "-C", str(oracle), "ref", f"REF_SRC={ref_src}"])
 
 
 if __name__ == "__main__":

@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(ACT_NT) k_act_local(KernelArgs a)
     const int C = ctl->ncand;
     if (threadIdx.x == 0) ctl->list_ticket = 0;
     if (C > a.d.slab_cap) {  // more candidates than the row buffer holds
-        if (threadIdx.x == 0) raise_error(ctl, MMS_ERR_SCRATCH_LIMIT);
+        if (threadIdx.x == 0) raise_error(ctl, MMS_ERR_SLAB_CAPACITY);
         return;
     }
     int short_rng = 0;

@@ -682,6 +682,7 @@ const char *mms_status_string(mms_status s)
     case MMS_ERR_NOMEM: return "out of memory";
     case MMS_ERR_SCRATCH_LIMIT: return "grid larger than the fixed device scratch (at most 2^30 interior cells)";
     case MMS_ERR_BOUNDS: return "a kernel index outside its buffer (bounds-checked build)";
+    case MMS_ERR_SLAB_CAPACITY: return "more nucleation candidates in one step than the slab's row buffer holds";
     }
     return "unknown status";
 }
@@ -1457,7 +1458,7 @@ static double reduce_scaled(const mms_ctx *ctx, mms_reduction what, double s)
     const Geo &g = ctx->ka.g;
     if (what == MMS_REDUCE_CE_SUM) return s;
     if (what == MMS_REDUCE_SOLID_VOLUME) return s * pow(p.cellSize, 3.0);
-    return (s * pow(p.cellSize, 3.0)) / ((g.gx * g.gy * g.gz) * pow(p.cellSize, 3));
+    return (s * pow(p.cellSize, 3.0)) / ((double)((long long)g.gx * g.gy * g.gz) * pow(p.cellSize, 3));
 }
 
 // The fs sum of the current fields: from the last step's per-tile sums when

@@ -20,9 +20,17 @@
 // streams without ordering, or different host threads) share that array and
 // race; calls on one stream are ordered and safe.
 //
-// Set-up.  The array's device address is looked up once per device, on the
-// first call made with that device current, and kept; that first call should
-// come before any stream capture on that device.
+// Set-up.  The array's device address is looked up on the first call made
+// with a device current, and kept together with the CUDA context it belongs
+// to; a call that finds another context current on that device (after a
+// primary-context reset, or under a driver-API context the caller made
+// current) looks the address up again in that context.  The first call in a
+// context should come before any stream capture in it.
+//
+// Errors.  The kernels are launched with cudaLaunchKernel and its return
+// code is checked, so a pending (non-sticky) error of the caller's own CUDA
+// work is neither cleared nor reported as this call's.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -44,7 +52,38 @@ constexpr int NA_MAX_DEVICES = 64;
 static __device__ __align__(256) double na_scratch[2 * NA_MAX_BLOCKS];
 
 std::mutex na_mu;
-double *na_addr[NA_MAX_DEVICES];  // zero-initialised: not looked up yet
+// Per device: the id of the context the address was looked up in (CUDA
+// context ids are unique for the life of the process, so a context made
+// after a reset never matches an older one), and the address.
+unsigned long long na_ctxid[NA_MAX_DEVICES];  // zero-initialised: not looked up yet
+double *na_addr[NA_MAX_DEVICES];
+
+typedef CUresult (*ctx_get_current_fn)(CUcontext *);
+typedef CUresult (*ctx_get_id_fn)(CUcontext, unsigned long long *);
+
+// A driver function through the runtime's driver entry point (the library
+// does not link libcuda directly).  Null when the driver does not offer it.
+void *driver_fn(const char *name)
+{
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+        return nullptr;
+    return p;
+}
+
+// Id of the context current on the calling thread; 0 if none is current or
+// the driver cannot say.
+unsigned long long current_context_id()
+{
+    static ctx_get_current_fn get = (ctx_get_current_fn)driver_fn("cuCtxGetCurrent");
+    static ctx_get_id_fn get_id = (ctx_get_id_fn)driver_fn("cuCtxGetId");
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get || !get_id || get(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // Sum of (s, c) pairs with the error of each addition carried in c
 // (Knuth's TwoSum), so the result does not depend on the field's size.
@@ -124,17 +163,18 @@ __global__ void __launch_bounds__(NA_FIN_NT) k_reduce_na_finish(const double *__
     }
 }
 
-// Device address of na_scratch for the current device, looked up on first use.
+// Device address of na_scratch in the context current on device `dev`:
+// looked up on first use, and again whenever another context is current.
 double *scratch_for(int dev)
 {
     std::lock_guard<std::mutex> lock(na_mu);
-    if (!na_addr[dev]) {
+    const unsigned long long id = current_context_id();
+    if (!na_addr[dev] || !id || id != na_ctxid[dev]) {
         void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, na_scratch) != cudaSuccess || !p) {
-            cudaGetLastError();
-            return nullptr;
-        }
+        // makes the device's primary context current if no context is
+        if (cudaGetSymbolAddress(&p, na_scratch) != cudaSuccess || !p) return nullptr;
         na_addr[dev] = (double *)p;
+        na_ctxid[dev] = current_context_id();
     }
     return na_addr[dev];
 }
@@ -154,24 +194,22 @@ extern "C" mms_status mms_reduce_field_noalloc(const void *field, mms_precision 
     if (nb > NA_MAX_BLOCKS) return MMS_ERR_SCRATCH_LIMIT;
 
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        cudaGetLastError();
-        return MMS_ERR_NO_DEVICE;
-    }
+    if (cudaGetDevice(&dev) != cudaSuccess) return MMS_ERR_NO_DEVICE;
     if (dev < 0 || dev >= NA_MAX_DEVICES) return MMS_ERR_ARG;
     double *partial = scratch_for(dev);
     if (!partial) return MMS_ERR_CUDA;
 
     cudaStream_t st = (cudaStream_t)cuda_stream;
-    const int clamp = (what != MMS_REDUCE_CE_SUM);
-    if (dtype == MMS_PREC_F64)
-        k_reduce_na_partials<double><<<(unsigned)nb, NA_NT, 0, st>>>((const double *)field, gdimx, gdimy,
-                                                                     n, clamp, partial);
-    else
-        k_reduce_na_partials<float><<<(unsigned)nb, NA_NT, 0, st>>>((const float *)field, gdimx, gdimy,
-                                                                    n, clamp, partial);
-    const double vol = std::pow(cell_size, 3.0);
-    k_reduce_na_finish<<<1, NA_FIN_NT, 0, st>>>(partial, (int)nb, (int)what, vol, (double)n, out);
-    if (cudaGetLastError() != cudaSuccess) return MMS_ERR_CUDA;
+    int clamp = (what != MMS_REDUCE_CE_SUM), gx = gdimx, gy = gdimy, nblocks = (int)nb, w = (int)what;
+    long long ncell = n;
+    const void *fld = field;
+    void *pa[] = {(void *)&fld, &gx, &gy, &ncell, &clamp, &partial};
+    const void *k1 = (dtype == MMS_PREC_F64) ? (const void *)k_reduce_na_partials<double>
+                                             : (const void *)k_reduce_na_partials<float>;
+    if (cudaLaunchKernel(k1, dim3((unsigned)nb), dim3(NA_NT), pa, 0, st) != cudaSuccess) return MMS_ERR_CUDA;
+    double vol = std::pow(cell_size, 3.0), dn = (double)n;
+    void *fa[] = {&partial, &nblocks, &w, &vol, &dn, &out};
+    if (cudaLaunchKernel((const void *)k_reduce_na_finish, dim3(1), dim3(NA_FIN_NT), fa, 0, st) != cudaSuccess)
+        return MMS_ERR_CUDA;
     return MMS_OK;
 }

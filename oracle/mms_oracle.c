@@ -5,7 +5,7 @@
  * and bench.py's cpu_baseline leg.  Nothing in the product links, imports or
  * executes it.
  *
- * Pinning: tests/test_oracle_vs_reference.py compares every field this file
+ * Pinning: tests/test_oracle_golden.py compares every field this file
  * produces, bit for bit, with dumps of the reference itself (compiled from
  * its own sources under oracle/_ref by oracle/Makefile), and the known
  * answers of the reference's regression tests (tests/testOneGrain.py:25-39).

@@ -42,17 +42,53 @@ def test_noalloc_rejects_before_device_work(built):
     assert b"scratch" in M.load_library().mms_status_string(MMS_ERR_SCRATCH_LIMIT)
 
 
-@pytest.mark.gpu
-def test_noalloc_matches_mms_reduce(built, cuda_device):
-    import torch
-    fn = _noalloc()
+def _stepped_small4():
+    """small4 after 300 steps: a few thousand cells, one partial-sum block."""
     p = M.read_deck(golden_deck("small4"))
     with M.Domain(p, precision=M.PREC_F64) as dom:
         dom.step(300)
         fields = {"fs": dom.download("fs"), "ce": dom.download("ce")}
         want = {w: dom.reduce(w) for w in REDUCE}
+    return p, fields, want
+
+
+def _ragged_uploaded():
+    """A 70 x 50 x 40 grid (140,000 interior cells: eight full partial-sum
+    blocks and a ninth partial one) holding seeded fields with fs partly above
+    1, so the clamp of the fraction-solid sums matters, uploaded into a
+    context whose own reductions give the expected values."""
+    from mumatscale_b200 import workloads as W
+    import tempfile
+    from pathlib import Path
+    deck, _, _, _ = W.one_grain(8)
+    text = deck.replace("NCellsPerSB 8 8 8", "NCellsPerSB 70 50 40")
+    assert text != deck
+    f = Path(tempfile.mkdtemp()) / "ragged.in"
+    f.write_text(text)
+    p = M.read_deck(f)
+    rng = np.random.default_rng(7)
+    shape = (42, 52, 72)
+    fs = rng.uniform(-0.05, 1.2, shape)
+    ce = rng.uniform(3.0, 6.0, shape)
+    with M.Domain(p, precision=M.PREC_F64) as dom:
+        dom.upload("fs", fs)
+        dom.upload("ce", ce)
+        fields = {"fs": dom.download("fs"), "ce": dom.download("ce")}
+        want = {w: dom.reduce(w) for w in REDUCE}
+    assert fields["fs"].shape == shape
+    return p, fields, want
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["small4", "ragged_multiblock"])
+def test_noalloc_matches_mms_reduce(built, cuda_device, case):
+    import torch
+    fn = _noalloc()
+    p, fields, want = _stepped_small4() if case == "small4" else _ragged_uploaded()
     gz, gy, gx = (s - 2 for s in fields["fs"].shape)
     assert 0 < want["fs_fraction"] < 1
+    nblocks = -(-gx * gy * gz // 16384)
+    assert (nblocks == 1) == (case == "small4")
 
     dev = torch.device("cuda", cuda_device)
     torch.cuda.set_device(dev)
