@@ -61,6 +61,8 @@ static char *g_arena = NULL;
 static int g_rank = 0;
 static int g_np = 1;
 static pid_t g_children[MAXNP];
+static int g_reaped[MAXNP];      /* rank 0: child already collected by waitpid */
+static int g_child_status[MAXNP];
 static int g_cart_dims[8];
 static int g_cart_ndims = 0;
 
@@ -153,15 +155,41 @@ static void lock(void) { pthread_mutex_lock(&g_shm->mu); }
 static void unlock(void) { pthread_mutex_unlock(&g_shm->mu); }
 static pid_t g_parent = 0;
 
+/* Rank 0: collects children that have ended; returns 1 if one of them
+ * ended abnormally (killed by a signal, or a non-zero exit). */
+static int child_failed(void)
+{
+    int bad = 0;
+    for (int r = 1; r < g_np; r++) {
+        if (g_reaped[r]) continue;
+        int st = 0;
+        if (waitpid(g_children[r], &st, WNOHANG) == g_children[r]) {
+            g_reaped[r] = 1;
+            g_child_status[r] = st;
+            if (!WIFEXITED(st) || WEXITSTATUS(st) != 0) bad = 1;
+        }
+    }
+    return bad;
+}
+
 /* Waits on the shared condition variable for at most one second, then
- * returns; a rank that sees the abort flag, or (as a child) finds rank 0
- * gone, exits instead of waiting forever.  Caller holds the mutex. */
+ * returns.  A rank that sees the abort flag, or (as a child) finds rank 0
+ * gone, exits instead of waiting forever; rank 0 raises the abort flag and
+ * exits when a child rank has died (it would never reach the call being
+ * waited for).  Caller holds the mutex. */
 static void wait_or_die(void)
 {
     struct timespec ts;
     clock_gettime(CLOCK_REALTIME, &ts);
     ts.tv_sec += 1;
     pthread_cond_timedwait(&g_shm->cv, &g_shm->mu, &ts);
+    if (g_rank == 0 && !g_shm->abort_flag && child_failed()) {
+        g_shm->abort_flag = 1;
+        pthread_cond_broadcast(&g_shm->cv);
+        pthread_mutex_unlock(&g_shm->mu);
+        fprintf(stderr, "mpi_shim: a rank died; ending the run\n");
+        _exit(1);
+    }
     if (g_shm->abort_flag || (g_rank != 0 && getppid() != g_parent)) {
         pthread_mutex_unlock(&g_shm->mu);
         _exit(1);
@@ -243,8 +271,8 @@ int MPI_Finalize(void)
     if (g_rank == 0) {
         int bad = 0;
         for (int r = 1; r < g_np; r++) {
-            int st = 0;
-            waitpid(g_children[r], &st, 0);
+            int st = g_child_status[r];
+            if (!g_reaped[r]) waitpid(g_children[r], &st, 0);
             if (!WIFEXITED(st) || WEXITSTATUS(st) != 0) bad = 1;
         }
         if (bad) fprintf(stderr, "mpi_shim: a child rank exited abnormally\n");
@@ -265,7 +293,7 @@ int MPI_Abort(MPI_Comm comm, int code)
     if (g_rank == 0) {
         for (int r = 1; r < g_np; r++) {
             int st;
-            waitpid(g_children[r], &st, 0);
+            if (!g_reaped[r]) waitpid(g_children[r], &st, 0);
         }
     }
     _exit(code ? code : 1);

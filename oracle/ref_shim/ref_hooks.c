@@ -20,6 +20,17 @@
  *                               TipCurvature 1, call the reference's own
  *                               sb_curvature (curvature.c:31) first; the
  *                               reference defines it but never calls it.
+ *  --wrap=loop                 (loop.c:186)       with
+ *                               MMSREF_INJECT_SUBSTRATE=<file>, pre-fill a
+ *                               substrate of grains before the first step, as
+ *                               mms_set_grains plus a gr/fs upload does on the
+ *                               device: grains 1..n get the file's rotation
+ *                               matrices (num_grains = n + 1, so nucleated
+ *                               grains continue from n + 1), and interior
+ *                               planes 1..top of every column (x, y) take the
+ *                               column's grain id with fs = 1.  File: int32
+ *                               gx, gy, top, n; int32 col[gy][gx] (grain id of
+ *                               each column, 0 = none); f64 rot[n][9].
  *
  * Dump file layout (little endian), one file per rank and step,
  * <dir>/r<rank>_s<timestep>.bin:
@@ -46,6 +57,7 @@ void __real_doiteration(void);
 void __real_init_sb_nucleation(SB_struct *sb);
 void __real_activateNewGrains(void);
 void __real_fs_change_diffuse(SB_struct *lsp, void *unused);
+void __real_loop(uint64_t restart, double gStartTime);
 void sb_curvature(void *vlsp, void *unused);
 
 static long total_cells(void)
@@ -208,4 +220,52 @@ void __wrap_fs_change_diffuse(SB_struct *sb, void *unused)
     const char *c = getenv("MMSREF_CURV");
     if (c && atoi(c) && bp->tip_curv) sb_curvature(sb, NULL);
     __real_fs_change_diffuse(sb, unused);
+}
+
+void __wrap_loop(uint64_t restart, double gStartTime)
+{
+    const char *path = getenv("MMSREF_INJECT_SUBSTRATE");
+    if (path && !restart) {
+        FILE *f = fopen(path, "rb");
+        if (!f) {
+            perror(path);
+            exit(3);
+        }
+        int32_t hdr[4];
+        if (fread(hdr, sizeof(int32_t), 4, f) != 4) exit(3);
+        const int gx = hdr[0], gy = hdr[1], top = hdr[2], n = hdr[3];
+        if (gx != bp->gnsbx * bp->gsdimx || gy != bp->gnsby * bp->gsdimy || n < 0 ||
+            (uint64_t)n + 1 > bp->maxTotalGrains + 1) {
+            fprintf(stderr, "%s: substrate does not fit this deck\n", path);
+            exit(3);
+        }
+        int32_t *col = (int32_t *)malloc(sizeof(int32_t) * (size_t)gx * gy);
+        double *rot = (double *)malloc(sizeof(double) * 9 * (size_t)(n ? n : 1));
+        if (fread(col, sizeof(int32_t), (size_t)gx * gy, f) != (size_t)gx * gy ||
+            fread(rot, sizeof(double), 9 * (size_t)n, f) != 9 * (size_t)n)
+            exit(3);
+        fclose(f);
+        for (int g = 0; g < n; g++) {
+            memset(&grain_cache[g + 1], 0, sizeof(grain_t));
+            memcpy(&grain_cache[g + 1].rotmat[0][0], rot + 9 * (size_t)g, sizeof(double) * 9);
+        }
+        bp->num_grains = n + 1;
+        for (int k = 1; k <= bp->gsdimz; k++) {
+            const int K = (int)lsp->coords.z * bp->gsdimz + k;  /* global interior plane, 1-based */
+            if (K > top) continue;
+            for (int j = 1; j <= bp->gsdimy; j++)
+                for (int i = 1; i <= bp->gsdimx; i++) {
+                    const int X = (int)lsp->coords.x * bp->gsdimx + i - 1;
+                    const int Y = (int)lsp->coords.y * bp->gsdimy + j - 1;
+                    const int id = col[(size_t)Y * gx + X];
+                    if (id <= 0) continue;
+                    const long idx = SBIDX(i, j, k);
+                    lsp->gr[idx] = id;
+                    lsp->fs[idx] = 1.0;
+                }
+        }
+        free(col);
+        free(rot);
+    }
+    __real_loop(restart, gStartTime);
 }
