@@ -1,27 +1,37 @@
 #!/usr/bin/env python3
 """Throughput of the muMatScale CA step on B200: cell-updates/s.
 
-Workload: the multi-grain directional-solidification deck (256^3 cells,
-dx = 2 um, Al-Cu C0 = 4.5 wt%, m = -2.6 K/wt%, k = 0.14, D_l = 3e-9,
-D_s = 3e-13 m^2/s, G = 1e4 K/m along z, V = 1e-3 m/s, dt with
-D_l dt/dx^2 = 0.04 (the reference aborts at 0.15 and 0.10 on this alloy), surface sites 1e10 m^-2 and bulk sites 1e13 m^-3 with
-undercooling N(2 K, 0.5 K), random orientations), restated as a
-reference-format deck so that the reference runs the same physics.  A
+Default workload (the driver's line): the AM single-track melt pool, 512 x
+256 x 128 cells, dx = 1 um, binary Al-Cu (C0 = 4.5 wt%, m = -2.6 K/wt%, k =
+0.14, D_l = 3e-9, D_s = 3e-13 m^2/s), the reference's moving-source
+quadrature temperature (AnalyticalThermal 1, temperature.c:62-123) at 0.5
+m/s, 150 W, absorptivity 0.4, k_th = 100 W/m/K, alpha = 3e-5 m^2/s; a
+substrate of columnar grains (mean width 20 um, random orientations) in
+interior planes 1..120; bulk sites at 1e14 m^-3 with undercooling N(3 K,
+1 K).  The deck is split into the same NSubblocks as the reference arm
+uses, so both arms draw the same sites from the same per-rank streams.  A
 "step" is one timestep (doiteration) of the whole domain; the metric counts
 interior cells x steps / second.
 
-GPU arm (default): the FP64 plain form is ``value`` (bit-identical to the
-reference); the FP32 form is reported beside it.  Timing: W untimed steps,
-then K steps bracketed by CUDA events on the stream the library launches
-on, synchronised on both sides; under torchrun every rank runs its own
-replica (the z-slab sharded version is not built: replicas only) and the
-maximum over ranks is taken.  Inputs (about 1.1 GB of fields) are larger
-than the 126 MB L2, so no flush is needed.
+GPU arm: ``value`` is the FP32 form (FP32 ce/cl/fs, tensor-core
+temperature, FP64 octahedra, thresholds and reductions); the FP64 plain form
+is reported beside it, with the FP32 form's error against it after the
+timed steps (grain-id mismatch fraction, relative L2 of ce, max |fs error|,
+max |T error| / max T).  Timing: W untimed steps, then K steps bracketed by
+CUDA events on the stream the library launches on, synchronised on both
+sides; the fields (about 0.7 GB in FP32, 1.1 GB in FP64) are larger than
+the 126 MB L2, so no flush is needed.  ``e2e``: the same K steps through the
+public API from a fresh context, with the substrate uploaded from pinned
+host memory, the fraction solid read back every step and the grain ids and
+ce read back at the end, all inside the timed region.  Under torchrun every
+rank runs its own replica (weak scaling; --workload slabs splits one
+domain) and the maximum over ranks is taken.  The multi-grain
+directional-solidification deck (256^3) is reported under ``cfg2``.
 
 Reference arm (--impl reference): the unmodified reference compiled from
 its sources (oracle/_ref/mmsref), run as MPI ranks over the host cores
-through the project's shared-memory MPI shim on the same deck decomposed
-into NSubblocks, timing K steps after W steps from per-step timestamps.
+through the project's shared-memory MPI shim on the same deck and
+substrate, timing K steps after W steps from per-step timestamps.
 """
 from __future__ import annotations
 
@@ -58,6 +68,15 @@ DT = 0.04 * DX * DX / 3e-9
 BYTES_DIFFUSE = {"f64": 3 * 8 * 2 + 4, "f32": 3 * 4 * 2 + 4}
 # full-step dense bytes per cell-update (ce, cl, fs read+write, gr, threshold)
 BYTES_STEP = {"f64": 56, "f32": 32}
+# the AM deck's stencil also reads the temperature field (FP64)
+BYTES_DIFFUSE_AM = {k: v + 8 for k, v in BYTES_DIFFUSE.items()}
+
+# AM melt-pool deck (the default workload)
+AM_DIMS = (512, 256, 128)
+AM_DX = 1e-6
+AM_TOP = AM_DIMS[2] - 8        # substrate: interior planes 1..120
+AM_SUB_WIDTH, AM_SUB_SEED = 20e-6, 11
+AM_DT = 0.04 * AM_DX * AM_DX / 3e-9
 
 
 def deck_text(nsb=(1, 1, 1), n=N_CELL, seed=20261203) -> str:
@@ -97,11 +116,49 @@ GNOriented 1
 """
 
 
+def am_deck_text(nsb=(1, 1, 1)) -> str:
+    """The AM melt-pool deck split into nsb subblocks (emulated ranks)."""
+    from mumatscale_b200 import workloads as W
+    assert all(AM_DIMS[i] % nsb[i] == 0 for i in range(3)), nsb
+    sb = [AM_DIMS[i] // nsb[i] for i in range(3)]
+    d = W.am_track(AM_DIMS, AM_DX)
+    d = d.replace("NSubblocks 1 1 1", f"NSubblocks {nsb[0]} {nsb[1]} {nsb[2]}")
+    return d.replace(f"NCellsPerSB {AM_DIMS[0]} {AM_DIMS[1]} {AM_DIMS[2]}", f"NCellsPerSB {sb[0]} {sb[1]} {sb[2]}")
+
+
+def am_substrate():
+    """The columnar substrate of the AM deck: (column grain ids, rotations)."""
+    from mumatscale_b200 import workloads as W
+    return W.columnar_columns(AM_DIMS[0], AM_DIMS[1], AM_DX, AM_SUB_WIDTH, AM_SUB_SEED)
+
+
+def am_host_fields(cols, gr=None, fs=None):
+    """gr and fs of the substrate in the halo'd layout (into gr / fs when
+    given, e.g. pinned buffers): ids in planes 1..AM_TOP, fs = 1 there."""
+    shape = (AM_DIMS[2] + 2, AM_DIMS[1] + 2, AM_DIMS[0] + 2)
+    import numpy as np
+    gr = np.zeros(shape, dtype=np.int32) if gr is None else gr.reshape(shape)
+    fs = np.zeros(shape, dtype=np.float64) if fs is None else fs.reshape(shape)
+    gr[...] = 0
+    gr[1:AM_TOP + 1, 1:-1, 1:-1] = cols[None]
+    fs[...] = 0.0
+    fs[gr > 0] = 1.0
+    return gr, fs
+
+
+def am_fill(dom, rot, gr, fs) -> None:
+    """The substrate into a fresh context: grains 1..n, then gr and fs."""
+    dom.set_grains(rot)
+    dom.upload("gr", gr)
+    dom.upload("fs", fs)
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """SM clocks and clock-event (throttle) reasons sampled during the timed
-    region: NVML read from a thread every 5 ms (the device found by its PCI
-    bus id), else nvidia-smi every 100 ms.  Reads only; changes nothing."""
+    region: NVML read from a thread every 2 ms and once more as the region
+    ends (the device found by its PCI bus id), else nvidia-smi every 100 ms.
+    Reads only; changes nothing."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -130,25 +187,29 @@ class ClockSampler:
         except Exception:
             return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
 
-    def _poll(self):
+    def _sample(self):
         nv, h = self.nvml
         bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
                 "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
                 "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
                 "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
-        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        try:
+            sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append((sm, self._max, {k for k, b in bits.items() if r & b}))
+        except Exception:
+            pass
+
+    def _poll(self):
         while not self._stop.is_set():
-            try:
-                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
-                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                self.samples.append((sm, mx, {k for k, b in bits.items() if r & b}))
-            except Exception:
-                pass
-            self._stop.wait(0.005)
+            self._sample()
+            self._stop.wait(0.002)
 
     def __enter__(self):
         try:
             self.nvml = self._nvml_handle()
+            nv, h = self.nvml
+            self._max = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
             self._t = threading.Thread(target=self._poll, daemon=True)
             self._t.start()
             return self
@@ -169,6 +230,10 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        # one reading taken here, as the timed region ends, so that a region
+        # shorter than the polling thread's first wake-up still has one
+        if self.nvml:
+            self._sample()
         self._stop.set()
         if self.nvml:
             self._t.join(timeout=5)
@@ -218,12 +283,27 @@ def measured_peak_gbs() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_cell(dtype: str):
+def measured_peak_tflops() -> float:
+    """Dense bf16 GEMM peak (burst) of MEASURED_PEAKS.json, else the fallback."""
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return float(json.loads(f.read_text())["bf16_tflops"])
+        except Exception:
+            pass
+    return 1590.0
+
+
+def ncu_traffic_per_cell(dtype: str, workload: str = "ds256"):
+    """DRAM bytes per cell of one stencil launch from a committed ncu summary
+    (profiles/k_diffuse_fs_traffic.json: keys "f64"/"f32" for the 256^3
+    directional deck, "am_f64"/"am_f32" for the AM deck), or None."""
     f = ROOT / "profiles" / "k_diffuse_fs_traffic.json"
+    key = dtype if workload == "ds256" else f"{workload}_{dtype}"
     if f.exists():
         try:
             d = json.loads(f.read_text())
-            return d[dtype]["dram_bytes_per_cell"]
+            return d[key]["dram_bytes_per_cell"]
         except Exception:
             return None
     return None
@@ -243,8 +323,12 @@ def ref_procs(cores: int) -> tuple[int, tuple[int, int, int]]:
     return n, (nsb[0], nsb[1], nsb[2])
 
 
-def run_reference(nsteps_w: int, nsteps_k: int, cores: int | None = None, timeout: float = 1800):
-    """Times the unmodified reference (oracle/_ref/mmsref) on the bench deck."""
+def run_reference(workload: str, nsteps_w: int, nsteps_k: int, cores: int | None = None,
+                  timeout: float = 1800):
+    """Times the unmodified reference (oracle/_ref/mmsref) on a bench deck:
+    workload "am" (the default AM melt pool with its substrate, injected
+    through MMSREF_INJECT_SUBSTRATE) or "ds256" (directional solidification).
+    Returns (result, None) or (None, why)."""
     ref = ROOT / "oracle" / "_ref" / "mmsref"
     if not ref.exists():
         return None, "oracle/_ref/mmsref not built"
@@ -252,13 +336,27 @@ def run_reference(nsteps_w: int, nsteps_k: int, cores: int | None = None, timeou
     nproc, nsb = ref_procs(cores)
     with tempfile.TemporaryDirectory() as td:
         deck = Path(td) / "bench.in"
-        text = deck_text(nsb).replace("FinishTime 0", f"FinishTime {(nsteps_w + nsteps_k - 0.5) * DT!r}")
+        env = dict(os.environ, MMSREF_NP=str(nproc), OMP_NUM_THREADS="1")
+        if workload == "am":
+            from mumatscale_b200 import workloads as W
+            text = am_deck_text(nsb).replace("FinishTime 0\n",
+                                             f"FinishTime {(nsteps_w + nsteps_k - 0.5) * AM_DT!r}\n")
+            cols, rot = am_substrate()
+            W.write_substrate_file(Path(td) / "substrate.bin", cols, rot, AM_TOP)
+            env["MMSREF_INJECT_SUBSTRATE"] = str(Path(td) / "substrate.bin")
+            cells = AM_DIMS[0] * AM_DIMS[1] * AM_DIMS[2]
+        else:
+            text = deck_text(nsb).replace("FinishTime 0", f"FinishTime {(nsteps_w + nsteps_k - 0.5) * DT!r}")
+            cells = N_CELL ** 3
         deck.write_text(text)
         times = Path(td) / "times.txt"
-        env = dict(os.environ, MMSREF_NP=str(nproc), MMSREF_STEP_TIMES=str(times), OMP_NUM_THREADS="1")
+        env["MMSREF_STEP_TIMES"] = str(times)
         t0 = time.time()
-        r = subprocess.run([str(ref), "-c", str(deck)], cwd=td, env=env, capture_output=True, text=True,
-                           timeout=timeout)
+        try:
+            r = subprocess.run([str(ref), "-c", str(deck)], cwd=td, env=env, capture_output=True, text=True,
+                               timeout=timeout)
+        except subprocess.TimeoutExpired:
+            return None, f"reference did not finish within {timeout:.0f} s"
         wall = time.time() - t0
         if r.returncode != 0:
             return None, f"reference exited {r.returncode}: {r.stderr[-300:]}"
@@ -271,14 +369,20 @@ def run_reference(nsteps_w: int, nsteps_k: int, cores: int | None = None, timeou
         t_end = ts.get(nsteps_w + nsteps_k)
         if t_start is None or t_end is None:
             return None, "reference step timestamps missing"
-        cells = N_CELL ** 3
+        grains = None
+        for line in r.stdout.splitlines():
+            w = line.split()
+            if len(w) > 1 and w[1] == "grains.":
+                grains = int(w[0])  # output_grains: num_grains - 1 (grain.c:823)
         sec = t_end - t_start
         return {"value": cells * nsteps_k / sec, "sec": sec, "procs": nproc, "nsubblocks": nsb,
-                "wall": wall, "steps": nsteps_k}, None
+                "wall": wall, "steps": nsteps_k, "grains": grains, "cells": cells}, None
 
 
 # ---------------------------------------------------------------- GPU arm
-def gpu_arm(args) -> None:
+def ds256_workload(args) -> None:
+    """The multi-grain directional-solidification deck (256^3) as its own
+    line: FP64 plain form as value, FP32 beside it, e2e, CPU baseline."""
     import numpy as np
     import torch
     import mumatscale_b200 as M
@@ -401,7 +505,7 @@ def gpu_arm(args) -> None:
              for k, v in f64["kernels"].items() if v[1]}
     cpu = None
     if not args.no_cpu_baseline:
-        res, why = run_reference(2, args.cpu_steps)
+        res, why = run_reference("ds256", 2, args.cpu_steps)
         if res:
             cpu = {"value": res["value"], "unit": UNIT, "cores": res["procs"], "kind": "reference",
                    "sample": f"{res['steps']} timesteps of the same 256^3 deck after 2 warm-up steps, "
@@ -435,6 +539,273 @@ def gpu_arm(args) -> None:
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def _errors(d32, d64) -> dict:
+    """The FP32 form against the FP64 plain form, interior cells: grain-id
+    mismatch fraction, relative L2 of ce, max |fs error|, max |T error| over
+    max |T| (all cells)."""
+    import numpy as np
+
+    def inner(x):
+        return x[1:-1, 1:-1, 1:-1]
+    g32, g64 = inner(d32.download("gr")), inner(d64.download("gr"))
+    c32, c64 = inner(d32.download("ce")), inner(d64.download("ce"))
+    f32, f64 = inner(d32.download("fs")), inner(d64.download("fs"))
+    t32, t64 = d32.download("temperature"), d64.download("temperature")
+    return {"grain_id_mismatch": float((g32 != g64).mean()),
+            "ce_rel_l2": float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64)),
+            "fs_max_abs": float(np.abs(f32 - f64).max()),
+            "T_max_rel": float(np.abs(t32 - t64).max() / max(np.abs(t64).max(), 1e-300)),
+            "at_step": d64.timestep}
+
+
+def _dist(ws):
+    import torch
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(dist_env()[2])
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return barrier, max_over_ranks
+
+
+def _roofline(ks: dict, steps: int, cells: int, form: str, peaks: dict) -> dict:
+    """Roofline of the kernel with the largest device time in ks
+    (name -> (ms over `steps` steps, launches))."""
+    name = max(ks, key=lambda k: ks[k][0])
+    ms, n = ks[name]
+    per_launch = ms / 1e3 / max(n, 1)
+    if name == "k_temp_am":
+        # tables + contraction per step: 2 x 400 multiply-adds per halo'd cell
+        # (algorithmic; the TF32 x 3 form issues three MMAs per product)
+        halo = (AM_DIMS[0] + 2) * (AM_DIMS[1] + 2) * (AM_DIMS[2] + 2)
+        flops = 2.0 * 400 * halo
+        ach = flops / per_launch / 1e12
+        pk = peaks["bf16_tflops"]
+        return {"bound": "tensor", "kernel": name, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                "frac": ach / pk, "peak_source": peaks["source"] + " (dense bf16 GEMM; TF32 runs at half its rate)",
+                "algorithmic_flops_per_launch": flops, "traffic": None,
+                "kernel_ms_per_launch": per_launch * 1e3}
+    b = BYTES_DIFFUSE_AM[form] if name == "k_diffuse_fs" else BYTES_STEP[form]
+    ach = b * cells / per_launch / 1e9
+    tr = ncu_traffic_per_cell(form, "am")
+    return {"bound": "hbm", "kernel": name, "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": ach / peaks["hbm_gbs"], "peak_source": peaks["source"],
+            "algorithmic_bytes_per_cell": b, "traffic": (tr * cells) if tr else None,
+            "kernel_ms_per_launch": per_launch * 1e3}
+
+
+def gpu_arm(args) -> None:
+    """The default line: the AM melt-pool deck, FP32 form as value."""
+    import numpy as np
+    import torch
+    import mumatscale_b200 as M
+
+    ws, rank, _ = dist_env()
+    barrier, max_over_ranks = _dist(ws)
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.current_stream()
+    K, Wm = args.steps, args.warmup
+    cells = AM_DIMS[0] * AM_DIMS[1] * AM_DIMS[2]
+    nproc, nsb = ref_procs(os.cpu_count() or 1)
+    td = tempfile.mkdtemp()
+    deck = Path(td) / "am.in"
+    deck.write_text(am_deck_text(nsb))
+    params = M.read_deck(deck)
+    cols, rot = am_substrate()
+    gr0, fs0 = am_host_fields(cols)
+    doms, out = {}, {}
+    for form, prec in (("f32", M.PREC_F32), ("f64", M.PREC_F64)):
+        dom = M.Domain(params, precision=prec, device=dev)
+        dom.set_stream(stream.cuda_stream)
+        am_fill(dom, rot, gr0, fs0)
+        tile = dom.autotune(reps=3)
+        dom.step(Wm)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = dom.kernel_launches
+        with ClockSampler(dev) as clk:
+            e0.record(stream)
+            dom.step(K)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        out[form] = {"ms_total": ms, "launches": dom.kernel_launches - l0, "clocks": clk.summary(),
+                     "tile": {"cells_per_thread": tile[0], "zchunk": tile[1], "cta_cells": [32 * tile[0], 8]},
+                     "grains": dom.num_grains - 1}
+        doms[form] = dom
+    errors = _errors(doms["f32"], doms["f64"])
+    for form, dom in doms.items():
+        # per-kernel device time over a second pass of K steps
+        dom.set_profiling(True)
+        dom.step(K)
+        torch.cuda.synchronize()
+        out[form]["kernels"] = dom.kernel_stats()
+        dom.set_profiling(False)
+        dom.close()
+    del doms
+
+    # end to end through the public API, FP32 form: a fresh context (created
+    # before the clock starts), then the substrate uploaded from pinned host
+    # memory, K steps each followed by a device->host read of the fraction
+    # solid (loop.c's screen value), and the grain ids and ce read back
+    n = (AM_DIMS[0] + 2) * (AM_DIMS[1] + 2) * (AM_DIMS[2] + 2)
+    h_gr = torch.empty(n, dtype=torch.int32).pin_memory()
+    h_fs = torch.empty(n, dtype=torch.float64).pin_memory()
+    am_host_fields(cols, h_gr.numpy(), h_fs.numpy())
+    o_gr = torch.empty(n, dtype=torch.int32).pin_memory()
+    o_ce = torch.empty(n, dtype=torch.float64).pin_memory()
+    with M.Domain(params, precision=M.PREC_F32, device=dev) as dom:
+        dom.set_stream(stream.cuda_stream)
+        dom.set_stencil_tile(out["f32"]["tile"]["cells_per_thread"], out["f32"]["tile"]["zchunk"])
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        am_fill(dom, rot, h_gr.numpy(), h_fs.numpy())
+        h2d = rot.nbytes + h_gr.numel() * 4 + h_fs.numel() * 8
+        d2h = 0
+        for _ in range(K):
+            dom.step_reduce(1, "fs_fraction")
+            d2h += 8
+        dom.download("gr", out=o_gr.numpy())
+        dom.download("ce", out=o_ce.numpy())
+        d2h += o_gr.numel() * 4 + o_ce.numel() * 8
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": ws * cells * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d // K,
+           "d2h_bytes_per_step": d2h // K}
+
+    cfg2 = None if args.no_cfg2 else ds256_device(args, ws, stream, barrier, max_over_ranks)
+
+    if rank != 0:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    f32, f64 = out["f32"], out["f64"]
+    value = ws * cells * K / (f32["ms_total"] / 1e3)
+    value64 = ws * cells * K / (f64["ms_total"] / 1e3)
+    peak, peak_kind = measured_peak_gbs()
+    peaks = {"hbm_gbs": peak, "bf16_tflops": measured_peak_tflops(), "source": peak_kind}
+    roof = _roofline(f32["kernels"], K, cells, "f32", peaks)
+    kms, kn = f32["kernels"]["k_diffuse_fs"]
+    st32 = BYTES_DIFFUSE_AM["f32"] * cells / (kms / 1e3 / max(kn, 1)) / 1e9
+    kms64, kn64 = f64["kernels"]["k_diffuse_fs"]
+    st64 = BYTES_DIFFUSE_AM["f64"] * cells / (kms64 / 1e3 / max(kn64, 1)) / 1e9
+
+    def per_step(ks):
+        return {k: round(v[0] / K, 5) for k, v in ks.items() if v[1]}
+    cpu = None
+    check = None
+    if not args.no_cpu_baseline:
+        w1, k1 = 1, args.cpu_steps if args.cpu_steps != 200 else 2
+        res, why = run_reference("am", w1, k1)
+        if res:
+            cpu = {"value": res["value"], "unit": UNIT, "cores": res["procs"], "kind": "reference",
+                   "sample": f"{res['steps']} timesteps of the same 512x256x128 AM deck and substrate after "
+                             f"{w1} warm-up step, {res['procs']} MPI ranks (NSubblocks {res['nsubblocks']}) of "
+                             f"the reference through the shared-memory MPI shim, {res['sec']:.2f} s"}
+            # the same number of steps on the device, FP64 plain form: grain counts agree
+            with M.Domain(params, precision=M.PREC_F64, device=dev) as d:
+                am_fill(d, rot, gr0, fs0)
+                d.step(w1 + k1)
+                check = {"steps": w1 + k1, "reference_grains": res["grains"], "fp64_grains": d.num_grains - 1}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": Wm,
+        "ms_per_step": f32["ms_total"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": am_config(nsb, f32["grains"]),
+        "parallelism": f"replicas x{ws}",
+        "fp64_plain": {"value": value64, "ms_per_step": f64["ms_total"] / K, "grains_after_run": f64["grains"],
+                       "k_diffuse_fs_gbs": st64, "k_diffuse_fs_frac": st64 / peak,
+                       "kernel_ms_per_step": per_step(f64["kernels"]), "stencil_tile": f64["tile"]},
+        "fp32_form": {"ratio_vs_fp64": value / value64, "errors_vs_fp64": errors,
+                      "k_diffuse_fs_gbs": st32, "k_diffuse_fs_frac": st32 / peak,
+                      "kernel_ms_per_step": per_step(f32["kernels"]), "stencil_tile": f32["tile"]},
+        "roofline": roof,
+        "e2e": e2e,
+        "gpu_launches": f32["launches"],
+        "clocks": f32["clocks"],
+        "clocks_fp64": f64["clocks"],
+        "cpu_baseline": cpu,
+        "grain_check_vs_reference": check,
+        "cfg2": cfg2,
+    }
+    print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def am_config(nsb, grains) -> dict:
+    """config of both arms' lines (the same keys and values for the same run)."""
+    return {"workload": "AM single-track melt pool, 512x256x128 cells, columnar substrate, FP32 form",
+            "cells": AM_DIMS[0] * AM_DIMS[1] * AM_DIMS[2], "dx_m": AM_DX, "dt_s": AM_DT,
+            "laser": {"speed_m_per_s": 0.5, "power_w": 150, "absorptivity": 0.4, "k_th": 100, "alpha": 3e-5},
+            "substrate": {"top_plane": AM_TOP, "mean_width_m": AM_SUB_WIDTH, "seed": AM_SUB_SEED},
+            "nsubblocks": list(nsb), "grains_after_run": grains,
+            "l2": "inputs larger than L2 (fields about 0.7 GB FP32, 1.1 GB FP64)"}
+
+
+def ds256_device(args, ws, stream, barrier, max_over_ranks) -> dict:
+    """The 256^3 directional-solidification deck, device-timed K steps of each
+    form (the cfg2 key of the default line)."""
+    import torch
+    import mumatscale_b200 as M
+    K, Wm = args.steps, args.warmup
+    td = tempfile.mkdtemp()
+    deck = Path(td) / "ds.in"
+    deck.write_text(deck_text())
+    params = M.read_deck(deck)
+    out = {}
+    for form, prec in (("f64", M.PREC_F64), ("f32", M.PREC_F32)):
+        with M.Domain(params, precision=prec) as dom:
+            dom.set_stream(stream.cuda_stream)
+            dom.autotune(reps=3)
+            dom.step(Wm)
+            torch.cuda.synchronize()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dom.step(K)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = max_over_ranks(e0.elapsed_time(e1))
+            dom.set_profiling(True)
+            dom.step(K)
+            torch.cuda.synchronize()
+            ks = dom.kernel_stats()
+            dom.set_profiling(False)
+            kms, kn = ks["k_diffuse_fs"]
+            gbs = BYTES_DIFFUSE[form] * N_CELL ** 3 / (kms / 1e3 / max(kn, 1)) / 1e9
+            out[form] = {"value": ws * N_CELL ** 3 * K / (ms / 1e3), "ms_per_step": ms / K,
+                         "k_diffuse_fs_gbs": gbs, "k_diffuse_fs_frac": gbs / measured_peak_gbs()[0]}
+    out["workload"] = "multi-grain directional solidification, 256^3 cells"
+    out["fp32_ratio_vs_fp64"] = out["f32"]["value"] / out["f64"]["value"]
+    return out
 
 
 def profile_arm(args) -> None:
@@ -534,56 +905,6 @@ def adjoint_workload(args) -> None:
             "fd_step_rel": h,
             "gradient_cell_updates_per_s": {"f64": cells_n * steps / f64["gradient_s"],
                                             "f32": cells_n * steps / f32["gradient_s"]}}
-    print(json.dumps(line))
-
-
-def am_workload(args) -> None:
-    """AM single-track melt pool, 512 x 256 x 128 cells, dx = 1 um, substrate
-    of columnar grains (mean width 20 um): FP64 plain form and FP32 form
-    cell-updates/s, K timed steps after W, inputs resident in HBM.  The
-    reference's quadrature temperature is part of every step.  Prints one
-    JSON line."""
-    import torch
-    import mumatscale_b200 as M
-    from mumatscale_b200 import workloads as W
-    dims, dx = (512, 256, 128), 1e-6
-    td = tempfile.mkdtemp()
-    f = Path(td) / "am.in"
-    f.write_text(W.am_track(dims, dx))
-    p = M.read_deck(f)
-    cells = dims[0] * dims[1] * dims[2]
-    K, Wm = args.steps, args.warmup
-    stream = torch.cuda.current_stream()
-    out = {}
-    for form, prec in (("f64", M.PREC_F64), ("f32", M.PREC_F32)):
-        dom = M.Domain(p, precision=prec)
-        dom.set_stream(stream.cuda_stream)
-        ng = W.setup_substrate(dom, dims[2] - 8, dx)
-        tile = dom.autotune(reps=3)
-        dom.step(Wm)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with ClockSampler(torch.cuda.current_device()) as clk:
-            e0.record(stream)
-            dom.step(K)
-            e1.record(stream)
-            torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        dom.set_profiling(True)
-        dom.step(K)
-        torch.cuda.synchronize()
-        ks = dom.kernel_stats()
-        dom.set_profiling(False)
-        tot = sum(v[0] for v in ks.values())
-        out[form] = {"value": cells * K / (ms / 1e3), "ms_per_step": ms / K,
-                     "temperature_share": ks["k_temp_am"][0] / tot if tot else None,
-                     "kernel_ms_per_step": {k: v[0] / K for k, v in ks.items() if v[1]},
-                     "substrate_grains": ng, "grains": dom.num_grains, "fs_fraction": dom.reduce("fs_fraction"),
-                     "tile": list(tile[:2]), "clocks": clk.summary()}
-        dom.close()
-    line = {"workload": "AM single-track melt pool, 512x256x128 cells, dx 1 um, columnar substrate",
-            "metric": UNIT, "unit": UNIT, "steps": K, "warmup": Wm, "data": "synthetic",
-            "f64": out["f64"], "f32": out["f32"], "ratio_f32_vs_f64": out["f32"]["value"] / out["f64"]["value"]}
     print(json.dumps(line))
 
 
@@ -779,21 +1100,32 @@ def slabs_workload(args) -> None:
 
 
 def reference_arm(args) -> None:
+    """The reference's own CPU path on the default (AM) deck, or on the 256^3
+    directional deck with --workload ds256; rank 0 only."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    res, why = run_reference(args.warmup, args.steps)
+    wl = "ds256" if args.workload == "ds256" else "am"
+    res, why = run_reference(wl, args.warmup, args.steps)
     if not res:
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return
+    if wl == "am":
+        config, dtype = am_config(res["nsubblocks"], res["grains"]), "f64"
+        config["workload"] = config["workload"].replace("FP32 form", "the reference (FP64)")
+    else:
+        config = {"workload": "multi-grain directional solidification, 256^3 cells, FP64 plain form",
+                  "cells": N_CELL ** 3, "dx_m": DX, "dt_s": DT, "G_K_per_m": 1e4, "V_m_per_s": 1e-3,
+                  "nsubblocks": list(res["nsubblocks"]), "grains_after_run": res["grains"]}
+        dtype = "f64"
     line = {
         "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["sec"] * 1e3 / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "multi-grain directional solidification, 256^3 cells, FP64 plain form",
-                   "cells": N_CELL ** 3, "parallelism": f"{res['procs']} MPI ranks on host cores"},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+        "config": config, "parallelism": f"{res['procs']} MPI ranks on host cores",
         "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": res["procs"], "kind": "reference",
-                         "sample": f"{args.steps} timesteps after {args.warmup}, NSubblocks {res['nsubblocks']}"},
+                         "sample": f"{args.steps} timesteps after {args.warmup}, NSubblocks {res['nsubblocks']}, "
+                                   f"{res['procs']} MPI ranks through the shared-memory MPI shim"},
         "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -805,7 +1137,9 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--cpu-steps", type=int, default=200)
+    ap.add_argument("--cpu-steps", type=int, default=200,
+                    help="timed steps of the CPU baseline leg (default: 2 on the AM deck, 200 on ds256)")
+    ap.add_argument("--no-cfg2", action="store_true", help="leave the 256^3 directional deck out of the line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", choices=["f64", "f32"], default=None,
                     help="run the workload for an ncu capture only")
@@ -813,19 +1147,22 @@ def main() -> None:
     ap.add_argument("--reduce", type=int, default=0,
                     help="profile mode: rounds of (step with tile sums, plain step, field reduction) after the steps")
     ap.add_argument("--tile", default="auto", help="profile mode: stencil tile 'cells_per_thread,zchunk'")
-    ap.add_argument("--workload", default="ds256", choices=["ds256", "adjoint", "am", "ensemble", "slabs"],
-                    help="ds256: the headline directional-solidification run (default); adjoint, am, "
-                         "ensemble, slabs: the adjoint calibration, AM melt-pool, batched-ensemble and "
-                         "one-domain-over-N-GPUs workloads (each its own JSON line)")
+    ap.add_argument("--workload", default=None, choices=["am", "ds256", "adjoint", "ensemble", "slabs"],
+                    help="am: the AM melt-pool deck, the headline line (default); ds256, adjoint, "
+                         "ensemble, slabs: the 256^3 directional-solidification, adjoint calibration, "
+                         "batched-ensemble and one-domain-over-N-GPUs workloads (each its own JSON line). "
+                         "With --profile the default is ds256.")
     args = ap.parse_args()
+    if args.workload is None:
+        args.workload = "ds256" if args.profile else "am"
     if args.warmup < 3:
         args.warmup = 3
     if args.profile:
         profile_arm(args)
     elif args.workload == "adjoint" and args.impl != "reference":
         adjoint_workload(args)
-    elif args.workload == "am" and args.impl != "reference":
-        am_workload(args)
+    elif args.workload == "ds256" and args.impl != "reference":
+        ds256_workload(args)
     elif args.workload == "ensemble" and args.impl != "reference":
         ensemble_workload(args)
     elif args.workload == "slabs" and args.impl != "reference":

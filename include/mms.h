@@ -131,6 +131,13 @@ typedef struct mms_params {
      * and threshold distributions, not the reference's sequence.  FixedNuc
      * and NucVolume sites are the reference's in both. */
     int site_setup;
+    /* bp->checkpointfreq, which the reference's deck parser sets from
+     * DataWriteStart (read_ctrl.c:594-600; it has no keyword of its own):
+     * mms_run writes a checkpoint (mms_checkpoint_save to cp_main.mms in the
+     * working directory, the counterpart of the reference's cp_main.h5) every
+     * checkpoint_freq steps, as loop.c:244-247 calls writeCheckpoint;
+     * 0 = never */
+    int checkpoint_freq;
 } mms_params;
 
 typedef enum mms_field {
@@ -274,6 +281,16 @@ mms_status mms_set_sites(mms_ctx *ctx, int64_t n, const int32_t *gxyz,
 mms_status mms_set_site_orientations(mms_ctx *ctx, int64_t n, const int32_t *gxyz,
                                      const double *rotmat9);
 
+/* Failure-detection test hook, no counterpart in the reference (whose
+ * failures abort the process, debug.h:54-58).  From the next step on, the
+ * interface-list block at list position `block` publishes no status word, so
+ * the decoupled look-back of the block after it waits for a word that nothing
+ * writes; that wait gives up after `polls` polls (0: 2^22, about a second)
+ * and the step returns MMS_ERR_TIMEOUT, with no device fault and the device
+ * usable.  block = -1 turns the hook off.  The context is in error after such
+ * a step; destroy it. */
+mms_status mms_test_hold_list_block(mms_ctx *ctx, int block, unsigned polls);
+
 /* A pre-filled microstructure (for example a substrate of columnar grains):
  * defines grains 1..n with the given row-major rotation matrices, so that
  * nucleated grains continue from id n+1.  Only before the first step; the
@@ -329,6 +346,8 @@ mms_status mms_xdmf_renumbering(mms_ctx *ctx, int capacity, uint64_t *out, int *
  * continues exactly as the saved context would have (the role of
  * checkpoint.c's restart, checkpoint.c:955-1244, without HDF5). */
 mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path);
+/* the file mms_run writes every checkpoint_freq steps, and mmsb200 -r reads */
+#define MMS_CHECKPOINT_FILE "cp_main.mms"
 mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path);
 
 /* ---- the time loop (loop.c:186-271) ----------------------------------------- */

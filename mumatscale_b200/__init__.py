@@ -91,6 +91,7 @@ class Params(C.Structure):
         ("fixed_nucs", C.POINTER(FixedNuc)), ("n_fixed_nucs", C.c_int),
         ("nuc_volumes", C.POINTER(NucVolume)), ("n_nuc_volumes", C.c_int),
         ("precision", C.c_int), ("device", C.c_int), ("site_setup", C.c_int),
+        ("checkpoint_freq", C.c_int),
     ]
 
     @property
@@ -168,6 +169,7 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_deck_read": (I, [C.c_char_p, C.POINTER(Params)]),
         "mms_params_free_lists": (None, [C.POINTER(Params)]),
         "mms_params_size": (C.c_size_t, []),
+        "mms_test_hold_list_block": (I, [P, I, C.c_uint]),
         "mms_create": (I, [C.POINTER(Params), C.POINTER(P)]),
         "mms_destroy": (I, [P]),
         "mms_step": (I, [P, I]),
@@ -496,6 +498,12 @@ class Domain:
         _check(_lib().mms_xdmf_renumbering(self._ctx, n.value, out.ctypes.data, C.byref(n)), "mms_xdmf_renumbering",
                self._ctx)
         return out
+
+    def test_hold_list_block(self, block: int, polls: int = 0) -> None:
+        """Failure-detection test hook (mms_test_hold_list_block): from the
+        next step on, list block `block` publishes no status word and the
+        look-back waits give up after `polls` polls (-1: off)."""
+        _check(_lib().mms_test_hold_list_block(self._ctx, block, polls), "mms_test_hold_list_block", self._ctx)
 
     def set_grains(self, rotmats: np.ndarray) -> None:
         """Grains 1..n of a pre-filled microstructure (row-major 3x3 rotations)."""

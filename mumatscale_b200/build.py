@@ -71,7 +71,7 @@ def build(force: bool = False, verbose: bool = False, bounds: bool = False) -> P
         objs += [BUILD / (src + ".o") for src in CXX_SOURCES]
         if force or _stale(LIB_BOUNDS, objs):
             _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB_BOUNDS), *map(str, objs),
-                  "-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"])
+                  "-Xlinker", "--no-undefined", "-lz", "-lpthread", "-ldl", "-lrt"])
         return LIB_BOUNDS
     for src in CXX_SOURCES:
         obj = BUILD / (src + ".o")
@@ -80,7 +80,7 @@ def build(force: bool = False, verbose: bool = False, bounds: bool = False) -> P
         objs.append(obj)
     if force or _stale(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), *map(str, objs),
-              "-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"])
+              "-Xlinker", "--no-undefined", "-lz", "-lpthread", "-ldl", "-lrt"])
     main_src = CSRC / "mms_main.c"
     if force or _stale(EXE, [main_src, LIB, ROOT / "include" / "mms.h"]):
         _run([CC, "-O2", "-std=gnu11", "-o", str(EXE), str(main_src), str(LIB),

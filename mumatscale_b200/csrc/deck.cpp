@@ -184,8 +184,11 @@ mms_status parse_file(const char *path, mms_params *bp, Lists &lists, int depth,
         } else if (is("DataWriteFreq")) {
             need(std::sscanf(lp, "%d", &bp->data_write_freq), 1, token);
         } else if (is("DataWriteStart")) {
-            // read_ctrl.c:594-600 stores the value in both fields
+            // read_ctrl.c:594-600 stores the value in both fields: the data
+            // write start and the checkpoint frequency (the reference has no
+            // keyword of its own for the latter)
             need(std::sscanf(lp, "%d", &bp->data_write_start), 1, token);
+            bp->checkpoint_freq = bp->data_write_start;
         } else if (is("DataFormat")) {
             c = std::sscanf(lp, "%255s", strarg);
             if (need(c, 1, token)) {

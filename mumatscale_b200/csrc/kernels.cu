@@ -163,7 +163,19 @@ __global__ void k_am_tables(KernelArgs a, AmParams m)
         if (q < nx) {
             const double lx = (p.origin[0] + ((double)q + 0.5) * p.cellSize) - s.xnow;
             const double u = lx + m.lv * lt;
-            X[(long long)i * nx + q] = (Real)exp(-(u * u) / ai);
+            const Real xv = (Real)exp(-(u * u) / ai);
+            X[(long long)i * nx + q] = xv;
+            if (sizeof(Real) == 4 && a.d.am_ximg && q >= 1 && q <= g.gx) {
+                // the tensor-core operand image (am_tc.cu): [x tile][K-step][head,
+                // remainder][128 x 8], K-major no-swizzle core matrices
+                const int r = (q - 1) & 127, xt = (q - 1) >> 7, ks = i >> 3, k = i & 7;
+                const long long blk = ((long long)xt * (AM_NT / 8) + ks) * 2 * 1024;
+                const int off = ((r >> 3) * 256 + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4) >> 2;
+                const unsigned hu = (__float_as_uint((float)xv) + 0x1000u) & 0xffffe000u;
+                const float hi = __uint_as_float(hu);
+                a.d.am_ximg[blk + off] = hi;
+                a.d.am_ximg[blk + 1024 + off] = (float)xv - hi;
+            }
         } else if (q < nx + ny) {
             const int J = q - nx;
             const double ly = (p.origin[1] + ((double)J + 0.5) * p.cellSize) - s.ynow;
@@ -1398,11 +1410,13 @@ __device__ __forceinline__ unsigned long long ls_word(unsigned long long tag, un
 }
 
 // Bounded wait for list block j's status word of this step; returns it,
-// or 0 after about a second.
+// or 0 after `polls` polls (0: 2^22, about a second).
 __device__ __forceinline__ unsigned long long ls_wait(const unsigned long long *st, long long j,
-                                                      unsigned long long tag, unsigned long long want_state)
+                                                      unsigned long long tag, unsigned long long want_state,
+                                                      unsigned polls)
 {
-    for (unsigned it = 0; it < (1u << 22); it++) {
+    const unsigned n = polls ? polls : (1u << 22);
+    for (unsigned it = 0; it < n; it++) {
         unsigned long long w = *((volatile const unsigned long long *)&st[j]);
         if ((w >> 34) == tag && ((w >> 32) & 3ULL) >= want_state) return w;
         if (it > 32) __nanosleep(128);
@@ -1462,13 +1476,16 @@ __device__ __forceinline__ void list_body(const KernelArgs &a, int nblocks)
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         int excl = 0, ok = 1;
+        const unsigned polls = ctl->wait_polls;
+        // test hook: a held block publishes nothing (its successor's wait runs out)
+        const bool held = ctl->hold_list_block == b + 1;
         if (b > 0) {
-            if (lane == 0) *((volatile unsigned long long *)&st[b]) = ls_word(tag, LS_AGG, agg);
+            if (lane == 0 && !held) *((volatile unsigned long long *)&st[b]) = ls_word(tag, LS_AGG, agg);
             long long j0 = b - 1;
             while (true) {
                 const long long j = j0 - lane;
                 unsigned long long w = ls_word(tag, LS_PRE, 0);  // before block 0: prefix 0
-                if (j >= 0) w = ls_wait(st, j, tag, LS_AGG);
+                if (j >= 0) w = ls_wait(st, j, tag, LS_AGG, polls);
                 const int bad = __any_sync(FULL_MASK, w == 0);
                 if (bad) {
                     ok = 0;
@@ -1487,13 +1504,13 @@ __device__ __forceinline__ void list_body(const KernelArgs &a, int nblocks)
         if (lane == 0) {
             a.d.blk_off[b] = excl;
             __threadfence();
-            *((volatile unsigned long long *)&st[b]) = ls_word(tag, LS_PRE, excl + agg);
+            if (!held) *((volatile unsigned long long *)&st[b]) = ls_word(tag, LS_PRE, excl + agg);
             const long long first = (long long)r * g.blocks_per_rank;
             if (ok && b == first + g.blocks_per_rank - 1) {
                 // last block of the rank: its list length and dc_tmp bookkeeping
                 int start = excl;
                 if (b != first) {
-                    if (ls_wait(st, first, tag, LS_PRE)) {
+                    if (ls_wait(st, first, tag, LS_PRE, polls)) {
                         __threadfence();
                         start = *((volatile const int *)&a.d.blk_off[first]);
                     } else {

@@ -1132,6 +1132,7 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
     if (p.am) {
         if ((st = dalloc(ctx, &d.T, N))) return fail(st);
         if ((st = dalloc(ctx, &d.am_tab, (size_t)400 * (g.gx + g.gy + g.gz + 6) + (size_t)(g.gz + 2)))) return fail(st);
+        if (ctx->prec == MMS_PREC_F32 && (st = dalloc(ctx, &d.am_ximg, (size_t)am_ximg_size(g.gx)))) return fail(st);
         if (p.amlayer > 1 && (st = dalloc(ctx, &d.lsindex, N))) return fail(st);
     }
     if (p.tip_curv && (st = dalloc(ctx, &d.curv, N))) return fail(st);
@@ -1251,6 +1252,20 @@ mms_status mms_destroy(mms_ctx *ctx)
     delete ctx->prof;
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
+    return MMS_OK;
+}
+
+mms_status mms_test_hold_list_block(mms_ctx *ctx, int block, unsigned polls)
+{
+    if (!ctx || block < -1) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    Ctl c = *ctx->h_ctl;
+    c.hold_list_block = block + 1;
+    c.wait_polls = polls;
+    CU(h2d(ctx, ctx->ka.d.ctl, &c, sizeof c));
+    *ctx->h_ctl = c;
     return MMS_OK;
 }
 
@@ -1768,6 +1783,8 @@ mms_status mms_run(mms_ctx *ctx, int verbose)
         // run to the next screen step, or to FinishTime if that comes first
         uint64_t n = (p.screenpfreq > 0) ? (uint64_t)p.screenpfreq - (ts % (uint64_t)p.screenpfreq) : (1ULL << 30);
         if (data) n = std::min<uint64_t>(n, (uint64_t)p.data_write_freq - (ts % (uint64_t)p.data_write_freq));
+        if (p.checkpoint_freq > 0)
+            n = std::min<uint64_t>(n, (uint64_t)p.checkpoint_freq - (ts % (uint64_t)p.checkpoint_freq));
         if (p.finish_time) {
             // first t with t*ts_delt >= finish_time (checkDone, loop.c:155-156)
             uint64_t t = (uint64_t)std::floor(p.finish_time / p.ts_delt);
@@ -1791,6 +1808,10 @@ mms_status mms_run(mms_ctx *ctx, int verbose)
             fs = fs_now;
             if (verbose) screen(fs);
         }
+        // writeCheckpoint (loop.c:244-247), in this library's raw format
+        if (p.checkpoint_freq > 0 && ts % (uint64_t)p.checkpoint_freq == 0 &&
+            (st = mms_checkpoint_save(ctx, MMS_CHECKPOINT_FILE)))
+            return st;
         bool done = false;
         if (p.finish_time && ((ts * p.ts_delt) >= p.finish_time)) {
             done = true;
@@ -2554,7 +2575,7 @@ mms_status mms_checkpoint_save(mms_ctx *ctx, const char *path)
     const int cur = (int)(c.timestep & 1ULL);
     CkHeader h{};
     std::memcpy(h.magic, "MMSCKPT", 8);
-    h.version = 3;
+    h.version = 4;
     h.prec = ctx->prec;
     h.gx = g.gx;
     h.gy = g.gy;
@@ -2639,7 +2660,7 @@ mms_status mms_checkpoint_load(mms_ctx *ctx, const char *path)
         ctx->err = why;
         return s;
     };
-    if (!fread_all(fp, &h, sizeof h) || std::memcmp(h.magic, "MMSCKPT", 8) != 0 || h.version != 3)
+    if (!fread_all(fp, &h, sizeof h) || std::memcmp(h.magic, "MMSCKPT", 8) != 0 || h.version != 4)
         return fail(MMS_ERR_IO, "not a checkpoint of this library");
     if (h.prec != ctx->prec || h.gx != g.gx || h.gy != g.gy || h.gz != g.gz || h.nranks != g.nranks ||
         h.rng_cap != d.rng_cap || h.N != (int64_t)N || h.P != g.P ||

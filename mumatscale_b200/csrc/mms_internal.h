@@ -32,6 +32,13 @@ struct Ctl {
     int list_ticket;              // k_list blocks started this step
     int new_grains;               // grains created by the last activation
     int rng_used_max;             // the most draws any rank consumed since the last refill
+    // failure-detection test hook (mms_test_hold_list_block): k + 1 = the
+    // interface-list block at position k publishes no status word, so the
+    // look-back of the block after it waits for a word nothing writes; 0 =
+    // none.  wait_polls: poll bound of the look-back waits (0 = about a
+    // second, 2^22 polls)
+    int hold_list_block;
+    unsigned wait_polls;
 };
 
 enum StallReason : int {
@@ -150,6 +157,8 @@ struct DevPtrs {
     unsigned *solid_bits;  // gr > 0 after fs_change (written by the stencil)
     double *T;            // AM temperature at the current step (N) or null
     double *am_tab;       // AM quadrature tables (400 x (gx+gy+gz+6)) and plane flags
+    float *am_ximg;       // FP32 form: the X table split into TF32 head and remainder in the
+                          // tensor core's operand layout (am_tc.cu), or null
     int *lsindex;         // AM layer flag or null
     double *curv;         // curvature (N) when TipCurvature
     // nucleation sites, sorted by (emulated rank, local raster)
@@ -292,6 +301,7 @@ struct AmParams {
 // FP32 AM contraction on the tensor cores (am_tc.cu)
 int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream);
 int am_tc_prepare();
+long long am_ximg_size(int gx);  // floats of a.d.am_ximg
 // Temperature of the next step for the AM model (tables + contraction);
 // FP32 tables and sums in the FP32 form.
 int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof);

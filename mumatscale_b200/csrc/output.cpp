@@ -6,10 +6,21 @@
 // (dimx+1)(dimy+1)(dimz+1) grid points at the cell centres' coordinates
 // (scoord2realcoord, functions.c:122-139), with the cell arrays Temperature
 // (Float64) and Grain (Int32); cells and points run x-major (x outer, z
-// inner) as in the reference.  The encoding is the reference's plain-text
-// one (its USE_COMPRESSION 0 build): the zlib block encoding is not
-// reproduced.
+// inner) as in the reference.
+//
+// Encoding: the reference's default build (USE_COMPRESSION 1,
+// io_vtk.c:20-22; its plain-text branch does not compile), VTK's "binary"
+// format with vtkZLibDataCompressor.  Every data array is a list of blocks
+// (one per x plane of the subblock, or one block for offsets and types),
+// each compressed on its own with zlib's compress(); the array is written as
+// the base64 text of its header, uint32 {number of blocks, block size, 0,
+// compressed size of each block}, followed by the base64 text of the
+// concatenated compressed blocks (vtkCompress.c:86-129).  With the same zlib
+// the files are byte-identical to the reference's.
+#include <zlib.h>
+
 #include <cerrno>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -27,6 +38,48 @@ double real_coord(const mms_params &p, int axis, long long c)
     return p.origin_offset[axis] + ((double)c + 0.5) * p.cellSize;
 }
 
+// Base64 (RFC 4648 alphabet, '=' padding) of len bytes.
+void put_base64(FILE *fp, const unsigned char *d, size_t len)
+{
+    static const char tab[] = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/";
+    std::string out;
+    out.reserve((len + 2) / 3 * 4);
+    for (size_t i = 0; i < len; i += 3) {
+        const size_t n = len - i < 3 ? len - i : 3;
+        const unsigned v = (unsigned)d[i] << 16 | (n > 1 ? (unsigned)d[i + 1] << 8 : 0u) | (n > 2 ? d[i + 2] : 0u);
+        out += tab[(v >> 18) & 63];
+        out += tab[(v >> 12) & 63];
+        out += n > 1 ? tab[(v >> 6) & 63] : '=';
+        out += n > 2 ? tab[v & 63] : '=';
+    }
+    std::fwrite(out.data(), 1, out.size(), fp);
+}
+
+// One data array in VTK's zlib block encoding.
+struct ZBlocks {
+    std::vector<uint32_t> hdr{0, 0, 0};  // blocks, block size, last-block size (0: full)
+    std::vector<unsigned char> data;
+    std::vector<unsigned char> tmp;
+    bool ok = true;
+    void add(const void *p, uint32_t len)
+    {
+        if (hdr[0] == 0) hdr[1] = len;
+        else if (len != hdr[1]) ok = false;
+        hdr[0]++;
+        uLongf n = compressBound(len);
+        tmp.resize(n);
+        if (compress(tmp.data(), &n, (const Bytef *)p, len) != Z_OK) ok = false;
+        hdr.push_back((uint32_t)n);
+        data.insert(data.end(), tmp.begin(), tmp.begin() + n);
+    }
+    bool write(FILE *fp) const
+    {
+        put_base64(fp, (const unsigned char *)hdr.data(), hdr.size() * sizeof(uint32_t));
+        put_base64(fp, data.data(), data.size());
+        return ok;
+    }
+};
+
 bool write_pvtu(const mms_params &p, const std::string &base, long long ts)
 {
     const std::string fn = base + "_" + std::to_string(ts) + ".pvtu";
@@ -40,7 +93,7 @@ bool write_pvtu(const mms_params &p, const std::string &base, long long ts)
     std::fprintf(fp, "      <PDataArray type=\"Int32\" Name=\"Grain\"/>\n");
     std::fprintf(fp, "    </PCellData>\n");
     std::fprintf(fp, "    <PPoints>\n");
-    std::fprintf(fp, "      <PDataArray type=\"Float32\" NumberOfComponents=\"3\"/>\n");
+    std::fprintf(fp, "      <PDataArray type=\"Float64\" NumberOfComponents=\"3\"/>\n");
     std::fprintf(fp, "    </PPoints>\n");
     const int nsub = p.gnsbx * p.gnsby * p.gnsbz;
     for (int s = 0; s < nsub; s++)
@@ -68,54 +121,97 @@ bool write_vtu(const mms_params &p, const std::string &base, long long ts, int s
     };
     const long long ncells = (long long)dimx * dimy * dimz;
     const long long npoints = (long long)(dimx + 1) * (dimy + 1) * (dimz + 1);
+    bool ok = true;
     std::fprintf(fp, "<?xml version=\"1.0\"?>\n");
-    std::fprintf(fp, "<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n");
+    std::fprintf(fp, "<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\" "
+                     "compressor=\"vtkZLibDataCompressor\">\n");
     std::fprintf(fp, "  <UnstructuredGrid>\n");
     std::fprintf(fp, "      <Piece NumberOfPoints=\"%lld\" NumberOfCells=\"%lld\" >\n", npoints, ncells);
     std::fprintf(fp, "        <CellData>\n");
-    std::fprintf(fp, "        <DataArray type=\"Float64\" Name=\"Temperature\" format=\"ascii\">\n");
-    for (int i = 1; i <= dimx; i++)
-        for (int j = 1; j <= dimy; j++)
-            for (int k = 1; k <= dimz; k++) std::fprintf(fp, "%lf\n", T[gidx(i, j, k)]);
-    std::fprintf(fp, "\n        </DataArray>\n");
-    std::fprintf(fp, "        <DataArray type=\"Int32\" Name=\"Grain\" format=\"ascii\">\n");
-    for (int i = 1; i <= dimx; i++)
-        for (int j = 1; j <= dimy; j++)
-            for (int k = 1; k <= dimz; k++) std::fprintf(fp, "%d\n", gr[gidx(i, j, k)]);
-    std::fprintf(fp, "\n        </DataArray>\n");
+    {
+        // writeDataArrayFloat / writeDataArrayInt32: one block per x plane
+        ZBlocks bt, bg;
+        std::vector<double> tv((size_t)dimy * dimz);
+        std::vector<int32_t> gv((size_t)dimy * dimz);
+        for (int i = 1; i <= dimx; i++) {
+            size_t n = 0;
+            for (int j = 1; j <= dimy; j++)
+                for (int k = 1; k <= dimz; k++, n++) {
+                    tv[n] = T[gidx(i, j, k)];
+                    gv[n] = gr[gidx(i, j, k)];
+                }
+            bt.add(tv.data(), (uint32_t)(tv.size() * sizeof(double)));
+            bg.add(gv.data(), (uint32_t)(gv.size() * sizeof(int32_t)));
+        }
+        std::fprintf(fp, "        <DataArray type=\"Float64\" Name=\"Temperature\" format=\"binary\">\n");
+        ok &= bt.write(fp);
+        std::fprintf(fp, "\n        </DataArray>\n");
+        std::fprintf(fp, "        <DataArray type=\"Int32\" Name=\"Grain\" format=\"binary\">\n");
+        ok &= bg.write(fp);
+        std::fprintf(fp, "\n        </DataArray>\n");
+    }
     std::fprintf(fp, "      </CellData>\n");
     std::fprintf(fp, "      <Points>\n");
-    std::fprintf(fp, "        <DataArray type=\"Float32\" NumberOfComponents=\"3\" format=\"ascii\">\n");
-    for (int i = 0; i <= dimx; i++)
-        for (int j = 0; j <= dimy; j++)
-            for (int k = 0; k <= dimz; k++)
-                std::fprintf(fp, "%g %g %g\n", (float)real_coord(p, 0, (long long)sx * dimx + i),
-                             (float)real_coord(p, 1, (long long)sy * dimy + j),
-                             (float)real_coord(p, 2, (long long)sz * dimz + k));
+    std::fprintf(fp, "        <DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"binary\">\n");
+    {
+        ZBlocks b;
+        std::vector<double> v((size_t)3 * (dimy + 1) * (dimz + 1));
+        for (int i = 0; i <= dimx; i++) {
+            size_t n = 0;
+            for (int j = 0; j <= dimy; j++)
+                for (int k = 0; k <= dimz; k++) {
+                    v[n++] = real_coord(p, 0, (long long)sx * dimx + i);
+                    v[n++] = real_coord(p, 1, (long long)sy * dimy + j);
+                    v[n++] = real_coord(p, 2, (long long)sz * dimz + k);
+                }
+            b.add(v.data(), (uint32_t)(v.size() * sizeof(double)));
+        }
+        ok &= b.write(fp);
+    }
     std::fprintf(fp, "        </DataArray>\n");
     std::fprintf(fp, "      </Points>\n");
     std::fprintf(fp, "      <Cells>\n");
-    std::fprintf(fp, "        <DataArray type=\"Int32\" Name=\"connectivity\" format=\"ascii\">\n");
-    const long long row = dimz + 1, plane = (long long)(dimy + 1) * (dimz + 1);
-    for (int i = 0; i < dimx; i++)
-        for (int j = 0; j < dimy; j++)
-            for (int k = 0; k < dimz; k++) {
-                const long long c0 = i * plane + j * row + k;
-                std::fprintf(fp, "%lld %lld %lld %lld %lld %lld %lld %lld\n", c0, c0 + 1, c0 + row, c0 + row + 1,
-                             c0 + plane, c0 + plane + 1, c0 + plane + row, c0 + plane + row + 1);
-            }
+    std::fprintf(fp, "        <DataArray type=\"Int32\" Name=\"connectivity\" format=\"binary\">\n");
+    {
+        ZBlocks b;
+        std::vector<int32_t> v((size_t)dimy * dimz * 8);
+        const int row = dimz + 1, plane = (dimy + 1) * (dimz + 1);
+        for (int i = 0; i < dimx; i++) {
+            size_t n = 0;
+            for (int j = 0; j < dimy; j++)
+                for (int k = 0; k < dimz; k++) {
+                    const int c0 = i * plane + j * row + k;
+                    const int32_t q[8] = {c0, c0 + 1, c0 + row, c0 + row + 1,
+                                          c0 + plane, c0 + plane + 1, c0 + plane + row, c0 + plane + row + 1};
+                    for (int e = 0; e < 8; e++) v[n++] = q[e];
+                }
+            b.add(v.data(), (uint32_t)(v.size() * sizeof(int32_t)));
+        }
+        ok &= b.write(fp);
+    }
     std::fprintf(fp, "        </DataArray>\n");
-    std::fprintf(fp, "        <DataArray type=\"Int32\" Name=\"offsets\" format=\"ascii\">\n");
-    for (long long n = 1; n <= ncells; n++) std::fprintf(fp, "%lld ", n * 8);
-    std::fprintf(fp, "\n        </DataArray>\n");
-    std::fprintf(fp, "        <DataArray type=\"UInt8\" Name=\"types\" format=\"ascii\">\n");
-    for (long long n = 1; n <= ncells; n++) std::fprintf(fp, "%d ", 11);
-    std::fprintf(fp, "\n        </DataArray>\n");
-    std::fprintf(fp, "      </Cells>\n");
+    std::fprintf(fp, "        <DataArray type=\"Int32\" Name=\"offsets\" format=\"binary\">\n");
+    {
+        ZBlocks b;
+        std::vector<int32_t> v((size_t)ncells);
+        for (long long n = 1; n <= ncells; n++) v[n - 1] = (int32_t)(n * 8);
+        b.add(v.data(), (uint32_t)(v.size() * sizeof(int32_t)));
+        ok &= b.write(fp);
+    }
+    std::fprintf(fp, "        </DataArray>\n");
+    std::fprintf(fp, "        <DataArray type=\"UInt8\" Name=\"types\" format=\"binary\">\n");
+    {
+        ZBlocks b;
+        std::vector<unsigned char> v((size_t)ncells, 11);  // VTK_VOXEL
+        b.add(v.data(), (uint32_t)v.size());
+        ok &= b.write(fp);
+    }
+    std::fprintf(fp, "        </DataArray>\n");
+    std::fprintf(fp, "       </Cells>\n");
     std::fprintf(fp, "    </Piece>\n");
     std::fprintf(fp, "  </UnstructuredGrid>\n");
     std::fprintf(fp, "</VTKFile>\n");
-    return std::fclose(fp) == 0;
+    return (std::fclose(fp) == 0) && ok;
 }
 
 }  // namespace

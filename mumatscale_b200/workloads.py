@@ -123,13 +123,11 @@ Density {100 / 3e-5 / 395!r}
                        rho_v=1e14, mu=3.0, sigma=1.0, rho_s=0.0, max_grains=1000000, seed=seed, extra=extra)
 
 
-def columnar_substrate(shape_zyx, dx: float, top_plane: int, mean_width: float = 20e-6, seed: int = 11):
-    """Columnar grains filling interior planes 1..top_plane: a Voronoi
-    tessellation of the x-y plane with one seed per mean_width^2, random
-    orientations.  Returns (gr, rotmats (n x 9)) with gr in the halo'd
-    layout (int32, zeros outside the substrate)."""
-    nz, ny, nx = shape_zyx
-    gx, gy = nx - 2, ny - 2
+def columnar_columns(gx: int, gy: int, dx: float, mean_width: float = 20e-6, seed: int = 11):
+    """Grain id of every (x, y) column of a columnar substrate: a Voronoi
+    tessellation of the x-y plane with one seed per mean_width^2, ids 1..n;
+    and the n grains' rotation matrices (row-major, random orientations).
+    Returns (cols (gy x gx int32), rotmats (n x 9))."""
     rng = np.random.default_rng(seed)
     n = max(1, int(round(gx * gy * dx * dx / (mean_width * mean_width))))
     sx = rng.uniform(0, gx, n)
@@ -143,11 +141,31 @@ def columnar_substrate(shape_zyx, dx: float, top_plane: int, mean_width: float =
         m = d < bd
         bd[m] = d[m]
         best[m] = s
-    cols = (best + 1).reshape(gy, gx)
+    cols = (best + 1).reshape(gy, gx).astype(np.int32)
+    rot = np.stack([quat_to_rotmat(q).ravel() for q in random_quaternions(rng, n)])
+    return cols, rot
+
+
+def columnar_substrate(shape_zyx, dx: float, top_plane: int, mean_width: float = 20e-6, seed: int = 11):
+    """Columnar grains filling interior planes 1..top_plane (see
+    columnar_columns).  Returns (gr, rotmats (n x 9)) with gr in the halo'd
+    layout (int32, zeros outside the substrate)."""
+    nz, ny, nx = shape_zyx
+    cols, rot = columnar_columns(nx - 2, ny - 2, dx, mean_width, seed)
     gr = np.zeros(shape_zyx, dtype=np.int32)
     gr[1:top_plane + 1, 1:-1, 1:-1] = cols[None]
-    rot = np.stack([quat_to_rotmat(q).ravel() for q in random_quaternions(rng, n)])
     return gr, rot
+
+
+def write_substrate_file(path, cols: np.ndarray, rot: np.ndarray, top_plane: int) -> None:
+    """The same substrate for the reference, in the format its harness reads
+    (MMSREF_INJECT_SUBSTRATE of oracle/ref_shim/ref_hooks.c): int32 gx, gy,
+    top, n; int32 cols[gy][gx]; f64 rot[n][9]."""
+    gy, gx = cols.shape
+    with open(path, "wb") as f:
+        f.write(np.array([gx, gy, top_plane, len(rot)], dtype="<i4").tobytes())
+        f.write(np.ascontiguousarray(cols, dtype="<i4").tobytes())
+        f.write(np.ascontiguousarray(rot, dtype="<f8").tobytes())
 
 
 def setup_substrate(dom, top_plane: int, dx: float, mean_width: float = 20e-6, seed: int = 11) -> int:

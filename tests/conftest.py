@@ -14,7 +14,7 @@ GOLDEN = ROOT / "tests" / "golden"
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
-GOLDEN_DECKS = ["small1", "small4", "cap1", "curv1", "grad1", "nucvol1", "am1"]
+GOLDEN_DECKS = ["small1", "small4", "cap1", "curv1", "grad1", "nucvol1", "am1", "amsub4"]
 
 
 def pytest_configure(config):
@@ -38,6 +38,34 @@ def golden(name: str) -> dict:
 
 def golden_deck(name: str) -> Path:
     return GOLDEN / golden(name)["deck"]
+
+
+def setup_golden_substrate(target, name: str) -> int:
+    """Pre-fills the columnar substrate a golden deck was recorded with (the
+    reference got it through MMSREF_INJECT_SUBSTRATE): grains 1..n with their
+    rotations, their ids in interior planes 1..top and fs = 1 there.  target:
+    a mumatscale_b200.Domain or a tests._oracle.Oracle before its first step.
+    Returns n (0 when the deck has no substrate)."""
+    rec = golden(name).get("substrate")
+    if not rec:
+        return 0
+    import hashlib
+    import mumatscale_b200 as M
+    from mumatscale_b200 import workloads as W
+    p = M.read_deck(golden_deck(name))
+    gx, gy = p.gnsbx * p.gsdimx, p.gnsby * p.gsdimy
+    cols, rot = W.columnar_columns(gx, gy, p.cellSize, rec["mean_width"], rec["seed"])
+    # the same substrate as the recording (seeded generator)
+    assert hashlib.sha256(cols.astype("<i4").tobytes()).hexdigest() == rec["cols"]
+    assert hashlib.sha256(rot.astype("<f8").tobytes()).hexdigest() == rec["rotmat"]
+    gr = target.download("gr")
+    fs = target.download("fs")
+    gr[1:rec["top_plane"] + 1, 1:-1, 1:-1] = cols[None]
+    fs[gr > 0] = 1.0
+    target.set_grains(rot)
+    target.upload("gr", gr)
+    target.upload("fs", fs)
+    return len(rot)
 
 
 @pytest.fixture(scope="session")

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import mumatscale_b200 as M
-from conftest import GOLDEN_DECKS, golden, golden_deck
+from conftest import GOLDEN_DECKS, golden, golden_deck, setup_golden_substrate
 from digests import digest, mismatches, state_digests
 
 pytestmark = pytest.mark.gpu
@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 # CUDA's exp is not glibc's, so once the laser is on (t >= 1e-4 s, step 100
 # of am1) temperatures differ in the last bits and the AM deck is compared
 # with tolerances (test_am_tolerance) instead of bit for bit.
-EXACT_UNTIL = {"am1": 100}
+EXACT_UNTIL = {"am1": 100, "amsub4": 7}
 
 
 @pytest.mark.parametrize("name", GOLDEN_DECKS)
@@ -28,6 +28,7 @@ def test_fp64_bit_exact_vs_reference(built, cuda_device, name):
     p = M.read_deck(golden_deck(name))
     with M.Domain(p, precision=M.PREC_F64) as dom:
         assert digest(dom.download("nuc_threshold")) == rec["setup"]["nuc_threshold"]
+        setup_golden_substrate(dom, name)
         last = 0
         for s, want in rec["steps"].items():
             s = int(s)

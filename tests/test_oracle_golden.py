@@ -6,8 +6,13 @@ from __future__ import annotations
 import pytest
 
 import mumatscale_b200 as M
-from conftest import GOLDEN_DECKS, golden, golden_deck
+from conftest import GOLDEN_DECKS, golden, golden_deck, setup_golden_substrate
 from digests import digest, mismatches, state_digests
+
+# recorded steps checked on the CPU, where the whole record would take long:
+# amsub4's laser turns on at step 8 (400 exponentials per cell and step from
+# then on in the CPU oracle, as in the reference)
+MAX_STEP = {"amsub4": 20}
 
 
 @pytest.mark.parametrize("name", GOLDEN_DECKS)
@@ -17,9 +22,12 @@ def test_oracle_matches_reference_dumps(built, name):
     p = M.read_deck(golden_deck(name))
     o = Oracle(p, curvature=bool(rec["env"].get("MMSREF_CURV")))
     assert digest(o.download("nuc_threshold")) == rec["setup"]["nuc_threshold"]
+    setup_golden_substrate(o, name)
     last = 0
     for s, want in rec["steps"].items():
         s = int(s)
+        if s > MAX_STEP.get(name, 1 << 30):
+            break
         o.step(s - last)
         last = s
         assert o.timestep == s

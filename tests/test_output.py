@@ -1,4 +1,4 @@
-"""ParaView output in the io_vtk.c layout (host side; no GPU)."""
+"""ParaView (io_vtk.c) and XDMF (io_xdmf.c) output in the reference's layouts."""
 from __future__ import annotations
 
 import xml.etree.ElementTree as ET
@@ -20,6 +20,28 @@ def _arr(piece, name):
     raise KeyError(name)
 
 
+_DT = {"Float64": "<f8", "Int32": "<i4", "UInt8": "u1"}
+
+
+def _decode(da) -> np.ndarray:
+    """A DataArray in VTK's zlib block encoding (vtkZLibDataCompressor, 32-bit
+    header): base64 header {blocks, block size, last size, compressed sizes},
+    then the base64 of the concatenated zlib blocks."""
+    import base64
+    import zlib
+    text = "".join(da.text.split())
+    nb = int(np.frombuffer(base64.b64decode(text[:8])[:4], "<u4")[0])
+    hlen = (3 + nb) * 4
+    henc = (hlen + 2) // 3 * 4
+    hdr = np.frombuffer(base64.b64decode(text[:henc]), "<u4")
+    data = base64.b64decode(text[henc:])
+    out, off = [], 0
+    for c in hdr[3:3 + nb]:
+        out.append(zlib.decompress(data[off:off + c]))
+        off += int(c)
+    return np.frombuffer(b"".join(out), _DT[da.get("type")])
+
+
 def test_vtk_layout_matches_reference_writer(built, tmp_path):
     p = M.read_deck(golden_deck("small4"))          # 2 x 2 x 1 subblocks
     gx, gy, gz = p.grid
@@ -36,27 +58,58 @@ def test_vtk_layout_matches_reference_writer(built, tmp_path):
     for s in range(nsub):
         sx, sy, sz = s % p.gnsbx, (s // p.gnsbx) % p.gnsby, s // (p.gnsbx * p.gnsby)
         root = ET.parse(f"{base}_{s:04d}/42.vtu").getroot()
+        assert root.get("compressor") == "vtkZLibDataCompressor"
         piece = next(root.iter("Piece"))
         assert int(piece.get("NumberOfCells")) == dx * dy * dz
         assert int(piece.get("NumberOfPoints")) == (dx + 1) * (dy + 1) * (dz + 1)
-        temp = np.array(_arr(piece, "Temperature").text.split(), dtype=float)
-        grain = np.array(_arr(piece, "Grain").text.split(), dtype=int)
+        temp = _decode(_arr(piece, "Temperature"))
+        grain = _decode(_arr(piece, "Grain"))
         # writeDataArrayFloat/Int32 (io_vtk.c:95-200): x outer, z inner, interior cells
         sub = (slice(sz * dz + 1, sz * dz + dz + 1), slice(sy * dy + 1, sy * dy + dy + 1),
                slice(sx * dx + 1, sx * dx + dx + 1))
-        want_t = np.transpose(T[sub], (2, 1, 0)).ravel()
-        assert np.allclose(temp, want_t, rtol=0, atol=5e-7)          # "%lf"
+        assert np.array_equal(temp, np.transpose(T[sub], (2, 1, 0)).ravel())   # raw doubles
         assert np.array_equal(grain, np.transpose(gr[sub], (2, 1, 0)).ravel())
-        types = np.array(_arr(piece, "types").text.split(), dtype=int)
+        types = _decode(_arr(piece, "types"))
         assert (types == 11).all() and len(types) == dx * dy * dz
-        offs = np.array(_arr(piece, "offsets").text.split(), dtype=int)
+        offs = _decode(_arr(piece, "offsets"))
         assert offs[0] == 8 and offs[-1] == 8 * dx * dy * dz
-        conn = np.array(_arr(piece, "connectivity").text.split(), dtype=int).reshape(-1, 8)
+        conn = _decode(_arr(piece, "connectivity")).reshape(-1, 8)
         row, plane = dz + 1, (dy + 1) * (dz + 1)
         assert list(conn[0]) == [0, 1, row, row + 1, plane, plane + 1, plane + row, plane + row + 1]
-        pts = np.array(next(piece.iter("Points")).find("DataArray").text.split(), dtype=float).reshape(-1, 3)
-        x0 = p.origin_offset[0] + (sx * dx + 0.5) * p.cellSize
-        assert abs(pts[0, 0] - x0) <= 1e-6 * abs(x0) + 1e-12
+        pts = _decode(next(piece.iter("Points")).find("DataArray")).reshape(-1, 3)
+        assert pts[0, 0] == p.origin_offset[0] + (sx * dx + 0.5) * p.cellSize
+
+
+def _vtk_deck(tmp_path: Path) -> Path:
+    from conftest import golden
+    rec = golden("vtk_small4")
+    deck = tmp_path / "small4_vtk.in"
+    deck.write_text(golden_deck("small4").read_text() + "\n" + "\n".join(rec["extra"]) + "\n")
+    return deck
+
+
+def test_vtk_bytes_match_reference_files(built, tmp_path):
+    """The writer fed with the CPU oracle's fields (pinned to the reference)
+    produces the reference's own VTK files byte for byte: small4 with
+    DataFormat VTK and DataWriteFreq 200, steps 0, 200, 400, 401."""
+    import hashlib
+    from _oracle import Oracle
+    from conftest import golden
+    want = golden("vtk_small4")["files"]
+    p = M.read_deck(golden_deck("small4"))
+    o = Oracle(p)
+    import os
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        for ts in (0, 200, 400, 401):
+            o.step(ts - o.timestep)
+            M.write_vtk_arrays(p, "small4", ts, o.download("temperature"), o.download("gr"))
+    finally:
+        os.chdir(cwd)
+    got = {str(f.relative_to(tmp_path)): hashlib.sha256(f.read_bytes()).hexdigest()
+           for f in sorted(tmp_path.rglob("*")) if f.suffix in (".vtu", ".pvtu")}
+    assert got == want
 
 
 @pytest.mark.gpu
@@ -67,7 +120,7 @@ def test_vtk_from_device(built, cuda_device, tmp_path):
         base = str(tmp_path / "dev")
         dom.write_vtk(base)
         piece = next(ET.parse(f"{base}_0000/100.vtu").getroot().iter("Piece"))
-        grain = np.array(_arr(piece, "Grain").text.split(), dtype=int)
+        grain = _decode(_arr(piece, "Grain"))
         gr = dom.download("gr")[1:-1, 1:-1, 1:-1]
         assert np.array_equal(grain, np.transpose(gr, (2, 1, 0)).ravel())
 
@@ -238,8 +291,30 @@ def test_run_loop_writes_vtk(built, cuda_device, tmp_path):
         assert (tmp_path / f"v4_{ts}.pvtu").exists(), ts
     nsub = p.gnsbx * p.gnsby * p.gnsbz
     piece = ET.parse(tmp_path / "v4_0000" / "401.vtu").getroot()
-    got = np.array(_arr(piece, "Grain").text.split(), dtype=np.int32)
+    got = _decode(_arr(piece, "Grain"))
     sd = (p.gsdimz, p.gsdimy, p.gsdimx)
     # subblock 0, cells in the reference's x-major order (x outer, z inner)
     want = gr[1:sd[0] + 1, 1:sd[1] + 1, 1:sd[2] + 1].transpose(2, 1, 0).reshape(-1)
     assert nsub == 4 and np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_run_loop_vtk_bytes_match_reference(built, cuda_device, tmp_path):
+    """mmsb200's run loop on small4 with DataFormat VTK writes the very files
+    the reference writes (digests recorded from the reference itself)."""
+    import hashlib
+    import os
+    from conftest import golden
+    want = golden("vtk_small4")["files"]
+    deck = _vtk_deck(tmp_path)
+    p = M.read_deck(deck)
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        with M.Domain(p, precision=M.PREC_F64) as dom:
+            dom.run(verbose=0)
+    finally:
+        os.chdir(cwd)
+    got = {str(f.relative_to(tmp_path)): hashlib.sha256(f.read_bytes()).hexdigest()
+           for f in sorted(tmp_path.rglob("*")) if f.suffix in (".vtu", ".pvtu")}
+    assert got == want
