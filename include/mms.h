@@ -138,6 +138,16 @@ typedef struct mms_params {
      * checkpoint_freq steps, as loop.c:244-247 calls writeCheckpoint;
      * 0 = never */
     int checkpoint_freq;
+    /* No counterpart in the reference.  0: sb_curvature as the reference
+     * writes it (curvature.c:81-405), quirks included: the normal is
+     * normalised only when its length is 0 (curvature.c:194), a height
+     * direction is chosen only when some normal component is exactly 0
+     * (curvature.c:203), so curvature is 0 on generic interfaces, and the
+     * upper smoothed face takes fs[idl] for fs[idu] (curvature.c:176).
+     * 1: those three corrected (normalised when non-zero, the dominant
+     * component always chosen, fs[idu]); for studies of the Gibbs-Thomson
+     * term, not for parity. */
+    int curvature_corrected;
 } mms_params;
 
 typedef enum mms_field {
@@ -152,8 +162,10 @@ typedef enum mms_field {
     MMS_FIELD_NUC_THRESHOLD = 6, /* f32 [N]   nucleation undercooling, +inf = no site */
     MMS_FIELD_TEMPERATURE = 7,   /* f64 [N]   temperature at the current timestep (download only) */
     MMS_FIELD_MOLD = 8,          /* i8  [N]   mold flag (download only) */
-    MMS_FIELD_OGR = 9            /* i32 [N]   grain ids before the last capture, the
+    MMS_FIELD_OGR = 9,           /* i32 [N]   grain ids before the last capture, the
                                                 reference's ogr (growth.c:635-638; download only) */
+    MMS_FIELD_CURV = 10          /* f64 [N]   curvature the last step used (TipCurvature 1;
+                                                zeros otherwise; download only) */
 } mms_field;
 
 typedef enum mms_reduction {

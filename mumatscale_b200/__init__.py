@@ -31,12 +31,12 @@ PREC_F32 = 1
 
 FIELD = {
     "ce": 0, "cl": 1, "fs": 2, "gr": 3, "dc": 4, "d": 5,
-    "nuc_threshold": 6, "temperature": 7, "mold": 8, "ogr": 9,
+    "nuc_threshold": 6, "temperature": 7, "mold": 8, "ogr": 9, "curv": 10,
 }
 _FIELD_DTYPE = {
     0: (np.float64, 1), 1: (np.float64, 1), 2: (np.float64, 1), 3: (np.int32, 1),
     4: (np.float64, 3), 5: (np.float64, 1), 6: (np.float32, 1), 7: (np.float64, 1),
-    8: (np.int8, 1), 9: (np.int32, 1),
+    8: (np.int8, 1), 9: (np.int32, 1), 10: (np.float64, 1),
 }
 REDUCE = {"fs_fraction": 0, "solid_volume": 1, "ce_sum": 2}
 
@@ -91,7 +91,7 @@ class Params(C.Structure):
         ("fixed_nucs", C.POINTER(FixedNuc)), ("n_fixed_nucs", C.c_int),
         ("nuc_volumes", C.POINTER(NucVolume)), ("n_nuc_volumes", C.c_int),
         ("precision", C.c_int), ("device", C.c_int), ("site_setup", C.c_int),
-        ("checkpoint_freq", C.c_int),
+        ("checkpoint_freq", C.c_int), ("curvature_corrected", C.c_int),
     ]
 
     @property

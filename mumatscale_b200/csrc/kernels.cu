@@ -723,19 +723,25 @@ __global__ void k_curv(KernelArgs a)
                   alpha * (fs(idfl) + fs(idfr) + fs(iduf) + fs(iddf)) + beta * fs(idf)) / (1 + 4 * alpha + beta);
     double fsb = (fs(idubr) + fs(idubl) + fs(iddbl) + fs(iddbr) +
                   alpha * (fs(idbl) + fs(idbr) + fs(idub) + fs(iddb)) + beta * fs(idb)) / (1 + 4 * alpha + beta);
+    // the reference weights fs[idl] here (curvature.c:176); corrected: fs[idu]
+    const bool fixed = a.p.curv_fixed != 0;
     double fsu = (fs(idufl) + fs(idufr) + fs(idubr) + fs(idubl) +
-                  alpha * (fs(idul) + fs(idur) + fs(idub) + fs(iduf)) + beta * fs(idl)) / (1 + 4 * alpha + beta);
+                  alpha * (fs(idul) + fs(idur) + fs(idub) + fs(iduf)) + beta * fs(fixed ? idu : idl)) /
+                 (1 + 4 * alpha + beta);
     double fsd = (fs(iddbr) + fs(iddbl) + fs(iddfl) + fs(iddfr) +
                   alpha * (fs(iddr) + fs(iddl) + fs(iddf) + fs(iddb)) + beta * fs(idd)) / (1 + 4 * alpha + beta);
     double nx = (fsl - fsr_) / 2.0, ny = (fsf - fsb) / 2.0, nz = (fsu - fsd) / 2.0;
     double nall = sqrt(nx * nx + ny * ny + nz * nz);
-    if (!(nall)) {
+    // the reference normalises only a zero normal (curvature.c:194) and picks
+    // a height direction only when a component is exactly zero
+    // (curvature.c:203); corrected: a non-zero normal, and always
+    if (fixed ? (nall != 0.0) : !(nall)) {
         nx = nx / nall;
         ny = ny / nall;
         nz = nz / nall;
     }
     int nor_dir = 0;
-    if (!(nx) || !(ny) || !(nz)) {
+    if (fixed || !(nx) || !(ny) || !(nz)) {
         if ((fabs(nx) >= fabs(ny)) && (fabs(nx) >= fabs(nz))) nor_dir = 1;
         else if ((fabs(ny) >= fabs(nz)) && (fabs(ny) >= fabs(nx))) nor_dir = 2;
         else if ((fabs(nz) >= fabs(ny)) && (fabs(nz) >= fabs(nx))) nor_dir = 3;
@@ -1035,8 +1041,20 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
     long long crow = (long long)k0 * g.sz + (long long)j * g.sy;
     bool alive = true;
     double fsum = 0.0;  // this thread's new fs values, in plane order
+    // AM temperature array: each cell's value is loaded one plane ahead, so
+    // that its latency overlaps a plane of work
+    const bool t_arr = p.temp_mode == 2;
+    double Tn[CPT];
+#pragma unroll
+    for (int u = 0; u < CPT; u++) Tn[u] = (t_arr && act[u]) ? __ldg(a.d.T + crow + i0 + tx + DTX * u) : 0.0;
     for (int t = 0; t <= k1 - k0; t++) {
         const int k = k0 + t;
+        double Tc[CPT];
+#pragma unroll
+        for (int u = 0; u < CPT; u++) {
+            Tc[u] = Tn[u];
+            if (t_arr && act[u] && t < k1 - k0) Tn[u] = __ldg(a.d.T + crow + g.sz + i0 + tx + DTX * u);
+        }
         // planes t and t+1 completed in earlier iterations
         bool ok = mbar_wait(&bars[s2], ph2);
         if (t == 0) ok &= mbar_wait(&bars[s0], phase(0)) && mbar_wait(&bars[s1], phase(1));
@@ -1065,7 +1083,7 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
                 const long long c = crow + i;
                 const Real oce = sce[hcc[u]];
                 const int grc = sgr[hgg[u]];
-                const double Td = t_per_plane ? Tp : temp_cell(p, a.d.T, c, j, k, ts);
+                const double Td = t_per_plane ? Tp : (t_arr ? Tc[u] : temp_cell(p, a.d.T, c, j, k, ts));
                 const bool interior = in_xy[u] && in_z;
                 Real cen, cl_new, fs_new;
                 int gr_new, br;

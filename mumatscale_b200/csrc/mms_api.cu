@@ -1086,6 +1086,7 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
     ph.Tliq = p.liquidusTemp;
     ph.Tsol = p.solidusTemp;
     ph.tip_curv = p.tip_curv;
+    ph.curv_fixed = p.curvature_corrected;
     ph.gibbs = p.gibbs_coef;
     ph.fsgrow = p.rev_fsgrow;
     ph.max_grains = p.maxTotalGrains;
@@ -1568,6 +1569,13 @@ mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
     }
     case MMS_FIELD_DC:
         CU(copy_out(ctx, host, d.dc, sizeof(Dc3)));
+        return MMS_OK;
+    case MMS_FIELD_CURV:
+        if (!d.curv) {
+            std::memset(host, 0, (size_t)g.rN * sizeof(double));
+            return MMS_OK;
+        }
+        CU(copy_out(ctx, host, d.curv, sizeof(double)));
         return MMS_OK;
     case MMS_FIELD_D:
     case MMS_FIELD_TEMPERATURE: {

@@ -123,6 +123,7 @@ struct Phys {
     // fs change (growth.c:181-197)
     double liq_slope, k_inv, km, km_inv, m_inv, D_xt, cinit, Tliq, Tsol;
     int tip_curv;
+    int curv_fixed;  // mms_params.curvature_corrected
     double gibbs;
     // growth (growth.c:348)
     double fsgrow;

@@ -887,21 +887,24 @@ static void curvature(mmso *o)
                     double fsb = (fs[idubr] + fs[idubl] + fs[iddbl] + fs[iddbr] +
                                   alpha * (fs[idbl] + fs[idbr] + fs[idub] + fs[iddb]) +
                                   beta * fs[idb]) / (1 + 4 * alpha + beta);
+                    /* curvature.c:176 weights fs[idl]; the corrected option fs[idu] */
+                    const int fixed = p->curvature_corrected != 0;
                     double fsu = (fs[idufl] + fs[idufr] + fs[idubr] + fs[idubl] +
                                   alpha * (fs[idul] + fs[idur] + fs[idub] + fs[iduf]) +
-                                  beta * fs[idl]) / (1 + 4 * alpha + beta);
+                                  beta * fs[fixed ? idu : idl]) / (1 + 4 * alpha + beta);
                     double fsd = (fs[iddbr] + fs[iddbl] + fs[iddfl] + fs[iddfr] +
                                   alpha * (fs[iddr] + fs[iddl] + fs[iddf] + fs[iddb]) +
                                   beta * fs[idd]) / (1 + 4 * alpha + beta);
                     double nx_ = (fsl - fsr) / 2.0, ny_ = (fsf - fsb) / 2.0, nz_ = (fsu - fsd) / 2.0;
                     double nall = sqrt(nx_ * nx_ + ny_ * ny_ + nz_ * nz_);
-                    if (!(nall)) {
+                    /* curvature.c:194 and 203 as written, or corrected */
+                    if (fixed ? (nall != 0.0) : !(nall)) {
                         nx_ = nx_ / nall;
                         ny_ = ny_ / nall;
                         nz_ = nz_ / nall;
                     }
                     int nor_dir = 0;
-                    if (!(nx_) || !(ny_) || !(nz_)) {
+                    if (fixed || !(nx_) || !(ny_) || !(nz_)) {
                         if ((fabs(nx_) >= fabs(ny_)) && (fabs(nx_) >= fabs(nz_))) nor_dir = 1;
                         else if ((fabs(ny_) >= fabs(nz_)) && (fabs(ny_) >= fabs(nx_))) nor_dir = 2;
                         else if ((fabs(nz_) >= fabs(ny_)) && (fabs(nz_) >= fabs(nx_))) nor_dir = 3;
@@ -1198,6 +1201,7 @@ int mmso_get_field(mmso *o, int field, void *out)
     case MMS_FIELD_NUC_THRESHOLD: memcpy(out, o->thr, N * sizeof(float)); break;
     case MMS_FIELD_TEMPERATURE: memcpy(out, o->T, N * sizeof(double)); break;
     case MMS_FIELD_MOLD: memcpy(out, o->mold, N); break;
+    case MMS_FIELD_CURV: memcpy(out, o->curv, N * sizeof(double)); break;
     default: return MMS_ERR_ARG;
     }
     return MMS_OK;

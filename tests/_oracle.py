@@ -56,9 +56,9 @@ def load():
 
 _DT = {0: (np.float64, 1), 1: (np.float64, 1), 2: (np.float64, 1), 3: (np.int32, 1),
        4: (np.float64, 3), 5: (np.float64, 1), 6: (np.float32, 1), 7: (np.float64, 1),
-       8: (np.int8, 1), 9: (np.int32, 1)}
+       8: (np.int8, 1), 9: (np.int32, 1), 10: (np.float64, 1)}
 FIELD = {"ce": 0, "cl": 1, "fs": 2, "gr": 3, "dc": 4, "d": 5, "nuc_threshold": 6,
-         "temperature": 7, "mold": 8, "ogr": 9}
+         "temperature": 7, "mold": 8, "ogr": 9, "curv": 10}
 
 
 class Oracle:

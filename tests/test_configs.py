@@ -119,3 +119,31 @@ def test_word_aligned_subblocks_bit_exact_vs_oracle(built, cuda_device, sb):
             assert dom.num_grains == o.num_grains
             assert mismatches(state_digests(dom), state_digests(o)) == [], s
         assert dom.num_grains > 10
+
+
+@pytest.mark.gpu
+def test_corrected_curvature_vs_oracle(built, cuda_device):
+    """mms_params.curvature_corrected = 1: the three quirks of sb_curvature
+    fixed (curvature.c:176, 194, 203) on both sides.  On the curvature golden
+    deck the device's curvature field equals the oracle's (to the last bits
+    glibc's pow(x, 1.5) and the device's correctly rounded x^1.5 allow); it
+    is non-zero on over a thousand interface cells at step 400, where the
+    reference's own formula gives none (it is 0 unless a normal component
+    is exactly 0)."""
+    import numpy as np
+    from _oracle import Oracle
+    from conftest import golden_deck
+    counts = {}
+    for fixed in (0, 1):
+        p = M.read_deck(golden_deck("curv1"))
+        p.curvature_corrected = fixed
+        o = Oracle(p, curvature=True)
+        with M.Domain(p, precision=M.PREC_F64) as dom:
+            for s in (200, 400):
+                o.step(s - o.timestep)
+                dom.step(s - dom.timestep)
+                c, c0 = dom.download("curv"), o.download("curv")
+                assert np.array_equal(c != 0, c0 != 0), (fixed, s)
+                assert np.allclose(c, c0, rtol=1e-9, atol=0), (fixed, s)
+            counts[fixed] = int((c0 != 0).sum())
+    assert counts[0] == 0 and counts[1] > 1000, counts
