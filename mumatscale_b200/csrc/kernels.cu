@@ -396,24 +396,25 @@ constexpr int ACT_NT = 1024;
 // Ordered gather of the per-block candidate lists into cand[0, C), then per
 // candidate its orientation source and the prefix count of random draws
 // (cand_ex), per rank its first candidate and its number of draws.
+template <int NT>
 __device__ __forceinline__ void act_gather(const KernelArgs &a, int C, int *need, int *first, int *sh)
 {
     const Phys &p = a.p;
     const int nr = a.g.nranks;
     int *ex = a.d.cand_ex;
-    for (int r = threadIdx.x; r < nr; r += ACT_NT) need[r] = 0, first[r] = -1;
+    for (int r = threadIdx.x; r < nr; r += NT) need[r] = 0, first[r] = -1;
     int off = 0;
-    for (int base = 0; base < a.d.nuc_blocks; base += ACT_NT) {
+    for (int base = 0; base < a.d.nuc_blocks; base += NT) {
         int b = base + threadIdx.x;
         int n = (b < a.d.nuc_blocks) ? a.d.nuc_blk_cnt[b] : 0;
         int tot;
-        int pos = off + block_exclusive_scan<ACT_NT>(n, tot, sh);
+        int pos = off + block_exclusive_scan<NT>(n, tot, sh);
         for (int i = 0; i < n; i++) a.d.cand[pos + i] = a.d.cand_stage[(long long)b * NUC_NT + i];
         off += tot;
     }
     __syncthreads();
     int run = 0;
-    for (int base = 0; base < C; base += ACT_NT) {
+    for (int base = 0; base < C; base += NT) {
         int i = base + threadIdx.x;
         int rnd = 0, r = 0;
         if (i < C) {
@@ -424,7 +425,7 @@ __device__ __forceinline__ void act_gather(const KernelArgs &a, int C, int *need
             if (rnd) atomicAdd(&need[r], 1);
         }
         int tot;
-        int e = run + block_exclusive_scan<ACT_NT>(rnd, tot, sh);
+        int e = run + block_exclusive_scan<NT>(rnd, tot, sh);
         if (i < C) ex[i] = e;
         run += tot;
     }
@@ -432,23 +433,25 @@ __device__ __forceinline__ void act_gather(const KernelArgs &a, int C, int *need
 }
 
 // Some rank lacks pre-drawn orientations for its draws of this step (block-wide).
+template <int NT>
 __device__ __forceinline__ bool act_short(const KernelArgs &a, const int *need)
 {
     int short_rng = 0;
-    for (int r = threadIdx.x; r < a.g.nranks; r += ACT_NT)
+    for (int r = threadIdx.x; r < a.g.nranks; r += NT)
         if (a.d.rng_used[r] + need[r] > a.d.rng_cap) short_rng = 1;
     return __syncthreads_or(short_rng) != 0;
 }
 
 // Grain id0 + i for candidate i: gr, rotation and record; with rows, the
 // record as the other slabs of a split domain receive it.
+template <int NT>
 __device__ __forceinline__ void act_assign(const KernelArgs &a, int C, long long id0, unsigned long long ts,
                                            const int *first, SlabRow *rows)
 {
     const Phys &p = a.p;
     const Geo &g = a.g;
     const int *ex = a.d.cand_ex;
-    for (int i = threadIdx.x; i < C; i += ACT_NT) {
+    for (int i = threadIdx.x; i < C; i += NT) {
         const int s = a.d.cand[i];
         if (!in_bounds(a.d.ctl, s, a.d.nsites)) continue;
         const long long cell = a.d.site_cell[s];
@@ -499,11 +502,12 @@ __device__ __forceinline__ void act_assign(const KernelArgs &a, int C, long long
     }
 }
 
+template <int NT>
 __device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
 {
     Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
-    __shared__ int sh[ACT_NT / 32];
+    __shared__ int sh[NT / 32];
     __shared__ int s_abort;
     const int C = ctl->ncand;
     const unsigned long long ts = ctl->timestep + 1;
@@ -520,7 +524,7 @@ __device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
     int *need = rank_scratch;        // random draws per rank
     int *first = rank_scratch + nr;  // first candidate of each rank
     if (threadIdx.x == 0) s_abort = 0;
-    act_gather(a, C, need, first, sh);
+    act_gather<NT>(a, C, need, first, sh);
     if (threadIdx.x == 0) {
         if ((unsigned long long)(ctl->num_grains + (long long)C) > p.max_grains + 1) {
             ctl->status = MMS_ERR_GRAIN_OVERFLOW;
@@ -530,7 +534,7 @@ __device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
     }
     __syncthreads();
     if (s_abort) return;
-    if (act_short(a, need)) {
+    if (act_short<NT>(a, need)) {
         // refill on the host, then this kernel runs again with the same
         // candidates (nothing has been written yet)
         if (threadIdx.x == 0) {
@@ -540,9 +544,9 @@ __device__ __forceinline__ void act_body(const KernelArgs &a, int *rank_scratch)
         return;
     }
     const long long num_grains = ctl->num_grains;
-    act_assign(a, C, num_grains, ts, first, nullptr);
+    act_assign<NT>(a, C, num_grains, ts, first, nullptr);
     __syncthreads();
-    for (int r = threadIdx.x; r < nr; r += ACT_NT)
+    for (int r = threadIdx.x; r < nr; r += NT)
         if (need[r]) atomicMax(&ctl->rng_used_max, a.d.rng_used[r] += need[r]);
     if (threadIdx.x == 0) {
         ctl->num_grains = (int)(num_grains + C);
@@ -569,8 +573,8 @@ __global__ void __launch_bounds__(ACT_NT) k_act_local(KernelArgs a)
     int short_rng = 0;
     if (C > 0) {
         int *need = a.d.act_scratch, *first = a.d.act_scratch + a.g.nranks;
-        act_gather(a, C, need, first, sh);
-        short_rng = act_short(a, need) ? 1 : 0;
+        act_gather<ACT_NT>(a, C, need, first, sh);
+        short_rng = act_short<ACT_NT>(a, need) ? 1 : 0;
     }
     if (threadIdx.x == 0) {
         a.d.x1_send[0] = C;
@@ -617,7 +621,7 @@ __global__ void __launch_bounds__(ACT_NT) k_act_slab(KernelArgs a)
     if (C > 0) {
         const int nr = a.g.nranks;
         const int *need = a.d.act_scratch, *first = a.d.act_scratch + nr;
-        act_assign(a, C, num_grains + off, ts, first, a.d.x2_send);
+        act_assign<ACT_NT>(a, C, num_grains + off, ts, first, a.d.x2_send);
         __syncthreads();
         for (int r = threadIdx.x; r < nr; r += ACT_NT)
             if (need[r]) atomicMax(&ctl->rng_used_max, a.d.rng_used[r] += need[r]);
@@ -661,7 +665,28 @@ __global__ void __launch_bounds__(256) k_slab_merge(KernelArgs a)
 
 __global__ void __launch_bounds__(ACT_NT) k_act(KernelArgs a, int *rank_scratch)
 {
-    act_body(a, rank_scratch);
+    act_body<ACT_NT>(a, rank_scratch);
+}
+
+// Nucleation and activation in one launch: every block tests its sites as
+// k_nuc does; the block that finishes last (a counter in the control block,
+// after a fence in every thread that wrote candidates) then runs
+// activateNewGrains over the candidates of all blocks, as k_act would.
+template <typename Real>
+__global__ void __launch_bounds__(NUC_NT) k_nuc_act(KernelArgs a)
+{
+    Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;  // nothing in this launch changes the stall state before the last block
+    nuc_body<Real>(a, blockIdx.x);
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&ctl->nuc_done, 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) ctl->nuc_done = 0;
+    act_body<NUC_NT>(a, a.d.act_scratch);
 }
 
 // ---------------------------------------------------------------- curvature
@@ -1772,7 +1797,7 @@ __global__ void __launch_bounds__(ACT_NT) k_act_batch(const void *items, size_t 
     __shared__ __align__(16) KernelArgs sa;
     int local;
     batch_enter<ACT_NT>(items, stride, begin, n, sa, local);
-    act_body(sa, sa.d.act_scratch);
+    act_body<ACT_NT>(sa, sa.d.act_scratch);
 }
 
 __global__ void __launch_bounds__(LIST_NT) k_list_batch(const void *items, size_t stride, const int *begin, int n)
@@ -2152,15 +2177,17 @@ static int launch_pre_t(const KernelArgs &a, cudaStream_t st, int start_stage, P
     int n = 0;
     const Geo &g = a.g;
     if (start_stage == 0 && a.d.nsites > 0) {
+        // nucleation, and activation in the block that finishes last
         PROF_BEGIN(KID_NUC);
-        k_nuc<Real><<<a.d.nuc_blocks, NUC_NT, 0, st>>>(a);
+        k_nuc_act<Real><<<a.d.nuc_blocks, NUC_NT, 0, st>>>(a);
         PROF_END(KID_NUC);
         n++;
+    } else {
+        PROF_BEGIN(KID_ACT);
+        k_act<<<1, ACT_NT, 0, st>>>(a, a.d.act_scratch);
+        PROF_END(KID_ACT);
+        n++;
     }
-    PROF_BEGIN(KID_ACT);
-    k_act<<<1, ACT_NT, 0, st>>>(a, a.d.act_scratch);
-    PROF_END(KID_ACT);
-    n++;
     if (a.p.tip_curv) {
         long long tot = (long long)g.nranks * g.sbcells;
         PROF_BEGIN(KID_CURV);

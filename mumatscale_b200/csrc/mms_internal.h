@@ -39,6 +39,8 @@ struct Ctl {
     // second, 2^22 polls)
     int hold_list_block;
     unsigned wait_polls;
+    int nuc_done;                 // k_nuc_act blocks finished this step (the last one activates)
+    int pad_;
 };
 
 enum StallReason : int {
