@@ -480,6 +480,31 @@ mms_status mms_slab_launch(mms_ctx *ctx, int phase, int resume);
 mms_status mms_slab_exchange_plan(mms_ctx *ctx, int point, uint64_t timestep, mms_slab_xfer *out, int max,
                                   int *n);
 mms_status mms_slab_poll(mms_ctx *ctx, uint64_t *timestep, int *stalled);
+/* One process per device over NCCL (the role of the reference's MPI
+ * exchanges inside doiteration, calculate.c:232-337, and of the grain
+ * Allgatherv, grain.c:892-904).  The library does not link NCCL: it loads
+ * the entry points from nccl_path (NULL: "libnccl.so.2", which finds a copy
+ * the process has already loaded, e.g. torch's).
+ *   mms_slab_nccl_unique_id  one rank makes the 128-byte ncclUniqueId, which
+ *                            the caller sends to every rank of the group
+ *   mms_slab_nccl_init       every slab context (slab index = NCCL rank)
+ *                            joins the communicator
+ *   mms_slab_nccl_step       nsteps steps: the three launch phases, with the
+ *                            two exchange points as NCCL groups (halo planes
+ *                            as send/recv with the neighbouring slabs, the
+ *                            candidate and new-grain lists as all-gathers),
+ *                            all on the context's stream; every 64 steps an
+ *                            all-reduce checks that every slab is at the same
+ *                            step and stall state, and a shortage of
+ *                            pre-drawn orientations is refilled and resumed
+ *                            on every slab.  Every rank calls it with the
+ *                            same nsteps.
+ *   mms_slab_nccl_reduce     the whole domain's reduction: this slab's sum,
+ *                            all-reduced over the group. */
+mms_status mms_slab_nccl_unique_id(const char *nccl_path, void *id128);
+mms_status mms_slab_nccl_init(mms_ctx *ctx, const char *nccl_path, const void *id128);
+mms_status mms_slab_nccl_step(mms_ctx *ctx, int nsteps);
+mms_status mms_slab_nccl_reduce(mms_ctx *ctx, mms_reduction what, double *out);
 mms_status mms_slab_refill(mms_ctx *ctx);
 
 /* ---- adjoint (frozen cellular automaton) -------------------------------------- */

@@ -170,6 +170,10 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_params_free_lists": (None, [C.POINTER(Params)]),
         "mms_params_size": (C.c_size_t, []),
         "mms_test_hold_list_block": (I, [P, I, C.c_uint]),
+        "mms_slab_nccl_unique_id": (I, [C.c_char_p, P]),
+        "mms_slab_nccl_init": (I, [P, C.c_char_p, P]),
+        "mms_slab_nccl_step": (I, [P, I]),
+        "mms_slab_nccl_reduce": (I, [P, I, C.POINTER(D)]),
         "mms_create": (I, [C.POINTER(Params), C.POINTER(P)]),
         "mms_destroy": (I, [P]),
         "mms_step": (I, [P, I]),

@@ -5,6 +5,8 @@
 // glibc rand() streams and must be replayed exactly), and drives the
 // per-step kernel sequence of kernels.cu on one CUDA stream.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <algorithm>
 #include <array>
@@ -16,6 +18,8 @@
 #include <cstring>
 #include <ctime>
 #include <map>
+#include <mutex>
+#include <type_traits>
 #include <string>
 #include <sys/time.h>
 #include <unordered_map>
@@ -143,6 +147,10 @@ struct mms_ctx {
     mms_params gp{};
     Geo gg{};
     std::vector<cudaEvent_t> slab_events;  // mms_slab_group_step's ordering events
+    // one process per device: the NCCL communicator of the slab group
+    // (mms_slab_nccl_init) and 64 bytes of device scratch for its checks
+    void *nccl_comm = nullptr;
+    void *nccl_scratch = nullptr;
     // XDMF output: rank 0's rand() stream where its first still-undrawn
     // orientation begins (r0_snap_k draws after setup and any renumbering),
     // the grain renumbering of the last write, the time series written
@@ -1236,6 +1244,68 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
 
 }  // namespace
 
+// ---- NCCL, loaded at run time -------------------------------------------
+// The library does not link NCCL: the slab group's exchanges use the entry
+// points of the libnccl the caller names (by default "libnccl.so.2", which
+// finds a copy already loaded in the process, such as torch's).
+struct NcclApi {
+    ncclResult_t (*GetUniqueId)(ncclUniqueId *);
+    ncclResult_t (*CommInitRank)(ncclComm_t *, int, ncclUniqueId, int);
+    ncclResult_t (*CommDestroy)(ncclComm_t);
+    ncclResult_t (*Send)(const void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
+    ncclResult_t (*Recv)(void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t);
+    ncclResult_t (*AllGather)(const void *, void *, size_t, ncclDataType_t, ncclComm_t, cudaStream_t);
+    ncclResult_t (*AllReduce)(const void *, void *, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                              cudaStream_t);
+    ncclResult_t (*GroupStart)();
+    ncclResult_t (*GroupEnd)();
+    const char *(*GetErrorString)(ncclResult_t);
+};
+
+static std::mutex g_nccl_mu;
+static NcclApi g_nccl;
+static bool g_nccl_ok = false;
+
+static const NcclApi *nccl_api(const char *path, std::string *err)
+{
+    std::lock_guard<std::mutex> lock(g_nccl_mu);
+    if (g_nccl_ok) return &g_nccl;
+    void *h = dlopen(path && *path ? path : "libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
+    if (!h) {
+        if (err) *err = std::string("dlopen NCCL: ") + dlerror();
+        return nullptr;
+    }
+    NcclApi a{};
+    bool ok = true;
+    auto sym = [&](auto &fn, const char *name) {
+        fn = reinterpret_cast<std::remove_reference_t<decltype(fn)>>(dlsym(h, name));
+        ok = ok && fn;
+    };
+    sym(a.GetUniqueId, "ncclGetUniqueId");
+    sym(a.CommInitRank, "ncclCommInitRank");
+    sym(a.CommDestroy, "ncclCommDestroy");
+    sym(a.Send, "ncclSend");
+    sym(a.Recv, "ncclRecv");
+    sym(a.AllGather, "ncclAllGather");
+    sym(a.AllReduce, "ncclAllReduce");
+    sym(a.GroupStart, "ncclGroupStart");
+    sym(a.GroupEnd, "ncclGroupEnd");
+    sym(a.GetErrorString, "ncclGetErrorString");
+    if (!ok) {
+        if (err) *err = "NCCL library lacks an entry point";
+        return nullptr;
+    }
+    g_nccl = a;
+    g_nccl_ok = true;
+    return &g_nccl;
+}
+
+static void nccl_release(mms_ctx *ctx)
+{
+    if (ctx->nccl_comm && g_nccl_ok) g_nccl.CommDestroy((ncclComm_t)ctx->nccl_comm);
+    ctx->nccl_comm = nullptr;
+}
+
 extern "C" {
 
 mms_status mms_destroy(mms_ctx *ctx)
@@ -1247,6 +1317,7 @@ mms_status mms_destroy(mms_ctx *ctx)
     ctx->allocs.clear();
     for (cudaEvent_t e : ctx->slab_events) cudaEventDestroy(e);
     ctx->slab_events.clear();
+    nccl_release(ctx);
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
     if (ctx->h_red) cudaFreeHost(ctx->h_red);
     drop_graph(ctx);
@@ -3064,6 +3135,192 @@ mms_status mms_slab_group_step(mms_ctx *const *slabs, int nslabs, int nsteps)
         for (int s = 0; s < nslabs; s++)
             if ((st = refill_rng(slabs[s], false))) return st;
     }
+    return MMS_OK;
+}
+
+// ---- one process per device over NCCL -----------------------------------
+
+mms_status mms_slab_nccl_unique_id(const char *nccl_path, void *id128)
+{
+    if (!id128) return MMS_ERR_ARG;
+    const NcclApi *n = nccl_api(nccl_path, nullptr);
+    if (!n) return MMS_ERR_ARG;
+    ncclUniqueId id;
+    if (n->GetUniqueId(&id) != ncclSuccess) return MMS_ERR_CUDA;
+    std::memcpy(id128, &id, sizeof id);
+    return MMS_OK;
+}
+
+mms_status mms_slab_nccl_init(mms_ctx *ctx, const char *nccl_path, const void *id128)
+{
+    if (!ctx || !id128) return MMS_ERR_ARG;
+    if (ctx->nccl_comm) return MMS_ERR_STATE;
+    std::string err;
+    const NcclApi *n = nccl_api(nccl_path, &err);
+    if (!n) {
+        ctx->err = err;
+        return MMS_ERR_ARG;
+    }
+    cudaSetDevice(ctx->device);
+    if (!ctx->nccl_scratch) {
+        long long *p = nullptr;
+        mms_status st = dalloc(ctx, &p, 8);
+        if (st) return st;
+        ctx->nccl_scratch = p;
+    }
+    ncclUniqueId id;
+    std::memcpy(&id, id128, sizeof id);
+    ncclComm_t comm = nullptr;
+    const ncclResult_t r = n->CommInitRank(&comm, ctx->nslabs, id, ctx->slab);
+    if (r != ncclSuccess) {
+        ctx->err = std::string("ncclCommInitRank: ") + n->GetErrorString(r);
+        return MMS_ERR_CUDA;
+    }
+    ctx->nccl_comm = comm;
+    return MMS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+mms_status nccl_fail(mms_ctx *ctx, const char *what, ncclResult_t r)
+{
+    ctx->err = std::string(what) + ": " + g_nccl.GetErrorString(r);
+    return MMS_ERR_CUDA;
+}
+
+// One exchange point of the plan (slab_plan), as one NCCL group on the
+// slab's stream: the halo planes as send/recv pairs with the neighbouring
+// slabs, the gather as an all-gather.
+mms_status nccl_exchange(mms_ctx *ctx, int point, unsigned long long ts)
+{
+    std::vector<mms_slab_xfer> v;
+    slab_plan(ctx, point, ts, v);
+    ncclComm_t comm = (ncclComm_t)ctx->nccl_comm;
+    ncclResult_t r = g_nccl.GroupStart();
+    for (const mms_slab_xfer &x : v) {
+        if (r != ncclSuccess) break;
+        if (x.kind == MMS_XFER_HALO) {
+            r = g_nccl.Send(x.send, (size_t)x.bytes, ncclUint8, x.peer, comm, ctx->stream);
+            if (r == ncclSuccess) r = g_nccl.Recv(x.recv, (size_t)x.bytes, ncclUint8, x.peer, comm, ctx->stream);
+        } else {
+            r = g_nccl.AllGather(x.send, x.recv, (size_t)x.bytes, ncclUint8, comm, ctx->stream);
+        }
+    }
+    const ncclResult_t r2 = g_nccl.GroupEnd();
+    if (r != ncclSuccess) return nccl_fail(ctx, "NCCL exchange", r);
+    if (r2 != ncclSuccess) return nccl_fail(ctx, "ncclGroupEnd", r2);
+    return MMS_OK;
+}
+
+mms_status nccl_one(mms_ctx *ctx, unsigned long long ts, int resume)
+{
+    mms_status st;
+    if ((st = slab_launch(ctx, 0, resume)) || (st = nccl_exchange(ctx, 0, ts)) || (st = slab_launch(ctx, 1, 0)) ||
+        (st = nccl_exchange(ctx, 1, ts)) || (st = slab_launch(ctx, 2, 0)))
+        return st;
+    return MMS_OK;
+}
+
+// This slab's {timestep, stalled for orientations, error status}, and
+// whether every slab of the group holds the same triple (an all-reduce of
+// the values and their negatives with MAX); v[2] becomes the group's
+// largest error status.
+mms_status nccl_agree(mms_ctx *ctx, long long v[3], bool *same)
+{
+    mms_status st = read_ctl(ctx);
+    if (st) return st;
+    const Ctl &c = *ctx->h_ctl;
+    v[0] = (long long)c.timestep;
+    v[1] = c.stall == STALL_RNG ? 1 : 0;
+    v[2] = c.stall == STALL_ERROR ? (c.status ? c.status : MMS_ERR_STATE) : 0;
+    long long h[6] = {v[0], v[1], v[2], -v[0], -v[1], -v[2]};
+    long long *d = (long long *)ctx->nccl_scratch;
+    CU(cudaMemcpyAsync(d, h, sizeof h, cudaMemcpyHostToDevice, ctx->stream));
+    const ncclResult_t r = g_nccl.AllReduce(d, d, 6, ncclInt64, ncclMax, (ncclComm_t)ctx->nccl_comm, ctx->stream);
+    if (r != ncclSuccess) return nccl_fail(ctx, "ncclAllReduce", r);
+    CU(cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    *same = h[0] == -h[3] && h[1] == -h[4] && h[2] == -h[5];
+    v[2] = h[2];
+    return MMS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mms_status mms_slab_nccl_step(mms_ctx *ctx, int nsteps)
+{
+    Range range("mms_slab_nccl_step");
+    if (!ctx || nsteps < 0) return MMS_ERR_ARG;
+    if (!ctx->nccl_comm) return MMS_ERR_STATE;
+    cudaSetDevice(ctx->device);
+    ctx->stepped = true;
+    long long v[3];
+    bool same = false;
+    mms_status st;
+    if ((st = nccl_agree(ctx, v, &same))) return st;
+    if (!same) {
+        ctx->err = "slabs are not at the same step";
+        return MMS_ERR_STATE;
+    }
+    if (v[2]) return (mms_status)v[2];
+    if (v[1]) {
+        ctx->err = "slab is stalled before stepping";
+        return MMS_ERR_STATE;
+    }
+    unsigned long long ts = (unsigned long long)v[0];
+    const unsigned long long target = ts + (unsigned long long)nsteps;
+    const int chunk = 64;
+    while (ts < target) {
+        const int n = (int)std::min<unsigned long long>(chunk, target - ts);
+        for (int k = 0; k < n; k++)
+            if ((st = nccl_one(ctx, ts + k, 0))) return st;
+        // every slab reaches the same state: the same step, and a stall
+        // (a shortage of pre-drawn orientations anywhere) at the same
+        // activation, after which the launched steps did nothing
+        if ((st = nccl_agree(ctx, v, &same))) return st;
+        if (!same) {
+            ctx->err = "slabs diverged (timestep or stall state differs between ranks)";
+            return MMS_ERR_STATE;
+        }
+        if (v[2]) return (mms_status)v[2];
+        if (v[1]) {
+            if ((st = mms_slab_refill(ctx)) || (st = nccl_one(ctx, (unsigned long long)v[0], 1))) return st;
+            ts = (unsigned long long)v[0] + 1;
+            continue;
+        }
+        ts = (unsigned long long)v[0];
+        if ((st = refill_rng(ctx, false))) return st;
+    }
+    return MMS_OK;
+}
+
+mms_status mms_slab_nccl_reduce(mms_ctx *ctx, mms_reduction what, double *out)
+{
+    if (!ctx || !out) return MMS_ERR_ARG;
+    if (!ctx->nccl_comm) return MMS_ERR_STATE;
+    const bool frac = what == MMS_REDUCE_FS_FRACTION;
+    double local = 0.0;
+    mms_status st = mms_reduce(ctx, frac ? MMS_REDUCE_SOLID_VOLUME : what, &local);
+    if (st) return st;
+    cudaSetDevice(ctx->device);
+    double *d = (double *)ctx->nccl_scratch;
+    CU(cudaMemcpyAsync(d, &local, sizeof local, cudaMemcpyHostToDevice, ctx->stream));
+    const ncclResult_t r = g_nccl.AllReduce(d, d, 1, ncclFloat64, ncclSum, (ncclComm_t)ctx->nccl_comm, ctx->stream);
+    if (r != ncclSuccess) return nccl_fail(ctx, "ncclAllReduce", r);
+    double sum = 0.0;
+    CU(cudaMemcpyAsync(&sum, d, sizeof sum, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    if (frac) {
+        const mms_params &g = ctx->gp;
+        const double cells = (double)((long long)g.gnsbx * g.gsdimx * (long long)g.gnsby * g.gsdimy *
+                                      (long long)g.gnsbz * g.gsdimz);
+        sum = sum / (cells * std::pow(g.cellSize, 3.0));
+    }
+    *out = sum;
     return MMS_OK;
 }
 

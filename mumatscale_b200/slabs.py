@@ -14,14 +14,21 @@ the library lists (``mms_slab_exchange_plan``):
 Reductions (fraction solid, solid volume, ce sum) are each slab's own sum
 followed by an all-reduce over the group.
 
-Transports: ``"nccl"`` runs the plane swaps as batched NCCL send/recv and
-the gathers as NCCL all-gathers, straight from device memory on the
-slab's stream; ``"host"`` stages every transfer through host memory, for
-process groups whose backend only moves host tensors (gloo).
+Transports: ``"nccl"`` hands the whole step loop to the library
+(``mms_slab_nccl_step``): the phase launches and, at each exchange point,
+one NCCL group (send/recv of the planes with the neighbouring slabs, an
+all-gather of the lists) on the slab's stream, through a communicator of
+the library's own whose id rank 0 sends to the others; Python makes one
+call per ``step``.  ``"host"`` stages every transfer through host memory
+and drives the step from Python, for process groups whose backend only
+moves host tensors (gloo).
 """
 from __future__ import annotations
 
-from . import PREC_F64, XFER_GATHER, XFER_HALO, Params, SlabDomain
+import ctypes as C
+import os
+
+from . import PREC_F64, XFER_GATHER, XFER_HALO, Params, SlabDomain, _check, _lib
 
 __all__ = ["DistributedSlab", "exchange"]
 
@@ -62,6 +69,21 @@ def exchange(entries, group=None) -> None:
             dist.all_gather(chunks, send, group=group)
 
 
+def nccl_library_path() -> str | None:
+    """The libnccl torch uses (its nvidia-nccl wheel), so that the library
+    binds to the same NCCL the process already has; None: let the dynamic
+    loader find libnccl.so.2."""
+    try:
+        import nvidia.nccl
+        for d in nvidia.nccl.__path__:
+            f = os.path.join(d, "lib", "libnccl.so.2")
+            if os.path.exists(f):
+                return f
+    except Exception:
+        pass
+    return None
+
+
 class DistributedSlab:
     """This process's slab of a domain split over the ranks of ``group``
     (slab index = rank)."""
@@ -85,16 +107,41 @@ class DistributedSlab:
             raise ValueError("transport must be 'nccl' or 'host'")
         self.transport = transport
         self.chunk = chunk
+        self._plans = {}
+        if transport == "nccl":
+            self._nccl_init()
+
+    def _nccl_init(self) -> None:
+        """Joins the library's NCCL communicator of the group: rank 0 makes
+        the unique id and the group's collective sends it to every rank."""
+        import torch.distributed as dist
+        path = nccl_library_path()
+        self._nccl_path = path.encode() if path else None
+        uid = C.create_string_buffer(128)
+        if self.rank == 0:
+            _check(_lib().mms_slab_nccl_unique_id(self._nccl_path, uid), "mms_slab_nccl_unique_id")
+        box = [uid.raw if self.rank == 0 else None]
+        dist.broadcast_object_list(box, src=dist.get_global_rank(self.group, 0) if self.group else 0,
+                                   group=self.group)
+        uid = C.create_string_buffer(box[0], 128)
+        _check(_lib().mms_slab_nccl_init(self.dom._ctx, self._nccl_path, uid), "mms_slab_nccl_init", self.dom._ctx)
 
     def _entries(self, point: int, ts: int):
+        """The transfers of an exchange point as tensors over the library's
+        buffers.  The plan depends on the step only through its parity
+        (which of the two cl / fs buffers is current), so it is built once
+        per (point, parity)."""
         import torch
-        out = []
-        for kind, peer, send, recv, nbytes in self.dom.exchange_plan(point, ts):
-            s = torch.as_tensor(_DeviceBytes(send, nbytes), device=self.device)
-            r_bytes = nbytes * (self.world if kind == XFER_GATHER else 1)
-            r = torch.as_tensor(_DeviceBytes(recv, r_bytes), device=self.device)
-            out.append((kind, peer, s, r))
-        return out
+        key = (point, ts & 1)
+        if key not in self._plans:
+            out = []
+            for kind, peer, send, recv, nbytes in self.dom.exchange_plan(point, ts):
+                s = torch.as_tensor(_DeviceBytes(send, nbytes), device=self.device)
+                r_bytes = nbytes * (self.world if kind == XFER_GATHER else 1)
+                r = torch.as_tensor(_DeviceBytes(recv, r_bytes), device=self.device)
+                out.append((kind, peer, s, r))
+            self._plans[key] = out
+        return self._plans[key]
 
     def _exchange(self, point: int, ts: int) -> None:
         import torch
@@ -128,6 +175,9 @@ class DistributedSlab:
             raise RuntimeError("slabs diverged (timestep or stall state differs between ranks)")
 
     def step(self, nsteps: int = 1) -> None:
+        if self.transport == "nccl":
+            _check(_lib().mms_slab_nccl_step(self.dom._ctx, int(nsteps)), "mms_slab_nccl_step", self.dom._ctx)
+            return
         ts, stalled = self.dom.poll()
         self._agree(ts, stalled)
         if stalled:
@@ -153,6 +203,12 @@ class DistributedSlab:
         summation order differs from one domain's).  Every rank calls it."""
         import torch
         import torch.distributed as dist
+        if self.transport == "nccl":
+            from . import REDUCE
+            v = C.c_double()
+            _check(_lib().mms_slab_nccl_reduce(self.dom._ctx, REDUCE[what], C.byref(v)), "mms_slab_nccl_reduce",
+                   self.dom._ctx)
+            return v.value
         local = self.dom.reduce("solid_volume" if what == "fs_fraction" else what)
         dev = self.device if dist.get_backend(self.group) == "nccl" else "cpu"
         t = torch.tensor([local], dtype=torch.float64, device=dev)

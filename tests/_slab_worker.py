@@ -1,7 +1,8 @@
 """One rank of a slab-split run (test infrastructure): launched by
 tests/test_slabs.py as a process per slab; steps its slab with
-mumatscale_b200.slabs.DistributedSlab over a gloo group (host transport)
-and saves its fields and grain records to <out>/slab<rank>.npz."""
+mumatscale_b200.slabs.DistributedSlab over a gloo group (host transport) or
+an NCCL group (the library's own NCCL step loop) and saves its fields and
+grain records to <out>/slab<rank>.npz."""
 from __future__ import annotations
 
 import argparse
@@ -21,13 +22,17 @@ def main() -> int:
     ap.add_argument("--steps", type=int, required=True)
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--out", required=True)
+    ap.add_argument("--backend", default="gloo", choices=["gloo", "nccl"])
     a = ap.parse_args()
     import numpy as np
     import torch.distributed as dist
 
     import mumatscale_b200 as M
     from mumatscale_b200.slabs import DistributedSlab
-    dist.init_process_group("gloo", init_method="env://",
+    if a.backend == "nccl":
+        import torch
+        torch.cuda.set_device(0)
+    dist.init_process_group(a.backend, init_method="env://",
                             timeout=__import__("datetime").timedelta(seconds=120))
     p = M.read_deck(a.deck)
     p.gnsbz, p.gsdimz = a.nsbz, a.sdimz

@@ -127,7 +127,7 @@ def _reduce_rank(rank: int, world: int, port: int, q) -> None:
         p.gnsbx, p.gnsby, p.gnsbz = 1, 1, 2
         p.gsdimx, p.gsdimy, p.gsdimz = 4, 4, 4
         p.cellSize = 2.0
-        s.group, s.params, s.device = None, p, "cpu"
+        s.group, s.params, s.device, s.transport = None, p, "cpu", "host"
         s.dom = _StubSlab({"solid_volume": 8.0 * (rank + 1), "ce_sum": 10.0 + rank})
         q.put((rank, s.reduce("fs_fraction"), s.reduce("solid_volume"), s.reduce("ce_sum")))
     finally:
@@ -268,3 +268,35 @@ def test_distributed_slabs_host_transport(built, cuda_device, tmp_path):
             # the group's all-reduced sums: every rank holds the domain's
             for got, w in zip(q["red"], want):
                 assert abs(got - w) <= 1e-12 * abs(w), (got, w)
+
+
+@pytest.mark.gpu
+def test_distributed_slab_nccl_one_rank(built, cuda_device, tmp_path):
+    """The library's NCCL step loop (mms_slab_nccl_*) as far as one GPU
+    allows: a one-rank NCCL group holding the whole domain as its one slab.
+    The communicator, the per-step all-gathers of candidates and new grains,
+    the agreement all-reduce every 64 steps and the all-reduced sums run;
+    the halo send/recv between neighbouring slabs needs two GPUs and does
+    not run here.  The state equals the single domain's bit for bit."""
+    steps = 150
+    deck = str(golden_deck("small4"))
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK="0", WORLD_SIZE="1",
+               NCCL_NVLS_ENABLE="0")
+    pr = subprocess.run([sys.executable, str(ROOT / "tests" / "_slab_worker.py"), "--deck", deck, "--nsbz", "1",
+                         "--sdimz", "16", "--steps", str(steps), "--out", str(tmp_path), "--backend", "nccl"],
+                        env=env, timeout=600)
+    assert pr.returncode == 0
+    p = _deck("small4", nsbz=1, sdimz=16)
+    q = np.load(tmp_path / "slab0.npz")
+    with M.Domain(p) as dom:
+        dom.step(steps)
+        for f in FIELDS:
+            assert np.array_equal(q[f], dom.download(f)), f
+        assert int(q["timestep"]) == steps
+        assert np.array_equal(_grain_table(dom.grains()), np.concatenate([q["rot"], q["ang"], q["nuc"]], axis=1))
+        want = [dom.reduce(w) for w in ("fs_fraction", "solid_volume", "ce_sum")]
+        for got, w in zip(q["red"], want):
+            assert abs(got - w) <= 1e-12 * abs(w), (got, w)
