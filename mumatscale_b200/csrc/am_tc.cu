@@ -94,12 +94,13 @@ __device__ __forceinline__ bool tc_bar_try(unsigned long long *bar, unsigned par
     return ok != 0;
 }
 
-// bounded (about a second)
+// bounded (2^22 polls, about a second); try_wait suspends the thread in
+// hardware between polls, so only a long wait backs off with short sleeps
 __device__ __forceinline__ bool tc_bar_wait(unsigned long long *bar, unsigned parity)
 {
     for (unsigned it = 0; it < (1u << 22); it++) {
         if (tc_bar_try(bar, parity)) return true;
-        if (it > 32) __nanosleep(256);
+        if (it > (1u << 14)) __nanosleep(64);
     }
     return false;
 }
@@ -344,7 +345,7 @@ __device__ __forceinline__ bool t2_wait(unsigned long long *bar, unsigned parity
     for (unsigned it = 0; it < (1u << 22); it++) {
         if (tc_bar_try(bar, parity)) return true;
         if (!strict && (it & 31) == 31 && *abort) return false;
-        if (it > 32) __nanosleep(256);
+        if (it > (1u << 14)) __nanosleep(64);
     }
     *abort = 1;
     return false;

@@ -108,12 +108,16 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
     return ok != 0;
 }
 
-// Bounded wait: gives up after about a second of polling.
+// Bounded wait: gives up after 2^22 polls (about a second).  try_wait
+// itself suspends the thread until the phase completes or a hardware time
+// limit passes, so the first 2^14 polls follow each other directly; only a
+// long wait backs off with short sleeps (a longer sleep delays the wake-up
+// of every warp waiting on a plane that has just landed).
 __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity)
 {
     for (unsigned it = 0; it < (1u << 22); it++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (it > 32) __nanosleep(256);
+        if (it > (1u << 14)) __nanosleep(64);
     }
     return false;
 }

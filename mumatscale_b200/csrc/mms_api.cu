@@ -3197,6 +3197,11 @@ mms_status nccl_exchange(mms_ctx *ctx, int point, unsigned long long ts)
 {
     std::vector<mms_slab_xfer> v;
     slab_plan(ctx, point, ts, v);
+    for (const mms_slab_xfer &x : v)
+        if (!x.send || !x.recv) {  // a slab context without its exchange buffers
+            ctx->err = "slab exchange buffers missing";
+            return MMS_ERR_STATE;
+        }
     ncclComm_t comm = (ncclComm_t)ctx->nccl_comm;
     ncclResult_t r = g_nccl.GroupStart();
     for (const mms_slab_xfer &x : v) {
@@ -3270,6 +3275,17 @@ mms_status mms_slab_nccl_step(mms_ctx *ctx, int nsteps)
     if (v[1]) {
         ctx->err = "slab is stalled before stepping";
         return MMS_ERR_STATE;
+    }
+    // a group of one slab has nothing to exchange: its context steps like a
+    // whole domain (as mms_slab_group_step does; its exchange buffers are
+    // not allocated), and the group only checks that it agrees
+    if (ctx->nslabs == 1) {
+        if ((st = mms_step(ctx, nsteps)) || (st = nccl_agree(ctx, v, &same))) return st;
+        if (!same) {
+            ctx->err = "slabs diverged (timestep or stall state differs between ranks)";
+            return MMS_ERR_STATE;
+        }
+        return v[2] ? (mms_status)v[2] : MMS_OK;
     }
     unsigned long long ts = (unsigned long long)v[0];
     const unsigned long long target = ts + (unsigned long long)nsteps;

@@ -272,12 +272,13 @@ def test_distributed_slabs_host_transport(built, cuda_device, tmp_path):
 
 @pytest.mark.gpu
 def test_distributed_slab_nccl_one_rank(built, cuda_device, tmp_path):
-    """The library's NCCL step loop (mms_slab_nccl_*) as far as one GPU
-    allows: a one-rank NCCL group holding the whole domain as its one slab.
-    The communicator, the per-step all-gathers of candidates and new grains,
-    the agreement all-reduce every 64 steps and the all-reduced sums run;
-    the halo send/recv between neighbouring slabs needs two GPUs and does
-    not run here.  The state equals the single domain's bit for bit."""
+    """The library's NCCL path (mms_slab_nccl_*) as far as one GPU allows:
+    a one-rank NCCL group holding the whole domain as its one slab.  The
+    run-time loading of NCCL, the communicator, the agreement all-reduce and
+    the all-reduced sums run; a one-slab group steps like a whole domain, so
+    the per-step exchanges (halo send/recv and the all-gathers) need two
+    GPUs and do not run here.  The state equals the single domain's bit for
+    bit."""
     steps = 150
     deck = str(golden_deck("small4"))
     with socket.socket() as s:
