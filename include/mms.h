@@ -389,9 +389,19 @@ mms_status mms_kernel_stats(mms_ctx *ctx, int id, double *total_ms, uint64_t *la
  * 0 = chosen from the grid size).  Results do not depend on the tile. */
 mms_status mms_set_stencil_tile(mms_ctx *ctx, int cells_per_thread, int zchunk);
 mms_status mms_get_stencil_tile(const mms_ctx *ctx, int *cells_per_thread, int *zchunk);
+/* FP32 form, moving-source (AM) temperature: rows per tile of its
+ * tensor-core contraction (tiles of 128 x cells by `rows` (y, z) rows): 64 to
+ * 128 in steps of 16, 256, or 0 = the multiple of 16 up to 128 that balances
+ * the tiles over the SMs (the default).  Results do not depend on it. */
+mms_status mms_set_am_tile(mms_ctx *ctx, int rows);
+mms_status mms_get_am_tile(const mms_ctx *ctx, int *rows);
 /* Times every tile candidate on shadow copies of the fields the stencil
  * writes (the domain's state is left as it was), keeps the fastest by median
- * of `reps` launches and returns it (any output pointer may be NULL). */
+ * of `reps` launches and returns it (any output pointer may be NULL).  For
+ * the FP32 form of the moving-source (AM) temperature model it also picks
+ * the tensor-core contraction's tile (128 x cells by 128 or 256 rows), timed
+ * on a shadow of the temperature field.  Results do not depend on either
+ * choice. */
 mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchunk, double *best_ms);
 
 /* ---- batched independent domains --------------------------------------------- */

@@ -201,6 +201,8 @@ def load_library(build_if_missing: bool = True) -> C.CDLL:
         "mms_kernel_stats": (I, [P, I, C.POINTER(D), C.POINTER(C.c_uint64)]),
         "mms_set_stencil_tile": (I, [P, I, I]),
         "mms_get_stencil_tile": (I, [P, C.POINTER(I), C.POINTER(I)]),
+        "mms_set_am_tile": (I, [P, I]),
+        "mms_get_am_tile": (I, [P, C.POINTER(I)]),
         "mms_autotune": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(D)]),
         "mms_adjoint_record": (I, [P, I, I]),
         "mms_adjoint_gradient": (I, [P, P, C.POINTER(AdjointResult)]),
@@ -384,6 +386,15 @@ class Domain:
         cpt, zc = C.c_int(), C.c_int()
         _check(_lib().mms_get_stencil_tile(self._ctx, C.byref(cpt), C.byref(zc)), "mms_get_stencil_tile", self._ctx)
         return cpt.value, zc.value
+
+    def set_am_tile(self, rows: int) -> None:
+        """FP32 AM contraction tile rows: 64-128 (multiple of 16), 256, or 0 = balanced."""
+        _check(_lib().mms_set_am_tile(self._ctx, rows), "mms_set_am_tile", self._ctx)
+
+    def am_tile(self) -> int:
+        r = C.c_int()
+        _check(_lib().mms_get_am_tile(self._ctx, C.byref(r)), "mms_get_am_tile", self._ctx)
+        return r.value
 
     def autotune(self, reps: int = 5) -> tuple[int, int, float]:
         """Picks the fastest stencil tile (state untouched); returns (cells_per_thread, zchunk, ms)."""

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(ADJ_NT) k_replay(Geo g, Phys p, const Real *__
         cl_new = (sizeof(Real) == 8) ? cen * q.k_inv : cen * q.k_inv + q.c0k;
         fs_new = lspfs;
     } else {
-        const double Td = temp_cell(p, nullptr, c, j, k, ts);
+        const double Td = temp_cell(p, nullptr, nullptr, c, j, k, ts);
         if (sizeof(Real) == 8) {
             const Real Tcell = (Real)Td;
             Real c_int = q.cinit + q.m_inv * (Tcell - q.Tliq);
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(ADJ_NT) k_adj_b(Geo g, Phys p, const unsigned 
             acc[AS_KINV] = (double)a_cl * ((double)ce1[c] + (double)off);  // cl' = ce' k_inv
         } else if (br == BR_GROW || br == BR_CLAMP) {
             const Real D_xt = (Real)p.D_xt, km = (Real)p.km, km_inv = (Real)p.km_inv, m_inv = (Real)p.m_inv;
-            const double Td = temp_cell(p, nullptr, c, j, k, ts);
+            const double Td = temp_cell(p, nullptr, nullptr, c, j, k, ts);
             const Real kap = p.tip_curv ? (Real)curv[c] : (Real)0;
             const Real c_int = (Real)p.cinit + m_inv * ((Real)(Td - p.Tliq) + (Real)p.gibbs * kap);
             const Real u = (Real)1 - km * lspfs;

@@ -1,26 +1,49 @@
 // am_tc.cu — the AM temperature contraction of the FP32 form on the
 // 5th-generation tensor cores.
 //
-//   T[row, x] = liniT + Tfront sum_i YZ[row, i] X[i, x],   YZ = Y_i(y) Z_i(z)
+//   T[x, row] = liniT + Tfront sum_i X_i(x) YZ_i(row),   YZ_i(row) = Y_i(y) Z_i(z)
 //
-// is a (rows x 400) by (400 x nx) matrix product.  A CTA computes a tile of
-// 128 rows by N x cells (N <= 256, a multiple of 32) with tcgen05.mma
-// kind::tf32, accumulating in tensor memory.  TF32 keeps 10 mantissa bits,
-// so every operand is split as v = hi + lo (hi = v rounded to TF32, lo the
-// exact FP32 remainder) and the product is hi*hi + hi*lo + lo*hi, three MMAs
-// per step of 8 nodes; the dropped lo*lo term and lo's own TF32 rounding are
-// ~2^-22 relative.
+// over the 400 quadrature nodes i of the moving-source model
+// (temperature.c:62-123) is a (x cells x 400) by (400 x rows) matrix product.
+// A CTA computes tiles of 128 x cells (MMA M, the A side) by N (y, z) rows
+// (MMA N, the B side) with tcgen05.mma kind::tf32, accumulating in tensor
+// memory.  TF32 keeps 10 mantissa bits, so every operand is split as
+// v = hi + lo (hi = v rounded to TF32, lo the exact FP32 remainder) and the
+// product is hi*hi + hi*lo + lo*hi, three MMAs per step of 8 nodes; the
+// dropped lo*lo term and lo's own TF32 rounding are ~2^-22 relative.
 //
-// Per chunk of 16 nodes the threads write the split operands into one of two
-// shared-memory buffers in the K-major, no-swizzle layout of the tensor core
-// (8 x 16-byte core matrices: rows 16 B apart, the two 16-byte halves of a
-// row's 8 nodes 128 B apart, 8-row groups 256 B apart), fence them to the
-// async proxy, and one thread issues the MMAs and commits them to the
-// buffer's mbarrier; a buffer is written again only after that barrier
-// (waited on with a bound) shows its MMAs complete, so the staging of one
-// chunk overlaps the MMAs of the previous one.
-// The epilogue reads the accumulators with tcgen05.ld (warp w sees TMEM lanes
-// 32 (w mod 4) ...) and writes T.
+// Accumulation.  The tensor core adds the 8 products of an MMA and the
+// accumulator with truncation, so each MMA into an accumulator loses up to
+// one unit in the last place of the running sum, always toward zero.  Two
+// measures keep that small: the hi*hi products go to one accumulator and the
+// ~2^-11 smaller cross products to another (so the large sum takes 50 MMAs,
+// not 150), and the nodes are summed from the oldest (widest, smallest
+// terms) to the most recent, so that a cell's largest terms are added last,
+// onto a sum that is still small.  The epilogue adds the two accumulators
+// and forms liniT + Tfront sum in FP64.
+//
+// Persistent, warp-specialised, one CTA per SM:
+//   warp 0       A: the x side, one bulk copy per stage from the operand image
+//                k_am_tables writes once per step (already split into TF32
+//                head and remainder and laid out as the tensor core reads it)
+//   warp 1       the MMAs (one thread), committed to mbarriers
+//   warps 2-5    B: the rows' YZ products, split and stored into shared memory
+//   warps 6-9    epilogue: tcgen05.ld of both accumulators, T (kept in FP32
+//                in this form) and the layer flag to global memory
+// Stages of 16 nodes (A 16 KB, B 16 or 32 KB) circulate in a shared-memory
+// ring.  With N = 128 the 512 tensor-memory columns hold two sets of
+// accumulators, so a tile's epilogue runs while the next tile accumulates;
+// with N = 256 one set fills them.
+//
+// The halo columns x = 0 and gx + 1 are not computed here: no kernel of a
+// step reads the temperature there.  k_am_halo fills them from the same
+// tables where they are read (the temperature download, and every step when
+// the multi-layer flag lsindex is kept).
+//
+// Every wait is bounded; on expiry a thread raises MMS_ERR_TIMEOUT and sets
+// a shared abort flag that ends every other role's waits, then each role
+// drains what it has in flight (bulk copies, committed MMAs) before the
+// tensor memory is freed.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -29,35 +52,32 @@
 
 namespace mms {
 
-constexpr int TC_M = 128;          // rows per tile (MMA M)
-constexpr int TC_NMAX = 256;       // x cells per tile at most (MMA N)
-constexpr int TC_KC = 16;          // nodes per shared-memory chunk
-constexpr int TC_KS = TC_KC / 8;   // MMA K-steps per chunk
-constexpr int TC_NT = 256;
-constexpr int TC_A_BYTES = TC_M * 8 * 4;       // one K-step of A (one part)
-constexpr int TC_B_BYTES = TC_NMAX * 8 * 4;    // one K-step of B (one part), room for N = 256
-constexpr int TC_SET = 2 * TC_KS * TC_A_BYTES + 2 * TC_KS * TC_B_BYTES;  // hi and lo of A and B
-constexpr int TC_SMEM = 2 * TC_SET;            // two chunks in flight
+constexpr int TC_M = 128;                // x cells per tile (MMA M)
+constexpr int TC_KC = 16;                // nodes per stage
+constexpr int TC_KS = TC_KC / 8;         // MMA K-steps per stage
+constexpr int TC_NCH = AM_NT / TC_KC;    // stages per tile
+constexpr int TC_A_KS = TC_M * 8 * 4;    // one K-step, one part (head or remainder) of A
+constexpr int TC_A = TC_KS * 2 * TC_A_KS;
+constexpr int TC_NT = 320;
+constexpr int TC_PROD0 = 64, TC_EPI0 = 192;  // first thread of the producers / epilogue
+static_assert(AM_NT % TC_KC == 0, "nodes per stage");
+
+template <int NB>
+struct TcCfg {
+    static constexpr int B_KS = NB * 8 * 4;                 // one K-step, one part of B
+    static constexpr int STAGE = TC_A + TC_KS * 2 * B_KS;   // 32 KB (N = 128) or 48 KB (N = 256)
+    static constexpr int S = NB == 128 ? 6 : 4;             // stages in the ring
+    static constexpr int SMEM = S * STAGE + 128;            // + alignment of the ring
+    static constexpr int BUFS = NB == 128 ? 2 : 1;          // accumulator sets (2 NB columns each)
+    static constexpr int RPT = NB / 128;                    // B rows per producer thread
+};
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-// v rounded to TF32 (10 mantissa bits, ties away from zero) and the remainder
-__device__ __forceinline__ void tf32_split(float v, float &hi, float &lo)
-{
-    const unsigned u = (__float_as_uint(v) + 0x1000u) & 0xffffe000u;
-    hi = __uint_as_float(u);
-    lo = v - hi;
-}
-
-// byte offset of element (r, k) (k < 8) in a K-major no-swizzle operand block
-__device__ __forceinline__ int kmajor_off(int r, int k)
-{
-    return (r >> 3) * 256 + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4;
-}
-
-// shared-memory matrix descriptor: start >> 4, leading-dimension byte offset
-// 128 (the second 16-byte half of the K-step), stride byte offset 256 (the
-// next 8-row group), descriptor version 1, no swizzle
+// shared-memory matrix descriptor of a K-major, no-swizzle operand block (8 x
+// 16-byte core matrices: rows 16 B apart, the two 16-byte halves of a row's 8
+// nodes 128 B apart, 8-row groups 256 B apart): start >> 4, leading-dimension
+// byte offset 128, stride byte offset 256, descriptor version 1
 __device__ __forceinline__ unsigned long long kmajor_desc(unsigned saddr)
 {
     return (unsigned long long)((saddr >> 4) & 0x3fffu) | ((unsigned long long)(128 >> 4) << 16) |
@@ -94,241 +114,18 @@ __device__ __forceinline__ bool tc_bar_try(unsigned long long *bar, unsigned par
     return ok != 0;
 }
 
-// bounded (2^22 polls, about a second); try_wait suspends the thread in
-// hardware between polls, so only a long wait backs off with short sleeps
-__device__ __forceinline__ bool tc_bar_wait(unsigned long long *bar, unsigned parity)
-{
-    for (unsigned it = 0; it < (1u << 22); it++) {
-        if (tc_bar_try(bar, parity)) return true;
-        if (it > (1u << 14)) __nanosleep(64);
-    }
-    return false;
-}
-
-__global__ void __launch_bounds__(TC_NT, 2) k_am_contract_tc(KernelArgs a, AmParams m, int N)
-{
-    const Ctl *ctl = a.d.ctl;
-    if (stalled(ctl)) return;
-    extern __shared__ __align__(1024) unsigned char tsm[];
-    __shared__ __align__(8) unsigned long long bar[2];
-    __shared__ unsigned tmem_base;
-    __shared__ int s_abort;
-    const Geo &g = a.g;
-    const Phys &p = a.p;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nx = g.gx + 2, ny = g.gy + 2, nz = g.gz + 2;
-    const float *__restrict__ X = (const float *)a.d.am_tab;
-    const float *__restrict__ Y = X + (long long)AM_NT * nx;
-    const float *__restrict__ Z = Y + (long long)AM_NT * ny;
-    const int *zon = (const int *)(Z + (long long)AM_NT * nz);
-    const int x0 = blockIdx.x * N;
-    const long long r0 = (long long)blockIdx.y * TC_M;
-    const long long nrows = (long long)ny * nz;
-
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base)),
-                     "r"(256u)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar[1])) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        s_abort = 0;
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const unsigned dtmem = tmem_base;
-    // kind::tf32, F32 accumulate, A and B K-major, M = 128, N
-    const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(TC_M >> 4) << 24);
-
-    // staging: A (YZ products) by row srow, nodes sk0, sk0 + 2, ...; B (X) by
-    // column tid for tid < N, every node of the chunk
-    const int srow = tid & (TC_M - 1), sk0 = tid >> 7;
-    const long long row = r0 + srow;
-    const bool rin = row < nrows;
-    const int Kr = rin ? (int)(row / ny) : 0, Jr = rin ? (int)(row - (long long)Kr * ny) : 0;
-    const float *Yr = Y + Jr, *Zr = Z + Kr;
-    const bool bcol = tid < N && x0 + tid < nx;
-    const float *Xc = X + (x0 + (tid < N ? tid : 0));
-
-    unsigned ph[2] = {0u, 0u};
-    int step = 0, c = 0;
-    // operands of the next chunk, loaded one chunk ahead so that their
-    // latency overlaps the stores, fences and MMA issue of the current one
-    float av[TC_KC / 2], bv[TC_KC];
-    auto load_chunk = [&](int i0) {
-#pragma unroll
-        for (int j = 0; j < TC_KC / 2; j++) {
-            const int k = sk0 + 2 * j;
-            av[j] = rin ? __ldg(Yr + (long long)(i0 + k) * ny) * __ldg(Zr + (long long)(i0 + k) * nz) : 0.f;
-        }
-#pragma unroll
-        for (int k = 0; k < TC_KC; k++) bv[k] = bcol ? __ldg(Xc + (long long)(i0 + k) * nx) : 0.f;
-    };
-    load_chunk(0);
-    for (int i0 = 0; i0 < AM_NT; i0 += TC_KC, c++) {
-        const int b = c & 1;
-        unsigned char *set = tsm + b * TC_SET;
-        unsigned char *A_hi = set, *A_lo = set + TC_KS * TC_A_BYTES;
-        unsigned char *B_hi = set + 2 * TC_KS * TC_A_BYTES, *B_lo = B_hi + TC_KS * TC_B_BYTES;
-        // this buffer's previous MMAs (chunk c - 2) must be complete
-        if (c >= 2) {
-            if (!tc_bar_wait(&bar[b], ph[b])) s_abort = 1;
-            ph[b] ^= 1u;
-        }
-        __syncthreads();
-        if (s_abort) break;
-#pragma unroll
-        for (int j = 0; j < TC_KC / 2; j++) {
-            const int k = sk0 + 2 * j;
-            float hi, lo;
-            tf32_split(av[j], hi, lo);
-            const int off = (k >> 3) * TC_A_BYTES + kmajor_off(srow, k & 7);
-            *(float *)(A_hi + off) = hi;
-            *(float *)(A_lo + off) = lo;
-        }
-        if (tid < N) {
-#pragma unroll
-            for (int k = 0; k < TC_KC; k++) {
-                float hi, lo;
-                tf32_split(bv[k], hi, lo);
-                const int off = (k >> 3) * TC_B_BYTES + kmajor_off(tid, k & 7);
-                *(float *)(B_hi + off) = hi;
-                *(float *)(B_lo + off) = lo;
-            }
-        }
-        if (i0 + TC_KC < AM_NT) load_chunk(i0 + TC_KC);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            for (int s2 = 0; s2 < TC_KS; s2++) {
-                const unsigned long long ah = kmajor_desc(smem_addr(A_hi + s2 * TC_A_BYTES));
-                const unsigned long long al = kmajor_desc(smem_addr(A_lo + s2 * TC_A_BYTES));
-                const unsigned long long bh = kmajor_desc(smem_addr(B_hi + s2 * TC_B_BYTES));
-                const unsigned long long bl = kmajor_desc(smem_addr(B_lo + s2 * TC_B_BYTES));
-                tc_mma(dtmem, ah, bh, idesc, step > 0 ? 1u : 0u);
-                tc_mma(dtmem, ah, bl, idesc, 1u);
-                tc_mma(dtmem, al, bh, idesc, 1u);
-                step++;
-            }
-            tc_commit(&bar[b]);
-        }
-    }
-    // the last chunk of each buffer (bounded waits; after an abort these
-    // drain whatever is still in flight before the tensor memory is freed)
-    for (int b = 0; b < 2 && b < c; b++) {
-        const int last = (c - 1 - b);       // chunks c-1 and c-2
-        const int bb = last & 1;
-        if (!tc_bar_wait(&bar[bb], ph[bb])) s_abort = 1;
-        ph[bb] ^= 1u;
-    }
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (s_abort) {
-        if (tid == 0) raise_error(a.d.ctl, MMS_ERR_TIMEOUT);
-    } else {
-        // epilogue: warp w reads TMEM lanes 32 (w mod 4) .. + 31 (its rows),
-        // columns of its half of the tile, 16 at a time
-        const AmStep st = am_step(p, m, ctl->timestep + 1);
-        const int q = warp & 3, half = warp >> 2;
-        const int rowl = 32 * q + lane;
-        const long long rrow = r0 + rowl;
-        const bool ok = rrow < nrows;
-        const int K = ok ? (int)(rrow / ny) : 0, J = ok ? (int)(rrow - (long long)K * ny) : 0;
-        const bool on = ok && zon[K] != 0;
-        const int c0 = half * (N / 2), c1 = (half + 1) * (N / 2);
-        for (int cc = c0; cc < c1; cc += 16) {
-            unsigned v[16];
-            const unsigned taddr = dtmem + ((unsigned)(32 * q) << 16) + (unsigned)cc;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                "%13, %14, %15}, [%16];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (ok) {
-#pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const int x = x0 + cc + j;
-                    if (cc + j >= c1 || x >= nx) break;
-                    const long long cell = (long long)K * g.sz + (long long)J * g.sy + x;
-                    const double T = on ? st.liniT + st.Tfront * (double)__uint_as_float(v[j]) : 0.0;
-                    a.d.T[cell] = T;
-                    if (a.d.lsindex && T > p.Tliq) a.d.lsindex[cell] = 1;
-                }
-            }
-        }
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (warp == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(dtmem), "r"(256u) : "memory");
-    }
-}
-
-// ----------------------------------------------------------------------------
-// Persistent, warp-specialised form.  The product is computed transposed,
-//
-//   T^T[x, row] = sum_i X[i, x] YZ[row, i],
-//
-// so the operand shared by every CTA (X, one 400 x gx table per step) is the
-// MMA's A side (M = 128 x cells) and is written once per step, already split
-// into TF32 head and remainder and laid out as the tensor core reads it, by
-// k_am_tables (am_ximg); a CTA brings a chunk of it in with one
-// cp.async.bulk.  The B side, N (<= 256) (y, z) rows of YZ products, is
-// formed by four producer warps straight into shared memory.  A tile is 128
-// x cells by N rows; its accumulator takes N of the 512 tensor-memory
-// columns, so the epilogue of one tile (four more warps: tcgen05.ld, then T
-// and the layer flag) runs while the next tile accumulates in the other
-// half.  Warp 0 loads A, warp 1 issues the MMAs (one thread), warps 2-5
-// produce B, warps 6-9 drain the accumulators.  Per stage (16 nodes): A 16
-// KB, B 32 KB; four stages in flight.  The halo columns x = 0 and gx + 1
-// (outside the 128-cell x tiles) are summed on the CUDA cores by the
-// epilogue warps while their first accumulator fills.
-//
-// Every wait is bounded; on expiry a thread raises MMS_ERR_TIMEOUT and sets a
-// shared abort flag that ends every other role's waits, then each role
-// drains what it has in flight (bulk copies, committed MMAs) before the
-// tensor memory is freed.
-constexpr int T2_M = 128;                       // x cells per tile (MMA M)
-constexpr int T2_NMAX = 256;                    // (y, z) rows per tile (MMA N) at most
-constexpr int T2_KC = 16;                       // nodes per stage
-constexpr int T2_KS = T2_KC / 8;                // MMA K-steps per stage
-constexpr int T2_S = 4;                         // stages
-constexpr int T2_NCH = AM_NT / T2_KC;           // stages per tile
-constexpr int T2_A_KS = T2_M * 8 * 4;           // one K-step, one part (head or remainder) of A
-constexpr int T2_B_KS = T2_NMAX * 8 * 4;        // the same of B (room for N = 256)
-constexpr int T2_A = T2_KS * 2 * T2_A_KS;       // A bytes per stage
-constexpr int T2_STAGE = T2_A + T2_KS * 2 * T2_B_KS;
-constexpr int T2_SMEM = T2_S * T2_STAGE + 128;  // + alignment of the ring
-constexpr int T2_NT = 320;
-constexpr int T2_PROD0 = 64, T2_EPI0 = 192;     // first thread of the producers / epilogue
-static_assert(AM_NT % T2_KC == 0, "nodes per stage");
-
-// the A image of one step: [x tile][K-step (50)][head, remainder][128 x 8]
-__host__ __device__ constexpr long long am_ximg_floats(int gx)
-{
-    return (long long)((gx + T2_M - 1) / T2_M) * (AM_NT / 8) * 2 * (T2_M * 8);
-}
-
-__device__ __forceinline__ void t2_arrive(unsigned long long *bar)
+__device__ __forceinline__ void tc_arrive(unsigned long long *bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-__device__ __forceinline__ void t2_arrive_tx(unsigned long long *bar, unsigned bytes)
+__device__ __forceinline__ void tc_arrive_tx(unsigned long long *bar, unsigned bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
 }
 
-__device__ __forceinline__ void t2_bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+__device__ __forceinline__ void tc_bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
 {
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -337,9 +134,11 @@ __device__ __forceinline__ void t2_bulk_load(void *dst, const void *src, unsigne
         : "memory");
 }
 
-// Bounded wait (about a second) that also gives up as soon as another role
-// has raised the abort flag; `strict` waits ignore the flag (draining).
-__device__ __forceinline__ bool t2_wait(unsigned long long *bar, unsigned parity, volatile int *abort,
+// Bounded wait (2^22 polls, about a second) that also gives up as soon as
+// another role has raised the abort flag; `strict` waits ignore the flag
+// (draining).  try_wait suspends the thread in hardware between polls, so
+// only a long wait backs off with short sleeps.
+__device__ __forceinline__ bool tc_wait(unsigned long long *bar, unsigned parity, volatile int *abort,
                                         bool strict = false)
 {
     for (unsigned it = 0; it < (1u << 22); it++) {
@@ -351,28 +150,39 @@ __device__ __forceinline__ bool t2_wait(unsigned long long *bar, unsigned parity
     return false;
 }
 
-struct T2Tile {
-    int xt;          // x tile: cells 1 + 128 xt ...
-    long long r0;    // first (y, z) row
-};
-
-__device__ __forceinline__ T2Tile t2_tile(long long t, int ntx, int N)
+// v rounded to TF32 (10 mantissa bits, ties away from zero) and the remainder
+__device__ __forceinline__ void tf32_split(float v, float &hi, float &lo)
 {
-    T2Tile w;
-    w.xt = (int)(t % ntx);
-    w.r0 = (t / ntx) * (long long)N;
-    return w;
+    const unsigned u = (__float_as_uint(v) + 0x1000u) & 0xffffe000u;
+    hi = __uint_as_float(u);
+    lo = v - hi;
 }
 
-__global__ void __launch_bounds__(T2_NT, 1)
-    k_am_contract_tc2(const __grid_constant__ KernelArgs a, const __grid_constant__ AmParams m, int N, int ntx,
-                      long long ntiles)
+static_assert(TC_M == 128, "am_ximg_part lays the X image out in 128-cell tiles");
+
+// 32 consecutive tensor-memory columns of this warp's 32 lanes
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&v)[16])
 {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+
+template <int NB>
+__global__ void __launch_bounds__(TC_NT, 1)
+    k_am_contract_tc(const __grid_constant__ KernelArgs a, const __grid_constant__ AmParams m, int N, int ntx,
+                     long long ntiles)
+{
+    using C = TcCfg<NB>;
+    constexpr int S = C::S;
     Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
-    extern __shared__ unsigned char t2_raw[];
-    unsigned char *ring = (unsigned char *)(((unsigned long long)t2_raw + 127) & ~127ULL);
-    __shared__ __align__(8) unsigned long long fullA[T2_S], fullB[T2_S], empty[T2_S], accf[2], acce[2];
+    extern __shared__ unsigned char tc_raw[];
+    unsigned char *ring = (unsigned char *)(((unsigned long long)tc_raw + 127) & ~127ULL);
+    __shared__ __align__(8) unsigned long long fullA[S], fullB[S], empty[S], accf[2], acce[2];
     __shared__ unsigned tmem_base;
     __shared__ int s_abort;
     const Geo &g = a.g;
@@ -394,10 +204,10 @@ __global__ void __launch_bounds__(T2_NT, 1)
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int s2 = 0; s2 < T2_S; s2++) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&fullA[s2])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_addr(&fullB[s2])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&empty[s2])) : "memory");
+        for (int s = 0; s < S; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&fullA[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_addr(&fullB[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&empty[s])) : "memory");
         }
         for (int b = 0; b < 2; b++) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&accf[b])) : "memory");
@@ -412,118 +222,145 @@ __global__ void __launch_bounds__(T2_NT, 1)
     const unsigned tmem = tmem_base;
 
     if (warp == 0) {
-        // ---- A: one bulk copy of 16 KB per stage
+        // ---- A: one bulk copy of 16 KB per stage; stage c holds the nodes of
+        // chunk TC_NCH - 1 - c (oldest first)
         if (lane == 0) {
             long long q = 0;
             bool ok = true;
             for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                const T2Tile w = t2_tile(t, ntx, N);
-                const float *src = ximg + (long long)w.xt * (AM_NT / 8) * 2 * (T2_M * 8);
-                for (int c = 0; c < T2_NCH; c++, q++) {
-                    const int s2 = (int)(q % T2_S);
-                    if (q >= T2_S && !t2_wait(&empty[s2], (unsigned)((q / T2_S - 1) & 1), abort)) {
+                const int xt = (int)(t % ntx);
+                const float *src = ximg + (long long)xt * (AM_NT / 8) * 2 * (TC_M * 8);
+                for (int c = 0; c < TC_NCH; c++, q++) {
+                    const int s = (int)(q % S);
+                    if (q >= S && !tc_wait(&empty[s], (unsigned)((q / S - 1) & 1), abort)) {
                         ok = false;
                         break;
                     }
-                    t2_arrive_tx(&fullA[s2], (unsigned)T2_A);
-                    t2_bulk_load(ring + s2 * T2_STAGE, src + (long long)c * T2_KS * 2 * (T2_M * 8), (unsigned)T2_A,
-                                 &fullA[s2]);
+                    tc_arrive_tx(&fullA[s], (unsigned)TC_A);
+                    tc_bulk_load(ring + s * C::STAGE, src + (long long)(TC_NCH - 1 - c) * TC_KS * 2 * (TC_M * 8),
+                                 (unsigned)TC_A, &fullA[s]);
                 }
             }
             // copies still in flight land before the CTA may exit
-            for (long long j = (q > T2_S ? q - T2_S : 0); j < q; j++)
-                t2_wait(&fullA[j % T2_S], (unsigned)((j / T2_S) & 1), abort, true);
+            for (long long j = (q > S ? q - S : 0); j < q; j++)
+                tc_wait(&fullA[j % S], (unsigned)((j / S) & 1), abort, true);
         }
     } else if (warp == 1) {
         // ---- MMA issue (one thread)
         if (lane == 0) {
             // kind::tf32, F32 accumulate, A and B K-major, M = 128, N
             const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(N >> 3) << 17) |
-                                   ((unsigned)(T2_M >> 4) << 24);
+                                   ((unsigned)(TC_M >> 4) << 24);
             long long q = 0, tl = 0;
             unsigned long long *last = nullptr;
             unsigned last_par = 0;
             bool ok = true;
             for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x, tl++) {
-                const int b = (int)(tl & 1);
-                if (tl >= 2 && !t2_wait(&acce[b], (unsigned)((tl / 2 - 1) & 1), abort)) break;
+                const int b = C::BUFS == 2 ? (int)(tl & 1) : 0;
+                const long long use = C::BUFS == 2 ? tl / 2 : tl;  // earlier tiles in this set
+                if (use >= 1 && !tc_wait(&acce[b], (unsigned)((use - 1) & 1), abort)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const unsigned d = tmem + (unsigned)(b * T2_NMAX);
-                for (int c = 0; c < T2_NCH; c++, q++) {
-                    const int s2 = (int)(q % T2_S);
-                    const unsigned par = (unsigned)((q / T2_S) & 1);
-                    if (!t2_wait(&fullA[s2], par, abort) || !t2_wait(&fullB[s2], par, abort)) {
+                const unsigned dhh = tmem + (unsigned)(b * 2 * NB), dxx = dhh + (unsigned)NB;
+                for (int c = 0; c < TC_NCH; c++, q++) {
+                    const int s = (int)(q % S);
+                    const unsigned par = (unsigned)((q / S) & 1);
+                    if (!tc_wait(&fullA[s], par, abort) || !tc_wait(&fullB[s], par, abort)) {
                         ok = false;
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    unsigned char *A = ring + s2 * T2_STAGE, *B = A + T2_A;
+                    unsigned char *A = ring + s * C::STAGE, *B = A + TC_A;
 #pragma unroll
-                    for (int k = 0; k < T2_KS; k++) {
-                        const unsigned long long ah = kmajor_desc(smem_addr(A + (2 * k) * T2_A_KS));
-                        const unsigned long long al = kmajor_desc(smem_addr(A + (2 * k + 1) * T2_A_KS));
-                        const unsigned long long bh = kmajor_desc(smem_addr(B + (2 * k) * T2_B_KS));
-                        const unsigned long long bl = kmajor_desc(smem_addr(B + (2 * k + 1) * T2_B_KS));
-                        tc_mma(d, ah, bh, idesc, (c > 0 || k > 0) ? 1u : 0u);
-                        tc_mma(d, ah, bl, idesc, 1u);
-                        tc_mma(d, al, bh, idesc, 1u);
+                    for (int kk = 0; kk < TC_KS; kk++) {
+                        const int k = TC_KS - 1 - kk;  // the later (older) K-step of the stage first
+                        const unsigned long long ah = kmajor_desc(smem_addr(A + (2 * k) * TC_A_KS));
+                        const unsigned long long al = kmajor_desc(smem_addr(A + (2 * k + 1) * TC_A_KS));
+                        const unsigned long long bh = kmajor_desc(smem_addr(B + (2 * k) * C::B_KS));
+                        const unsigned long long bl = kmajor_desc(smem_addr(B + (2 * k + 1) * C::B_KS));
+                        const unsigned acc = (c > 0 || kk > 0) ? 1u : 0u;
+                        tc_mma(dhh, ah, bh, idesc, acc);
+                        tc_mma(dxx, ah, bl, idesc, acc);
+                        tc_mma(dxx, al, bh, idesc, 1u);
                     }
-                    tc_commit(&empty[s2]);
-                    last = &empty[s2];
+                    tc_commit(&empty[s]);
+                    last = &empty[s];
                     last_par = par;
                 }
                 if (!ok) break;
                 tc_commit(&accf[b]);
                 last = &accf[b];
-                last_par = (unsigned)((tl / 2) & 1);
+                last_par = (unsigned)(use & 1);
             }
             // every committed MMA completes before the tensor memory is freed
-            if (last) t2_wait(last, last_par, abort, true);
+            if (last) tc_wait(last, last_par, abort, true);
         }
-    } else if (tid < T2_EPI0) {
-        // ---- B: (y, z) rows pr and pr + 128 of the tile, 16 nodes per stage
-        const int pr = tid - T2_PROD0;
+    } else if (tid < TC_EPI0) {
+        // ---- B: rows pr (+ 128) of the tile, the 16 nodes of each stage.
+        // The tables are read from the node-contiguous copies YT[J][i] and
+        // ZT[K][i]: a row's 16 nodes are four 16-byte loads, and CTAs working
+        // on different rows read different lines (node-major tables made
+        // every SM read the same few lines at the same moment).  The next
+        // stage's loads are in flight while this stage is split and stored.
+        const int pr = tid - TC_PROD0;
+        const float *__restrict__ YT = am_yt(a.d.am_ximg, g.gx);
+        const float *__restrict__ ZT = am_zt(a.d.am_ximg, g.gx, g.gy);
         long long q = 0;
         bool ok = true;
+        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 ny4[C::RPT][TC_KC / 4], nz4[C::RPT][TC_KC / 4];  // the next stage's table values
+        const float4 *yrow[C::RPT], *zrow[C::RPT];
+        bool on[C::RPT];
+        auto fetch = [&](int c) {
+            const int i0 = (TC_NCH - 1 - c) * TC_KC;
+#pragma unroll
+            for (int h = 0; h < C::RPT; h++)
+#pragma unroll
+                for (int k = 0; k < TC_KC / 4; k++) {
+                    ny4[h][k] = on[h] ? __ldg(yrow[h] + i0 / 4 + k) : zero4;
+                    nz4[h][k] = on[h] ? __ldg(zrow[h] + i0 / 4 + k) : zero4;
+                }
+        };
         for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-            const T2Tile w = t2_tile(t, ntx, N);
-            int J[2], K[2];
-            bool on[2];
+            const long long r0 = (t / ntx) * (long long)N;
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
+            for (int h = 0; h < C::RPT; h++) {
                 const int n = pr + 128 * h;
-                const long long R = w.r0 + n;
+                const long long R = r0 + n;
                 on[h] = n < N && R < nrows;
-                K[h] = on[h] ? (int)(R / ny) : 0;
-                J[h] = on[h] ? (int)(R - (long long)K[h] * ny) : 0;
+                const int K = on[h] ? (int)(R / ny) : 0, J = on[h] ? (int)(R - (long long)K * ny) : 0;
+                yrow[h] = (const float4 *)(YT + (long long)J * AM_NT);
+                zrow[h] = (const float4 *)(ZT + (long long)K * AM_NT);
             }
-            for (int c = 0; c < T2_NCH; c++, q++) {
-                const int s2 = (int)(q % T2_S);
-                float v[2][T2_KC];
+            fetch(0);
+            for (int c = 0; c < TC_NCH; c++, q++) {
+                const int s = (int)(q % S);
+                float v[C::RPT][TC_KC];
 #pragma unroll
-                for (int h = 0; h < 2; h++)
+                for (int h = 0; h < C::RPT; h++)
 #pragma unroll
-                    for (int k = 0; k < T2_KC; k++) {
-                        const int i = c * T2_KC + k;
-                        v[h][k] = on[h] ? __ldg(Y + (long long)i * ny + J[h]) * __ldg(Z + (long long)i * nz + K[h])
-                                        : 0.f;
+                    for (int k = 0; k < TC_KC / 4; k++) {
+                        v[h][4 * k] = ny4[h][k].x * nz4[h][k].x;
+                        v[h][4 * k + 1] = ny4[h][k].y * nz4[h][k].y;
+                        v[h][4 * k + 2] = ny4[h][k].z * nz4[h][k].z;
+                        v[h][4 * k + 3] = ny4[h][k].w * nz4[h][k].w;
                     }
-                if (q >= T2_S && !t2_wait(&empty[s2], (unsigned)((q / T2_S - 1) & 1), abort)) {
+                if (c + 1 < TC_NCH) fetch(c + 1);
+                if (q >= S && !tc_wait(&empty[s], (unsigned)((q / S - 1) & 1), abort)) {
                     ok = false;
                     break;
                 }
-                unsigned char *B = ring + s2 * T2_STAGE + T2_A;
+                unsigned char *B = ring + s * C::STAGE + TC_A;
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
+                for (int h = 0; h < C::RPT; h++) {
                     const int n = pr + 128 * h;
                     if (n >= N) continue;
                     const int off = (n >> 3) * 256 + (n & 7) * 16;
 #pragma unroll
-                    for (int k = 0; k < T2_KS; k++) {
+                    for (int k = 0; k < TC_KS; k++) {
                         float hi[8], lo[8];
 #pragma unroll
                         for (int e = 0; e < 8; e++) tf32_split(v[h][8 * k + e], hi[e], lo[e]);
-                        unsigned char *bh = B + (2 * k) * T2_B_KS + off, *bl = B + (2 * k + 1) * T2_B_KS + off;
+                        unsigned char *bh = B + (2 * k) * C::B_KS + off, *bl = B + (2 * k + 1) * C::B_KS + off;
                         *(float4 *)bh = make_float4(hi[0], hi[1], hi[2], hi[3]);
                         *(float4 *)(bh + 128) = make_float4(hi[4], hi[5], hi[6], hi[7]);
                         *(float4 *)bl = make_float4(lo[0], lo[1], lo[2], lo[3]);
@@ -531,74 +368,57 @@ __global__ void __launch_bounds__(T2_NT, 1)
                     }
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                t2_arrive(&fullB[s2]);
+                tc_arrive(&fullB[s]);
             }
         }
     } else {
         // ---- epilogue: warp w reads tensor-memory lanes 32 (w mod 4) .. + 31
-        const int qd = warp & 3, e = tid - T2_EPI0;
+        const int qd = warp & 3;
         const int xl = 32 * qd + lane;
         const AmStep st = am_step(p, m, ctl->timestep + 1);
         long long tl = 0;
         for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, tl++) {
-            const T2Tile w = t2_tile(t, ntx, N);
-            const int b = (int)(tl & 1);
-            // halo columns of the rows of this tile, while the accumulator fills
-            for (int hx = 0; hx < 2; hx++) {
-                const int xh = hx == 0 ? 0 : nx - 1;
-                if ((hx == 0 && w.xt != 0) || (hx == 1 && w.xt != ntx - 1)) continue;
-                for (int n = e; n < N; n += 128) {
-                    const long long R = w.r0 + n;
-                    if (R >= nrows) break;
-                    const int K = (int)(R / ny), J = (int)(R - (long long)K * ny);
-                    float acc = 0.f;
-                    if (zon[K])
-                        for (int i = 0; i < AM_NT; i++)
-                            acc = fmaf(__ldg(X + (long long)i * nx + xh),
-                                       __ldg(Y + (long long)i * ny + J) * __ldg(Z + (long long)i * nz + K), acc);
-                    const long long cell = (long long)K * g.sz + (long long)J * g.sy + xh;
-                    const double T = zon[K] ? st.liniT + st.Tfront * (double)acc : 0.0;
-                    a.d.T[cell] = T;
-                    if (a.d.lsindex && T > p.Tliq) a.d.lsindex[cell] = 1;
-                }
-            }
-            const bool got = t2_wait(&accf[b], (unsigned)((tl / 2) & 1), abort);
+            const int xt = (int)(t % ntx);
+            const long long r0 = (t / ntx) * (long long)N;
+            const int b = C::BUFS == 2 ? (int)(tl & 1) : 0;
+            const long long use = C::BUFS == 2 ? tl / 2 : tl;
+            const bool got = tc_wait(&accf[b], (unsigned)(use & 1), abort);
             // the warp-wide tcgen05.ld below needs the whole warp, converged
             if (!__all_sync(0xffffffffu, got)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const int x = 1 + T2_M * w.xt + xl;
+            const int x = 1 + TC_M * xt + xl;
             const bool xin = x <= g.gx;
-            long long R = w.r0;
+            long long R = r0;
             int K = (int)(R / ny), J = (int)(R - (long long)K * ny);
+            long long cell = (long long)K * g.sz + (long long)J * g.sy + x;
+            bool on = zon[K] != 0;
+            const unsigned lanes = (unsigned)(32 * qd) << 16;
             for (int cc = 0; cc < N; cc += 16) {
-                unsigned v[16];
-                const unsigned taddr = tmem + ((unsigned)(32 * qd) << 16) + (unsigned)(b * T2_NMAX + cc);
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-                    "%12, %13, %14, %15}, [%16];"
-                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                      "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                      "=r"(v[14]), "=r"(v[15])
-                    : "r"(taddr));
+                unsigned vh[16], vx[16];
+                tmem_ld16(tmem + lanes + (unsigned)(b * 2 * NB + cc), vh);
+                tmem_ld16(tmem + lanes + (unsigned)(b * 2 * NB + NB + cc), vx);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
                     if (xin && R < nrows) {
-                        const long long cell = (long long)K * g.sz + (long long)J * g.sy + x;
-                        const bool on = zon[K] != 0;
-                        const double T = on ? st.liniT + st.Tfront * (double)__uint_as_float(v[j]) : 0.0;
-                        a.d.T[cell] = T;
-                        if (a.d.lsindex && T > p.Tliq) a.d.lsindex[cell] = 1;
+                        // the two accumulators (the cross sum is ~2^-11 of the other)
+                        const float sum = __uint_as_float(vh[j]) + __uint_as_float(vx[j]);
+                        const float T = on ? (float)(st.liniT + st.Tfront * (double)sum) : 0.f;
+                        a.d.T32[cell] = T;
+                        if (a.d.lsindex && (double)T > p.Tliq) a.d.lsindex[cell] = 1;
                     }
                     R++;
+                    cell += g.sy;
                     if (++J == ny) {
                         J = 0;
                         K++;
+                        cell += g.sz - (long long)ny * g.sy;
+                        on = K < nz && zon[K] != 0;
                     }
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            t2_arrive(&acce[b]);
+            tc_arrive(&acce[b]);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -611,13 +431,57 @@ __global__ void __launch_bounds__(T2_NT, 1)
     }
 }
 
-// Rows per tile: the multiple of 16 (128 .. 256) whose tiles, dealt to one
-// persistent CTA per SM, leave the fewest rows on the busiest CTA.
-static int t2_rows_per_tile(long long nrows, int ntx, int nsm)
+// Temperature of the halo columns x = 0 and gx + 1 from the tables of step
+// ctl->timestep + ahead (FP32 form): the sum over the nodes in node order
+// with fused multiply-adds, into out (a temperature download buffer) or,
+// when out is null, into the FP32 temperature field with the layer flag.
+// One thread per (column, row); rows are consecutive across a warp, so the Y
+// loads coalesce.  Nothing is written when the tables were built for
+// another step.
+__global__ void __launch_bounds__(256) k_am_halo(KernelArgs a, AmParams m, double *out, int ahead)
 {
-    int best = T2_NMAX;
+    const Ctl *ctl = a.d.ctl;
+    const Geo &g = a.g;
+    const Phys &p = a.p;
+    const int nx = g.gx + 2, ny = g.gy + 2, nz = g.gz + 2;
+    const float *__restrict__ X = (const float *)a.d.am_tab;
+    const float *__restrict__ Y = X + (long long)AM_NT * nx;
+    const float *__restrict__ Z = Y + (long long)AM_NT * ny;
+    const int *zon = (const int *)(Z + (long long)AM_NT * nz);
+    const unsigned long long ts = ctl->timestep + (unsigned long long)ahead;
+    if (*am_tab_step(zon, nz) != ts) return;
+    const long long nrows = (long long)ny * nz;
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= 2 * nrows) return;
+    const int side = (int)(e / nrows);
+    const long long R = e - side * nrows;
+    const int K = (int)(R / ny), J = (int)(R - (long long)K * ny);
+    const int xh = side == 0 ? 0 : nx - 1;
+    float acc = 0.f;
+    if (zon[K])
+        for (int i = 0; i < AM_NT; i++)
+            acc = fmaf(__ldg(X + (long long)i * nx + xh), __ldg(Y + (long long)i * ny + J) * __ldg(Z + (long long)i * nz + K),
+                       acc);
+    const AmStep st = am_step(p, m, ts);
+    const long long cell = (long long)K * g.sz + (long long)J * g.sy + xh;
+    const double T = zon[K] ? st.liniT + st.Tfront * (double)acc : 0.0;
+    if (out) {
+        out[cell] = T;
+    } else {
+        const float T32 = (float)T;
+        a.d.T32[cell] = T32;
+        if (a.d.lsindex && (double)T32 > p.Tliq) a.d.lsindex[cell] = 1;
+    }
+}
+
+// Rows per tile for N = 128 tiles: the multiple of 16 (64 .. 128) whose
+// tiles, dealt to one persistent CTA per SM, leave the fewest rows on the
+// busiest CTA (ties: the larger tile, which reads the A image fewer times).
+static int tc_rows_per_tile(long long nrows, int ntx, int nsm, int nmax, int nmin)
+{
+    int best = nmax;
     long long best_load = -1;
-    for (int n = T2_NMAX; n >= 128; n -= 16) {
+    for (int n = nmax; n >= nmin; n -= 16) {
         const long long tiles = ntx * ((nrows + n - 1) / n);
         const long long load = ((tiles + nsm - 1) / nsm) * n;
         if (best_load < 0 || load < best_load) {
@@ -640,45 +504,48 @@ static int sm_count()
     return n;
 }
 
-// tile width: the fewest tiles of at most 256 x cells, rounded up to 32
-// (the epilogue splits a tile's columns in two halves of 16-column loads)
-int am_tc_tile_n(int nx)
-{
-    const int ntx = (nx + TC_NMAX - 1) / TC_NMAX;
-    int n = (nx + ntx - 1) / ntx;
-    return (n + 31) / 32 * 32;
-}
-
 // the kernels' shared-memory sizes; called once per context at set-up (not
 // during stream capture)
 int am_tc_prepare()
 {
     sm_count();
-    return cudaFuncSetAttribute(k_am_contract_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM) ==
-               cudaSuccess &&
-           cudaFuncSetAttribute(k_am_contract_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, T2_SMEM) ==
-               cudaSuccess;
+    return cudaFuncSetAttribute(k_am_contract_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TcCfg<128>::SMEM) == cudaSuccess &&
+           cudaFuncSetAttribute(k_am_contract_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                TcCfg<256>::SMEM) == cudaSuccess;
 }
 
-long long am_ximg_size(int gx) { return am_ximg_floats(gx); }
+long long am_ximg_size(int gx, int gy, int gz) { return am_ximg_part(gx) + (long long)(gy + gz + 4) * AM_NT; }
 
-int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream)
+// rows: 256-row tiles (one accumulator set), 64-128 rows (two), 0 = the
+// balanced choice up to 128
+int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, int rows)
 {
     const Geo &g = a.g;
-    if (a.d.am_ximg) {
-        const int ntx = (g.gx + T2_M - 1) / T2_M;
-        const long long nrows = (long long)(g.gy + 2) * (g.gz + 2);
-        const int nsm = sm_count();
-        const int N = t2_rows_per_tile(nrows, ntx, nsm);
-        const long long ntiles = (long long)ntx * ((nrows + N - 1) / N);
-        const unsigned grid = (unsigned)(ntiles < nsm ? ntiles : nsm);
-        k_am_contract_tc2<<<grid, T2_NT, T2_SMEM, (cudaStream_t)stream>>>(a, m, N, ntx, ntiles);
-        return 1;
+    const int ntx = (g.gx + TC_M - 1) / TC_M;
+    const long long nrows = (long long)(g.gy + 2) * (g.gz + 2);
+    const int nsm = sm_count();
+    const bool wide = rows == 256;
+    const int N = wide ? 256 : (rows >= 64 && rows <= 128 ? rows / 16 * 16 : tc_rows_per_tile(nrows, ntx, nsm, 128, 64));
+    const long long ntiles = (long long)ntx * ((nrows + N - 1) / N);
+    const unsigned grid = (unsigned)(ntiles < nsm ? ntiles : nsm);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (wide) k_am_contract_tc<256><<<grid, TC_NT, TcCfg<256>::SMEM, st>>>(a, m, N, ntx, ntiles);
+    else k_am_contract_tc<128><<<grid, TC_NT, TcCfg<128>::SMEM, st>>>(a, m, N, ntx, ntiles);
+    int n = 1;
+    if (a.d.lsindex) {
+        // the layer flag is kept for every cell, halo columns included
+        const long long e = 2 * nrows;
+        k_am_halo<<<(unsigned)((e + 255) / 256), 256, 0, st>>>(a, m, nullptr, 1);
+        n++;
     }
-    const int nx = g.gx + 2;
-    const int N = am_tc_tile_n(nx);
-    dim3 grid((unsigned)((nx + N - 1) / N), (unsigned)(((long long)(g.gy + 2) * (g.gz + 2) + TC_M - 1) / TC_M));
-    k_am_contract_tc<<<grid, TC_NT, TC_SMEM, (cudaStream_t)stream>>>(a, m, N);
+    return n;
+}
+
+int launch_am_halo_fill(const KernelArgs &a, const AmParams &m, double *dev_out, void *stream)
+{
+    const long long e = 2LL * (a.g.gy + 2) * (a.g.gz + 2);
+    k_am_halo<<<(unsigned)((e + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a, m, dev_out, 0);
     return 1;
 }
 

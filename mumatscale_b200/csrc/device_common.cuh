@@ -41,10 +41,10 @@ __device__ __forceinline__ bool in_bounds(Ctl *c, long long i, long long n)
 // direct_temp_calc (temperature.c:24-61) for the analytic models; the AM
 // quadrature is precomputed into an array by k_temp_am.  K is the local
 // plane; p.kz0 places a slab's planes in the whole domain.
-__device__ __forceinline__ double temp_cell(const Phys &p, const double *Tarr, long long cell,
+__device__ __forceinline__ double temp_cell(const Phys &p, const double *Tarr, const float *T32, long long cell,
                                             long long J, long long K, unsigned long long ts)
 {
-    if (p.temp_mode == 2) return Tarr[cell];
+    if (p.temp_mode == 2) return T32 ? (double)T32[cell] : Tarr[cell];
     double sim_time = (double)ts * p.ts_delt;
     if (p.temp_mode == 0) return p.T0 - sim_time * p.cool_rate;
     double ry = p.origin[1] + ((double)(int)J + 0.5) * p.cellSize;
@@ -84,6 +84,27 @@ __device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
 // AM moving-source quadrature: nodes, and the source position and prefactor
 // of a step (direct_temp_calc thermal_ana == 1, temperature.c:62-123)
 constexpr int AM_NT = 400;
+
+// The FP32 form's tensor-core operand buffer (a.d.am_ximg): the X image of
+// am_tc.cu ([x tile of 128][K-step of 8 nodes][TF32 head, remainder][128 x
+// 8]), then Y and Z with the 400 nodes contiguous for each row (YT[J][i],
+// ZT[K][i]).
+__host__ __device__ constexpr long long am_ximg_part(int gx)
+{
+    return (long long)((gx + 127) / 128) * (AM_NT / 8) * 2 * (128 * 8);
+}
+__host__ __device__ inline float *am_yt(float *img, int gx) { return img + am_ximg_part(gx); }
+__host__ __device__ inline float *am_zt(float *img, int gx, int gy)
+{
+    return img + am_ximg_part(gx) + (long long)(gy + 2) * AM_NT;
+}
+
+// The step the AM tables (k_am_tables: X, Y, Z, then the per-plane flags
+// zon[nz]) were last built for, kept in the table buffer after the flags.
+__device__ __forceinline__ unsigned long long *am_tab_step(const int *zon, int nz)
+{
+    return (unsigned long long *)(((unsigned long long)(zon + nz) + 7ULL) & ~7ULL);
+}
 
 struct AmStep {
     double xnow, ynow, znow, lalpha, ls, ldt, Tfront, liniT;

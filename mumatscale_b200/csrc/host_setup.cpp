@@ -285,7 +285,9 @@ Geo make_geo(const mms_params &p)
     g.rsy = g.gx + 2;
     g.rsz = (long long)(g.gx + 2) * (g.gy + 2);
     g.rN = g.rsz * (g.gz + 2);
-    g.P = (g.gx + 2 + 7) / 8 * 8;
+    // rows of the halo'd x extent plus the 3-element lead the stencil's tensor
+    // maps start with (kernels.cu, alignment note), a multiple of 8 elements
+    g.P = (g.gx + 2 + 3 + 7) / 8 * 8;
     g.sy = g.P;
     g.sz = g.P * (g.gy + 2);
     g.N = g.sz * (g.gz + 2);

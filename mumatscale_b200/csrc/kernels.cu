@@ -183,16 +183,23 @@ __global__ void k_am_tables(KernelArgs a, AmParams m)
         } else if (q < nx + ny) {
             const int J = q - nx;
             const double ly = (p.origin[1] + ((double)J + 0.5) * p.cellSize) - s.ynow;
-            Y[(long long)i * ny + J] = (Real)exp(-(ly * ly) / ai);
+            const Real yv = (Real)exp(-(ly * ly) / ai);
+            Y[(long long)i * ny + J] = yv;
+            // the tensor-core producers' copy, nodes contiguous per row (am_tc.cu)
+            if (sizeof(Real) == 4 && a.d.am_ximg) am_yt(a.d.am_ximg, g.gx)[(long long)J * AM_NT + i] = (float)yv;
         } else {
             const int K = q - nx - ny;
             const double rz = p.origin[2] + ((double)(K + p.kz0) + 0.5) * p.cellSize;
             const double lz = rz - s.znow;
             const double Tlocal = sqrt(s.lalpha * lt) * ai;
-            Z[(long long)i * nz + K] = (Real)(s.ldt * exp(-(lz * lz / (4. * s.lalpha * lt))) / Tlocal);
+            const Real zv = (Real)(s.ldt * exp(-(lz * lz / (4. * s.lalpha * lt))) / Tlocal);
+            Z[(long long)i * nz + K] = zv;
+            if (sizeof(Real) == 4 && a.d.am_ximg)
+                am_zt(a.d.am_ximg, g.gx, g.gy)[(long long)K * AM_NT + i] = (float)zv;
             if (i == 0) zon[K] = (rz <= s.znow + p.cellSize) ? 1 : 0;
         }
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *am_tab_step(zon, nz) = ctl->timestep + 1;
 }
 
 // T over tiles of (XL MX) x-cells by (G MY) (y, z) rows, G = 256 / XL: each
@@ -335,7 +342,7 @@ __device__ __forceinline__ void nuc_body(const KernelArgs &a, int bid)
         if (a.d.gr[c] <= 0) {
             const Real *cl = (const Real *)a.d.cl[(int)(ctl->timestep & 1ULL)];
             long long K = c / g.sz, J = (c % g.sz) / g.sy;
-            double Ttemp = temp_cell(p, a.d.T, c, J, K, ts);
+            double Ttemp = temp_cell(p, a.d.T, a.d.T32, c, J, K, ts);
             int layerno = 1, initnuc = 1;
             if (p.am) {
                 double sim_time = (double)ts * p.ts_delt;
@@ -832,11 +839,8 @@ __global__ void k_curv(KernelArgs a)
 // interior: no face of this cell touches the domain halo, so every (1 -
 // mold) factor is 1.0 and the multiplication by it (exact) is skipped.
 template <typename Real>
-__device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p, Real conc, Real lspfs,
-                                            const Real (&nb_cl)[6], const Real (&nb_fs)[6],
-                                            const Real (&one_m)[6], bool interior, Real oce, int grc,
-                                            double Td, const double *curv, long long c, Real &cen,
-                                            Real &cl_new, Real &fs_new, int &gr_new, int &br)
+__device__ __forceinline__ Real diff_sum(const PhysR<Real> &q, Real conc, Real lspfs, const Real (&nb_cl)[6],
+                                         const Real (&nb_fs)[6], const Real (&one_m)[6], bool interior)
 {
     Real nbsum = 0;
     if (sizeof(Real) == 4) {
@@ -867,6 +871,15 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
             nbsum += r * (nb_cl[n] - conc);
         }
     }
+    return nbsum;
+}
+
+// fs_change_diffuse (growth.c:220-272) of one cell given its diffusion sum.
+template <typename Real>
+__device__ __forceinline__ void fs_update(const PhysR<Real> &q, const Phys &p, Real conc, Real lspfs, Real nbsum,
+                                          Real oce, int grc, double Td, const double *curv, long long c, Real &cen,
+                                          Real &cl_new, Real &fs_new, int &gr_new, int &br)
+{
     cen = oce + nbsum;
     gr_new = grc;
     if (sizeof(Real) == 8) {
@@ -937,13 +950,36 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
     }
 }
 
+template <typename Real>
+__device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p, Real conc, Real lspfs,
+                                            const Real (&nb_cl)[6], const Real (&nb_fs)[6],
+                                            const Real (&one_m)[6], bool interior, Real oce, int grc,
+                                            double Td, const double *curv, long long c, Real &cen,
+                                            Real &cl_new, Real &fs_new, int &gr_new, int &br)
+{
+    fs_update<Real>(q, p, conc, lspfs, diff_sum<Real>(q, conc, lspfs, nb_cl, nb_fs, one_m, interior), oce, grc, Td,
+                    curv, c, cen, cl_new, fs_new, gr_new, br);
+}
+
 constexpr int DTX = 32, DTY = 8;
 
 // TMA-fed variant.  A CTA of 32 x 8 threads owns a (32 CPT) x 8 column of
-// cells (each thread CPT cells along x, 32 apart) and marches up a z-chunk;
-// planes of cl and fs with their x/y halo (and ce, gr without) are brought
-// into a TS-deep shared-memory ring by cp.async.bulk.tensor, one mbarrier
-// per slot, issued TS-1 planes ahead of the plane being updated.
+// cells and marches up a z-chunk: one cell per thread (CPT = 1,
+// stencil_tile) or two adjacent cells per thread (CPT = 2,
+// stencil_tile_pair), which read their cells and neighbours as 8- or
+// 16-byte words of shared memory and write them as such words of global
+// memory.  Planes of cl and fs with their x/y halo (and ce, gr without) are
+// brought into a TS-deep shared-memory ring by cp.async.bulk.tensor, one
+// mbarrier per slot, issued TS-1 planes ahead of the plane being updated.
+//
+// Alignment.  The fields start 16 - sizeof(element) bytes past a 16-byte
+// boundary (field_lead in mms_api.cu) and rows are a multiple of 8
+// elements, so interior cell 1 of every row, and every 32nd cell after it,
+// is 16-byte aligned.  The tensor maps begin at that boundary, lead =
+// 16 / sizeof(element) - 1 elements before the field, with x extent
+// gx + 2 + lead: a cl/fs box starts at map x = i0 - 1 (a multiple of the tile
+// width) and so holds the tile's first cell i0 at column HX = lead + 1; the
+// ce and gr boxes start at i0 itself.
 template <typename Real, int CPT>
 struct Depth {
     // planes in the ring: deeper for FP32 with one cell per thread, whose
@@ -958,11 +994,13 @@ constexpr int round128(int b) { return (b + 127) / 128 * 128; }
 template <typename Real, int CPT>
 struct Stage {
     static constexpr int TX = DTX * CPT;
-    // box widths: a multiple of 16 bytes, starting at the aligned column i0-1
+    // box widths: a multiple of 16 bytes
     static constexpr int EPA = 16 / (int)sizeof(Real);
-    static constexpr int BXH = (TX + 2 + EPA - 1) / EPA * EPA;  // cl, fs: DTY+2 rows
-    static constexpr int BXC = BXH;                              // ce: DTY rows
-    static constexpr int BXG = (TX + 2 + 3) / 4 * 4;             // gr (int): DTY rows
+    static constexpr int LEAD = EPA - 1;                             // field lead (elements)
+    static constexpr int HX = EPA;                                   // column of cell i0 in a cl/fs box
+    static constexpr int BXH = (TX + HX + 1 + EPA - 1) / EPA * EPA;  // cl, fs: DTY+2 rows, to the right halo
+    static constexpr int BXC = TX;                                   // ce: DTY rows from i0
+    static constexpr int BXG = TX;                                   // gr (int, lead 3): DTY rows from i0
     static constexpr int CL = round128(BXH * (DTY + 2) * (int)sizeof(Real));
     static constexpr int CE = round128(BXC * DTY * (int)sizeof(Real));
     static constexpr int GR = round128(BXG * DTY * 4);
@@ -1029,8 +1067,8 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
         tma_load_3d(stage(s), mcl, i0 - 1, j0 - 1, k, &bars[s]);
         tma_load_3d(stage(s) + L::CL, mfs, i0 - 1, j0 - 1, k, &bars[s]);
         if (center) {
-            tma_load_3d(stage(s) + 2 * L::CL, &maps.ce, i0 - 1, j0, k, &bars[s]);
-            tma_load_3d(stage(s) + 2 * L::CL + L::CE, &maps.gr, i0 - 1, j0, k, &bars[s]);
+            tma_load_3d(stage(s) + 2 * L::CL, &maps.ce, i0 + L::LEAD, j0, k, &bars[s]);
+            tma_load_3d(stage(s) + 2 * L::CL + L::CE, &maps.gr, i0 + 3, j0, k, &bars[s]);
         }
     };
     auto phase = [&](int pl) { return (unsigned)(((base + pl) / TS) & 1u); };
@@ -1038,7 +1076,7 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
     // (direct_temp_calc's isothermal and gradient models in 3D)
     const bool t_per_plane = (p.temp_mode == 0) || (p.temp_mode == 1 && !p.gz_is_one);
     if (tid == 0) sh.abort = 0;
-    if (t_per_plane && tid <= k1 - k0) sh.sT[tid] = temp_cell(p, a.d.T, 0, 1, k0 + tid, ts);
+    if (t_per_plane && tid <= k1 - k0) sh.sT[tid] = temp_cell(p, a.d.T, a.d.T32, 0, 1, k0 + tid, ts);
     __syncthreads();
     if (tid == 0)
         for (int pl = 0; pl < TS && pl < nplanes; pl++) issue(pl);
@@ -1056,9 +1094,9 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
 #pragma unroll
     for (int u = 0; u < CPT; u++) {
         const int i = i0 + tx + DTX * u;
-        hh[u] = (ty + 1) * L::BXH + tx + DTX * u + 1;
-        hcc[u] = ty * L::BXC + tx + DTX * u + 1;
-        hgg[u] = ty * L::BXG + tx + DTX * u + 1;
+        hh[u] = (ty + 1) * L::BXH + tx + DTX * u + L::HX;
+        hcc[u] = ty * L::BXC + tx + DTX * u;
+        hgg[u] = ty * L::BXG + tx + DTX * u;
         act[u] = i <= g.gx && jrow;
         in_xy[u] = i > 1 && i < g.gx && j > 1 && j < g.gy;
         omx_p[u] = i == g.gx ? one_x : (Real)1;
@@ -1075,14 +1113,18 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
     const bool t_arr = p.temp_mode == 2;
     double Tn[CPT];
 #pragma unroll
-    for (int u = 0; u < CPT; u++) Tn[u] = (t_arr && act[u]) ? __ldg(a.d.T + crow + i0 + tx + DTX * u) : 0.0;
+    // (the FP32 form keeps it in FP32)
+    auto t_load = [&](long long c) -> double {
+        return sizeof(Real) == 4 ? (double)__ldg(a.d.T32 + c) : __ldg(a.d.T + c);
+    };
+    for (int u = 0; u < CPT; u++) Tn[u] = (t_arr && act[u]) ? t_load(crow + i0 + tx + DTX * u) : 0.0;
     for (int t = 0; t <= k1 - k0; t++) {
         const int k = k0 + t;
         double Tc[CPT];
 #pragma unroll
         for (int u = 0; u < CPT; u++) {
             Tc[u] = Tn[u];
-            if (t_arr && act[u] && t < k1 - k0) Tn[u] = __ldg(a.d.T + crow + g.sz + i0 + tx + DTX * u);
+            if (t_arr && act[u] && t < k1 - k0) Tn[u] = t_load(crow + g.sz + i0 + tx + DTX * u);
         }
         // planes t and t+1 completed in earlier iterations
         bool ok = mbar_wait(&bars[s2], ph2);
@@ -1112,7 +1154,7 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
                 const long long c = crow + i;
                 const Real oce = sce[hcc[u]];
                 const int grc = sgr[hgg[u]];
-                const double Td = t_per_plane ? Tp : (t_arr ? Tc[u] : temp_cell(p, a.d.T, c, j, k, ts));
+                const double Td = t_per_plane ? Tp : (t_arr ? Tc[u] : temp_cell(p, a.d.T, a.d.T32, c, j, k, ts));
                 const bool interior = in_xy[u] && in_z;
                 Real cen, cl_new, fs_new;
                 int gr_new, br;
@@ -1178,6 +1220,292 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
     return alive;
 }
 
+// Two adjacent cells per thread (CPT = 2): thread tx of row ty owns cells
+// i = i0 + 2 tx and i + 1.  Each plane it reads the pair and its four x/y
+// neighbour pairs of cl and fs as single 8- (FP32) or 16-byte (FP64) words
+// of shared memory, the pair above (plane k + 1) likewise, and takes the
+// pairs of planes k and k - 1 from registers, rolled up the z-chunk; the x
+// neighbours of the two cells are the neighbouring pairs' inner halves.  The
+// FP32 form sums the six neighbour terms of both cells with paired FP32
+// instructions (each component rounds exactly as the scalar fmaf chain of
+// diff_sum); the FP64 form sums each cell in the reference's order.  Cells,
+// temperatures and results move as one word per field and pair.  The solid
+// bitmask words of the CTA's 64 cells come from two warp OR-reductions.
+template <typename Real>
+struct Vec2;
+template <>
+struct Vec2<float> {
+    using T = float2;
+};
+template <>
+struct Vec2<double> {
+    using T = double2;
+};
+
+template <typename Real>
+__device__ __forceinline__ typename Vec2<Real>::T vec2(Real x, Real y)
+{
+    typename Vec2<Real>::T v;
+    v.x = x;
+    v.y = y;
+    return v;
+}
+
+template <typename Real>
+__device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const TmaMaps &maps, int zchunk, int bx, int by,
+                                                  int bz, unsigned char *smem, StencilShared<Depth<Real, 2>::TS> &sh,
+                                                  unsigned &ring, double *part = nullptr, long long part_idx = 0)
+{
+    using L = Stage<Real, 2>;
+    using V = typename Vec2<Real>::T;
+    constexpr int TS = Depth<Real, 2>::TS;
+    Ctl *ctl = a.d.ctl;
+    unsigned long long *bars = sh.bars;
+    const Geo &g = a.g;
+    const Phys &p = a.p;
+    const unsigned long long ts = ctl->timestep;
+    const int pin = (int)((ts - 1) & 1ULL), pout = (int)(ts & 1ULL);
+    Real *__restrict__ clO = (Real *)a.d.cl[pout];
+    Real *__restrict__ fsO = (Real *)a.d.fs[pout];
+    Real *__restrict__ ce = (Real *)a.d.ce;
+    int *__restrict__ gr = a.d.gr;
+    const PhysR<Real> q = phys_r<Real>(p);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DTX + tx;
+    const int i0 = bx * L::TX + 1, j0 = by * DTY + 1;
+    const int i = i0 + 2 * tx, j = j0 + ty;
+    const int k0 = bz * zchunk + 1;
+    const int k1 = min(k0 + zchunk - 1, g.gz);
+    const int nplanes = k1 - k0 + 3;  // k0-1 .. k1+1
+    const CUtensorMap *mcl = &maps.cl[pin];
+    const CUtensorMap *mfs = &maps.fs[pin];
+    const unsigned base = ring;
+
+    auto stage = [&](int s) { return smem + s * L::BYTES; };
+    auto issue = [&](int pl) {
+        const int s = (int)((base + pl) % TS), k = k0 - 1 + pl;
+        const bool center = (k >= k0 && k <= k1);
+        mbar_expect_tx(&bars[s], L::TX_HALO + (center ? L::TX_CENTER : 0u));
+        tma_load_3d(stage(s), mcl, i0 - 1, j0 - 1, k, &bars[s]);
+        tma_load_3d(stage(s) + L::CL, mfs, i0 - 1, j0 - 1, k, &bars[s]);
+        if (center) {
+            tma_load_3d(stage(s) + 2 * L::CL, &maps.ce, i0 + L::LEAD, j0, k, &bars[s]);
+            tma_load_3d(stage(s) + 2 * L::CL + L::CE, &maps.gr, i0 + 3, j0, k, &bars[s]);
+        }
+    };
+    auto phase = [&](int pl) { return (unsigned)(((base + pl) / TS) & 1u); };
+    const bool t_per_plane = (p.temp_mode == 0) || (p.temp_mode == 1 && !p.gz_is_one);
+    if (tid == 0) sh.abort = 0;
+    if (t_per_plane && tid <= k1 - k0) sh.sT[tid] = temp_cell(p, a.d.T, a.d.T32, 0, 1, k0 + tid, ts);
+    __syncthreads();
+    if (tid == 0)
+        for (int pl = 0; pl < TS && pl < nplanes; pl++) issue(pl);
+    int issued = min(TS, nplanes);  // same value in every thread
+
+    const Real one_x = (Real)(1 - g.padx), one_y = (Real)(1 - g.pady), one_zp = (Real)(1 - g.padz_hi),
+               one_zm = (Real)(1 - g.padz_lo);
+    const long long wrow = (long long)g.wpr;
+    const bool jrow = j <= g.gy;
+    const bool act0 = i <= g.gx && jrow, act1 = i + 1 <= g.gx && jrow;
+    // (1 - mold) of the faces: +x and -x of cell i, +x of cell i + 1 (its -x
+    // face is cell i), +y and -y of both
+    const Real o0xp = i == g.gx ? one_x : (Real)1, o0xm = i == 1 ? one_x : (Real)1;
+    const Real o1xp = i + 1 == g.gx ? one_x : (Real)1;
+    const Real omy_p = j == g.gy ? one_y : (Real)1, omy_m = j == 1 ? one_y : (Real)1;
+    // the CTA's tile touches a domain face in x or y (uniform over the CTA);
+    // elsewhere every (1 - mold) factor is 1 and the (exact) product by it is
+    // skipped
+    const bool edge_xy = (i0 == 1) || (i0 + L::TX - 1 >= g.gx) || (j0 == 1) || (j0 + DTY - 1 >= g.gy);
+    const int hc = (ty + 1) * L::BXH + L::HX + 2 * tx;  // cell i in a cl/fs box
+    const int hcc = ty * L::BXC + 2 * tx;                // cell i in a ce/gr box
+    int s0 = (int)(base % TS), s1 = (int)((base + 1) % TS), s2 = (int)((base + 2) % TS);
+    unsigned ph2 = phase(2);
+    long long crow = (long long)k0 * g.sz + (long long)j * g.sy;
+    bool alive = true;
+    double fsum = 0.0;  // this thread's new fs values, in plane order
+    // AM temperature array (FP32 in the FP32 form): the pair's values are
+    // loaded one plane ahead, so that their latency overlaps a plane of work
+    const bool t_arr = p.temp_mode == 2;
+    auto t_load = [&](long long c, double &t0, double &t1) {
+        if (sizeof(Real) == 4) {
+            const float2 v = __ldg((const float2 *)(a.d.T32 + c));
+            t0 = v.x;
+            t1 = v.y;
+        } else {
+            const double2 v = __ldg((const double2 *)(a.d.T + c));
+            t0 = v.x;
+            t1 = v.y;
+        }
+    };
+    double Tn0 = 0.0, Tn1 = 0.0;
+    if (t_arr && act0) t_load(crow + i, Tn0, Tn1);
+    V zm_cl = vec2<Real>(0, 0), zc_cl = zm_cl, zm_fs = zm_cl, zc_fs = zm_cl;
+    for (int t = 0; t <= k1 - k0; t++) {
+        const int k = k0 + t;
+        const double T0 = Tn0, T1 = Tn1;
+        if (t_arr && act0 && t < k1 - k0) t_load(crow + g.sz + i, Tn0, Tn1);
+        // planes t and t+1 completed in earlier iterations
+        bool ok = mbar_wait(&bars[s2], ph2);
+        if (t == 0) ok &= mbar_wait(&bars[s0], phase(0)) && mbar_wait(&bars[s1], phase(1));
+        if (!ok) sh.abort = 1;
+        const Real *cc = (const Real *)stage(s1), *cp = (const Real *)stage(s2);
+        const Real *fc = (const Real *)(stage(s1) + L::CL), *fp = (const Real *)(stage(s2) + L::CL);
+        const Real *sce = (const Real *)(stage(s1) + 2 * L::CL);
+        const int *sgr = (const int *)(stage(s1) + 2 * L::CL + L::CE);
+        if (t == 0 && ok) {
+            zm_cl = *(const V *)((const Real *)stage(s0) + hc);
+            zm_fs = *(const V *)((const Real *)(stage(s0) + L::CL) + hc);
+            zc_cl = *(const V *)(cc + hc);
+            zc_fs = *(const V *)(fc + hc);
+        }
+        const Real omz_p = k == g.gz ? one_zp : (Real)1, omz_m = k == 1 ? one_zm : (Real)1;
+        const bool edge = edge_xy || k == 1 || k == g.gz;
+        V zp_cl = zc_cl, zp_fs = zc_fs;
+        int solid0 = 0, solid1 = 0;
+        if (act0 && ok) {
+            zp_cl = *(const V *)(cp + hc);
+            zp_fs = *(const V *)(fp + hc);
+            const V lcl = *(const V *)(cc + hc - 2), rcl = *(const V *)(cc + hc + 2);
+            const V ucl = *(const V *)(cc + hc + L::BXH), dcl = *(const V *)(cc + hc - L::BXH);
+            const V lfs = *(const V *)(fc + hc - 2), rfs = *(const V *)(fc + hc + 2);
+            const V ufs = *(const V *)(fc + hc + L::BXH), dfs = *(const V *)(fc + hc - L::BXH);
+            const V oce = *(const V *)(sce + hcc);
+            const int2 grc = *(const int2 *)(sgr + hcc);
+            Real nb0, nb1;
+            if (sizeof(Real) == 4) {
+                // the neighbour terms of both cells at once: +x, -x, +y, -y, +z, -z
+                const float B = 0.5f * ((float)q.rs - (float)q.rl);
+                const float2 B2 = make_float2(B, B), rl2 = make_float2((float)q.rl, (float)q.rl);
+                const float2 conc = make_float2((float)zc_cl.x, (float)zc_cl.y);
+                const float2 nconc = make_float2(-conc.x, -conc.y);
+                const float2 A2 = __ffma2_rn(B2, make_float2((float)zc_fs.x, (float)zc_fs.y), rl2);
+                const float2 ncl[6] = {make_float2((float)zc_cl.y, (float)rcl.x), make_float2((float)lcl.y, (float)zc_cl.x),
+                                       make_float2((float)ucl.x, (float)ucl.y), make_float2((float)dcl.x, (float)dcl.y),
+                                       make_float2((float)zp_cl.x, (float)zp_cl.y),
+                                       make_float2((float)zm_cl.x, (float)zm_cl.y)};
+                const float2 nfs[6] = {make_float2((float)zc_fs.y, (float)rfs.x), make_float2((float)lfs.y, (float)zc_fs.x),
+                                       make_float2((float)ufs.x, (float)ufs.y), make_float2((float)dfs.x, (float)dfs.y),
+                                       make_float2((float)zp_fs.x, (float)zp_fs.y),
+                                       make_float2((float)zm_fs.x, (float)zm_fs.y)};
+                const float2 om[6] = {make_float2((float)o0xp, (float)o1xp), make_float2((float)o0xm, 1.f),
+                                      make_float2((float)omy_p, (float)omy_p), make_float2((float)omy_m, (float)omy_m),
+                                      make_float2((float)omz_p, (float)omz_p), make_float2((float)omz_m, (float)omz_m)};
+                float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int n = 0; n < 6; n++) {
+                    float2 r = __ffma2_rn(B2, nfs[n], A2);
+                    if (edge) r = __fmul2_rn(r, om[n]);
+                    acc = __ffma2_rn(r, __fadd2_rn(ncl[n], nconc), acc);
+                }
+                nb0 = (Real)acc.x;
+                nb1 = (Real)acc.y;
+            } else {
+                const Real c0[6] = {zc_cl.y, lcl.y, ucl.x, dcl.x, zp_cl.x, zm_cl.x};
+                const Real f0[6] = {zc_fs.y, lfs.y, ufs.x, dfs.x, zp_fs.x, zm_fs.x};
+                const Real m0[6] = {o0xp, o0xm, omy_p, omy_m, omz_p, omz_m};
+                const Real c1[6] = {rcl.x, zc_cl.x, ucl.y, dcl.y, zp_cl.y, zm_cl.y};
+                const Real f1[6] = {rfs.x, zc_fs.x, ufs.y, dfs.y, zp_fs.y, zm_fs.y};
+                const Real m1[6] = {o1xp, (Real)1, omy_p, omy_m, omz_p, omz_m};
+                nb0 = diff_sum<Real>(q, zc_cl.x, zc_fs.x, c0, f0, m0, !edge);
+                nb1 = diff_sum<Real>(q, zc_cl.y, zc_fs.y, c1, f1, m1, !edge);
+            }
+            const long long c = crow + i;
+            const double Tp = t_per_plane ? sh.sT[t] : 0.0;
+            const double Td0 = t_per_plane ? Tp : (t_arr ? T0 : temp_cell(p, a.d.T, a.d.T32, c, j, k, ts));
+            Real cen0, cl0, fs0;
+            int g0, br0;
+            fs_update<Real>(q, p, zc_cl.x, zc_fs.x, nb0, oce.x, grc.x, Td0, a.d.curv, c, cen0, cl0, fs0, g0, br0);
+            if (sizeof(Real) == 8 ? cen0 < 0 : cen0 < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
+            solid0 = g0 > 0;
+            if (part) fsum += (double)fs0;
+            if (act1) {
+                const double Td1 = t_per_plane ? Tp : (t_arr ? T1 : temp_cell(p, a.d.T, a.d.T32, c + 1, j, k, ts));
+                Real cen1, cl1, fs1;
+                int g1, br1;
+                fs_update<Real>(q, p, zc_cl.y, zc_fs.y, nb1, oce.y, grc.y, Td1, a.d.curv, c + 1, cen1, cl1, fs1, g1,
+                                br1);
+                if (sizeof(Real) == 8 ? cen1 < 0 : cen1 < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
+                solid1 = g1 > 0;
+                if (part) fsum += (double)fs1;
+                if (in_bounds(ctl, c + 1, g.N)) {
+                    *(V *)(ce + c) = vec2<Real>(cen0, cen1);
+                    *(V *)(clO + c) = vec2<Real>(cl0, cl1);
+                    *(V *)(fsO + c) = vec2<Real>(fs0, fs1);
+                    if (g0 != grc.x || g1 != grc.y) *(int2 *)(gr + c) = make_int2(g0, g1);
+                }
+            } else if (in_bounds(ctl, c, g.N)) {
+                // the last interior cell of an odd-length row: cell i + 1 is the halo
+                ce[c] = cen0;
+                clO[c] = cl0;
+                fsO[c] = fs0;
+                if (g0 != grc.x) gr[c] = g0;
+            }
+        }
+        // the CTA's 64 cells of row j: bits 2 tx, 2 tx + 1 of words 2 bx (tx <
+        // 16) and 2 bx + 1
+        const unsigned mine = ((unsigned)solid0 | ((unsigned)solid1 << 1)) << ((2 * tx) & 31);
+        const unsigned w0 = __reduce_or_sync(FULL_MASK, tx < 16 ? mine : 0u);
+        const unsigned w1 = __reduce_or_sync(FULL_MASK, tx >= 16 ? mine : 0u);
+        if (tx == 0 && jrow) {
+            const long long wi = ((long long)k * (g.gy + 2) + j) * wrow + 2 * bx;
+            if (2 * bx < g.wpr && in_bounds(ctl, wi, g.nwords)) a.d.solid_bits[wi] = w0;
+            if (2 * bx + 1 < g.wpr && in_bounds(ctl, wi + 1, g.nwords)) a.d.solid_bits[wi + 1] = w1;
+        }
+        __syncthreads();
+        if (sh.abort) {
+            // a copy did not land within the bound: report, then wait (again
+            // bounded) for every copy still in flight before leaving
+            if (tid == 0) {
+                raise_error(ctl, MMS_ERR_TIMEOUT);
+                for (int pl = t; pl < issued; pl++) mbar_wait(&bars[(base + pl) % TS], phase(pl));
+            }
+            alive = false;
+            break;
+        }
+        if (t + TS < nplanes) {
+            if (tid == 0) issue(t + TS);
+            issued = t + TS + 1;
+        }
+        // advance the ring and the thread's column
+        s0 = s1;
+        s1 = s2;
+        s2 = (s2 + 1 == TS) ? 0 : s2 + 1;
+        if (s2 == 0) ph2 ^= 1u;
+        zm_cl = zc_cl;
+        zm_fs = zc_fs;
+        zc_cl = zp_cl;
+        zc_fs = zp_fs;
+        crow += g.sz;
+    }
+    ring = base + (unsigned)nplanes;
+    if (part && alive) {
+        // fixed-order tree: lanes, then the 8 warps
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) fsum += __shfl_down_sync(FULL_MASK, fsum, o);
+        if (tx == 0) sh.fsum[ty] = fsum;
+        __syncthreads();
+        if (tid == 0) {
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < DTY; w++) v += sh.fsum[w];
+            part[2 * part_idx] = v;
+            part[2 * part_idx + 1] = 0.0;
+        }
+    }
+    return alive;
+}
+
+// The tile of either width.
+template <typename Real, int CPT>
+__device__ __forceinline__ bool run_tile(const KernelArgs &a, const TmaMaps &maps, int zchunk, int bx, int by, int bz,
+                                         unsigned char *smem, StencilShared<Depth<Real, CPT>::TS> &sh, unsigned &ring,
+                                         double *part = nullptr, long long part_idx = 0)
+{
+    if constexpr (CPT == 2)
+        return stencil_tile_pair<Real>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
+    else
+        return stencil_tile<Real, 1>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
+}
+
 // SUMFS: each tile also leaves its sum of the new fraction solid in
 // a.d.fs_part (the step a reduction follows; ~3 % slower otherwise).
 template <typename Real, int CPT, bool SUMFS>
@@ -1193,7 +1521,7 @@ __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
         fence_barrier_init();
     }
     unsigned ring = 0;
-    stencil_tile<Real, CPT>(a, maps, zchunk, blockIdx.x, blockIdx.y, blockIdx.z, smem, sh, ring,
+    run_tile<Real, CPT>(a, maps, zchunk, blockIdx.x, blockIdx.y, blockIdx.z, smem, sh, ring,
                             SUMFS ? a.d.fs_part : nullptr,
                             ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
 }
@@ -1251,7 +1579,7 @@ __global__ void __launch_bounds__(DTX *DTY, (Depth<Real, CPT>::MINB))
         const int bx = (int)(local % it.tiles_x);
         const int by = (int)((local / it.tiles_x) % it.tiles_y);
         const int bz = (int)(local / ((long long)it.tiles_x * it.tiles_y));
-        if (!stencil_tile<Real, CPT>(sa, it.maps, it.zchunk, bx, by, bz, smem, sh, ring)) break;
+        if (!run_tile<Real, CPT>(sa, it.maps, it.zchunk, bx, by, bz, smem, sh, ring)) break;
     }
 }
 
@@ -1319,7 +1647,7 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchun
                                    j == g.gy ? one_y : (Real)1, j == 1 ? one_y : (Real)1,
                                    k == g.gz ? one_zp : (Real)1, k == 1 ? one_zm : (Real)1};
             const int grc = gr[c];
-            const double Td = temp_cell(p, a.d.T, c, j, k, ts);
+            const double Td = temp_cell(p, a.d.T, a.d.T32, c, j, k, ts);
             Real cen, cl_new, fs_new;
             int gr_new, br;
             const bool interior = i > 1 && i < g.gx && j > 1 && j < g.gy && k > 1 && k < g.gz;
@@ -1826,9 +2154,10 @@ __global__ void __launch_bounds__(LIST_NT) k_capture_batch(const void *items, si
 constexpr int RED_NT = 256;
 // Per-block partial sums over interior cells of min(1, fs) (reduce_fs,
 // growth.c:541-566) or of ce.  A warp per interior row at a time: the lanes
-// load the row's 16-byte vectors from element VEC on (rows start on a
-// 64-byte boundary, so these are aligned), and the head (elements 1 ..
-// VEC-1) and tail (after the last whole vector) one element per lane.  Each
+// load the row's 16-byte vectors from interior cell 1 on (the field layout
+// puts cell 1 of every row on a 16-byte boundary; see the stencil's
+// alignment note), and the tail (after the last whole vector) one element
+// per lane.  Each
 // lane adds its values plainly and enters the row's total into its running
 // sum with compensation (TwoSum).  A warp issues every load of a row before
 // adding (four or more 16-byte loads per lane in flight).
@@ -1846,10 +2175,10 @@ __global__ void __launch_bounds__(RED_NT) k_reduce(KernelArgs a, int what, doubl
     const int lane = threadIdx.x & 31;
     const unsigned warp = (blockIdx.x * RED_NT + threadIdx.x) >> 5, nwarps = (gridDim.x * RED_NT) >> 5;
     const int gx = g.gx;
-    const int nfull = max(0, (gx + 1) / VEC - 1);        // vectors covering [VEC, VEC (nfull + 1))
-    const int nhead = min(VEC - 1, gx), tail0 = VEC * (nfull + 1), ntail = max(0, gx - tail0 + 1);
-    // this lane's head or tail element (0: none)
-    const int lone = lane < nhead ? 1 + lane : (lane - nhead < ntail ? tail0 + lane - nhead : 0);
+    const int nfull = gx / VEC;  // vectors covering [1, 1 + VEC nfull)
+    const int tail0 = 1 + VEC * nfull, ntail = gx - VEC * nfull;
+    // this lane's tail element (0: none)
+    const int lone = lane < ntail ? tail0 + lane : 0;
     const unsigned gy = (unsigned)g.gy, gy_m = gy <= 1 ? 0xffffffffu : (unsigned)((1ULL << 32) / gy);
     auto val = [&](Real v) -> double { return (double)((cap && (Real)1 < v) ? (Real)1 : v); };
     double s = 0.0, comp = 0.0;
@@ -1865,7 +2194,7 @@ __global__ void __launch_bounds__(RED_NT) k_reduce(KernelArgs a, int what, doubl
         unsigned jj;
         const unsigned kk = fast_divmod(r, gy, gy_m, jj);
         const Real *row = f + (long long)(kk + 1) * g.sz + (long long)(jj + 1) * g.sy;
-        const V *vrow = (const V *)(row + VEC);
+        const V *vrow = (const V *)(row + 1);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const int p = 128 * c + lane + 32 * k;
@@ -1960,7 +2289,7 @@ __global__ void k_fill_temperature(KernelArgs a, double *out)
     long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (c >= g.N) return;
     long long K = c / g.sz, J = (c % g.sz) / g.sy;
-    out[c] = temp_cell(a.p, a.d.T, c, J, K, ctl->timestep);
+    out[c] = temp_cell(a.p, a.d.T, a.d.T32, c, J, K, ctl->timestep);
 }
 // Zero the entries of cells captured by the last step (list cells whose
 // capture produced a grain id): turns gr into the reference's ogr, and
@@ -2068,11 +2397,18 @@ static EncodeTiledFn encode_fn()
     return fn;
 }
 
-static bool encode3d(CUtensorMap *m, CUtensorMapDataType dt, int es, void *base, const Geo &g, int bx, int by)
+// A field as a 3D tensor map with x extent gx + 2 + lead, starting lead =
+// 16 / es - 1 elements before the field (at the 16-byte boundary the field's
+// allocation keeps there; see the stencil's alignment note).  False when the
+// field is not laid out so, or the encoder refuses.
+static bool encode3d(CUtensorMap *m, CUtensorMapDataType dt, int es, void *field, const Geo &g, int bx, int by)
 {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return false;
-    cuuint64_t dims[3] = {(cuuint64_t)(g.gx + 2), (cuuint64_t)(g.gy + 2), (cuuint64_t)(g.gz + 2)};
+    const int lead = 16 / es - 1;
+    char *base = (char *)field - (long long)lead * es;
+    if (((unsigned long long)base & 15ULL) != 0 || g.P < g.gx + 2 + lead) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)(g.gx + 2 + lead), (cuuint64_t)(g.gy + 2), (cuuint64_t)(g.gz + 2)};
     cuuint64_t strides[2] = {(cuuint64_t)(g.P * es), (cuuint64_t)(g.P * (g.gy + 2) * es)};
     cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
     cuuint32_t estr[3] = {1, 1, 1};
@@ -2096,6 +2432,11 @@ static int make_tma_t(const KernelArgs &a, TmaHolder &out)
     }
     ok &= encode3d(&m.ce, dt, es, a.d.ce, a.g, L::BXC, DTY);
     ok &= encode3d(&m.gr, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, a.d.gr, a.g, L::BXG, DTY);
+    if (CPT == 2 && a.p.temp_mode == 2) {
+        // the pair tile reads the temperature array in pairs too
+        const void *T = sizeof(Real) == 4 ? (const void *)a.d.T32 : (const void *)a.d.T;
+        ok &= T && (((unsigned long long)T + sizeof(Real)) & 15ULL) == 0;
+    }
     std::memcpy(out.bytes, &m, sizeof m);
     out.ok = ok ? 1 : 0;
     if (ok) {
@@ -2390,7 +2731,7 @@ int launch_step(const KernelArgs &a, const TmaHolder &tma, int precision, void *
     return launch_step_t<double>(a, tma, st, start_stage, prof, sumfs);
 }
 
-int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof)
+int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof, int rows)
 {
     cudaStream_t st = (cudaStream_t)stream;
     const Geo &g = a.g;
@@ -2398,18 +2739,20 @@ int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *
     auto grid_of = [&](int tx, int tr) {
         return dim3((unsigned)((g.gx + 2 + tx - 1) / tx), (unsigned)(((long long)(g.gy + 2) * (g.gz + 2) + tr - 1) / tr));
     };
+    int n = 1;
     PROF_BEGIN(KID_TEMP_AM);
     if (precision == MMS_PREC_F32) {
         // tables in FP32; the contraction on the tensor cores (am_tc.cu)
         k_am_tables<float><<<(unsigned)((tab + 255) / 256), 256, 0, st>>>(a, m);
-        launch_am_contract_tc(a, m, st);
+        n += launch_am_contract_tc(a, m, st, rows);
     } else {
         using T = AmTile<double>;
         k_am_tables<double><<<(unsigned)((tab + 255) / 256), 256, 0, st>>>(a, m);
         k_am_contract<double><<<grid_of(T::XL * T::MX, AMC_NT / T::XL * T::MY), AMC_NT, 0, st>>>(a, m);
+        n++;
     }
     PROF_END(KID_TEMP_AM);
-    return 2;
+    return n;
 }
 
 // Folds the per-block (sum, compensation) pairs in a fixed order.

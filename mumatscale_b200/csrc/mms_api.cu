@@ -94,6 +94,10 @@ struct EventProfiler : mms::Profiler {
 struct mms_ctx {
     mms_params p{};
     TmaHolder tma{};
+    // FP32 AM contraction tile rows: 64-128 (a multiple of 16; two
+    // accumulator sets), 256 (one), 0 = the balanced choice up to 128; set by
+    // mms_set_am_tile or mms_autotune
+    int am_rows = 0;
     // one timestep captured as a CUDA graph (kernel arguments only change
     // when sites or orientation overrides are replaced)
     cudaGraphExec_t step_graph = nullptr;
@@ -215,6 +219,22 @@ mms_status dalloc(mms_ctx *ctx, T **ptr, size_t count)
     ctx->allocs.push_back(p);
     ctx->bytes += bytes;
     *ptr = (T *)p;
+    return MMS_OK;
+}
+
+// A field the stencil reads and writes (ce, cl, fs, gr, the AM
+// temperature): allocated with 16 bytes of room in front and placed
+// 16 - es bytes past a 16-byte boundary, so that interior cell 1 of every
+// row is 16-byte aligned (rows are a multiple of 8 elements).  The stencil
+// moves pairs of cells as single words, and its tensor maps start at that
+// boundary.
+template <typename T>
+mms_status dalloc_field(mms_ctx *ctx, T **ptr, size_t count, size_t es = sizeof(T))
+{
+    char *raw = nullptr;
+    mms_status st = dalloc(ctx, &raw, count * es + 16);
+    if (st) return st;
+    *ptr = (T *)(raw + 16 - es);
     return MMS_OK;
 }
 
@@ -511,7 +531,7 @@ int launch_one_step(mms_ctx *ctx, int start_stage, bool sumfs)
     int n = 0;
     const mms_params &p = ctx->p;
     if (start_stage == 0 && p.am) {
-        n += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, ctx->prof);
+        n += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, ctx->prof, ctx->am_rows);
     }
     n += launch_step(ctx->ka, ctx->tma, ctx->prec, ctx->stream, start_stage, ctx->prof, sumfs);
     return n;
@@ -733,6 +753,23 @@ mms_status mms_set_stencil_tile(mms_ctx *ctx, int cells_per_thread, int zchunk)
     return MMS_OK;
 }
 
+mms_status mms_set_am_tile(mms_ctx *ctx, int rows)
+{
+    if (!ctx || !(rows == 0 || rows == 256 || (rows >= 64 && rows <= 128 && rows % 16 == 0))) return MMS_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->am_rows = rows;
+    drop_graph(ctx);
+    return MMS_OK;
+}
+
+mms_status mms_get_am_tile(const mms_ctx *ctx, int *rows)
+{
+    if (!ctx || !rows) return MMS_ERR_ARG;
+    *rows = ctx->am_rows;
+    return MMS_OK;
+}
+
 mms_status mms_get_stencil_tile(const mms_ctx *ctx, int *cells_per_thread, int *zchunk)
 {
     if (!ctx || !cells_per_thread || !zchunk) return MMS_ERR_ARG;
@@ -760,10 +797,13 @@ mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchu
     KernelArgs sa = ctx->ka;
     const int pout = (int)((ctx->h_ctl->timestep + 1) & 1ULL);
     std::vector<void *> shadow;
-    auto shadow_of = [&](const void *src, size_t bytes, void **dst) -> cudaError_t {
-        cudaError_t e = cudaMalloc(dst, bytes);
+    // es > 0: a field, placed as dalloc_field places it (es = its element size)
+    auto shadow_of = [&](const void *src, size_t bytes, void **dst, size_t es = 0) -> cudaError_t {
+        void *raw = nullptr;
+        cudaError_t e = cudaMalloc(&raw, bytes + (es ? 16 : 0));
         if (e != cudaSuccess) return e;
-        shadow.push_back(*dst);
+        shadow.push_back(raw);
+        *dst = es ? (void *)((char *)raw + 16 - es) : raw;
         return cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
     };
     auto release = [&]() {
@@ -772,8 +812,8 @@ mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchu
     };
     void *sce, *scl, *sfs, *sgr, *sbits, *sctl;
     cudaError_t e;
-    if ((e = shadow_of(sa.d.ce, N * rs, &sce)) || (e = shadow_of(sa.d.cl[pout], N * rs, &scl)) ||
-        (e = shadow_of(sa.d.fs[pout], N * rs, &sfs)) || (e = shadow_of(sa.d.gr, N * sizeof(int), &sgr)) ||
+    if ((e = shadow_of(sa.d.ce, N * rs, &sce, rs)) || (e = shadow_of(sa.d.cl[pout], N * rs, &scl, rs)) ||
+        (e = shadow_of(sa.d.fs[pout], N * rs, &sfs, rs)) || (e = shadow_of(sa.d.gr, N * sizeof(int), &sgr, 4)) ||
         (e = shadow_of(sa.d.solid_bits, (size_t)g.nwords * sizeof(unsigned), &sbits)) ||
         (e = shadow_of(sa.d.ctl, sizeof(Ctl), &sctl))) {
         release();
@@ -833,11 +873,60 @@ mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchu
             pick = cd;
         }
     }
+    // FP32 AM form: the contraction's tile (128-row tiles with two
+    // accumulator sets, or 256-row tiles with one), timed with the tables on
+    // shadows of the temperature and the layer flag; the tables are scratch
+    // rebuilt by every step, and are rebuilt for the current step afterwards
+    int am_rows = ctx->am_rows;
+    if (ctx->ka.p.temp_mode == 2 && ctx->prec == MMS_PREC_F32) {
+        void *sT = nullptr, *sls = nullptr;
+        if ((e = shadow_of(sa.d.T32, N * sizeof(float), &sT, 4)) ||
+            (sa.d.lsindex && (e = shadow_of(sa.d.lsindex, N * sizeof(int), &sls)))) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            release();
+            ctx->err = std::string("autotune shadow buffers: ") + cudaGetErrorString(e);
+            return e == cudaErrorMemoryAllocation ? MMS_ERR_NOMEM : MMS_ERR_CUDA;
+        }
+        sa.d.T32 = (float *)sT;
+        if (sls) sa.d.lsindex = (int *)sls;
+        const AmParams m = am_params(ctx->p);
+        double best_am = 1e300;
+        for (int rows : {0, 128, 256}) {
+            std::vector<float> ms;
+            for (int r = 0; r < reps + 2; r++) {
+                cudaEventRecord(e0, ctx->stream);
+                launch_temp_am(sa, m, ctx->prec, ctx->stream, nullptr, rows);
+                cudaEventRecord(e1, ctx->stream);
+                cudaEventSynchronize(e1);
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e0, e1);
+                if (r >= 2) ms.push_back(t);
+            }
+            std::sort(ms.begin(), ms.end());
+            if (ms[ms.size() / 2] < best_am) {
+                best_am = ms[ms.size() / 2];
+                am_rows = rows;
+            }
+        }
+        Ctl c2 = c;
+        c2.timestep = ctx->h_ctl->timestep >= 1 ? ctx->h_ctl->timestep - 1 : 0;
+        cudaMemcpyAsync(sctl, &c2, sizeof c2, cudaMemcpyHostToDevice, ctx->stream);
+        launch_temp_am(sa, m, ctx->prec, ctx->stream, nullptr, am_rows);
+        if ((e = cudaGetLastError()) != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            release();
+            ctx->err = std::string("autotune launch: ") + cudaGetErrorString(e);
+            return MMS_ERR_CUDA;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     release();
     ctx->tma.cpt = pick.cpt;
     ctx->tma.zc = pick.zc;
+    ctx->am_rows = am_rows;
     make_tma(ctx->ka, ctx->prec, ctx->tma);
     drop_graph(ctx);
     if (cells_per_thread) *cells_per_thread = pick.cpt;
@@ -1127,21 +1216,23 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
         return s;
     };
     char *tmp;
-    if ((st = dalloc(ctx, &tmp, N * rs))) return fail(st);
+    if ((st = dalloc_field(ctx, &tmp, N, rs))) return fail(st);
     d.ce = tmp;
     for (int b = 0; b < 2; b++) {
-        if ((st = dalloc(ctx, &tmp, N * rs))) return fail(st);
+        if ((st = dalloc_field(ctx, &tmp, N, rs))) return fail(st);
         d.cl[b] = tmp;
-        if ((st = dalloc(ctx, &tmp, N * rs))) return fail(st);
+        if ((st = dalloc_field(ctx, &tmp, N, rs))) return fail(st);
         d.fs[b] = tmp;
     }
-    if ((st = dalloc(ctx, &d.gr, N)) || (st = dalloc(ctx, &d.dc, N)) || (st = dalloc(ctx, &d.ctl, 1)) ||
+    if ((st = dalloc_field(ctx, &d.gr, N)) || (st = dalloc(ctx, &d.dc, N)) || (st = dalloc(ctx, &d.ctl, 1)) ||
         (st = dalloc(ctx, &d.solid_bits, (size_t)g.nwords)))
         return fail(st);
     if (p.am) {
-        if ((st = dalloc(ctx, &d.T, N))) return fail(st);
+        // the FP32 form keeps the temperature in FP32
+        if ((st = (ctx->prec == MMS_PREC_F32 ? dalloc_field(ctx, &d.T32, N) : dalloc_field(ctx, &d.T, N))))
+            return fail(st);
         if ((st = dalloc(ctx, &d.am_tab, (size_t)400 * (g.gx + g.gy + g.gz + 6) + (size_t)(g.gz + 2)))) return fail(st);
-        if (ctx->prec == MMS_PREC_F32 && (st = dalloc(ctx, &d.am_ximg, (size_t)am_ximg_size(g.gx)))) return fail(st);
+        if (ctx->prec == MMS_PREC_F32 && (st = dalloc(ctx, &d.am_ximg, (size_t)am_ximg_size(g.gx, g.gy, g.gz)))) return fail(st);
         if (p.amlayer > 1 && (st = dalloc(ctx, &d.lsindex, N))) return fail(st);
     }
     if (p.tip_curv && (st = dalloc(ctx, &d.curv, N))) return fail(st);
@@ -1196,7 +1287,7 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
     if (p.am && ctx->prec == MMS_PREC_F32) am_tc_prepare();
     if (p.am && p.amlayer > 1) {
         // tempPrepareSB_int lsindex (temperature.c:183-189) at timestep 0
-        ctx->launches += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, nullptr);
+        ctx->launches += launch_temp_am(ctx->ka, am_params(p), ctx->prec, ctx->stream, nullptr, ctx->am_rows);
     }
     std::vector<float> thr;  // whole domain, reference layout (host site setup)
     if (p.site_setup == 1) {
@@ -1657,6 +1748,10 @@ mms_status mms_download(mms_ctx *ctx, mms_field field, void *host)
             ctx->launches += launch_mask_captured(ctx->ka, tmp, 1, ctx->stream);
         } else {
             ctx->launches += launch_fill_temperature(ctx->ka, tmp, ctx->stream);
+            // FP32 AM form: the halo columns, which no kernel of a step reads,
+            // from the tables of the current step
+            if (ctx->ka.p.temp_mode == 2 && ctx->prec == MMS_PREC_F32)
+                ctx->launches += launch_am_halo_fill(ctx->ka, am_params(ctx->p), tmp, ctx->stream);
         }
         CU(copy_out(ctx, host, tmp, sizeof(double)));
         dfree(ctx, tmp);
@@ -2300,7 +2395,7 @@ int batch_launch_step(mms_batch *b)
     // fn(ctx, nullptr) asks whether the domain has such work
     branches([&](mms_ctx *ctx, cudaStream_t s) -> int {
         if (!ctx->p.am) return 0;
-        return s ? launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, s, nullptr) : 1;
+        return s ? launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, s, nullptr, ctx->am_rows) : 1;
     });
     const int *bg = b->begin;
     n += launch_small_batch(0, b->items, bg, nd, b->totals[0], b->prec, b->stream);
@@ -2521,17 +2616,19 @@ mms_status mms_batch_autotune(mms_batch *b, int reps, int *cells_per_thread, int
         const size_t N = (size_t)g.N, rs = ctx->prec == MMS_PREC_F32 ? sizeof(float) : sizeof(double);
         KernelArgs sa = ctx->ka;
         const int pout = (int)((ctx->h_ctl->timestep + 1) & 1ULL);
-        auto sh = [&](const void *src, size_t bytes) -> void * {
-            void *d = nullptr;
-            if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
-            shadow.push_back(d);
+        // es > 0: a field, placed as dalloc_field places it
+        auto sh = [&](const void *src, size_t bytes, size_t es = 0) -> void * {
+            void *raw = nullptr;
+            if (cudaMalloc(&raw, bytes + (es ? 16 : 0)) != cudaSuccess) return nullptr;
+            shadow.push_back(raw);
+            void *d = es ? (void *)((char *)raw + 16 - es) : raw;
             cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, b->stream);
             return d;
         };
-        sa.d.ce = sh(sa.d.ce, N * rs);
-        sa.d.cl[pout] = sh(sa.d.cl[pout], N * rs);
-        sa.d.fs[pout] = sh(sa.d.fs[pout], N * rs);
-        sa.d.gr = (int *)sh(sa.d.gr, N * sizeof(int));
+        sa.d.ce = sh(sa.d.ce, N * rs, rs);
+        sa.d.cl[pout] = sh(sa.d.cl[pout], N * rs, rs);
+        sa.d.fs[pout] = sh(sa.d.fs[pout], N * rs, rs);
+        sa.d.gr = (int *)sh(sa.d.gr, N * sizeof(int), 4);
         sa.d.solid_bits = (unsigned *)sh(sa.d.solid_bits, (size_t)g.nwords * sizeof(unsigned));
         sa.d.ctl = (Ctl *)sh(sa.d.ctl, sizeof(Ctl));
         if (!sa.d.ce || !sa.d.cl[pout] || !sa.d.fs[pout] || !sa.d.gr || !sa.d.solid_bits || !sa.d.ctl) {
@@ -2905,7 +3002,7 @@ mms_status slab_launch(mms_ctx *ctx, int phase, int resume)
     cudaSetDevice(ctx->device);
     ctx->ctl_known = ctx->fs_part_valid = false;
     if (phase == 0 && !resume && ctx->p.am)
-        ctx->launches += launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, ctx->stream, nullptr);
+        ctx->launches += launch_temp_am(ctx->ka, am_params(ctx->p), ctx->prec, ctx->stream, nullptr, ctx->am_rows);
     ctx->launches += launch_slab_phase(ctx->ka, ctx->tma, ctx->prec, ctx->stream, phase, resume);
     CU(cudaGetLastError());
     return MMS_OK;

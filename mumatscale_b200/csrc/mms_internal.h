@@ -158,10 +158,12 @@ struct DevPtrs {
     int *gr;
     Dc3 *dc;
     unsigned *solid_bits;  // gr > 0 after fs_change (written by the stencil)
-    double *T;            // AM temperature at the current step (N) or null
+    double *T;            // AM temperature at the current step (N), FP64 form, or null
+    float *T32;           // the same in the FP32 form (N), or null
     double *am_tab;       // AM quadrature tables (400 x (gx+gy+gz+6)) and plane flags
     float *am_ximg;       // FP32 form: the X table split into TF32 head and remainder in the
-                          // tensor core's operand layout (am_tc.cu), or null
+                          // tensor core's operand layout, then the Y and Z tables with the
+                          // nodes contiguous (am_tc.cu), or null
     int *lsindex;         // AM layer flag or null
     double *curv;         // curvature (N) when TipCurvature
     // nucleation sites, sorted by (emulated rank, local raster)
@@ -301,13 +303,20 @@ struct AmParams {
     double lsd, lv, lhs, lab, lpow, liniT, lthcon, rho_cp, x0, y0, z0;
     int amtracks, nsbx_times_sbx;
 };
-// FP32 AM contraction on the tensor cores (am_tc.cu)
-int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream);
+// FP32 AM contraction on the tensor cores (am_tc.cu): tiles of 128 x cells
+// by `rows` (y, z) rows: 64-128 (two accumulator sets), 256 (one), or 0 =
+// the multiple of 16 up to 128 that balances the tiles over the SMs.  The halo columns x = 0 and
+// gx + 1 are filled only where they are read: launch_am_halo_fill writes
+// them into a temperature download buffer from the tables of the current
+// step (they are computed every step when the layer flag lsindex is kept).
+int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, int rows);
+int launch_am_halo_fill(const KernelArgs &a, const AmParams &m, double *dev_out, void *stream);
 int am_tc_prepare();
-long long am_ximg_size(int gx);  // floats of a.d.am_ximg
+long long am_ximg_size(int gx, int gy, int gz);  // floats of a.d.am_ximg
 // Temperature of the next step for the AM model (tables + contraction);
-// FP32 tables and sums in the FP32 form.
-int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof);
+// FP32 tables and sums in the FP32 form (`rows`: its contraction's tile).
+int launch_temp_am(const KernelArgs &a, const AmParams &m, int precision, void *stream, Profiler *prof,
+                   int rows = 0);
 constexpr int RED_BLOCKS = 148 * 8;  // partial sums of k_reduce (red holds 2 per block + 1)
 int launch_reduce(const KernelArgs &a, int precision, int what, double *host_out, void *stream, double *pinned);
 // The TMA stencil launched with sumfs leaves each tile's sum of the new

@@ -91,6 +91,43 @@ def test_am_fp32_form_error(built, cuda_device):
             assert rel < 1e-5, rel
 
 
+def test_am_fp32_form_cfg3_shape(built, cuda_device):
+    """The FP32 form on the reduced melt-pool deck amsub4 (the AM source
+    crossing a columnar substrate with bulk nucleation, 4 emulated ranks)
+    against the FP64 plain form, which is pinned to the reference's dumps
+    (test_fp64_bit_exact_vs_reference) and to the oracle within tolerance
+    (test_am_tolerance), at the bounds stated for the AM melt-pool workload:
+    grain-id mismatch < 0.1 % of cells and solute (ce) relative L2 error
+    < 1e-5, plus temperature max error < 1e-6 of its maximum and fs max
+    error < 1e-3.  The laser turns on at step 8 and crosses the domain by
+    step 30; the run goes on to step 200 as the pool solidifies."""
+    p = M.read_deck(golden_deck("amsub4"))
+    doms = {prec: M.Domain(p, precision=prec) for prec in (M.PREC_F64, M.PREC_F32)}
+    try:
+        for d in doms.values():
+            setup_golden_substrate(d, "amsub4")
+        d64, d32 = doms[M.PREC_F64], doms[M.PREC_F32]
+        for s in (20, 30, 60, 120, 200):
+            for d in doms.values():
+                d.step(s - d.timestep)
+            T, T0 = d32.download("temperature"), d64.download("temperature")
+            terr = float(np.abs(T - T0).max() / np.abs(T0).max())
+            gr, gr0 = d32.download("gr")[1:-1, 1:-1, 1:-1], d64.download("gr")[1:-1, 1:-1, 1:-1]
+            mism = float((gr != gr0).mean())
+            ce, ce0 = d32.download("ce"), d64.download("ce")
+            rel = float(np.linalg.norm(ce - ce0) / np.linalg.norm(ce0))
+            fs_err = float(np.abs(d32.download("fs") - d64.download("fs")).max())
+            msg = f"step {s}: T {terr:.3g}, grain ids {mism:.3g}, ce L2 {rel:.3g}, fs {fs_err:.3g}"
+            assert d32.num_grains == d64.num_grains, msg
+            assert terr < 1e-6, msg
+            assert mism < 1e-3, msg
+            assert rel < 1e-5, msg
+            assert fs_err < 1e-3, msg
+    finally:
+        for d in doms.values():
+            d.close()
+
+
 @pytest.mark.parametrize("name", ["small1", "small4", "grad1"])
 def test_fp64_matches_oracle_every_step(built, cuda_device, name):
     """Step-by-step equality for the first 150 steps (catches transient
