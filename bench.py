@@ -68,8 +68,9 @@ DT = 0.04 * DX * DX / 3e-9
 BYTES_DIFFUSE = {"f64": 3 * 8 * 2 + 4, "f32": 3 * 4 * 2 + 4}
 # full-step dense bytes per cell-update (ce, cl, fs read+write, gr, threshold)
 BYTES_STEP = {"f64": 56, "f32": 32}
-# the AM deck's stencil also reads the temperature field (FP64)
-BYTES_DIFFUSE_AM = {k: v + 8 for k, v in BYTES_DIFFUSE.items()}
+# the AM deck's stencil also reads the temperature field (FP64 in the FP64
+# form, FP32 in the FP32 form)
+BYTES_DIFFUSE_AM = {"f64": BYTES_DIFFUSE["f64"] + 8, "f32": BYTES_DIFFUSE["f32"] + 4}
 
 # AM melt-pool deck (the default workload)
 AM_DIMS = (512, 256, 128)
@@ -592,14 +593,19 @@ def _roofline(ks: dict, steps: int, cells: int, form: str, peaks: dict) -> dict:
     ms, n = ks[name]
     per_launch = ms / 1e3 / max(n, 1)
     if name == "k_temp_am":
-        # tables + contraction per step: 2 x 400 multiply-adds per halo'd cell
-        # (algorithmic; the TF32 x 3 form issues three MMAs per product)
-        halo = (AM_DIMS[0] + 2) * (AM_DIMS[1] + 2) * (AM_DIMS[2] + 2)
-        flops = 2.0 * 400 * halo
+        # tables + contraction per step: 2 x 400 multiply-adds per cell the
+        # step computes (x = 1..gx of every halo'd (y, z) row; the halo
+        # columns are filled only where read).  Algorithmic: the FP32 form
+        # issues three TF32 products per multiply-add (head x head, head x
+        # remainder, remainder x head), and TF32 runs at half the bf16 rate,
+        # so its tensor-core bound is peak / 6 in these units
+        cells_t = AM_DIMS[0] * (AM_DIMS[1] + 2) * (AM_DIMS[2] + 2)
+        flops = 2.0 * 400 * cells_t
         ach = flops / per_launch / 1e12
         pk = peaks["bf16_tflops"]
         return {"bound": "tensor", "kernel": name, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
-                "frac": ach / pk, "peak_source": peaks["source"] + " (dense bf16 GEMM; TF32 runs at half its rate)",
+                "frac": ach / pk, "frac_of_tf32x3_bound": ach / (pk / 6.0),
+                "peak_source": peaks["source"] + " (dense bf16 GEMM)",
                 "algorithmic_flops_per_launch": flops, "traffic": None,
                 "kernel_ms_per_launch": per_launch * 1e3}
     b = BYTES_DIFFUSE_AM[form] if name == "k_diffuse_fs" else BYTES_STEP[form]

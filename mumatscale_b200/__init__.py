@@ -388,7 +388,7 @@ class Domain:
         return cpt.value, zc.value
 
     def set_am_tile(self, rows: int) -> None:
-        """FP32 AM contraction tile rows: 64-128 (multiple of 16), 256, or 0 = balanced."""
+        """FP32 AM contraction tile rows: 64-128 (multiple of 16), 256, or 0 = the default (128)."""
         _check(_lib().mms_set_am_tile(self._ctx, rows), "mms_set_am_tile", self._ctx)
 
     def am_tile(self) -> int:

@@ -28,10 +28,12 @@
 //                head and remainder and laid out as the tensor core reads it)
 //   warp 1       the MMAs (one thread), committed to mbarriers
 //   warps 2-5    B: the rows' YZ products, split and stored into shared memory
-//   warps 6-9    epilogue: tcgen05.ld of both accumulators, T (kept in FP32
-//                in this form) and the layer flag to global memory
+//   warps 6-13   epilogue: tcgen05.ld of both accumulators, T (kept in FP32
+//                in this form) and the layer flag to global memory; two
+//                warps per group of 32 tensor-memory lanes, each taking every
+//                other 16 columns
 // Stages of 16 nodes (A 16 KB, B 16 or 32 KB) circulate in a shared-memory
-// ring.  With N = 128 the 512 tensor-memory columns hold two sets of
+// ring of seven (N = 128) or four (N = 256).  With N = 128 the 512 tensor-memory columns hold two sets of
 // accumulators, so a tile's epilogue runs while the next tile accumulates;
 // with N = 256 one set fills them.
 //
@@ -58,15 +60,16 @@ constexpr int TC_KS = TC_KC / 8;         // MMA K-steps per stage
 constexpr int TC_NCH = AM_NT / TC_KC;    // stages per tile
 constexpr int TC_A_KS = TC_M * 8 * 4;    // one K-step, one part (head or remainder) of A
 constexpr int TC_A = TC_KS * 2 * TC_A_KS;
-constexpr int TC_NT = 320;
+constexpr int TC_NT = 448;
 constexpr int TC_PROD0 = 64, TC_EPI0 = 192;  // first thread of the producers / epilogue
+constexpr int TC_NEPI = TC_NT - TC_EPI0;     // epilogue threads (eight warps)
 static_assert(AM_NT % TC_KC == 0, "nodes per stage");
 
 template <int NB>
 struct TcCfg {
     static constexpr int B_KS = NB * 8 * 4;                 // one K-step, one part of B
     static constexpr int STAGE = TC_A + TC_KS * 2 * B_KS;   // 32 KB (N = 128) or 48 KB (N = 256)
-    static constexpr int S = NB == 128 ? 6 : 4;             // stages in the ring
+    static constexpr int S = NB == 128 ? 7 : 4;             // stages in the ring
     static constexpr int SMEM = S * STAGE + 128;            // + alignment of the ring
     static constexpr int BUFS = NB == 128 ? 2 : 1;          // accumulator sets (2 NB columns each)
     static constexpr int RPT = NB / 128;                    // B rows per producer thread
@@ -160,7 +163,7 @@ __device__ __forceinline__ void tf32_split(float v, float &hi, float &lo)
 
 static_assert(TC_M == 128, "am_ximg_part lays the X image out in 128-cell tiles");
 
-// 32 consecutive tensor-memory columns of this warp's 32 lanes
+// 16 consecutive tensor-memory columns of this warp's 32 lanes
 __device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&v)[16])
 {
     asm volatile(
@@ -169,6 +172,20 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&v)[16])
         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
           "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
         : "r"(taddr));
+}
+
+// Waits for this thread's tcgen05.ld in flight; the registers they fill are
+// operands, so that no use of them is scheduled before the wait.
+__device__ __forceinline__ void tmem_wait_ld(unsigned (&a)[16], unsigned (&b)[16])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7]),
+                   "+r"(a[8]), "+r"(a[9]), "+r"(a[10]), "+r"(a[11]), "+r"(a[12]), "+r"(a[13]), "+r"(a[14]),
+                   "+r"(a[15]), "+r"(b[0]), "+r"(b[1]), "+r"(b[2]), "+r"(b[3]), "+r"(b[4]), "+r"(b[5]), "+r"(b[6]),
+                   "+r"(b[7]), "+r"(b[8]), "+r"(b[9]), "+r"(b[10]), "+r"(b[11]), "+r"(b[12]), "+r"(b[13]),
+                   "+r"(b[14]), "+r"(b[15])
+                 :
+                 : "memory");
 }
 
 template <int NB>
@@ -211,7 +228,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
         }
         for (int b = 0; b < 2; b++) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&accf[b])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_addr(&acce[b])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&acce[b])), "r"(TC_NEPI)
+                         : "memory");
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_abort = 0;
@@ -300,7 +318,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
         // ZT[K][i]: a row's 16 nodes are four 16-byte loads, and CTAs working
         // on different rows read different lines (node-major tables made
         // every SM read the same few lines at the same moment).  The next
-        // stage's loads are in flight while this stage is split and stored.
+        // stage's loads (across tiles too) are in flight while this stage is
+        // split and stored.
         const int pr = tid - TC_PROD0;
         const float *__restrict__ YT = am_yt(a.d.am_ximg, g.gx);
         const float *__restrict__ ZT = am_zt(a.d.am_ximg, g.gx, g.gy);
@@ -320,7 +339,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
                     nz4[h][k] = on[h] ? __ldg(zrow[h] + i0 / 4 + k) : zero4;
                 }
         };
-        for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        // this thread's rows of tile t
+        auto rows_of = [&](long long t) {
             const long long r0 = (t / ntx) * (long long)N;
 #pragma unroll
             for (int h = 0; h < C::RPT; h++) {
@@ -331,7 +351,12 @@ __global__ void __launch_bounds__(TC_NT, 1)
                 yrow[h] = (const float4 *)(YT + (long long)J * AM_NT);
                 zrow[h] = (const float4 *)(ZT + (long long)K * AM_NT);
             }
+        };
+        if (blockIdx.x < ntiles) {
+            rows_of(blockIdx.x);
             fetch(0);
+        }
+        for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
             for (int c = 0; c < TC_NCH; c++, q++) {
                 const int s = (int)(q % S);
                 float v[C::RPT][TC_KC];
@@ -344,7 +369,13 @@ __global__ void __launch_bounds__(TC_NT, 1)
                         v[h][4 * k + 2] = ny4[h][k].z * nz4[h][k].z;
                         v[h][4 * k + 3] = ny4[h][k].w * nz4[h][k].w;
                     }
-                if (c + 1 < TC_NCH) fetch(c + 1);
+                if (c + 1 < TC_NCH) {
+                    fetch(c + 1);
+                } else if (t + gridDim.x < ntiles) {
+                    // the next tile's first stage (v already holds this one's)
+                    rows_of(t + gridDim.x);
+                    fetch(0);
+                }
                 if (q >= S && !tc_wait(&empty[s], (unsigned)((q / S - 1) & 1), abort)) {
                     ok = false;
                     break;
@@ -373,7 +404,10 @@ __global__ void __launch_bounds__(TC_NT, 1)
         }
     } else {
         // ---- epilogue: warp w reads tensor-memory lanes 32 (w mod 4) .. + 31
-        const int qd = warp & 3;
+        // (its 32 x cells); of each tile's 16-column chunks (rows), warps
+        // 6-9 take the even ones and warps 10-13 the odd ones, loading the
+        // next chunk while the current one is stored
+        const int qd = warp & 3, hf = (warp - TC_EPI0 / 32) >> 2;
         const int xl = 32 * qd + lane;
         const AmStep st = am_step(p, m, ctl->timestep + 1);
         long long tl = 0;
@@ -388,16 +422,13 @@ __global__ void __launch_bounds__(TC_NT, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int x = 1 + TC_M * xt + xl;
             const bool xin = x <= g.gx;
-            long long R = r0;
-            int K = (int)(R / ny), J = (int)(R - (long long)K * ny);
-            long long cell = (long long)K * g.sz + (long long)J * g.sy + x;
-            bool on = zon[K] != 0;
-            const unsigned lanes = (unsigned)(32 * qd) << 16;
-            for (int cc = 0; cc < N; cc += 16) {
-                unsigned vh[16], vx[16];
-                tmem_ld16(tmem + lanes + (unsigned)(b * 2 * NB + cc), vh);
-                tmem_ld16(tmem + lanes + (unsigned)(b * 2 * NB + NB + cc), vx);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const unsigned col = tmem + ((unsigned)(32 * qd) << 16) + (unsigned)(b * 2 * NB);
+            // T of rows r0 + cc .. + 15 from the chunk's two accumulators
+            auto store16 = [&](int cc, const unsigned (&vh)[16], const unsigned (&vx)[16]) {
+                long long R = r0 + cc;
+                int K = (int)(R / ny), J = (int)(R - (long long)K * ny);
+                long long cell = (long long)K * g.sz + (long long)J * g.sy + x;
+                bool on = zon[K] != 0;
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
                     if (xin && R < nrows) {
@@ -416,6 +447,31 @@ __global__ void __launch_bounds__(TC_NT, 1)
                         on = K < nz && zon[K] != 0;
                     }
                 }
+            };
+            unsigned ha[16], xa[16], hb[16], xb[16];
+            int cc = 16 * hf;
+            if (cc < N) {
+                tmem_ld16(col + (unsigned)cc, ha);
+                tmem_ld16(col + (unsigned)(NB + cc), xa);
+            }
+            tmem_wait_ld(ha, xa);
+            while (cc < N) {
+                const int c1 = cc + 32;
+                if (c1 < N) {
+                    tmem_ld16(col + (unsigned)c1, hb);
+                    tmem_ld16(col + (unsigned)(NB + c1), xb);
+                }
+                store16(cc, ha, xa);
+                tmem_wait_ld(hb, xb);
+                if (c1 >= N) break;
+                const int c2 = c1 + 32;
+                if (c2 < N) {
+                    tmem_ld16(col + (unsigned)c2, ha);
+                    tmem_ld16(col + (unsigned)(NB + c2), xa);
+                }
+                store16(c1, hb, xb);
+                tmem_wait_ld(ha, xa);
+                cc = c2;
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             tc_arrive(&acce[b]);
@@ -474,24 +530,6 @@ __global__ void __launch_bounds__(256) k_am_halo(KernelArgs a, AmParams m, doubl
     }
 }
 
-// Rows per tile for N = 128 tiles: the multiple of 16 (64 .. 128) whose
-// tiles, dealt to one persistent CTA per SM, leave the fewest rows on the
-// busiest CTA (ties: the larger tile, which reads the A image fewer times).
-static int tc_rows_per_tile(long long nrows, int ntx, int nsm, int nmax, int nmin)
-{
-    int best = nmax;
-    long long best_load = -1;
-    for (int n = nmax; n >= nmin; n -= 16) {
-        const long long tiles = ntx * ((nrows + n - 1) / n);
-        const long long load = ((tiles + nsm - 1) / nsm) * n;
-        if (best_load < 0 || load < best_load) {
-            best_load = load;
-            best = n;
-        }
-    }
-    return best;
-}
-
 static int sm_count()
 {
     static int n = [] {
@@ -517,8 +555,12 @@ int am_tc_prepare()
 
 long long am_ximg_size(int gx, int gy, int gz) { return am_ximg_part(gx) + (long long)(gy + gz + 4) * AM_NT; }
 
-// rows: 256-row tiles (one accumulator set), 64-128 rows (two), 0 = the
-// balanced choice up to 128
+// rows: 256-row tiles (one accumulator set), 64-128 rows (two), 0 = 128.
+// A tile's cost is mostly per stage (its A copy, its MMAs' fixed costs), so
+// the largest tile with two accumulator sets is the default even where
+// smaller tiles would deal more evenly over the SMs (measured at
+// 512 x 256 x 128: 128 rows 0.160 ms, 112 0.175, 96 0.182, 64 0.250, 256
+// 0.228, tables included).
 int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, int rows)
 {
     const Geo &g = a.g;
@@ -526,7 +568,7 @@ int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, 
     const long long nrows = (long long)(g.gy + 2) * (g.gz + 2);
     const int nsm = sm_count();
     const bool wide = rows == 256;
-    const int N = wide ? 256 : (rows >= 64 && rows <= 128 ? rows / 16 * 16 : tc_rows_per_tile(nrows, ntx, nsm, 128, 64));
+    const int N = wide ? 256 : (rows >= 64 && rows <= 128 ? rows / 16 * 16 : 128);
     const long long ntiles = (long long)ntx * ((nrows + N - 1) / N);
     const unsigned grid = (unsigned)(ntiles < nsm ? ntiles : nsm);
     cudaStream_t st = (cudaStream_t)stream;

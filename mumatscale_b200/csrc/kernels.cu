@@ -1323,26 +1323,28 @@ __device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const Tma
     bool alive = true;
     double fsum = 0.0;  // this thread's new fs values, in plane order
     // AM temperature array (FP32 in the FP32 form): the pair's values are
-    // loaded one plane ahead, so that their latency overlaps a plane of work
+    // loaded two planes ahead, so that their latency overlaps two planes of
+    // work
     const bool t_arr = p.temp_mode == 2;
-    auto t_load = [&](long long c, double &t0, double &t1) {
+    auto t_load = [&](long long c) -> V {
         if (sizeof(Real) == 4) {
             const float2 v = __ldg((const float2 *)(a.d.T32 + c));
-            t0 = v.x;
-            t1 = v.y;
-        } else {
-            const double2 v = __ldg((const double2 *)(a.d.T + c));
-            t0 = v.x;
-            t1 = v.y;
+            return vec2<Real>((Real)v.x, (Real)v.y);
         }
+        const double2 v = __ldg((const double2 *)(a.d.T + c));
+        return vec2<Real>((Real)v.x, (Real)v.y);
     };
-    double Tn0 = 0.0, Tn1 = 0.0;
-    if (t_arr && act0) t_load(crow + i, Tn0, Tn1);
+    V Tn = vec2<Real>(0, 0), Tnn = Tn;
+    if (t_arr && act0) {
+        Tn = t_load(crow + i);
+        if (k1 > k0) Tnn = t_load(crow + g.sz + i);
+    }
     V zm_cl = vec2<Real>(0, 0), zc_cl = zm_cl, zm_fs = zm_cl, zc_fs = zm_cl;
     for (int t = 0; t <= k1 - k0; t++) {
         const int k = k0 + t;
-        const double T0 = Tn0, T1 = Tn1;
-        if (t_arr && act0 && t < k1 - k0) t_load(crow + g.sz + i, Tn0, Tn1);
+        const double T0 = (double)Tn.x, T1 = (double)Tn.y;
+        Tn = Tnn;
+        if (t_arr && act0 && t + 1 < k1 - k0) Tnn = t_load(crow + 2 * g.sz + i);
         // planes t and t+1 completed in earlier iterations
         bool ok = mbar_wait(&bars[s2], ph2);
         if (t == 0) ok &= mbar_wait(&bars[s0], phase(0)) && mbar_wait(&bars[s1], phase(1));
@@ -1494,16 +1496,19 @@ __device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const Tma
     return alive;
 }
 
-// The tile of either width.
+// The tile of either width.  Two cells per thread: adjacent pairs in the FP32
+// form; in the FP64 form two cells 32 apart (stencil_tile), whose scalar
+// loads keep the register count within three CTAs per SM (the FP64 pair tile
+// needs two CTAs' budget and measured slower, 4.67 vs 4.82 TB/s at 256^3).
 template <typename Real, int CPT>
 __device__ __forceinline__ bool run_tile(const KernelArgs &a, const TmaMaps &maps, int zchunk, int bx, int by, int bz,
                                          unsigned char *smem, StencilShared<Depth<Real, CPT>::TS> &sh, unsigned &ring,
                                          double *part = nullptr, long long part_idx = 0)
 {
-    if constexpr (CPT == 2)
+    if constexpr (CPT == 2 && sizeof(Real) == 4)
         return stencil_tile_pair<Real>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
     else
-        return stencil_tile<Real, 1>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
+        return stencil_tile<Real, CPT>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
 }
 
 // SUMFS: each tile also leaves its sum of the new fraction solid in

@@ -95,8 +95,8 @@ struct mms_ctx {
     mms_params p{};
     TmaHolder tma{};
     // FP32 AM contraction tile rows: 64-128 (a multiple of 16; two
-    // accumulator sets), 256 (one), 0 = the balanced choice up to 128; set by
-    // mms_set_am_tile or mms_autotune
+    // accumulator sets), 256 (one), 0 = 128; set by mms_set_am_tile or
+    // mms_autotune
     int am_rows = 0;
     // one timestep captured as a CUDA graph (kernel arguments only change
     // when sites or orientation overrides are replaced)
@@ -198,7 +198,7 @@ namespace {
     } while (0)
 
 template <typename T>
-mms_status dalloc(mms_ctx *ctx, T **ptr, size_t count)
+mms_status dalloc(mms_ctx *ctx, T **ptr, size_t count, bool zero = true)
 {
     void *p = nullptr;
     size_t bytes = sizeof(T) * (count ? count : 1);
@@ -206,6 +206,12 @@ mms_status dalloc(mms_ctx *ctx, T **ptr, size_t count)
     if (e != cudaSuccess) {
         ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
         return MMS_ERR_NOMEM;
+    }
+    if (!zero) {
+        ctx->allocs.push_back(p);
+        ctx->bytes += bytes;
+        *ptr = (T *)p;
+        return MMS_OK;
     }
     // zeroed before returning: later host copies into this buffer go through
     // the legacy default stream, which does not wait for ctx->stream
@@ -526,6 +532,17 @@ mms_status ensure_graph(mms_ctx *ctx)
     return MMS_OK;
 }
 
+// The step graphs captured ahead of the first step (at creation and after a
+// tile change), so that the first stepping call does not pay for the
+// capture; a failure here leaves them to be captured by that call.
+void prepare_graphs(mms_ctx *ctx)
+{
+    if (ensure_graph(ctx) != MMS_OK) {
+        ctx->err.clear();
+        cudaGetLastError();
+    }
+}
+
 int launch_one_step(mms_ctx *ctx, int start_stage, bool sumfs)
 {
     int n = 0;
@@ -628,7 +645,9 @@ mms_status sync_grains(mms_ctx *ctx)
     return MMS_OK;
 }
 
-// staging buffer of one whole field in the reference layout (grown on demand)
+// staging buffer of one whole field in the reference layout: an FP64 field's
+// size from creation on, grown (never shrunk) for wider fields (dc); its
+// contents are always written before they are read, so it is not cleared
 void *stage_buffer(mms_ctx *ctx, size_t bytes)
 {
     if (ctx->stage_bytes < bytes) {
@@ -636,7 +655,7 @@ void *stage_buffer(mms_ctx *ctx, size_t bytes)
         ctx->stage = nullptr;
         ctx->stage_bytes = 0;
         char *p = nullptr;
-        if (dalloc(ctx, &p, bytes) != MMS_OK) return nullptr;
+        if (dalloc(ctx, &p, bytes, false) != MMS_OK) return nullptr;
         ctx->stage = p;
         ctx->stage_bytes = bytes;
     }
@@ -750,6 +769,7 @@ mms_status mms_set_stencil_tile(mms_ctx *ctx, int cells_per_thread, int zchunk)
     make_tma(ctx->ka, ctx->prec, ctx->tma);
     drop_graph(ctx);
     ctx->fs_part_valid = false;
+    if (ctx->nslabs == 1) prepare_graphs(ctx);
     return MMS_OK;
 }
 
@@ -760,6 +780,7 @@ mms_status mms_set_am_tile(mms_ctx *ctx, int rows)
     CU(cudaStreamSynchronize(ctx->stream));
     ctx->am_rows = rows;
     drop_graph(ctx);
+    if (ctx->nslabs == 1) prepare_graphs(ctx);
     return MMS_OK;
 }
 
@@ -892,7 +913,7 @@ mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchu
         if (sls) sa.d.lsindex = (int *)sls;
         const AmParams m = am_params(ctx->p);
         double best_am = 1e300;
-        for (int rows : {0, 128, 256}) {
+        for (int rows : {0, 256}) {
             std::vector<float> ms;
             for (int r = 0; r < reps + 2; r++) {
                 cudaEventRecord(e0, ctx->stream);
@@ -929,6 +950,7 @@ mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchu
     ctx->am_rows = am_rows;
     make_tma(ctx->ka, ctx->prec, ctx->tma);
     drop_graph(ctx);
+    if (ctx->nslabs == 1) prepare_graphs(ctx);
     if (cells_per_thread) *cells_per_thread = pick.cpt;
     if (zchunk) *zchunk = pick.zc;
     if (best_ms) *best_ms = best;
@@ -1327,8 +1349,12 @@ mms_status create_ctx(const mms_params *pin, int nslabs, int slab, mms_ctx **out
     }
     ctx->grains.resize(1);
     std::memset(&ctx->grains[0], 0, sizeof(mms_grain));
+    // the host-copy staging buffer for FP64 fields, so the first uploads
+    // and downloads do not allocate
+    if (!stage_buffer(ctx, (size_t)g.rN * sizeof(double))) return fail(MMS_ERR_NOMEM);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(MMS_ERR_CUDA);
     if (cudaGetLastError() != cudaSuccess) return fail(MMS_ERR_CUDA);
+    if (nslabs == 1) prepare_graphs(ctx);
     *out = ctx;
     return MMS_OK;
 }

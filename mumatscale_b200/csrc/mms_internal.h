@@ -305,7 +305,7 @@ struct AmParams {
 };
 // FP32 AM contraction on the tensor cores (am_tc.cu): tiles of 128 x cells
 // by `rows` (y, z) rows: 64-128 (two accumulator sets), 256 (one), or 0 =
-// the multiple of 16 up to 128 that balances the tiles over the SMs.  The halo columns x = 0 and
+// 128.  The halo columns x = 0 and
 // gx + 1 are filled only where they are read: launch_am_halo_fill writes
 // them into a temperature download buffer from the tables of the current
 // step (they are computed every step when the layer flag lsindex is kept).
