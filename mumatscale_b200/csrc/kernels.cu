@@ -159,9 +159,10 @@ __global__ void k_am_tables(KernelArgs a, AmParams m)
     const int nx = g.gx + 2, ny = g.gy + 2, nz = g.gz + 2, nc = nx + ny + nz;
     Real *X = (Real *)a.d.am_tab, *Y = X + (long long)AM_NT * nx, *Z = Y + (long long)AM_NT * ny;
     int *zon = (int *)(Z + (long long)AM_NT * nz);
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)AM_NT * nc;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(e / nc), q = (int)(e % nc);
+    // fewer than 2^31 table entries (400 per halo'd row or column): 32-bit
+    // indices and division
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < (unsigned)(AM_NT * nc); e += gridDim.x * blockDim.x) {
+        const int i = (int)(e / (unsigned)nc), q = (int)(e - (unsigned)i * (unsigned)nc);
         const double lt = (0.5 + i) * s.ldt;
         const double ai = s.ls * s.ls + 4. * s.lalpha * lt;
         if (q < nx) {
