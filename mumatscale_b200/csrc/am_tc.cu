@@ -47,6 +47,7 @@
 // drains what it has in flight (bulk copies, committed MMAs) before the
 // tensor memory is freed.
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "device_common.cuh"
@@ -55,10 +56,11 @@
 namespace mms {
 
 constexpr int TC_M = 128;                // x cells per tile (MMA M)
+constexpr int TC_KE = 16;                // nodes per MMA K-step (FP16 operands)
 constexpr int TC_KC = 16;                // nodes per stage
-constexpr int TC_KS = TC_KC / 8;         // MMA K-steps per stage
+constexpr int TC_KS = TC_KC / TC_KE;     // MMA K-steps per stage
 constexpr int TC_NCH = AM_NT / TC_KC;    // stages per tile
-constexpr int TC_A_KS = TC_M * 8 * 4;    // one K-step, one part (head or remainder) of A
+constexpr int TC_A_KS = TC_M * TC_KE * 2;  // one K-step, one part (head or remainder) of A, bytes
 constexpr int TC_A = TC_KS * 2 * TC_A_KS;
 constexpr int TC_NT = 448;
 constexpr int TC_PROD0 = 64, TC_EPI0 = 192;  // first thread of the producers / epilogue
@@ -67,9 +69,9 @@ static_assert(AM_NT % TC_KC == 0, "nodes per stage");
 
 template <int NB>
 struct TcCfg {
-    static constexpr int B_KS = NB * 8 * 4;                 // one K-step, one part of B
-    static constexpr int STAGE = TC_A + TC_KS * 2 * B_KS;   // 32 KB (N = 128) or 48 KB (N = 256)
-    static constexpr int S = NB == 128 ? 7 : 4;             // stages in the ring
+    static constexpr int B_KS = NB * TC_KE * 2;             // one K-step, one part of B, bytes
+    static constexpr int STAGE = TC_A + TC_KS * 2 * B_KS;   // 16 KB (N = 128) or 24 KB (N = 256)
+    static constexpr int S = NB == 128 ? 12 : 8;            // stages in the ring
     static constexpr int SMEM = S * STAGE + 128;            // + alignment of the ring
     static constexpr int BUFS = NB == 128 ? 2 : 1;          // accumulator sets (2 NB columns each)
     static constexpr int RPT = NB / 128;                    // B rows per producer thread
@@ -93,7 +95,7 @@ __device__ __forceinline__ void tc_mma(unsigned dtmem, unsigned long long adesc,
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
         :
         : "r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
@@ -153,12 +155,14 @@ __device__ __forceinline__ bool tc_wait(unsigned long long *bar, unsigned parity
     return false;
 }
 
-// v rounded to TF32 (10 mantissa bits, ties away from zero) and the remainder
-__device__ __forceinline__ void tf32_split(float v, float &hi, float &lo)
+// v as an FP16 head and the FP16 rounding of the remainder, packed by two
+__device__ __forceinline__ void half_split2(float v0, float v1, unsigned &hi, unsigned &lo)
 {
-    const unsigned u = (__float_as_uint(v) + 0x1000u) & 0xffffe000u;
-    hi = __uint_as_float(u);
-    lo = v - hi;
+    const __half2 h = __floats2half2_rn(v0, v1);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(v0 - hf.x, v1 - hf.y);
+    hi = *(const unsigned *)&h;
+    lo = *(const unsigned *)&l;
 }
 
 static_assert(TC_M == 128, "am_ximg_part lays the X image out in 128-cell tiles");
@@ -210,7 +214,6 @@ __global__ void __launch_bounds__(TC_NT, 1)
     const float *__restrict__ Y = X + (long long)AM_NT * nx;
     const float *__restrict__ Z = Y + (long long)AM_NT * ny;
     const int *zon = (const int *)(Z + (long long)AM_NT * nz);
-    const float *__restrict__ ximg = a.d.am_ximg;
     const long long nrows = (long long)ny * nz;
     volatile int *abort = &s_abort;
 
@@ -247,7 +250,7 @@ __global__ void __launch_bounds__(TC_NT, 1)
             bool ok = true;
             for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 const int xt = (int)(t % ntx);
-                const float *src = ximg + (long long)xt * (AM_NT / 8) * 2 * (TC_M * 8);
+                const unsigned char *src = (const unsigned char *)a.d.am_ximg + (long long)xt * TC_NCH * TC_A;
                 for (int c = 0; c < TC_NCH; c++, q++) {
                     const int s = (int)(q % S);
                     if (q >= S && !tc_wait(&empty[s], (unsigned)((q / S - 1) & 1), abort)) {
@@ -255,8 +258,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
                         break;
                     }
                     tc_arrive_tx(&fullA[s], (unsigned)TC_A);
-                    tc_bulk_load(ring + s * C::STAGE, src + (long long)(TC_NCH - 1 - c) * TC_KS * 2 * (TC_M * 8),
-                                 (unsigned)TC_A, &fullA[s]);
+                    tc_bulk_load(ring + s * C::STAGE, src + (long long)(TC_NCH - 1 - c) * TC_A, (unsigned)TC_A,
+                                 &fullA[s]);
                 }
             }
             // copies still in flight land before the CTA may exit
@@ -266,8 +269,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
     } else if (warp == 1) {
         // ---- MMA issue (one thread)
         if (lane == 0) {
-            // kind::tf32, F32 accumulate, A and B K-major, M = 128, N
-            const unsigned idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(N >> 3) << 17) |
+            // kind::f16 with FP16 A and B, F32 accumulate, both K-major, M = 128, N
+            const unsigned idesc = (1u << 4) | (0u << 7) | (0u << 10) | ((unsigned)(N >> 3) << 17) |
                                    ((unsigned)(TC_M >> 4) << 24);
             long long q = 0, tl = 0;
             unsigned long long *last = nullptr;
@@ -321,6 +324,7 @@ __global__ void __launch_bounds__(TC_NT, 1)
         // stage's loads (across tiles too) are in flight while this stage is
         // split and stored.
         const int pr = tid - TC_PROD0;
+        const float sB = (float)am_b_scale(am_step(p, m, ctl->timestep + 1));
         const float *__restrict__ YT = am_yt(a.d.am_ximg, g.gx);
         const float *__restrict__ ZT = am_zt(a.d.am_ximg, g.gx, g.gy);
         long long q = 0;
@@ -364,10 +368,10 @@ __global__ void __launch_bounds__(TC_NT, 1)
                 for (int h = 0; h < C::RPT; h++)
 #pragma unroll
                     for (int k = 0; k < TC_KC / 4; k++) {
-                        v[h][4 * k] = ny4[h][k].x * nz4[h][k].x;
-                        v[h][4 * k + 1] = ny4[h][k].y * nz4[h][k].y;
-                        v[h][4 * k + 2] = ny4[h][k].z * nz4[h][k].z;
-                        v[h][4 * k + 3] = ny4[h][k].w * nz4[h][k].w;
+                        v[h][4 * k] = ny4[h][k].x * nz4[h][k].x * sB;
+                        v[h][4 * k + 1] = ny4[h][k].y * nz4[h][k].y * sB;
+                        v[h][4 * k + 2] = ny4[h][k].z * nz4[h][k].z * sB;
+                        v[h][4 * k + 3] = ny4[h][k].w * nz4[h][k].w * sB;
                     }
                 if (c + 1 < TC_NCH) {
                     fetch(c + 1);
@@ -388,14 +392,15 @@ __global__ void __launch_bounds__(TC_NT, 1)
                     const int off = (n >> 3) * 256 + (n & 7) * 16;
 #pragma unroll
                     for (int k = 0; k < TC_KS; k++) {
-                        float hi[8], lo[8];
+                        unsigned hi[8], lo[8];  // the K-step's 16 nodes as FP16 pairs
 #pragma unroll
-                        for (int e = 0; e < 8; e++) tf32_split(v[h][8 * k + e], hi[e], lo[e]);
+                        for (int e = 0; e < 8; e++)
+                            half_split2(v[h][TC_KE * k + 2 * e], v[h][TC_KE * k + 2 * e + 1], hi[e], lo[e]);
                         unsigned char *bh = B + (2 * k) * C::B_KS + off, *bl = B + (2 * k + 1) * C::B_KS + off;
-                        *(float4 *)bh = make_float4(hi[0], hi[1], hi[2], hi[3]);
-                        *(float4 *)(bh + 128) = make_float4(hi[4], hi[5], hi[6], hi[7]);
-                        *(float4 *)bl = make_float4(lo[0], lo[1], lo[2], lo[3]);
-                        *(float4 *)(bl + 128) = make_float4(lo[4], lo[5], lo[6], lo[7]);
+                        *(uint4 *)bh = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+                        *(uint4 *)(bh + 128) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+                        *(uint4 *)bl = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+                        *(uint4 *)(bl + 128) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
                     }
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -410,6 +415,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
         const int qd = warp & 3, hf = (warp - TC_EPI0 / 32) >> 2;
         const int xl = 32 * qd + lane;
         const AmStep st = am_step(p, m, ctl->timestep + 1);
+        // the sums are of (2^14 X) (sB YZ): back to X YZ, times Tfront
+        const double tf = st.Tfront / (16384.0 * am_b_scale(st));
         long long tl = 0;
         for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, tl++) {
             const int xt = (int)(t % ntx);
@@ -434,7 +441,7 @@ __global__ void __launch_bounds__(TC_NT, 1)
                     if (xin && R < nrows) {
                         // the two accumulators (the cross sum is ~2^-11 of the other)
                         const float sum = __uint_as_float(vh[j]) + __uint_as_float(vx[j]);
-                        const float T = on ? (float)(st.liniT + st.Tfront * (double)sum) : 0.f;
+                        const float T = on ? (float)(st.liniT + tf * (double)sum) : 0.f;
                         a.d.T32[cell] = T;
                         if (a.d.lsindex && (double)T > p.Tliq) a.d.lsindex[cell] = 1;
                     }

@@ -86,13 +86,14 @@ __device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
 constexpr int AM_NT = 400;
 
 // The FP32 form's tensor-core operand buffer (a.d.am_ximg): the X image of
-// am_tc.cu ([x tile of 128][K-step of 8 nodes][TF32 head, remainder][128 x
-// 8]), then Y and Z with the 400 nodes contiguous for each row (YT[J][i],
-// ZT[K][i]).
+// am_tc.cu (2^14 X as FP16 head and remainder: [x tile of 128][K-step of 16
+// nodes][head, remainder][128 x 16 halves]), then Y and Z with the 400 nodes
+// contiguous for each row (YT[J][i], ZT[K][i], FP32).  Sizes in floats.
 __host__ __device__ constexpr long long am_ximg_part(int gx)
 {
-    return (long long)((gx + 127) / 128) * (AM_NT / 8) * 2 * (128 * 8);
+    return (long long)((gx + 127) / 128) * (AM_NT / 16) * 2 * (128 * 16) / 2;
 }
+
 __host__ __device__ inline float *am_yt(float *img, int gx) { return img + am_ximg_part(gx); }
 __host__ __device__ inline float *am_zt(float *img, int gx, int gy)
 {
@@ -133,6 +134,20 @@ __device__ __forceinline__ AmStep am_step(const Phys &p, const AmParams &m, unsi
     s.Tfront = m.lab * pw * s.lalpha / (5.568328 * m.lthcon);
     s.liniT = m.liniT;
     return s;
+}
+
+// The power of two that scales the products Y_i(y) Z_i(z) into FP16's range
+// for the tensor cores: Y <= 1, and Z_i <= ldt / Tl_i <= ldt / Tl_0 (Tl_i =
+// sqrt(alpha t_i) (s^2 + 4 alpha t_i) grows with t_i), so the largest
+// product is at most ldt / Tl_0, which the scale maps to at most 2^14.
+// Subnormal FP16 values keep an absolute resolution of 2^-24, 2^-38 of that
+// maximum, so no per-row scale is needed.
+__device__ __forceinline__ double am_b_scale(const AmStep &s)
+{
+    const double lt0 = 0.5 * s.ldt;
+    const double zb = s.ldt / (sqrt(s.lalpha * lt0) * (s.ls * s.ls + 4. * s.lalpha * lt0));
+    if (!(zb > 0.0) || !(zb < 1e300)) return 1.0;
+    return exp2(14.0 - ceil(log2(zb)));
 }
 
 }  // namespace mms

@@ -26,6 +26,7 @@
 // grain rotation, which is exactly what grow_octahedra stored for it.
 // Arrays use the device layout of Geo (row pitch P).
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -171,15 +172,17 @@ __global__ void k_am_tables(KernelArgs a, AmParams m)
             const Real xv = (Real)exp(-(u * u) / ai);
             X[(long long)i * nx + q] = xv;
             if (sizeof(Real) == 4 && a.d.am_ximg && q >= 1 && q <= g.gx) {
-                // the tensor-core operand image (am_tc.cu): [x tile][K-step][head,
-                // remainder][128 x 8], K-major no-swizzle core matrices
-                const int r = (q - 1) & 127, xt = (q - 1) >> 7, ks = i >> 3, k = i & 7;
-                const long long blk = ((long long)xt * (AM_NT / 8) + ks) * 2 * 1024;
-                const int off = ((r >> 3) * 256 + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4) >> 2;
-                const unsigned hu = (__float_as_uint((float)xv) + 0x1000u) & 0xffffe000u;
-                const float hi = __uint_as_float(hu);
-                a.d.am_ximg[blk + off] = hi;
-                a.d.am_ximg[blk + 1024 + off] = (float)xv - hi;
+                // the tensor-core operand image (am_tc.cu): 2^14 X as FP16 head
+                // and remainder, [x tile][16-node K-step][head, remainder][128 x
+                // 16], K-major no-swizzle core matrices (offsets in halves)
+                const int r = (q - 1) & 127, xt = (q - 1) >> 7, ks = i >> 4, k = i & 15;
+                const long long blk = ((long long)xt * (AM_NT / 16) + ks) * 2 * 2048;
+                const int off = (r >> 3) * 128 + (k >> 3) * 64 + (r & 7) * 8 + (k & 7);
+                const float xs = (float)xv * 16384.f;
+                const __half hi = __float2half_rn(xs);
+                __half *img = (__half *)a.d.am_ximg;
+                img[blk + off] = hi;
+                img[blk + 2048 + off] = __float2half_rn(xs - __half2float(hi));
             }
         } else if (q < nx + ny) {
             const int J = q - nx;
@@ -340,10 +343,19 @@ __device__ __forceinline__ void nuc_body(const KernelArgs &a, int bid)
     if (s < a.d.nsites) {
         unsigned long long ts = ctl->timestep + 1;
         long long c = a.d.site_cell[s];
-        if (a.d.gr[c] <= 0) {
-            const Real *cl = (const Real *)a.d.cl[(int)(ctl->timestep & 1ULL)];
-            long long K = c / g.sz, J = (c % g.sz) / g.sy;
-            double Ttemp = temp_cell(p, a.d.T, a.d.T32, c, J, K, ts);
+        // the site's grain id, liquid concentration, threshold and (AM)
+        // temperature are loaded together, before the grain-id test
+        const Real *cl = (const Real *)a.d.cl[(int)(ctl->timestep & 1ULL)];
+        const int grc = a.d.gr[c];
+        const double clc = (double)cl[c];
+        const double thr = (double)a.d.site_thr[s];
+        const double Tarr = p.temp_mode == 2 ? (a.d.T32 ? (double)a.d.T32[c] : a.d.T[c]) : 0.0;
+        if (grc <= 0) {
+            double Ttemp = Tarr;
+            if (p.temp_mode != 2) {
+                const long long K = c / g.sz, J = (c % g.sz) / g.sy;
+                Ttemp = temp_cell(p, a.d.T, a.d.T32, c, J, K, ts);
+            }
             int layerno = 1, initnuc = 1;
             if (p.am) {
                 double sim_time = (double)ts * p.ts_delt;
@@ -358,8 +370,8 @@ __device__ __forceinline__ void nuc_body(const KernelArgs &a, int bid)
                 double Tunder = p.Tliq - Ttemp;
                 double m = p.ma * Ttemp * Ttemp + p.mb * Ttemp + p.mc;
                 // the FP32 form stores cl - Cinit
-                Tunder += m * ((sizeof(Real) == 8) ? ((double)cl[c] - p.cinit) : (double)cl[c]);
-                if (Tunder > (double)a.d.site_thr[s]) hit = 1;
+                Tunder += m * ((sizeof(Real) == 8) ? (clc - p.cinit) : clc);
+                if (Tunder > thr) hit = 1;
             }
         }
     }
