@@ -596,15 +596,15 @@ def _roofline(ks: dict, steps: int, cells: int, form: str, peaks: dict) -> dict:
         # tables + contraction per step: 2 x 400 multiply-adds per cell the
         # step computes (x = 1..gx of every halo'd (y, z) row; the halo
         # columns are filled only where read).  Algorithmic: the FP32 form
-        # issues three TF32 products per multiply-add (head x head, head x
-        # remainder, remainder x head), and TF32 runs at half the bf16 rate,
-        # so its tensor-core bound is peak / 6 in these units
+        # issues three FP16 products per multiply-add (head x head, head x
+        # remainder, remainder x head) at the dense FP16/bf16 rate, so its
+        # tensor-core bound is peak / 3 in these units
         cells_t = AM_DIMS[0] * (AM_DIMS[1] + 2) * (AM_DIMS[2] + 2)
         flops = 2.0 * 400 * cells_t
         ach = flops / per_launch / 1e12
         pk = peaks["bf16_tflops"]
         return {"bound": "tensor", "kernel": name, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
-                "frac": ach / pk, "frac_of_tf32x3_bound": ach / (pk / 6.0),
+                "frac": ach / pk, "frac_of_split_bound": ach / (pk / 3.0),
                 "peak_source": peaks["source"] + " (dense bf16 GEMM)",
                 "algorithmic_flops_per_launch": flops, "traffic": None,
                 "kernel_ms_per_launch": per_launch * 1e3}

@@ -6,36 +6,47 @@
 // over the 400 quadrature nodes i of the moving-source model
 // (temperature.c:62-123) is a (x cells x 400) by (400 x rows) matrix product.
 // A CTA computes tiles of 128 x cells (MMA M, the A side) by N (y, z) rows
-// (MMA N, the B side) with tcgen05.mma kind::tf32, accumulating in tensor
-// memory.  TF32 keeps 10 mantissa bits, so every operand is split as
-// v = hi + lo (hi = v rounded to TF32, lo the exact FP32 remainder) and the
-// product is hi*hi + hi*lo + lo*hi, three MMAs per step of 8 nodes; the
-// dropped lo*lo term and lo's own TF32 rounding are ~2^-22 relative.
+// (MMA N, the B side) with tcgen05.mma kind::f16 on FP16 operands,
+// accumulating in FP32 in tensor memory.
 //
-// Accumulation.  The tensor core adds the 8 products of an MMA and the
-// accumulator with truncation, so each MMA into an accumulator loses up to
-// one unit in the last place of the running sum, always toward zero.  Two
-// measures keep that small: the hi*hi products go to one accumulator and the
-// ~2^-11 smaller cross products to another (so the large sum takes 50 MMAs,
-// not 150), and the nodes are summed from the oldest (widest, smallest
-// terms) to the most recent, so that a cell's largest terms are added last,
-// onto a sum that is still small.  The epilogue adds the two accumulators
-// and forms liniT + Tfront sum in FP64.
+// Operands.  FP16 keeps 11 significant bits, so every operand is split as
+// v = hi + lo (hi = v rounded to FP16, lo the FP16 rounding of the
+// remainder) and the product is hi*hi + hi*lo + lo*hi, three MMAs per step
+// of 16 nodes; the dropped lo*lo term and lo's rounding are ~2^-22 relative.
+// The operands are scaled into FP16's range by powers of two (exact): X <= 1
+// by 2^14, and Y Z by am_b_scale, which maps its upper bound ldt / Tl_0 to at
+// most 2^14; FP16's subnormals keep an absolute resolution of 2^-24, 2^-38 of
+// the scaled maximum, so one scale per operand serves every row and column.
+// The epilogue divides the scales out.  Against the TF32 x 3 form this
+// halves the MMAs (K = 16 per instruction instead of 8) and the operand
+// bytes moved through shared memory.
+//
+// Accumulation.  The tensor core adds an MMA's products and the accumulator
+// with truncation, so each MMA into an accumulator loses up to one unit in
+// the last place of the running sum, always toward zero.  Two measures keep
+// that small: the hi*hi products go to one accumulator and the ~2^-11
+// smaller cross products to another (so the large sum takes 25 MMAs, not
+// 75), and the nodes are summed from the oldest (widest, smallest terms) to
+// the most recent, so that a cell's largest terms are added last, onto a sum
+// that is still small.  The epilogue adds the two accumulators and forms
+// liniT + Tfront sum in FP64.
 //
 // Persistent, warp-specialised, one CTA per SM:
 //   warp 0       A: the x side, one bulk copy per stage from the operand image
-//                k_am_tables writes once per step (already split into TF32
-//                head and remainder and laid out as the tensor core reads it)
+//                k_am_tables writes once per step (already scaled, split into
+//                FP16 head and remainder and laid out as the tensor core
+//                reads it)
 //   warp 1       the MMAs (one thread), committed to mbarriers
-//   warps 2-5    B: the rows' YZ products, split and stored into shared memory
+//   warps 2-5    B: the rows' YZ products, scaled, split and stored into
+//                shared memory
 //   warps 6-13   epilogue: tcgen05.ld of both accumulators, T (kept in FP32
 //                in this form) and the layer flag to global memory; two
 //                warps per group of 32 tensor-memory lanes, each taking every
 //                other 16 columns
-// Stages of 16 nodes (A 16 KB, B 16 or 32 KB) circulate in a shared-memory
-// ring of seven (N = 128) or four (N = 256).  With N = 128 the 512 tensor-memory columns hold two sets of
-// accumulators, so a tile's epilogue runs while the next tile accumulates;
-// with N = 256 one set fills them.
+// Stages of 16 nodes (A 8 KB, B 8 or 16 KB) circulate in a shared-memory
+// ring of twelve (N = 128) or eight (N = 256).  With N = 128 the 512
+// tensor-memory columns hold two sets of accumulators, so a tile's epilogue
+// runs while the next tile accumulates; with N = 256 one set fills them.
 //
 // The halo columns x = 0 and gx + 1 are not computed here: no kernel of a
 // step reads the temperature there.  k_am_halo fills them from the same
@@ -270,8 +281,13 @@ __global__ void __launch_bounds__(TC_NT, 1)
         // ---- MMA issue (one thread)
         if (lane == 0) {
             // kind::f16 with FP16 A and B, F32 accumulate, both K-major, M = 128, N
+            // (idesc2: N = 2 NB, B's head and remainder as one operand, when a
+            // tile's rows fill NB so that the remainder starts at row N)
             const unsigned idesc = (1u << 4) | (0u << 7) | (0u << 10) | ((unsigned)(N >> 3) << 17) |
                                    ((unsigned)(TC_M >> 4) << 24);
+            const bool pair_b = N == NB && 2 * NB <= 256;
+            const unsigned idesc2 = (1u << 4) | (0u << 7) | (0u << 10) | ((unsigned)((2 * NB) >> 3) << 17) |
+                                    ((unsigned)(TC_M >> 4) << 24);
             long long q = 0, tl = 0;
             unsigned long long *last = nullptr;
             unsigned last_par = 0;
@@ -299,9 +315,18 @@ __global__ void __launch_bounds__(TC_NT, 1)
                         const unsigned long long bh = kmajor_desc(smem_addr(B + (2 * k) * C::B_KS));
                         const unsigned long long bl = kmajor_desc(smem_addr(B + (2 * k + 1) * C::B_KS));
                         const unsigned acc = (c > 0 || kk > 0) ? 1u : 0u;
-                        tc_mma(dhh, ah, bh, idesc, acc);
-                        tc_mma(dxx, ah, bl, idesc, acc);
-                        tc_mma(dxx, al, bh, idesc, 1u);
+                        if (pair_b) {
+                            // the head and remainder of B are rows 0..N-1 and
+                            // N..2N-1 of one 2N-row operand, and the cross
+                            // accumulator is the hh one's next N columns: one
+                            // MMA gives hi*hi and hi*lo, a second adds lo*hi
+                            tc_mma(dhh, ah, bh, idesc2, acc);
+                            tc_mma(dxx, al, bh, idesc, 1u);
+                        } else {
+                            tc_mma(dhh, ah, bh, idesc, acc);
+                            tc_mma(dxx, ah, bl, idesc, acc);
+                            tc_mma(dxx, al, bh, idesc, 1u);
+                        }
                     }
                     tc_commit(&empty[s]);
                     last = &empty[s];
