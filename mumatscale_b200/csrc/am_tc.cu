@@ -43,8 +43,12 @@
 //                in this form) and the layer flag to global memory; two
 //                warps per group of 32 tensor-memory lanes, each taking every
 //                other 16 columns
-// Stages of 16 nodes (A 8 KB, B 8 or 16 KB) circulate in a shared-memory
-// ring of twelve (N = 128) or eight (N = 256).  With N = 128 the 512
+// Stages circulate in a shared-memory ring: with N = 128 seven stages of two
+// K-steps (32 nodes; A 16 KB, B 16 KB; the last stage of a tile holds the
+// one K-step left of 25), with N = 256 eight of one K-step (A 8 KB, B
+// 16 KB).  A stage costs each role a fixed handshake (a barrier wait, index
+// arithmetic, a commit or an arrival) of several hundred cycles, so the
+// stages are as large as the ring allows.  With N = 128 the 512
 // tensor-memory columns hold two sets of accumulators, so a tile's epilogue
 // runs while the next tile accumulates; with N = 256 one set fills them.
 //
@@ -66,26 +70,37 @@
 
 namespace mms {
 
-constexpr int TC_M = 128;                // x cells per tile (MMA M)
-constexpr int TC_KE = 16;                // nodes per MMA K-step (FP16 operands)
-constexpr int TC_KC = 16;                // nodes per stage
-constexpr int TC_KS = TC_KC / TC_KE;     // MMA K-steps per stage
-constexpr int TC_NCH = AM_NT / TC_KC;    // stages per tile
+constexpr int TC_M = 128;                  // x cells per tile (MMA M)
+constexpr int TC_KE = 16;                  // nodes per MMA K-step (FP16 operands)
+constexpr int TC_NKS = AM_NT / TC_KE;      // K-steps per tile
 constexpr int TC_A_KS = TC_M * TC_KE * 2;  // one K-step, one part (head or remainder) of A, bytes
-constexpr int TC_A = TC_KS * 2 * TC_A_KS;
+constexpr int TC_A_CH = 2 * TC_A_KS;       // one K-step of A, both parts: a chunk of the operand image
 constexpr int TC_NT = 448;
 constexpr int TC_PROD0 = 64, TC_EPI0 = 192;  // first thread of the producers / epilogue
+constexpr int TC_NPROD = TC_EPI0 - TC_PROD0; // producer threads (four warps)
 constexpr int TC_NEPI = TC_NT - TC_EPI0;     // epilogue threads (eight warps)
-static_assert(AM_NT % TC_KC == 0, "nodes per stage");
+static_assert(AM_NT % TC_KE == 0, "nodes per K-step");
 
 template <int NB>
 struct TcCfg {
+    static constexpr int KS = NB == 128 ? 2 : 1;            // K-steps per stage
+    static constexpr int NCH = (TC_NKS + KS - 1) / KS;      // stages per tile (the last may hold fewer)
     static constexpr int B_KS = NB * TC_KE * 2;             // one K-step, one part of B, bytes
-    static constexpr int STAGE = TC_A + TC_KS * 2 * B_KS;   // 16 KB (N = 128) or 24 KB (N = 256)
-    static constexpr int S = NB == 128 ? 12 : 8;            // stages in the ring
+    static constexpr int A_ST = KS * TC_A_CH;               // A bytes of a full stage
+    static constexpr int STAGE = A_ST + KS * 2 * B_KS;      // 32 KB (N = 128) or 24 KB (N = 256)
+    static constexpr int S = NB == 128 ? 7 : 8;             // stages in the ring
     static constexpr int SMEM = S * STAGE + 128;            // + alignment of the ring
     static constexpr int BUFS = NB == 128 ? 2 : 1;          // accumulator sets (2 NB columns each)
     static constexpr int RPT = NB / 128;                    // B rows per producer thread
+    // Stage c holds the K-steps (16-node chunks of the node order) lo(c) ..
+    // lo(c) + nk(c) - 1: the stages run from the oldest nodes (the highest
+    // chunks) to the most recent, and the last one holds what is left.
+    static __device__ __forceinline__ int lo(int c)
+    {
+        const int l = TC_NKS - KS * (c + 1);
+        return l > 0 ? l : 0;
+    }
+    static __device__ __forceinline__ int nk(int c) { return TC_NKS - KS * c - lo(c); }
 };
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -166,12 +181,20 @@ __device__ __forceinline__ bool tc_wait(unsigned long long *bar, unsigned parity
     return false;
 }
 
-// v as an FP16 head and the FP16 rounding of the remainder, packed by two
+// v as a head of 11 significant bits and the FP16 rounding of the
+// remainder, packed by two.  The head is Veltkamp's split (t = (2^13 + 1) v,
+// head = t - (t - v), with every operation rounded on its own): v = head +
+// remainder exactly in FP32, and the head converts to FP16 exactly wherever
+// FP16 holds 11 bits (|head| >= 2^-14; below that the conversion's error is
+// at most 2^-25, FP16's subnormal resolution).  Two conversions per pair
+// instead of four (no conversion of the head back to FP32): the conversion
+// pipe is the narrow one here.
 __device__ __forceinline__ void half_split2(float v0, float v1, unsigned &hi, unsigned &lo)
 {
-    const __half2 h = __floats2half2_rn(v0, v1);
-    const float2 hf = __half22float2(h);
-    const __half2 l = __floats2half2_rn(v0 - hf.x, v1 - hf.y);
+    const float t0 = __fmul_rn(v0, 8193.f), t1 = __fmul_rn(v1, 8193.f);
+    const float h0 = __fsub_rn(t0, __fsub_rn(t0, v0)), h1 = __fsub_rn(t1, __fsub_rn(t1, v1));
+    const __half2 h = __floats2half2_rn(h0, h1);
+    const __half2 l = __floats2half2_rn(__fsub_rn(v0, h0), __fsub_rn(v1, h1));
     hi = *(const unsigned *)&h;
     lo = *(const unsigned *)&l;
 }
@@ -214,7 +237,9 @@ __global__ void __launch_bounds__(TC_NT, 1)
     if (stalled(ctl)) return;
     extern __shared__ unsigned char tc_raw[];
     unsigned char *ring = (unsigned char *)(((unsigned long long)tc_raw + 127) & ~127ULL);
-    __shared__ __align__(8) unsigned long long fullA[S], fullB[S], empty[S], accf[2], acce[2];
+    // full[s]: the stage's A copy (one arrival with its byte count) and the
+    // 128 producers' B rows; empty[s]: the MMAs that read the stage are done
+    __shared__ __align__(8) unsigned long long full[S], empty[S], accf[2], acce[2];
     __shared__ unsigned tmem_base;
     __shared__ int s_abort;
     const Geo &g = a.g;
@@ -236,8 +261,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
     }
     if (tid == 0) {
         for (int s = 0; s < S; s++) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&fullA[s])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_addr(&fullB[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(1 + TC_NPROD)
+                         : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&empty[s])) : "memory");
         }
         for (int b = 0; b < 2; b++) {
@@ -253,29 +278,35 @@ __global__ void __launch_bounds__(TC_NT, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const unsigned tmem = tmem_base;
 
+    // The roles count stages with a ring slot s and the parity ph of its
+    // current round: full[s] completes once per round (wait on ph); a slot is
+    // refilled once empty[s] has completed the previous round (wait on ph ^ 1).
     if (warp == 0) {
-        // ---- A: one bulk copy of 16 KB per stage; stage c holds the nodes of
-        // chunk TC_NCH - 1 - c (oldest first)
+        // ---- A: one bulk copy per stage of its K-steps' chunks of the
+        // operand image (contiguous in node order)
         if (lane == 0) {
-            long long q = 0;
+            unsigned s = 0, ph = 0, issued = 0;
             bool ok = true;
             for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 const int xt = (int)(t % ntx);
-                const unsigned char *src = (const unsigned char *)a.d.am_ximg + (long long)xt * TC_NCH * TC_A;
-                for (int c = 0; c < TC_NCH; c++, q++) {
-                    const int s = (int)(q % S);
-                    if (q >= S && !tc_wait(&empty[s], (unsigned)((q / S - 1) & 1), abort)) {
+                const unsigned char *src = (const unsigned char *)a.d.am_ximg + (long long)xt * TC_NKS * TC_A_CH;
+                for (int c = 0; c < C::NCH; c++) {
+                    if (issued >= (unsigned)S && !tc_wait(&empty[s], ph ^ 1u, abort)) {
                         ok = false;
                         break;
                     }
-                    tc_arrive_tx(&fullA[s], (unsigned)TC_A);
-                    tc_bulk_load(ring + s * C::STAGE, src + (long long)(TC_NCH - 1 - c) * TC_A, (unsigned)TC_A,
-                                 &fullA[s]);
+                    const unsigned bytes = (unsigned)(C::nk(c) * TC_A_CH);
+                    tc_arrive_tx(&full[s], bytes);
+                    tc_bulk_load(ring + s * C::STAGE, src + C::lo(c) * TC_A_CH, bytes, &full[s]);
+                    issued++;
+                    if (++s == (unsigned)S) s = 0, ph ^= 1u;
                 }
             }
-            // copies still in flight land before the CTA may exit
-            for (long long j = (q > S ? q - S : 0); j < q; j++)
-                tc_wait(&fullA[j % S], (unsigned)((j / S) & 1), abort, true);
+            // copies still in flight land before the CTA may exit (after an
+            // abort the producers' arrivals may be missing: the bounded wait
+            // then outlasts the copies)
+            for (unsigned j = (issued > (unsigned)S ? issued - S : 0); j < issued; j++)
+                tc_wait(&full[j % S], (j / S) & 1u, abort, true);
         }
     } else if (warp == 1) {
         // ---- MMA issue (one thread)
@@ -288,32 +319,37 @@ __global__ void __launch_bounds__(TC_NT, 1)
             const bool pair_b = N == NB && 2 * NB <= 256;
             const unsigned idesc2 = (1u << 4) | (0u << 7) | (0u << 10) | ((unsigned)((2 * NB) >> 3) << 17) |
                                     ((unsigned)(TC_M >> 4) << 24);
-            long long q = 0, tl = 0;
+            // descriptors of the ring's operands: the start address field is
+            // the byte address / 16 (below 2^14 for any shared address), so a
+            // stage's descriptors are the ring's plus the offset / 16
+            const unsigned long long d0 = kmajor_desc(smem_addr(ring));
+            unsigned s = 0, ph = 0, tl = 0;
             unsigned long long *last = nullptr;
             unsigned last_par = 0;
             bool ok = true;
             for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x, tl++) {
                 const int b = C::BUFS == 2 ? (int)(tl & 1) : 0;
-                const long long use = C::BUFS == 2 ? tl / 2 : tl;  // earlier tiles in this set
-                if (use >= 1 && !tc_wait(&acce[b], (unsigned)((use - 1) & 1), abort)) break;
+                const unsigned use = C::BUFS == 2 ? tl >> 1 : tl;  // earlier tiles in this set
+                if (use >= 1 && !tc_wait(&acce[b], (use - 1) & 1u, abort)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const unsigned dhh = tmem + (unsigned)(b * 2 * NB), dxx = dhh + (unsigned)NB;
-                for (int c = 0; c < TC_NCH; c++, q++) {
-                    const int s = (int)(q % S);
-                    const unsigned par = (unsigned)((q / S) & 1);
-                    if (!tc_wait(&fullA[s], par, abort) || !tc_wait(&fullB[s], par, abort)) {
+                for (int c = 0; c < C::NCH; c++) {
+                    if (!tc_wait(&full[s], ph, abort)) {
                         ok = false;
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    unsigned char *A = ring + s * C::STAGE, *B = A + TC_A;
+                    const unsigned long long da = d0 + (unsigned)((s * C::STAGE) >> 4);
+                    const unsigned long long db = da + (unsigned)(C::A_ST >> 4);
+                    const int n = C::nk(c);
 #pragma unroll
-                    for (int kk = 0; kk < TC_KS; kk++) {
-                        const int k = TC_KS - 1 - kk;  // the later (older) K-step of the stage first
-                        const unsigned long long ah = kmajor_desc(smem_addr(A + (2 * k) * TC_A_KS));
-                        const unsigned long long al = kmajor_desc(smem_addr(A + (2 * k + 1) * TC_A_KS));
-                        const unsigned long long bh = kmajor_desc(smem_addr(B + (2 * k) * C::B_KS));
-                        const unsigned long long bl = kmajor_desc(smem_addr(B + (2 * k + 1) * C::B_KS));
+                    for (int kk = 0; kk < C::KS; kk++) {
+                        if (kk >= n) break;
+                        const int k = n - 1 - kk;  // the later (older) K-step of the stage first
+                        const unsigned long long ah = da + (unsigned)((2 * k) * TC_A_KS >> 4);
+                        const unsigned long long al = da + (unsigned)((2 * k + 1) * TC_A_KS >> 4);
+                        const unsigned long long bh = db + (unsigned)((2 * k) * C::B_KS >> 4);
+                        const unsigned long long bl = db + (unsigned)((2 * k + 1) * C::B_KS >> 4);
                         const unsigned acc = (c > 0 || kk > 0) ? 1u : 0u;
                         if (pair_b) {
                             // the head and remainder of B are rows 0..N-1 and
@@ -330,42 +366,45 @@ __global__ void __launch_bounds__(TC_NT, 1)
                     }
                     tc_commit(&empty[s]);
                     last = &empty[s];
-                    last_par = par;
+                    last_par = ph;
+                    if (++s == (unsigned)S) s = 0, ph ^= 1u;
                 }
                 if (!ok) break;
                 tc_commit(&accf[b]);
                 last = &accf[b];
-                last_par = (unsigned)(use & 1);
+                last_par = use & 1u;
             }
             // every committed MMA completes before the tensor memory is freed
             if (last) tc_wait(last, last_par, abort, true);
         }
     } else if (tid < TC_EPI0) {
-        // ---- B: rows pr (+ 128) of the tile, the 16 nodes of each stage.
-        // The tables are read from the node-contiguous copies YT[J][i] and
-        // ZT[K][i]: a row's 16 nodes are four 16-byte loads, and CTAs working
-        // on different rows read different lines (node-major tables made
-        // every SM read the same few lines at the same moment).  The next
-        // stage's loads (across tiles too) are in flight while this stage is
-        // split and stored.
+        // ---- B: rows pr (+ 128) of the tile, a stage's nodes one K-step (16
+        // nodes) at a time.  The tables are read from the node-contiguous
+        // copies YT[J][i] and ZT[K][i]: a row's 16 nodes are four 16-byte
+        // loads, and CTAs working on different rows read different lines
+        // (node-major tables made every SM read the same few lines at the
+        // same moment).  The next K-step's loads (of the next stage or tile
+        // too) are in flight while this one is split and stored, and while
+        // the next stage's slot is waited for.
         const int pr = tid - TC_PROD0;
         const float sB = (float)am_b_scale(am_step(p, m, ctl->timestep + 1));
         const float *__restrict__ YT = am_yt(a.d.am_ximg, g.gx);
         const float *__restrict__ ZT = am_zt(a.d.am_ximg, g.gx, g.gy);
-        long long q = 0;
-        bool ok = true;
+        unsigned s = 0, ph = 0;
+        bool wrapped = false, ok = true;
         const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        float4 ny4[C::RPT][TC_KC / 4], nz4[C::RPT][TC_KC / 4];  // the next stage's table values
+        float4 ny4[C::RPT][TC_KE / 4], nz4[C::RPT][TC_KE / 4];  // the next K-step's table values
         const float4 *yrow[C::RPT], *zrow[C::RPT];
         bool on[C::RPT];
-        auto fetch = [&](int c) {
-            const int i0 = (TC_NCH - 1 - c) * TC_KC;
+        // the loads of K-step k of stage c
+        auto fetch = [&](int c, int k) {
+            const int i4 = (C::lo(c) + k) * (TC_KE / 4);
 #pragma unroll
             for (int h = 0; h < C::RPT; h++)
 #pragma unroll
-                for (int k = 0; k < TC_KC / 4; k++) {
-                    ny4[h][k] = on[h] ? __ldg(yrow[h] + i0 / 4 + k) : zero4;
-                    nz4[h][k] = on[h] ? __ldg(zrow[h] + i0 / 4 + k) : zero4;
+                for (int e = 0; e < TC_KE / 4; e++) {
+                    ny4[h][e] = on[h] ? __ldg(yrow[h] + i4 + e) : zero4;
+                    nz4[h][e] = on[h] ? __ldg(zrow[h] + i4 + e) : zero4;
                 }
         };
         // this thread's rows of tile t
@@ -383,44 +422,46 @@ __global__ void __launch_bounds__(TC_NT, 1)
         };
         if (blockIdx.x < ntiles) {
             rows_of(blockIdx.x);
-            fetch(0);
+            fetch(0, 0);
         }
         for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-            for (int c = 0; c < TC_NCH; c++, q++) {
-                const int s = (int)(q % S);
-                float v[C::RPT][TC_KC];
-#pragma unroll
-                for (int h = 0; h < C::RPT; h++)
-#pragma unroll
-                    for (int k = 0; k < TC_KC / 4; k++) {
-                        v[h][4 * k] = ny4[h][k].x * nz4[h][k].x * sB;
-                        v[h][4 * k + 1] = ny4[h][k].y * nz4[h][k].y * sB;
-                        v[h][4 * k + 2] = ny4[h][k].z * nz4[h][k].z * sB;
-                        v[h][4 * k + 3] = ny4[h][k].w * nz4[h][k].w * sB;
-                    }
-                if (c + 1 < TC_NCH) {
-                    fetch(c + 1);
-                } else if (t + gridDim.x < ntiles) {
-                    // the next tile's first stage (v already holds this one's)
-                    rows_of(t + gridDim.x);
-                    fetch(0);
-                }
-                if (q >= S && !tc_wait(&empty[s], (unsigned)((q / S - 1) & 1), abort)) {
+            for (int c = 0; c < C::NCH; c++) {
+                if (wrapped && !tc_wait(&empty[s], ph ^ 1u, abort)) {
                     ok = false;
                     break;
                 }
-                unsigned char *B = ring + s * C::STAGE + TC_A;
+                unsigned char *B = ring + s * C::STAGE + C::A_ST;
+                const int nks = C::nk(c);
 #pragma unroll
-                for (int h = 0; h < C::RPT; h++) {
-                    const int n = pr + 128 * h;
-                    if (n >= N) continue;
-                    const int off = (n >> 3) * 256 + (n & 7) * 16;
+                for (int k = 0; k < C::KS; k++) {
+                    if (k >= nks) break;
+                    float v[C::RPT][TC_KE];
 #pragma unroll
-                    for (int k = 0; k < TC_KS; k++) {
+                    for (int h = 0; h < C::RPT; h++)
+#pragma unroll
+                        for (int e = 0; e < TC_KE / 4; e++) {
+                            v[h][4 * e] = ny4[h][e].x * nz4[h][e].x * sB;
+                            v[h][4 * e + 1] = ny4[h][e].y * nz4[h][e].y * sB;
+                            v[h][4 * e + 2] = ny4[h][e].z * nz4[h][e].z * sB;
+                            v[h][4 * e + 3] = ny4[h][e].w * nz4[h][e].w * sB;
+                        }
+                    if (k + 1 < nks) {
+                        fetch(c, k + 1);
+                    } else if (c + 1 < C::NCH) {
+                        fetch(c + 1, 0);
+                    } else if (t + gridDim.x < ntiles) {
+                        // the next tile's first K-step
+                        rows_of(t + gridDim.x);
+                        fetch(0, 0);
+                    }
+#pragma unroll
+                    for (int h = 0; h < C::RPT; h++) {
+                        const int n = pr + 128 * h;
+                        if (n >= N) continue;
+                        const int off = (n >> 3) * 256 + (n & 7) * 16;
                         unsigned hi[8], lo[8];  // the K-step's 16 nodes as FP16 pairs
 #pragma unroll
-                        for (int e = 0; e < 8; e++)
-                            half_split2(v[h][TC_KE * k + 2 * e], v[h][TC_KE * k + 2 * e + 1], hi[e], lo[e]);
+                        for (int e = 0; e < 8; e++) half_split2(v[h][2 * e], v[h][2 * e + 1], hi[e], lo[e]);
                         unsigned char *bh = B + (2 * k) * C::B_KS + off, *bl = B + (2 * k + 1) * C::B_KS + off;
                         *(uint4 *)bh = make_uint4(hi[0], hi[1], hi[2], hi[3]);
                         *(uint4 *)(bh + 128) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
@@ -429,7 +470,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
                     }
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                tc_arrive(&fullB[s]);
+                tc_arrive(&full[s]);
+                if (++s == (unsigned)S) s = 0, ph ^= 1u, wrapped = true;
             }
         }
     } else {
@@ -442,40 +484,78 @@ __global__ void __launch_bounds__(TC_NT, 1)
         const AmStep st = am_step(p, m, ctl->timestep + 1);
         // the sums are of (2^14 X) (sB YZ): back to X YZ, times Tfront
         const double tf = st.Tfront / (16384.0 * am_b_scale(st));
+        // kernel parameters in registers: a store through T32 might alias
+        // the parameter block as far as the compiler knows, so every read of
+        // it after a store would be a load again
+        float *const T32 = a.d.T32;
+        int *const lsx = a.d.lsindex;
+        const double Tliq = p.Tliq;
+        const long long sy = g.sy, sz = g.sz;
+        const int gx = g.gx;
         long long tl = 0;
         for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, tl++) {
             const int xt = (int)(t % ntx);
             const long long r0 = (t / ntx) * (long long)N;
             const int b = C::BUFS == 2 ? (int)(tl & 1) : 0;
             const long long use = C::BUFS == 2 ? tl / 2 : tl;
+            // the tile's first row and the flags of its z plane and the next
+            // (the rows cross at most one plane when ny >= N), read before
+            // the wait so that the loads are not on the chunks' path
+            const int K0 = (int)(r0 / ny), J0 = (int)(r0 - (long long)K0 * ny);
+            const bool on0 = zon[K0] != 0, on1 = K0 + 1 < nz && zon[K0 + 1] != 0;
             const bool got = tc_wait(&accf[b], (unsigned)(use & 1), abort);
             // the warp-wide tcgen05.ld below needs the whole warp, converged
             if (!__all_sync(0xffffffffu, got)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int x = 1 + TC_M * xt + xl;
-            const bool xin = x <= g.gx;
+            const bool xin = x <= gx;
             const unsigned col = tmem + ((unsigned)(32 * qd) << 16) + (unsigned)(b * 2 * NB);
-            // T of rows r0 + cc .. + 15 from the chunk's two accumulators
+            // T of rows r0 + cc .. + 15 from the chunk's two accumulators.  The
+            // sixteen values are formed first, free of the row walk's
+            // branches, so that their conversions and FP64 multiply-adds
+            // overlap; then they are stored, in one run when the rows stay in
+            // one z plane.
             auto store16 = [&](int cc, const unsigned (&vh)[16], const unsigned (&vx)[16]) {
+                if (!xin) return;
+                float Tv[16];
+#pragma unroll
+                for (int j = 0; j < 16; j++) {
+                    // the two accumulators (the cross sum is ~2^-11 of the other)
+                    const float sum = __uint_as_float(vh[j]) + __uint_as_float(vx[j]);
+                    Tv[j] = (float)(st.liniT + tf * (double)sum);
+                }
                 long long R = r0 + cc;
+                if (ny >= N && R + 16 <= nrows) {
+                    int J = J0 + cc, K = K0;
+                    bool on = on0;
+                    if (J >= ny) J -= ny, K++, on = on1;
+                    if (J + 16 <= ny) {
+                        float *const out = T32 + ((long long)K * sz + (long long)J * sy + x);
+#pragma unroll
+                        for (int j = 0; j < 16; j++) {
+                            const float T = on ? Tv[j] : 0.f;
+                            out[j * sy] = T;
+                            if (lsx && (double)T > Tliq) lsx[(out - T32) + j * sy] = 1;
+                        }
+                        return;
+                    }
+                }
                 int K = (int)(R / ny), J = (int)(R - (long long)K * ny);
-                long long cell = (long long)K * g.sz + (long long)J * g.sy + x;
+                long long cell = (long long)K * sz + (long long)J * sy + x;
                 bool on = zon[K] != 0;
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
-                    if (xin && R < nrows) {
-                        // the two accumulators (the cross sum is ~2^-11 of the other)
-                        const float sum = __uint_as_float(vh[j]) + __uint_as_float(vx[j]);
-                        const float T = on ? (float)(st.liniT + tf * (double)sum) : 0.f;
-                        a.d.T32[cell] = T;
-                        if (a.d.lsindex && (double)T > p.Tliq) a.d.lsindex[cell] = 1;
+                    if (R < nrows) {
+                        const float T = on ? Tv[j] : 0.f;
+                        T32[cell] = T;
+                        if (lsx && (double)T > Tliq) lsx[cell] = 1;
                     }
                     R++;
-                    cell += g.sy;
+                    cell += sy;
                     if (++J == ny) {
                         J = 0;
                         K++;
-                        cell += g.sz - (long long)ny * g.sy;
+                        cell += sz - (long long)ny * sy;
                         on = K < nz && zon[K] != 0;
                     }
                 }
