@@ -29,17 +29,23 @@
 // 75), and the nodes are summed from the oldest (widest, smallest terms) to
 // the most recent, so that a cell's largest terms are added last, onto a sum
 // that is still small.  The epilogue adds the two accumulators and forms
-// liniT + Tfront sum in FP64.
+// liniT + Tfront sum in FP32 with the constants split into head and
+// remainder (within one unit in the last place of the FP32 result).
+//
+// Operand images.  Both operands reach shared memory by bulk copies of
+// images written once per step, already scaled, split into FP16 head and
+// remainder and laid out as the tensor core reads them: k_am_tables writes
+// the X image (x blocks of 128), k_am_bimg the B image (blocks of N (y, z)
+// rows, 1.6 KB per row).  The B image is the larger (53 MB at 512 x 256 x
+// 128) but is written at memory bandwidth by a plain elementwise kernel and
+// read by the contraction from L2 (the x blocks of a row block are
+// consecutive tiles); forming it inside the contraction took four warps per
+// SM whose serial per-stage work set the pace.
 //
 // Persistent, warp-specialised, one CTA per SM:
-//   warp 0       A: the x side, one bulk copy per stage from the operand image
-//                k_am_tables writes once per step (already scaled, split into
-//                FP16 head and remainder and laid out as the tensor core
-//                reads it)
+//   warp 0       both operands: per stage one bulk copy from each image
 //   warp 1       the MMAs (one thread), committed to mbarriers
-//   warps 2-5    B: the rows' YZ products, scaled, split and stored into
-//                shared memory
-//   warps 6-13   epilogue: tcgen05.ld of both accumulators, T (kept in FP32
+//   warps 2-9    epilogue: tcgen05.ld of both accumulators, T (kept in FP32
 //                in this form) and the layer flag to global memory; two
 //                warps per group of 32 tensor-memory lanes, each taking every
 //                other 16 columns
@@ -75,9 +81,8 @@ constexpr int TC_KE = 16;                  // nodes per MMA K-step (FP16 operand
 constexpr int TC_NKS = AM_NT / TC_KE;      // K-steps per tile
 constexpr int TC_A_KS = TC_M * TC_KE * 2;  // one K-step, one part (head or remainder) of A, bytes
 constexpr int TC_A_CH = 2 * TC_A_KS;       // one K-step of A, both parts: a chunk of the operand image
-constexpr int TC_NT = 448;
-constexpr int TC_PROD0 = 64, TC_EPI0 = 192;  // first thread of the producers / epilogue
-constexpr int TC_NPROD = TC_EPI0 - TC_PROD0; // producer threads (four warps)
+constexpr int TC_NT = 320;
+constexpr int TC_EPI0 = 64;                  // first thread of the epilogue
 constexpr int TC_NEPI = TC_NT - TC_EPI0;     // epilogue threads (eight warps)
 static_assert(AM_NT % TC_KE == 0, "nodes per K-step");
 
@@ -85,13 +90,12 @@ template <int NB>
 struct TcCfg {
     static constexpr int KS = NB == 128 ? 2 : 1;            // K-steps per stage
     static constexpr int NCH = (TC_NKS + KS - 1) / KS;      // stages per tile (the last may hold fewer)
-    static constexpr int B_KS = NB * TC_KE * 2;             // one K-step, one part of B, bytes
+    static constexpr int B_KS = NB * TC_KE * 2;             // one K-step, one part of B, bytes, at N = NB
     static constexpr int A_ST = KS * TC_A_CH;               // A bytes of a full stage
     static constexpr int STAGE = A_ST + KS * 2 * B_KS;      // 32 KB (N = 128) or 24 KB (N = 256)
     static constexpr int S = NB == 128 ? 7 : 8;             // stages in the ring
     static constexpr int SMEM = S * STAGE + 128;            // + alignment of the ring
     static constexpr int BUFS = NB == 128 ? 2 : 1;          // accumulator sets (2 NB columns each)
-    static constexpr int RPT = NB / 128;                    // B rows per producer thread
     // Stage c holds the K-steps (16-node chunks of the node order) lo(c) ..
     // lo(c) + nk(c) - 1: the stages run from the oldest nodes (the highest
     // chunks) to the most recent, and the last one holds what is left.
@@ -237,8 +241,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
     if (stalled(ctl)) return;
     extern __shared__ unsigned char tc_raw[];
     unsigned char *ring = (unsigned char *)(((unsigned long long)tc_raw + 127) & ~127ULL);
-    // full[s]: the stage's A copy (one arrival with its byte count) and the
-    // 128 producers' B rows; empty[s]: the MMAs that read the stage are done
+    // full[s]: the stage's A and B copies have landed (one arrival with
+    // their byte count); empty[s]: the MMAs that read the stage are done
     __shared__ __align__(8) unsigned long long full[S], empty[S], accf[2], acce[2];
     __shared__ unsigned tmem_base;
     __shared__ int s_abort;
@@ -261,8 +265,7 @@ __global__ void __launch_bounds__(TC_NT, 1)
     }
     if (tid == 0) {
         for (int s = 0; s < S; s++) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(1 + TC_NPROD)
-                         : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full[s])) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&empty[s])) : "memory");
         }
         for (int b = 0; b < 2; b++) {
@@ -281,30 +284,35 @@ __global__ void __launch_bounds__(TC_NT, 1)
     // The roles count stages with a ring slot s and the parity ph of its
     // current round: full[s] completes once per round (wait on ph); a slot is
     // refilled once empty[s] has completed the previous round (wait on ph ^ 1).
+    // B's bytes per K-step and part at this tile height
+    const int BN = N * TC_KE * 2;
     if (warp == 0) {
-        // ---- A: one bulk copy per stage of its K-steps' chunks of the
-        // operand image (contiguous in node order)
+        // ---- A and B: per stage one bulk copy of its K-steps' chunks from
+        // each operand image (contiguous in node order): X's image for the
+        // tile's x block, the B image for its row block
         if (lane == 0) {
             unsigned s = 0, ph = 0, issued = 0;
             bool ok = true;
+            const unsigned char *bimg = am_bimg(a.d.am_ximg, g.gx, g.gy, g.gz);
             for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 const int xt = (int)(t % ntx);
-                const unsigned char *src = (const unsigned char *)a.d.am_ximg + (long long)xt * TC_NKS * TC_A_CH;
+                const long long rb = t / ntx;
+                const unsigned char *srcA = (const unsigned char *)a.d.am_ximg + (long long)xt * TC_NKS * TC_A_CH;
+                const unsigned char *srcB = bimg + rb * TC_NKS * 2 * BN;
                 for (int c = 0; c < C::NCH; c++) {
                     if (issued >= (unsigned)S && !tc_wait(&empty[s], ph ^ 1u, abort)) {
                         ok = false;
                         break;
                     }
-                    const unsigned bytes = (unsigned)(C::nk(c) * TC_A_CH);
-                    tc_arrive_tx(&full[s], bytes);
-                    tc_bulk_load(ring + s * C::STAGE, src + C::lo(c) * TC_A_CH, bytes, &full[s]);
+                    const unsigned ba = (unsigned)(C::nk(c) * TC_A_CH), bb = (unsigned)(C::nk(c) * 2 * BN);
+                    tc_arrive_tx(&full[s], ba + bb);
+                    tc_bulk_load(ring + s * C::STAGE, srcA + C::lo(c) * TC_A_CH, ba, &full[s]);
+                    tc_bulk_load(ring + s * C::STAGE + C::A_ST, srcB + C::lo(c) * 2 * BN, bb, &full[s]);
                     issued++;
                     if (++s == (unsigned)S) s = 0, ph ^= 1u;
                 }
             }
-            // copies still in flight land before the CTA may exit (after an
-            // abort the producers' arrivals may be missing: the bounded wait
-            // then outlasts the copies)
+            // copies still in flight land before the CTA may exit
             for (unsigned j = (issued > (unsigned)S ? issued - S : 0); j < issued; j++)
                 tc_wait(&full[j % S], (j / S) & 1u, abort, true);
         }
@@ -312,12 +320,12 @@ __global__ void __launch_bounds__(TC_NT, 1)
         // ---- MMA issue (one thread)
         if (lane == 0) {
             // kind::f16 with FP16 A and B, F32 accumulate, both K-major, M = 128, N
-            // (idesc2: N = 2 NB, B's head and remainder as one operand, when a
-            // tile's rows fill NB so that the remainder starts at row N)
+            // (idesc2: N = 2 N, B's head and remainder as one operand: in the
+            // stage the remainder's rows follow the head's)
             const unsigned idesc = (1u << 4) | (0u << 7) | (0u << 10) | ((unsigned)(N >> 3) << 17) |
                                    ((unsigned)(TC_M >> 4) << 24);
-            const bool pair_b = N == NB && 2 * NB <= 256;
-            const unsigned idesc2 = (1u << 4) | (0u << 7) | (0u << 10) | ((unsigned)((2 * NB) >> 3) << 17) |
+            const bool pair_b = 2 * N <= 256;
+            const unsigned idesc2 = (1u << 4) | (0u << 7) | (0u << 10) | ((unsigned)((2 * N) >> 3) << 17) |
                                     ((unsigned)(TC_M >> 4) << 24);
             // descriptors of the ring's operands: the start address field is
             // the byte address / 16 (below 2^14 for any shared address), so a
@@ -332,7 +340,7 @@ __global__ void __launch_bounds__(TC_NT, 1)
                 const unsigned use = C::BUFS == 2 ? tl >> 1 : tl;  // earlier tiles in this set
                 if (use >= 1 && !tc_wait(&acce[b], (use - 1) & 1u, abort)) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const unsigned dhh = tmem + (unsigned)(b * 2 * NB), dxx = dhh + (unsigned)NB;
+                const unsigned dhh = tmem + (unsigned)(b * 2 * NB), dxx = dhh + (unsigned)N;
                 for (int c = 0; c < C::NCH; c++) {
                     if (!tc_wait(&full[s], ph, abort)) {
                         ok = false;
@@ -348,8 +356,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
                         const int k = n - 1 - kk;  // the later (older) K-step of the stage first
                         const unsigned long long ah = da + (unsigned)((2 * k) * TC_A_KS >> 4);
                         const unsigned long long al = da + (unsigned)((2 * k + 1) * TC_A_KS >> 4);
-                        const unsigned long long bh = db + (unsigned)((2 * k) * C::B_KS >> 4);
-                        const unsigned long long bl = db + (unsigned)((2 * k + 1) * C::B_KS >> 4);
+                        const unsigned long long bh = db + (unsigned)((2 * k) * BN >> 4);
+                        const unsigned long long bl = db + (unsigned)((2 * k + 1) * BN >> 4);
                         const unsigned acc = (c > 0 || kk > 0) ? 1u : 0u;
                         if (pair_b) {
                             // the head and remainder of B are rows 0..N-1 and
@@ -377,113 +385,22 @@ __global__ void __launch_bounds__(TC_NT, 1)
             // every committed MMA completes before the tensor memory is freed
             if (last) tc_wait(last, last_par, abort, true);
         }
-    } else if (tid < TC_EPI0) {
-        // ---- B: rows pr (+ 128) of the tile, a stage's nodes one K-step (16
-        // nodes) at a time.  The tables are read from the node-contiguous
-        // copies YT[J][i] and ZT[K][i]: a row's 16 nodes are four 16-byte
-        // loads, and CTAs working on different rows read different lines
-        // (node-major tables made every SM read the same few lines at the
-        // same moment).  The next K-step's loads (of the next stage or tile
-        // too) are in flight while this one is split and stored, and while
-        // the next stage's slot is waited for.
-        const int pr = tid - TC_PROD0;
-        const float sB = (float)am_b_scale(am_step(p, m, ctl->timestep + 1));
-        const float *__restrict__ YT = am_yt(a.d.am_ximg, g.gx);
-        const float *__restrict__ ZT = am_zt(a.d.am_ximg, g.gx, g.gy);
-        unsigned s = 0, ph = 0;
-        bool wrapped = false, ok = true;
-        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        float4 ny4[C::RPT][TC_KE / 4], nz4[C::RPT][TC_KE / 4];  // the next K-step's table values
-        const float4 *yrow[C::RPT], *zrow[C::RPT];
-        bool on[C::RPT];
-        // the loads of K-step k of stage c
-        auto fetch = [&](int c, int k) {
-            const int i4 = (C::lo(c) + k) * (TC_KE / 4);
-#pragma unroll
-            for (int h = 0; h < C::RPT; h++)
-#pragma unroll
-                for (int e = 0; e < TC_KE / 4; e++) {
-                    ny4[h][e] = on[h] ? __ldg(yrow[h] + i4 + e) : zero4;
-                    nz4[h][e] = on[h] ? __ldg(zrow[h] + i4 + e) : zero4;
-                }
-        };
-        // this thread's rows of tile t
-        auto rows_of = [&](long long t) {
-            const long long r0 = (t / ntx) * (long long)N;
-#pragma unroll
-            for (int h = 0; h < C::RPT; h++) {
-                const int n = pr + 128 * h;
-                const long long R = r0 + n;
-                on[h] = n < N && R < nrows;
-                const int K = on[h] ? (int)(R / ny) : 0, J = on[h] ? (int)(R - (long long)K * ny) : 0;
-                yrow[h] = (const float4 *)(YT + (long long)J * AM_NT);
-                zrow[h] = (const float4 *)(ZT + (long long)K * AM_NT);
-            }
-        };
-        if (blockIdx.x < ntiles) {
-            rows_of(blockIdx.x);
-            fetch(0, 0);
-        }
-        for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-            for (int c = 0; c < C::NCH; c++) {
-                if (wrapped && !tc_wait(&empty[s], ph ^ 1u, abort)) {
-                    ok = false;
-                    break;
-                }
-                unsigned char *B = ring + s * C::STAGE + C::A_ST;
-                const int nks = C::nk(c);
-#pragma unroll
-                for (int k = 0; k < C::KS; k++) {
-                    if (k >= nks) break;
-                    float v[C::RPT][TC_KE];
-#pragma unroll
-                    for (int h = 0; h < C::RPT; h++)
-#pragma unroll
-                        for (int e = 0; e < TC_KE / 4; e++) {
-                            v[h][4 * e] = ny4[h][e].x * nz4[h][e].x * sB;
-                            v[h][4 * e + 1] = ny4[h][e].y * nz4[h][e].y * sB;
-                            v[h][4 * e + 2] = ny4[h][e].z * nz4[h][e].z * sB;
-                            v[h][4 * e + 3] = ny4[h][e].w * nz4[h][e].w * sB;
-                        }
-                    if (k + 1 < nks) {
-                        fetch(c, k + 1);
-                    } else if (c + 1 < C::NCH) {
-                        fetch(c + 1, 0);
-                    } else if (t + gridDim.x < ntiles) {
-                        // the next tile's first K-step
-                        rows_of(t + gridDim.x);
-                        fetch(0, 0);
-                    }
-#pragma unroll
-                    for (int h = 0; h < C::RPT; h++) {
-                        const int n = pr + 128 * h;
-                        if (n >= N) continue;
-                        const int off = (n >> 3) * 256 + (n & 7) * 16;
-                        unsigned hi[8], lo[8];  // the K-step's 16 nodes as FP16 pairs
-#pragma unroll
-                        for (int e = 0; e < 8; e++) half_split2(v[h][2 * e], v[h][2 * e + 1], hi[e], lo[e]);
-                        unsigned char *bh = B + (2 * k) * C::B_KS + off, *bl = B + (2 * k + 1) * C::B_KS + off;
-                        *(uint4 *)bh = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-                        *(uint4 *)(bh + 128) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
-                        *(uint4 *)bl = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-                        *(uint4 *)(bl + 128) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
-                    }
-                }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                tc_arrive(&full[s]);
-                if (++s == (unsigned)S) s = 0, ph ^= 1u, wrapped = true;
-            }
-        }
     } else {
         // ---- epilogue: warp w reads tensor-memory lanes 32 (w mod 4) .. + 31
         // (its 32 x cells); of each tile's 16-column chunks (rows), warps
-        // 6-9 take the even ones and warps 10-13 the odd ones, loading the
-        // next chunk while the current one is stored
+        // 2-5 take the even ones and warps 6-9 the odd ones, loading the next
+        // chunk while the current one is stored
         const int qd = warp & 3, hf = (warp - TC_EPI0 / 32) >> 2;
         const int xl = 32 * qd + lane;
         const AmStep st = am_step(p, m, ctl->timestep + 1);
-        // the sums are of (2^14 X) (sB YZ): back to X YZ, times Tfront
+        // the sums are of (2^14 X) (sB YZ): back to X YZ, times Tfront.  T =
+        // liniT + tf sum in FP32 with tf and liniT each as a head and the
+        // FP32 rounding of its remainder: two roundings (the FMA of the heads
+        // and the final addition) against one for the FP64 form of the same
+        // expression, no FP32-FP64 conversions
         const double tf = st.Tfront / (16384.0 * am_b_scale(st));
+        const float tf_h = (float)tf, tf_l = (float)(tf - (double)tf_h);
+        const float li_h = (float)st.liniT, li_l = (float)(st.liniT - (double)li_h);
         // kernel parameters in registers: a store through T32 might alias
         // the parameter block as far as the compiler knows, so every read of
         // it after a store would be a load again
@@ -512,9 +429,8 @@ __global__ void __launch_bounds__(TC_NT, 1)
             const unsigned col = tmem + ((unsigned)(32 * qd) << 16) + (unsigned)(b * 2 * NB);
             // T of rows r0 + cc .. + 15 from the chunk's two accumulators.  The
             // sixteen values are formed first, free of the row walk's
-            // branches, so that their conversions and FP64 multiply-adds
-            // overlap; then they are stored, in one run when the rows stay in
-            // one z plane.
+            // branches, so that their arithmetic overlaps; then they are
+            // stored, in one run when the rows stay in one z plane.
             auto store16 = [&](int cc, const unsigned (&vh)[16], const unsigned (&vx)[16]) {
                 if (!xin) return;
                 float Tv[16];
@@ -522,7 +438,7 @@ __global__ void __launch_bounds__(TC_NT, 1)
                 for (int j = 0; j < 16; j++) {
                     // the two accumulators (the cross sum is ~2^-11 of the other)
                     const float sum = __uint_as_float(vh[j]) + __uint_as_float(vx[j]);
-                    Tv[j] = (float)(st.liniT + tf * (double)sum);
+                    Tv[j] = __fadd_rn(__fmaf_rn(tf_h, sum, li_h), __fmaf_rn(tf_l, sum, li_l));
                 }
                 long long R = r0 + cc;
                 if (ny >= N && R + 16 <= nrows) {
@@ -564,14 +480,14 @@ __global__ void __launch_bounds__(TC_NT, 1)
             int cc = 16 * hf;
             if (cc < N) {
                 tmem_ld16(col + (unsigned)cc, ha);
-                tmem_ld16(col + (unsigned)(NB + cc), xa);
+                tmem_ld16(col + (unsigned)(N + cc), xa);
             }
             tmem_wait_ld(ha, xa);
             while (cc < N) {
                 const int c1 = cc + 32;
                 if (c1 < N) {
                     tmem_ld16(col + (unsigned)c1, hb);
-                    tmem_ld16(col + (unsigned)(NB + c1), xb);
+                    tmem_ld16(col + (unsigned)(N + c1), xb);
                 }
                 store16(cc, ha, xa);
                 tmem_wait_ld(hb, xb);
@@ -579,7 +495,7 @@ __global__ void __launch_bounds__(TC_NT, 1)
                 const int c2 = c1 + 32;
                 if (c2 < N) {
                     tmem_ld16(col + (unsigned)c2, ha);
-                    tmem_ld16(col + (unsigned)(NB + c2), xa);
+                    tmem_ld16(col + (unsigned)(N + c2), xa);
                 }
                 store16(c1, hb, xb);
                 tmem_wait_ld(ha, xa);
@@ -597,6 +513,51 @@ __global__ void __launch_bounds__(TC_NT, 1)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
     }
+}
+
+// The B operand image of a step: for every (y, z) row R (row R mod N of
+// block R / N) and K-step k, the 16 scaled products sB Y_i(y) Z_i(z) of the
+// K-step's nodes as FP16 head and remainder, in the layout the contraction's
+// stages copy as they are (the rows of the last block past the last row are
+// zero).  One thread per (row, K-step), consecutive rows across a warp; the
+// Y and Z rows come from the node-contiguous copies k_am_tables writes.
+__global__ void __launch_bounds__(256) k_am_bimg(const __grid_constant__ KernelArgs a,
+                                                 const __grid_constant__ AmParams m, int N)
+{
+    const Ctl *ctl = a.d.ctl;
+    if (stalled(ctl)) return;
+    const Geo &g = a.g;
+    const int ny = g.gy + 2, nz = g.gz + 2;
+    const long long nrows = (long long)ny * nz, rp = (nrows + N - 1) / N * N;
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= rp * TC_NKS) return;
+    const int k = (int)(e / rp);
+    const long long R = e - k * rp, rb = R / N;
+    const int n = (int)(R - rb * N), BN = N * TC_KE * 2;
+    uint4 h0 = make_uint4(0, 0, 0, 0), h1 = h0, l0 = h0, l1 = h0;
+    if (R < nrows) {
+        const int K = (int)(R / ny), J = (int)(R - (long long)K * ny);
+        const float4 *y = (const float4 *)(am_yt(a.d.am_ximg, g.gx) + (long long)J * AM_NT + k * TC_KE);
+        const float4 *z = (const float4 *)(am_zt(a.d.am_ximg, g.gx, g.gy) + (long long)K * AM_NT + k * TC_KE);
+        const float sB = (float)am_b_scale(am_step(a.p, m, ctl->timestep + 1));
+        unsigned hi[8], lo[8];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float4 yv = __ldg(y + q), zv = __ldg(z + q);
+            half_split2(yv.x * zv.x * sB, yv.y * zv.y * sB, hi[2 * q], lo[2 * q]);
+            half_split2(yv.z * zv.z * sB, yv.w * zv.w * sB, hi[2 * q + 1], lo[2 * q + 1]);
+        }
+        h0 = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        h1 = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+        l0 = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        l1 = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+    }
+    unsigned char *dst = am_bimg(a.d.am_ximg, g.gx, g.gy, g.gz) + (rb * TC_NKS + k) * 2 * BN + (n >> 3) * 256 +
+                         (n & 7) * 16;
+    *(uint4 *)dst = h0;
+    *(uint4 *)(dst + 128) = h1;
+    *(uint4 *)(dst + BN) = l0;
+    *(uint4 *)(dst + BN + 128) = l1;
 }
 
 // Temperature of the halo columns x = 0 and gx + 1 from the tables of step
@@ -665,14 +626,18 @@ int am_tc_prepare()
                                 TcCfg<256>::SMEM) == cudaSuccess;
 }
 
-long long am_ximg_size(int gx, int gy, int gz) { return am_ximg_part(gx) + (long long)(gy + gz + 4) * AM_NT; }
+long long am_ximg_size(int gx, int gy, int gz)
+{
+    return am_ximg_part(gx) + (long long)(gy + gz + 4) * AM_NT + am_bimg_part(gy, gz);
+}
 
 // rows: 256-row tiles (one accumulator set), 64-128 rows (two), 0 = 128.
-// A tile's cost is mostly per stage (its A copy, its MMAs' fixed costs), so
-// the largest tile with two accumulator sets is the default even where
-// smaller tiles would deal more evenly over the SMs (measured at
-// 512 x 256 x 128: 128 rows 0.160 ms, 112 0.175, 96 0.182, 64 0.250, 256
-// 0.228, tables included).
+// With two sets a tile's epilogue overlaps the next tile's MMAs; 256-row
+// tiles take fewer, larger MMAs per node (three N = 256 against two N = 256
+// and two N = 128 for the same products) and fewer stages, which outweighs
+// their epilogue running alone at 512 x 256 x 128 (tables and B image
+// included: 128 rows 0.125 ms, 112 0.132, 96 0.139, 80 0.157, 64 0.178, 256
+// 0.113); mms_autotune times 128 and 256 on the domain.
 int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, int rows)
 {
     const Geo &g = a.g;
@@ -684,9 +649,11 @@ int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, 
     const long long ntiles = (long long)ntx * ((nrows + N - 1) / N);
     const unsigned grid = (unsigned)(ntiles < nsm ? ntiles : nsm);
     cudaStream_t st = (cudaStream_t)stream;
+    const long long be = (nrows + N - 1) / N * N * TC_NKS;
+    k_am_bimg<<<(unsigned)((be + 255) / 256), 256, 0, st>>>(a, m, N);
     if (wide) k_am_contract_tc<256><<<grid, TC_NT, TcCfg<256>::SMEM, st>>>(a, m, N, ntx, ntiles);
     else k_am_contract_tc<128><<<grid, TC_NT, TcCfg<128>::SMEM, st>>>(a, m, N, ntx, ntiles);
-    int n = 1;
+    int n = 2;
     if (a.d.lsindex) {
         // the layer flag is kept for every cell, halo columns included
         const long long e = 2 * nrows;

@@ -88,7 +88,10 @@ constexpr int AM_NT = 400;
 // The FP32 form's tensor-core operand buffer (a.d.am_ximg): the X image of
 // am_tc.cu (2^14 X as FP16 head and remainder: [x tile of 128][K-step of 16
 // nodes][head, remainder][128 x 16 halves]), then Y and Z with the 400 nodes
-// contiguous for each row (YT[J][i], ZT[K][i], FP32).  Sizes in floats.
+// contiguous for each row (YT[J][i], ZT[K][i], FP32), then the B image (the
+// scaled products Y Z as FP16 head and remainder: [block of N (y, z)
+// rows][K-step][head, remainder][N x 16 halves], N the contraction's tile
+// height, room for any N up to 256).  Sizes in floats.
 __host__ __device__ constexpr long long am_ximg_part(int gx)
 {
     return (long long)((gx + 127) / 128) * (AM_NT / 16) * 2 * (128 * 16) / 2;
@@ -98,6 +101,15 @@ __host__ __device__ inline float *am_yt(float *img, int gx) { return img + am_xi
 __host__ __device__ inline float *am_zt(float *img, int gx, int gy)
 {
     return img + am_ximg_part(gx) + (long long)(gy + 2) * AM_NT;
+}
+__host__ __device__ inline unsigned char *am_bimg(float *img, int gx, int gy, int gz)
+{
+    return (unsigned char *)(img + am_ximg_part(gx) + (long long)(gy + gz + 4) * AM_NT);
+}
+// 2 x 2 bytes per node and row: one float per node and row
+__host__ __device__ constexpr long long am_bimg_part(int gy, int gz)
+{
+    return ((long long)(gy + 2) * (gz + 2) + 255) * AM_NT;
 }
 
 // The step the AM tables (k_am_tables: X, Y, Z, then the per-plane flags
