@@ -519,27 +519,31 @@ __global__ void __launch_bounds__(TC_NT, 1)
 // block R / N) and K-step k, the 16 scaled products sB Y_i(y) Z_i(z) of the
 // K-step's nodes as FP16 head and remainder, in the layout the contraction's
 // stages copy as they are (the rows of the last block past the last row are
-// zero).  One thread per (row, K-step), consecutive rows across a warp; the
-// Y and Z rows come from the node-contiguous copies k_am_tables writes.
+// zero).  Grid: x over rows (consecutive rows across a warp), y over
+// K-steps; the scale is formed once per CTA.  The Y and Z rows come from the
+// node-contiguous copies k_am_tables writes.
 __global__ void __launch_bounds__(256) k_am_bimg(const __grid_constant__ KernelArgs a,
                                                  const __grid_constant__ AmParams m, int N)
 {
     const Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
+    __shared__ float s_sB;
+    if (threadIdx.x == 0) s_sB = (float)am_b_scale(am_step(a.p, m, ctl->timestep + 1));
+    __syncthreads();
     const Geo &g = a.g;
     const int ny = g.gy + 2, nz = g.gz + 2;
-    const long long nrows = (long long)ny * nz, rp = (nrows + N - 1) / N * N;
-    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (e >= rp * TC_NKS) return;
-    const int k = (int)(e / rp);
-    const long long R = e - k * rp, rb = R / N;
-    const int n = (int)(R - rb * N), BN = N * TC_KE * 2;
+    const unsigned nrows = (unsigned)ny * (unsigned)nz, rp = (nrows + N - 1) / N * N;
+    const unsigned R = blockIdx.x * blockDim.x + threadIdx.x;
+    if (R >= rp) return;
+    const int k = blockIdx.y;
+    const unsigned rb = R / (unsigned)N;
+    const int n = (int)(R - rb * (unsigned)N), BN = N * TC_KE * 2;
     uint4 h0 = make_uint4(0, 0, 0, 0), h1 = h0, l0 = h0, l1 = h0;
     if (R < nrows) {
-        const int K = (int)(R / ny), J = (int)(R - (long long)K * ny);
+        const unsigned K = R / (unsigned)ny, J = R - K * (unsigned)ny;
         const float4 *y = (const float4 *)(am_yt(a.d.am_ximg, g.gx) + (long long)J * AM_NT + k * TC_KE);
         const float4 *z = (const float4 *)(am_zt(a.d.am_ximg, g.gx, g.gy) + (long long)K * AM_NT + k * TC_KE);
-        const float sB = (float)am_b_scale(am_step(a.p, m, ctl->timestep + 1));
+        const float sB = s_sB;
         unsigned hi[8], lo[8];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
@@ -552,8 +556,8 @@ __global__ void __launch_bounds__(256) k_am_bimg(const __grid_constant__ KernelA
         l0 = make_uint4(lo[0], lo[1], lo[2], lo[3]);
         l1 = make_uint4(lo[4], lo[5], lo[6], lo[7]);
     }
-    unsigned char *dst = am_bimg(a.d.am_ximg, g.gx, g.gy, g.gz) + (rb * TC_NKS + k) * 2 * BN + (n >> 3) * 256 +
-                         (n & 7) * 16;
+    unsigned char *dst = am_bimg(a.d.am_ximg, g.gx, g.gy, g.gz) + ((long long)rb * TC_NKS + k) * 2 * BN +
+                         (n >> 3) * 256 + (n & 7) * 16;
     *(uint4 *)dst = h0;
     *(uint4 *)(dst + 128) = h1;
     *(uint4 *)(dst + BN) = l0;
@@ -649,8 +653,8 @@ int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, 
     const long long ntiles = (long long)ntx * ((nrows + N - 1) / N);
     const unsigned grid = (unsigned)(ntiles < nsm ? ntiles : nsm);
     cudaStream_t st = (cudaStream_t)stream;
-    const long long be = (nrows + N - 1) / N * N * TC_NKS;
-    k_am_bimg<<<(unsigned)((be + 255) / 256), 256, 0, st>>>(a, m, N);
+    const long long rp = (nrows + N - 1) / N * N;
+    k_am_bimg<<<dim3((unsigned)((rp + 255) / 256), TC_NKS), 256, 0, st>>>(a, m, N);
     if (wide) k_am_contract_tc<256><<<grid, TC_NT, TcCfg<256>::SMEM, st>>>(a, m, N, ntx, ntiles);
     else k_am_contract_tc<128><<<grid, TC_NT, TcCfg<128>::SMEM, st>>>(a, m, N, ntx, ntiles);
     int n = 2;
