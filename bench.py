@@ -838,6 +838,8 @@ def profile_arm(args) -> None:
     if args.tile != "auto":
         cpt, zc = (int(v) for v in args.tile.split(","))
         dom.set_stencil_tile(cpt, zc)
+    if args.am_tile:
+        dom.set_am_tile(args.am_tile)
     dom.step(args.warmup + args.steps)
     # --reduce R: R rounds of a step with the fraction-solid tile sums
     # (mms_step_reduce), a plain step and a field pass (mms_reduce)
@@ -1153,6 +1155,8 @@ def main() -> None:
     ap.add_argument("--reduce", type=int, default=0,
                     help="profile mode: rounds of (step with tile sums, plain step, field reduction) after the steps")
     ap.add_argument("--tile", default="auto", help="profile mode: stencil tile 'cells_per_thread,zchunk'")
+    ap.add_argument("--am-tile", type=int, default=0,
+                    help="profile mode: rows per tile of the FP32 AM contraction (mms_set_am_tile; 0 = default)")
     ap.add_argument("--workload", default=None, choices=["am", "ds256", "adjoint", "ensemble", "slabs"],
                     help="am: the AM melt-pool deck, the headline line (default); ds256, adjoint, "
                          "ensemble, slabs: the 256^3 directional-solidification, adjoint calibration, "
