@@ -476,6 +476,14 @@ __global__ void __launch_bounds__(TC_NT, 1)
                     }
                 }
             };
+            // the accumulator set is released as soon as this thread's last
+            // tensor-memory load has completed, before that chunk is stored
+            bool released = false;
+            auto release = [&]() {
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                tc_arrive(&acce[b]);
+                released = true;
+            };
             unsigned ha[16], xa[16], hb[16], xb[16];
             int cc = 16 * hf;
             if (cc < N) {
@@ -488,21 +496,25 @@ __global__ void __launch_bounds__(TC_NT, 1)
                 if (c1 < N) {
                     tmem_ld16(col + (unsigned)c1, hb);
                     tmem_ld16(col + (unsigned)(N + c1), xb);
+                } else {
+                    release();
                 }
                 store16(cc, ha, xa);
-                tmem_wait_ld(hb, xb);
                 if (c1 >= N) break;
+                tmem_wait_ld(hb, xb);
                 const int c2 = c1 + 32;
                 if (c2 < N) {
                     tmem_ld16(col + (unsigned)c2, ha);
                     tmem_ld16(col + (unsigned)(N + c2), xa);
+                } else {
+                    release();
                 }
                 store16(c1, hb, xb);
+                if (c2 >= N) break;
                 tmem_wait_ld(ha, xa);
                 cc = c2;
             }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            tc_arrive(&acce[b]);
+            if (!released) release();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
