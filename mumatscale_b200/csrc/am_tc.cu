@@ -67,6 +67,8 @@
 // a shared abort flag that ends every other role's waits, then each role
 // drains what it has in flight (bulk copies, committed MMAs) before the
 // tensor memory is freed.
+#include <cstring>
+
 #include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -94,7 +96,13 @@ struct TcCfg {
     static constexpr int A_ST = KS * TC_A_CH;               // A bytes of a full stage
     static constexpr int STAGE = A_ST + KS * 2 * B_KS;      // 32 KB (N = 128) or 24 KB (N = 256)
     static constexpr int S = NB == 128 ? 7 : 8;             // stages in the ring
-    static constexpr int SMEM = S * STAGE + 128;            // + alignment of the ring
+    // 256-row tiles: the epilogue hands T to the tensor-store engine through
+    // staging buffers (two per group of four warps, 16 rows x 128 x cells
+    // of FP32 each), so that its stores drain while the next tile's MMAs run
+    static constexpr bool TST = NB == 256;
+    static constexpr int STG_BYTES = 16 * TC_M * 4;
+    static constexpr int STG = TST ? 4 * STG_BYTES : 0;
+    static constexpr int SMEM = S * STAGE + STG + 128;      // + alignment of the ring
     static constexpr int BUFS = NB == 128 ? 2 : 1;          // accumulator sets (2 NB columns each)
     // Stage c holds the K-steps (16-node chunks of the node order) lo(c) ..
     // lo(c) + nk(c) - 1: the stages run from the oldest nodes (the highest
@@ -233,7 +241,7 @@ __device__ __forceinline__ void tmem_wait_ld(unsigned (&a)[16], unsigned (&b)[16
 template <int NB>
 __global__ void __launch_bounds__(TC_NT, 1)
     k_am_contract_tc(const __grid_constant__ KernelArgs a, const __grid_constant__ AmParams m, int N, int ntx,
-                     long long ntiles)
+                     long long ntiles, const __grid_constant__ CUtensorMap tmap, int tst)
 {
     using C = TcCfg<NB>;
     constexpr int S = C::S;
@@ -409,6 +417,13 @@ __global__ void __launch_bounds__(TC_NT, 1)
         const double Tliq = p.Tliq;
         const long long sy = g.sy, sz = g.sz;
         const int gx = g.gx;
+        // tensor stores: this group's staging buffers, the chunks it has
+        // staged (the same count in its four warps), its issuing thread
+        const bool use_tst = C::TST && tst && !lsx;
+        float *const stg = (float *)(ring + S * C::STAGE + hf * 2 * C::STG_BYTES);
+        unsigned staged = 0;
+        const bool issuer = qd == 0 && lane == 0;
+        const unsigned bar_id = 1 + hf;
         long long tl = 0;
         for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, tl++) {
             const int xt = (int)(t % ntx);
@@ -420,9 +435,23 @@ __global__ void __launch_bounds__(TC_NT, 1)
             // the wait so that the loads are not on the chunks' path
             const int K0 = (int)(r0 / ny), J0 = (int)(r0 - (long long)K0 * ny);
             const bool on0 = zon[K0] != 0, on1 = K0 + 1 < nz && zon[K0 + 1] != 0;
-            const bool got = tc_wait(&accf[b], (unsigned)(use & 1), abort);
-            // the warp-wide tcgen05.ld below needs the whole warp, converged
-            if (!__all_sync(0xffffffffu, got)) break;
+            // the warp-wide tcgen05.ld below needs the whole warp, converged;
+            // with tensor stores the four warps of a group (which meet at
+            // named barriers) leave together too
+            bool got = __all_sync(0xffffffffu, tc_wait(&accf[b], (unsigned)(use & 1), abort));
+            if (C::TST) {
+                unsigned all;
+                asm volatile(
+                    "{\n\t.reg .pred p, q;\n\t"
+                    "setp.ne.u32 q, %1, 0;\n\t"
+                    "bar.red.and.pred p, %2, 128, q;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}"
+                    : "=r"(all)
+                    : "r"(got ? 1u : 0u), "r"(bar_id)
+                    : "memory");
+                got = all != 0;
+            }
+            if (!got) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int x = 1 + TC_M * xt + xl;
             const bool xin = x <= gx;
@@ -432,6 +461,37 @@ __global__ void __launch_bounds__(TC_NT, 1)
             // branches, so that their arithmetic overlaps; then they are
             // stored, in one run when the rows stay in one z plane.
             auto store16 = [&](int cc, const unsigned (&vh)[16], const unsigned (&vx)[16]) {
+                int Jc = J0 + cc, Kc = K0;
+                bool onc = on0;
+                if (Jc >= ny) Jc -= ny, Kc++, onc = on1;
+                if (use_tst && ny >= N && Jc + 16 <= ny) {
+                    // the chunk's 16 rows lie in plane Kc (rows past the last
+                    // plane and x cells past gx are outside the tensor map and
+                    // not written): stage them, then one thread of the group
+                    // issues the tensor store
+                    float *buf = stg + (staged & 1) * (C::STG_BYTES / 4);
+#pragma unroll
+                    for (int j = 0; j < 16; j++) {
+                        const float sum = __uint_as_float(vh[j]) + __uint_as_float(vx[j]);
+                        const float T = __fadd_rn(__fmaf_rn(tf_h, sum, li_h), __fmaf_rn(tf_l, sum, li_l));
+                        buf[j * TC_M + xl] = onc ? T : 0.f;
+                    }
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    asm volatile("bar.sync %0, 128;" ::"r"(bar_id) : "memory");
+                    if (issuer) {
+                        asm volatile(
+                            "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                                (unsigned long long)&tmap),
+                            "r"(4 + TC_M * xt), "r"(Jc), "r"(Kc), "r"(smem_addr(buf))
+                            : "memory");
+                        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                        // the buffer the next chunk fills was read by the store before this one
+                        asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                    }
+                    asm volatile("bar.sync %0, 128;" ::"r"(bar_id) : "memory");
+                    staged++;
+                    return;
+                }
                 if (!xin) return;
                 float Tv[16];
 #pragma unroll
@@ -516,6 +576,9 @@ __global__ void __launch_bounds__(TC_NT, 1)
             }
             if (!released) release();
         }
+        // the tensor stores complete (their shared-memory reads and their
+        // writes) before the CTA leaves
+        if (C::TST && issuer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -667,8 +730,13 @@ int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, 
     cudaStream_t st = (cudaStream_t)stream;
     const long long rp = (nrows + N - 1) / N * N;
     k_am_bimg<<<dim3((unsigned)((rp + 255) / 256), TC_NKS), 256, 0, st>>>(a, m, N);
-    if (wide) k_am_contract_tc<256><<<grid, TC_NT, TcCfg<256>::SMEM, st>>>(a, m, N, ntx, ntiles);
-    else k_am_contract_tc<128><<<grid, TC_NT, TcCfg<128>::SMEM, st>>>(a, m, N, ntx, ntiles);
+    // the temperature as a tensor-store target for 256-row tiles (the host
+    // encodes it at every launch; launches are captured into graphs once)
+    CUtensorMap tmap;
+    std::memset(&tmap, 0, sizeof tmap);
+    const int tst = wide && encode_t32_store(&tmap, a, TC_M, 16) ? 1 : 0;
+    if (wide) k_am_contract_tc<256><<<grid, TC_NT, TcCfg<256>::SMEM, st>>>(a, m, N, ntx, ntiles, tmap, tst);
+    else k_am_contract_tc<128><<<grid, TC_NT, TcCfg<128>::SMEM, st>>>(a, m, N, ntx, ntiles, tmap, tst);
     int n = 2;
     if (a.d.lsindex) {
         // the layer flag is kept for every cell, halo columns included

@@ -2434,6 +2434,28 @@ static bool encode3d(CUtensorMap *m, CUtensorMapDataType dt, int es, void *field
               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The FP32 temperature field as the target of tensor stores of the AM
+// contraction's epilogue (am_tc.cu): x extent gx + 1 + lead, so that a box
+// reaching past the last interior cell leaves the right halo column
+// untouched; boxes of bx x by x 1.  False when the encoder refuses or the
+// field is not laid out with its lead.
+bool encode_t32_store(void *map, const KernelArgs &a, int bx, int by)
+{
+    EncodeTiledFn fn = encode_fn();
+    const Geo &g = a.g;
+    if (!fn || !a.d.T32) return false;
+    const int es = 4, lead = 16 / es - 1;
+    char *base = (char *)a.d.T32 - (long long)lead * es;
+    if (((unsigned long long)base & 15ULL) != 0 || g.P < g.gx + 2 + lead) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)(g.gx + 1 + lead), (cuuint64_t)(g.gy + 2), (cuuint64_t)(g.gz + 2)};
+    cuuint64_t strides[2] = {(cuuint64_t)(g.P * es), (cuuint64_t)(g.P * (g.gy + 2) * es)};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    return fn((CUtensorMap *)map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <typename Real, int CPT>
 static int make_tma_t(const KernelArgs &a, TmaHolder &out)
 {

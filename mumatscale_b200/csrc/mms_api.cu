@@ -865,33 +865,42 @@ mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchu
     cudaEventCreate(&e1);
     double best = 1e300;
     Cand pick{ctx->tma.cpt, ctx->tma.zc};
+    // the candidates' launches interleaved round by round, so that a drift
+    // of the clocks during the tuning weighs on every candidate alike
+    std::vector<TmaHolder> ths;
+    std::vector<Cand> live;
     for (const Cand &cd : cands) {
         TmaHolder th{};
         th.cpt = cd.cpt;
         th.zc = cd.zc;
         if (ctx->tma.ok && !make_tma(sa, ctx->prec, th)) continue;
-        std::vector<float> ms;
-        for (int r = 0; r < reps + 2; r++) {
+        ths.push_back(th);
+        live.push_back(cd);
+    }
+    std::vector<std::vector<float>> ms(live.size());
+    for (int r = 0; r < reps + 2; r++)
+        for (size_t c = 0; c < live.size(); c++) {
             cudaEventRecord(e0, ctx->stream);
-            launch_stencil(sa, th, ctx->prec, ctx->stream);
+            launch_stencil(sa, ths[c], ctx->prec, ctx->stream);
             cudaEventRecord(e1, ctx->stream);
             cudaEventSynchronize(e1);
             float t = 0.f;
             cudaEventElapsedTime(&t, e0, e1);
-            if (r >= 2) ms.push_back(t);
+            if (r >= 2) ms[c].push_back(t);
         }
-        if ((e = cudaGetLastError()) != cudaSuccess) {
-            cudaEventDestroy(e0);
-            cudaEventDestroy(e1);
-            release();
-            ctx->err = std::string("autotune launch: ") + cudaGetErrorString(e);
-            return MMS_ERR_CUDA;
-        }
-        std::sort(ms.begin(), ms.end());
-        double med = ms[ms.size() / 2];
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        release();
+        ctx->err = std::string("autotune launch: ") + cudaGetErrorString(e);
+        return MMS_ERR_CUDA;
+    }
+    for (size_t c = 0; c < live.size(); c++) {
+        std::sort(ms[c].begin(), ms[c].end());
+        const double med = ms[c][ms[c].size() / 2];
         if (med < best) {
             best = med;
-            pick = cd;
+            pick = live[c];
         }
     }
     // FP32 AM form: the contraction's tile (128-row tiles with two
@@ -913,21 +922,23 @@ mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchu
         if (sls) sa.d.lsindex = (int *)sls;
         const AmParams m = am_params(ctx->p);
         double best_am = 1e300;
-        for (int rows : {0, 256}) {
-            std::vector<float> ms;
-            for (int r = 0; r < reps + 2; r++) {
+        const int am_cands[2] = {0, 256};
+        std::vector<float> am_ms[2];
+        for (int r = 0; r < reps + 2; r++)
+            for (int ci = 0; ci < 2; ci++) {
                 cudaEventRecord(e0, ctx->stream);
-                launch_temp_am(sa, m, ctx->prec, ctx->stream, nullptr, rows);
+                launch_temp_am(sa, m, ctx->prec, ctx->stream, nullptr, am_cands[ci]);
                 cudaEventRecord(e1, ctx->stream);
                 cudaEventSynchronize(e1);
                 float t = 0.f;
                 cudaEventElapsedTime(&t, e0, e1);
-                if (r >= 2) ms.push_back(t);
+                if (r >= 2) am_ms[ci].push_back(t);
             }
-            std::sort(ms.begin(), ms.end());
-            if (ms[ms.size() / 2] < best_am) {
-                best_am = ms[ms.size() / 2];
-                am_rows = rows;
+        for (int ci = 0; ci < 2; ci++) {
+            std::sort(am_ms[ci].begin(), am_ms[ci].end());
+            if (am_ms[ci][am_ms[ci].size() / 2] < best_am) {
+                best_am = am_ms[ci][am_ms[ci].size() / 2];
+                am_rows = am_cands[ci];
             }
         }
         Ctl c2 = c;

@@ -310,6 +310,8 @@ struct AmParams {
 // them into a temperature download buffer from the tables of the current
 // step (they are computed every step when the layer flag lsindex is kept).
 int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, int rows);
+// the FP32 temperature as a tensor-store target (kernels.cu; map: a CUtensorMap)
+bool encode_t32_store(void *map, const KernelArgs &a, int bx, int by);
 int launch_am_halo_fill(const KernelArgs &a, const AmParams &m, double *dev_out, void *stream);
 int am_tc_prepare();
 long long am_ximg_size(int gx, int gy, int gz);  // floats of a.d.am_ximg
