@@ -156,7 +156,11 @@ __global__ void k_am_tables(KernelArgs a, AmParams m)
     if (stalled(ctl)) return;
     const Geo &g = a.g;
     const Phys &p = a.p;
-    const AmStep s = am_step(p, m, ctl->timestep + 1);
+    // the step's source position and constants, formed once per CTA
+    __shared__ AmStep s_step;
+    if (threadIdx.x == 0) s_step = am_step(p, m, ctl->timestep + 1);
+    __syncthreads();
+    const AmStep s = s_step;
     const int nx = g.gx + 2, ny = g.gy + 2, nz = g.gz + 2, nc = nx + ny + nz;
     Real *X = (Real *)a.d.am_tab, *Y = X + (long long)AM_NT * nx, *Z = Y + (long long)AM_NT * ny;
     int *zon = (int *)(Z + (long long)AM_NT * nz);
