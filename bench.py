@@ -659,6 +659,8 @@ def gpu_arm(args) -> None:
         out[form] = {"ms_total": ms, "launches": dom.kernel_launches - l0, "clocks": clk.summary(),
                      "tile": {"cells_per_thread": tile[0], "zchunk": tile[1], "cta_cells": [32 * tile[0], 8]},
                      "grains": dom.num_grains - 1}
+        if form == "f32":
+            out[form]["tile"]["am_rows"] = dom.am_tile()
         doms[form] = dom
     errors = _errors(doms["f32"], doms["f64"])
     for form, dom in doms.items():
@@ -683,7 +685,9 @@ def gpu_arm(args) -> None:
     o_ce = torch.empty(n, dtype=torch.float64).pin_memory()
     with M.Domain(params, precision=M.PREC_F32, device=dev) as dom:
         dom.set_stream(stream.cuda_stream)
+        # the tiles the tuner picked for this deck above
         dom.set_stencil_tile(out["f32"]["tile"]["cells_per_thread"], out["f32"]["tile"]["zchunk"])
+        dom.set_am_tile(out["f32"]["tile"]["am_rows"])
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
