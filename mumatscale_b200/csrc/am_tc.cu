@@ -49,10 +49,9 @@
 //                in this form) and the layer flag to global memory; two
 //                warps per group of 32 tensor-memory lanes, each taking every
 //                other 16 columns
-// Stages circulate in a shared-memory ring: with N = 128 seven stages of two
-// K-steps (32 nodes; A 16 KB, B 16 KB; the last stage of a tile holds the
-// one K-step left of 25), with N = 256 eight of one K-step (A 8 KB, B
-// 16 KB).  A stage costs each role a fixed handshake (a barrier wait, index
+// Stages of two K-steps (32 nodes; the last stage of a tile holds the one
+// K-step left of 25) circulate in a shared-memory ring: seven of 32 KB with
+// N = 128, four of 48 KB with N = 256.  A stage costs each role a fixed handshake (a barrier wait, index
 // arithmetic, a commit or an arrival) of several hundred cycles, so the
 // stages are as large as the ring allows.  With N = 128 the 512
 // tensor-memory columns hold two sets of accumulators, so a tile's epilogue
@@ -90,12 +89,12 @@ static_assert(AM_NT % TC_KE == 0, "nodes per K-step");
 
 template <int NB>
 struct TcCfg {
-    static constexpr int KS = NB == 128 ? 2 : 1;            // K-steps per stage
+    static constexpr int KS = 2;                            // K-steps per stage
     static constexpr int NCH = (TC_NKS + KS - 1) / KS;      // stages per tile (the last may hold fewer)
     static constexpr int B_KS = NB * TC_KE * 2;             // one K-step, one part of B, bytes, at N = NB
     static constexpr int A_ST = KS * TC_A_CH;               // A bytes of a full stage
-    static constexpr int STAGE = A_ST + KS * 2 * B_KS;      // 32 KB (N = 128) or 24 KB (N = 256)
-    static constexpr int S = NB == 128 ? 7 : 8;             // stages in the ring
+    static constexpr int STAGE = A_ST + KS * 2 * B_KS;      // 32 KB (N = 128) or 48 KB (N = 256)
+    static constexpr int S = NB == 128 ? 7 : 4;             // stages in the ring
     // 256-row tiles: the epilogue hands T to the tensor-store engine through
     // staging buffers (two per group of four warps, 16 rows x 128 x cells
     // of FP32 each), so that its stores drain while the next tile's MMAs run
