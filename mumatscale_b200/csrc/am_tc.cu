@@ -594,18 +594,20 @@ __global__ void __launch_bounds__(TC_NT, 1)
 // K-step's nodes as FP16 head and remainder, in the layout the contraction's
 // stages copy as they are (the rows of the last block past the last row are
 // zero).  Grid: x over rows (consecutive rows across a warp), y over
-// K-steps; the scale is formed once per CTA.  The Y and Z rows come from the
-// node-contiguous copies k_am_tables writes.
+// K-steps.  The Y and Z rows come from the node-contiguous copies
+// k_am_tables writes, the scale from the word it leaves after its step
+// marker.
 __global__ void __launch_bounds__(256) k_am_bimg(const __grid_constant__ KernelArgs a,
                                                  const __grid_constant__ AmParams m, int N)
 {
     const Ctl *ctl = a.d.ctl;
     if (stalled(ctl)) return;
-    __shared__ float s_sB;
-    if (threadIdx.x == 0) s_sB = (float)am_b_scale(am_step(a.p, m, ctl->timestep + 1));
-    __syncthreads();
     const Geo &g = a.g;
-    const int ny = g.gy + 2, nz = g.gz + 2;
+    const int nx = g.gx + 2, ny = g.gy + 2, nz = g.gz + 2;
+    // the step's scale, which k_am_tables leaves after its step marker
+    const float *tabs = (const float *)a.d.am_tab;
+    const int *zon = (const int *)(tabs + (long long)AM_NT * (nx + ny + nz));
+    (void)m;
     const unsigned nrows = (unsigned)ny * (unsigned)nz, rp = (nrows + N - 1) / N * N;
     const unsigned R = blockIdx.x * blockDim.x + threadIdx.x;
     if (R >= rp) return;
@@ -617,7 +619,7 @@ __global__ void __launch_bounds__(256) k_am_bimg(const __grid_constant__ KernelA
         const unsigned K = R / (unsigned)ny, J = R - K * (unsigned)ny;
         const float4 *y = (const float4 *)(am_yt(a.d.am_ximg, g.gx) + (long long)J * AM_NT + k * TC_KE);
         const float4 *z = (const float4 *)(am_zt(a.d.am_ximg, g.gx, g.gy) + (long long)K * AM_NT + k * TC_KE);
-        const float sB = s_sB;
+        const float sB = *am_tab_sb(zon, nz);
         unsigned hi[8], lo[8];
 #pragma unroll
         for (int q = 0; q < 4; q++) {

@@ -118,6 +118,9 @@ __device__ __forceinline__ unsigned long long *am_tab_step(const int *zon, int n
 {
     return (unsigned long long *)(((unsigned long long)(zon + nz) + 7ULL) & ~7ULL);
 }
+// FP32 form: the scale of the B operand (am_b_scale) of the step the tables
+// were built for, after the step marker (the FP32 tables leave the room)
+__device__ __forceinline__ float *am_tab_sb(const int *zon, int nz) { return (float *)(am_tab_step(zon, nz) + 1); }
 
 struct AmStep {
     double xnow, ynow, znow, lalpha, ls, ldt, Tfront, liniT;

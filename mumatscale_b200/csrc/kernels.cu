@@ -207,7 +207,10 @@ __global__ void k_am_tables(KernelArgs a, AmParams m)
             if (i == 0) zon[K] = (rz <= s.znow + p.cellSize) ? 1 : 0;
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) *am_tab_step(zon, nz) = ctl->timestep + 1;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *am_tab_step(zon, nz) = ctl->timestep + 1;
+        if (sizeof(Real) == 4) *am_tab_sb(zon, nz) = (float)am_b_scale(s);
+    }
 }
 
 // T over tiles of (XL MX) x-cells by (G MY) (y, z) rows, G = 256 / XL: each
