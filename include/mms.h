@@ -391,8 +391,8 @@ mms_status mms_set_stencil_tile(mms_ctx *ctx, int cells_per_thread, int zchunk);
 mms_status mms_get_stencil_tile(const mms_ctx *ctx, int *cells_per_thread, int *zchunk);
 /* FP32 form, moving-source (AM) temperature: rows per tile of its
  * tensor-core contraction (tiles of 128 x cells by `rows` (y, z) rows): 64 to
- * 128 in steps of 16, 256, or 0 = 128 (the default).  Results do not depend
- * on it. */
+ * 128 in steps of 16, 256, or 0 (the default) = 256 when the grid holds at
+ * least two 256-row tiles per SM, else 128.  Results do not depend on it. */
 mms_status mms_set_am_tile(mms_ctx *ctx, int rows);
 mms_status mms_get_am_tile(const mms_ctx *ctx, int *rows);
 /* Times every tile candidate on shadow copies of the fields the stencil

@@ -711,7 +711,8 @@ long long am_ximg_size(int gx, int gy, int gz)
     return am_ximg_part(gx) + (long long)(gy + gz + 4) * AM_NT + am_bimg_part(gy, gz);
 }
 
-// rows: 256-row tiles (one accumulator set), 64-128 rows (two), 0 = 128.
+// rows: 256-row tiles (one accumulator set), 64-128 rows (two), 0 = 256
+// when the grid has at least two 256-row tiles per SM, else 128.
 // With two sets a tile's epilogue overlaps the next tile's MMAs; 256-row
 // tiles take fewer, larger MMAs per node (three N = 256 against two N = 256
 // and two N = 128 for the same products) and fewer stages, which outweighs
@@ -724,6 +725,12 @@ int launch_am_contract_tc(const KernelArgs &a, const AmParams &m, void *stream, 
     const int ntx = (g.gx + TC_M - 1) / TC_M;
     const long long nrows = (long long)(g.gy + 2) * (g.gz + 2);
     const int nsm = sm_count();
+    if (rows == 0) {
+        // 256-row tiles when there are enough of them to keep every SM busy
+        // for two, else 128
+        const long long wide_tiles = (long long)ntx * ((nrows + 255) / 256);
+        rows = wide_tiles >= 2LL * nsm ? 256 : 128;
+    }
     const bool wide = rows == 256;
     const int N = wide ? 256 : (rows >= 64 && rows <= 128 ? rows / 16 * 16 : 128);
     const long long ntiles = (long long)ntx * ((nrows + N - 1) / N);

@@ -922,7 +922,7 @@ mms_status mms_autotune(mms_ctx *ctx, int reps, int *cells_per_thread, int *zchu
         if (sls) sa.d.lsindex = (int *)sls;
         const AmParams m = am_params(ctx->p);
         double best_am = 1e300;
-        const int am_cands[2] = {0, 256};
+        const int am_cands[2] = {128, 256};
         std::vector<float> am_ms[2];
         for (int r = 0; r < reps + 2; r++)
             for (int ci = 0; ci < 2; ci++) {

@@ -91,7 +91,8 @@ def test_am_fp32_form_error(built, cuda_device):
             assert rel < 1e-5, rel
 
 
-def test_am_fp32_form_cfg3_shape(built, cuda_device):
+@pytest.mark.parametrize("am_rows", [128, 256])
+def test_am_fp32_form_cfg3_shape(built, cuda_device, am_rows):
     """The FP32 form on the reduced melt-pool deck amsub4 (the AM source
     crossing a columnar substrate with bulk nucleation, 4 emulated ranks)
     against the FP64 plain form, which is pinned to the reference's dumps
@@ -100,13 +101,18 @@ def test_am_fp32_form_cfg3_shape(built, cuda_device):
     grain-id mismatch < 0.1 % of cells and solute (ce) relative L2 error
     < 1e-5, plus temperature max error < 1e-6 of its maximum and fs max
     error < 1e-3.  The laser turns on at step 8 and crosses the domain by
-    step 30; the run goes on to step 200 as the pool solidifies."""
+    step 30; the run goes on to step 200 as the pool solidifies.  Both
+    tile heights of the tensor-core contraction: 128 rows (two accumulator
+    sets) and 256 rows (one set; rows of 50 here, so every chunk is stored
+    directly)."""
     p = M.read_deck(golden_deck("amsub4"))
     doms = {prec: M.Domain(p, precision=prec) for prec in (M.PREC_F64, M.PREC_F32)}
     try:
         for d in doms.values():
             setup_golden_substrate(d, "amsub4")
         d64, d32 = doms[M.PREC_F64], doms[M.PREC_F32]
+        d32.set_am_tile(am_rows)
+        assert d32.am_tile() == am_rows
         for s in (20, 30, 60, 120, 200):
             for d in doms.values():
                 d.step(s - d.timestep)
@@ -126,6 +132,38 @@ def test_am_fp32_form_cfg3_shape(built, cuda_device):
     finally:
         for d in doms.values():
             d.close()
+
+
+def test_am_tile_heights_tensor_stores(built, cuda_device, tmp_path):
+    """The FP32 form's temperature with 256-row tiles on a grid whose y rows
+    fill them (64 x 256 x 16 cells: ny = 258 >= 256, so the epilogue stages
+    its chunks for tensor stores; one x block of 128 holds only 64 cells and
+    the last row tile is partial, both clipped by the tensor map; chunks
+    that cross a z plane are stored directly) against 128-row tiles (two
+    accumulator sets, direct stores) and against the FP64 form, with the
+    moving source inside the domain (step 14): within 1e-6 of the maximum."""
+    from mumatscale_b200 import workloads as W
+
+    dims = (64, 256, 16)
+    deck = tmp_path / "am_rows.in"
+    deck.write_text(W.am_track(dims, 1e-6))
+    p = M.read_deck(deck)
+    T = {}
+    for key, prec, rows in (("f64", M.PREC_F64, 0), ("r128", M.PREC_F32, 128), ("r256", M.PREC_F32, 256)):
+        with M.Domain(p, precision=prec) as d:
+            W.setup_substrate(d, dims[2] - 8, 1e-6)
+            if rows:
+                d.set_am_tile(rows)
+                assert d.am_tile() == rows
+            d.step(14)
+            T[key] = d.download("temperature").astype(np.float64)
+    tmax = float(np.abs(T["f64"]).max())
+    assert tmax > 1000.0  # the source is on and inside the domain
+    for key in ("r128", "r256"):
+        err = float(np.abs(T[key] - T["f64"]).max()) / tmax
+        assert err < 1e-6, f"{key}: {err:.3g}"
+    d_rows = float(np.abs(T["r256"] - T["r128"]).max()) / tmax
+    assert d_rows < 1e-6, f"256 vs 128 rows: {d_rows:.3g}"
 
 
 @pytest.mark.parametrize("name", ["small1", "small4", "grad1"])
