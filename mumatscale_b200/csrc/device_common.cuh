@@ -60,6 +60,9 @@ __device__ __forceinline__ double temp_cell(const Phys &p, const double *Tarr, c
 template <typename Real>
 struct PhysR {
     Real rs, rl, liq_slope, k_inv, km, km_inv, m_inv, D_xt, cinit, Tliq, gibbs, c0k;
+    // FP32 form: the liquidus rounded down to FP32, and as an FP32 head and
+    // the FP32 rounding of its remainder (FP32 temperature arrays)
+    float tliq_rd, tliq_h, tliq_l;
 };
 
 template <typename Real>
@@ -78,6 +81,9 @@ __device__ __forceinline__ PhysR<Real> phys_r(const Phys &p)
     q.Tliq = (Real)p.Tliq;
     q.gibbs = (Real)p.gibbs;
     q.c0k = (Real)(p.cinit * (p.k_inv - 1.0));
+    q.tliq_rd = __double2float_rd(p.Tliq);
+    q.tliq_h = (float)p.Tliq;
+    q.tliq_l = (float)(p.Tliq - (double)q.tliq_h);
     return q;
 }
 

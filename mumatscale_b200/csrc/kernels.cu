@@ -895,14 +895,68 @@ __device__ __forceinline__ Real diff_sum(const PhysR<Real> &q, Real conc, Real l
 }
 
 // fs_change_diffuse (growth.c:220-272) of one cell given its diffusion sum.
+// The fs change of the FP32 form from dT = T - Tliq and the range test
+// (off: T < 1 or T > Tliq), shared by the FP64- and FP32-temperature entries
+__device__ __forceinline__ void fs_update_f32(const PhysR<float> &q, const Phys &p, float conc, float lspfs,
+                                              float nbsum, float oce, int grc, float dT, bool off, const double *curv,
+                                              long long c, float &cen, float &cl_new, float &fs_new, int &gr_new,
+                                              int &br)
+{
+    using Real = float;
+    cen = oce + nbsum;
+    gr_new = grc;
+    Real c_int = q.m_inv * dT;               // c_int - Cinit
+    Real Tunder = -dT + q.liq_slope * conc;  // conc = cl - Cinit
+    if (grc <= 0 || off) {
+        cl_new = cen;
+        fs_new = 0;
+        gr_new = 0;
+        br = BR_RESET;
+    } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
+        cl_new = cen * q.k_inv + q.c0k;      // ce / k - Cinit
+        fs_new = lspfs;
+        br = BR_KEEP;
+    } else {
+        if (p.tip_curv) c_int = q.m_inv * (dT + q.gibbs * (Real)curv[c]);
+        // dce = the diffusion sum; dcl (u - 1/u terms) and dfs with the
+        // dce terms of growth.c:257-261 cancelled algebraically:
+        // dcl u - dce = (c_int - cl) 2 D_xt u
+        const float dce = (float)nbsum;
+        const float u = 1.f - (float)q.km * (float)lspfs;
+        const float t2 = ((float)c_int - (float)conc) * (2.f * (float)q.D_xt);
+        const float dcl = t2 + __fdividef(dce, u);
+        const float dfs = __fdividef(t2 * u * (float)q.km_inv, (float)conc + (float)q.cinit);
+        cl_new = conc + dcl;
+        fs_new = lspfs + dfs;
+        br = ((Real)1.0 < fs_new) ? BR_CLAMP : BR_GROW;
+        fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
+        if (fs_new < (Real)0.) {
+            fs_new = 0.;
+            gr_new = 0;
+            cl_new = cen;
+            br = BR_NEG;
+        }
+    }
+}
+
+// FP32 form with a temperature held in FP32 (the AM model's array): the
+// range test on that value exactly as fs_update makes it (x > Tliq exactly
+// when x > Tliq rounded down to FP32) and T - Tliq through Tliq's FP32 head
+// and remainder, with no FP32-FP64 conversions
+__device__ __forceinline__ void am_dt(const PhysR<float> &q, float Tf, float &dT, bool &off)
+{
+    dT = __fsub_rn(__fsub_rn(Tf, q.tliq_h), q.tliq_l);
+    off = Tf < 1.f || Tf > q.tliq_rd;
+}
+
 template <typename Real>
 __device__ __forceinline__ void fs_update(const PhysR<Real> &q, const Phys &p, Real conc, Real lspfs, Real nbsum,
                                           Real oce, int grc, double Td, const double *curv, long long c, Real &cen,
-                                          Real &cl_new, Real &fs_new, int &gr_new, int &br)
+                                          Real &cl_new, Real &fs_new, int &gr_new, int &br, bool t32 = false)
 {
     cen = oce + nbsum;
     gr_new = grc;
-    if (sizeof(Real) == 8) {
+    if constexpr (sizeof(Real) == 8) {
         // fs_change_diffuse, growth.c:220-272, operation for operation
         const Real Tcell = (Real)Td;
         Real c_int = q.cinit + q.m_inv * (Tcell - q.Tliq);
@@ -934,39 +988,18 @@ __device__ __forceinline__ void fs_update(const PhysR<Real> &q, const Phys &p, R
             }
         }
     } else {
-        const Real dT = (Real)(Td - p.Tliq);
-        Real c_int = q.m_inv * dT;               // c_int - Cinit
-        Real Tunder = -dT + q.liq_slope * conc;  // conc = cl - Cinit
-        if (grc <= 0 || Td < 1.0 || Td > p.Tliq) {
-            cl_new = cen;
-            fs_new = 0;
-            gr_new = 0;
-            br = BR_RESET;
-        } else if (lspfs == (Real)1.0 && (Tunder >= (Real)0.0)) {
-            cl_new = cen * q.k_inv + q.c0k;      // ce / k - Cinit
-            fs_new = lspfs;
-            br = BR_KEEP;
+        // t32: Td holds the value of an FP32 temperature array (the AM
+        // model), whose every path takes the FP32-temperature form of the
+        // test and the difference
+        float dT;
+        bool off;
+        if (t32) {
+            am_dt(q, (float)Td, dT, off);
         } else {
-            if (p.tip_curv) c_int = q.m_inv * (dT + q.gibbs * (Real)curv[c]);
-            // dce = the diffusion sum; dcl (u - 1/u terms) and dfs with the
-            // dce terms of growth.c:257-261 cancelled algebraically:
-            // dcl u - dce = (c_int - cl) 2 D_xt u
-            const float dce = (float)nbsum;
-            const float u = 1.f - (float)q.km * (float)lspfs;
-            const float t2 = ((float)c_int - (float)conc) * (2.f * (float)q.D_xt);
-            const float dcl = t2 + __fdividef(dce, u);
-            const float dfs = __fdividef(t2 * u * (float)q.km_inv, (float)conc + (float)q.cinit);
-            cl_new = conc + dcl;
-            fs_new = lspfs + dfs;
-            br = ((Real)1.0 < fs_new) ? BR_CLAMP : BR_GROW;
-            fs_new = ((Real)1.0 < fs_new) ? (Real)1.0 : fs_new;
-            if (fs_new < (Real)0.) {
-                fs_new = 0.;
-                gr_new = 0;
-                cl_new = cen;
-                br = BR_NEG;
-            }
+            dT = (float)(Td - p.Tliq);
+            off = Td < 1.0 || Td > p.Tliq;
         }
+        fs_update_f32(q, p, conc, lspfs, nbsum, oce, grc, dT, off, curv, c, cen, cl_new, fs_new, gr_new, br);
     }
 }
 
@@ -975,10 +1008,10 @@ __device__ __forceinline__ void cell_update(const PhysR<Real> &q, const Phys &p,
                                             const Real (&nb_cl)[6], const Real (&nb_fs)[6],
                                             const Real (&one_m)[6], bool interior, Real oce, int grc,
                                             double Td, const double *curv, long long c, Real &cen,
-                                            Real &cl_new, Real &fs_new, int &gr_new, int &br)
+                                            Real &cl_new, Real &fs_new, int &gr_new, int &br, bool t32 = false)
 {
     fs_update<Real>(q, p, conc, lspfs, diff_sum<Real>(q, conc, lspfs, nb_cl, nb_fs, one_m, interior), oce, grc, Td,
-                    curv, c, cen, cl_new, fs_new, gr_new, br);
+                    curv, c, cen, cl_new, fs_new, gr_new, br, t32);
 }
 
 constexpr int DTX = 32, DTY = 8;
@@ -1132,11 +1165,11 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
     // that its latency overlaps a plane of work
     const bool t_arr = p.temp_mode == 2;
     double Tn[CPT];
-#pragma unroll
     // (the FP32 form keeps it in FP32)
     auto t_load = [&](long long c) -> double {
         return sizeof(Real) == 4 ? (double)__ldg(a.d.T32 + c) : __ldg(a.d.T + c);
     };
+#pragma unroll
     for (int u = 0; u < CPT; u++) Tn[u] = (t_arr && act[u]) ? t_load(crow + i0 + tx + DTX * u) : 0.0;
     for (int t = 0; t <= k1 - k0; t++) {
         const int k = k0 + t;
@@ -1179,7 +1212,7 @@ __device__ __forceinline__ bool stencil_tile(const KernelArgs &a, const TmaMaps 
                 Real cen, cl_new, fs_new;
                 int gr_new, br;
                 cell_update<Real>(q, p, cc[h], fc[h], nb_cl, nb_fs, one_m, interior, oce, grc, Td, a.d.curv, c,
-                                  cen, cl_new, fs_new, gr_new, br);
+                                  cen, cl_new, fs_new, gr_new, br, sizeof(Real) == 4 && t_arr);
                 if (!in_bounds(ctl, c, g.N)) continue;
                 ce[c] = cen;
                 clO[c] = cl_new;
@@ -1271,7 +1304,10 @@ __device__ __forceinline__ typename Vec2<Real>::T vec2(Real x, Real y)
     return v;
 }
 
-template <typename Real>
+// TA: the FP32 form with an FP32 temperature array (the AM model), whose
+// cells take the FP32-temperature update; a separate instantiation, so that
+// the other forms' inner loop carries no trace of it
+template <typename Real, bool TA = false>
 __device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const TmaMaps &maps, int zchunk, int bx, int by,
                                                   int bz, unsigned char *smem, StencilShared<Depth<Real, 2>::TS> &sh,
                                                   unsigned &ring, double *part = nullptr, long long part_idx = 0)
@@ -1362,6 +1398,7 @@ __device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const Tma
     V zm_cl = vec2<Real>(0, 0), zc_cl = zm_cl, zm_fs = zm_cl, zc_fs = zm_cl;
     for (int t = 0; t <= k1 - k0; t++) {
         const int k = k0 + t;
+        const Real Tn0 = Tn.x, Tn1 = Tn.y;
         const double T0 = (double)Tn.x, T1 = (double)Tn.y;
         Tn = Tnn;
         if (t_arr && act0 && t + 1 < k1 - k0) Tnn = t_load(crow + 2 * g.sz + i);
@@ -1435,7 +1472,15 @@ __device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const Tma
             const double Td0 = t_per_plane ? Tp : (t_arr ? T0 : temp_cell(p, a.d.T, a.d.T32, c, j, k, ts));
             Real cen0, cl0, fs0;
             int g0, br0;
-            fs_update<Real>(q, p, zc_cl.x, zc_fs.x, nb0, oce.x, grc.x, Td0, a.d.curv, c, cen0, cl0, fs0, g0, br0);
+            if constexpr (sizeof(Real) == 4 && TA) {
+                // the FP32 temperature array straight into the FP32 update
+                float dT;
+                bool off;
+                am_dt(q, (float)Tn0, dT, off);
+                fs_update_f32(q, p, zc_cl.x, zc_fs.x, nb0, oce.x, grc.x, dT, off, a.d.curv, c, cen0, cl0, fs0, g0, br0);
+            } else {
+                fs_update<Real>(q, p, zc_cl.x, zc_fs.x, nb0, oce.x, grc.x, Td0, a.d.curv, c, cen0, cl0, fs0, g0, br0);
+            }
             if (sizeof(Real) == 8 ? cen0 < 0 : cen0 < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
             solid0 = g0 > 0;
             if (part) fsum += (double)fs0;
@@ -1443,8 +1488,16 @@ __device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const Tma
                 const double Td1 = t_per_plane ? Tp : (t_arr ? T1 : temp_cell(p, a.d.T, a.d.T32, c + 1, j, k, ts));
                 Real cen1, cl1, fs1;
                 int g1, br1;
-                fs_update<Real>(q, p, zc_cl.y, zc_fs.y, nb1, oce.y, grc.y, Td1, a.d.curv, c + 1, cen1, cl1, fs1, g1,
-                                br1);
+                if constexpr (sizeof(Real) == 4 && TA) {
+                    float dT;
+                    bool off;
+                    am_dt(q, (float)Tn1, dT, off);
+                    fs_update_f32(q, p, zc_cl.y, zc_fs.y, nb1, oce.y, grc.y, dT, off, a.d.curv, c + 1, cen1, cl1, fs1,
+                                  g1, br1);
+                } else {
+                    fs_update<Real>(q, p, zc_cl.y, zc_fs.y, nb1, oce.y, grc.y, Td1, a.d.curv, c + 1, cen1, cl1, fs1,
+                                    g1, br1);
+                }
                 if (sizeof(Real) == 8 ? cen1 < 0 : cen1 < -q.cinit) raise_error(ctl, MMS_ERR_NEGATIVE_CE);
                 solid1 = g1 > 0;
                 if (part) fsum += (double)fs1;
@@ -1526,7 +1579,9 @@ __device__ __forceinline__ bool run_tile(const KernelArgs &a, const TmaMaps &map
                                          double *part = nullptr, long long part_idx = 0)
 {
     if constexpr (CPT == 2 && sizeof(Real) == 4)
-        return stencil_tile_pair<Real>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
+        return a.p.temp_mode == 2
+                   ? stencil_tile_pair<Real, true>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx)
+                   : stencil_tile_pair<Real, false>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
     else
         return stencil_tile<Real, CPT>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
 }
@@ -1677,7 +1732,7 @@ __global__ void __launch_bounds__(DTX *DTY) k_diffuse_fs(KernelArgs a, int zchun
             int gr_new, br;
             const bool interior = i > 1 && i < g.gx && j > 1 && j < g.gy && k > 1 && k < g.gz;
             cell_update<Real>(q, p, s_cl[sc][ly][lx], s_fs[sc][ly][lx], nb_cl, nb_fs, one_m, interior, ce[c], grc,
-                              Td, a.d.curv, c, cen, cl_new, fs_new, gr_new, br);
+                              Td, a.d.curv, c, cen, cl_new, fs_new, gr_new, br, sizeof(Real) == 4 && p.temp_mode == 2);
             ce[c] = cen;
             clO[c] = cl_new;
             fsO[c] = fs_new;
