@@ -1304,10 +1304,12 @@ __device__ __forceinline__ typename Vec2<Real>::T vec2(Real x, Real y)
     return v;
 }
 
-// TA: the FP32 form with an FP32 temperature array (the AM model), whose
-// cells take the FP32-temperature update; a separate instantiation, so that
-// the other forms' inner loop carries no trace of it
-template <typename Real, bool TA = false>
+// TM, FP32 form only: 1 with an FP32 temperature array (the AM model), whose
+// cells take the FP32-temperature update; 2 with a temperature per plane,
+// whose difference from the liquidus and range test are formed once per
+// plane; 0 otherwise.  Separate instantiations, so that each inner loop
+// carries only its own form; all give what fs_update gives.
+template <typename Real, int TM = 0>
 __device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const TmaMaps &maps, int zchunk, int bx, int by,
                                                   int bz, unsigned char *smem, StencilShared<Depth<Real, 2>::TS> &sh,
                                                   unsigned &ring, double *part = nullptr, long long part_idx = 0)
@@ -1472,12 +1474,18 @@ __device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const Tma
             const double Td0 = t_per_plane ? Tp : (t_arr ? T0 : temp_cell(p, a.d.T, a.d.T32, c, j, k, ts));
             Real cen0, cl0, fs0;
             int g0, br0;
-            if constexpr (sizeof(Real) == 4 && TA) {
+            // TM 2: the plane temperature's terms of fs_update's FP32 form
+            const float dTp = TM == 2 ? (float)(Tp - p.Tliq) : 0.f;
+            const bool offp = TM == 2 && (Tp < 1.0 || Tp > p.Tliq);
+            if constexpr (sizeof(Real) == 4 && TM == 1) {
                 // the FP32 temperature array straight into the FP32 update
                 float dT;
                 bool off;
                 am_dt(q, (float)Tn0, dT, off);
                 fs_update_f32(q, p, zc_cl.x, zc_fs.x, nb0, oce.x, grc.x, dT, off, a.d.curv, c, cen0, cl0, fs0, g0, br0);
+            } else if constexpr (sizeof(Real) == 4 && TM == 2) {
+                fs_update_f32(q, p, zc_cl.x, zc_fs.x, nb0, oce.x, grc.x, dTp, offp, a.d.curv, c, cen0, cl0, fs0, g0,
+                              br0);
             } else {
                 fs_update<Real>(q, p, zc_cl.x, zc_fs.x, nb0, oce.x, grc.x, Td0, a.d.curv, c, cen0, cl0, fs0, g0, br0);
             }
@@ -1488,12 +1496,15 @@ __device__ __forceinline__ bool stencil_tile_pair(const KernelArgs &a, const Tma
                 const double Td1 = t_per_plane ? Tp : (t_arr ? T1 : temp_cell(p, a.d.T, a.d.T32, c + 1, j, k, ts));
                 Real cen1, cl1, fs1;
                 int g1, br1;
-                if constexpr (sizeof(Real) == 4 && TA) {
+                if constexpr (sizeof(Real) == 4 && TM == 1) {
                     float dT;
                     bool off;
                     am_dt(q, (float)Tn1, dT, off);
                     fs_update_f32(q, p, zc_cl.y, zc_fs.y, nb1, oce.y, grc.y, dT, off, a.d.curv, c + 1, cen1, cl1, fs1,
                                   g1, br1);
+                } else if constexpr (sizeof(Real) == 4 && TM == 2) {
+                    fs_update_f32(q, p, zc_cl.y, zc_fs.y, nb1, oce.y, grc.y, dTp, offp, a.d.curv, c + 1, cen1, cl1,
+                                  fs1, g1, br1);
                 } else {
                     fs_update<Real>(q, p, zc_cl.y, zc_fs.y, nb1, oce.y, grc.y, Td1, a.d.curv, c + 1, cen1, cl1, fs1,
                                     g1, br1);
@@ -1579,9 +1590,15 @@ __device__ __forceinline__ bool run_tile(const KernelArgs &a, const TmaMaps &map
                                          double *part = nullptr, long long part_idx = 0)
 {
     if constexpr (CPT == 2 && sizeof(Real) == 4)
-        return a.p.temp_mode == 2
-                   ? stencil_tile_pair<Real, true>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx)
-                   : stencil_tile_pair<Real, false>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
+    {
+        // the tile's temperature form (the same test as stencil_tile_pair's
+        // t_per_plane)
+        if (a.p.temp_mode == 2)
+            return stencil_tile_pair<Real, 1>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
+        if (a.p.temp_mode == 0 || (a.p.temp_mode == 1 && !a.p.gz_is_one))
+            return stencil_tile_pair<Real, 2>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
+        return stencil_tile_pair<Real, 0>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
+    }
     else
         return stencil_tile<Real, CPT>(a, maps, zchunk, bx, by, bz, smem, sh, ring, part, part_idx);
 }
