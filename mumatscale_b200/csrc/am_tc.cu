@@ -51,9 +51,9 @@
 //                other 16 columns
 // Stages of two K-steps (32 nodes; the last stage of a tile holds the one
 // K-step left of 25) circulate in a shared-memory ring: seven of 32 KB with
-// N = 128, four of 48 KB with N = 256.  A stage costs each role a fixed handshake (a barrier wait, index
-// arithmetic, a commit or an arrival) of several hundred cycles, so the
-// stages are as large as the ring allows.  With N = 128 the 512
+// N = 128, four of 48 KB with N = 256.  A stage costs each role a fixed
+// handshake (a barrier wait, index arithmetic, a commit or an arrival) of
+// several hundred cycles, so the stages are as large as the ring allows.  With N = 128 the 512
 // tensor-memory columns hold two sets of accumulators, so a tile's epilogue
 // runs while the next tile accumulates; with N = 256 one set fills them.
 //
